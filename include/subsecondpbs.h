@@ -1,0 +1,258 @@
+/*
+ * subsecondpbs.h - plain C ABI of the B200 pencil-beam dose library
+ * (libsubsecondpbs_b200.so).
+ *
+ * Every entry point takes plain pointers and sizes, so ctypes, cffi or any
+ * C-compatible FFI can bind it directly. The C++ drop-in face that keeps the
+ * reference's struct-based signature lives in raytracedicom_integration.h and is
+ * implemented on top of these functions.
+ *
+ * Reference interfaces replaced (paths within Nelgcis/subsecondPBS):
+ *   subsecondWrapper            include/core/raytracedicom_integration.h:132-139,
+ *                               src/core/raytracedicom_wrapper.cu:2446-5661
+ *   RTDBeamSettings             include/core/raytracedicom_integration.h:31-97
+ *   RTDEnergyStruct             include/core/raytracedicom_integration.h:99-128
+ *   cudaCalDoseRTD.raytracedicom_wrapper (pybind)
+ *                               src/bindings/raytracedicom_pybind.cpp:1679-1871,2057-2086
+ *
+ * Error behaviour: the reference prints to stderr and returns silently on
+ * invalid input (raytracedicom_wrapper.cu:1025-1157), throws std::runtime_error on
+ * geometry failures (raytracedicom_wrapper.cu:3084,3177,3418) and exit(1)s on CUDA
+ * errors (common.cuh:14-20). Here every failure is a non-zero status code with a
+ * message available from pbs_last_error(); nothing exits the process.
+ */
+#ifndef SUBSECONDPBS_H
+#define SUBSECONDPBS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PBS_API __attribute__((visibility("default")))
+#else
+#define PBS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define PBS_OK 0
+#define PBS_ERR_INVALID_ARGUMENT 1 /* input validation (reference: stderr + return) */
+#define PBS_ERR_GEOMETRY 2         /* beam geometry cannot be planned (reference: throw) */
+#define PBS_ERR_CUDA 3             /* CUDA runtime error (reference: exit(1)) */
+#define PBS_ERR_OUT_OF_MEMORY 4    /* device allocation failed or budget exceeded */
+#define PBS_ERR_UNSUPPORTED 5      /* requested mode is not available */
+#define PBS_ERR_NOT_READY 6        /* context is missing CT, tables or dose grid */
+#define PBS_ERR_TIMEOUT 7          /* a bounded device wait gave up */
+
+/* ---- CT input interpretation (reference: RTD_CT_INPUT_TYPE, wrapper.cu:2280-2441) */
+#define PBS_CT_AUTO 0
+#define PBS_CT_HU 1
+#define PBS_CT_HU_PLUS_1000 2
+#define PBS_CT_DENSITY 3
+#define PBS_CT_SPR 4
+
+/* ---- context options ---------------------------------------------------- */
+/* Reproduce the reference's BEV depth indexing in the per-layer transfer: the
+ * reference stores BEV planes at absolute tracer steps but samples them shifted by
+ * the beam's first-inside step (wrapper.cu:5308-5313 vs 5392-5394). Default 0:
+ * planes are sampled where they were written (upstream RayTraceDicom behaviour). */
+#define PBS_OPT_COMPAT_BEV_Z_SHIFT 1
+/* Record CUDA events around each pipeline stage (read with pbs_context_stage_times). */
+#define PBS_OPT_STAGE_TIMING 2
+/* Device memory budget in MiB for the per-layer IDD/sigma working set (layers are
+ * processed in chunks that fit). Default 2048. */
+#define PBS_OPT_LAYER_BUDGET_MIB 3
+/* Forced CT interpretation (PBS_CT_*); default PBS_CT_AUTO, overridden by the
+ * RTD_CT_INPUT_TYPE environment variable when set. */
+#define PBS_OPT_CT_INPUT_TYPE 4
+/* Keep intermediate per-layer buffers of the last beam for pbs_context_debug_copy. */
+#define PBS_OPT_KEEP_DEBUG 5
+
+/* ---- stage timer slots -------------------------------------------------- */
+#define PBS_STAGE_TRACE 0
+#define PBS_STAGE_PLAN 1
+#define PBS_STAGE_CONV 2
+#define PBS_STAGE_IDD 3
+#define PBS_STAGE_BIN 4
+#define PBS_STAGE_SUPERPOSE 5
+#define PBS_STAGE_TRANSFER 6
+#define PBS_STAGE_COUNT 7
+
+/* ---- debug buffers (pbs_context_debug_copy) ----------------------------- */
+#define PBS_DBG_DENSITY 1     /* float [steps][rayY][rayX]  BEV density            */
+#define PBS_DBG_WEPL 2        /* float [steps][rayY][rayX]  cumulative WEPL (mm)   */
+#define PBS_DBG_FIRST_INSIDE 3  /* int [rayY][rayX]                                */
+#define PBS_DBG_FIRST_OUTSIDE 4 /* int [rayY][rayX]                                */
+#define PBS_DBG_WEPL_MIN 5    /* float [steps]                                      */
+#define PBS_DBG_RAY_WEIGHTS 6 /* float [layers][rayY][rayX]                         */
+#define PBS_DBG_IDD 7         /* float [steps][superpY][superpX] for `layer` (0 outside [first, afterLast)) */
+#define PBS_DBG_RSIGMA 8      /* float [steps][superpY][superpX] for `layer` (+inf outside)                */
+#define PBS_DBG_TILE_BINS 9   /* uint8 [steps][tilesY][tilesX] for `layer`: bit7 live, bits0-6 radius bucket */
+#define PBS_DBG_BEV_DOSE 10   /* float [steps][superpY+64][superpX+64], layer-summed, absolute step index */
+#define PBS_DBG_DOSE64 11     /* double [Z][Y][X] accumulated dose                   */
+#define PBS_DBG_FIRST_PASSIVE 12 /* int [rayY][rayX] for `layer`                    */
+
+/* Mirrors RTDBeamSettings (include/core/raytracedicom_integration.h:31-97). Array
+ * members carry their element counts (floats/ints, not rows) so the reference's
+ * size validation (wrapper.cu:1099-1157) can be reproduced. NULL/0 = absent. */
+typedef struct PbsBeamDesc {
+    const float* energies;             size_t n_energies;              /* [L] MeV/u            */
+    const float* spot_sigmas;          size_t n_spot_sigmas;           /* [L][2] sigma x,y     */
+    float ray_spacing[2];
+    unsigned int steps;
+    float source_dist[2];
+    float spot_offset[3];
+    float spot_delta[3];
+    int max_subspots_per_layer;
+    const float* subspot_data;         size_t n_subspot_data;          /* [L][M][5]            */
+    const int* layer_spot_counts;      size_t n_layer_spot_counts;     /* [L]                  */
+    const float* spot_positions;       size_t n_spot_positions;        /* [N][2]               */
+    int spot_positions_are_indices;
+    const float* spot_weights;         size_t n_spot_weights;          /* [N]                  */
+    const float* spot_beam_directions; size_t n_spot_beam_directions;  /* [N][3]               */
+    const float* layer_longitudinal_cutoffs; size_t n_layer_longitudinal_cutoffs; /* [L]       */
+    const float* water_equivalence;    size_t n_water_equivalence;     /* 9 header + body      */
+    const float* ray_weq_header;       size_t n_ray_weq_header;        /* 9                    */
+    const float* profile_data;         size_t n_profile_data;
+    const float* profile_setting;      size_t n_profile_setting;
+    const float* beam_para_data;       size_t n_beam_para_data;
+    float beam_direction[3];
+    float bm_x_direction[3];
+    float bm_y_direction[3];
+    float source_position[3];
+    float sad;
+    float ref_plane_z;
+    const int* roi_linear_indices;     size_t n_roi_linear_indices;
+} PbsBeamDesc;
+
+/* Mirrors RTDEnergyStruct (include/core/raytracedicom_integration.h:99-128). */
+typedef struct PbsEnergyDesc {
+    int n_energy_samples;
+    int n_energies;
+    const float* energies_per_u;    size_t n_energies_per_u;
+    const float* peak_depths;       size_t n_peak_depths;
+    const float* scale_facts;       size_t n_scale_facts;
+    const float* cidd_matrix;       size_t n_cidd_matrix;     /* [nEnergies][nEnergySamples] */
+    int n_density_samples;
+    float density_scale_fact;
+    const float* density_vector;    size_t n_density_vector;
+    int n_sp_samples;
+    float sp_scale_fact;
+    const float* sp_vector;         size_t n_sp_vector;
+    int n_rrl_samples;
+    float rrl_scale_fact;
+    const float* rrl_vector;        size_t n_rrl_vector;
+    const float* nuc_weight_matrix;   size_t n_nuc_weight_matrix;   /* [nEnergies][nEnergySamples] */
+    const float* nuc_sq_sigma_matrix; size_t n_nuc_sq_sigma_matrix; /* [nEnergies][nEnergySamples] */
+    int nuclear_tables_aligned_to_primary_axis;
+} PbsEnergyDesc;
+
+/* Integer/float plan of the last beam added to a context. */
+typedef struct PbsBeamStats {
+    int num_layers;
+    int conv_mode;            /* 0 raw spot lattice (wrapper.cu:3733), 1 legacy CPB (3454) */
+    int ray_dims[2];
+    int superp_dims[2];
+    int tracer_steps;
+    int lattice_dims[2];
+    float lattice_delta[2];
+    float lattice_offset[2];
+    float cpb_corner[2];
+    float cpb_resolution[2];
+    float fan_corner[3];
+    float fan_delta[3];
+    float source_dist[2];
+    float len_to_mm;
+    float energy_depth_to_mm;
+    float max_peak_depth_mm;
+    int first_inside;         /* beam min of per-ray first-inside step          */
+    int first_outside;        /* beam max of per-ray first-outside step         */
+    int guaranteed_passive;   /* min(first step past 1.05*max peak, first_outside) */
+    int transfer_start[3];
+    int transfer_max[3];
+    long long live_tiles;     /* superposed (tile, step) pairs over all layers   */
+    long long superpose_fma;  /* sum over live tiles of 256*(2R+1)^2             */
+} PbsBeamStats;
+
+typedef struct PbsLayerStats {
+    float energy_idx;         /* fractional LUT row (wrapper.cu:3926-3997)       */
+    float energy_scale_fact;  /* WEPL mm -> LUT depth index                      */
+    float peak_depth;         /* mm                                              */
+    float entry_sigma[2];     /* mm at the entry plane (wrapper.cu:3830-3833)    */
+    int after_last_step;      /* wrapper.cu:4302-4304                            */
+    int max_first_passive;
+    int calc_passive;         /* wrapper.cu:4975-4990                            */
+    int tile_rad_counts[34];  /* histogram before overflow merge                 */
+    int batched_counts[33];   /* complete_superposition.cu:476-483               */
+    int live_tiles;
+} PbsLayerStats;
+
+/* ---- library ------------------------------------------------------------ */
+PBS_API const char* pbs_version(void);
+PBS_API const char* pbs_last_error(void);
+PBS_API int pbs_device_count(int* count);
+
+/* One-shot pipeline with the reference's semantics: dose_data is read, the dose
+ * of every beam is accumulated into it and it is written back. Host pointers. */
+PBS_API int pbs_subsecond_wrapper(const float* ct_data, const int ct_dims[3], const float ct_resolution[3],
+                          const float ct_corner[3], float* dose_data, const int dose_dims[3],
+                          const float dose_resolution[3], const float dose_corner[3],
+                          const PbsBeamDesc* beams, size_t num_beams, const PbsEnergyDesc* energy,
+                          int gpu_id, int nuclear_correction, int verbose);
+
+/* Host-side planning of one beam only (no device work): validation, gantry frame,
+ * spot lattice, ray grid, tracer steps and per-layer energy parameters. Fills the
+ * host-known fields of `out` (device-derived fields are left 0). When
+ * `layer_params` is not NULL it receives [L][8] floats per layer: energy_idx,
+ * energy_scale_fact, peak_depth, conv_peak_depth, sigma_sq_air_quad,
+ * sigma_sq_air_lin, sigma_x_mm, sigma_y_mm. When `lattice` is not NULL and
+ * `lattice_len` equals L*ny*nx it receives the dense spot-weight lattice. */
+PBS_API int pbs_plan_beam(const PbsBeamDesc* beam, const PbsEnergyDesc* energy, const int ct_dims[3],
+                          const float ct_resolution[3], const float ct_corner[3], const int dose_dims[3],
+                          const float dose_resolution[3], const float dose_corner[3], PbsBeamStats* out,
+                          float* layer_params, float* lattice, size_t lattice_len);
+
+/* ---- resident context (serving, benchmarking, multi-beam plans) --------- */
+typedef struct PbsContext PbsContext;
+
+PBS_API int pbs_context_create(int gpu_id, PbsContext** out);
+PBS_API int pbs_context_destroy(PbsContext* ctx);
+PBS_API int pbs_context_set_option(PbsContext* ctx, int option, long long value);
+/* Upload the lookup tables (kept resident until replaced). */
+PBS_API int pbs_context_set_energy(PbsContext* ctx, const PbsEnergyDesc* energy);
+/* Upload (ct_on_device=0) or adopt a copy of (ct_on_device=1) a float CT
+ * [Z][Y][X]; converted to HU+1000 on the device and kept resident. */
+PBS_API int pbs_context_set_ct(PbsContext* ctx, const float* ct, int ct_on_device, const int dims[3],
+                       const float resolution[3], const float corner[3]);
+/* Define the dose grid; allocates the FP64 accumulator. */
+PBS_API int pbs_context_set_dose_grid(PbsContext* ctx, const int dims[3], const float resolution[3],
+                              const float corner[3]);
+/* Reset the accumulator to `initial` (float [Z][Y][X], host or device) or to 0. */
+PBS_API int pbs_context_reset_dose(PbsContext* ctx, const float* initial, int initial_on_device);
+/* Plan the beam on the host and enqueue its whole pipeline on the context stream.
+ * Returns without waiting for the device. */
+PBS_API int pbs_context_add_beam(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction);
+/* Convert the accumulator to float and copy it out (host or device pointer). */
+PBS_API int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device);
+PBS_API int pbs_context_synchronize(PbsContext* ctx);
+/* cudaStream_t the context enqueues on. */
+PBS_API void* pbs_context_stream(PbsContext* ctx);
+/* Device pointer of the FP64 accumulator [Z][Y][X]. */
+PBS_API void* pbs_context_dose_device_ptr(PbsContext* ctx);
+/* Stats of the last beam (synchronizes the context stream). */
+PBS_API int pbs_context_beam_stats(PbsContext* ctx, PbsBeamStats* out);
+PBS_API int pbs_context_layer_stats(PbsContext* ctx, int layer, PbsLayerStats* out);
+/* Milliseconds per stage (PBS_STAGE_*) of the last beam; needs PBS_OPT_STAGE_TIMING. */
+PBS_API int pbs_context_stage_times(PbsContext* ctx, float* ms, int n);
+/* Copy an intermediate buffer of the last beam (PBS_DBG_*) to host memory;
+ * needs PBS_OPT_KEEP_DEBUG for the per-layer buffers. */
+PBS_API int pbs_context_debug_copy(PbsContext* ctx, int which, int layer, void* host_out, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUBSECONDPBS_H */

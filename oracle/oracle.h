@@ -1,0 +1,99 @@
+/*
+ * CPU oracle of the pencil-beam dose path (test infrastructure only).
+ *
+ * A plain-C restatement of the reference pipeline behind subsecondWrapper
+ * (src/core/raytracedicom_wrapper.cu:2446-5661): CT adapter, beam geometry and
+ * ray grid, BEV ray tracing, beam reductions, spot->ray convolution (both fluence
+ * modes), IDD/sigma, tile radius binning and batching, tile superposition and the
+ * per-layer divergent transfer. Geometry and every integer decision use IEEE
+ * single precision in the reference's operand order (so ray grids, step counts,
+ * cut-off steps, radius buckets and transfer boxes are reproduced exactly); all
+ * dose arithmetic (sampling, cumulative sums, erf weights, superposition,
+ * accumulation) is double precision. Layers are transferred one at a time into
+ * the dose grid exactly as the reference does.
+ *
+ * The oracle is the checker of the CUDA library, never a fallback for it.
+ */
+#ifndef PBS_ORACLE_H
+#define PBS_ORACLE_H
+
+#include <stddef.h>
+
+#include "../include/subsecondpbs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OraclePlan {
+    int num_layers;
+    int conv_mode;
+    int ray_x, ray_y;
+    int pitch_x, pitch_y;
+    int tiles_x, tiles_y;
+    int steps;
+    int lat_nx, lat_ny;
+    float lat_dx, lat_dy, lat_ox, lat_oy;
+    float cpb_corner[2], cpb_res[2];
+    float fan_corner[3], fan_delta[3];
+    float source_dist[2];
+    float len_to_mm, energy_depth_to_mm, max_peak_depth_mm;
+    int bev_x, bev_y;
+} OraclePlan;
+
+/* Optional captures of the last beam; every pointer may be NULL. Sizes use the
+ * OraclePlan of the beam (rays = ray_x*ray_y, pad = pitch_x*pitch_y,
+ * tiles = tiles_x*tiles_y, S = steps, L = num_layers). */
+typedef struct OracleCapture {
+    double* density;        /* [S][rays]                                   */
+    double* wepl;           /* [S][rays]                                   */
+    int* first_inside;      /* [rays]                                      */
+    int* first_outside;     /* [rays]                                      */
+    double* wepl_min;       /* [S]                                         */
+    int* beam_ints;         /* [4]: first_inside, first_outside, guaranteed_passive, max_calc_passive */
+    double* ray_weights;    /* [L][rays]                                   */
+    float* entry_sigma;     /* [L][2]                                      */
+    double* idd;            /* [L][S][pad] (0 outside the computed range)  */
+    double* rsigma;         /* [L][S][pad] (+inf outside)                  */
+    unsigned char* codes;   /* [L][S][tiles]: bit7 live, bits0-5 bucket; 0xff outside */
+    int* layer_ints;        /* [L][8]: after_last, max_first_passive, calc_passive, live_tiles, tx0,ty0,tz0 start (3) */
+    int* layer_box;         /* [L][6]: transfer start xyz, max xyz        */
+    int* hist;              /* [L][34] before overflow merge               */
+    int* batched;           /* [L][33]                                     */
+    double* bev;            /* [S][bev_y][bev_x] layer-summed, absolute step */
+    double superpose_fma;   /* out: sum over live tiles of 256*(2R+1)^2     */
+} OracleCapture;
+
+/* Host plan of one beam (no dose work). `layer_params` ([L][8], may be NULL)
+ * receives energy_idx, energy_scale_fact, peak_depth, conv_peak_depth,
+ * sigma_sq_air_quad, sigma_sq_air_lin, sigma_x_mm, sigma_y_mm. `lattice`
+ * ([L][ny][nx], may be NULL, `lattice_len` floats) receives the dense spot lattice.
+ * Returns PBS_OK or a PBS_ERR_* code; oracle_last_error() has the message. */
+int oracle_plan(const PbsBeamDesc* beam, const PbsEnergyDesc* energy, const int ct_dims[3],
+                const float ct_res[3], const float ct_corner[3], const int dose_dims[3],
+                const float dose_res[3], const float dose_corner[3], OraclePlan* out, float* layer_params,
+                float* lattice, size_t lattice_len);
+
+/* Full pipeline: accumulates the dose of every beam into `dose` (double
+ * [Z][Y][X], read and written). `ct_type` is a PBS_CT_* value (PBS_CT_AUTO
+ * detects it as the reference does). `capture` (may be NULL) receives the
+ * intermediate arrays of the last beam. `threads` <= 0 uses all cores. */
+int oracle_dose(const float* ct, const int ct_dims[3], const float ct_res[3], const float ct_corner[3],
+                double* dose, const int dose_dims[3], const float dose_res[3], const float dose_corner[3],
+                const PbsBeamDesc* beams, size_t num_beams, const PbsEnergyDesc* energy, int ct_type,
+                int compat_bev_z_shift, int threads, OracleCapture* capture);
+
+/* Tile radius bucket from a tile's minimum rSigmaEff (complete_superposition.cu:242). */
+int oracle_radius_bucket(float min_rsigma);
+
+/* Batching of a 34-bucket histogram (complete_superposition.cu:412-490): fills
+ * batched[33] and map[34] (bucket -> processing radius). */
+void oracle_batch(const int hist_in[34], int batched[33], int map[34]);
+
+const char* oracle_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PBS_ORACLE_H */

@@ -1,0 +1,745 @@
+// Resident dose context: device-resident lookup tables, CT and FP64 dose grid, and
+// the per-beam launch sequence. A beam is planned on the host and then runs as one
+// asynchronous sequence of kernels on the context stream with no host round trip:
+// every trace-dependent decision (entry step, cut-off steps, passive steps, tile
+// radii, batching, transfer box) is made on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "kernels.h"
+#include "plan.h"
+
+namespace pbs {
+
+namespace {
+thread_local std::string g_lastError;
+}
+
+void set_error(const std::string& msg) { g_lastError = msg; }
+const char* last_error() { return g_lastError.c_str(); }
+
+static int cuda_fail(cudaError_t e, const char* where) {
+    set_error(std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? PBS_ERR_OUT_OF_MEMORY : PBS_ERR_CUDA;
+}
+
+#define PBS_CUDA(call, where)                     \
+    do {                                          \
+        cudaError_t e_ = (call);                  \
+        if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+    } while (0)
+
+int DevBuf::ensure(size_t b) {
+    if (b <= bytes) return PBS_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    if (b == 0) return PBS_OK;
+    cudaError_t e = cudaMalloc(&ptr, b);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    bytes = b;
+    return PBS_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+int PinnedBuf::ensure(size_t b) {
+    if (b <= bytes) return PBS_OK;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&ptr, b);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return cuda_fail(e, "cudaMallocHost");
+    }
+    bytes = b;
+    return PBS_OK;
+}
+
+void PinnedBuf::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+Context::~Context() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
+                      &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
+                      &work, &lp, &ls, &bs, &stats})
+        b->release();
+    staging.release();
+    if (stagingEvent) cudaEventDestroy(stagingEvent);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Context::init(int gpu) {
+    device = gpu;
+    int n = 0;
+    PBS_CUDA(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+    if (gpu < 0 || gpu >= n) {
+        set_error("gpu_id " + std::to_string(gpu) + " out of range (" + std::to_string(n) + " devices)");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    PBS_CUDA(cudaSetDevice(gpu), "cudaSetDevice");
+    PBS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    PBS_CUDA(cudaEventCreateWithFlags(&stagingEvent, cudaEventDisableTiming), "cudaEventCreate");
+    for (auto& e : ev) PBS_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    return PBS_OK;
+}
+
+// Copies `n` host bytes to the device through the pinned staging buffer so the
+// copy is asynchronous with respect to earlier work on the stream.
+int Context::upload(void* dst, const void* src, size_t n) {
+    if (n == 0) return PBS_OK;
+    PBS_CUDA(cudaEventSynchronize(stagingEvent), "cudaEventSynchronize");
+    int rc = staging.ensure(n);
+    if (rc) return rc;
+    std::memcpy(staging.ptr, src, n);
+    PBS_CUDA(cudaMemcpyAsync(dst, staging.ptr, n, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+    PBS_CUDA(cudaEventRecord(stagingEvent, stream), "cudaEventRecord");
+    return PBS_OK;
+}
+
+int Context::set_energy(const PbsEnergyDesc& e) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!(e.n_energies > 0 && e.n_energy_samples > 0) || !e.energies_per_u || !e.peak_depths || !e.scale_facts ||
+        !e.cidd_matrix || e.n_energies_per_u != size_t(e.n_energies) || e.n_peak_depths != size_t(e.n_energies) ||
+        e.n_scale_facts != size_t(e.n_energies) ||
+        e.n_cidd_matrix != size_t(e.n_energies) * size_t(e.n_energy_samples)) {
+        set_error("[RTD_ENTRY_ASSERT] energy table dimensions are inconsistent");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (!e.density_vector || !e.sp_vector || !e.rrl_vector || e.n_density_samples <= 0 || e.n_sp_samples <= 0 ||
+        e.n_rrl_samples <= 0 || size_t(e.n_density_samples) > e.n_density_vector ||
+        size_t(e.n_sp_samples) > e.n_sp_vector || size_t(e.n_rrl_samples) > e.n_rrl_vector) {
+        set_error("[RTD_ENTRY_ASSERT] density, stopping-power, and radiation-length LUTs are inconsistent");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    energiesPerU.assign(e.energies_per_u, e.energies_per_u + e.n_energies);
+    peakDepths.assign(e.peak_depths, e.peak_depths + e.n_energies);
+    scaleFacts.assign(e.scale_facts, e.scale_facts + e.n_energies);
+    ciddHost.assign(e.cidd_matrix, e.cidd_matrix + e.n_cidd_matrix);
+    densityHost.assign(e.density_vector, e.density_vector + e.n_density_vector);
+    spHost.assign(e.sp_vector, e.sp_vector + e.n_sp_vector);
+    rrlHost.assign(e.rrl_vector, e.rrl_vector + e.n_rrl_vector);
+    energy = e;
+    energy.energies_per_u = energiesPerU.data();
+    energy.peak_depths = peakDepths.data();
+    energy.scale_facts = scaleFacts.data();
+    energy.cidd_matrix = ciddHost.data();
+    energy.density_vector = densityHost.data();
+    energy.sp_vector = spHost.data();
+    energy.rrl_vector = rrlHost.data();
+    energy.nuc_weight_matrix = nullptr;
+    energy.n_nuc_weight_matrix = 0;
+    energy.nuc_sq_sigma_matrix = nullptr;
+    energy.n_nuc_sq_sigma_matrix = 0;
+    int rc;
+    if ((rc = cidd.ensure(ciddHost.size() * 4)) || (rc = density.ensure(densityHost.size() * 4)) ||
+        (rc = sp.ensure(spHost.size() * 4)) || (rc = rrl.ensure(rrlHost.size() * 4)))
+        return rc;
+    PBS_CUDA(cudaMemcpyAsync(cidd.ptr, ciddHost.data(), ciddHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
+    PBS_CUDA(cudaMemcpyAsync(density.ptr, densityHost.data(), densityHost.size() * 4, cudaMemcpyHostToDevice, stream),
+             "LUT");
+    PBS_CUDA(cudaMemcpyAsync(sp.ptr, spHost.data(), spHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
+    PBS_CUDA(cudaMemcpyAsync(rrl.ptr, rrlHost.data(), rrlHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    luts.cidd = static_cast<const float*>(cidd.ptr);
+    luts.nS = e.n_energy_samples;
+    luts.nE = e.n_energies;
+    luts.density = static_cast<const float*>(density.ptr);
+    luts.nDensity = e.n_density_samples;
+    luts.densityScale = e.density_scale_fact;
+    luts.sp = static_cast<const float*>(sp.ptr);
+    luts.nSp = e.n_sp_samples;
+    luts.spScale = e.sp_scale_fact;
+    luts.rrl = static_cast<const float*>(rrl.ptr);
+    luts.nRrl = e.n_rrl_samples;
+    luts.rrlScale = e.rrl_scale_fact;
+    hasEnergy = true;
+    return PBS_OK;
+}
+
+int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!data || g.dims[0] <= 0 || g.dims[1] <= 0 || g.dims[2] <= 0 ||
+        !(g.res[0] > 0.0f && g.res[1] > 0.0f && g.res[2] > 0.0f)) {
+        set_error("[RTD_ENTRY_ASSERT] CT grid must have positive dims and resolution");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
+    int rc = ct.ensure(n * 4);
+    if (rc) return rc;
+    int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
+    if (onDevice) {
+        PBS_CUDA(cudaMemcpyAsync(ct.ptr, data, n * 4, cudaMemcpyDeviceToDevice, stream), "CT D2D");
+        if (type == PBS_CT_AUTO) {
+            rc = stats.ensure(64);
+            if (rc) return rc;
+            PBS_CUDA(launch_ct_stats(static_cast<float*>(ct.ptr), n, static_cast<float*>(stats.ptr), stream), "ct_stats");
+            float mm[2];
+            PBS_CUDA(cudaMemcpyAsync(mm, stats.ptr, 8, cudaMemcpyDeviceToHost, stream), "CT stats");
+            PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+            type = auto_detect_ct_type(mm[0], mm[1]);
+        }
+    } else {
+        if (type == PBS_CT_AUTO) {
+            float mn, mx;
+            sample_ct_stats(data, n, mn, mx);
+            type = auto_detect_ct_type(mn, mx);
+        }
+        PBS_CUDA(cudaMemcpyAsync(ct.ptr, data, n * 4, cudaMemcpyHostToDevice, stream), "CT H2D");
+    }
+    if (type == PBS_CT_DENSITY || type == PBS_CT_SPR) {
+        if (!hasEnergy) {
+            set_error("[CT_ADAPTER] density/SPR CT needs the lookup tables; call set_energy first");
+            return PBS_ERR_NOT_READY;
+        }
+        const bool useDensity = type == PBS_CT_DENSITY;
+        const float scale = useDensity ? energy.density_scale_fact : energy.sp_scale_fact;
+        const int lutN = int(useDensity ? densityHost.size() : spHost.size());
+        if (lutN == 0 || scale == 0.0f) {
+            set_error("[CT_ADAPTER] LUT is empty or scale factor is 0; cannot convert");
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+        PBS_CUDA(launch_ct_convert(static_cast<float*>(ct.ptr), n, type,
+                                   static_cast<const float*>(useDensity ? density.ptr : sp.ptr), lutN, scale, stream),
+                 "ct_convert");
+    } else {
+        PBS_CUDA(launch_ct_convert(static_cast<float*>(ct.ptr), n, type, nullptr, 0, 1.0f, stream), "ct_convert");
+    }
+    ctType = type;
+    ctGrid = g;
+    hasCt = true;
+    return PBS_OK;
+}
+
+int Context::set_dose_grid(const GridDesc& g) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (g.dims[0] <= 0 || g.dims[1] <= 0 || g.dims[2] <= 0 ||
+        !(g.res[0] > 0.0f && g.res[1] > 0.0f && g.res[2] > 0.0f)) {
+        set_error("[RTD_ENTRY_ASSERT] dose grid must have positive dims and resolution");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
+    int rc = dose64.ensure(n * 8);
+    if (rc) return rc;
+    doseGrid = g;
+    hasDose = true;
+    return reset_dose(nullptr, 0);
+}
+
+int Context::reset_dose(const float* init, int onDevice) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    const float* src = nullptr;
+    if (init) {
+        if (onDevice) {
+            src = init;
+        } else {
+            int rc = floatOut.ensure(n * 4);
+            if (rc) return rc;
+            PBS_CUDA(cudaMemcpyAsync(floatOut.ptr, init, n * 4, cudaMemcpyHostToDevice, stream), "dose H2D");
+            src = static_cast<const float*>(floatOut.ptr);
+        }
+    }
+    PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), src, n, stream), "dose_init");
+    return PBS_OK;
+}
+
+int Context::read_dose(float* out, int onDevice) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    if (onDevice) {
+        PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), out, n, stream), "dose_to_float");
+        return PBS_OK;
+    }
+    int rc = floatOut.ensure(n * 4);
+    if (rc) return rc;
+    PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), static_cast<float*>(floatOut.ptr), n, stream),
+             "dose_to_float");
+    PBS_CUDA(cudaMemcpyAsync(out, floatOut.ptr, n * 4, cudaMemcpyDeviceToHost, stream), "dose D2H");
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    return PBS_OK;
+}
+
+int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!hasEnergy || !hasCt || !hasDose) {
+        set_error("context needs lookup tables, CT and dose grid before add_beam");
+        return PBS_ERR_NOT_READY;
+    }
+    if (nuclear) {
+        set_error("nuclear_correction=true requested, but this build has no nuclear halo tables loaded");
+        return PBS_ERR_UNSUPPORTED;
+    }
+    std::string err;
+    if (!validate_beam(b, 0, err)) {
+        set_error(err);
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    lastBeamValid = false;
+    int rc = plan_beam(b, energy, ctGrid, doseGrid, plan, err);
+    if (rc) {
+        set_error(err);
+        return rc;
+    }
+    const BeamPlan& P = plan;
+    BeamGeomDev& g = geom;
+    std::memset(&g, 0, sizeof(g));
+    g.tracer = P.tracer;
+    g.rayIdxToDoseIdx = P.rayIdxToDoseIdx;
+    g.rayX = P.rayDims[0];
+    g.rayY = P.rayDims[1];
+    g.pitchX = P.superpDims[0];
+    g.pitchY = P.superpDims[1];
+    g.tilesX = g.pitchX / kTileX;
+    g.tilesY = g.pitchY / kTileY;
+    g.steps = P.tracerSteps;
+    g.numLayers = P.numLayers;
+    g.maxPeakDepthMm = P.maxPeakDepthMm;
+    g.fanCorner = P.fanCorner;
+    g.fanDelta = P.fanDelta;
+    g.sourceDist = P.sourceDist;
+    g.volConst = P.volConst;
+    g.volLin = P.volLin;
+    g.volSq = P.volSq;
+    g.latNx = P.lattice.nx;
+    g.latNy = P.lattice.ny;
+    g.latDx = P.lattice.dx;
+    g.latDy = P.lattice.dy;
+    g.latOx = P.lattice.ox;
+    g.latOy = P.lattice.oy;
+    g.cpbCornerX = P.cpbCorner.x;
+    g.cpbCornerY = P.cpbCorner.y;
+    g.cpbResX = P.cpbRes.x;
+    g.cpbResY = P.cpbRes.y;
+    g.bevX = g.pitchX + 2 * kMaxR;
+    g.bevY = g.pitchY + 2 * kMaxR;
+    g.doseX = doseGrid.dims[0];
+    g.doseY = doseGrid.dims[1];
+    g.doseZ = doseGrid.dims[2];
+    g.compatBevZShift = compatBevZShift;
+
+    const int L = P.numLayers;
+    const size_t S = size_t(P.tracerSteps);
+    const size_t rays = size_t(g.rayX) * g.rayY;
+    const size_t padPlane = size_t(g.pitchX) * g.pitchY;
+    const size_t tiles = size_t(g.tilesX) * g.tilesY;
+    const size_t perLayer = S * padPlane * 8 + S * tiles * (1 + sizeof(int4));
+    const size_t budget = size_t(std::max<long long>(layerBudgetMiB, 1)) << 20;
+    int chunk = int(std::max<size_t>(1, std::min<size_t>(budget / std::max<size_t>(perLayer, 1), size_t(L))));
+    chunk = std::min(chunk, 64);
+    chunkLayers = chunk;
+
+    if ((rc = dens.ensure(S * rays * 4)) || (rc = wepl.ensure(S * rays * 4)) || (rc = weplMin.ensure(S * 4)) ||
+        (rc = firstIn.ensure(rays * 4)) || (rc = firstOut.ensure(rays * 4)) || (rc = rayW.ensure(size_t(L) * rays * 4)) ||
+        (rc = bev.ensure(S * g.bevX * g.bevY * 4)) || (rc = codes.ensure(size_t(chunk) * S * tiles)) ||
+        (rc = work.ensure(size_t(chunk) * S * tiles * sizeof(int4))) ||
+        (rc = iddBuf.ensure(size_t(chunk) * S * padPlane * 4)) || (rc = rsBuf.ensure(size_t(chunk) * S * padPlane * 4)) ||
+        (rc = firstPassive.ensure(size_t(chunk) * rays * 4)) || (rc = lp.ensure(size_t(L) * sizeof(LayerParamsDev))) ||
+        (rc = ls.ensure(size_t(L) * sizeof(LayerStateDev))) || (rc = bs.ensure(sizeof(BeamStateDev))))
+        return rc;
+    if (keepDebug && chunk < L) {
+        set_error("PBS_OPT_KEEP_DEBUG needs every layer of the beam in one chunk; raise PBS_OPT_LAYER_BUDGET_MIB");
+        return PBS_ERR_OUT_OF_MEMORY;
+    }
+
+    // Host -> device inputs of the beam: layer parameters, initial beam state and
+    // the fluence source (dense spot lattice or legacy subspot table).
+    std::vector<LayerParamsDev> hlp(L);
+    for (int l = 0; l < L; ++l) {
+        const LayerHost& H = P.layers[l];
+        LayerParamsDev& d = hlp[l];
+        d.energyIdx = H.energyIdx;
+        d.energyScaleFact = H.energyScaleFact;
+        d.peakDepth = H.peakDepth;
+        d.rangeStopDepth = H.rangeStopDepth;
+        d.sigmaSqAirQuad = H.sigmaSqAirQuad;
+        d.sigmaSqAirLin = H.sigmaSqAirLin;
+        d.convPeakDepth = H.convPeakDepth;
+        d.sigmaXmm = H.sigmaXmm;
+        d.sigmaYmm = H.sigmaYmm;
+        d.spotDist = H.spotDist;
+    }
+    BeamStateDev hbs;
+    std::memset(&hbs, 0, sizeof(hbs));
+    hbs.firstInside = INT32_MAX;
+    hbs.firstOutside = INT32_MIN;
+    const size_t latBytes = P.hasLattice ? P.lattice.weights.size() * 4 : 0;
+    const size_t subBytes = P.hasLattice ? 0 : b.n_subspot_data * 4;
+    const size_t upBytes = hlp.size() * sizeof(LayerParamsDev) + sizeof(BeamStateDev) + latBytes + subBytes;
+    {
+        PBS_CUDA(cudaEventSynchronize(stagingEvent), "cudaEventSynchronize");
+        if ((rc = staging.ensure(upBytes + 256))) return rc;
+        char* p = static_cast<char*>(staging.ptr);
+        std::memcpy(p, hlp.data(), hlp.size() * sizeof(LayerParamsDev));
+        PBS_CUDA(cudaMemcpyAsync(lp.ptr, p, hlp.size() * sizeof(LayerParamsDev), cudaMemcpyHostToDevice, stream), "H2D");
+        p += hlp.size() * sizeof(LayerParamsDev);
+        std::memcpy(p, &hbs, sizeof(hbs));
+        PBS_CUDA(cudaMemcpyAsync(bs.ptr, p, sizeof(hbs), cudaMemcpyHostToDevice, stream), "H2D");
+        p += sizeof(hbs);
+        if (latBytes) {
+            if ((rc = lattice.ensure(latBytes)) || (rc = interm.ensure(size_t(L) * g.latNy * g.rayX * 4))) return rc;
+            std::memcpy(p, P.lattice.weights.data(), latBytes);
+            PBS_CUDA(cudaMemcpyAsync(lattice.ptr, p, latBytes, cudaMemcpyHostToDevice, stream), "H2D");
+        }
+        if (subBytes) {
+            if ((rc = subspots.ensure(subBytes)) || (rc = cpb.ensure(size_t(L) * rays * 4))) return rc;
+            std::memcpy(p, b.subspot_data, subBytes);
+            PBS_CUDA(cudaMemcpyAsync(subspots.ptr, p, subBytes, cudaMemcpyHostToDevice, stream), "H2D");
+        }
+        PBS_CUDA(cudaEventRecord(stagingEvent, stream), "cudaEventRecord");
+    }
+
+    LayerParamsDev* dlp = static_cast<LayerParamsDev*>(lp.ptr);
+    LayerStateDev* dls = static_cast<LayerStateDev*>(ls.ptr);
+    BeamStateDev* dbs = static_cast<BeamStateDev*>(bs.ptr);
+    float* dDens = static_cast<float*>(dens.ptr);
+    float* dWepl = static_cast<float*>(wepl.ptr);
+    int* dFi = static_cast<int*>(firstIn.ptr);
+    int* dFo = static_cast<int*>(firstOut.ptr);
+    float* dRayW = static_cast<float*>(rayW.ptr);
+    float* dBev = static_cast<float*>(bev.ptr);
+    auto mark = [&](int slot) -> int {
+        if (stageTiming) PBS_CUDA(cudaEventRecord(ev[slot], stream), "cudaEventRecord");
+        return PBS_OK;
+    };
+
+    PBS_CUDA(cudaMemsetAsync(dBev, 0, S * g.bevX * g.bevY * 4, stream), "memset BEV");
+    if ((rc = mark(0))) return rc;
+    PBS_CUDA(launch_trace(g, luts, static_cast<const float*>(ct.ptr), ctGrid.dims[0], ctGrid.dims[1], ctGrid.dims[2],
+                          dDens, dWepl, dFi, dFo, dbs, stream),
+             "trace");
+    PBS_CUDA(launch_wepl_min(g, dWepl, dFo, static_cast<float*>(weplMin.ptr), stream), "wepl_min");
+    if ((rc = mark(1))) return rc;
+    PBS_CUDA(launch_beam_planner(g, static_cast<const float*>(weplMin.ptr), dlp, dls, dbs, stream), "beam_planner");
+    if ((rc = mark(2))) return rc;
+    if (P.hasLattice) {
+        PBS_CUDA(launch_conv_lattice(g, static_cast<const float*>(lattice.ptr), static_cast<float*>(interm.ptr), dRayW,
+                                     dls, dbs, stream),
+                 "conv_lattice");
+    } else {
+        PBS_CUDA(launch_conv_cpb(g, static_cast<const float*>(subspots.ptr), b.max_subspots_per_layer,
+                                 static_cast<float*>(cpb.ptr), dRayW, stream),
+                 "conv_cpb");
+    }
+    if ((rc = mark(3))) return rc;
+    int smCount = 148;
+    cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
+    const int workCap = int(size_t(chunk) * S * tiles);
+    for (int l0 = 0; l0 < L; l0 += chunk) {
+        const int nl = std::min(chunk, L - l0);
+        PBS_CUDA(launch_idd(g, luts, l0, nl, dDens, dWepl, dFi, dFo, dRayW, dlp, dls, dbs,
+                            static_cast<float*>(iddBuf.ptr), static_cast<float*>(rsBuf.ptr),
+                            static_cast<uint8_t*>(codes.ptr), static_cast<int*>(firstPassive.ptr), stream),
+                 "idd");
+        if (l0 == 0 && (rc = mark(4))) return rc;
+        PBS_CUDA(launch_bin_plan(g, l0, nl, static_cast<const uint8_t*>(codes.ptr), dls, dbs,
+                                 static_cast<int4*>(work.ptr), workCap, stream),
+                 "bin_plan");
+        if (l0 == 0 && (rc = mark(5))) return rc;
+        PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
+                                  static_cast<const int4*>(work.ptr), dbs, dBev, smCount * 2, stream),
+                 "superpose");
+    }
+    if ((rc = mark(6))) return rc;
+    PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
+    PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
+    if ((rc = mark(7))) return rc;
+    lastBeamValid = true;
+    lastStageTimed = stageTiming != 0;
+    return PBS_OK;
+}
+
+int Context::beam_stats(PbsBeamStats* out) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!lastBeamValid) {
+        set_error("no beam has been added");
+        return PBS_ERR_NOT_READY;
+    }
+    BeamStateDev h;
+    PBS_CUDA(cudaMemcpyAsync(&h, bs.ptr, sizeof(h), cudaMemcpyDeviceToHost, stream), "stats D2H");
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    const BeamPlan& P = plan;
+    std::memset(out, 0, sizeof(*out));
+    out->num_layers = P.numLayers;
+    out->conv_mode = P.convMode;
+    out->ray_dims[0] = P.rayDims[0];
+    out->ray_dims[1] = P.rayDims[1];
+    out->superp_dims[0] = P.superpDims[0];
+    out->superp_dims[1] = P.superpDims[1];
+    out->tracer_steps = P.tracerSteps;
+    out->lattice_dims[0] = P.lattice.nx;
+    out->lattice_dims[1] = P.lattice.ny;
+    out->lattice_delta[0] = P.lattice.dx;
+    out->lattice_delta[1] = P.lattice.dy;
+    out->lattice_offset[0] = P.lattice.ox;
+    out->lattice_offset[1] = P.lattice.oy;
+    out->cpb_corner[0] = P.cpbCorner.x;
+    out->cpb_corner[1] = P.cpbCorner.y;
+    out->cpb_resolution[0] = P.cpbRes.x;
+    out->cpb_resolution[1] = P.cpbRes.y;
+    out->fan_corner[0] = P.fanCorner.x;
+    out->fan_corner[1] = P.fanCorner.y;
+    out->fan_corner[2] = P.fanCorner.z;
+    out->fan_delta[0] = P.fanDelta.x;
+    out->fan_delta[1] = P.fanDelta.y;
+    out->fan_delta[2] = P.fanDelta.z;
+    out->source_dist[0] = P.sourceDist.x;
+    out->source_dist[1] = P.sourceDist.y;
+    out->len_to_mm = P.lenToMm;
+    out->energy_depth_to_mm = P.energyDepthToMm;
+    out->max_peak_depth_mm = P.maxPeakDepthMm;
+    out->first_inside = h.firstInside;
+    out->first_outside = h.firstOutside;
+    out->guaranteed_passive = h.guaranteedPassive;
+    for (int i = 0; i < 3; ++i) {
+        out->transfer_start[i] = h.transferStart[i];
+        out->transfer_max[i] = h.transferMax[i];
+    }
+    out->live_tiles = h.liveTiles;
+    out->superpose_fma = h.superposeFma;
+    if (h.errorFlags) {
+        set_error("device reported an error flag (work list overflow)");
+        return PBS_ERR_CUDA;
+    }
+    return PBS_OK;
+}
+
+int Context::layer_stats(int layer, PbsLayerStats* out) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!lastBeamValid || layer < 0 || layer >= plan.numLayers) {
+        set_error("layer out of range or no beam");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    LayerStateDev h;
+    PBS_CUDA(cudaMemcpyAsync(&h, static_cast<LayerStateDev*>(ls.ptr) + layer, sizeof(h), cudaMemcpyDeviceToHost, stream),
+             "stats D2H");
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    const LayerHost& H = plan.layers[layer];
+    std::memset(out, 0, sizeof(*out));
+    out->energy_idx = H.energyIdx;
+    out->energy_scale_fact = H.energyScaleFact;
+    out->peak_depth = H.peakDepth;
+    out->entry_sigma[0] = h.entrySigmaX;
+    out->entry_sigma[1] = h.entrySigmaY;
+    out->after_last_step = h.afterLast;
+    out->max_first_passive = h.maxFirstPassive;
+    out->calc_passive = h.calcPassive;
+    for (int i = 0; i < kBuckets; ++i) out->tile_rad_counts[i] = h.hist[i];
+    for (int i = 0; i <= kMaxR; ++i) out->batched_counts[i] = h.batchedCounts[i];
+    out->live_tiles = h.liveTiles;
+    return PBS_OK;
+}
+
+int Context::stage_times(float* ms, int n) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!lastStageTimed) {
+        set_error("stage timing was not enabled for the last beam");
+        return PBS_ERR_NOT_READY;
+    }
+    PBS_CUDA(cudaEventSynchronize(ev[7]), "cudaEventSynchronize");
+    // Slots: 0 trace+wepl_min, 1 planner, 2 conv, 3 idd (first chunk), 4 bin (first chunk),
+    // 5 superposition (+ later chunks), 6 transfer.
+    const int map[PBS_STAGE_COUNT][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
+    for (int i = 0; i < n && i < PBS_STAGE_COUNT; ++i) {
+        float t = 0.f;
+        PBS_CUDA(cudaEventElapsedTime(&t, ev[map[i][0]], ev[map[i][1]]), "cudaEventElapsedTime");
+        ms[i] = t;
+    }
+    return PBS_OK;
+}
+
+int Context::debug_copy(int which, int layer, void* out, size_t bytes) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!lastBeamValid) {
+        set_error("no beam has been added");
+        return PBS_ERR_NOT_READY;
+    }
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    const size_t S = size_t(geom.steps), rays = size_t(geom.rayX) * geom.rayY;
+    const size_t padPlane = size_t(geom.pitchX) * geom.pitchY;
+    const size_t tiles = size_t(geom.tilesX) * geom.tilesY;
+    auto copy = [&](const void* src, size_t n) -> int {
+        if (bytes != n) {
+            set_error("debug_copy: expected " + std::to_string(n) + " bytes, got " + std::to_string(bytes));
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+        PBS_CUDA(cudaMemcpy(out, src, n, cudaMemcpyDeviceToHost), "debug D2H");
+        return PBS_OK;
+    };
+    const bool perLayer = which == PBS_DBG_IDD || which == PBS_DBG_RSIGMA || which == PBS_DBG_TILE_BINS ||
+                          which == PBS_DBG_FIRST_PASSIVE;
+    if (perLayer) {
+        if (!keepDebug || layer < 0 || layer >= plan.numLayers || layer >= chunkLayers) {
+            set_error("per-layer debug buffers need PBS_OPT_KEEP_DEBUG and a valid layer");
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+    }
+    BeamStateDev h;
+    PBS_CUDA(cudaMemcpy(&h, bs.ptr, sizeof(h), cudaMemcpyDeviceToHost), "debug D2H");
+    const int first = h.firstInside;
+    switch (which) {
+        case PBS_DBG_DENSITY: return copy(dens.ptr, S * rays * 4);
+        case PBS_DBG_WEPL: return copy(wepl.ptr, S * rays * 4);
+        case PBS_DBG_FIRST_INSIDE: return copy(firstIn.ptr, rays * 4);
+        case PBS_DBG_FIRST_OUTSIDE: return copy(firstOut.ptr, rays * 4);
+        case PBS_DBG_WEPL_MIN: return copy(weplMin.ptr, S * 4);
+        case PBS_DBG_RAY_WEIGHTS: return copy(rayW.ptr, size_t(plan.numLayers) * rays * 4);
+        case PBS_DBG_FIRST_PASSIVE: return copy(static_cast<char*>(firstPassive.ptr) + size_t(layer) * rays * 4, rays * 4);
+        case PBS_DBG_DOSE64: {
+            const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+            return copy(dose64.ptr, n * 8);
+        }
+        case PBS_DBG_BEV_DOSE: {
+            // Layer-summed BEV at absolute step index: planes before `first` are zero.
+            const size_t plane = size_t(geom.bevX) * geom.bevY;
+            if (bytes != S * plane * 4) {
+                set_error("debug_copy: BEV size mismatch");
+                return PBS_ERR_INVALID_ARGUMENT;
+            }
+            std::memset(out, 0, bytes);
+            const size_t nz = S - size_t(std::max(first, 0));
+            PBS_CUDA(cudaMemcpy(static_cast<char*>(out) + size_t(first) * plane * 4, bev.ptr, nz * plane * 4,
+                                cudaMemcpyDeviceToHost),
+                     "debug D2H");
+            return PBS_OK;
+        }
+        case PBS_DBG_IDD:
+        case PBS_DBG_RSIGMA: {
+            if (bytes != S * padPlane * 4) {
+                set_error("debug_copy: IDD size mismatch");
+                return PBS_ERR_INVALID_ARGUMENT;
+            }
+            LayerStateDev lh;
+            PBS_CUDA(cudaMemcpy(&lh, static_cast<LayerStateDev*>(ls.ptr) + layer, sizeof(lh), cudaMemcpyDeviceToHost),
+                     "debug D2H");
+            float* o = static_cast<float*>(out);
+            const float fill = which == PBS_DBG_IDD ? 0.0f : __builtin_inff();
+            std::fill(o, o + S * padPlane, fill);
+            const int nz = std::max(0, lh.afterLast - first);
+            const char* src = static_cast<const char*>(which == PBS_DBG_IDD ? iddBuf.ptr : rsBuf.ptr) +
+                              size_t(layer) * S * padPlane * 4;
+            if (nz > 0)
+                PBS_CUDA(cudaMemcpy(o + size_t(first) * padPlane, src, size_t(nz) * padPlane * 4, cudaMemcpyDeviceToHost),
+                         "debug D2H");
+            return PBS_OK;
+        }
+        case PBS_DBG_TILE_BINS: {
+            if (bytes != S * tiles) {
+                set_error("debug_copy: tile bins size mismatch");
+                return PBS_ERR_INVALID_ARGUMENT;
+            }
+            LayerStateDev lh;
+            PBS_CUDA(cudaMemcpy(&lh, static_cast<LayerStateDev*>(ls.ptr) + layer, sizeof(lh), cudaMemcpyDeviceToHost),
+                     "debug D2H");
+            uint8_t* o = static_cast<uint8_t*>(out);
+            std::memset(o, 0xff, bytes);
+            const int nz = std::max(0, lh.afterLast - first);
+            if (nz > 0)
+                PBS_CUDA(cudaMemcpy(o + size_t(first) * tiles, static_cast<const char*>(codes.ptr) + size_t(layer) * S * tiles,
+                                    size_t(nz) * tiles, cudaMemcpyDeviceToHost),
+                         "debug D2H");
+            return PBS_OK;
+        }
+        default:
+            set_error("unknown debug buffer");
+            return PBS_ERR_INVALID_ARGUMENT;
+    }
+}
+
+// ---- one-shot wrapper -----------------------------------------------------------
+
+namespace {
+std::mutex g_cacheMutex;
+std::map<int, Context*> g_cache;
+}  // namespace
+
+int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
+                      float* doseData, const int doseDims[3], const float doseRes[3], const float doseCorner[3],
+                      const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* energyData, int gpuId,
+                      int nuclear, int verbose) {
+    GridDesc cg, dg;
+    for (int i = 0; i < 3; ++i) {
+        cg.dims[i] = ctDims ? ctDims[i] : 0;
+        cg.res[i] = ctRes ? ctRes[i] : 0.f;
+        cg.corner[i] = ctCorner ? ctCorner[i] : 0.f;
+        dg.dims[i] = doseDims ? doseDims[i] : 0;
+        dg.res[i] = doseRes ? doseRes[i] : 0.f;
+        dg.corner[i] = doseCorner ? doseCorner[i] : 0.f;
+    }
+    std::string err;
+    if (!validate_global(ctData, cg, doseData, dg, beams, numBeams, energyData, err)) {
+        set_error(err);
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (nuclear) {
+        set_error("nuclear_correction=true requested, but this build has no nuclear halo tables loaded");
+        return PBS_ERR_UNSUPPORTED;
+    }
+    for (size_t i = 0; i < numBeams; ++i) {
+        if (!validate_beam(beams[i], i, err)) {
+            set_error(err);
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+    }
+    std::lock_guard<std::mutex> lock(g_cacheMutex);
+    Context*& ctx = g_cache[gpuId];
+    if (!ctx) {
+        Context* c = new Context();
+        int rc = c->init(gpuId);
+        if (rc) {
+            delete c;
+            return rc;
+        }
+        ctx = c;
+    }
+    int rc;
+    if ((rc = ctx->set_energy(*energyData))) return rc;
+    if ((rc = ctx->set_ct(ctData, 0, cg))) return rc;
+    if ((rc = ctx->set_dose_grid(dg))) return rc;
+    if ((rc = ctx->reset_dose(doseData, 0))) return rc;
+    for (size_t i = 0; i < numBeams; ++i) {
+        if ((rc = ctx->add_beam(beams[i], nuclear))) return rc;
+        if (verbose > 0) {
+            PbsBeamStats st;
+            if (ctx->beam_stats(&st) == PBS_OK)
+                std::fprintf(stderr,
+                             "[pbs] beam %zu: rays %dx%d steps %d layers %d first %d passive %d live tiles %lld\n", i,
+                             st.ray_dims[0], st.ray_dims[1], st.tracer_steps, st.num_layers, st.first_inside,
+                             st.guaranteed_passive, st.live_tiles);
+        }
+    }
+    return ctx->read_dose(doseData, 0);
+}
+
+}  // namespace pbs

@@ -1,0 +1,94 @@
+// Resident dose context (see context.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "pbs_types.h"
+#include "plan.h"
+
+namespace pbs {
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+// Grow-only device allocation.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b);
+    void release();
+};
+
+// Grow-only pinned host allocation.
+struct PinnedBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b);
+    void release();
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    // Options.
+    int compatBevZShift = 0;
+    int stageTiming = 0;
+    int keepDebug = 0;
+    int ctInputType = PBS_CT_AUTO;
+    long long layerBudgetMiB = 2048;
+
+    // Lookup tables.
+    bool hasEnergy = false;
+    PbsEnergyDesc energy{};
+    std::vector<float> energiesPerU, peakDepths, scaleFacts, ciddHost, densityHost, spHost, rrlHost;
+    DevBuf cidd, density, sp, rrl;
+    LutsDev luts{};
+
+    // CT (HU+1000) and dose accumulator.
+    bool hasCt = false;
+    int ctType = PBS_CT_AUTO;
+    GridDesc ctGrid{};
+    DevBuf ct;
+    bool hasDose = false;
+    GridDesc doseGrid{};
+    DevBuf dose64;
+
+    // Per-beam working set (grow-only).
+    DevBuf dens, wepl, weplMin, rayW, interm, lattice, iddBuf, rsBuf, bev, cpb, subspots, floatOut;
+    DevBuf firstIn, firstOut, firstPassive, codes, work, lp, ls, bs, stats;
+    PinnedBuf staging;
+    cudaEvent_t stagingEvent = nullptr;
+    cudaEvent_t ev[8] = {};
+
+    // Last beam.
+    BeamPlan plan;
+    BeamGeomDev geom{};
+    int chunkLayers = 0;
+    bool lastBeamValid = false;
+    bool lastStageTimed = false;
+
+    ~Context();
+    int init(int gpu);
+    int upload(void* dst, const void* src, size_t n);
+    int set_energy(const PbsEnergyDesc& e);
+    int set_ct(const float* data, int onDevice, const GridDesc& g);
+    int set_dose_grid(const GridDesc& g);
+    int reset_dose(const float* init, int onDevice);
+    int read_dose(float* out, int onDevice);
+    int add_beam(const PbsBeamDesc& b, int nuclear);
+    int beam_stats(PbsBeamStats* out);
+    int layer_stats(int layer, PbsLayerStats* out);
+    int stage_times(float* ms, int n);
+    int debug_copy(int which, int layer, void* out, size_t bytes);
+};
+
+int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
+                      float* doseData, const int doseDims[3], const float doseRes[3], const float doseCorner[3],
+                      const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* energyData, int gpuId,
+                      int nuclear, int verbose);
+
+}  // namespace pbs

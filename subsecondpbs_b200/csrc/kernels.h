@@ -1,0 +1,66 @@
+// Kernel launchers of the dose pipeline. All launches are asynchronous on `s`.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pbs_types.h"
+
+namespace pbs {
+
+// ---- CT preparation -------------------------------------------------------
+// Convert a float CT to HU+1000 in place according to `type` (PBS_CT_*).
+cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, int lutN, float lutScale,
+                              cudaStream_t s);
+// min/max of a strided sample (the reference's ~100k-sample statistics).
+cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStream_t s);
+
+// ---- tracing ------------------------------------------------------------------
+// rayTracingBEVKernel (src/core/bev_ray_tracing.cu:65-159) as a segmented scan.
+cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ctHu1000, int ctX, int ctY, int ctZ,
+                         float* density, float* wepl, int* firstInside, int* firstOutside, BeamStateDev* beam,
+                         cudaStream_t s);
+// sliceMinVarIgnoreNeverEnter (src/core/raytracedicom_wrapper.cu:1991-2023).
+cudaError_t launch_wepl_min(const BeamGeomDev& g, const float* wepl, const int* firstOutside, float* weplMin,
+                            cudaStream_t s);
+// Beam planner: guaranteed passive step, entry plane, per-layer cut-off steps and
+// entry sigmas (wrapper.cu:3651-3700, 3733-3833, 4302-4313).
+cudaError_t launch_beam_planner(const BeamGeomDev& g, const float* weplMin, const LayerParamsDev* lp,
+                                LayerStateDev* ls, BeamStateDev* beam, cudaStream_t s);
+
+// ---- spot -> ray fluence ----------------------------------------------------
+// x/yConvGathResampGpu (src/algorithms/convolution.cu:198-262) for all layers.
+cudaError_t launch_conv_lattice(const BeamGeomDev& g, const float* lattice, float* interm, float* rayW,
+                                const LayerStateDev* ls, const BeamStateDev* beam, cudaStream_t s);
+// Legacy CPB fluence (convolution.cu:21-152, 269-339): subspots -> CPB -> rays.
+cudaError_t launch_conv_cpb(const BeamGeomDev& g, const float* subspots, int maxSubspots, float* cpb, float* rayW,
+                            cudaStream_t s);
+
+// ---- IDD / sigma + tile radius codes -----------------------------------------
+// fillIddAndSigmaKernel (src/algorithms/idd_sigma.cu:46-259) fused with the
+// per-tile radius reduction of tileRadCalc (complete_superposition.cu:198-255).
+cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, int nLayers, const float* density,
+                       const float* wepl, const int* firstInside, const int* firstOutside, const float* rayW,
+                       const LayerParamsDev* lp, LayerStateDev* ls, const BeamStateDev* beam, float* idd,
+                       float* rsigma, uint8_t* codes, int* firstPassive, cudaStream_t s);
+// Histogram, overflow merge and batching (complete_superposition.cu:358-490) plus
+// the radius-sorted work list of live tiles.
+cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
+                            BeamStateDev* beam, int4* work, int workCapacity, cudaStream_t s);
+// kernelSuperposition<R> (complete_superposition.cu:264-335) over the work list,
+// summing all layers into one BEV dose.
+cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                             const BeamStateDev* beam, float* bev, int gridBlocks, cudaStream_t s);
+
+// ---- BEV -> dose ---------------------------------------------------------------
+// Transfer bounding box and parameters (wrapper.cu:5343-5403).
+cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cudaStream_t s);
+// primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44) accumulating in FP64.
+cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,
+                            cudaStream_t s);
+
+// ---- dose grid -------------------------------------------------------------------
+cudaError_t launch_dose_init(double* dose, const float* init, size_t n, cudaStream_t s);
+cudaError_t launch_dose_to_float(const double* dose, float* out, size_t n, cudaStream_t s);
+
+}  // namespace pbs

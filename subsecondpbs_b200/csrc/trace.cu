@@ -1,0 +1,354 @@
+// CT preparation, BEV ray tracing, per-step WEPL minimum and the device-side
+// beam planner.
+#include <float.h>
+
+#include <algorithm>
+
+#include "device_util.cuh"
+#include "kernels.h"
+#include "../../include/subsecondpbs.h"
+
+namespace pbs {
+
+namespace {
+
+constexpr float kInf20 = 1.0e20f;  // the reference's INF stored in a float (Macro.cuh:7)
+constexpr int kTraceSegments = 8;  // warps per tracing CTA; each marches one depth segment
+constexpr int kNone = 0x7fffffff;
+
+// Trilinear sample of a [Z][Y][X] volume, texel centres at i + 0.5, zero outside
+// (sample3DLinearBorder, src/core/bev_ray_tracing.cu:16-61).
+__device__ __forceinline__ float ct_sample_border(const float* __restrict__ vol, int dx, int dy, int dz, float x, float y,
+                                                  float z) {
+    float fx = x - 0.5f, fy = y - 0.5f, fz = z - 0.5f;
+    fx = fminf(fmaxf(fx, -2.0f), float(dx) + 1.0f);
+    fy = fminf(fmaxf(fy, -2.0f), float(dy) + 1.0f);
+    fz = fminf(fmaxf(fz, -2.0f), float(dz) + 1.0f);
+    const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+    const int x0 = int(flx), y0 = int(fly), z0 = int(flz);
+    const float tx = fx - flx, ty = fy - fly, tz = fz - flz;
+    auto at = [&](int xi, int yi, int zi) -> float {
+        if (xi < 0 || yi < 0 || zi < 0 || xi >= dx || yi >= dy || zi >= dz) return 0.0f;
+        return __ldg(vol + (static_cast<size_t>(zi) * dy + yi) * dx + xi);
+    };
+    const float c000 = at(x0, y0, z0), c100 = at(x0 + 1, y0, z0);
+    const float c010 = at(x0, y0 + 1, z0), c110 = at(x0 + 1, y0 + 1, z0);
+    const float c001 = at(x0, y0, z0 + 1), c101 = at(x0 + 1, y0, z0 + 1);
+    const float c011 = at(x0, y0 + 1, z0 + 1), c111 = at(x0 + 1, y0 + 1, z0 + 1);
+    const float c00 = c000 + (c100 - c000) * tx;
+    const float c10 = c010 + (c110 - c010) * tx;
+    const float c01 = c001 + (c101 - c001) * tx;
+    const float c11 = c011 + (c111 - c011) * tx;
+    const float c0 = c00 + (c10 - c00) * ty;
+    const float c1 = c01 + (c11 - c01) * ty;
+    return c0 + (c1 - c0) * tz;
+}
+
+__device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
+    const float y = v - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+}
+
+// One CTA traces 32 neighbouring rays of one ray row; warp w marches depth segment w.
+// Pass 1 sums each segment, the segment sums are prefix-scanned per ray, and pass 2
+// re-marches the segment writing density and compensated cumulative WEPL.
+__global__ void __launch_bounds__(32 * kTraceSegments)
+trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX, int ctY, int ctZ,
+             float* __restrict__ density, float* __restrict__ wepl, int* __restrict__ firstInside,
+             int* __restrict__ firstOutside, BeamStateDev* __restrict__ beam) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int x = blockIdx.x * 32 + lane;
+    const int y = blockIdx.y;
+    const bool active = x < g.rayX;
+    const int S = g.steps;
+    const int seg = (S + kTraceSegments - 1) / kTraceSegments;
+    const int s0 = min(S, w * seg), s1 = min(S, s0 + seg);
+
+    __shared__ float shHu[kTraceSegments][32];
+    __shared__ double shSp[kTraceSegments][32];
+    __shared__ int shFirst[kTraceSegments][32];
+    __shared__ int shLast[kTraceSegments][32];
+
+    V3 pos0 = v3(0.f, 0.f, 0.f), inc = v3(0.f, 0.f, 0.f);
+    float stepLen = 0.f;
+    if (active) {
+        const V3 start = tracer_start(g.tracer, x, y);
+        inc = tracer_inc(g.tracer, x, y);
+        stepLen = tracer_step_len(g.tracer, x, y);
+        // The reference advances the sample point by repeated float additions.
+        pos0 = v3(fadd(start.x, 0.5f), fadd(start.y, 0.5f), fadd(start.z, 0.5f));
+        for (int k = 0; k < s0; ++k) pos0 = add(pos0, inc);
+    }
+
+    // Pass 1: segment sums of HU+1000 and of WEPL increments.
+    float huSum = 0.f, spSum = 0.f, spComp = 0.f;
+    if (active) {
+        V3 pos = pos0;
+        for (int k = s0; k < s1; ++k) {
+            const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+            huSum += hu;
+            const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
+            kahan_add(spSum, spComp, stepLen * sp);
+            pos = add(pos, inc);
+        }
+    }
+    shHu[w][lane] = huSum;
+    shSp[w][lane] = double(spSum) - double(spComp);
+    __syncthreads();
+
+    float huPre = 0.f;
+    double spPre = 0.0;
+    for (int q = 0; q < w; ++q) {
+        huPre += shHu[q][lane];
+        spPre += shSp[q][lane];
+    }
+
+    // Pass 2: write the per-step samples.
+    int firstK = kNone, lastK = -1;
+    if (active) {
+        V3 pos = pos0;
+        float cumHu = huPre;
+        float cum = float(spPre);
+        float comp = float(double(cum) - spPre);
+        const size_t plane = static_cast<size_t>(g.rayX) * g.rayY;
+        size_t idx = static_cast<size_t>(s0) * plane + static_cast<size_t>(y) * g.rayX + x;
+        for (int k = s0; k < s1; ++k) {
+            const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+            cumHu += hu;
+            density[idx] = lut_linear_clamp(luts.density, luts.nDensity, hu * luts.densityScale + 0.5f);
+            const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
+            kahan_add(cum, comp, stepLen * sp);
+            wepl[idx] = cum;
+            if (firstK == kNone && !(cumHu < 150.0f)) firstK = k;
+            if (hu > 150.0f) lastK = k;
+            pos = add(pos, inc);
+            idx += plane;
+        }
+    }
+    shFirst[w][lane] = firstK;
+    shLast[w][lane] = lastK;
+    __syncthreads();
+
+    if (w == 0) {
+        int fk = kNone, lk = -1;
+        for (int q = 0; q < kTraceSegments; ++q) {
+            fk = min(fk, shFirst[q][lane]);
+            lk = max(lk, shLast[q][lane]);
+        }
+        // beforeFirstInside + 1 and lastInside + 1 in the reference's convention.
+        const int fi = (fk == kNone) ? S : max(fk, 1);
+        const int fo = (lk < 0) ? 1 : lk + 1;
+        int wmin = active ? fi : INT_MAX;
+        int wmax = active ? fo : INT_MIN;
+        if (active) {
+            firstInside[y * g.rayX + x] = fi;
+            firstOutside[y * g.rayX + x] = fo;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+            wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+        }
+        if (lane == 0) {
+            atomicMin(&beam->firstInside, wmin);
+            atomicMax(&beam->firstOutside, wmax);
+        }
+    }
+}
+
+__global__ void wepl_min_kernel(int nRays, const float* __restrict__ wepl, const int* __restrict__ firstOutside,
+                                float* __restrict__ weplMin) {
+    const int k = blockIdx.x;
+    const float* plane = wepl + static_cast<size_t>(k) * nRays;
+    float m = kInf20;
+    for (int r = threadIdx.x; r < nRays; r += blockDim.x) {
+        if (firstOutside[r] > 0) {
+            const float v = plane[r];
+            if (v < m) m = v;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float other = __shfl_xor_sync(0xffffffffu, m, o);
+        if (other < m) m = other;
+    }
+    __shared__ float part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = part[0];
+        for (int i = 1; i < int(blockDim.x >> 5); ++i)
+            if (part[i] < r) r = part[i];
+        weplMin[k] = r;
+    }
+}
+
+// include/utils/vector_find.h:61-82
+__device__ int find_first_larger_ordered_dev(const float* v, int n, float value) {
+    int upper = n - 1, lower = 0;
+    if (v[n - 1] <= value) return upper;
+    if (v[0] > value) return 0;
+    while (upper - lower > 1) {
+        const int pivot = (upper + lower) / 2;
+        if (v[pivot] <= value) lower = pivot;
+        else upper = pivot;
+    }
+    return lower + 1;
+}
+
+__global__ void beam_planner_kernel(BeamGeomDev g, const float* __restrict__ weplMin,
+                                    const LayerParamsDev* __restrict__ lp, LayerStateDev* __restrict__ ls,
+                                    BeamStateDev* __restrict__ beam) {
+    __shared__ int shPassive;
+    __shared__ float shEntryZ;
+    if (threadIdx.x == 0) {
+        const int first = beam->firstInside;
+        const float limitAll = fmul(kBpDepthCutoff, g.maxPeakDepthMm);
+        const int g0 = find_first_larger_ordered_dev(weplMin, g.steps, limitAll);
+        const int passive = min(g0, beam->firstOutside);
+        beam->guaranteedPassive = passive;
+        const float entryZ = fadd(fmul(float(first), g.fanDelta.z), g.fanCorner.z);
+        beam->entryZ = entryZ;
+        beam->pxSpMultX = fsub(1.0f, fdiv(entryZ, g.sourceDist.x));
+        beam->pxSpMultY = fsub(1.0f, fdiv(entryZ, g.sourceDist.y));
+        beam->maxCalcPassive = first;
+        beam->liveTiles = 0;
+        beam->superposeFma = 0;
+        shPassive = passive;
+        shEntryZ = entryZ;
+    }
+    __syncthreads();
+    const float z = shEntryZ;
+    for (int l = threadIdx.x; l < g.numLayers; l += blockDim.x) {
+        const LayerParamsDev p = lp[l];
+        LayerStateDev& st = ls[l];
+        const float limit = fmul(kBpDepthCutoff, p.peakDepth);
+        st.afterLast = min(find_first_larger_ordered_dev(weplMin, g.steps, limit), shPassive);
+        // Entry sigma of the convolution (wrapper.cu:3776-3833).
+        {
+            const float a = fdiv(0.00270f, fsub(p.convPeakDepth, 4.50f));
+            const float b = fdiv(-4.39f, fsub(p.convPeakDepth, 3.86f));
+            const float base = fadd(fmul(fmul(a, z), z), fmul(b, z));
+            st.entrySigmaX = fsqrt(fmaxf(0.0f, fadd(base, fmul(p.sigmaXmm, p.sigmaXmm))));
+            st.entrySigmaY = fsqrt(fmaxf(0.0f, fadd(base, fmul(p.sigmaYmm, p.sigmaYmm))));
+        }
+        // IDD entry variance (wrapper.cu:4309-4313).
+        {
+            const float a = fdiv(0.00270f, fsub(p.peakDepth, 4.50f));
+            const float b = fdiv(-4.39f, fsub(p.peakDepth, 3.86f));
+            st.entrySigmaSq = fadd(fadd(fmul(fmul(a, z), z), fmul(b, z)), fmul(p.sigmaXmm, p.sigmaXmm));
+        }
+        st.maxFirstPassive = INT_MIN;
+        st.calcPassive = 0;
+        st.liveTiles = 0;
+        for (int i = 0; i < kBuckets; ++i) {
+            st.hist[i] = 0;
+            st.batchedR[i] = 0;
+        }
+        for (int i = 0; i < 33; ++i) st.batchedCounts[i] = 0;
+    }
+}
+
+__global__ void ct_convert_kernel(float* ct, size_t n, int type, const float* __restrict__ lut, int lutN,
+                                  float lutScale) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const float v = ct[i];
+        if (type == PBS_CT_HU) {
+            ct[i] = v + 1000.0f;
+        } else if (type == PBS_CT_DENSITY || type == PBS_CT_SPR) {
+            // findFractionalIndexMonotonic (wrapper.cu:2339-2376), then / scale.
+            float idx;
+            const bool inc = lut[lutN - 1] >= lut[0];
+            if (lutN <= 1) {
+                idx = 0.0f;
+            } else if (inc ? (v <= lut[0]) : (v >= lut[0])) {
+                idx = 0.0f;
+            } else if (inc ? (v >= lut[lutN - 1]) : (v <= lut[lutN - 1])) {
+                idx = float(lutN - 1);
+            } else {
+                int lo = 0, hi = lutN - 1;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    const float vm = lut[mid];
+                    if (inc) {
+                        if (vm <= v) lo = mid; else hi = mid;
+                    } else {
+                        if (vm >= v) lo = mid; else hi = mid;
+                    }
+                }
+                const float v0 = lut[lo], den = __fsub_rn(lut[lo + 1], v0);
+                float t = 0.0f;
+                if (den != 0.0f) t = __fdiv_rn(__fsub_rn(v, v0), den);
+                t = fminf(fmaxf(t, 0.0f), 1.0f);
+                idx = __fadd_rn(float(lo), t);
+            }
+            ct[i] = __fdiv_rn(idx, lutScale);
+        }
+    }
+}
+
+__global__ void ct_stats_kernel(const float* __restrict__ ct, size_t n, size_t stride, float* minmax) {
+    float mn = ct[0], mx = ct[0];
+    for (size_t i = size_t(threadIdx.x) * stride; i < n; i += size_t(blockDim.x) * stride) {
+        mn = fminf(mn, ct[i]);
+        mx = fmaxf(mx, ct[i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    __shared__ float a[32], b[32];
+    if ((threadIdx.x & 31) == 0) {
+        a[threadIdx.x >> 5] = mn;
+        b[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < int(blockDim.x >> 5); ++i) {
+            mn = fminf(mn, a[i]);
+            mx = fmaxf(mx, b[i]);
+        }
+        minmax[0] = fminf(mn, a[0]);
+        minmax[1] = fmaxf(mx, b[0]);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, int lutN, float lutScale,
+                              cudaStream_t s) {
+    if (type == PBS_CT_HU_PLUS_1000 || n == 0) return cudaSuccess;
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, type, lut, lutN, lutScale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStream_t s) {
+    const size_t maxSamples = 100000;
+    const size_t stride = (n > maxSamples) ? (n / maxSamples) : 1;
+    ct_stats_kernel<<<1, 1024, 0, s>>>(ct, n, stride, minmax2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ct, int ctX, int ctY, int ctZ,
+                         float* density, float* wepl, int* firstInside, int* firstOutside, BeamStateDev* beam,
+                         cudaStream_t s) {
+    dim3 block(32, kTraceSegments);
+    dim3 grid((g.rayX + 31) / 32, g.rayY);
+    trace_kernel<<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside, firstOutside, beam);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wepl_min(const BeamGeomDev& g, const float* wepl, const int* firstOutside, float* weplMin,
+                            cudaStream_t s) {
+    wepl_min_kernel<<<g.steps, 256, 0, s>>>(g.rayX * g.rayY, wepl, firstOutside, weplMin);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_beam_planner(const BeamGeomDev& g, const float* weplMin, const LayerParamsDev* lp,
+                                LayerStateDev* ls, BeamStateDev* beam, cudaStream_t s) {
+    beam_planner_kernel<<<1, 64, 0, s>>>(g, weplMin, lp, ls, beam);
+    return cudaGetLastError();
+}
+
+}  // namespace pbs

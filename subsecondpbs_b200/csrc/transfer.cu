@@ -1,0 +1,140 @@
+// BEV -> dose transfer and dose-grid helpers.
+//
+// The layer-summed BEV dose of a beam is sampled once at the divergent fan index
+// of every dose voxel inside the transfer box and accumulated in FP64. The
+// reference transfers every layer separately into an FP32 grid
+// (wrapper.cu:5343-5505); the transfer is linear in the BEV dose, so one pass over
+// the summed volume gives the same sum up to rounding.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace pbs {
+
+namespace {
+
+// Trilinear sample with texel centres at i + 0.5 and zero outside the volume,
+// at texel-space coordinates (x, y, z) = texture coordinate - 0.5.
+__device__ __forceinline__ float bev_sample(const float* __restrict__ v, int nx, int ny, int nz, float x, float y,
+                                            float z) {
+    x = fminf(fmaxf(x, -2.0f), float(nx) + 1.0f);
+    y = fminf(fmaxf(y, -2.0f), float(ny) + 1.0f);
+    z = fminf(fmaxf(z, -2.0f), float(nz) + 1.0f);
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    const int x0 = int(fx), y0 = int(fy), z0 = int(fz);
+    const float tx = x - fx, ty = y - fy, tz = z - fz;
+    auto at = [&](int xi, int yi, int zi) -> float {
+        if (xi < 0 || yi < 0 || zi < 0 || xi >= nx || yi >= ny || zi >= nz) return 0.0f;
+        return __ldg(v + (static_cast<size_t>(zi) * ny + yi) * nx + xi);
+    };
+    const float c000 = at(x0, y0, z0), c100 = at(x0 + 1, y0, z0);
+    const float c010 = at(x0, y0 + 1, z0), c110 = at(x0 + 1, y0 + 1, z0);
+    const float c001 = at(x0, y0, z0 + 1), c101 = at(x0 + 1, y0, z0 + 1);
+    const float c011 = at(x0, y0 + 1, z0 + 1), c111 = at(x0 + 1, y0 + 1, z0 + 1);
+    const float c00 = c000 + (c100 - c000) * tx;
+    const float c10 = c010 + (c110 - c010) * tx;
+    const float c01 = c001 + (c101 - c001) * tx;
+    const float c11 = c011 + (c111 - c011) * tx;
+    const float c0 = c00 + (c10 - c00) * ty;
+    const float c1 = c01 + (c11 - c01) * ty;
+    return c0 + (c1 - c0) * tz;
+}
+
+// Transfer box from the eight BEV corners (wrapper.cu:5343-5394); the z range spans
+// the deepest superposed step of all layers.
+__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int first = beam->firstInside;
+    const int passive = beam->maxCalcPassive;
+    const float xs[2] = {-float(kMaxR), float(g.pitchX + kMaxR - 1)};
+    const float ys[2] = {-float(kMaxR), float(g.pitchY + kMaxR - 1)};
+    const float zs[2] = {float(first), float(passive - 1)};
+    V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
+    for (int zi = 0; zi < 2; ++zi)
+        for (int yi = 0; yi < 2; ++yi)
+            for (int xi = 0; xi < 2; ++xi) {
+                const V3 p = apply(g.rayIdxToDoseIdx, v3(xs[xi], ys[yi], zs[zi]));
+                mx.x = fmaxf(mx.x, p.x);
+                mx.y = fmaxf(mx.y, p.y);
+                mx.z = fmaxf(mx.z, p.z);
+                mn.x = fminf(mn.x, p.x);
+                mn.y = fminf(mn.y, p.y);
+                mn.z = fminf(mn.z, p.z);
+            }
+    beam->transferStart[0] = max((int(floorf(mn.x)) / 32) * 32, 0);
+    beam->transferStart[1] = max(int(floorf(mn.y)), 0);
+    beam->transferStart[2] = max(int(floorf(mn.z)), 0);
+    beam->transferMax[0] = min(int(ceilf(mx.x)), g.doseX - 1);
+    beam->transferMax[1] = min(int(ceilf(mx.y)), g.doseY - 1);
+    beam->transferMax[2] = min(int(ceilf(mx.z)), g.doseZ - 1);
+    const ToFan t = invert_and_shift(g.rayIdxToDoseIdx, v3(float(kMaxR), float(kMaxR), -float(first)));
+    beam->transfer = make_transfer_params(t);
+    beam->transferValid = passive > first && beam->transferStart[0] <= beam->transferMax[0] &&
+                          beam->transferStart[1] <= beam->transferMax[1] &&
+                          beam->transferStart[2] <= beam->transferMax[2];
+}
+
+// primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44). The reference launches
+// ceil(width/32) x ceil(height/8) blocks from the box start, so columns up to the
+// next block boundary inside the dose grid are transferred too.
+__global__ void __launch_bounds__(256)
+transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, const BeamStateDev* __restrict__ beam,
+                double* __restrict__ dose) {
+    if (!beam->transferValid) return;
+    const int sx = beam->transferStart[0], sy = beam->transferStart[1], sz = beam->transferStart[2];
+    const int mx = beam->transferMax[0], my = beam->transferMax[1], mz = beam->transferMax[2];
+    const int spanX = ((mx - sx + 1 + 31) / 32) * 32, spanY = ((my - sy + 1 + 7) / 8) * 8;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x < sx || y < sy || x >= sx + spanX || y >= sy + spanY || x >= g.doseX || y >= g.doseY) return;
+    const TransferParams T = beam->transfer;
+    const V3 start = transfer_start(T, x, y);
+    const float zShift = g.compatBevZShift ? float(beam->firstInside) : 0.0f;
+    const size_t slice = static_cast<size_t>(g.doseX) * g.doseY;
+    double* col = dose + static_cast<size_t>(y) * g.doseX + x;
+    for (int z = sz; z <= mz; ++z) {
+        const V3 f = transfer_fan_idx(T, start, z);
+        if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
+        const float v = bev_sample(bev, g.bevX, g.bevY, g.steps, f.x, f.y, f.z - zShift);
+        if (v > 0.0f) col[z * slice] += double(v);
+    }
+}
+
+__global__ void dose_init_kernel(double* dose, const float* init, size_t n) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        dose[i] = init ? double(init[i]) : 0.0;
+}
+
+__global__ void dose_to_float_kernel(const double* dose, float* out, size_t n) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = float(dose[i]);
+}
+
+}  // namespace
+
+cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cudaStream_t s) {
+    transfer_planner_kernel<<<1, 32, 0, s>>>(g, beam);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,
+                            cudaStream_t s) {
+    dim3 block(32, 8);
+    dim3 grid((g.doseX + 31) / 32, (g.doseY + 7) / 8);
+    transfer_kernel<<<grid, block, 0, s>>>(g, bev, beam, dose);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dose_init(double* dose, const float* init, size_t n, cudaStream_t s) {
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 32));
+    dose_init_kernel<<<blocks, 256, 0, s>>>(dose, init, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dose_to_float(const double* dose, float* out, size_t n, cudaStream_t s) {
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 32));
+    dose_to_float_kernel<<<blocks, 256, 0, s>>>(dose, out, n);
+    return cudaGetLastError();
+}
+
+}  // namespace pbs

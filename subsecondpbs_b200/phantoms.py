@@ -1,0 +1,168 @@
+"""Seeded synthetic workloads in the layout the reference's Python API takes.
+
+No public dataset exists for this path; every input is generated from a seeded
+numpy PCG64 stream:
+
+* `water_phantom_case` - homogeneous water box along +z with one energy layer on
+  an 11x11 square spot grid (the CPU-runnable plain-pipeline case).
+* `heterogeneous_case` - body ellipsoid with Gaussian HU noise, a lung slab and
+  two bone cylinders, one beam at gantry 90 deg with N energy layers of spots on a
+  5 mm hexagonal grid over a spherical target (the headline 256x256x160 case and
+  its scaled-down parity variants).
+
+Each case is a dict with `ct` (float32 [Z][Y][X]), grid tuples (x, y, z order as
+the reference's ct_dims/ct_resolution/ct_corner), the beam dict and the energy
+dict of src/bindings/raytracedicom_pybind.cpp:1711-1847.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .tables import synthetic_proton_tables
+
+SEED_BASE = 20261203
+
+_TABLE_CACHE: dict = {}
+
+
+def proton_tables() -> dict:
+    if "proton" not in _TABLE_CACHE:
+        _TABLE_CACHE["proton"] = synthetic_proton_tables()
+    return _TABLE_CACHE["proton"]
+
+
+def subspot_lut(n_layers: int, n_side: int, sigma_mm: np.ndarray, rng: np.random.Generator) -> np.ndarray:
+    """[L][n_side^2][5] subspot table (dx, dy, weight, sigma_x, sigma_y): an
+    n_side x n_side grid spanning +-1.5 sigma with Gaussian weights summing to 1."""
+    out = np.zeros((n_layers, n_side * n_side, 5), dtype=np.float32)
+    g = np.linspace(-1.5, 1.5, n_side)
+    gx, gy = np.meshgrid(g, g, indexing="xy")
+    w = np.exp(-0.5 * (gx ** 2 + gy ** 2)).reshape(-1)
+    w /= w.sum()
+    for layer in range(n_layers):
+        s = float(sigma_mm[layer])
+        out[layer, :, 0] = gx.reshape(-1) * s
+        out[layer, :, 1] = gy.reshape(-1) * s
+        out[layer, :, 2] = w
+        out[layer, :, 3] = s / n_side
+        out[layer, :, 4] = s / n_side
+    return out
+
+
+def _grid(dims, res):
+    dims = tuple(int(d) for d in dims)
+    res = tuple(float(r) for r in res)
+    corner = tuple(-0.5 * (d - 1) * r for d, r in zip(dims, res))
+    return dims, res, corner
+
+
+def water_phantom_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), energy_mev=150.0, n_side=11, spacing_mm=5.0,
+                       sigma_mm=4.0, sad_mm=10000.0, ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 1) -> dict:
+    """Homogeneous water: all HU = 0 passed as HU+1000 = 1000 (an all-zero HU volume
+    would be auto-detected as density by the reference, raytracedicom_wrapper.cu:2333)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dims, res, corner = _grid(dims, res)
+    ct = np.full((dims[2], dims[1], dims[0]), 1000.0, dtype=np.float32)
+    g = (np.arange(n_side) - (n_side - 1) / 2.0) * spacing_mm
+    px, py = np.meshgrid(g, g, indexing="xy")
+    pos = np.stack([px.reshape(-1), py.reshape(-1)], axis=1).astype(np.float32)
+    n = pos.shape[0]
+    iso = np.zeros(3)
+    bmz = np.array([0.0, 0.0, 1.0])
+    beam = {
+        "energies": np.array([energy_mev], dtype=np.float32),
+        "spot_sigmas": np.array([[sigma_mm, sigma_mm]], dtype=np.float32),
+        "ray_spacing": (ray_spacing, ray_spacing),
+        "steps": 0,
+        "source_dist": (sad_mm, sad_mm),
+        "spot_offset": (0.0, 0.0, 0.0),
+        "spot_delta": (spacing_mm, spacing_mm, 0.0),
+        "beam_direction": tuple(bmz),
+        "beam_xdir": (1.0, 0.0, 0.0),
+        "beam_ydir": (0.0, 1.0, 0.0),
+        "sad": sad_mm,
+        "source_position": tuple(iso - bmz * sad_mm),
+        "layer_spot_counts": np.array([n], dtype=np.int32),
+        "spot_positions": pos.reshape(-1),
+        "spot_weights": np.ones(n, dtype=np.float32),
+        "subspot_data": subspot_lut(1, n_sub, np.array([sigma_mm]), rng),
+    }
+    return {"name": "water_phantom", "ct": ct, "ct_dims": dims, "ct_resolution": res, "ct_corner": corner,
+            "dose_dims": dims, "dose_resolution": res, "dose_corner": corner, "beam": beam,
+            "energy": proton_tables()}
+
+
+def heterogeneous_ct(dims, res, rng: np.random.Generator) -> np.ndarray:
+    """HU volume [Z][Y][X]: air -1000 outside a body ellipsoid (semi-axes 0.45 of
+    the extents) of HU N(0, 20); a lung slab N(-800, 50) and two bone cylinders
+    U(700, 1200) inside it."""
+    nx, ny, nz = dims
+    z, y, x = np.meshgrid(np.arange(nz, dtype=np.float32), np.arange(ny, dtype=np.float32),
+                          np.arange(nx, dtype=np.float32), indexing="ij")
+    cx, cy, cz = (nx - 1) / 2.0, (ny - 1) / 2.0, (nz - 1) / 2.0
+    ax, ay, az = 0.45 * nx, 0.45 * ny, 0.45 * nz
+    body = ((x - cx) / ax) ** 2 + ((y - cy) / ay) ** 2 + ((z - cz) / az) ** 2 <= 1.0
+    ct = np.full((nz, ny, nx), -1000.0, dtype=np.float32)
+    ct[body] = rng.normal(0.0, 20.0, size=int(body.sum())).astype(np.float32)
+    # Lung slab: a band in y on the +y side of the body.
+    lung = body & (y > cy + 0.10 * ny) & (y < cy + 0.30 * ny) & (np.abs(z - cz) < 0.30 * nz)
+    ct[lung] = rng.normal(-800.0, 50.0, size=int(lung.sum())).astype(np.float32)
+    # Two bone cylinders along z.
+    for ox, oy in ((-0.18, -0.12), (0.20, -0.20)):
+        r = 0.05 * min(nx, ny)
+        cyl = body & (((x - (cx + ox * nx)) ** 2 + (y - (cy + oy * ny)) ** 2) <= r * r)
+        ct[cyl] = rng.uniform(700.0, 1200.0, size=int(cyl.sum())).astype(np.float32)
+    return ct
+
+
+def hex_spots(radius_mm: float, pitch_mm: float) -> np.ndarray:
+    """Hexagonal lattice points (rows pitch*sqrt(3)/2 apart, alternate rows shifted
+    by pitch/2) inside a disc, [N][2] in mm."""
+    dy = pitch_mm * np.sqrt(3.0) / 2.0
+    pts = []
+    nrow = int(np.ceil(radius_mm / dy)) + 1
+    ncol = int(np.ceil(radius_mm / pitch_mm)) + 2
+    for j in range(-nrow, nrow + 1):
+        shift = 0.5 * pitch_mm if (j % 2) else 0.0
+        for i in range(-ncol, ncol + 1):
+            x, y = i * pitch_mm + shift, j * dy
+            if x * x + y * y <= radius_mm * radius_mm:
+                pts.append((x, y))
+    return np.array(pts, dtype=np.float32)
+
+
+def heterogeneous_case(dims=(256, 256, 160), res=(2.0, 2.0, 2.0), n_layers=20, e_range=(70.0, 180.0),
+                       target_radius_mm=32.0, hex_pitch_mm=5.0, sigma_range=(6.0, 3.0), sad_mm=2000.0,
+                       ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 2) -> dict:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dims, res, corner = _grid(dims, res)
+    ct = heterogeneous_ct(dims, res, rng)
+    energies = np.linspace(e_range[0], e_range[1], n_layers).astype(np.float32)
+    sig = np.linspace(sigma_range[0], sigma_range[1], n_layers).astype(np.float32)
+    spots = hex_spots(target_radius_mm, hex_pitch_mm)
+    counts = np.full(n_layers, spots.shape[0], dtype=np.int32)
+    pos = np.tile(spots, (n_layers, 1))
+    weights = rng.lognormal(0.0, 0.5, size=pos.shape[0]).astype(np.float32)
+    iso = np.zeros(3)
+    bmz = np.array([-1.0, 0.0, 0.0])  # gantry 90 deg: the beam travels along -x
+    beam = {
+        "energies": energies,
+        "spot_sigmas": np.stack([sig, sig], axis=1),
+        "ray_spacing": (ray_spacing, ray_spacing),
+        "steps": 0,
+        "source_dist": (sad_mm, sad_mm),
+        "spot_offset": (0.0, 0.0, 0.0),
+        "spot_delta": (hex_pitch_mm, hex_pitch_mm * np.sqrt(3.0) / 2.0, 0.0),
+        "beam_direction": tuple(bmz),
+        "beam_xdir": (0.0, 1.0, 0.0),
+        "beam_ydir": (0.0, 0.0, 1.0),
+        "sad": sad_mm,
+        "source_position": tuple(iso - bmz * sad_mm),
+        "layer_spot_counts": counts,
+        "spot_positions": pos.reshape(-1),
+        "spot_weights": weights,
+        "subspot_data": subspot_lut(n_layers, n_sub, sig, rng),
+    }
+    return {"name": "heterogeneous", "ct": ct, "ct_dims": dims, "ct_resolution": res, "ct_corner": corner,
+            "dose_dims": dims, "dose_resolution": res, "dose_corner": corner, "beam": beam,
+            "energy": proton_tables()}
