@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the pencil-beam dose path: ms per beam dose on the heterogeneous
+256x256x160 CT (2 mm) with one 20-layer proton beam of ~3000 spots.
+
+One step = the whole dose of one beam: host planning, BEV tracing, spot->ray
+fluence, IDD/sigma, tile binning, superposition, transfer into the FP64 dose grid
+and the float readout of the grid, with CT and lookup tables resident in HBM.
+`e2e` repeats the step through the C ABI (pbs_subsecond_wrapper) from pinned host
+buffers, host<->device copies included. Under torchrun every rank computes one
+beam of an opposed-beam plan (gantry 90/270) and the FP64 beam doses are summed
+to rank 0 with one NCCL reduce per step (weak scaling).
+
+`--impl reference` times the reference path's CPU restatement (the oracle port)
+on the host cores; the reference ships no CPU implementation of this path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ms per beam dose (256²×160, 3k spots); served plans/s, p50/p99 latency"
+WORKLOAD = ("heterogeneous CT 256x256x160 at 2 mm (body ellipsoid, lung slab, 2 bone cylinders), "
+            "1 proton beam at gantry 90 deg, 20 layers 70-180 MeV, 3020 spots on a 5 mm hex grid, "
+            "7x7 subspots, 1 mm rays")
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = [r.split(",") for r in Path(self.path).read_text().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _cpu_oracle_ms(case, budget_s=12.0, max_runs=20):
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < max_runs and (not times or time.perf_counter() < t_end):
+        t = time.perf_counter()
+        O.dose(case, threads=threads)
+        times.append((time.perf_counter() - t) * 1e3)
+    return statistics.median(times), threads, len(times)
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from subsecondpbs_b200 import phantoms
+    from oracle import oracle as O
+
+    case = phantoms.heterogeneous_case()
+    threads = os.cpu_count() or 1
+    for _ in range(max(args.warmup, 1)):
+        O.dose(case, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        O.dose(case, threads=threads)
+        times.append((time.perf_counter() - t) * 1e3)
+    ms = statistics.mean(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantom, analytic LUTs in the reference format)",
+        "config": {"workload": WORKLOAD, "l2": "not applicable (CPU)"},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"full workload: {args.steps} beams after {args.warmup} warm-up beams"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from subsecondpbs_b200 import _lib, phantoms
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine, fp32_peak_tflops
+
+    world, rank, local = _dist()
+    if world > 1:
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    case = phantoms.heterogeneous_case()
+    beam = case["beam"] if world == 1 else phantoms.rotate_beam(case["beam"], 90.0 + 180.0 * (rank % 2))
+    dims = case["dose_dims"]
+    n_vox = int(np.prod(dims))
+
+    peak_fp32 = fp32_peak_tflops(local)
+
+    eng = DoseEngine(local, stage_timing=True)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    stream = torch.cuda.ExternalStream(eng.stream_handle, device=dev)
+    out = torch.empty((dims[2], dims[1], dims[0]), dtype=torch.float32, device=dev)
+    d64 = torch.empty((dims[2], dims[1], dims[0]), dtype=torch.float64, device=dev) if world > 1 else None
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    stage_acc = {k: [] for k in _lib.STAGES}
+    prepared = eng.prepare_beam(beam)
+
+    def step():
+        eng.reset_dose()
+        eng.add_beam(prepared)
+        eng.read_dose(out)
+        if d64 is not None:
+            eng.read_dose64(d64)
+            with torch.cuda.stream(stream):
+                dist.reduce(d64, dst=0)
+
+    for _ in range(args.warmup):
+        step()
+        eng.synchronize()
+    stats = eng.beam_stats()
+
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.25)
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    per_step = []
+    t_begin.record(stream)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        per_step.append((e0, e1))
+        for k, v in eng.stage_times().items():
+            stage_acc[k].append(v)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in per_step]
+    ms = float(np.mean(step_ms))
+    total_ms = t_begin.elapsed_time(t_end)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # End to end through the C ABI from pinned host buffers.
+    lib = _lib.load()
+    ct_pin = torch.from_numpy(np.ascontiguousarray(case["ct"], dtype=np.float32)).pin_memory()
+    dose_pin = torch.zeros((dims[2], dims[1], dims[0]), dtype=torch.float32).pin_memory()
+    from subsecondpbs_b200.cudaCalDoseRTD import _with_luts
+
+    energy = _with_luts(case["energy"], None)
+    bd, kb = _lib.beam_desc(beam)
+    ed, ke = _lib.energy_desc(energy)
+    fp = C.POINTER(C.c_float)
+    ct_ptr = C.cast(C.c_void_p(ct_pin.data_ptr()), fp)
+    dose_ptr = C.cast(C.c_void_p(dose_pin.data_ptr()), fp)
+
+    def e2e_call():
+        dose_pin.zero_()
+        rc = lib.pbs_subsecond_wrapper(ct_ptr, _lib.int3(case["ct_dims"]), _lib.float3(case["ct_resolution"]),
+                                       _lib.float3(case["ct_corner"]), dose_ptr, _lib.int3(dims),
+                                       _lib.float3(case["dose_resolution"]), _lib.float3(case["dose_corner"]),
+                                       C.byref(bd), 1, C.byref(ed), local, 0, 0)
+        _lib.check(rc)
+
+    for _ in range(2):
+        e2e_call()
+    e2e_times = []
+    for _ in range(args.e2e_steps):
+        t = time.perf_counter()
+        e2e_call()
+        e2e_times.append((time.perf_counter() - t) * 1e3)
+    e2e_ms = float(np.mean(e2e_times))
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    lut_bytes = sum(np.asarray(energy[k]).nbytes for k in
+                    ("energies_per_u", "peak_depths", "scale_facts", "cidd_matrix", "density_vector", "sp_vector",
+                     "rrl_vector"))
+    beam_bytes = sum(np.asarray(beam[k]).nbytes for k in
+                     ("energies", "spot_sigmas", "layer_spot_counts", "spot_positions", "spot_weights",
+                      "subspot_data"))
+    h2d = int(ct_pin.numel() * 4 + dose_pin.numel() * 4 + lut_bytes + beam_bytes)
+    d2h = int(dose_pin.numel() * 4)
+
+    if rank != 0:
+        dist.destroy_process_group()
+        return 0
+
+    # Roofline of the dominant kernel (superposition, FP32 pipe) and per-stage HBM figures.
+    sup_ms = float(np.mean(stage_acc["superpose"]))
+    fma = float(stats["superpose_fma"])
+    achieved = 2.0 * fma / (sup_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "superpose_traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+        except (ValueError, OSError):
+            traffic = None
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    rays = stats["ray_dims"][0] * stats["ray_dims"][1]
+    pad = stats["superp_dims"][0] * stats["superp_dims"][1]
+    S = stats["tracer_steps"]
+    first = stats["first_inside"]
+    idd_steps = sum(max(eng.layer_stats(l)["after_last_step"] - first, 0) for l in range(stats["num_layers"]))
+    tb = stats["transfer_start"], stats["transfer_max"]
+    box = int(np.prod([max(tb[1][i] - tb[0][i] + 1, 0) for i in range(3)]))
+    stage_ms = {k: float(np.mean(v)) for k, v in stage_acc.items()}
+    stage_bytes = {
+        "trace": 8.0 * rays * S,                      # density + WEPL written
+        "idd": 16.0 * pad * idd_steps,                # density + WEPL read, IDD + sigma written
+        "transfer": 16.0 * box,                       # FP64 dose read-modify-write over the box
+    }
+    roof_stages = []
+    for k, b in stage_bytes.items():
+        if stage_ms[k] > 0:
+            gbs = b / (stage_ms[k] * 1e-3) / 1e9
+            roof_stages.append({"stage": k, "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak,
+                                "unit": "GB/s", "frac": round(gbs / hbm_peak, 4), "algorithmic_bytes": b})
+
+    launches_per_step = int(stats["kernel_launches"]) + 2  # + dose reset and float readout
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cms, threads, runs = _cpu_oracle_ms(case)
+        cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "port",
+               "sample": f"full workload (one 20-layer beam) x {runs} runs, OpenMP over rays and steps"}
+
+    line = {
+        "metric": METRIC,
+        "value": ms / world,
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded phantom, analytic proton LUTs in the reference format)",
+        "config": {"workload": WORKLOAD, "beams_per_step": world, "parallelism": f"beam-sharded x{world}",
+                   "l2": "flushed between timed steps (256 MiB write outside the step events)",
+                   "accumulation": "FP64 dose grid", "total_ms_incl_flush": total_ms},
+        "roofline": {"kernel": "superpose_kernel", "bound": "fp32", "achieved": round(achieved, 3),
+                     "peak": round(peak_fp32, 3), "unit": "TFLOP/s", "frac": round(achieved / peak_fp32, 4),
+                     "traffic": traffic, "peak_source": "in-run FFMA microbenchmark (FP32 pipe, no tensor cores)",
+                     "algorithmic_flops": 2.0 * fma},
+        "roofline_stages": roof_stages,
+        "stages_ms": stage_ms,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers"},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks,
+        "plan": {"ray_dims": stats["ray_dims"], "tracer_steps": S, "live_tiles": stats["live_tiles"],
+                 "superpose_fma": stats["superpose_fma"]},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    del kb, ke
+    return 0
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

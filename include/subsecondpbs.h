@@ -175,6 +175,8 @@ typedef struct PbsBeamStats {
     int transfer_max[3];
     long long live_tiles;     /* superposed (tile, step) pairs over all layers   */
     long long superpose_fma;  /* sum over live tiles of 256*(2R+1)^2             */
+    int kernel_launches;      /* kernels this library launched for the beam      */
+    int layer_chunks;         /* layer chunks the per-layer working set was split into */
 } PbsBeamStats;
 
 typedef struct PbsLayerStats {
@@ -237,6 +239,12 @@ PBS_API int pbs_context_reset_dose(PbsContext* ctx, const float* initial, int in
 PBS_API int pbs_context_add_beam(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction);
 /* Convert the accumulator to float and copy it out (host or device pointer). */
 PBS_API int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device);
+/* Copy the FP64 accumulator [Z][Y][X] out (host or device pointer), e.g. for a
+ * cross-GPU reduction of beam doses. */
+PBS_API int pbs_context_read_dose64(PbsContext* ctx, double* out, int out_on_device);
+/* Measure the FP32 FMA throughput of `gpu_id` with a register-resident FFMA loop
+ * (TFLOP/s, 2 flops per FMA): the denominator of the superposition roofline. */
+PBS_API int pbs_measure_fp32_peak(int gpu_id, double* tflops);
 PBS_API int pbs_context_synchronize(PbsContext* ctx);
 /* cudaStream_t the context enqueues on. */
 PBS_API void* pbs_context_stream(PbsContext* ctx);

@@ -122,6 +122,7 @@ class PbsBeamStats(C.Structure):
         ("first_inside", C.c_int), ("first_outside", C.c_int), ("guaranteed_passive", C.c_int),
         ("transfer_start", _arr(C.c_int, 3)), ("transfer_max", _arr(C.c_int, 3)),
         ("live_tiles", C.c_longlong), ("superpose_fma", C.c_longlong),
+        ("kernel_launches", C.c_int), ("layer_chunks", C.c_int),
     ]
 
 
@@ -187,6 +188,8 @@ def load() -> C.CDLL:
         "pbs_context_reset_dose": (i, [vp, vp, i]),
         "pbs_context_add_beam": (i, [vp, C.POINTER(PbsBeamDesc), i]),
         "pbs_context_read_dose": (i, [vp, vp, i]),
+        "pbs_context_read_dose64": (i, [vp, vp, i]),
+        "pbs_measure_fp32_peak": (i, [i, C.POINTER(C.c_double)]),
         "pbs_context_synchronize": (i, [vp]),
         "pbs_context_stream": (vp, [vp]),
         "pbs_context_dose_device_ptr": (vp, [vp]),

@@ -204,6 +204,17 @@ int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device) {
     return ctx->impl.read_dose(out, out_on_device);
 }
 
+int pbs_context_read_dose64(PbsContext* ctx, double* out, int out_on_device) {
+    if (int rc = guard(ctx)) return rc;
+    if (!out) return PBS_ERR_INVALID_ARGUMENT;
+    return ctx->impl.read_dose64(out, out_on_device);
+}
+
+int pbs_measure_fp32_peak(int gpu_id, double* tflops) {
+    if (!tflops) return PBS_ERR_INVALID_ARGUMENT;
+    return pbs::measure_fp32_peak(gpu_id, tflops);
+}
+
 int pbs_context_synchronize(PbsContext* ctx) {
     if (int rc = guard(ctx)) return rc;
     cudaSetDevice(ctx->impl.device);

@@ -291,6 +291,20 @@ int Context::read_dose(float* out, int onDevice) {
     return PBS_OK;
 }
 
+int Context::read_dose64(double* out, int onDevice) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    PBS_CUDA(cudaMemcpyAsync(out, dose64.ptr, n * 8, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                             stream),
+             "dose64 copy");
+    if (!onDevice) PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    return PBS_OK;
+}
+
 int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
     if (!hasEnergy || !hasCt || !hasDose) {
@@ -475,6 +489,9 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
     if ((rc = mark(7))) return rc;
+    lastChunks = (L + chunk - 1) / chunk;
+    // trace, wepl_min, planner, two fluence kernels, three per chunk, transfer planner, transfer.
+    lastLaunches = 7 + 3 * lastChunks;
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;
@@ -528,6 +545,8 @@ int Context::beam_stats(PbsBeamStats* out) {
     }
     out->live_tiles = h.liveTiles;
     out->superpose_fma = h.superposeFma;
+    out->kernel_launches = lastLaunches;
+    out->layer_chunks = lastChunks;
     if (h.errorFlags) {
         set_error("device reported an error flag (work list overflow)");
         return PBS_ERR_CUDA;

@@ -68,6 +68,8 @@ struct Context {
     BeamPlan plan;
     BeamGeomDev geom{};
     int chunkLayers = 0;
+    int lastLaunches = 0;
+    int lastChunks = 0;
     bool lastBeamValid = false;
     bool lastStageTimed = false;
 
@@ -79,12 +81,15 @@ struct Context {
     int set_dose_grid(const GridDesc& g);
     int reset_dose(const float* init, int onDevice);
     int read_dose(float* out, int onDevice);
+    int read_dose64(double* out, int onDevice);
     int add_beam(const PbsBeamDesc& b, int nuclear);
     int beam_stats(PbsBeamStats* out);
     int layer_stats(int layer, PbsLayerStats* out);
     int stage_times(float* ms, int n);
     int debug_copy(int which, int layer, void* out, size_t bytes);
 };
+
+int measure_fp32_peak(int gpu, double* tflops);
 
 int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
                       float* doseData, const int doseDims[3], const float doseRes[3], const float doseCorner[3],

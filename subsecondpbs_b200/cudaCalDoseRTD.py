@@ -143,10 +143,16 @@ class DoseEngine:
         _lib.check(self._lib.pbs_context_reset_dose(self._h, ptr, on_dev))
         del keep
 
-    def add_beam(self, beam: dict, nuclear_correction: bool = False) -> None:
-        bd, keep = _lib.beam_desc(beam)
+    def add_beam(self, beam, nuclear_correction: bool = False) -> None:
+        """Enqueue the dose of `beam` (a beam dict or a `prepare_beam` result)."""
+        bd, keep = beam if isinstance(beam, tuple) else _lib.beam_desc(beam)
         _lib.check(self._lib.pbs_context_add_beam(self._h, C.byref(bd), int(bool(nuclear_correction))))
         del keep
+
+    @staticmethod
+    def prepare_beam(beam: dict):
+        """Convert a beam dict to its C descriptor once (for repeated add_beam calls)."""
+        return _lib.beam_desc(beam)
 
     def read_dose(self, out=None):
         """Dose as float32 [Z][Y][X]: into `out` (numpy or CUDA tensor) or a new array."""
@@ -154,6 +160,14 @@ class DoseEngine:
             out = np.empty((self.dose_dims[2], self.dose_dims[1], self.dose_dims[0]), dtype=np.float32)
         on_dev, ptr, keep = self._ptr(out, np.float32)
         _lib.check(self._lib.pbs_context_read_dose(self._h, ptr, on_dev))
+        return out
+
+    def read_dose64(self, out=None):
+        """The FP64 accumulator [Z][Y][X] into `out` (numpy or CUDA float64 tensor)."""
+        if out is None:
+            out = np.empty((self.dose_dims[2], self.dose_dims[1], self.dose_dims[0]), dtype=np.float64)
+        on_dev, ptr, keep = self._ptr(out, np.float64)
+        _lib.check(self._lib.pbs_context_read_dose64(self._h, ptr, on_dev))
         return out
 
     def synchronize(self) -> None:
@@ -198,6 +212,14 @@ class DoseEngine:
         if arr is not a and isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous:
             arr = a
         return 0, arr.ctypes.data_as(C.c_void_p), arr
+
+
+def fp32_peak_tflops(gpu_id: int = 0) -> float:
+    """Measured FP32 FMA throughput of the GPU (TFLOP/s)."""
+    lib = _lib.load()
+    v = C.c_double(0.0)
+    _lib.check(lib.pbs_measure_fp32_peak(int(gpu_id), C.byref(v)))
+    return float(v.value)
 
 
 def plan_beam(beam: dict, energy: dict, ct_dims, ct_resolution, ct_corner, dose_dims, dose_resolution,

@@ -131,6 +131,78 @@ def hex_spots(radius_mm: float, pitch_mm: float) -> np.ndarray:
     return np.array(pts, dtype=np.float32)
 
 
+def rotate_beam(beam: dict, gantry_deg: float) -> dict:
+    """Copy of `beam` at another gantry angle (rotation about the z axis through the
+    isocentre at the origin); 90 deg is the beam travelling along -x."""
+    t = np.deg2rad(gantry_deg)
+    d = np.array([-np.sin(t), -np.cos(t), 0.0])
+    out = dict(beam)
+    out["beam_direction"] = tuple(d)
+    out["beam_xdir"] = (float(np.cos(t)), float(-np.sin(t)), 0.0)
+    out["beam_ydir"] = (0.0, 0.0, 1.0)
+    out["source_position"] = tuple(-d * float(beam["sad"]))
+    return out
+
+
+def legacy_beam(beam: dict) -> dict:
+    """The beam without raw spot lists: its spots become the subspot table
+    [L][maxSpots][5] = (x, y, w, sigma_x, sigma_y), which drives the legacy CPB
+    fluence path (raytracedicom_wrapper.cu:3454-3507)."""
+    counts = np.asarray(beam["layer_spot_counts"]).astype(int)
+    pos = np.asarray(beam["spot_positions"], np.float32).reshape(-1, 2)
+    w = np.asarray(beam["spot_weights"], np.float32)
+    sig = np.asarray(beam["spot_sigmas"], np.float32).reshape(-1, 2)
+    m = int(counts.max())
+    sub = np.zeros((len(counts), m, 5), np.float32)
+    off = 0
+    for layer, c in enumerate(counts):
+        sub[layer, :c, 0] = pos[off:off + c, 0]
+        sub[layer, :c, 1] = pos[off:off + c, 1]
+        sub[layer, :c, 2] = w[off:off + c]
+        sub[layer, :c, 3] = sig[layer, 0]
+        sub[layer, :c, 4] = sig[layer, 1]
+        off += c
+    out = {k: v for k, v in beam.items() if k not in ("layer_spot_counts", "spot_positions", "spot_weights")}
+    out["subspot_data"] = sub
+    return out
+
+
+def to_centimetres(case: dict) -> dict:
+    """The same case expressed in centimetres (CT z spacing < 0.3 switches the
+    reference's length unit, raytracedicom_wrapper.cu:2729)."""
+    out = dict(case)
+    for k in ("ct_resolution", "ct_corner", "dose_resolution", "dose_corner"):
+        out[k] = tuple(float(v) / 10.0 for v in case[k])
+    b = dict(case["beam"])
+    b["spot_positions"] = np.asarray(b["spot_positions"], np.float32) / 10.0
+    b["spot_sigmas"] = np.asarray(b["spot_sigmas"], np.float32) / 10.0
+    b["ray_spacing"] = tuple(float(v) / 10.0 for v in b["ray_spacing"])
+    b["source_dist"] = tuple(float(v) / 10.0 for v in b["source_dist"])
+    b["spot_delta"] = tuple(float(v) / 10.0 for v in b["spot_delta"])
+    b["sad"] = float(b["sad"]) / 10.0
+    b["source_position"] = tuple(float(v) / 10.0 for v in b["source_position"])
+    sub = np.asarray(b["subspot_data"], np.float32).copy()
+    sub[..., [0, 1, 3, 4]] /= 10.0
+    b["subspot_data"] = sub
+    out["beam"] = b
+    return out
+
+
+def with_spot_directions(beam: dict, sad_x: float, sad_y: float) -> dict:
+    """Adds per-spot beam directions diverging from virtual sources at sad_x / sad_y
+    (the CarbonPBS beam_dir input from which the reference recovers the source
+    distances, raytracedicom_wrapper.cu:1847-1921)."""
+    bz = np.asarray(beam["beam_direction"], np.float64)
+    bx = np.asarray(beam["beam_xdir"], np.float64)
+    by = np.asarray(beam["beam_ydir"], np.float64)
+    pos = np.asarray(beam["spot_positions"], np.float64).reshape(-1, 2)
+    d = bz[None, :] + bx[None, :] * (pos[:, :1] / sad_x) + by[None, :] * (pos[:, 1:] / sad_y)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    out = dict(beam)
+    out["spot_beam_directions"] = d.astype(np.float32).reshape(-1)
+    return out
+
+
 def heterogeneous_case(dims=(256, 256, 160), res=(2.0, 2.0, 2.0), n_layers=20, e_range=(70.0, 180.0),
                        target_radius_mm=32.0, hex_pitch_mm=5.0, sigma_range=(6.0, 3.0), sad_mm=2000.0,
                        ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 2) -> dict:

@@ -1,0 +1,126 @@
+"""Shared helpers of the parity tests: run the CUDA library and the oracle on the
+same inputs and compare them."""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import oracle as O
+from subsecondpbs_b200 import _lib as L
+
+# Dose tolerance of the path: 0.5 % of Dmax in voxels above 10 % of Dmax, and a
+# 1 %/1 mm gamma pass rate of at least 99.9 %.
+DOSE_TOL_FRAC_DMAX = 5e-3
+GAMMA_PASS_MIN = 0.999
+
+
+def max_rel_err(dose, ref, thr=0.1):
+    dmax = float(ref.max())
+    mask = ref > thr * dmax
+    return float(np.abs(dose.astype(np.float64) - ref)[mask].max() / dmax)
+
+
+def gamma_pass_rate(dose, ref, spacing_mm, dd=0.01, dta_mm=1.0, thr=0.1):
+    """1 %/1 mm global gamma over voxels above `thr` of Dmax; the evaluated dose is
+    sampled at the voxel and at +-dta along each axis (linear interpolation)."""
+    ref = np.asarray(ref, np.float64)
+    ev = np.asarray(dose, np.float64)
+    dmax = ref.max()
+    mask = ref > thr * dmax
+    best = ((ev - ref) / (dd * dmax)) ** 2
+    for axis, sp in zip((2, 1, 0), spacing_mm):
+        f = min(dta_mm / sp, 1.0)
+        for sgn in (-1, 1):
+            nb = np.roll(ev, -sgn, axis=axis)
+            shifted = ev + f * (nb - ev)
+            g = ((shifted - ref) / (dd * dmax)) ** 2 + (f * sp / dta_mm) ** 2
+            best = np.minimum(best, g)
+    return float((best[mask] <= 1.0).mean())
+
+
+def run_gpu(case, beams=None, compat=False, keep_debug=True, initial=None, ct_input_type=None):
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    eng = DoseEngine(0, keep_debug=keep_debug, compat_bev_z_shift=compat, ct_input_type=ct_input_type)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    if initial is not None:
+        eng.reset_dose(np.asarray(initial, np.float32))
+    for b in beams or [case["beam"]]:
+        eng.add_beam(b)
+    eng.synchronize()
+    return eng
+
+
+def stage_report(eng, cap) -> dict:
+    """Per-stage differences between the library's debug buffers and the oracle's
+    captures of the same beam."""
+    pl = cap["plan"]
+    S, RY, RX = pl["steps"], pl["ray_y"], pl["ray_x"]
+    nl = pl["num_layers"]
+    st = eng.beam_stats()
+    rep = {
+        "beam_ints_gpu": [st["first_inside"], st["first_outside"], st["guaranteed_passive"]],
+        "beam_ints_oracle": [int(v) for v in cap["beam_ints"][:3]],
+        "fma_gpu": st["superpose_fma"], "fma_oracle": cap["superpose_fma"],
+    }
+    wepl = eng.debug(L.PBS_DBG_WEPL, 0, (S, RY, RX))
+    dens = eng.debug(L.PBS_DBG_DENSITY, 0, (S, RY, RX))
+    rep["wepl_max_abs_mm"] = float(np.abs(wepl - cap["wepl"]).max())
+    rep["density_max_abs"] = float(np.abs(dens - cap["density"]).max())
+    rep["first_inside_mismatch"] = int((eng.debug(L.PBS_DBG_FIRST_INSIDE, 0, (RY, RX), np.int32)
+                                        != cap["first_inside"]).sum())
+    rep["first_outside_mismatch"] = int((eng.debug(L.PBS_DBG_FIRST_OUTSIDE, 0, (RY, RX), np.int32)
+                                         != cap["first_outside"]).sum())
+    wm = eng.debug(L.PBS_DBG_WEPL_MIN, 0, (S,))
+    rep["wepl_min_max_abs_mm"] = float(np.abs(wm - cap["wepl_min"]).max())
+    rw = eng.debug(L.PBS_DBG_RAY_WEIGHTS, 0, (nl, RY, RX))
+    rep["ray_weight_rel"] = float(np.abs(rw - cap["ray_weights"]).max() / cap["ray_weights"].max())
+    layers = []
+    for l in range(nl):
+        ls = eng.layer_stats(l)
+        oi = cap["layer_ints"][l]
+        lay = {
+            "ints_gpu": [ls["after_last_step"], ls["max_first_passive"], ls["calc_passive"], ls["live_tiles"]],
+            "ints_oracle": [int(v) for v in oi[:4]],
+            "hist_equal": list(ls["tile_rad_counts"]) == [int(v) for v in cap["hist"][l]],
+            "batched_equal": list(ls["batched_counts"]) == [int(v) for v in cap["batched"][l]],
+        }
+        if "idd" in cap:
+            idd = eng.debug(L.PBS_DBG_IDD, l, (S, pl["pitch_y"], pl["pitch_x"]))
+            rs = eng.debug(L.PBS_DBG_RSIGMA, l, (S, pl["pitch_y"], pl["pitch_x"]))
+            codes = eng.debug(L.PBS_DBG_TILE_BINS, l, (S, pl["tiles_y"], pl["tiles_x"]), np.uint8)
+            oidd, ors, oc = cap["idd"][l], cap["rsigma"][l], cap["codes"][l]
+            fin = np.isfinite(rs) & np.isfinite(ors)
+            lay["idd_rel"] = float(np.abs(idd - oidd).max() / max(oidd.max(), 1e-300))
+            lay["rsigma_rel"] = float((np.abs(rs[fin] - ors[fin]) / np.maximum(ors[fin], 1e-30)).max()) if fin.any() else 0.0
+            lay["rsigma_inf_mismatch"] = int((np.isfinite(rs) != np.isfinite(ors)).sum())
+            lay["code_mismatch"] = int(((codes != oc) & (oc != 255)).sum())
+        layers.append(lay)
+    rep["layers"] = layers
+    bev = eng.debug(L.PBS_DBG_BEV_DOSE, 0, (S, pl["bev_y"], pl["bev_x"]))
+    rep["bev_rel"] = float(np.abs(bev - cap["bev"]).max() / max(cap["bev"].max(), 1e-300))
+    return rep
+
+
+def assert_stage_parity(rep, wepl_tol_mm=1e-3):
+    assert rep["beam_ints_gpu"] == rep["beam_ints_oracle"]
+    assert rep["fma_gpu"] == rep["fma_oracle"]
+    assert rep["first_inside_mismatch"] == 0 and rep["first_outside_mismatch"] == 0
+    assert rep["wepl_max_abs_mm"] < wepl_tol_mm
+    assert rep["wepl_min_max_abs_mm"] < wepl_tol_mm
+    assert rep["density_max_abs"] < 1e-5
+    assert rep["ray_weight_rel"] < 1e-5
+    for lay in rep["layers"]:
+        assert lay["ints_gpu"] == lay["ints_oracle"]
+        assert lay["hist_equal"] and lay["batched_equal"]
+        if "idd_rel" in lay:
+            assert lay["code_mismatch"] == 0
+            assert lay["rsigma_inf_mismatch"] == 0
+            assert lay["idd_rel"] < 1e-3
+            assert lay["rsigma_rel"] < 1e-4
+    assert rep["bev_rel"] < 1e-4
+
+
+def oracle_run(case, **kw):
+    return O.dose(case, **kw)
