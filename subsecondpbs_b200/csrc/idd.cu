@@ -256,6 +256,7 @@ bin_plan_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restric
             total = workCapacity;
         }
         beam->workCount = total;
+        beam->workNext = 0;
         beam->liveTiles += acc;
         beam->superposeFma += fma;
         int mp = beam->maxCalcPassive;

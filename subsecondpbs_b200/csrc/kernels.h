@@ -50,7 +50,7 @@ cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const
 // kernelSuperposition<R> (complete_superposition.cu:264-335) over the work list,
 // summing all layers into one BEV dose.
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                             const BeamStateDev* beam, float* bev, int gridBlocks, cudaStream_t s);
+                             BeamStateDev* beam, float* bev, int gridBlocks, cudaStream_t s);
 
 // ---- BEV -> dose ---------------------------------------------------------------
 // Transfer bounding box and parameters (wrapper.cu:5343-5403).

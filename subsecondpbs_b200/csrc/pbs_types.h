@@ -47,6 +47,7 @@ struct BeamStateDev {
     float pxSpMultX, pxSpMultY;
     int maxCalcPassive;
     int workCount;          // superposition work items of the current layer chunk
+    int workNext;           // next unclaimed work item (dynamic scheduling)
     long long liveTiles;
     long long superposeFma;
     int transferStart[3];
