@@ -206,6 +206,13 @@ static float vinterp(const float* v, int n, float idx) {
     return v[f] + (v[f + 1] - v[f]) * dec;
 }
 
+/* Optional emulation of the texture unit's interpolation weights, which hardware
+ * stores as 9-bit fixed point with 8 fractional bits (CUDA programming guide,
+ * texture fetching appendix). 0 = exact weights (default). */
+static int g_texq = 0;
+static double texw(double a) { return g_texq == 1 ? rint(a * 256.0) / 256.0 : (g_texq == 2 ? floor(a * 256.0) / 256.0 : a); }
+void oracle_set_texture_quantization(int on) { g_texq = on; }
+
 /* tex1D linear/clamp/unnormalised evaluated in double. */
 static double lut1(const float* t, int n, double x) {
     double xb = x - 0.5;
@@ -213,7 +220,7 @@ static double lut1(const float* t, int n, double x) {
     if (xb > (double)n) xb = (double)n;
     double fl = floor(xb);
     int i = (int)fl;
-    double a = xb - fl;
+    double a = texw(xb - fl);
     int i0 = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
     int i1 = i + 1 < 0 ? 0 : (i + 1 > n - 1 ? n - 1 : i + 1);
     return (1.0 - a) * t[i0] + a * t[i1];
@@ -229,7 +236,7 @@ static double tri_border(const float* vol, int dx, int dy, int dz, double x, dou
     if (fz > dz + 1.0) fz = dz + 1.0;
     double flx = floor(fx), fly = floor(fy), flz = floor(fz);
     int x0 = (int)flx, y0 = (int)fly, z0 = (int)flz;
-    double tx = fx - flx, ty = fy - fly, tz = fz - flz;
+    double tx = texw(fx - flx), ty = texw(fy - fly), tz = texw(fz - flz);
     double c[2][2][2];
     for (int a = 0; a < 2; ++a)
         for (int b = 0; b < 2; ++b)
@@ -252,7 +259,7 @@ static double tri_border_d(const double* vol, int dx, int dy, int dz, double x, 
     if (z > dz + 1.0) z = dz + 1.0;
     double flx = floor(x), fly = floor(y), flz = floor(z);
     int x0 = (int)flx, y0 = (int)fly, z0 = (int)flz;
-    double tx = x - flx, ty = y - fly, tz = z - flz;
+    double tx = texw(x - flx), ty = texw(y - fly), tz = texw(z - flz);
     double acc = 0.0;
     for (int a = 0; a < 2; ++a)
         for (int b = 0; b < 2; ++b)
@@ -962,7 +969,7 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
             double eb = eIdx;
             if (eb < -1.0) eb = -1.0;
             if (eb > nE) eb = nE;
-            double fl = floor(eb), bb = eb - fl;
+            double fl = floor(eb), bb = texw(eb - fl);
             int e0 = (int)fl < 0 ? 0 : ((int)fl > nE - 1 ? nE - 1 : (int)fl);
             int e1 = (int)fl + 1 < 0 ? 0 : ((int)fl + 1 > nE - 1 ? nE - 1 : (int)fl + 1);
             for (int d = 0; d < nS; ++d)
@@ -997,7 +1004,7 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
                             double xb = xi - 0.5;
                             if (xb < -1.0) xb = -1.0;
                             if (xb > nS) xb = nS;
-                            double fl = floor(xb), aa = xb - fl;
+                            double fl = floor(xb), aa = texw(xb - fl);
                             int i0 = (int)fl < 0 ? 0 : ((int)fl > nS - 1 ? nS - 1 : (int)fl);
                             int i1 = (int)fl + 1 < 0 ? 0 : ((int)fl + 1 > nS - 1 ? nS - 1 : (int)fl + 1);
                             cd_ = (1.0 - aa) * row[i0] + aa * row[i1];

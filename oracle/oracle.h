@@ -90,6 +90,10 @@ int oracle_radius_bucket(float min_rsigma);
  * batched[33] and map[34] (bucket -> processing radius). */
 void oracle_batch(const int hist_in[34], int batched[33], int map[34]);
 
+/* 1: quantise interpolation weights to 1/256 like the texture unit the reference
+ * samples its CT, LUTs, CIDD table and BEV dose with; 0 (default): exact weights. */
+void oracle_set_texture_quantization(int on);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus

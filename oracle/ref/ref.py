@@ -1,0 +1,95 @@
+"""ctypes driver of the reference library built by build_ref.sh (test
+infrastructure only; runs where a GPU and oracle/_ref/ exist)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE.parent / "_ref" / "librtd.so"
+
+
+def available(path: Path = REF_LIB) -> bool:
+    return path.exists()
+
+
+def _load(path: Path = REF_LIB):
+    from subsecondpbs_b200 import _lib as P
+
+    lib = C.CDLL(str(path))
+    fp, ip = C.POINTER(C.c_float), C.POINTER(C.c_int)
+    lib.ref_subsecond_wrapper.restype = C.c_int
+    lib.ref_subsecond_wrapper.argtypes = [fp, ip, fp, fp, fp, ip, fp, fp, C.POINTER(P.PbsBeamDesc), C.c_size_t,
+                                          C.POINTER(P.PbsEnergyDesc), C.c_int, C.c_int, C.c_int]
+    return lib
+
+
+class _CaptureStdout:
+    """Redirects the process-level stdout/stderr (C printf and std::cout) to a file."""
+
+    def __enter__(self):
+        import sys
+
+        sys.stdout.flush()
+        sys.stderr.flush()
+        self.tmp = tempfile.TemporaryFile(mode="w+b")
+        self.saved = (os.dup(1), os.dup(2))
+        os.dup2(self.tmp.fileno(), 1)
+        os.dup2(self.tmp.fileno(), 2)
+        return self
+
+    def __exit__(self, *exc):
+        libc = C.CDLL(None)
+        libc.fflush(None)
+        os.dup2(self.saved[0], 1)
+        os.dup2(self.saved[1], 2)
+        os.close(self.saved[0])
+        os.close(self.saved[1])
+        self.tmp.seek(0)
+        self.text = self.tmp.read().decode(errors="replace")
+        self.tmp.close()
+
+
+_BATCH = re.compile(r"Primary superposition batched launches:((?: \[rad=\d+:\d+\])*)")
+_ITEM = re.compile(r"\[rad=(\d+):(\d+)\]")
+
+
+def run(case: dict, beams=None, nuclear: bool = False, verbose: int = 1, path: Path = REF_LIB):
+    """Run the reference on `case`; returns (dose float32 [Z][Y][X], per-layer batched
+    counts parsed from its verbose output (list of 33-int lists), captured text)."""
+    from subsecondpbs_b200 import _lib as P
+    from subsecondpbs_b200.cudaCalDoseRTD import _with_luts
+
+    lib = _load(path)
+    beams = beams if beams is not None else [case["beam"]]
+    descs, keep = [], []
+    for b in beams:
+        d, k = P.beam_desc(b)
+        descs.append(d)
+        keep.append(k)
+    arr = (P.PbsBeamDesc * len(descs))(*descs)
+    ed, ke = P.energy_desc(_with_luts(case["energy"], None))
+    ct = np.ascontiguousarray(case["ct"], dtype=np.float32)
+    dd = case["dose_dims"]
+    dose = np.zeros((dd[2], dd[1], dd[0]), dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    with _CaptureStdout() as cap:
+        rc = lib.ref_subsecond_wrapper(ct.ctypes.data_as(fp), P.int3(case["ct_dims"]), P.float3(case["ct_resolution"]),
+                                       P.float3(case["ct_corner"]), dose.ctypes.data_as(fp), P.int3(dd),
+                                       P.float3(case["dose_resolution"]), P.float3(case["dose_corner"]), arr,
+                                       len(descs), C.byref(ed), 0, int(nuclear), int(verbose))
+    if rc != 0:
+        raise RuntimeError(f"reference returned {rc}:\n{cap.text[-2000:]}")
+    batched = []
+    for m in _BATCH.finditer(cap.text):
+        row = [0] * 33
+        for r, n in _ITEM.findall(m.group(1)):
+            row[int(r)] = int(n)
+        batched.append(row)
+    del keep, ke
+    return dose, batched, cap.text

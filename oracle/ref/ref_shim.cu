@@ -1,0 +1,104 @@
+// C shim over the reference's subsecondWrapper (test infrastructure only): fills the
+// reference's RTDBeamSettings / RTDEnergyStruct from the flat descriptors of
+// include/subsecondpbs.h so the reference can be driven from ctypes on identical
+// inputs. Compiled together with the reference sources by build_ref.sh.
+#include <cstdio>
+#include <exception>
+#include <vector>
+
+#include "raytracedicom_integration.h"  // the reference's header (include/core)
+#include "../../include/subsecondpbs.h"
+
+namespace {
+
+template <typename T>
+std::vector<T> vec(const T* p, size_t n) {
+    return p && n ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+
+float3 f3(const float* v) { return make_float3(v[0], v[1], v[2]); }
+
+}  // namespace
+
+extern "C" int ref_subsecond_wrapper(const float* ct, const int* ctDims, const float* ctRes, const float* ctCorner,
+                                     float* dose, const int* doseDims, const float* doseRes, const float* doseCorner,
+                                     const PbsBeamDesc* beams, size_t nBeams, const PbsEnergyDesc* e, int gpuId,
+                                     int nuclear, int verbose) {
+    std::vector<RTDBeamSettings> bs(nBeams);
+    for (size_t i = 0; i < nBeams; ++i) {
+        const PbsBeamDesc& d = beams[i];
+        RTDBeamSettings& b = bs[i];
+        b.energies = vec(d.energies, d.n_energies);
+        b.spotSigmas.clear();
+        for (size_t k = 0; 2 * k + 1 < d.n_spot_sigmas; ++k)
+            b.spotSigmas.push_back(make_float2(d.spot_sigmas[2 * k], d.spot_sigmas[2 * k + 1]));
+        b.raySpacing = make_float2(d.ray_spacing[0], d.ray_spacing[1]);
+        b.steps = d.steps;
+        b.sourceDist = make_float2(d.source_dist[0], d.source_dist[1]);
+        b.spotOffset = f3(d.spot_offset);
+        b.spotDelta = f3(d.spot_delta);
+        b.gantryToImOffset = make_float3(0, 0, 0);
+        b.gantryToImMatrix = make_float3(0, 0, 0);
+        b.gantryToDoseOffset = make_float3(0, 0, 0);
+        b.gantryToDoseMatrix = make_float3(0, 0, 0);
+        b.maxSubspotsPerLayer = d.max_subspots_per_layer;
+        b.subspotData = vec(d.subspot_data, d.n_subspot_data);
+        b.layerSpotCounts = vec(d.layer_spot_counts, d.n_layer_spot_counts);
+        b.spotPositions = vec(d.spot_positions, d.n_spot_positions);
+        b.spotPositionsAreIndices = d.spot_positions_are_indices != 0;
+        b.spotWeights = vec(d.spot_weights, d.n_spot_weights);
+        b.spotBeamDirections = vec(d.spot_beam_directions, d.n_spot_beam_directions);
+        b.layerLongitudinalCutoffs = vec(d.layer_longitudinal_cutoffs, d.n_layer_longitudinal_cutoffs);
+        b.waterEquivalence = vec(d.water_equivalence, d.n_water_equivalence);
+        b.rayWeqHeader = vec(d.ray_weq_header, d.n_ray_weq_header);
+        b.profileData = vec(d.profile_data, d.n_profile_data);
+        b.profileSetting = vec(d.profile_setting, d.n_profile_setting);
+        b.beamParaData = vec(d.beam_para_data, d.n_beam_para_data);
+        b.beamDirection = f3(d.beam_direction);
+        b.bmXDirection = f3(d.bm_x_direction);
+        b.bmYDirection = f3(d.bm_y_direction);
+        b.sourcePosition = f3(d.source_position);
+        b.sad = d.sad;
+        b.refPlaneZ = d.ref_plane_z;
+        b.roiLinearIndices = vec(d.roi_linear_indices, d.n_roi_linear_indices);
+    }
+    RTDEnergyStruct es;
+    es.nEnergySamples = e->n_energy_samples;
+    es.nEnergies = e->n_energies;
+    es.energiesPerU = vec(e->energies_per_u, e->n_energies_per_u);
+    es.peakDepths = vec(e->peak_depths, e->n_peak_depths);
+    es.scaleFacts = vec(e->scale_facts, e->n_scale_facts);
+    es.ciddMatrix = vec(e->cidd_matrix, e->n_cidd_matrix);
+    es.nDensitySamples = e->n_density_samples;
+    es.densityScaleFact = e->density_scale_fact;
+    es.densityVector = vec(e->density_vector, e->n_density_vector);
+    es.nSpSamples = e->n_sp_samples;
+    es.spScaleFact = e->sp_scale_fact;
+    es.spVector = vec(e->sp_vector, e->n_sp_vector);
+    es.nRRlSamples = e->n_rrl_samples;
+    es.rRlScaleFact = e->rrl_scale_fact;
+    es.rRlVector = vec(e->rrl_vector, e->n_rrl_vector);
+    if (e->nuc_weight_matrix && e->n_nuc_weight_matrix) {
+        es.nNucEnergySamples = e->n_energy_samples;
+        es.nNucEnergies = e->n_energies;
+        es.nucEnergiesPerU = es.energiesPerU;
+        es.nucPeakDepths = es.peakDepths;
+        es.nucScaleFacts = es.scaleFacts;
+        es.nucWeightMatrix = vec(e->nuc_weight_matrix, e->n_nuc_weight_matrix);
+        es.nucSqSigmaMatrix = vec(e->nuc_sq_sigma_matrix, e->n_nuc_sq_sigma_matrix);
+        es.nuclearTablesAlignedToPrimaryAxis = e->nuclear_tables_aligned_to_primary_axis != 0;
+    }
+    const int3 cd = make_int3(ctDims[0], ctDims[1], ctDims[2]);
+    const int3 dd = make_int3(doseDims[0], doseDims[1], doseDims[2]);
+    try {
+        subsecondWrapper(ct, cd, make_float3(ctRes[0], ctRes[1], ctRes[2]),
+                         make_float3(ctCorner[0], ctCorner[1], ctCorner[2]), dose, dd,
+                         make_float3(doseRes[0], doseRes[1], doseRes[2]),
+                         make_float3(doseCorner[0], doseCorner[1], doseCorner[2]), bs.data(), bs.size(), &es, gpuId,
+                         nuclear != 0, verbose);
+    } catch (const std::exception& ex) {
+        std::fprintf(stderr, "reference threw: %s\n", ex.what());
+        return 2;
+    }
+    return 0;
+}

@@ -1,0 +1,75 @@
+"""Generates the golden fixtures of this directory by running the reference itself.
+
+The reference's dose path is CUDA-only, so this script runs on a GPU machine with
+the reference library built from the reference's own sources by
+oracle/ref/build_ref.sh (oracle/_ref/librtd.so). For every case it stores the
+reference's float32 dose grid and the per-layer batched radius counts the
+reference prints with verbose=1 (complete_superposition.cu:476-495), together with
+the arguments that regenerate the seeded inputs with subsecondpbs_b200.phantoms.
+
+Usage: python tests/golden/make_golden.py --out <dir>
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from subsecondpbs_b200 import phantoms  # noqa: E402
+
+# name -> (builder, kwargs, beam transform)
+CASES = {
+    "water_small": ("water_phantom_case", {"dims": [32, 32, 96], "n_side": 5, "energy_mev": 120.0}, None),
+    "water_config1": ("water_phantom_case", {}, None),
+    "hetero_small": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                            "e_range": [80.0, 120.0]}, None),
+    "hetero_rot30": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                            "e_range": [80.0, 120.0]}, {"rotate": 30.0}),
+    "hetero_legacy": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 2, "target_radius_mm": 12.0,
+                                             "e_range": [90.0, 110.0]}, {"legacy": True}),
+}
+
+
+def build_case(name: str):
+    builder, kw, tf = CASES[name]
+    kw = {k: (tuple(v) if isinstance(v, list) else v) for k, v in kw.items()}
+    case = getattr(phantoms, builder)(**kw)
+    beam = case["beam"]
+    if tf and "rotate" in tf:
+        beam = phantoms.rotate_beam(beam, tf["rotate"])
+    if tf and tf.get("legacy"):
+        beam = phantoms.legacy_beam(beam)
+    return case, beam
+
+
+def main(argv=None) -> int:
+    from oracle.ref import ref
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--cases", nargs="*", default=list(CASES))
+    a = ap.parse_args(argv)
+    out = Path(a.out)
+    out.mkdir(parents=True, exist_ok=True)
+    for name in a.cases:
+        case, beam = build_case(name)
+        dose, batched, text = ref.run(case, beams=[beam], verbose=1)
+        builder, kw, tf = CASES[name]
+        meta = {"case": name, "builder": builder, "kwargs": kw, "transform": tf,
+                "reference": "Nelgcis/subsecondPBS subsecondWrapper built by oracle/ref/build_ref.sh (NUCLEAR_CORR=OFF)",
+                "dose_max": float(dose.max()), "dose_sum": float(dose.sum())}
+        np.savez_compressed(out / f"{name}.npz", dose=dose.astype(np.float32),
+                            batched=np.asarray(batched, np.int32).reshape(-1, 33), meta=json.dumps(meta))
+        (out / f"{name}.log").write_text(text[-20000:])
+        print(name, dose.shape, float(dose.max()), len(batched), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

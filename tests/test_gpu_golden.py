@@ -1,0 +1,25 @@
+"""The CUDA library against outputs of the reference itself (tests/golden, see
+test_cpu_golden.py), with the reference's BEV depth indexing reproduced
+(PBS_OPT_COMPAT_BEV_Z_SHIFT)."""
+import numpy as np
+import pytest
+
+from _parity import gamma_pass_rate, max_rel_err, run_gpu
+from test_cpu_golden import PINS, load_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(PINS))
+def test_cuda_matches_reference_outputs(name):
+    z, meta, case, beam = load_case(name)
+    tol, gmin, flips = PINS[name]
+    eng = run_gpu(case, beams=[beam], compat=True, keep_debug=False)
+    dose = eng.read_dose()
+    ref = z["dose"].astype(np.float64)
+    assert max_rel_err(dose, ref) < tol
+    assert gamma_pass_rate(dose, ref, case["dose_resolution"]) >= gmin
+    moved = 0
+    for l in range(z["batched"].shape[0]):
+        moved += int(np.abs(np.asarray(eng.layer_stats(l)["batched_counts"]) - z["batched"][l]).sum()) // 2
+    assert moved <= flips
