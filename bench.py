@@ -281,7 +281,7 @@ def run_ours(args):
     tfile = ROOT / "profiles" / "superpose_traffic.json"
     if tfile.exists():
         try:
-            traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+            traffic = json.loads(tfile.read_text()).get("dram_bytes_per_beam")
         except (ValueError, OSError):
             traffic = None
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}

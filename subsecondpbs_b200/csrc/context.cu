@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -104,6 +105,9 @@ int Context::init(int gpu) {
     PBS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     PBS_CUDA(cudaEventCreateWithFlags(&stagingEvent, cudaEventDisableTiming), "cudaEventCreate");
     for (auto& e : ev) PBS_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    // Callers of the reference-shaped entry points cannot pass options: the
+    // environment selects the reference's BEV depth shift for them.
+    if (const char* v = std::getenv("PBS_COMPAT_BEV_Z_SHIFT")) compatBevZShift = std::atoi(v) != 0;
     return PBS_OK;
 }
 
@@ -382,6 +386,10 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
         (rc = firstPassive.ensure(size_t(chunk) * rays * 4)) || (rc = lp.ensure(size_t(L) * sizeof(LayerParamsDev))) ||
         (rc = ls.ensure(size_t(L) * sizeof(LayerStateDev))) || (rc = bs.ensure(sizeof(BeamStateDev))))
         return rc;
+    if (idd_smem_bytes(g, luts) > size_t(200) * 1024) {
+        set_error("beam needs " + std::to_string(P.tracerSteps) + " tracer steps; at most ~3000 are supported");
+        return PBS_ERR_UNSUPPORTED;
+    }
     if (keepDebug && chunk < L) {
         set_error("PBS_OPT_KEEP_DEBUG needs every layer of the beam in one chunk; raise PBS_OPT_LAYER_BUDGET_MIB");
         return PBS_ERR_OUT_OF_MEMORY;
@@ -451,11 +459,10 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     PBS_CUDA(cudaMemsetAsync(dBev, 0, S * g.bevX * g.bevY * 4, stream), "memset BEV");
     if ((rc = mark(0))) return rc;
     PBS_CUDA(launch_trace(g, luts, static_cast<const float*>(ct.ptr), ctGrid.dims[0], ctGrid.dims[1], ctGrid.dims[2],
-                          dDens, dWepl, dFi, dFo, dbs, stream),
+                          dDens, dWepl, dFi, dFo, static_cast<float*>(weplMin.ptr), dbs, stream),
              "trace");
-    PBS_CUDA(launch_wepl_min(g, dWepl, dFo, static_cast<float*>(weplMin.ptr), stream), "wepl_min");
     if ((rc = mark(1))) return rc;
-    PBS_CUDA(launch_beam_planner(g, static_cast<const float*>(weplMin.ptr), dlp, dls, dbs, stream), "beam_planner");
+    PBS_CUDA(launch_beam_planner(g, static_cast<float*>(weplMin.ptr), dlp, dls, dbs, stream), "beam_planner");
     if ((rc = mark(2))) return rc;
     if (P.hasLattice) {
         PBS_CUDA(launch_conv_lattice(g, static_cast<const float*>(lattice.ptr), static_cast<float*>(interm.ptr), dRayW,
@@ -482,7 +489,7 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
                  "bin_plan");
         if (l0 == 0 && (rc = mark(5))) return rc;
         PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
-                                  static_cast<const int4*>(work.ptr), dbs, dBev, smCount * 2, stream),
+                                  static_cast<const int4*>(work.ptr), dbs, dBev, smCount, stream),
                  "superpose");
     }
     if ((rc = mark(6))) return rc;
@@ -490,8 +497,9 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
     if ((rc = mark(7))) return rc;
     lastChunks = (L + chunk - 1) / chunk;
-    // trace, wepl_min, planner, two fluence kernels, three per chunk, transfer planner, transfer.
-    lastLaunches = 7 + 3 * lastChunks;
+    // trace, planner, two fluence kernels, five per chunk (IDD, layer plan, work
+    // scatter, two superposition ranges), transfer planner, transfer.
+    lastLaunches = 6 + 5 * lastChunks;
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;

@@ -1,8 +1,10 @@
 // Per-layer integrated depth dose and effective sigma along every ray, fused with the
-// per-tile radius reduction, and the device-side radius histogram / batching that
-// turns the tile codes into a radius-sorted superposition work list.
+// per-tile radius reduction and the per-layer radius histogram, followed by the
+// device-side batching (one small CTA) and the radius-sorted work-list scatter.
 #include <float.h>
 #include <limits.h>
+
+#include <algorithm>
 
 #include "device_util.cuh"
 #include "kernels.h"
@@ -19,18 +21,23 @@ constexpr float kSigmaDelta = 0.21f;
 constexpr int kMaxChunkLayers = 64;
 
 // One CTA = one 32x8 tile of rays for one layer. Each thread walks its ray from the
-// beam's first-inside step to the layer's cut-off step; after every step the CTA
-// reduces min(rSigmaEff) and any(idd > 0) over the tile and stores the radius bucket.
+// beam's first-inside step to the layer's cut-off step (fillIddAndSigmaKernel,
+// idd_sigma.cu:46-259). After every step each warp reduces min(rSigmaEff) and
+// any(idd > 0) over its 32 rays into shared memory; once the walk is done the CTA
+// turns the eight warp partials of every step into the tile's radius bucket
+// (tileRadCalc, complete_superposition.cu:198-255), stores the code and adds the
+// tile's bucket counts to the layer histogram.
 __global__ void __launch_bounds__(256)
 idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ density,
            const float* __restrict__ wepl, const int* __restrict__ firstInside, const int* __restrict__ firstOutside,
            const float* __restrict__ rayW, const LayerParamsDev* __restrict__ lp, LayerStateDev* __restrict__ ls,
            const BeamStateDev* __restrict__ beam, float* __restrict__ iddOut, float* __restrict__ rsigOut,
            uint8_t* __restrict__ codes, int* __restrict__ firstPassiveOut) {
-    extern __shared__ float ciddRow[];
-    __shared__ float shMin[2][8];
-    __shared__ int shLive[2][8];
-    __shared__ int shPassive[8];
+    extern __shared__ float smem[];
+    float* ciddRow = smem;                                    // [nS]
+    float* partMin = smem + luts.nS;                          // [steps][8]
+    int* partLive = reinterpret_cast<int*>(partMin + g.steps * 8);  // [steps][8]
+    __shared__ int shHist[kBuckets], shLive[kBuckets], shPassive[8];
 
     const int lc = blockIdx.z;
     const int l = layer0 + lc;
@@ -57,6 +64,10 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             const float a0 = __ldg(r0 + d), a1 = __ldg(r1 + d);
             ciddRow[d] = a0 + (a1 - a0) * b;
         }
+        if (tid < kBuckets) {
+            shHist[tid] = 0;
+            shLive[tid] = 0;
+        }
     }
     __syncthreads();
 
@@ -66,7 +77,6 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
     float* iddL = iddOut + lc * layerStride;
     float* rsL = rsigOut + lc * layerStride;
-    uint8_t* codeL = codes + static_cast<size_t>(lc) * g.steps * g.tilesX * g.tilesY;
     const size_t ridx = static_cast<size_t>(y) * g.rayX + x;
 
     int firstIn = 0;
@@ -91,7 +101,6 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     float incDiv = p.sigmaSqAirLin + (2.0f * float(first) - 1.0f) * quad;
     float sigmaSq = -incDiv;
 
-    int buf = 0;
     for (int stepNo = first; stepNo < afterLastL; ++stepNo) {
         float res = 0.0f;
         float rSigmaEff = __int_as_float(0x7f800000);
@@ -131,31 +140,18 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             res = 0.0f;
             rSigmaEff = __int_as_float(0x7f800000);
         }
-        const size_t o = static_cast<size_t>(stepNo - first) * padPlane + static_cast<size_t>(y) * g.pitchX + x;
+        const int zr = stepNo - first;
+        const size_t o = static_cast<size_t>(zr) * padPlane + static_cast<size_t>(y) * g.pitchX + x;
         iddL[o] = res;
         rsL[o] = rSigmaEff;
 
-        // Tile reduction: min rSigmaEff and whether any ray deposits.
         float m = rSigmaEff;
         for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, off));
         const int anyLive = __any_sync(0xffffffffu, res > 0.0f);
         if (lane == 0) {
-            shMin[buf][warp] = m;
-            shLive[buf][warp] = anyLive;
+            partMin[zr * 8 + warp] = m;
+            partLive[zr * 8 + warp] = anyLive;
         }
-        __syncthreads();
-        if (tid == 0) {
-            float tm = shMin[buf][0];
-            int tl = shLive[buf][0];
-            for (int w = 1; w < 8; ++w) {
-                tm = fminf(tm, shMin[buf][w]);
-                tl |= shLive[buf][w];
-            }
-            const int R = tile_radius_bucket(tm);
-            codeL[static_cast<size_t>(stepNo - first) * g.tilesX * g.tilesY + ty * g.tilesX + tx] =
-                static_cast<uint8_t>(R | (tl ? 0x80 : 0));
-        }
-        buf ^= 1;
     }
 
     int fp = real ? static_cast<int>(afterLast) : INT_MIN;
@@ -163,6 +159,29 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     for (int off = 16; off > 0; off >>= 1) fp = max(fp, __shfl_xor_sync(0xffffffffu, fp, off));
     if (lane == 0) shPassive[warp] = fp;
     __syncthreads();
+
+    // Tile codes of every step and the tile's histogram contribution.
+    const int nSteps = max(afterLastL - first, 0);
+    uint8_t* codeL = codes + static_cast<size_t>(lc) * g.steps * g.tilesX * g.tilesY;
+    const int tiles = g.tilesX * g.tilesY;
+    for (int zr = tid; zr < nSteps; zr += 256) {
+        float tm = partMin[zr * 8];
+        int tl = partLive[zr * 8];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) {
+            tm = fminf(tm, partMin[zr * 8 + w]);
+            tl |= partLive[zr * 8 + w];
+        }
+        const int R = tile_radius_bucket(tm);
+        codeL[static_cast<size_t>(zr) * tiles + ty * g.tilesX + tx] = static_cast<uint8_t>(R | (tl ? 0x80 : 0));
+        atomicAdd(&shHist[R], 1);
+        if (tl) atomicAdd(&shLive[R], 1);
+    }
+    __syncthreads();
+    if (tid < kBuckets) {
+        if (shHist[tid]) atomicAdd(&ls[l].histAll[tid], shHist[tid]);
+        if (shLive[tid]) atomicAdd(&ls[l].liveHist[tid], shLive[tid]);
+    }
     if (tid == 0) {
         int v = shPassive[0];
         for (int w = 1; w < 8; ++w) v = max(v, shPassive[w]);
@@ -170,118 +189,121 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     }
 }
 
-// Single CTA per layer chunk. Per layer: passive step clamp (wrapper.cu:4975-4990),
-// radius histogram over [first, calcPassive), overflow merge into R=32
-// (complete_superposition.cu:412-460), batching of sparse buckets into the next
-// larger radius (complete_superposition.cu:476-483). Then a radius-descending work
-// list of the live tiles for the whole chunk.
-__global__ void __launch_bounds__(1024)
-bin_plan_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restrict__ codes,
-                LayerStateDev* __restrict__ ls, BeamStateDev* __restrict__ beam, int4* __restrict__ work,
-                int workCapacity) {
-    __shared__ int hist[kBuckets];
-    __shared__ int mapR[kMaxChunkLayers][kBuckets];
-    __shared__ int zCount[kMaxChunkLayers];
-    __shared__ int countR[kMaxR + 1];
-    __shared__ int offR[kMaxR + 1];
-    __shared__ int liveL[kMaxChunkLayers];
-    const int tid = threadIdx.x;
+// One thread per layer of the chunk: passive step (wrapper.cu:4975-4990), histogram
+// over [first, calcPassive) (tiles at steps >= calcPassive hold only dead rays and
+// fall in bucket 0), overflow merge into R=32 (complete_superposition.cu:412-460)
+// and batching of sparse buckets into the radius above them
+// (complete_superposition.cu:476-483). Thread 0 then lays out the chunk's work list
+// in descending radius.
+__global__ void __launch_bounds__(kMaxChunkLayers)
+layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restrict__ ls,
+                  BeamStateDev* __restrict__ beam, int workCapacity) {
+    const int lc = threadIdx.x;
     const int first = beam->firstInside;
     const int tiles = g.tilesX * g.tilesY;
-
-    if (tid <= kMaxR) countR[tid] = 0;
-    for (int lc = 0; lc < nLayers; ++lc) {
-        const int l = layer0 + lc;
-        if (tid < kBuckets) hist[tid] = 0;
-        if (tid == 0) {
-            int calc = ls[l].maxFirstPassive;
-            if (calc < first + 1) calc = first + 1;
-            if (calc < 0) calc = first + 1;
-            if (calc > ls[l].afterLast) calc = ls[l].afterLast;
-            if (calc > g.steps) calc = g.steps;
-            ls[l].calcPassive = calc;
-            zCount[lc] = max(calc - first, 0);
-            liveL[lc] = 0;
+    if (lc < nLayers) {
+        LayerStateDev& st = ls[layer0 + lc];
+        int calc = st.maxFirstPassive;
+        if (calc < first + 1) calc = first + 1;
+        if (calc < 0) calc = first + 1;
+        if (calc > st.afterLast) calc = st.afterLast;
+        if (calc > g.steps) calc = g.steps;
+        st.calcPassive = calc;
+        int hist[kBuckets];
+        for (int i = 0; i < kBuckets; ++i) hist[i] = st.histAll[i];
+        if (st.afterLast > calc && st.afterLast > first) hist[0] -= (st.afterLast - max(calc, first)) * tiles;
+        for (int i = 0; i < kBuckets; ++i) st.hist[i] = hist[i];
+        if (hist[kMaxR + 1] > 0) {
+            hist[kMaxR] += hist[kMaxR + 1];
+            hist[kMaxR + 1] = 0;
         }
-        __syncthreads();
-        const uint8_t* cl = codes + static_cast<size_t>(lc) * g.steps * tiles;
-        const int n = zCount[lc] * tiles;
-        for (int i = tid; i < n; i += blockDim.x) atomicAdd(&hist[cl[i] & 0x3f], 1);
-        __syncthreads();
-        if (tid == 0) {
-            for (int i = 0; i < kBuckets; ++i) ls[l].hist[i] = hist[i];
-            if (hist[kMaxR + 1] > 0) {
-                hist[kMaxR] += hist[kMaxR + 1];
-                hist[kMaxR + 1] = 0;
-            }
-            int layerMax = 0;
-            for (int i = 0; i < kBuckets; ++i)
-                if (hist[i] > 0) layerMax = i;
-            int batched[kMaxR + 1];
-            for (int i = 0; i <= kMaxR; ++i) batched[i] = 0;
-            batched[0] = hist[0];
-            mapR[lc][0] = 0;
-            int recRad = layerMax;
-            for (int rad = layerMax; rad > 0; --rad) {
-                mapR[lc][rad] = recRad;
-                batched[recRad] += hist[rad];
-                if (batched[recRad] >= kMinTilesInBatch) recRad = rad - 1;
-            }
-            for (int rad = layerMax + 1; rad <= kMaxR; ++rad) mapR[lc][rad] = rad;
-            mapR[lc][kMaxR + 1] = mapR[lc][kMaxR];
-            for (int i = 0; i <= kMaxR; ++i) ls[l].batchedCounts[i] = batched[i];
-            for (int i = 0; i < kBuckets; ++i) ls[l].batchedR[i] = mapR[lc][i];
+        int layerMax = 0;
+        for (int i = 0; i < kBuckets; ++i)
+            if (hist[i] > 0) layerMax = i;
+        int batched[kMaxR + 1];
+        int map[kBuckets];
+        for (int i = 0; i <= kMaxR; ++i) batched[i] = 0;
+        for (int i = 0; i < kBuckets; ++i) map[i] = i;
+        batched[0] = hist[0];
+        map[0] = 0;
+        int recRad = layerMax;
+        for (int rad = layerMax; rad > 0; --rad) {
+            map[rad] = recRad;
+            batched[recRad] += hist[rad];
+            if (batched[recRad] >= kMinTilesInBatch) recRad = rad - 1;
         }
-        __syncthreads();
-        for (int i = tid; i < n; i += blockDim.x) {
-            const int c = cl[i];
-            if (c & 0x80) {
-                atomicAdd(&countR[mapR[lc][c & 0x3f]], 1);
-                atomicAdd(&liveL[lc], 1);
-            }
+        map[kMaxR + 1] = map[kMaxR];
+        int live = 0;
+        for (int i = 0; i <= kMaxR; ++i) {
+            st.batchedCounts[i] = batched[i];
+            st.liveR[i] = 0;
+            st.curR[i] = 0;
         }
-        __syncthreads();
-    }
-    if (tid == 0) {
-        int acc = 0;
-        long long fma = 0;
-        for (int r = kMaxR; r >= 0; --r) {
-            offR[r] = acc;
-            acc += countR[r];
-            fma += static_cast<long long>(countR[r]) * 256 * (2 * r + 1) * (2 * r + 1);
+        for (int b = 0; b < kBuckets; ++b) {
+            st.batchedR[b] = map[b];
+            st.liveR[map[b]] += st.liveHist[b];
+            live += st.liveHist[b];
         }
-        int total = acc;
-        if (total > workCapacity) {
-            atomicOr(&beam->errorFlags, 1);
-            total = workCapacity;
-        }
-        beam->workCount = total;
-        beam->workNext = 0;
-        beam->liveTiles += acc;
-        beam->superposeFma += fma;
-        int mp = beam->maxCalcPassive;
-        for (int lc = 0; lc < nLayers; ++lc) {
-            ls[layer0 + lc].liveTiles = liveL[lc];
-            mp = max(mp, ls[layer0 + lc].calcPassive);
-        }
-        beam->maxCalcPassive = mp;
+        st.liveTiles = live;
     }
     __syncthreads();
-    for (int lc = 0; lc < nLayers; ++lc) {
-        const uint8_t* cl = codes + static_cast<size_t>(lc) * g.steps * tiles;
-        const int n = zCount[lc] * tiles;
-        for (int i = tid; i < n; i += blockDim.x) {
-            const int c = cl[i];
-            if (c & 0x80) {
-                const int R = mapR[lc][c & 0x3f];
-                const int slot = atomicAdd(&offR[R], 1);
-                if (slot < workCapacity) work[slot] = make_int4(lc, i % tiles, i / tiles, R);
+    if (lc == 0) {
+        int acc = 0;
+        long long fma = 0;
+        int mp = beam->maxCalcPassive;
+        int split = 0;
+        for (int r = kMaxR; r >= 0; --r) {
+            if (r == kSplitR) split = acc;
+            for (int q = 0; q < nLayers; ++q) {
+                LayerStateDev& st = ls[layer0 + q];
+                st.offR[r] = acc;
+                acc += st.liveR[r];
+                fma += static_cast<long long>(st.liveR[r]) * 256 * (2 * r + 1) * (2 * r + 1);
             }
         }
+        for (int q = 0; q < nLayers; ++q) mp = max(mp, ls[layer0 + q].calcPassive);
+        beam->maxCalcPassive = mp;
+        if (acc > workCapacity) {
+            atomicOr(&beam->errorFlags, 1);
+            acc = workCapacity;
+        }
+        beam->workCount = acc;
+        beam->workNext = 0;
+        beam->workSplit = min(split, acc);
+        beam->workNextSmall = 0;
+        beam->liveTiles += acc;
+        beam->superposeFma += fma;
+    }
+}
+
+// One thread per (layer, step, tile) code of the chunk: live tiles are written to
+// their layer's radius group of the work list.
+__global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restrict__ codes,
+                                    LayerStateDev* __restrict__ ls, const BeamStateDev* __restrict__ beam,
+                                    int4* __restrict__ work, int workCapacity) {
+    const int tiles = g.tilesX * g.tilesY;
+    const int first = beam->firstInside;
+    const size_t perLayer = static_cast<size_t>(g.steps) * tiles;
+    const size_t total = perLayer * nLayers;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int lc = int(i / perLayer);
+        const int rem = int(i - size_t(lc) * perLayer);
+        const int zr = rem / tiles;
+        LayerStateDev& st = ls[layer0 + lc];
+        if (zr >= st.afterLast - first) continue;
+        const int c = codes[i];
+        if (!(c & 0x80)) continue;
+        const int R = st.batchedR[c & 0x3f];
+        const int slot = st.offR[R] + atomicAdd(&st.curR[R], 1);
+        if (slot < workCapacity) work[slot] = make_int4(lc, rem - zr * tiles, zr, R);
     }
 }
 
 }  // namespace
+
+size_t idd_smem_bytes(const BeamGeomDev& g, const LutsDev& luts) {
+    return static_cast<size_t>(luts.nS) * sizeof(float) + static_cast<size_t>(g.steps) * 8 * (sizeof(float) + sizeof(int));
+}
 
 cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, int nLayers, const float* density,
                        const float* wepl, const int* firstInside, const int* firstOutside, const float* rayW,
@@ -289,7 +311,9 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
                        float* rsigma, uint8_t* codes, int* firstPassive, cudaStream_t s) {
     dim3 grid(g.tilesX, g.tilesY, nLayers);
     dim3 block(32, 8);
-    const size_t smem = static_cast<size_t>(luts.nS) * sizeof(float);
+    const size_t smem = idd_smem_bytes(g, luts);
+    cudaError_t e = cudaFuncSetAttribute(idd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
     idd_kernel<<<grid, block, smem, s>>>(g, luts, layer0, density, wepl, firstInside, firstOutside, rayW, lp, ls, beam,
                                          idd, rsigma, codes, firstPassive);
     return cudaGetLastError();
@@ -298,7 +322,10 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
                             BeamStateDev* beam, int4* work, int workCapacity, cudaStream_t s) {
     if (nLayers > kMaxChunkLayers) return cudaErrorInvalidValue;
-    bin_plan_kernel<<<1, 1024, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work, workCapacity);
+    layer_plan_kernel<<<1, kMaxChunkLayers, 0, s>>>(g, layer0, nLayers, ls, beam, workCapacity);
+    const size_t total = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY * nLayers;
+    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 8));
+    work_scatter_kernel<<<blocks, 256, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work, workCapacity);
     return cudaGetLastError();
 }
 

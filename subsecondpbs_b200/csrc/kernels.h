@@ -16,16 +16,15 @@ cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, i
 cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStream_t s);
 
 // ---- tracing ------------------------------------------------------------------
-// rayTracingBEVKernel (src/core/bev_ray_tracing.cu:65-159) as a segmented scan.
+// rayTracingBEVKernel (src/core/bev_ray_tracing.cu:65-159) as a segmented scan,
+// with the per-step WEPL minimum of sliceMinVarIgnoreNeverEnter
+// (src/core/raytracedicom_wrapper.cu:1991-2023) folded into its second pass.
 cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ctHu1000, int ctX, int ctY, int ctZ,
-                         float* density, float* wepl, int* firstInside, int* firstOutside, BeamStateDev* beam,
-                         cudaStream_t s);
-// sliceMinVarIgnoreNeverEnter (src/core/raytracedicom_wrapper.cu:1991-2023).
-cudaError_t launch_wepl_min(const BeamGeomDev& g, const float* wepl, const int* firstOutside, float* weplMin,
-                            cudaStream_t s);
+                         float* density, float* wepl, int* firstInside, int* firstOutside, float* weplMin,
+                         BeamStateDev* beam, cudaStream_t s);
 // Beam planner: guaranteed passive step, entry plane, per-layer cut-off steps and
 // entry sigmas (wrapper.cu:3651-3700, 3733-3833, 4302-4313).
-cudaError_t launch_beam_planner(const BeamGeomDev& g, const float* weplMin, const LayerParamsDev* lp,
+cudaError_t launch_beam_planner(const BeamGeomDev& g, float* weplMin, const LayerParamsDev* lp,
                                 LayerStateDev* ls, BeamStateDev* beam, cudaStream_t s);
 
 // ---- spot -> ray fluence ----------------------------------------------------
@@ -37,6 +36,8 @@ cudaError_t launch_conv_cpb(const BeamGeomDev& g, const float* subspots, int max
                             cudaStream_t s);
 
 // ---- IDD / sigma + tile radius codes -----------------------------------------
+// Dynamic shared memory the IDD kernel needs (CIDD row + per-step warp partials).
+size_t idd_smem_bytes(const BeamGeomDev& g, const LutsDev& luts);
 // fillIddAndSigmaKernel (src/algorithms/idd_sigma.cu:46-259) fused with the
 // per-tile radius reduction of tileRadCalc (complete_superposition.cu:198-255).
 cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, int nLayers, const float* density,
@@ -48,9 +49,10 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
                             BeamStateDev* beam, int4* work, int workCapacity, cudaStream_t s);
 // kernelSuperposition<R> (complete_superposition.cu:264-335) over the work list,
-// summing all layers into one BEV dose.
+// summing all layers into one BEV dose: two persistent launches (radii 16..32,
+// then 0..15) sized for `numSMs` multiprocessors.
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                             BeamStateDev* beam, float* bev, int gridBlocks, cudaStream_t s);
+                             BeamStateDev* beam, float* bev, int numSMs, cudaStream_t s);
 
 // ---- BEV -> dose ---------------------------------------------------------------
 // Transfer bounding box and parameters (wrapper.cu:5343-5403).

@@ -36,6 +36,11 @@ struct LayerStateDev {
     int batchedR[kBuckets];     // bucket -> processing radius
     int batchedCounts[33];
     int liveTiles;
+    int histAll[kBuckets];      // histogram over [first, afterLast) accumulated by the IDD kernel
+    int liveHist[kBuckets];     // live tiles per raw bucket
+    int liveR[33];              // live tiles per processing radius
+    int offR[33];               // first work-list slot of this layer's radius-R items
+    int curR[33];               // scatter cursors
 };
 
 // Beam-level values produced on the device.
@@ -47,7 +52,9 @@ struct BeamStateDev {
     float pxSpMultX, pxSpMultY;
     int maxCalcPassive;
     int workCount;          // superposition work items of the current layer chunk
-    int workNext;           // next unclaimed work item (dynamic scheduling)
+    int workNext;           // next unclaimed item of radius > 15 (dynamic scheduling)
+    int workSplit;          // items of radius > 15 (they lead the radius-sorted list)
+    int workNextSmall;      // next unclaimed item of radius <= 15, relative to workSplit
     long long liveTiles;
     long long superposeFma;
     int transferStart[3];

@@ -4,18 +4,24 @@
 // 32x8 tile of source rays at one step of one layer with its batched radius R
 // (kernelSuperposition<R>, complete_superposition.cu:264-335). Every source s
 // spreads idd_s * e_s(dy) * e_s(dx) over a (2R+1)^2 footprint, where
-// e_s(0) = erf(r/2) and e_s(i) = (erf((i+1/2) r) - erf((i-1/2) r)) / 2.
+// e_s(0) = erf(r/2) and e_s(k) = (erf((k+1/2) r) - erf((k-1/2) r)) / 2.
 //
-// Register-blocked formulation (FP32 FMA pipe):
-//   * a CTA owns one tile; warp w owns source row w of the tile;
-//   * lanes are output columns (one 32-column chunk at a time); each lane keeps
-//     the 2R+1 output rows its source row reaches in registers;
-//   * per source, the lane factor idd_s * e_s(|dx|) is one shared-memory load and
-//     the row factors e_s(0..R) are broadcast 16-byte loads, each reused for the
-//     two symmetric rows R-k and R+k, feeding 2R+1 FMAs;
-//   * the eight warps' partial rows are summed in a shared tile and the tile is
-//     added to the BEV dose of its step (all layers share one BEV volume).
-// A persistent grid pulls items from the list with an atomic counter.
+// Formulation on the FP32 FMA pipe (one CTA per tile, persistent grid):
+//   * table phase: each thread builds its source's rows e_s(0..R) (float4 chunks,
+//     chunk-major so that the stores and the broadcast reads are conflict-free)
+//     and idd_s * e_s(0..R) (odd row stride);
+//   * accumulation phase: a warp lane is one column offset d in [-R, R] of one
+//     source column; a source column's eight sources share the lane's output
+//     column, so the lane keeps the whole footprint height (8+2R rows) in
+//     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. When 2R+1 <= 32
+//     several source columns, spaced so that their footprints are disjoint, share
+//     one warp instruction; wider footprints split into 32-column chunks. A column
+//     ends with one shared-memory add per footprint row; columns without a
+//     depositing source are skipped;
+//   * the tile footprint is then added to the BEV dose of its step (all layers of
+//     the beam share one BEV volume).
+// Radii up to 15 and radii 16..32 run as two instances of the kernel: the small
+// one needs a third of the registers and shared memory and runs three CTAs per SM.
 #include "kernels.h"
 
 namespace pbs {
@@ -23,146 +29,232 @@ namespace pbs {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kEStride = 36;                      // >= kMaxR + 1, multiple of 4 (16-byte rows)
-constexpr int kOutH = kTileY + 2 * kMaxR;         // 72
-constexpr int kOutW = kTileX + 2 * kMaxR;         // 96
-constexpr size_t kSmemBytes = (2 * kThreads * kEStride + kOutH * kOutW) * sizeof(float);
+constexpr int kWarps = kThreads / 32;
 
-template <int R>
-__device__ __forceinline__ void superpose_rows(const float* __restrict__ E, const float* __restrict__ EW,
-                                               float* __restrict__ out, int warp, int lane) {
-    constexpr int N = 2 * R + 1;
+template <int RMax>
+struct Shape {
+    static constexpr int kQ = (RMax + 1 + 3) / 4;            // float4 chunks of e_s(k), k <= RMax
+    static constexpr int kEWStride = (RMax + 1) | 1;          // odd: lanes of one row hit distinct banks
+    static constexpr int kOutFloats = (kTileY + 2 * RMax) * (kTileX + 2 * RMax);
+    static constexpr size_t kSmemBytes =
+        (size_t(kQ) * kThreads * 4 + size_t(kThreads) * kEWStride + kOutFloats) * sizeof(float);
+};
+
+// Slot of source s in the chunk-major e_s table: the low three bits are XORed with
+// bits 3..5 so that source columns 8, 16 or 32 apart (read together by the lane
+// groups of one instruction) land in different banks.
+__device__ __forceinline__ int e4_slot(int s) { return s ^ ((s >> 3) & 7); }
+
+struct TileArgs {
+    const float* idd;
+    const float* rsig;
+    float* bev;
+    size_t src;        // this thread's source ray in the IDD / rSigma arrays
+    float* dst;        // footprint origin in the BEV dose
+    int bevX;
+};
+
+// Table phase, accumulation phase and write-out of one tile at radius R.
+template <int R, int RMax>
+__device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* __restrict__ EW,
+                                               float* __restrict__ out, unsigned* __restrict__ sMask,
+                                               const TileArgs& a) {
+    constexpr int W = 2 * R + 1;
+    constexpr int H = kTileY + 2 * R;
     constexpr int Wo = kTileX + 2 * R;
-    constexpr int kChunks = (Wo + 31) / 32;
-    constexpr int kVec = (R + 1 + 3) / 4;
-    const int sy = warp;
+    constexpr int Q = (R + 1 + 3) / 4;
+    constexpr int EWS = Shape<RMax>::kEWStride;
+    const int t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31;
+
+    // ---- table phase (complete_superposition.cu:298-307) --------------------
+    {
+        const float dose = a.idd[a.src];
+        const bool live = dose > 0.0f;
+        const unsigned mask = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) sMask[warp] = mask;
+        float e[4 * Q];
+        if (live) {
+            const float rs = a.rsig[a.src];
+            float fPrev = erff(rs * 0.5f);
+            e[0] = fPrev;
+#pragma unroll
+            for (int k = 1; k <= R; ++k) {
+                const float f = erff(rs * (float(k) + 0.5f));
+                e[k] = 0.5f * (f - fPrev);
+                fPrev = f;
+            }
+#pragma unroll
+            for (int k = 0; k <= R; ++k) EW[t * EWS + k] = dose * e[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k <= R; ++k) e[k] = 0.0f;
+        }
+#pragma unroll
+        for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
+        const int pt = e4_slot(t);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
+        for (int i = t; i < H * Wo; i += kThreads) out[i] = 0.0f;
+    }
+    __syncthreads();
+
+    // ---- accumulation phase --------------------------------------------------
+    {
+        constexpr bool kGrouped = W <= 32;
+        constexpr int G = kGrouped ? 32 / W : 1;                   // source columns per instruction
+        constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing (>= W: disjoint)
+        constexpr int CH = kGrouped ? 1 : (W + 31) / 32;           // 32-lane chunks of one column
+        constexpr int kUnits = kGrouped ? S : 32 * CH;
+        unsigned lm[kTileY];
+#pragma unroll
+        for (int sy = 0; sy < kTileY; ++sy) lm[sy] = sMask[sy];
 #pragma unroll 1
-    for (int cc = 0; cc < kChunks; ++cc) {
-        const int ox = cc * 32 + lane;
-        float acc[N];
-#pragma unroll
-        for (int j = 0; j < N; ++j) acc[j] = 0.0f;
-        const int sxLo = max(0, cc * 32 - 2 * R);
-        const int sxHi = min(kTileX - 1, cc * 32 + 31);
-        const float* eRow = E + (sy * kTileX) * kEStride;
-        const float* wRow = EW + (sy * kTileX) * kEStride;
-#pragma unroll 2
-        for (int sx = sxLo; sx <= sxHi; ++sx) {
-            const int d = ox - sx - R;  // column offset from the source, in [-R, R] when reached
+        for (int u = warp; u < kUnits; u += kWarps) {
+            int sx, d;
+            bool valid;
+            if (kGrouped) {
+                const int g = lane / W;
+                d = lane - g * W - R;
+                sx = u + g * S;
+                valid = g < G && sx < kTileX;
+            } else {
+                sx = u / CH;
+                d = (u - sx * CH) * 32 + lane - R;
+                valid = d <= R;
+            }
+            if (!valid) {
+                sx = 0;
+                d = 0;
+            }
             const int ad = d < 0 ? -d : d;
-            const float w = (ad <= R) ? wRow[sx * kEStride + ad] : 0.0f;
-            const float4* ev = reinterpret_cast<const float4*>(eRow + sx * kEStride);
+            unsigned colLive = 0;
 #pragma unroll
-            for (int q = 0; q < kVec; ++q) {
-                const float4 v = ev[q];
-                const float e4[4] = {v.x, v.y, v.z, v.w};
+            for (int sy = 0; sy < kTileY; ++sy) colLive |= ((lm[sy] >> sx) & 1u) << sy;
+            if (!valid) colLive = 0;
+            if (!__any_sync(0xffffffffu, colLive != 0)) continue;
+            float acc[H];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const int k = 4 * q + c;
-                    if (k <= R) {
-                        acc[R + k] = fmaf(w, e4[c], acc[R + k]);
-                        if (k > 0) acc[R - k] = fmaf(w, e4[c], acc[R - k]);
+            for (int i = 0; i < H; ++i) acc[i] = 0.0f;
+#pragma unroll
+            for (int sy = 0; sy < kTileY; ++sy) {
+                const int s = sy * kTileX + sx;
+                const float w = ((colLive >> sy) & 1u) ? EW[s * EWS + ad] : 0.0f;
+                const int ps = e4_slot(s);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const float4 v = E4[q * kThreads + ps];
+                    const float ev[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int k = 4 * q + c;
+                        if (k <= R) {
+                            acc[sy + R + k] = fmaf(w, ev[c], acc[sy + R + k]);
+                            if (k > 0) acc[sy + R - k] = fmaf(w, ev[c], acc[sy + R - k]);
+                        }
                     }
                 }
             }
-        }
-        if (ox < Wo) {
+            if (colLive) {
+                float* col = out + sx + R + d;
 #pragma unroll
-            for (int j = 0; j < N; ++j)
-                if (acc[j] != 0.0f) atomicAdd(out + (sy + j) * Wo + ox, acc[j]);
+                for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, acc[i]);
+            }
         }
+    }
+    __syncthreads();
+
+    // ---- write-out -------------------------------------------------------------
+    for (int i = t; i < H * Wo; i += kThreads) {
+        const float v = out[i];
+        const int oy = i / Wo, ox = i - oy * Wo;
+        if (v != 0.0f) atomicAdd(a.dst + static_cast<size_t>(oy) * a.bevX + ox, v);
     }
 }
 
-#define PBS_SUPERPOSE_CASE(R) \
-    case R: superpose_rows<R>(E, EW, out, warp, lane); break;
+// Chain of compile-time radii RLo..RHi; returns false if r is outside it.
+template <int R, int RHi, int RMax>
+__device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, float* out, unsigned* sMask,
+                                                const TileArgs& a) {
+    if (r == R) {
+        superpose_tile<R, RMax>(E4, EW, out, sMask, a);
+        return true;
+    }
+    if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sMask, a);
+    return false;
+}
 
-__global__ void __launch_bounds__(kThreads, 2)
+// Persistent CTA loop over the work items [begin, end) of radii RLo..RHi, claimed
+// one at a time through `counter` (the next claim is issued before the current
+// tile runs so that its latency is hidden).
+template <int RLo, int RHi, int MinBlocks>
+__global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
-                 const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev) {
+                 const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev, int small) {
     extern __shared__ __align__(16) float sm[];
-    float* E = sm;                               // [256][kEStride]  e_s(k), k = 0..R
-    float* EW = sm + kThreads * kEStride;        // [256][kEStride]  idd_s * e_s(k)
-    float* out = sm + 2 * kThreads * kEStride;   // [8+2R][32+2R]    tile footprint
-    __shared__ int sItem;
+    float4* E4 = reinterpret_cast<float4*>(sm);                                  // [Q][256] e_s(4q..4q+3), slot e4_slot(s)
+    float* EW = sm + Shape<RHi>::kQ * kThreads * 4;                              // [256][EWS] idd_s e_s(k)
+    float* out = EW + kThreads * Shape<RHi>::kEWStride;                          // [8+2R][32+2R] footprint
+    __shared__ int sItem[2];
+    __shared__ unsigned sMask[kTileY];
 
     const int t = threadIdx.x;
-    const int warp = t >> 5, lane = t & 31;
-    const int count = beam->workCount;
+    const int split = beam->workSplit;
+    const int begin = small ? split : 0;
+    const int end = small ? beam->workCount : split;
+    int* counter = small ? &beam->workNextSmall : &beam->workNext;
     const size_t padPlane = static_cast<size_t>(g.pitchX) * g.pitchY;
     const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
     const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
 
+    if (t == 0) sItem[0] = atomicAdd(counter, 1);
+    __syncthreads();
+    int buf = 0;
     for (;;) {
-        if (t == 0) sItem = atomicAdd(&beam->workNext, 1);
-        __syncthreads();
-        const int w = sItem;
-        if (w >= count) break;
+        const int w = begin + sItem[buf];
+        if (w >= end) break;
+        if (t == 0) sItem[buf ^ 1] = atomicAdd(counter, 1);
         const int4 it = work[w];
         const int lc = it.x, tile = it.y, zRel = it.z, R = it.w;
         const int tx = tile % g.tilesX, ty = tile / g.tilesX;
-        const int Ho = kTileY + 2 * R, Wo = kTileX + 2 * R;
-
-        // Source ray t of the tile: erf-difference table (complete_superposition.cu:298-307).
-        {
-            const int sy = t >> 5, sx = t & 31;
-            const size_t src = lc * layerStride + zRel * padPlane + static_cast<size_t>(ty * kTileY + sy) * g.pitchX +
-                               tx * kTileX + sx;
-            const float dose = idd[src];
-            const float rs = rsig[src];
-            const bool live = dose > 0.0f;
-            float erfNew = erff(rs * 0.5f);
-            float erfOld = -erfNew;
-            float* e = E + t * kEStride;
-            float* ew = EW + t * kEStride;
-            for (int i = 0; i <= R; ++i) {
-                const float dv = 0.5f * (erfNew - erfOld);
-                e[i] = dv;
-                ew[i] = live ? dose * dv : 0.0f;
-                erfOld = erfNew;
-                erfNew = erff(rs * (float(i) + 1.5f));
-            }
-            for (int i = t; i < Ho * Wo; i += kThreads) out[i] = 0.0f;
+        TileArgs a;
+        a.idd = idd;
+        a.rsig = rsig;
+        a.bev = bev;
+        a.src = lc * layerStride + zRel * padPlane + static_cast<size_t>(ty * kTileY + (t >> 5)) * g.pitchX +
+                tx * kTileX + (t & 31);
+        a.dst = bev + static_cast<size_t>(zRel) * bevPlane + static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX +
+                (tx * kTileX - R + kMaxR);
+        a.bevX = g.bevX;
+        if (!dispatch_radius<RLo, RHi, RHi>(R, E4, EW, out, sMask, a)) {
+            if (t == 0) atomicOr(&beam->errorFlags, 2);
         }
+        // Every thread is past the tile (and has read sItem[buf]) before the
+        // next claim lands in that slot.
         __syncthreads();
-
-        switch (R) {
-            PBS_SUPERPOSE_CASE(0) PBS_SUPERPOSE_CASE(1) PBS_SUPERPOSE_CASE(2) PBS_SUPERPOSE_CASE(3)
-            PBS_SUPERPOSE_CASE(4) PBS_SUPERPOSE_CASE(5) PBS_SUPERPOSE_CASE(6) PBS_SUPERPOSE_CASE(7)
-            PBS_SUPERPOSE_CASE(8) PBS_SUPERPOSE_CASE(9) PBS_SUPERPOSE_CASE(10) PBS_SUPERPOSE_CASE(11)
-            PBS_SUPERPOSE_CASE(12) PBS_SUPERPOSE_CASE(13) PBS_SUPERPOSE_CASE(14) PBS_SUPERPOSE_CASE(15)
-            PBS_SUPERPOSE_CASE(16) PBS_SUPERPOSE_CASE(17) PBS_SUPERPOSE_CASE(18) PBS_SUPERPOSE_CASE(19)
-            PBS_SUPERPOSE_CASE(20) PBS_SUPERPOSE_CASE(21) PBS_SUPERPOSE_CASE(22) PBS_SUPERPOSE_CASE(23)
-            PBS_SUPERPOSE_CASE(24) PBS_SUPERPOSE_CASE(25) PBS_SUPERPOSE_CASE(26) PBS_SUPERPOSE_CASE(27)
-            PBS_SUPERPOSE_CASE(28) PBS_SUPERPOSE_CASE(29) PBS_SUPERPOSE_CASE(30) PBS_SUPERPOSE_CASE(31)
-            PBS_SUPERPOSE_CASE(32)
-            default: break;
-        }
-        __syncthreads();
-
-        float* dst = bev + static_cast<size_t>(zRel) * bevPlane + static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX +
-                     (tx * kTileX - R + kMaxR);
-        for (int i = t; i < Ho * Wo; i += kThreads) {
-            const float v = out[i];
-            const int oy = i / Wo, ox = i - oy * Wo;
-            if (v != 0.0f) atomicAdd(dst + static_cast<size_t>(oy) * g.bevX + ox, v);
-        }
-        // The next claim overwrites sItem only after every thread passed the sync below.
-        __syncthreads();
+        buf ^= 1;
     }
 }
 
-#undef PBS_SUPERPOSE_CASE
+template <int RLo, int RHi, int MinBlocks>
+cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                         BeamStateDev* beam, float* bev, int gridBlocks, int small, cudaStream_t s) {
+    auto k = superpose_kernel<RLo, RHi, MinBlocks>;
+    const size_t smem = Shape<RHi>::kSmemBytes;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, small);
+    return cudaGetLastError();
+}
 
 }  // namespace
 
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                             BeamStateDev* beam, float* bev, int gridBlocks, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(superpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kSmemBytes));
+                             BeamStateDev* beam, float* bev, int numSMs, cudaStream_t s) {
+    // Items are sorted by descending radius: the wide radii come first.
+    cudaError_t e = launch_range<kSplitR + 1, kMaxR, 2>(g, idd, rsigma, work, beam, bev, numSMs * 2, 0, s);
     if (e != cudaSuccess) return e;
-    superpose_kernel<<<gridBlocks, kThreads, kSmemBytes, s>>>(g, idd, rsigma, work, beam, bev);
-    return cudaGetLastError();
+    return launch_range<0, kSplitR, 3>(g, idd, rsigma, work, beam, bev, numSMs * 3, 1, s);
 }
 
 }  // namespace pbs

@@ -54,10 +54,16 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
 // One CTA traces 32 neighbouring rays of one ray row; warp w marches depth segment w.
 // Pass 1 sums each segment, the segment sums are prefix-scanned per ray, and pass 2
 // re-marches the segment writing density and compensated cumulative WEPL.
+//
+// Pass 2 also folds each step's WEPL into the per-step minimum over rays
+// (sliceMinVarIgnoreNeverEnter, wrapper.cu:1991-2023): one warp minimum and one
+// atomic per warp and step on the bit patterns of the non-negative WEPL values. In
+// this path every ray has firstStepOutside >= 1 (lastInside starts at 0,
+// bev_ray_tracing.cu:157), so the reference's never-entered filter keeps every ray.
 __global__ void __launch_bounds__(32 * kTraceSegments)
 trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX, int ctY, int ctZ,
              float* __restrict__ density, float* __restrict__ wepl, int* __restrict__ firstInside,
-             int* __restrict__ firstOutside, BeamStateDev* __restrict__ beam) {
+             int* __restrict__ firstOutside, unsigned* __restrict__ weplMinBits, BeamStateDev* __restrict__ beam) {
     const int lane = threadIdx.x, w = threadIdx.y;
     const int x = blockIdx.x * 32 + lane;
     const int y = blockIdx.y;
@@ -105,9 +111,10 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
         spPre += shSp[q][lane];
     }
 
-    // Pass 2: write the per-step samples.
+    // Pass 2: write the per-step samples (every lane runs the loop: it holds the
+    // warp reductions of the step minimum).
     int firstK = kNone, lastK = -1;
-    if (active) {
+    {
         V3 pos = pos0;
         float cumHu = huPre;
         float cum = float(spPre);
@@ -115,16 +122,23 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
         const size_t plane = static_cast<size_t>(g.rayX) * g.rayY;
         size_t idx = static_cast<size_t>(s0) * plane + static_cast<size_t>(y) * g.rayX + x;
         for (int k = s0; k < s1; ++k) {
-            const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
-            cumHu += hu;
-            density[idx] = lut_linear_clamp(luts.density, luts.nDensity, hu * luts.densityScale + 0.5f);
-            const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
-            kahan_add(cum, comp, stepLen * sp);
-            wepl[idx] = cum;
-            if (firstK == kNone && !(cumHu < 150.0f)) firstK = k;
-            if (hu > 150.0f) lastK = k;
-            pos = add(pos, inc);
-            idx += plane;
+            unsigned bits = 0xffffffffu;
+            if (active) {
+                const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+                cumHu += hu;
+                density[idx] = lut_linear_clamp(luts.density, luts.nDensity, hu * luts.densityScale + 0.5f);
+                const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
+                kahan_add(cum, comp, stepLen * sp);
+                wepl[idx] = cum;
+                if (firstK == kNone && !(cumHu < 150.0f)) firstK = k;
+                if (hu > 150.0f) lastK = k;
+                pos = add(pos, inc);
+                idx += plane;
+                // NaN stays out of the minimum, as with the reference's `v < min` test.
+                bits = cum >= 0.0f ? (__float_as_uint(cum) & 0x7fffffffu) : (cum < 0.0f ? 0u : 0xffffffffu);
+            }
+            bits = __reduce_min_sync(0xffffffffu, bits);
+            if (lane == 0 && bits != 0xffffffffu) atomicMin(weplMinBits + k, bits);
         }
     }
     shFirst[w][lane] = firstK;
@@ -157,32 +171,6 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
     }
 }
 
-__global__ void wepl_min_kernel(int nRays, const float* __restrict__ wepl, const int* __restrict__ firstOutside,
-                                float* __restrict__ weplMin) {
-    const int k = blockIdx.x;
-    const float* plane = wepl + static_cast<size_t>(k) * nRays;
-    float m = kInf20;
-    for (int r = threadIdx.x; r < nRays; r += blockDim.x) {
-        if (firstOutside[r] > 0) {
-            const float v = plane[r];
-            if (v < m) m = v;
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        const float other = __shfl_xor_sync(0xffffffffu, m, o);
-        if (other < m) m = other;
-    }
-    __shared__ float part[32];
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float r = part[0];
-        for (int i = 1; i < int(blockDim.x >> 5); ++i)
-            if (part[i] < r) r = part[i];
-        weplMin[k] = r;
-    }
-}
-
 // include/utils/vector_find.h:61-82
 __device__ int find_first_larger_ordered_dev(const float* v, int n, float value) {
     int upper = n - 1, lower = 0;
@@ -196,11 +184,16 @@ __device__ int find_first_larger_ordered_dev(const float* v, int n, float value)
     return lower + 1;
 }
 
-__global__ void beam_planner_kernel(BeamGeomDev g, const float* __restrict__ weplMin,
+__global__ void beam_planner_kernel(BeamGeomDev g, float* __restrict__ weplMin,
                                     const LayerParamsDev* __restrict__ lp, LayerStateDev* __restrict__ ls,
                                     BeamStateDev* __restrict__ beam) {
     __shared__ int shPassive;
     __shared__ float shEntryZ;
+    // Steps that no ray reached keep the cleared pattern: they hold the
+    // reference's INF (Macro.cuh:7).
+    for (int k = threadIdx.x; k < g.steps; k += blockDim.x)
+        if (__float_as_uint(weplMin[k]) == 0xffffffffu) weplMin[k] = kInf20;
+    __syncthreads();
     if (threadIdx.x == 0) {
         const int first = beam->firstInside;
         const float limitAll = fmul(kBpDepthCutoff, g.maxPeakDepthMm);
@@ -244,6 +237,8 @@ __global__ void beam_planner_kernel(BeamGeomDev g, const float* __restrict__ wep
         for (int i = 0; i < kBuckets; ++i) {
             st.hist[i] = 0;
             st.batchedR[i] = 0;
+            st.histAll[i] = 0;
+            st.liveHist[i] = 0;
         }
         for (int i = 0; i < 33; ++i) st.batchedCounts[i] = 0;
     }
@@ -331,21 +326,19 @@ cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStrea
 }
 
 cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ct, int ctX, int ctY, int ctZ,
-                         float* density, float* wepl, int* firstInside, int* firstOutside, BeamStateDev* beam,
-                         cudaStream_t s) {
+                         float* density, float* wepl, int* firstInside, int* firstOutside, float* weplMin,
+                         BeamStateDev* beam, cudaStream_t s) {
+    // 0xff bytes: the largest unsigned pattern, the identity of the atomic minimum.
+    cudaError_t e = cudaMemsetAsync(weplMin, 0xff, sizeof(float) * size_t(g.steps), s);
+    if (e != cudaSuccess) return e;
     dim3 block(32, kTraceSegments);
     dim3 grid((g.rayX + 31) / 32, g.rayY);
-    trace_kernel<<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside, firstOutside, beam);
+    trace_kernel<<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside, firstOutside,
+                                        reinterpret_cast<unsigned*>(weplMin), beam);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wepl_min(const BeamGeomDev& g, const float* wepl, const int* firstOutside, float* weplMin,
-                            cudaStream_t s) {
-    wepl_min_kernel<<<g.steps, 256, 0, s>>>(g.rayX * g.rayY, wepl, firstOutside, weplMin);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_beam_planner(const BeamGeomDev& g, const float* weplMin, const LayerParamsDev* lp,
+cudaError_t launch_beam_planner(const BeamGeomDev& g, float* weplMin, const LayerParamsDev* lp,
                                 LayerStateDev* ls, BeamStateDev* beam, cudaStream_t s) {
     beam_planner_kernel<<<1, 64, 0, s>>>(g, weplMin, lp, ls, beam);
     return cudaGetLastError();

@@ -76,7 +76,10 @@ __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam) {
 
 // primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44). The reference launches
 // ceil(width/32) x ceil(height/8) blocks from the box start, so columns up to the
-// next block boundary inside the dose grid are transferred too.
+// next block boundary inside the dose grid are transferred too. Every voxel is
+// independent, so the z range of a column is split across blockIdx.z.
+constexpr int kTransferZChunk = 8;
+
 __global__ void __launch_bounds__(256)
 transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, const BeamStateDev* __restrict__ beam,
                 double* __restrict__ dose) {
@@ -87,12 +90,15 @@ transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, const BeamStateDev
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x < sx || y < sy || x >= sx + spanX || y >= sy + spanY || x >= g.doseX || y >= g.doseY) return;
+    const int z0 = max(sz, int(blockIdx.z) * kTransferZChunk);
+    const int z1 = min(mz, int(blockIdx.z) * kTransferZChunk + kTransferZChunk - 1);
+    if (z0 > z1) return;
     const TransferParams T = beam->transfer;
     const V3 start = transfer_start(T, x, y);
     const float zShift = g.compatBevZShift ? float(beam->firstInside) : 0.0f;
     const size_t slice = static_cast<size_t>(g.doseX) * g.doseY;
     double* col = dose + static_cast<size_t>(y) * g.doseX + x;
-    for (int z = sz; z <= mz; ++z) {
+    for (int z = z0; z <= z1; ++z) {
         const V3 f = transfer_fan_idx(T, start, z);
         if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
         const float v = bev_sample(bev, g.bevX, g.bevY, g.steps, f.x, f.y, f.z - zShift);
@@ -120,7 +126,7 @@ cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cu
 cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,
                             cudaStream_t s) {
     dim3 block(32, 8);
-    dim3 grid((g.doseX + 31) / 32, (g.doseY + 7) / 8);
+    dim3 grid((g.doseX + 31) / 32, (g.doseY + 7) / 8, (g.doseZ + kTransferZChunk - 1) / kTransferZChunk);
     transfer_kernel<<<grid, block, 0, s>>>(g, bev, beam, dose);
     return cudaGetLastError();
 }
