@@ -245,6 +245,28 @@ PBS_API int pbs_context_read_dose64(PbsContext* ctx, double* out, int out_on_dev
 /* Measure the FP32 FMA throughput of `gpu_id` with a register-resident FFMA loop
  * (TFLOP/s, 2 flops per FMA): the denominator of the superposition roofline. */
 PBS_API int pbs_measure_fp32_peak(int gpu_id, double* tflops);
+
+/* ---- allocation-free stage entry (no counterpart in the reference) ---------
+ * Legacy CPB fluence of `n_layers` layers on the calling thread's current
+ * device: subspots [n_layers][max_subspots][5] = (dx, dy, w, sigma_x, sigma_y)
+ * (device memory) are integrated over the CPB cells and mapped to ray weights
+ * [n_layers][ray_dims[1]][ray_dims[0]] (device memory, caller-owned, fully
+ * written), as the context path does for beams without a spot lattice
+ * (subspotToCPBConvolutionOptimizedKernel + mapCPBWeightsToRayWeightsKernel,
+ * src/algorithms/convolution.cu:95-152, 269-339; wrapper.cu:3454-3507).
+ * It exists for callers that cannot allocate device memory at the time of the
+ * call (a caller-managed memory pool, a process that must not grow its
+ * footprint): the CPB grid is a fixed static device array of 2^20 floats
+ * (4 MiB) per device, so ray_dims[0] * ray_dims[1] * n_layers must not exceed
+ * 1048576 (PBS_ERR_INVALID_ARGUMENT otherwise). No memory is allocated; the
+ * scratch cells used are cleared on `stream` before use. The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress): make that first
+ * call before any stream capture. All calls on one device share the scratch, so
+ * calls that overlap in time (other streams or threads) race and corrupt each
+ * other's result: serialise them. Launches are asynchronous on `stream`. */
+PBS_API int pbs_cpb_fluence_no_alloc(const float* d_subspots, int max_subspots, int n_layers, const int ray_dims[2],
+                                     const float cpb_corner[2], const float cpb_resolution[2], float* d_ray_weights,
+                                     void* stream);
 PBS_API int pbs_context_synchronize(PbsContext* ctx);
 /* cudaStream_t the context enqueues on. */
 PBS_API void* pbs_context_stream(PbsContext* ctx);
