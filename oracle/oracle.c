@@ -706,6 +706,12 @@ static int plan_beam(const PbsBeamDesc* b, const PbsEnergyDesc* e, const int* cd
     }
     P->p.bev_x = P->p.pitch_x + 2 * MAX_R;
     P->p.bev_y = P->p.pitch_y + 2 * MAX_R;
+    if (hasLat) { /* halo lattice padded to the tile size (wrapper.cu:862-864) */
+        P->p.nuc_x = ((P->lat.nx + TILE_X - 1) / TILE_X) * TILE_X;
+        P->p.nuc_y = ((P->lat.ny + TILE_Y - 1) / TILE_Y) * TILE_Y;
+        P->p.nuc_bev_x = P->p.nuc_x + 2 * MAX_R;
+        P->p.nuc_bev_y = P->p.nuc_y + 2 * MAX_R;
+    }
     /* Per-layer energy parameters (wrapper.cu:3926-4053, fill_idd_and_sigma_params.cuh:66-78). */
     P->lp = (float*)calloc((size_t)L * 8, sizeof(float));
     int nE = e->n_energies;
@@ -806,13 +812,177 @@ void oracle_batch(const int hist_in[34], int batched[33], int map[34]) {
 /* ---- pipeline ----------------------------------------------------------------- */
 static double erfd(double x) { return erf(x); }
 
+/* Tile radius codes of one step on a grid of TXg x TYg tiles (tileRadCalc,
+ * complete_superposition.cu:198-255): minimum rSigmaEff and any(idd > 0). */
+static void tile_codes(const double* iddK, const double* rsgK, int PXg, int TXg, int TYg, unsigned char* out) {
+    for (int ty = 0; ty < TYg; ++ty)
+        for (int tx = 0; tx < TXg; ++tx) {
+            double mn = INFINITY;
+            int anyLive = 0;
+            for (int sy = 0; sy < TILE_Y; ++sy)
+                for (int sx = 0; sx < TILE_X; ++sx) {
+                    size_t o = (size_t)(ty * TILE_Y + sy) * PXg + tx * TILE_X + sx;
+                    if (rsgK[o] < mn) mn = rsgK[o];
+                    if (iddK[o] > 0.0) anyLive = 1;
+                }
+            int R = oracle_radius_bucket((float)mn);
+            out[ty * TXg + tx] = (unsigned char)(R | (anyLive ? 0x80 : 0));
+        }
+}
+
+/* kernelSuperposition<R> (complete_superposition.cu:264-335) of the live tiles of
+ * one step into one BEV plane padded by MAX_R on every side. */
+static double superpose_step(const double* iddK, const double* rsgK, const unsigned char* codesK, const int* map,
+                             int PXg, int TXg, int TYg, double* plane, int BXg) {
+    double fma = 0.0, ed[MAX_R + 1];
+    for (int t = 0; t < TXg * TYg; ++t) {
+        unsigned char c = codesK[t];
+        if (!(c & 0x80)) continue;
+        int R = map[c & 0x3f];
+        fma += 256.0 * (2 * R + 1) * (2 * R + 1);
+        int tx = t % TXg, ty = t / TXg;
+        for (int sy = 0; sy < TILE_Y; ++sy)
+            for (int sx = 0; sx < TILE_X; ++sx) {
+                size_t o = (size_t)(ty * TILE_Y + sy) * PXg + tx * TILE_X + sx;
+                double dose_ = iddK[o];
+                if (!(dose_ > 0.0)) continue;
+                double rs = rsgK[o];
+                double en = erf(rs * 0.5), eo = -en;
+                for (int i = 0; i <= R; ++i) {
+                    ed[i] = 0.5 * (en - eo);
+                    eo = en;
+                    en = erf(rs * ((double)i + 1.5));
+                }
+                int oy0 = ty * TILE_Y + sy - R + MAX_R, ox0 = tx * TILE_X + sx - R + MAX_R;
+                for (int i = 0; i < 2 * R + 1; ++i) {
+                    double wy = dose_ * ed[abs(R - i)];
+                    double* rowp = plane + (size_t)(oy0 + i) * BXg + ox0;
+                    for (int j = 0; j < 2 * R + 1; ++j) rowp[j] += wy * ed[abs(R - j)];
+                }
+            }
+    }
+    return fma;
+}
+
+/* Divergent transfer of one layer's BEV dose (wrapper.cu:5343-5505 primary,
+ * 5510-5600 nuclear; prim_transf_kernel.cu:11-78): bounding box of the padded BEV
+ * grid in dose indices, then a trilinear sample per voxel added where positive. */
+static void transfer_layer(const FromFan* fanToDose, int gridX, int gridY, int first, int calc, int passive,
+                           int compat, const double* bev, int BXg, int BYg, double* dose, const int* dd, int box[6]) {
+    box[0] = box[1] = box[2] = 0;
+    box[3] = box[4] = box[5] = -1;
+    const float xs[2] = {-(float)MAX_R, (float)(gridX + MAX_R - 1)};
+    const float ys[2] = {-(float)MAX_R, (float)(gridY + MAX_R - 1)};
+    const float zs[2] = {(float)first, (float)(calc - 1)};
+    V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
+    for (int zi = 0; zi < 2; ++zi)
+        for (int yi = 0; yi < 2; ++yi)
+            for (int xi = 0; xi < 2; ++xi) {
+                V3 p = ffapply(*fanToDose, v3(xs[xi], ys[yi], zs[zi]));
+                mx.x = fmaxf(mx.x, p.x); mx.y = fmaxf(mx.y, p.y); mx.z = fmaxf(mx.z, p.z);
+                mn.x = fminf(mn.x, p.x); mn.y = fminf(mn.y, p.y); mn.z = fminf(mn.z, p.z);
+            }
+    int sx0 = ((int)floorf(mn.x) / 32) * 32;
+    box[0] = sx0 > 0 ? sx0 : 0;
+    box[1] = (int)floorf(mn.y) > 0 ? (int)floorf(mn.y) : 0;
+    box[2] = (int)floorf(mn.z) > 0 ? (int)floorf(mn.z) : 0;
+    box[3] = (int)ceilf(mx.x) < dd[0] - 1 ? (int)ceilf(mx.x) : dd[0] - 1;
+    box[4] = (int)ceilf(mx.y) < dd[1] - 1 ? (int)ceilf(mx.y) : dd[1] - 1;
+    box[5] = (int)ceilf(mx.z) < dd[2] - 1 ? (int)ceilf(mx.z) : dd[2] - 1;
+    if (!(box[0] <= box[3] && box[1] <= box[4] && box[2] <= box[5])) return;
+    ToFan tf = ff_invert_shift(*fanToDose, v3((float)MAX_R, (float)MAX_R, -(float)first));
+    TransferP T = transfer_params(tf);
+    int spanX = ((box[3] - box[0] + 1 + 31) / 32) * 32, spanY = ((box[4] - box[1] + 1 + 7) / 8) * 8;
+    int xEnd = box[0] + spanX < dd[0] ? box[0] + spanX : dd[0];
+    int yEnd = box[1] + spanY < dd[1] ? box[1] + spanY : dd[1];
+    /* The reference's BEV texture spans planes [0, guaranteedPassive). */
+    const int nz = passive;
+    const double zshift = compat ? 0.0 : (double)first;
+    const int b1 = box[1], b0 = box[0], b2 = box[2], b5 = box[5];
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int y = b1; y < yEnd; ++y)
+        for (int x = b0; x < xEnd; ++x)
+            for (int z = b2; z <= b5; ++z) {
+                V3 f = tp_fan(&T, x, y, z);
+                if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
+                double v = tri_border_d(bev, BXg, BYg, nz, f.x, f.y, (double)f.z + zshift);
+                if (v > 0.0) dose[((size_t)z * dd[1] + y) * dd[0] + x] += v;
+            }
+}
+
+/* Energy-interpolated row of a [nE][nS] table at a fixed energy coordinate: the
+ * bilinear texture lookup of the reference is a depth lerp of this row. */
+static void table_row(const float* tab, int nE, int nS, float eIdx, double* row) {
+    double eb = eIdx;
+    if (eb < -1.0) eb = -1.0;
+    if (eb > nE) eb = nE;
+    double fl = floor(eb), bb = texw(eb - fl);
+    int e0 = (int)fl < 0 ? 0 : ((int)fl > nE - 1 ? nE - 1 : (int)fl);
+    int e1 = (int)fl + 1 < 0 ? 0 : ((int)fl + 1 > nE - 1 ? nE - 1 : (int)fl + 1);
+    for (int d = 0; d < nS; ++d)
+        row[d] = (1.0 - bb) * tab[(size_t)e0 * nS + d] + bb * tab[(size_t)e1 * nS + d];
+}
+
+static double row_lookup(const double* row, int nS, double xi) {
+    double xb = xi - 0.5;
+    if (xb < -1.0) xb = -1.0;
+    if (xb > nS) xb = nS;
+    double fl = floor(xb), aa = texw(xb - fl);
+    int i0 = (int)fl < 0 ? 0 : ((int)fl > nS - 1 ? nS - 1 : (int)fl);
+    int i1 = (int)fl + 1 < 0 ? 0 : ((int)fl + 1 > nS - 1 ? nS - 1 : (int)fl + 1);
+    return (1.0 - aa) * row[i0] + aa * row[i1];
+}
+
 static int run_beam(const float* ct, const int* cd, double* dose, const int* dd, const PbsBeamDesc* b,
-                    const PbsEnergyDesc* e, const Plan* P, int compat, OracleCapture* cap) {
+                    const PbsEnergyDesc* e, const Plan* P, int compat, int nucModel, OracleCapture* cap) {
     const int L = P->p.num_layers, S = P->p.steps, RX = P->p.ray_x, RY = P->p.ray_y;
     const int PX = P->p.pitch_x, PY = P->p.pitch_y, TX = P->p.tiles_x, TY = P->p.tiles_y;
     const size_t rays = (size_t)RX * RY, pad = (size_t)PX * PY, tiles = (size_t)TX * TY;
     const int BX = P->p.bev_x, BY = P->p.bev_y;
     const size_t bevPlane = (size_t)BX * BY;
+    /* Nuclear halo plan (buildHaloLatticePlan, wrapper.cu:804-929, driven from
+     * wrapper.cu:3412-3452): the dense spot lattice padded to 32 x 8, and the ray
+     * under every lattice cell. */
+    const int nuc = nucModel >= 0;
+    const int NXn = P->p.nuc_x, NYn = P->p.nuc_y, NTX = NXn / TILE_X, NTY = NYn / TILE_Y;
+    const size_t nucPad = (size_t)NXn * NYn, nucTiles = (size_t)NTX * NTY;
+    const int NBX = P->p.nuc_bev_x, NBY = P->p.nuc_bev_y;
+    const size_t nucBevPlane = (size_t)NBX * NBY;
+    int* rayToNuc = NULL;
+    if (nuc) {
+        if (P->p.conv_mode != 0)
+            return fail(PBS_ERR_INVALID_ARGUMENT,
+                        "nuclear_correction=true requires raw spot lattice inputs; legacy CPB fallback cannot drive halo mode");
+        rayToNuc = (int*)malloc(sizeof(int) * rays);
+        for (size_t r = 0; r < rays; ++r) rayToNuc[r] = -1;
+        for (int sy = 0; sy < P->lat.ny; ++sy) {
+            const float gy = P->lat.oy + (float)sy * P->lat.dy;
+            const int ry = (int)lroundf((gy - P->p.cpb_corner[1]) / P->p.cpb_res[1]);
+            if (ry < 0 || ry >= RY) {
+                free(rayToNuc);
+                return fail(PBS_ERR_GEOMETRY, "dense halo lattice row mapped outside active ray grid");
+            }
+            for (int sx = 0; sx < P->lat.nx; ++sx) {
+                const float gx = P->lat.ox + (float)sx * P->lat.dx;
+                const int rx = (int)lroundf((gx - P->p.cpb_corner[0]) / P->p.cpb_res[0]);
+                if (rx < 0 || rx >= RX) {
+                    free(rayToNuc);
+                    return fail(PBS_ERR_GEOMETRY, "dense halo lattice column mapped outside active ray grid");
+                }
+                rayToNuc[(size_t)ry * RX + rx] = sy * NXn + sx;
+            }
+        }
+    }
+    /* Model constants (idd_sigma.cu:102-121) and the GAUSS_FIT entry-sigma scale
+     * (wrapper.cu:3788-3795, 3834-3841). */
+    double eRefSq = 198.81, sigDelta = 0.21;
+    int suppressDip = 0;
+    float entryScale = 1.0f;
+    if (nuc) {
+        if (nucModel == 0) { eRefSq = 190.44; sigDelta = 0.0; }
+        else if (nucModel == 1) { eRefSq = 216.09; sigDelta = 0.08; }
+        else { eRefSq = 169.00; sigDelta = 0.06; suppressDip = 1; entryScale = 0.97f; }
+    }
     double* dens = (double*)malloc(sizeof(double) * S * rays);
     double* wepl = (double*)malloc(sizeof(double) * S * rays);
     int* fin = (int*)malloc(sizeof(int) * rays);
@@ -871,6 +1041,10 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
             float sgx = base + lp[6] * lp[6], sgy = base + lp[7] * lp[7];
             eSig[2 * l] = sqrtf(sgx > 0.0f ? sgx : 0.0f);
             eSig[2 * l + 1] = sqrtf(sgy > 0.0f ? sgy : 0.0f);
+            if (entryScale != 1.0f) {
+                eSig[2 * l] *= entryScale;
+                eSig[2 * l + 1] *= entryScale;
+            }
         }
 #pragma omp parallel for schedule(dynamic, 1)
         for (int l = 0; l < L; ++l) {
@@ -953,33 +1127,57 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
     double* bevL = (double*)malloc(sizeof(double) * S * bevPlane);
     double* bevSum = cap && cap->bev ? cap->bev : NULL;
     if (bevSum) memset(bevSum, 0, sizeof(double) * S * bevPlane);
+    double *nIdd = NULL, *nRsg = NULL, *nBevL = NULL, *nBevSum = NULL;
+    unsigned char* nCodes = NULL;
+    if (nuc) {
+        nIdd = (double*)malloc(sizeof(double) * S * nucPad);
+        nRsg = (double*)malloc(sizeof(double) * S * nucPad);
+        nCodes = (unsigned char*)malloc((size_t)S * nucTiles);
+        nBevL = (double*)malloc(sizeof(double) * S * nucBevPlane);
+        nBevSum = cap && cap->nuc_bev ? cap->nuc_bev : NULL;
+        if (nBevSum) memset(nBevSum, 0, sizeof(double) * S * nucBevPlane);
+    }
     int maxCalc = first;
-    double fmaTotal = 0.0;
+    double fmaTotal = 0.0, nucFmaTotal = 0.0;
+    int rc = PBS_OK;
     const double NaNinf = INFINITY;
-    for (int l = 0; l < L; ++l) {
+    const int nS = e->n_energy_samples, nE = e->n_energies;
+    double* row = (double*)malloc(sizeof(double) * nS);
+    double* nwRow = (double*)malloc(sizeof(double) * nS);
+    double* nsRow = (double*)malloc(sizeof(double) * nS);
+    for (int l = 0; l < L && rc == PBS_OK; ++l) {
         const float* lp = P->lp + 8 * l;
         const float eIdx = lp[0], escale = lp[1], peak = lp[2];
         const float rangeStop = BP_CUT * peak;
         int afterLastL = ffl_d(wmin, S, BP_CUT * peak);
         if (afterLastL > passive) afterLastL = passive;
-        /* CIDD row at this energy: the bilinear lookup at a fixed energy coordinate. */
-        const int nS = e->n_energy_samples, nE = e->n_energies;
-        double* row = (double*)malloc(sizeof(double) * nS);
-        {
-            double eb = eIdx;
-            if (eb < -1.0) eb = -1.0;
-            if (eb > nE) eb = nE;
-            double fl = floor(eb), bb = texw(eb - fl);
-            int e0 = (int)fl < 0 ? 0 : ((int)fl > nE - 1 ? nE - 1 : (int)fl);
-            int e1 = (int)fl + 1 < 0 ? 0 : ((int)fl + 1 > nE - 1 ? nE - 1 : (int)fl + 1);
-            for (int d = 0; d < nS; ++d)
-                row[d] = (1.0 - bb) * e->cidd_matrix[(size_t)e0 * nS + d] + bb * e->cidd_matrix[(size_t)e1 * nS + d];
+        /* CIDD (and nuclear) rows at this energy. */
+        table_row(e->cidd_matrix, nE, nS, eIdx, row);
+        /* Halo inputs of the layer (wrapper.cu:4111-4135, 4140-4386). */
+        float spotDist = 0.0f, entrySigmaSq = 0.0f;
+        const float* haloW = NULL;
+        if (nuc) {
+            table_row(e->nuc_weight_matrix, nE, nS, eIdx, nwRow);
+            table_row(e->nuc_sq_sigma_matrix, nE, nS, eIdx, nsRow);
+            haloW = P->lat.w + (size_t)l * P->lat.nx * P->lat.ny;
+            const float spacing = b->spot_delta[0] > b->ray_spacing[0] * 1.5f ? b->spot_delta[0] : P->lat.dx;
+            if (fabsf(P->p.fan_delta[0]) > 1e-6f) spotDist = fabsf(spacing / P->p.fan_delta[0]);
+            const float a = 0.00270f / (peak - 4.50f), bq = -4.39f / (peak - 3.86f);
+            entrySigmaSq = a * entryZ * entryZ + bq * entryZ + lp[6] * lp[6];
         }
+        const int nucOn = nuc && spotDist > 0.0f;
+        const double rEref = nucOn ? eRefSq : 198.81, rDelta = nucOn ? sigDelta : 0.21;
+        const int rSuppress = nucOn ? suppressDip : 0;
         for (size_t i = 0; i < (size_t)S * pad; ++i) { idd[i] = 0.0; rsg[i] = NaNinf; }
+        if (nucOn)
+            for (size_t i = 0; i < (size_t)S * nucPad; ++i) { nIdd[i] = 0.0; nRsg[i] = NaNinf; }
         int maxFP = INT_MIN;
         const double quad = lp[4], lin = lp[5];
         const double stepLen = fabs((double)P->p.fan_delta[2]);
-        /* fillIddAndSigmaKernel (idd_sigma.cu:46-259). */
+        /* fillIddAndSigmaKernel (idd_sigma.cu:46-259). A ray without a halo cell
+         * writes no halo value (the reference offsets its -1 index by the first
+         * step before testing it, idd_sigma.cu:131-137, and so races on the last
+         * halo cell of the previous plane). */
 #pragma omp parallel for schedule(dynamic, 8) reduction(max : maxFP)
         for (int y = 0; y < RY; ++y)
             for (int x = 0; x < RX; ++x) {
@@ -988,59 +1186,67 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
                 int al0 = fout[r] < afterLastL ? fout[r] : afterLastL;
                 unsigned afterLast = (unsigned)al0;
                 double w = rayW[(size_t)l * rays + r];
+                const int nIdx = nucOn ? rayToNuc[r] : -1;
+                const double nW = nIdx >= 0 ? (double)haloW[(nIdx / NXn) * P->lat.nx + nIdx % NXn] : 0.0;
                 int live = 1;
                 if (w < 1e-6 || afterLast < (unsigned)first) { live = 0; afterLast = 0; }
                 double spOld = 0.0, cdOld = 0.0, incScat = 0.0, incinc = 0.0;
                 double incDiv = lin + (2.0 * first - 1.0) * quad;
                 double sig2 = -incDiv;
                 for (int k = first; k < afterLastL; ++k) {
-                    double res = 0.0, rs = NaNinf;
+                    double res = 0.0, rs = NaNinf, nRes = 0.0, nRs = NaNinf;
                     if (live) {
                         size_t idx = (size_t)k * rays + r;
                         double sp = wepl[idx];
-                        double xi = sp * escale + 0.5;
-                        double cd_ = 0.0;
-                        {
-                            double xb = xi - 0.5;
-                            if (xb < -1.0) xb = -1.0;
-                            if (xb > nS) xb = nS;
-                            double fl = floor(xb), aa = texw(xb - fl);
-                            int i0 = (int)fl < 0 ? 0 : ((int)fl > nS - 1 ? nS - 1 : (int)fl);
-                            int i1 = (int)fl + 1 < 0 ? 0 : ((int)fl + 1 > nS - 1 ? nS - 1 : (int)fl + 1);
-                            cd_ = (1.0 - aa) * row[i0] + aa * row[i1];
-                        }
+                        double cd_ = row_lookup(row, nS, sp * escale + 0.5);
                         double rho = dens[idx];
                         if (sp < peak) {
                             double resE = 8.639415 * pow((double)peak - 0.5 * (sp + spOld), 0.5649718);
                             double betaP = resE + 938.3 - 938.3 * 938.3 / (resE + 938.3);
                             double rRl = rho * lut1(e->rrl_vector, e->n_rrl_samples, rho * e->rrl_scale_fact + 0.5);
-                            double th2 = 198.81 / (betaP * betaP) * stepLen * rRl;
+                            double th2 = rEref / (betaP * betaP) * stepLen * rRl;
                             sig2 += incScat + incDiv;
                             incinc += 2.0 * th2 * stepLen * stepLen;
                             incScat += incinc;
                             incDiv += 2.0 * quad;
-                        } else {
+                        } else if (!rSuppress) {
                             sig2 -= 1.5 * (incScat + incDiv) * rho;
                         }
                         double zk = (double)P->p.fan_corner[2] + (double)k * P->p.fan_delta[2];
                         double vwx = P->p.fan_delta[0] * (1.0 - zk / P->p.source_dist[0]);
                         double vwy = P->p.fan_delta[1] * (1.0 - zk / P->p.source_dist[1]);
-                        rs = 0.5 * (vwx + vwy) / (sqrt(2.0) * (sqrt(sig2) + 0.21));
+                        rs = 0.5 * (vwx + vwy) / (sqrt(2.0) * (sqrt(sig2) + rDelta));
                         double kk = (double)k;
                         double vol = (double)P->volConst + kk * P->volLin + kk * kk * P->volSq;
                         double mass = rho * vol;
-                        if (mass > 1e-2) res = w * (cd_ - cdOld) / mass;
+                        double depthMid = 0.5 * (sp + spOld) * escale + 0.5;
+                        if (mass > 1e-2) {
+                            if (nucOn) {
+                                double nw = row_lookup(nwRow, nS, depthMid);
+                                res = (1.0 - nw) * w * (cd_ - cdOld) / mass;
+                                if (nIdx >= 0) nRes = nw * nW * (cd_ - cdOld) / (mass * (double)spotDist * spotDist);
+                            } else {
+                                res = w * (cd_ - cdOld) / mass;
+                            }
+                        }
+                        if (nucOn && nIdx >= 0) {
+                            double ns2 = row_lookup(nsRow, nS, depthMid);
+                            nRs = 0.5 * spotDist * (vwx + vwy) / (sqrt(2.0) * sqrt(sig2 + ns2 + (double)entrySigmaSq));
+                        }
                         spOld = sp;
                         cdOld = cd_;
                         if (sp > (double)rangeStop || (unsigned)k == afterLast) { live = 0; afterLast = (unsigned)k; }
                     }
-                    if (!live || k < firstIn - 1) { res = 0.0; rs = NaNinf; }
+                    if (!live || k < firstIn - 1) { res = 0.0; rs = NaNinf; nRes = 0.0; nRs = NaNinf; }
                     idd[(size_t)k * pad + (size_t)y * PX + x] = res;
                     rsg[(size_t)k * pad + (size_t)y * PX + x] = rs;
+                    if (nIdx >= 0) {
+                        nIdd[(size_t)k * nucPad + nIdx] = nRes;
+                        nRsg[(size_t)k * nucPad + nIdx] = nRs;
+                    }
                 }
                 if ((int)afterLast > maxFP) maxFP = (int)afterLast;
             }
-        free(row);
         /* beamFirstCalculatedPassive (wrapper.cu:4975-4990). */
         int calc = maxFP;
         if (calc < first + 1) calc = first + 1;
@@ -1051,104 +1257,60 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
         /* Tile radius buckets (tileRadCalc, complete_superposition.cu:198-255). */
         memset(codes, 0xff, (size_t)S * tiles);
         int hist[34] = {0}, live = 0;
-        for (int k = first; k < afterLastL; ++k)
-            for (int ty = 0; ty < TY; ++ty)
-                for (int tx = 0; tx < TX; ++tx) {
-                    double mn = NaNinf;
-                    int anyLive = 0;
-                    for (int sy = 0; sy < TILE_Y; ++sy)
-                        for (int sx = 0; sx < TILE_X; ++sx) {
-                            size_t o = (size_t)k * pad + (size_t)(ty * TILE_Y + sy) * PX + tx * TILE_X + sx;
-                            if (rsg[o] < mn) mn = rsg[o];
-                            if (idd[o] > 0.0) anyLive = 1;
-                        }
-                    int R = oracle_radius_bucket((float)mn);
-                    codes[(size_t)k * tiles + ty * TX + tx] = (unsigned char)(R | (anyLive ? 0x80 : 0));
-                    if (k < calc) {
-                        hist[R]++;
-                        live += anyLive;
-                    }
+        for (int k = first; k < afterLastL; ++k) {
+            tile_codes(idd + (size_t)k * pad, rsg + (size_t)k * pad, PX, TX, TY, codes + (size_t)k * tiles);
+            if (k < calc)
+                for (size_t t = 0; t < tiles; ++t) {
+                    unsigned char c = codes[(size_t)k * tiles + t];
+                    hist[c & 0x3f]++;
+                    live += (c & 0x80) ? 1 : 0;
                 }
+        }
         int batched[33], map[34];
         oracle_batch(hist, batched, map);
-        /* Superposition (kernelSuperposition<R>, complete_superposition.cu:264-335) at the
-         * batched radius, one layer BEV at absolute step index. */
+        /* Superposition at the batched radius into the layer BEV at absolute steps. */
         memset(bevL, 0, sizeof(double) * S * bevPlane);
         double fmaL = 0.0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : fmaL)
-        for (int k = first; k < calc; ++k) {
-            double* plane = bevL + (size_t)k * bevPlane;
-            double ed[MAX_R + 1];
-            for (int t = 0; t < (int)tiles; ++t) {
-                unsigned char c = codes[(size_t)k * tiles + t];
-                if (!(c & 0x80)) continue;
-                int R = map[c & 0x3f];
-                fmaL += 256.0 * (2 * R + 1) * (2 * R + 1);
-                int tx = t % TX, ty = t / TX;
-                for (int sy = 0; sy < TILE_Y; ++sy)
-                    for (int sx = 0; sx < TILE_X; ++sx) {
-                        size_t o = (size_t)k * pad + (size_t)(ty * TILE_Y + sy) * PX + tx * TILE_X + sx;
-                        double dose_ = idd[o];
-                        if (!(dose_ > 0.0)) continue;
-                        double rs = rsg[o];
-                        double en = erfd(rs * 0.5), eo = -en;
-                        for (int i = 0; i <= R; ++i) {
-                            ed[i] = 0.5 * (en - eo);
-                            eo = en;
-                            en = erfd(rs * ((double)i + 1.5));
-                        }
-                        int oy0 = ty * TILE_Y + sy - R + MAX_R, ox0 = tx * TILE_X + sx - R + MAX_R;
-                        for (int i = 0; i < 2 * R + 1; ++i) {
-                            double wy = dose_ * ed[abs(R - i)];
-                            double* rowp = plane + (size_t)(oy0 + i) * BX + ox0;
-                            for (int j = 0; j < 2 * R + 1; ++j) rowp[j] += wy * ed[abs(R - j)];
-                        }
-                    }
-            }
-        }
+        for (int k = first; k < calc; ++k)
+            fmaL += superpose_step(idd + (size_t)k * pad, rsg + (size_t)k * pad, codes + (size_t)k * tiles, map, PX,
+                                   TX, TY, bevL + (size_t)k * bevPlane, BX);
         fmaTotal += fmaL;
         if (bevSum)
             for (size_t i = 0; i < (size_t)S * bevPlane; ++i) bevSum[i] += bevL[i];
-        /* Per-layer transfer (wrapper.cu:5343-5505, prim_transf_kernel.cu:11-44). */
-        int box[6] = {0, 0, 0, -1, -1, -1};
-        {
-            const float xs[2] = {-(float)MAX_R, (float)(PX + MAX_R - 1)};
-            const float ys[2] = {-(float)MAX_R, (float)(PY + MAX_R - 1)};
-            const float zs[2] = {(float)first, (float)(calc - 1)};
-            V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
-            for (int zi = 0; zi < 2; ++zi)
-                for (int yi = 0; yi < 2; ++yi)
-                    for (int xi = 0; xi < 2; ++xi) {
-                        V3 p = ffapply(P->fanToDose, v3(xs[xi], ys[yi], zs[zi]));
-                        mx.x = fmaxf(mx.x, p.x); mx.y = fmaxf(mx.y, p.y); mx.z = fmaxf(mx.z, p.z);
-                        mn.x = fminf(mn.x, p.x); mn.y = fminf(mn.y, p.y); mn.z = fminf(mn.z, p.z);
-                    }
-            int sx0 = ((int)floorf(mn.x) / 32) * 32;
-            box[0] = sx0 > 0 ? sx0 : 0;
-            box[1] = (int)floorf(mn.y) > 0 ? (int)floorf(mn.y) : 0;
-            box[2] = (int)floorf(mn.z) > 0 ? (int)floorf(mn.z) : 0;
-            box[3] = (int)ceilf(mx.x) < dd[0] - 1 ? (int)ceilf(mx.x) : dd[0] - 1;
-            box[4] = (int)ceilf(mx.y) < dd[1] - 1 ? (int)ceilf(mx.y) : dd[1] - 1;
-            box[5] = (int)ceilf(mx.z) < dd[2] - 1 ? (int)ceilf(mx.z) : dd[2] - 1;
-        }
-        if (box[0] <= box[3] && box[1] <= box[4] && box[2] <= box[5]) {
-            ToFan tf = ff_invert_shift(P->fanToDose, v3((float)MAX_R, (float)MAX_R, -(float)first));
-            TransferP T = transfer_params(tf);
-            int spanX = ((box[3] - box[0] + 1 + 31) / 32) * 32, spanY = ((box[4] - box[1] + 1 + 7) / 8) * 8;
-            int xEnd = box[0] + spanX < dd[0] ? box[0] + spanX : dd[0];
-            int yEnd = box[1] + spanY < dd[1] ? box[1] + spanY : dd[1];
-            /* The reference's BEV texture spans planes [0, guaranteedPassive). */
-            const int nz = passive;
-            const double zshift = compat ? 0.0 : (double)first;
-#pragma omp parallel for schedule(dynamic, 4)
-            for (int y = box[1]; y < yEnd; ++y)
-                for (int x = box[0]; x < xEnd; ++x)
-                    for (int z = box[2]; z <= box[5]; ++z) {
-                        V3 f = tp_fan(&T, x, y, z);
-                        if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
-                        double v = tri_border_d(bevL, BX, BY, nz, f.x, f.y, (double)f.z + zshift);
-                        if (v > 0.0) dose[((size_t)z * dd[1] + y) * dd[0] + x] += v;
-                    }
+        int box[6];
+        transfer_layer(&P->fanToDose, PX, PY, first, calc, passive, compat, bevL, BX, BY, dose, dd, box);
+        /* Nuclear halo: tile radii over [first, calc) with no overflow merge
+         * (complete_superposition.cu:558-708), superposition on the halo grid and
+         * its own transfer (wrapper.cu:5510-5600, prim_transf_kernel.cu:46-78). */
+        int nHist[34] = {0}, nBatched[33] = {0}, nMap[34];
+        if (nucOn) {
+            memset(nCodes, 0xff, (size_t)S * nucTiles);
+            for (int k = first; k < calc; ++k) {
+                tile_codes(nIdd + (size_t)k * nucPad, nRsg + (size_t)k * nucPad, NXn, NTX, NTY,
+                           nCodes + (size_t)k * nucTiles);
+                for (size_t t = 0; t < nucTiles; ++t) nHist[nCodes[(size_t)k * nucTiles + t] & 0x3f]++;
+            }
+            if (nHist[MAX_R + 1] > 0) {
+                rc = fail(PBS_ERR_UNSUPPORTED, "nuclear superposition radius exceeds 32 (the reference throws, "
+                                               "complete_superposition.cu:609-627)");
+            } else {
+                oracle_batch(nHist, nBatched, nMap);
+                memset(nBevL, 0, sizeof(double) * S * nucBevPlane);
+                double nf = 0.0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : nf)
+                for (int k = first; k < calc; ++k)
+                    nf += superpose_step(nIdd + (size_t)k * nucPad, nRsg + (size_t)k * nucPad,
+                                         nCodes + (size_t)k * nucTiles, nMap, NXn, NTX, NTY,
+                                         nBevL + (size_t)k * nucBevPlane, NBX);
+                nucFmaTotal += nf;
+                if (nBevSum)
+                    for (size_t i = 0; i < (size_t)S * nucBevPlane; ++i) nBevSum[i] += nBevL[i];
+                FromFan nf2d = P->fanToDose;
+                nf2d.fan = idxt(v3(P->lat.dx, P->lat.dy, P->p.fan_delta[2]), v3(P->lat.ox, P->lat.oy, P->p.fan_corner[2]));
+                int nbox[6];
+                transfer_layer(&nf2d, NXn, NYn, first, calc, passive, compat, nBevL, NBX, NBY, dose, dd, nbox);
+            }
         }
         if (cap) {
             if (cap->idd) memcpy(cap->idd + (size_t)l * S * pad, idd, sizeof(double) * S * pad);
@@ -1161,8 +1323,16 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
             if (cap->layer_box) memcpy(cap->layer_box + 6 * l, box, sizeof box);
             if (cap->hist) memcpy(cap->hist + 34 * l, hist, sizeof hist);
             if (cap->batched) memcpy(cap->batched + 33 * l, batched, sizeof batched);
+            if (nucOn) {
+                if (cap->nuc_idd) memcpy(cap->nuc_idd + (size_t)l * S * nucPad, nIdd, sizeof(double) * S * nucPad);
+                if (cap->nuc_rsigma) memcpy(cap->nuc_rsigma + (size_t)l * S * nucPad, nRsg, sizeof(double) * S * nucPad);
+                if (cap->nuc_codes) memcpy(cap->nuc_codes + (size_t)l * S * nucTiles, nCodes, (size_t)S * nucTiles);
+                if (cap->nuc_hist) memcpy(cap->nuc_hist + 34 * l, nHist, sizeof nHist);
+                if (cap->nuc_batched) memcpy(cap->nuc_batched + 33 * l, nBatched, sizeof nBatched);
+            }
         }
     }
+    free(row); free(nwRow); free(nsRow);
     if (cap) {
         if (cap->density) memcpy(cap->density, dens, sizeof(double) * S * rays);
         if (cap->wepl) memcpy(cap->wepl, wepl, sizeof(double) * S * rays);
@@ -1178,16 +1348,37 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
             cap->beam_ints[3] = maxCalc;
         }
         cap->superpose_fma = fmaTotal;
+        cap->nuc_superpose_fma = nucFmaTotal;
+        if (cap->ray_to_nuc && rayToNuc) memcpy(cap->ray_to_nuc, rayToNuc, sizeof(int) * rays);
     }
     free(dens); free(wepl); free(fin); free(fout); free(wmin); free(rayW); free(eSig);
     free(idd); free(rsg); free(codes); free(bevL);
-    return PBS_OK;
+    free(nIdd); free(nRsg); free(nCodes); free(nBevL); free(rayToNuc);
+    return rc;
 }
 
 int oracle_dose(const float* ct, const int cd[3], const float cr[3], const float cc[3], double* dose,
                 const int dd[3], const float dr[3], const float dc[3], const PbsBeamDesc* beams, size_t nb,
                 const PbsEnergyDesc* e, int ct_type, int compat, int threads, OracleCapture* cap) {
+    return oracle_dose_nuclear(ct, cd, cr, cc, dose, dd, dr, dc, beams, nb, e, ct_type, compat, -1, threads, cap);
+}
+
+int oracle_dose_nuclear(const float* ct, const int cd[3], const float cr[3], const float cc[3], double* dose,
+                        const int dd[3], const float dr[3], const float dc[3], const PbsBeamDesc* beams, size_t nb,
+                        const PbsEnergyDesc* e, int ct_type, int compat, int nucModel, int threads,
+                        OracleCapture* cap) {
     if (!ct || !dose || !beams || !e || nb == 0) return fail(PBS_ERR_INVALID_ARGUMENT, "null input");
+    if (nucModel > 2) return fail(PBS_ERR_INVALID_ARGUMENT, "unknown nuclear model");
+    if (nucModel >= 0) { /* enforceNuclearCorrectionContract (wrapper.cu:1077-1097) */
+        const size_t n = (size_t)e->n_energies * e->n_energy_samples;
+        if (!e->nuc_weight_matrix || !e->nuc_sq_sigma_matrix || e->n_nuc_weight_matrix != n ||
+            e->n_nuc_sq_sigma_matrix != n)
+            return fail(PBS_ERR_INVALID_ARGUMENT, "nuclear_correction=true requested, but the energy tables do not "
+                                                  "carry nuclear_weight/sigma tables");
+        if (!e->nuclear_tables_aligned_to_primary_axis)
+            return fail(PBS_ERR_INVALID_ARGUMENT, "nuclear_correction=true requested, but nuclear LUTs are not "
+                                                  "aligned to the active primary energy-depth axis");
+    }
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -1210,7 +1401,7 @@ int oracle_dose(const float* ct, const int cd[3], const float cr[3], const float
     for (size_t bi = 0; bi < nb && !rc; ++bi) {
         Plan P;
         rc = plan_beam(&beams[bi], e, cd, cr, cc, dd, dr, dc, &P);
-        if (!rc) rc = run_beam(hu, cd, dose, dd, &beams[bi], e, &P, compat, bi + 1 == nb ? cap : NULL);
+        if (!rc) rc = run_beam(hu, cd, dose, dd, &beams[bi], e, &P, compat, nucModel, bi + 1 == nb ? cap : NULL);
         free_plan(&P);
     }
     free(hu);

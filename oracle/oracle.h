@@ -5,7 +5,8 @@
  * (src/core/raytracedicom_wrapper.cu:2446-5661): CT adapter, beam geometry and
  * ray grid, BEV ray tracing, beam reductions, spot->ray convolution (both fluence
  * modes), IDD/sigma, tile radius binning and batching, tile superposition and the
- * per-layer divergent transfer. Geometry and every integer decision use IEEE
+ * per-layer divergent transfer, and the nuclear halo branch (halo lattice IDD,
+ * its own tile superposition and transfer). Geometry and every integer decision use IEEE
  * single precision in the reference's operand order (so ray grids, step counts,
  * cut-off steps, radius buckets and transfer boxes are reproduced exactly); all
  * dose arithmetic (sampling, cumulative sums, erf weights, superposition,
@@ -39,6 +40,8 @@ typedef struct OraclePlan {
     float source_dist[2];
     float len_to_mm, energy_depth_to_mm, max_peak_depth_mm;
     int bev_x, bev_y;
+    int nuc_x, nuc_y;        /* halo lattice padded to 32 x 8 (0 without a spot lattice) */
+    int nuc_bev_x, nuc_bev_y;
 } OraclePlan;
 
 /* Optional captures of the last beam; every pointer may be NULL. Sizes use the
@@ -62,6 +65,15 @@ typedef struct OracleCapture {
     int* batched;           /* [L][33]                                     */
     double* bev;            /* [S][bev_y][bev_x] layer-summed, absolute step */
     double superpose_fma;   /* out: sum over live tiles of 256*(2R+1)^2     */
+    /* Nuclear halo (nuclear_model >= 0), on the halo lattice nuc = nuc_x*nuc_y. */
+    double* nuc_idd;        /* [L][S][nuc]                                 */
+    double* nuc_rsigma;     /* [L][S][nuc] (+inf outside)                  */
+    unsigned char* nuc_codes; /* [L][S][nuc tiles]                         */
+    int* nuc_hist;          /* [L][34]                                     */
+    int* nuc_batched;       /* [L][33]                                     */
+    double* nuc_bev;        /* [S][nuc_bev_y][nuc_bev_x] layer-summed       */
+    int* ray_to_nuc;        /* [rays] halo lattice cell of each ray or -1  */
+    double nuc_superpose_fma;
 } OracleCapture;
 
 /* Host plan of one beam (no dose work). `layer_params` ([L][8], may be NULL)
@@ -82,6 +94,13 @@ int oracle_dose(const float* ct, const int ct_dims[3], const float ct_res[3], co
                 double* dose, const int dose_dims[3], const float dose_res[3], const float dose_corner[3],
                 const PbsBeamDesc* beams, size_t num_beams, const PbsEnergyDesc* energy, int ct_type,
                 int compat_bev_z_shift, int threads, OracleCapture* capture);
+
+/* The same with the nuclear halo branch: nuclear_model -1 (off), 0 SOUKUP,
+ * 1 FLUKA, 2 GAUSS_FIT (the reference's NUCLEAR_CORR build values). */
+int oracle_dose_nuclear(const float* ct, const int ct_dims[3], const float ct_res[3], const float ct_corner[3],
+                        double* dose, const int dose_dims[3], const float dose_res[3], const float dose_corner[3],
+                        const PbsBeamDesc* beams, size_t num_beams, const PbsEnergyDesc* energy, int ct_type,
+                        int compat_bev_z_shift, int nuclear_model, int threads, OracleCapture* capture);
 
 /* Tile radius bucket from a tile's minimum rSigmaEff (complete_superposition.cu:242). */
 int oracle_radius_bucket(float min_rsigma);

@@ -33,6 +33,7 @@ class OraclePlan(C.Structure):
         ("source_dist", C.c_float * 2),
         ("len_to_mm", C.c_float), ("energy_depth_to_mm", C.c_float), ("max_peak_depth_mm", C.c_float),
         ("bev_x", C.c_int), ("bev_y", C.c_int),
+        ("nuc_x", C.c_int), ("nuc_y", C.c_int), ("nuc_bev_x", C.c_int), ("nuc_bev_y", C.c_int),
     ]
 
 
@@ -42,6 +43,8 @@ class OracleCapture(C.Structure):
         ("beam_ints", _IP), ("ray_weights", _DP), ("entry_sigma", _FP), ("idd", _DP), ("rsigma", _DP),
         ("codes", _UP), ("layer_ints", _IP), ("layer_box", _IP), ("hist", _IP), ("batched", _IP),
         ("bev", _DP), ("superpose_fma", C.c_double),
+        ("nuc_idd", _DP), ("nuc_rsigma", _DP), ("nuc_codes", _UP), ("nuc_hist", _IP), ("nuc_batched", _IP),
+        ("nuc_bev", _DP), ("ray_to_nuc", _IP), ("nuc_superpose_fma", C.c_double),
     ]
 
 
@@ -63,6 +66,10 @@ def load() -> C.CDLL:
     lib.oracle_dose.restype = C.c_int
     lib.oracle_dose.argtypes = [_FP, _IP, _FP, _FP, _DP, _IP, _FP, _FP, C.POINTER(P.PbsBeamDesc), C.c_size_t,
                                 C.POINTER(P.PbsEnergyDesc), C.c_int, C.c_int, C.c_int, C.POINTER(OracleCapture)]
+    lib.oracle_dose_nuclear.restype = C.c_int
+    lib.oracle_dose_nuclear.argtypes = [_FP, _IP, _FP, _FP, _DP, _IP, _FP, _FP, C.POINTER(P.PbsBeamDesc),
+                                        C.c_size_t, C.POINTER(P.PbsEnergyDesc), C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(OracleCapture)]
     lib.oracle_radius_bucket.restype = C.c_int
     lib.oracle_radius_bucket.argtypes = [C.c_float]
     lib.oracle_batch.restype = None
@@ -106,8 +113,10 @@ def plan(case: dict, beam: dict | None = None, with_lattice: bool = False) -> di
 
 
 def dose(case: dict, beams: list | None = None, initial=None, ct_type: int = 0, compat_bev_z_shift: bool = False,
-         threads: int = 0, capture: bool = False, capture_layers: bool = False) -> dict:
-    """Run the oracle; returns {'dose': float64 [Z][Y][X], 'capture': {...}}."""
+         threads: int = 0, capture: bool = False, capture_layers: bool = False, nuclear_model: int = -1) -> dict:
+    """Run the oracle; returns {'dose': float64 [Z][Y][X], 'capture': {...}}.
+    `nuclear_model` -1 runs without the nuclear halo; 0/1/2 select SOUKUP, FLUKA
+    and GAUSS_FIT (the energy dict then carries the nuclear tables)."""
     from subsecondpbs_b200 import _lib as P
     from subsecondpbs_b200.cudaCalDoseRTD import _with_luts
 
@@ -148,19 +157,30 @@ def dose(case: dict, beams: list | None = None, initial=None, ct_type: int = 0, 
             bufs["idd"] = np.zeros((L, S, pl["pitch_y"], pl["pitch_x"]))
             bufs["rsigma"] = np.zeros((L, S, pl["pitch_y"], pl["pitch_x"]))
             bufs["codes"] = np.zeros((L, S, pl["tiles_y"], pl["tiles_x"]), np.uint8)
+        if nuclear_model >= 0 and pl["nuc_x"] > 0:
+            ny, nx = pl["nuc_y"], pl["nuc_x"]
+            bufs["nuc_hist"] = np.zeros((L, 34), np.int32)
+            bufs["nuc_batched"] = np.zeros((L, 33), np.int32)
+            bufs["nuc_bev"] = np.zeros((S, pl["nuc_bev_y"], pl["nuc_bev_x"]))
+            bufs["ray_to_nuc"] = np.zeros((pl["ray_y"], pl["ray_x"]), np.int32)
+            if capture_layers:
+                bufs["nuc_idd"] = np.zeros((L, S, ny, nx))
+                bufs["nuc_rsigma"] = np.zeros((L, S, ny, nx))
+                bufs["nuc_codes"] = np.zeros((L, S, ny // 8, nx // 32), np.uint8)
         cap = OracleCapture()
         types = {n: t for n, t in OracleCapture._fields_}
         for name, a in bufs.items():
             setattr(cap, name, a.ctypes.data_as(types[name]))
         bufs["plan"] = pl
-    rc = lib.oracle_dose(ct.ctypes.data_as(_FP), P.int3(case["ct_dims"]), P.float3(case["ct_resolution"]),
-                         P.float3(case["ct_corner"]), dose_arr.ctypes.data_as(_DP), P.int3(dd),
-                         P.float3(case["dose_resolution"]), P.float3(case["dose_corner"]), arr, len(descs),
-                         C.byref(ed), int(ct_type), int(bool(compat_bev_z_shift)), int(threads),
-                         C.byref(cap) if cap is not None else None)
+    rc = lib.oracle_dose_nuclear(ct.ctypes.data_as(_FP), P.int3(case["ct_dims"]), P.float3(case["ct_resolution"]),
+                                 P.float3(case["ct_corner"]), dose_arr.ctypes.data_as(_DP), P.int3(dd),
+                                 P.float3(case["dose_resolution"]), P.float3(case["dose_corner"]), arr, len(descs),
+                                 C.byref(ed), int(ct_type), int(bool(compat_bev_z_shift)), int(nuclear_model),
+                                 int(threads), C.byref(cap) if cap is not None else None)
     _err(rc)
     if cap is not None:
         bufs["superpose_fma"] = cap.superpose_fma
+        bufs["nuc_superpose_fma"] = cap.nuc_superpose_fma
     del keep, ke
     return {"dose": dose_arr, "capture": bufs}
 

@@ -19,6 +19,15 @@ __device__ __forceinline__ float lut_linear_clamp(const float* __restrict__ t, i
     return v0 + (v1 - v0) * a;
 }
 
+// Unsigned key with the order of the float values (negative floats reversed).
+__device__ __forceinline__ unsigned float_order_key(float v) {
+    const unsigned b = __float_as_uint(v);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float float_from_order_key(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
 // Same lookup on a table staged in shared memory.
 __device__ __forceinline__ float lut_linear_clamp_smem(const float* t, int n, float x) {
     float xb = x - 0.5f;

@@ -35,7 +35,10 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
            uint8_t* __restrict__ codes, int* __restrict__ firstPassiveOut) {
     extern __shared__ float smem[];
     float* ciddRow = smem;                                    // [nS]
-    float* partMin = smem + luts.nS;                          // [steps][8]
+    float* rrlTab = ciddRow + luts.nS;                        // [nRrl]
+    float* stepNum = rrlTab + luts.nRrl;                      // [steps] 0.5 (voxel width x + y)
+    float* stepVolT = stepNum + g.steps;                      // [steps] step volume
+    float* partMin = stepVolT + g.steps;                      // [steps][8]
     int* partLive = reinterpret_cast<int*>(partMin + g.steps * 8);  // [steps][8]
     __shared__ int shHist[kBuckets], shLive[kBuckets], shPassive[8];
 
@@ -63,6 +66,17 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         for (int d = tid; d < luts.nS; d += 256) {
             const float a0 = __ldg(r0 + d), a1 = __ldg(r1 + d);
             ciddRow[d] = a0 + (a1 - a0) * b;
+        }
+        for (int d = tid; d < luts.nRrl; d += 256) rrlTab[d] = __ldg(luts.rrl + d);
+        // Per-step voxel widths and volumes are the same for every ray of the step
+        // (fill_idd_and_sigma_params.cuh:56-80).
+        for (int k = tid; k < g.steps; k += 256) {
+            const float zk = g.fanCorner.z + float(k) * g.fanDelta.z;
+            const float vwx = g.fanDelta.x * (1.0f - zk / g.sourceDist.x);
+            const float vwy = g.fanDelta.y * (1.0f - zk / g.sourceDist.y);
+            stepNum[k] = 0.5f * (vwx + vwy);
+            const unsigned int ku = static_cast<unsigned int>(k);
+            stepVolT[k] = g.volConst + float(ku) * g.volLin + float(ku * ku) * g.volSq;
         }
         if (tid < kBuckets) {
             shHist[tid] = 0;
@@ -101,18 +115,29 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     float incDiv = p.sigmaSqAirLin + (2.0f * float(first) - 1.0f) * quad;
     float sigmaSq = -incDiv;
 
+    // The next step's WEPL and density are loaded one step ahead.
+    float nextSp = 0.0f, nextDens = 0.0f;
+    if (live && first < afterLastL) {
+        const size_t idx = static_cast<size_t>(first) * rayPlane + ridx;
+        nextSp = wepl[idx];
+        nextDens = density[idx];
+    }
     for (int stepNo = first; stepNo < afterLastL; ++stepNo) {
         float res = 0.0f;
         float rSigmaEff = __int_as_float(0x7f800000);
         if (live) {
-            const size_t idx = static_cast<size_t>(stepNo) * rayPlane + ridx;
-            const float cumulSp = wepl[idx];
+            const float cumulSp = nextSp;
+            const float dens = nextDens;
+            if (stepNo + 1 < afterLastL) {
+                const size_t idx = static_cast<size_t>(stepNo + 1) * rayPlane + ridx;
+                nextSp = wepl[idx];
+                nextDens = density[idx];
+            }
             const float cumulDose = lut_linear_clamp_smem(ciddRow, luts.nS, cumulSp * p.energyScaleFact + 0.5f);
-            const float dens = density[idx];
             if (cumulSp < p.peakDepth) {
-                const float resE = kECoef * powf(p.peakDepth - 0.5f * (cumulSp + cumulSpOld), kPInv);
+                const float resE = kECoef * __powf(p.peakDepth - 0.5f * (cumulSp + cumulSpOld), kPInv);
                 const float betaP = resE + 938.3f - 938.3f * 938.3f / (resE + 938.3f);
-                const float rRl = dens * lut_linear_clamp(luts.rrl, luts.nRrl, dens * luts.rrlScale + 0.5f);
+                const float rRl = dens * lut_linear_clamp_smem(rrlTab, luts.nRrl, dens * luts.rrlScale + 0.5f);
                 const float thetaSq = kERefSq / (betaP * betaP) * stepLength * rRl;
                 sigmaSq += incScat + incDiv;
                 incincScat += 2.0f * thetaSq * stepLength * stepLength;
@@ -121,13 +146,8 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             } else {
                 sigmaSq -= 1.5f * (incScat + incDiv) * dens;
             }
-            const float zk = g.fanCorner.z + float(stepNo) * g.fanDelta.z;
-            const float vwx = g.fanDelta.x * (1.0f - zk / g.sourceDist.x);
-            const float vwy = g.fanDelta.y * (1.0f - zk / g.sourceDist.y);
-            rSigmaEff = 0.5f * (vwx + vwy) / (kSqrt2 * (sqrtf(sigmaSq) + kSigmaDelta));
-            const unsigned int k = static_cast<unsigned int>(stepNo);
-            const float stepVol = g.volConst + float(k) * g.volLin + float(k * k) * g.volSq;
-            const float mass = dens * stepVol;
+            rSigmaEff = stepNum[stepNo] / (kSqrt2 * (sqrtf(sigmaSq) + kSigmaDelta));
+            const float mass = dens * stepVolT[stepNo];
             if (mass > 1e-2f) res = rayWeight * (cumulDose - cumulDoseOld) / mass;
             cumulSpOld = cumulSp;
             cumulDoseOld = cumulDose;
@@ -145,11 +165,12 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         iddL[o] = res;
         rsL[o] = rSigmaEff;
 
-        float m = rSigmaEff;
-        for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, off));
+        // Warp minimum on order-preserving unsigned keys of the floats; the device's
+        // canonical NaN maps above +inf and drops out, as it does under fminf.
+        const unsigned mk = __reduce_min_sync(0xffffffffu, float_order_key(rSigmaEff));
         const int anyLive = __any_sync(0xffffffffu, res > 0.0f);
         if (lane == 0) {
-            partMin[zr * 8 + warp] = m;
+            partMin[zr * 8 + warp] = float_from_order_key(mk);
             partLive[zr * 8 + warp] = anyLive;
         }
     }
@@ -302,7 +323,8 @@ __global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, cons
 }  // namespace
 
 size_t idd_smem_bytes(const BeamGeomDev& g, const LutsDev& luts) {
-    return static_cast<size_t>(luts.nS) * sizeof(float) + static_cast<size_t>(g.steps) * 8 * (sizeof(float) + sizeof(int));
+    return (static_cast<size_t>(luts.nS) + luts.nRrl + 2 * static_cast<size_t>(g.steps)) * sizeof(float) +
+           static_cast<size_t>(g.steps) * 8 * (sizeof(float) + sizeof(int));
 }
 
 cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, int nLayers, const float* density,

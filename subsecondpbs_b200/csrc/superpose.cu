@@ -9,7 +9,7 @@
 // Formulation on the FP32 FMA pipe (one CTA per tile, persistent grid):
 //   * table phase: each thread builds its source's rows e_s(0..R) (float4 chunks,
 //     chunk-major so that the stores and the broadcast reads are conflict-free)
-//     and idd_s * e_s(0..R) (odd row stride);
+//     and idd_s * e_s(0..R) (odd row stride); sources without dose get zero rows;
 //   * accumulation phase: a warp lane is one column offset d in [-R, R] of one
 //     source column; a source column's eight sources share the lane's output
 //     column, so the lane keeps the whole footprint height (8+2R rows) in
@@ -40,10 +40,11 @@ struct Shape {
         (size_t(kQ) * kThreads * 4 + size_t(kThreads) * kEWStride + kOutFloats) * sizeof(float);
 };
 
-// Slot of source s in the chunk-major e_s table: the low three bits are XORed with
-// bits 3..5 so that source columns 8, 16 or 32 apart (read together by the lane
-// groups of one instruction) land in different banks.
-__device__ __forceinline__ int e4_slot(int s) { return s ^ ((s >> 3) & 7); }
+// Column part of the slot of source (sy, sx) in the chunk-major e_s table
+// (slot = sy * 32 + e4_col(sx)): the low bits are XORed with bits 3..4 so that
+// source columns 4, 8 or 16 apart (read together by the lane groups of one
+// instruction) land in different banks.
+__device__ __forceinline__ int e4_col(int sx) { return sx ^ ((sx >> 3) & 3); }
 
 struct TileArgs {
     const float* idd;
@@ -68,6 +69,8 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
     const int warp = t >> 5, lane = t & 31;
 
     // ---- table phase (complete_superposition.cu:298-307) --------------------
+    // Sources without dose get zero rows, so the accumulation needs no per-source
+    // test; sColMask[sx] collects the depositing sources of every source column.
     {
         const float dose = a.idd[a.src];
         const bool live = dose > 0.0f;
@@ -88,11 +91,14 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
             for (int k = 0; k <= R; ++k) EW[t * EWS + k] = dose * e[k];
         } else {
 #pragma unroll
-            for (int k = 0; k <= R; ++k) e[k] = 0.0f;
+            for (int k = 0; k <= R; ++k) {
+                e[k] = 0.0f;
+                EW[t * EWS + k] = 0.0f;
+            }
         }
 #pragma unroll
         for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
-        const int pt = e4_slot(t);
+        const int pt = warp * kTileX + e4_col(lane);
 #pragma unroll
         for (int q = 0; q < Q; ++q) E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
         for (int i = t; i < H * Wo; i += kThreads) out[i] = 0.0f;
@@ -106,9 +112,10 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing (>= W: disjoint)
         constexpr int CH = kGrouped ? 1 : (W + 31) / 32;           // 32-lane chunks of one column
         constexpr int kUnits = kGrouped ? S : 32 * CH;
-        unsigned lm[kTileY];
+        // Depositing sources of source column `lane`, as an 8-bit mask over sy.
+        unsigned colBits = 0;
 #pragma unroll
-        for (int sy = 0; sy < kTileY; ++sy) lm[sy] = sMask[sy];
+        for (int sy = 0; sy < kTileY; ++sy) colBits |= ((sMask[sy] >> lane) & 1u) << sy;
 #pragma unroll 1
         for (int u = warp; u < kUnits; u += kWarps) {
             int sx, d;
@@ -128,22 +135,21 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                 d = 0;
             }
             const int ad = d < 0 ? -d : d;
-            unsigned colLive = 0;
-#pragma unroll
-            for (int sy = 0; sy < kTileY; ++sy) colLive |= ((lm[sy] >> sx) & 1u) << sy;
-            if (!valid) colLive = 0;
+            const unsigned colAll = __shfl_sync(0xffffffffu, colBits, sx);
+            const unsigned colLive = valid ? colAll : 0u;
             if (!__any_sync(0xffffffffu, colLive != 0)) continue;
+            // Lanes outside the footprint read source column 0 and are never flushed.
+            const float* ewCol = EW + sx * EWS + ad;
+            const float4* eCol = E4 + e4_col(sx);
             float acc[H];
 #pragma unroll
             for (int i = 0; i < H; ++i) acc[i] = 0.0f;
 #pragma unroll
             for (int sy = 0; sy < kTileY; ++sy) {
-                const int s = sy * kTileX + sx;
-                const float w = ((colLive >> sy) & 1u) ? EW[s * EWS + ad] : 0.0f;
-                const int ps = e4_slot(s);
+                const float w = ewCol[sy * kTileX * EWS];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
-                    const float4 v = E4[q * kThreads + ps];
+                    const float4 v = eCol[q * kThreads + sy * kTileX];
                     const float ev[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
@@ -154,6 +160,9 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                         }
                     }
                 }
+                // Keeps the next source's loads from being hoisted over this one's
+                // FMAs (which would hold every row of the column in registers).
+                asm volatile("" ::: "memory");
             }
             if (colLive) {
                 float* col = out + sx + R + d;
@@ -192,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
                  const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev, int small) {
     extern __shared__ __align__(16) float sm[];
-    float4* E4 = reinterpret_cast<float4*>(sm);                                  // [Q][256] e_s(4q..4q+3), slot e4_slot(s)
+    float4* E4 = reinterpret_cast<float4*>(sm);                                  // [Q][256] e_s(4q..4q+3), slot sy*32+e4_col(sx)
     float* EW = sm + Shape<RHi>::kQ * kThreads * 4;                              // [256][EWS] idd_s e_s(k)
     float* out = EW + kThreads * Shape<RHi>::kEWStride;                          // [8+2R][32+2R] footprint
     __shared__ int sItem[2];

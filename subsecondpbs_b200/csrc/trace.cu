@@ -15,6 +15,7 @@ namespace {
 constexpr float kInf20 = 1.0e20f;  // the reference's INF stored in a float (Macro.cuh:7)
 constexpr int kTraceSegments = 8;  // warps per tracing CTA; each marches one depth segment
 constexpr int kNone = 0x7fffffff;
+constexpr size_t kTraceCacheMaxBytes = 160 * 1024;  // CT samples kept on chip up to ~1280 steps
 
 // Trilinear sample of a [Z][Y][X] volume, texel centres at i + 0.5, zero outside
 // (sample3DLinearBorder, src/core/bev_ray_tracing.cu:16-61).
@@ -60,10 +61,16 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
 // atomic per warp and step on the bit patterns of the non-negative WEPL values. In
 // this path every ray has firstStepOutside >= 1 (lastInside starts at 0,
 // bev_ray_tracing.cu:157), so the reference's never-entered filter keeps every ray.
+//
+// With kCache the first pass keeps every CT sample of the segment in shared memory
+// ([segment step][lane], 128 B per step and warp) and the second pass reads them
+// back instead of sampling the CT again.
+template <bool kCache>
 __global__ void __launch_bounds__(32 * kTraceSegments)
 trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX, int ctY, int ctZ,
              float* __restrict__ density, float* __restrict__ wepl, int* __restrict__ firstInside,
              int* __restrict__ firstOutside, unsigned* __restrict__ weplMinBits, BeamStateDev* __restrict__ beam) {
+    extern __shared__ float shCache[];  // [kTraceSegments][seg][32] with kCache
     const int lane = threadIdx.x, w = threadIdx.y;
     const int x = blockIdx.x * 32 + lane;
     const int y = blockIdx.y;
@@ -90,10 +97,12 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
 
     // Pass 1: segment sums of HU+1000 and of WEPL increments.
     float huSum = 0.f, spSum = 0.f, spComp = 0.f;
+    float* myCache = shCache + static_cast<size_t>(w) * seg * 32 + lane;
     if (active) {
         V3 pos = pos0;
         for (int k = s0; k < s1; ++k) {
             const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+            if (kCache) myCache[(k - s0) * 32] = hu;
             huSum += hu;
             const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
             kahan_add(spSum, spComp, stepLen * sp);
@@ -124,7 +133,8 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
         for (int k = s0; k < s1; ++k) {
             unsigned bits = 0xffffffffu;
             if (active) {
-                const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+                const float hu =
+                    kCache ? myCache[(k - s0) * 32] : ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
                 cumHu += hu;
                 density[idx] = lut_linear_clamp(luts.density, luts.nDensity, hu * luts.densityScale + 0.5f);
                 const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
@@ -333,8 +343,18 @@ cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float*
     if (e != cudaSuccess) return e;
     dim3 block(32, kTraceSegments);
     dim3 grid((g.rayX + 31) / 32, g.rayY);
-    trace_kernel<<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside, firstOutside,
-                                        reinterpret_cast<unsigned*>(weplMin), beam);
+    const int seg = (g.steps + kTraceSegments - 1) / kTraceSegments;
+    const size_t cache = static_cast<size_t>(kTraceSegments) * seg * 32 * sizeof(float);
+    unsigned* mins = reinterpret_cast<unsigned*>(weplMin);
+    if (cache <= kTraceCacheMaxBytes) {
+        e = cudaFuncSetAttribute(trace_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(cache));
+        if (e != cudaSuccess) return e;
+        trace_kernel<true><<<grid, block, cache, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside,
+                                                      firstOutside, mins, beam);
+    } else {
+        trace_kernel<false><<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside,
+                                                   firstOutside, mins, beam);
+    }
     return cudaGetLastError();
 }
 
