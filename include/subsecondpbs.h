@@ -70,6 +70,10 @@ extern "C" {
 #define PBS_OPT_CT_INPUT_TYPE 4
 /* Keep intermediate per-layer buffers of the last beam for pbs_context_debug_copy. */
 #define PBS_OPT_KEEP_DEBUG 5
+/* Nuclear halo model used by beams added with nuclear_correction = 1: 0 SOUKUP,
+ * 1 FLUKA, 2 GAUSS_FIT (default). These are the reference's NUCLEAR_CORR build
+ * choices (idd_sigma.cu:102-121, wrapper.cu:3788-3795), selected at run time here. */
+#define PBS_OPT_NUCLEAR_MODEL 6
 
 /* ---- stage timer slots -------------------------------------------------- */
 #define PBS_STAGE_TRACE 0
@@ -94,6 +98,13 @@ extern "C" {
 #define PBS_DBG_BEV_DOSE 10   /* float [steps][superpY+64][superpX+64], layer-summed, absolute step index */
 #define PBS_DBG_DOSE64 11     /* double [Z][Y][X] accumulated dose                   */
 #define PBS_DBG_FIRST_PASSIVE 12 /* int [rayY][rayX] for `layer`                    */
+/* Nuclear halo of the last beam (nuclear_correction = 1), on the halo lattice
+ * nucY x nucX = spot lattice rounded up to 8 x 32 (wrapper.cu:862-864). */
+#define PBS_DBG_NUC_IDD 13    /* float [steps][nucY][nucX] for `layer` (0 outside [first, calcPassive)) */
+#define PBS_DBG_NUC_RSIGMA 14 /* float [steps][nucY][nucX] for `layer` (+inf outside)                   */
+#define PBS_DBG_NUC_TILE_BINS 15 /* uint8 [steps][nucY/8][nucX/32] for `layer` (0xff outside)          */
+#define PBS_DBG_NUC_BEV_DOSE 16  /* float [steps][nucY+64][nucX+64], layer-summed, absolute step index */
+#define PBS_DBG_RAY_TO_NUC 17    /* int [rayY][rayX]: halo cell under each ray or -1                  */
 
 /* Mirrors RTDBeamSettings (include/core/raytracedicom_integration.h:31-97). Array
  * members carry their element counts (floats/ints, not rows) so the reference's
@@ -177,6 +188,9 @@ typedef struct PbsBeamStats {
     long long superpose_fma;  /* sum over live tiles of 256*(2R+1)^2             */
     int kernel_launches;      /* kernels this library launched for the beam      */
     int layer_chunks;         /* layer chunks the per-layer working set was split into */
+    int nuc_dims[2];          /* halo lattice (0 without the nuclear halo)       */
+    long long nuc_live_tiles; /* superposed halo (tile, step) pairs             */
+    long long nuc_superpose_fma;
 } PbsBeamStats;
 
 typedef struct PbsLayerStats {
@@ -190,6 +204,9 @@ typedef struct PbsLayerStats {
     int tile_rad_counts[34];  /* histogram before overflow merge                 */
     int batched_counts[33];   /* complete_superposition.cu:476-483               */
     int live_tiles;
+    int nuc_tile_rad_counts[34]; /* halo histogram over [first, calc_passive)    */
+    int nuc_batched_counts[33];
+    float spot_dist;          /* spot spacing in rays (halo sigma and normalisation) */
 } PbsLayerStats;
 
 /* ---- library ------------------------------------------------------------ */

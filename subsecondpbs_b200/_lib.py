@@ -29,6 +29,8 @@ PBS_OPT_STAGE_TIMING = 2
 PBS_OPT_LAYER_BUDGET_MIB = 3
 PBS_OPT_CT_INPUT_TYPE = 4
 PBS_OPT_KEEP_DEBUG = 5
+PBS_OPT_NUCLEAR_MODEL = 6
+NUCLEAR_SOUKUP, NUCLEAR_FLUKA, NUCLEAR_GAUSS_FIT = 0, 1, 2
 
 STAGES = ("trace", "plan", "conv", "idd", "bin", "superpose", "transfer")
 
@@ -44,6 +46,11 @@ PBS_DBG_TILE_BINS = 9
 PBS_DBG_BEV_DOSE = 10
 PBS_DBG_DOSE64 = 11
 PBS_DBG_FIRST_PASSIVE = 12
+PBS_DBG_NUC_IDD = 13
+PBS_DBG_NUC_RSIGMA = 14
+PBS_DBG_NUC_TILE_BINS = 15
+PBS_DBG_NUC_BEV_DOSE = 16
+PBS_DBG_RAY_TO_NUC = 17
 
 _FP = C.POINTER(C.c_float)
 _IP = C.POINTER(C.c_int)
@@ -123,6 +130,7 @@ class PbsBeamStats(C.Structure):
         ("transfer_start", _arr(C.c_int, 3)), ("transfer_max", _arr(C.c_int, 3)),
         ("live_tiles", C.c_longlong), ("superpose_fma", C.c_longlong),
         ("kernel_launches", C.c_int), ("layer_chunks", C.c_int),
+        ("nuc_dims", _arr(C.c_int, 2)), ("nuc_live_tiles", C.c_longlong), ("nuc_superpose_fma", C.c_longlong),
     ]
 
 
@@ -133,6 +141,8 @@ class PbsLayerStats(C.Structure):
         ("after_last_step", C.c_int), ("max_first_passive", C.c_int), ("calc_passive", C.c_int),
         ("tile_rad_counts", _arr(C.c_int, 34)), ("batched_counts", _arr(C.c_int, 33)),
         ("live_tiles", C.c_int),
+        ("nuc_tile_rad_counts", _arr(C.c_int, 34)), ("nuc_batched_counts", _arr(C.c_int, 33)),
+        ("spot_dist", C.c_float),
     ]
 
 

@@ -164,6 +164,10 @@ int pbs_context_set_option(PbsContext* ctx, int option, long long value) {
             ctx->impl.ctInputType = int(value);
             return PBS_OK;
         case PBS_OPT_KEEP_DEBUG: ctx->impl.keepDebug = value != 0; return PBS_OK;
+        case PBS_OPT_NUCLEAR_MODEL:
+            if (value < 0 || value > 2) break;
+            ctx->impl.nuclearModel = int(value);
+            return PBS_OK;
         default: break;
     }
     pbs::set_error("unknown option or value");
@@ -223,7 +227,7 @@ int pbs_context_synchronize(PbsContext* ctx) {
         pbs::set_error(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
         return PBS_ERR_CUDA;
     }
-    return PBS_OK;
+    return ctx->impl.take_device_errors();
 }
 
 void* pbs_context_stream(PbsContext* ctx) { return ctx ? static_cast<void*>(ctx->impl.stream) : nullptr; }
@@ -356,7 +360,9 @@ void subsecondWrapper(const float* ctData, const int3& ctDims, const float3& ctR
     const int rc = pbs::subsecond_wrapper(ctData, cd, cr, cc, doseData, dd, dr, dc,
                                           beamSettings ? beams.data() : nullptr, numBeams,
                                           energyData ? &e : nullptr, gpuId, nuclearCorrection, verbose);
-    if (rc == PBS_ERR_GEOMETRY) throw std::runtime_error(pbs::last_error());
+    // The reference throws for geometry failures and for every nuclear-halo contract
+    // failure (wrapper.cu:1077-1097, 3418-3450; complete_superposition.cu:609-627).
+    if (rc == PBS_ERR_GEOMETRY || rc == PBS_ERR_UNSUPPORTED) throw std::runtime_error(pbs::last_error());
     if (rc != PBS_OK) std::fprintf(stderr, "%s\n", pbs::last_error());
 }
 

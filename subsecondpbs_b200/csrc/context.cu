@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -84,7 +85,8 @@ Context::~Context() {
     if (stream) cudaStreamSynchronize(stream);
     for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
-                      &work, &lp, &ls, &bs, &stats})
+                      &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
+                      &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord})
         b->release();
     staging.release();
     if (stagingEvent) cudaEventDestroy(stagingEvent);
@@ -108,7 +110,32 @@ int Context::init(int gpu) {
     // Callers of the reference-shaped entry points cannot pass options: the
     // environment selects the reference's BEV depth shift for them.
     if (const char* v = std::getenv("PBS_COMPAT_BEV_Z_SHIFT")) compatBevZShift = std::atoi(v) != 0;
+    // The reference fixes its nuclear model at build time (NUCLEAR_CORR); here the
+    // environment picks it for the wrapper entry points: 0 SOUKUP, 1 FLUKA, 2 GAUSS_FIT.
+    if (const char* v = std::getenv("PBS_NUCLEAR_MODEL")) {
+        const int m = std::atoi(v);
+        if (m >= 0 && m <= 2) nuclearModel = m;
+    }
+    int rc = errWord.ensure(sizeof(int));
+    if (rc) return rc;
+    PBS_CUDA(cudaMemset(errWord.ptr, 0, sizeof(int)), "cudaMemset");
     return PBS_OK;
+}
+
+int Context::take_device_errors() {
+    int flags = 0;
+    PBS_CUDA(cudaMemcpy(&flags, errWord.ptr, sizeof(int), cudaMemcpyDeviceToHost), "error flags D2H");
+    if (!flags) return PBS_OK;
+    PBS_CUDA(cudaMemset(errWord.ptr, 0, sizeof(int)), "cudaMemset");
+    if (flags & 4) {
+        // complete_superposition.cu:609-627 throws here.
+        set_error("Nuclear superposition kernel radius exceeded kMaxSuperpR=32 (a halo sigma below the tile "
+                  "radius threshold); the dose of that beam is incomplete");
+        return PBS_ERR_UNSUPPORTED;
+    }
+    set_error("device reported an internal error flag " + std::to_string(flags) +
+              " (1: work list overflow, 2: radius outside a superposition instance)");
+    return PBS_ERR_CUDA;
 }
 
 // Copies `n` host bytes to the device through the pinned staging buffer so the
@@ -154,14 +181,28 @@ int Context::set_energy(const PbsEnergyDesc& e) {
     energy.density_vector = densityHost.data();
     energy.sp_vector = spHost.data();
     energy.rrl_vector = rrlHost.data();
-    energy.nuc_weight_matrix = nullptr;
-    energy.n_nuc_weight_matrix = 0;
-    energy.nuc_sq_sigma_matrix = nullptr;
-    energy.n_nuc_sq_sigma_matrix = 0;
+    // Nuclear weight / sigma^2 tables on the CIDD axes (energy_reader.cpp:135-182),
+    // kept only when both are complete.
+    const size_t nTab = size_t(e.n_energies) * size_t(e.n_energy_samples);
+    const bool hasNuc = e.nuc_weight_matrix && e.nuc_sq_sigma_matrix && e.n_nuc_weight_matrix == nTab &&
+                        e.n_nuc_sq_sigma_matrix == nTab;
+    nucWeightHost.assign(hasNuc ? e.nuc_weight_matrix : nullptr, hasNuc ? e.nuc_weight_matrix + nTab : nullptr);
+    nucSqSigmaHost.assign(hasNuc ? e.nuc_sq_sigma_matrix : nullptr, hasNuc ? e.nuc_sq_sigma_matrix + nTab : nullptr);
+    nucTablesAligned = hasNuc && e.nuclear_tables_aligned_to_primary_axis;
+    energy.nuc_weight_matrix = hasNuc ? nucWeightHost.data() : nullptr;
+    energy.n_nuc_weight_matrix = hasNuc ? nTab : 0;
+    energy.nuc_sq_sigma_matrix = hasNuc ? nucSqSigmaHost.data() : nullptr;
+    energy.n_nuc_sq_sigma_matrix = hasNuc ? nTab : 0;
     int rc;
     if ((rc = cidd.ensure(ciddHost.size() * 4)) || (rc = density.ensure(densityHost.size() * 4)) ||
         (rc = sp.ensure(spHost.size() * 4)) || (rc = rrl.ensure(rrlHost.size() * 4)))
         return rc;
+    if (hasNuc) {
+        if ((rc = nucWeight.ensure(nTab * 4)) || (rc = nucSqSigma.ensure(nTab * 4))) return rc;
+        PBS_CUDA(cudaMemcpyAsync(nucWeight.ptr, nucWeightHost.data(), nTab * 4, cudaMemcpyHostToDevice, stream), "LUT");
+        PBS_CUDA(cudaMemcpyAsync(nucSqSigma.ptr, nucSqSigmaHost.data(), nTab * 4, cudaMemcpyHostToDevice, stream),
+                 "LUT");
+    }
     PBS_CUDA(cudaMemcpyAsync(cidd.ptr, ciddHost.data(), ciddHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
     PBS_CUDA(cudaMemcpyAsync(density.ptr, densityHost.data(), densityHost.size() * 4, cudaMemcpyHostToDevice, stream),
              "LUT");
@@ -180,6 +221,8 @@ int Context::set_energy(const PbsEnergyDesc& e) {
     luts.rrl = static_cast<const float*>(rrl.ptr);
     luts.nRrl = e.n_rrl_samples;
     luts.rrlScale = e.rrl_scale_fact;
+    luts.nucWeight = hasNuc ? static_cast<const float*>(nucWeight.ptr) : nullptr;
+    luts.nucSqSigma = hasNuc ? static_cast<const float*>(nucSqSigma.ptr) : nullptr;
     hasEnergy = true;
     return PBS_OK;
 }
@@ -292,7 +335,7 @@ int Context::read_dose(float* out, int onDevice) {
              "dose_to_float");
     PBS_CUDA(cudaMemcpyAsync(out, floatOut.ptr, n * 4, cudaMemcpyDeviceToHost, stream), "dose D2H");
     PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-    return PBS_OK;
+    return take_device_errors();
 }
 
 int Context::read_dose64(double* out, int onDevice) {
@@ -305,7 +348,10 @@ int Context::read_dose64(double* out, int onDevice) {
     PBS_CUDA(cudaMemcpyAsync(out, dose64.ptr, n * 8, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                              stream),
              "dose64 copy");
-    if (!onDevice) PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    if (!onDevice) {
+        PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        return take_device_errors();
+    }
     return PBS_OK;
 }
 
@@ -315,9 +361,16 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
         set_error("context needs lookup tables, CT and dose grid before add_beam");
         return PBS_ERR_NOT_READY;
     }
-    if (nuclear) {
-        set_error("nuclear_correction=true requested, but this build has no nuclear halo tables loaded");
-        return PBS_ERR_UNSUPPORTED;
+    if (nuclear) {  // enforceNuclearCorrectionContract (wrapper.cu:1077-1097)
+        if (!luts.nucWeight || !luts.nucSqSigma) {
+            set_error("nuclear_correction=true requested, but RTDEnergyStruct does not carry nuclear_weight/sigma tables");
+            return PBS_ERR_UNSUPPORTED;
+        }
+        if (!nucTablesAligned) {
+            set_error("nuclear_correction=true requested, but nuclear LUTs are not aligned to the active primary "
+                      "energy-depth axis");
+            return PBS_ERR_UNSUPPORTED;
+        }
     }
     std::string err;
     if (!validate_beam(b, 0, err)) {
@@ -329,6 +382,10 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     if (rc) {
         set_error(err);
         return rc;
+    }
+    if (nuclear && !plan.hasLattice) {
+        set_error("nuclear_correction=true requires raw spot lattice inputs; legacy CPB fallback cannot drive halo mode");
+        return PBS_ERR_UNSUPPORTED;
     }
     const BeamPlan& P = plan;
     BeamGeomDev& g = geom;
@@ -366,6 +423,66 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     g.doseY = doseGrid.dims[1];
     g.doseZ = doseGrid.dims[2];
     g.compatBevZShift = compatBevZShift;
+    g.errWord = static_cast<int*>(errWord.ptr);
+    // Transport constants (idd_sigma.cu:102-121) and the nuclear halo grid.
+    g.eRefSq = 198.81f;
+    g.sigmaDelta = 0.21f;
+    g.suppressDistalDip = 0;
+    g.entrySigmaScale = 1.0f;
+    if (nuclear) {
+        if (nuclearModel == 0) {  // SOUKUP
+            g.eRefSq = 190.44f;
+            g.sigmaDelta = 0.0f;
+        } else if (nuclearModel == 1) {  // FLUKA
+            g.eRefSq = 216.09f;
+            g.sigmaDelta = 0.08f;
+        } else {  // GAUSS_FIT (wrapper.cu:3788-3795 narrows the entry sigma too)
+            g.eRefSq = 169.00f;
+            g.sigmaDelta = 0.06f;
+            g.suppressDistalDip = 1;
+            g.entrySigmaScale = 0.97f;
+        }
+        g.nucOn = 1;
+        g.nucX = (P.lattice.nx + kTileX - 1) / kTileX * kTileX;
+        g.nucY = (P.lattice.ny + kTileY - 1) / kTileY * kTileY;
+    }
+    // Halo lattice plan (buildHaloLatticePlan, wrapper.cu:804-929): the ray under
+    // every lattice cell; the halo grid is the spot lattice padded to 32 x 8.
+    std::vector<int> hRayToNuc;
+    if (nuclear) {
+        hRayToNuc.assign(size_t(g.rayX) * g.rayY, -1);
+        for (int sy = 0; sy < P.lattice.ny; ++sy) {
+            const float gy = P.lattice.oy + float(sy) * P.lattice.dy;
+            const int ry = int(std::lround((gy - P.cpbCorner.y) / P.cpbRes.y));
+            if (ry < 0 || ry >= g.rayY) {
+                set_error("failed to build halo lattice plan: dense halo lattice row mapped outside active ray grid");
+                return PBS_ERR_GEOMETRY;
+            }
+            for (int sx = 0; sx < P.lattice.nx; ++sx) {
+                const float gx = P.lattice.ox + float(sx) * P.lattice.dx;
+                const int rx = int(std::lround((gx - P.cpbCorner.x) / P.cpbRes.x));
+                if (rx < 0 || rx >= g.rayX) {
+                    set_error("failed to build halo lattice plan: dense halo lattice column mapped outside active ray "
+                              "grid");
+                    return PBS_ERR_GEOMETRY;
+                }
+                hRayToNuc[size_t(ry) * g.rayX + rx] = sy * g.nucX + sx;
+            }
+        }
+        BeamGeomDev& gn = nucGeom;
+        gn = g;
+        gn.pitchX = g.nucX;
+        gn.pitchY = g.nucY;
+        gn.tilesX = g.nucX / kTileX;
+        gn.tilesY = g.nucY / kTileY;
+        gn.bevX = g.nucX + 2 * kMaxR;
+        gn.bevY = g.nucY + 2 * kMaxR;
+        // Halo BEV index -> dose index: the lattice spacing and offset (used as mm,
+        // wrapper.cu:5522-5535) replace the ray grid in x and y.
+        gn.rayIdxToDoseIdx.fanIdxToFan = idxxf(v3(P.lattice.dx, P.lattice.dy, P.fanDelta.z),
+                                               v3(P.lattice.ox, P.lattice.oy, P.fanCorner.z));
+    }
+    lastNuclear = nuclear != 0;
 
     const int L = P.numLayers;
     const size_t S = size_t(P.tracerSteps);
@@ -385,6 +502,14 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
         (rc = iddBuf.ensure(size_t(chunk) * S * padPlane * 4)) || (rc = rsBuf.ensure(size_t(chunk) * S * padPlane * 4)) ||
         (rc = firstPassive.ensure(size_t(chunk) * rays * 4)) || (rc = lp.ensure(size_t(L) * sizeof(LayerParamsDev))) ||
         (rc = ls.ensure(size_t(L) * sizeof(LayerStateDev))) || (rc = bs.ensure(sizeof(BeamStateDev))))
+        return rc;
+    const size_t nucPlane = size_t(g.nucX) * g.nucY, nucTiles = nucPlane / (kTileX * kTileY);
+    if (nuclear &&
+        ((rc = rayToNuc.ensure(rays * 4)) || (rc = nucIddBuf.ensure(size_t(chunk) * S * nucPlane * 4)) ||
+         (rc = nucRsBuf.ensure(size_t(chunk) * S * nucPlane * 4)) || (rc = nucCodes.ensure(size_t(chunk) * S * nucTiles)) ||
+         (rc = nucWork.ensure(size_t(chunk) * S * nucTiles * sizeof(int4))) ||
+         (rc = nucBev.ensure(S * nucGeom.bevX * nucGeom.bevY * 4)) ||
+         (rc = nucLs.ensure(size_t(L) * sizeof(LayerStateDev))) || (rc = nucBs.ensure(sizeof(BeamStateDev)))))
         return rc;
     if (idd_smem_bytes(g, luts) > size_t(200) * 1024) {
         set_error("beam needs " + std::to_string(P.tracerSteps) + " tracer steps; at most ~3000 are supported");
@@ -411,14 +536,24 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
         d.sigmaXmm = H.sigmaXmm;
         d.sigmaYmm = H.sigmaYmm;
         d.spotDist = H.spotDist;
+        // With the halo the lattice spacing is taken as mm when the beam gives no
+        // explicit spot spacing (wrapper.cu:4333-4347).
+        if (nuclear && std::fabs(P.fanDelta.x) > 1e-6f) {
+            const float spacing = b.spot_delta[0] > b.ray_spacing[0] * 1.5f ? b.spot_delta[0] : P.lattice.dx;
+            d.spotDist = std::fabs(spacing / P.fanDelta.x);
+        }
     }
+    layerSpotDist.resize(L);
+    for (int l = 0; l < L; ++l) layerSpotDist[l] = hlp[l].spotDist;
     BeamStateDev hbs;
     std::memset(&hbs, 0, sizeof(hbs));
     hbs.firstInside = INT32_MAX;
     hbs.firstOutside = INT32_MIN;
     const size_t latBytes = P.hasLattice ? P.lattice.weights.size() * 4 : 0;
     const size_t subBytes = P.hasLattice ? 0 : b.n_subspot_data * 4;
-    const size_t upBytes = hlp.size() * sizeof(LayerParamsDev) + sizeof(BeamStateDev) + latBytes + subBytes;
+    const size_t nucMapBytes = nuclear ? hRayToNuc.size() * 4 : 0;
+    const size_t upBytes =
+        hlp.size() * sizeof(LayerParamsDev) + 2 * sizeof(BeamStateDev) + latBytes + subBytes + nucMapBytes;
     {
         PBS_CUDA(cudaEventSynchronize(stagingEvent), "cudaEventSynchronize");
         if ((rc = staging.ensure(upBytes + 256))) return rc;
@@ -433,11 +568,23 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
             if ((rc = lattice.ensure(latBytes)) || (rc = interm.ensure(size_t(L) * g.latNy * g.rayX * 4))) return rc;
             std::memcpy(p, P.lattice.weights.data(), latBytes);
             PBS_CUDA(cudaMemcpyAsync(lattice.ptr, p, latBytes, cudaMemcpyHostToDevice, stream), "H2D");
+            p += latBytes;
         }
         if (subBytes) {
             if ((rc = subspots.ensure(subBytes)) || (rc = cpb.ensure(size_t(L) * rays * 4))) return rc;
             std::memcpy(p, b.subspot_data, subBytes);
             PBS_CUDA(cudaMemcpyAsync(subspots.ptr, p, subBytes, cudaMemcpyHostToDevice, stream), "H2D");
+            p += subBytes;
+        }
+        if (nuclear) {
+            std::memcpy(p, hRayToNuc.data(), nucMapBytes);
+            PBS_CUDA(cudaMemcpyAsync(rayToNuc.ptr, p, nucMapBytes, cudaMemcpyHostToDevice, stream), "H2D");
+            p += nucMapBytes;
+            std::memcpy(p, &hbs, sizeof(hbs));
+            PBS_CUDA(cudaMemcpyAsync(nucBs.ptr, p, sizeof(hbs), cudaMemcpyHostToDevice, stream), "H2D");
+            p += sizeof(hbs);
+            PBS_CUDA(cudaMemsetAsync(nucLs.ptr, 0, size_t(L) * sizeof(LayerStateDev), stream), "memset");
+            PBS_CUDA(cudaMemsetAsync(nucBev.ptr, 0, S * nucGeom.bevX * nucGeom.bevY * 4, stream), "memset");
         }
         PBS_CUDA(cudaEventRecord(stagingEvent, stream), "cudaEventRecord");
     }
@@ -477,29 +624,57 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     int smCount = 148;
     cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
     const int workCap = int(size_t(chunk) * S * tiles);
+    const int nucWorkCap = int(size_t(chunk) * S * nucTiles);
+    float* dNucIdd = static_cast<float*>(nucIddBuf.ptr);
+    float* dNucRs = static_cast<float*>(nucRsBuf.ptr);
+    LayerStateDev* dNucLs = static_cast<LayerStateDev*>(nucLs.ptr);
+    BeamStateDev* dNucBs = static_cast<BeamStateDev*>(nucBs.ptr);
     for (int l0 = 0; l0 < L; l0 += chunk) {
         const int nl = std::min(chunk, L - l0);
+        if (nuclear) PBS_CUDA(launch_nuc_prepare(nucGeom, nl, dNucIdd, dNucRs, stream), "nuc_prepare");
         PBS_CUDA(launch_idd(g, luts, l0, nl, dDens, dWepl, dFi, dFo, dRayW, dlp, dls, dbs,
                             static_cast<float*>(iddBuf.ptr), static_cast<float*>(rsBuf.ptr),
-                            static_cast<uint8_t*>(codes.ptr), static_cast<int*>(firstPassive.ptr), stream),
+                            static_cast<uint8_t*>(codes.ptr), static_cast<int*>(firstPassive.ptr),
+                            static_cast<const int*>(rayToNuc.ptr), static_cast<const float*>(lattice.ptr), dNucIdd,
+                            dNucRs, stream),
                  "idd");
         if (l0 == 0 && (rc = mark(4))) return rc;
         PBS_CUDA(launch_bin_plan(g, l0, nl, static_cast<const uint8_t*>(codes.ptr), dls, dbs,
-                                 static_cast<int4*>(work.ptr), workCap, stream),
+                                 static_cast<int4*>(work.ptr), workCap, nullptr, nullptr, stream),
                  "bin_plan");
+        if (nuclear) {
+            PBS_CUDA(launch_nuc_codes(nucGeom, l0, nl, dNucIdd, dNucRs, dls, dbs, dNucLs,
+                                      static_cast<uint8_t*>(nucCodes.ptr), stream),
+                     "nuc_codes");
+            PBS_CUDA(launch_bin_plan(nucGeom, l0, nl, static_cast<const uint8_t*>(nucCodes.ptr), dNucLs, dNucBs,
+                                     static_cast<int4*>(nucWork.ptr), nucWorkCap, dls, dbs, stream),
+                     "nuc_bin_plan");
+        }
         if (l0 == 0 && (rc = mark(5))) return rc;
         PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
                                   static_cast<const int4*>(work.ptr), dbs, dBev, smCount, stream),
                  "superpose");
+        if (nuclear)
+            PBS_CUDA(launch_superpose(nucGeom, dNucIdd, dNucRs, static_cast<const int4*>(nucWork.ptr), dNucBs,
+                                      static_cast<float*>(nucBev.ptr), smCount, stream),
+                     "nuc_superpose");
     }
     if ((rc = mark(6))) return rc;
     PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
+    if (nuclear) {
+        PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, stream), "nuc_transfer_planner");
+        PBS_CUDA(launch_transfer(nucGeom, static_cast<const float*>(nucBev.ptr), dNucBs,
+                                 static_cast<double*>(dose64.ptr), stream),
+                 "nuc_transfer");
+    }
     if ((rc = mark(7))) return rc;
     lastChunks = (L + chunk - 1) / chunk;
     // trace, planner, two fluence kernels, five per chunk (IDD, layer plan, work
-    // scatter, two superposition ranges), transfer planner, transfer.
-    lastLaunches = 6 + 5 * lastChunks;
+    // scatter, two superposition ranges), transfer planner, transfer; the halo adds
+    // six per chunk (clear, codes, layer plan, scatter, two superposition ranges)
+    // and its transfer planner and transfer.
+    lastLaunches = 6 + 5 * lastChunks + (nuclear ? 6 * lastChunks + 2 : 0);
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;
@@ -555,8 +730,22 @@ int Context::beam_stats(PbsBeamStats* out) {
     out->superpose_fma = h.superposeFma;
     out->kernel_launches = lastLaunches;
     out->layer_chunks = lastChunks;
-    if (h.errorFlags) {
-        set_error("device reported an error flag (work list overflow)");
+    int flags = h.errorFlags;
+    if (lastNuclear) {
+        BeamStateDev hn;
+        PBS_CUDA(cudaMemcpy(&hn, nucBs.ptr, sizeof(hn), cudaMemcpyDeviceToHost), "stats D2H");
+        out->nuc_dims[0] = geom.nucX;
+        out->nuc_dims[1] = geom.nucY;
+        out->nuc_live_tiles = hn.liveTiles;
+        out->nuc_superpose_fma = hn.superposeFma;
+        flags |= hn.errorFlags;
+    }
+    if (flags & 4) {
+        set_error("Nuclear superposition kernel radius exceeded kMaxSuperpR=32");
+        return PBS_ERR_UNSUPPORTED;
+    }
+    if (flags) {
+        set_error("device reported an internal error flag " + std::to_string(flags));
         return PBS_ERR_CUDA;
     }
     return PBS_OK;
@@ -585,6 +774,14 @@ int Context::layer_stats(int layer, PbsLayerStats* out) {
     for (int i = 0; i < kBuckets; ++i) out->tile_rad_counts[i] = h.hist[i];
     for (int i = 0; i <= kMaxR; ++i) out->batched_counts[i] = h.batchedCounts[i];
     out->live_tiles = h.liveTiles;
+    out->spot_dist = layer < int(layerSpotDist.size()) ? layerSpotDist[layer] : 0.0f;
+    if (lastNuclear) {
+        LayerStateDev hn;
+        PBS_CUDA(cudaMemcpy(&hn, static_cast<LayerStateDev*>(nucLs.ptr) + layer, sizeof(hn), cudaMemcpyDeviceToHost),
+                 "stats D2H");
+        for (int i = 0; i < kBuckets; ++i) out->nuc_tile_rad_counts[i] = hn.hist[i];
+        for (int i = 0; i <= kMaxR; ++i) out->nuc_batched_counts[i] = hn.batchedCounts[i];
+    }
     return PBS_OK;
 }
 
@@ -625,7 +822,13 @@ int Context::debug_copy(int which, int layer, void* out, size_t bytes) {
         return PBS_OK;
     };
     const bool perLayer = which == PBS_DBG_IDD || which == PBS_DBG_RSIGMA || which == PBS_DBG_TILE_BINS ||
-                          which == PBS_DBG_FIRST_PASSIVE;
+                          which == PBS_DBG_FIRST_PASSIVE || which == PBS_DBG_NUC_IDD || which == PBS_DBG_NUC_RSIGMA ||
+                          which == PBS_DBG_NUC_TILE_BINS;
+    const bool nucBuf = which >= PBS_DBG_NUC_IDD && which <= PBS_DBG_RAY_TO_NUC;
+    if (nucBuf && !lastNuclear) {
+        set_error("the last beam has no nuclear halo");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
     if (perLayer) {
         if (!keepDebug || layer < 0 || layer >= plan.numLayers || layer >= chunkLayers) {
             set_error("per-layer debug buffers need PBS_OPT_KEEP_DEBUG and a valid layer");
@@ -698,6 +901,50 @@ int Context::debug_copy(int which, int layer, void* out, size_t bytes) {
                          "debug D2H");
             return PBS_OK;
         }
+        case PBS_DBG_RAY_TO_NUC: return copy(rayToNuc.ptr, rays * 4);
+        case PBS_DBG_NUC_BEV_DOSE: {
+            const size_t plane = size_t(nucGeom.bevX) * nucGeom.bevY;
+            if (bytes != S * plane * 4) {
+                set_error("debug_copy: halo BEV size mismatch");
+                return PBS_ERR_INVALID_ARGUMENT;
+            }
+            std::memset(out, 0, bytes);
+            const size_t nz = S - size_t(std::max(first, 0));
+            PBS_CUDA(cudaMemcpy(static_cast<char*>(out) + size_t(first) * plane * 4, nucBev.ptr, nz * plane * 4,
+                                cudaMemcpyDeviceToHost),
+                     "debug D2H");
+            return PBS_OK;
+        }
+        case PBS_DBG_NUC_IDD:
+        case PBS_DBG_NUC_RSIGMA:
+        case PBS_DBG_NUC_TILE_BINS: {
+            const size_t nucPlane = size_t(geom.nucX) * geom.nucY;
+            const size_t nucTiles = nucPlane / (kTileX * kTileY);
+            const bool bins = which == PBS_DBG_NUC_TILE_BINS;
+            const size_t elem = bins ? 1 : 4, per = bins ? nucTiles : nucPlane;
+            if (bytes != S * per * elem) {
+                set_error("debug_copy: halo buffer size mismatch");
+                return PBS_ERR_INVALID_ARGUMENT;
+            }
+            LayerStateDev lh;
+            PBS_CUDA(cudaMemcpy(&lh, static_cast<LayerStateDev*>(ls.ptr) + layer, sizeof(lh), cudaMemcpyDeviceToHost),
+                     "debug D2H");
+            if (bins) {
+                std::memset(out, 0xff, bytes);
+            } else {
+                float* o = static_cast<float*>(out);
+                std::fill(o, o + S * per, which == PBS_DBG_NUC_IDD ? 0.0f : __builtin_inff());
+            }
+            // The halo is computed over [first, afterLast); its codes over [first, calcPassive).
+            const int nz = std::max(0, (bins ? lh.calcPassive : lh.afterLast) - first);
+            const void* srcBase = bins ? nucCodes.ptr : (which == PBS_DBG_NUC_IDD ? nucIddBuf.ptr : nucRsBuf.ptr);
+            const char* src = static_cast<const char*>(srcBase) + size_t(layer) * S * per * elem;
+            if (nz > 0)
+                PBS_CUDA(cudaMemcpy(static_cast<char*>(out) + size_t(first) * per * elem, src, size_t(nz) * per * elem,
+                                    cudaMemcpyDeviceToHost),
+                         "debug D2H");
+            return PBS_OK;
+        }
         default:
             set_error("unknown debug buffer");
             return PBS_ERR_INVALID_ARGUMENT;
@@ -728,10 +975,6 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
     if (!validate_global(ctData, cg, doseData, dg, beams, numBeams, energyData, err)) {
         set_error(err);
         return PBS_ERR_INVALID_ARGUMENT;
-    }
-    if (nuclear) {
-        set_error("nuclear_correction=true requested, but this build has no nuclear halo tables loaded");
-        return PBS_ERR_UNSUPPORTED;
     }
     for (size_t i = 0; i < numBeams; ++i) {
         if (!validate_beam(beams[i], i, err)) {

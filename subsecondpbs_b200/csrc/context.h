@@ -40,12 +40,15 @@ struct Context {
     int keepDebug = 0;
     int ctInputType = PBS_CT_AUTO;
     long long layerBudgetMiB = 2048;
+    int nuclearModel = 2;  // GAUSS_FIT
 
     // Lookup tables.
     bool hasEnergy = false;
     PbsEnergyDesc energy{};
     std::vector<float> energiesPerU, peakDepths, scaleFacts, ciddHost, densityHost, spHost, rrlHost;
-    DevBuf cidd, density, sp, rrl;
+    std::vector<float> nucWeightHost, nucSqSigmaHost;
+    bool nucTablesAligned = false;
+    DevBuf cidd, density, sp, rrl, nucWeight, nucSqSigma;
     LutsDev luts{};
 
     // CT (HU+1000) and dose accumulator.
@@ -60,6 +63,11 @@ struct Context {
     // Per-beam working set (grow-only).
     DevBuf dens, wepl, weplMin, rayW, interm, lattice, iddBuf, rsBuf, bev, cpb, subspots, floatOut;
     DevBuf firstIn, firstOut, firstPassive, codes, work, lp, ls, bs, stats;
+    // Nuclear halo working set and the device word collecting error flags.
+    DevBuf rayToNuc, nucIddBuf, nucRsBuf, nucCodes, nucWork, nucBev, nucLs, nucBs, errWord;
+    BeamGeomDev nucGeom{};
+    bool lastNuclear = false;
+    std::vector<float> layerSpotDist;
     PinnedBuf staging;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
@@ -77,6 +85,9 @@ struct Context {
     int init(int gpu);
     int upload(void* dst, const void* src, size_t n);
     int set_energy(const PbsEnergyDesc& e);
+    // Reads (and clears) the error flags the kernels raised since the last check;
+    // the stream must be synchronised. PBS_OK when none.
+    int take_device_errors();
     int set_ct(const float* data, int onDevice, const GridDesc& g);
     int set_dose_grid(const GridDesc& g);
     int reset_dose(const float* init, int onDevice);

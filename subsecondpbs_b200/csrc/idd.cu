@@ -16,8 +16,6 @@ namespace {
 constexpr float kPInv = 0.5649718f;   // 1/p, p = 1.77 (raytracedicom_integration.h:22)
 constexpr float kECoef = 8.639415f;   // (10 alpha)^(-1/p) (raytracedicom_integration.h:23)
 constexpr float kSqrt2 = 1.41421356f;
-constexpr float kERefSq = 198.81f;    // 14.1^2
-constexpr float kSigmaDelta = 0.21f;
 constexpr int kMaxChunkLayers = 64;
 
 // One CTA = one 32x8 tile of rays for one layer. Each thread walks its ray from the
@@ -27,15 +25,19 @@ constexpr int kMaxChunkLayers = 64;
 // turns the eight warp partials of every step into the tile's radius bucket
 // (tileRadCalc, complete_superposition.cu:198-255), stores the code and adds the
 // tile's bucket counts to the layer histogram.
+template <bool kNuclear>
 __global__ void __launch_bounds__(256)
 idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ density,
            const float* __restrict__ wepl, const int* __restrict__ firstInside, const int* __restrict__ firstOutside,
            const float* __restrict__ rayW, const LayerParamsDev* __restrict__ lp, LayerStateDev* __restrict__ ls,
            const BeamStateDev* __restrict__ beam, float* __restrict__ iddOut, float* __restrict__ rsigOut,
-           uint8_t* __restrict__ codes, int* __restrict__ firstPassiveOut) {
+           uint8_t* __restrict__ codes, int* __restrict__ firstPassiveOut, const int* __restrict__ rayToNuc,
+           const float* __restrict__ lattice, float* __restrict__ nucIddOut, float* __restrict__ nucRsOut) {
     extern __shared__ float smem[];
     float* ciddRow = smem;                                    // [nS]
-    float* rrlTab = ciddRow + luts.nS;                        // [nRrl]
+    float* nucWRow = ciddRow + luts.nS;                       // [nS] with the nuclear halo
+    float* nucSRow = nucWRow + (kNuclear ? luts.nS : 0);      // [nS] with the nuclear halo
+    float* rrlTab = nucSRow + (kNuclear ? luts.nS : 0);       // [nRrl]
     float* stepNum = rrlTab + luts.nRrl;                      // [steps] 0.5 (voxel width x + y)
     float* stepVolT = stepNum + g.steps;                      // [steps] step volume
     float* partMin = stepVolT + g.steps;                      // [steps][8]
@@ -66,6 +68,19 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         for (int d = tid; d < luts.nS; d += 256) {
             const float a0 = __ldg(r0 + d), a1 = __ldg(r1 + d);
             ciddRow[d] = a0 + (a1 - a0) * b;
+        }
+        if (kNuclear) {
+            // Nuclear weight and sigma^2 tables share the CIDD axes (energy_reader.cpp:135-182).
+            const float* w0 = luts.nucWeight + static_cast<size_t>(e0) * luts.nS;
+            const float* w1 = luts.nucWeight + static_cast<size_t>(e1) * luts.nS;
+            const float* q0 = luts.nucSqSigma + static_cast<size_t>(e0) * luts.nS;
+            const float* q1 = luts.nucSqSigma + static_cast<size_t>(e1) * luts.nS;
+            for (int d = tid; d < luts.nS; d += 256) {
+                const float a0 = __ldg(w0 + d), a1 = __ldg(w1 + d);
+                nucWRow[d] = a0 + (a1 - a0) * b;
+                const float c0 = __ldg(q0 + d), c1 = __ldg(q1 + d);
+                nucSRow[d] = c0 + (c1 - c0) * b;
+            }
         }
         for (int d = tid; d < luts.nRrl; d += 256) rrlTab[d] = __ldg(luts.rrl + d);
         // Per-step voxel widths and volumes are the same for every ray of the step
@@ -108,6 +123,26 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         }
     }
 
+    // Nuclear halo of this ray (idd_sigma.cu:88-98, 131-142): only rays under a
+    // halo lattice cell carry a halo value; the cell's raw spot weight is its
+    // weight. Every ray's primary dose keeps the (1 - nuclear weight) share.
+    const bool nucOn = kNuclear && p.spotDist > 0.0f;
+    int nucIdx = -1;
+    float nucRayWeight = 0.0f;
+    if (nucOn && real) {
+        nucIdx = rayToNuc[ridx];
+        if (nucIdx >= 0)
+            nucRayWeight = lattice[(static_cast<size_t>(l) * g.latNy + nucIdx / g.nucX) * g.latNx + nucIdx % g.nucX];
+    }
+    const size_t nucPlane = static_cast<size_t>(g.nucX) * g.nucY;
+    float* nucIddL = nucIddOut + lc * static_cast<size_t>(g.steps) * nucPlane;
+    float* nucRsL = nucRsOut + lc * static_cast<size_t>(g.steps) * nucPlane;
+    const float spotDist = p.spotDist;
+    const float entrySigmaSq = ls[l].entrySigmaSq;
+    const float eRefSq = nucOn ? g.eRefSq : 198.81f;
+    const float sigmaDelta = nucOn ? g.sigmaDelta : 0.21f;
+    const bool suppressDip = nucOn && g.suppressDistalDip;
+
     const float stepLength = fabsf(g.fanDelta.z);
     const float quad = p.sigmaSqAirQuad;
     float cumulSpOld = 0.0f, cumulDoseOld = 0.0f;
@@ -125,6 +160,8 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     for (int stepNo = first; stepNo < afterLastL; ++stepNo) {
         float res = 0.0f;
         float rSigmaEff = __int_as_float(0x7f800000);
+        float nucRes = 0.0f;
+        float nucRSigmaEff = __int_as_float(0x7f800000);
         if (live) {
             const float cumulSp = nextSp;
             const float dens = nextDens;
@@ -138,17 +175,32 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
                 const float resE = kECoef * __powf(p.peakDepth - 0.5f * (cumulSp + cumulSpOld), kPInv);
                 const float betaP = resE + 938.3f - 938.3f * 938.3f / (resE + 938.3f);
                 const float rRl = dens * lut_linear_clamp_smem(rrlTab, luts.nRrl, dens * luts.rrlScale + 0.5f);
-                const float thetaSq = kERefSq / (betaP * betaP) * stepLength * rRl;
+                const float thetaSq = eRefSq / (betaP * betaP) * stepLength * rRl;
                 sigmaSq += incScat + incDiv;
                 incincScat += 2.0f * thetaSq * stepLength * stepLength;
                 incScat += incincScat;
                 incDiv += 2.0f * quad;
-            } else {
+            } else if (!suppressDip) {
                 sigmaSq -= 1.5f * (incScat + incDiv) * dens;
             }
-            rSigmaEff = stepNum[stepNo] / (kSqrt2 * (sqrtf(sigmaSq) + kSigmaDelta));
+            rSigmaEff = stepNum[stepNo] / (kSqrt2 * (sqrtf(sigmaSq) + sigmaDelta));
             const float mass = dens * stepVolT[stepNo];
-            if (mass > 1e-2f) res = rayWeight * (cumulDose - cumulDoseOld) / mass;
+            if (nucOn) {
+                const float depthMidIdx = 0.5f * (cumulSp + cumulSpOld) * p.energyScaleFact + 0.5f;
+                if (mass > 1e-2f) {
+                    const float nucWeight = lut_linear_clamp_smem(nucWRow, luts.nS, depthMidIdx);
+                    res = (1.0f - nucWeight) * rayWeight * (cumulDose - cumulDoseOld) / mass;
+                    if (nucIdx >= 0)
+                        nucRes = nucWeight * nucRayWeight * (cumulDose - cumulDoseOld) / (mass * spotDist * spotDist);
+                }
+                if (nucIdx >= 0) {
+                    const float nucSqSigma = lut_linear_clamp_smem(nucSRow, luts.nS, depthMidIdx);
+                    nucRSigmaEff = 0.5f * spotDist * (2.0f * stepNum[stepNo]) /
+                                   (kSqrt2 * sqrtf(sigmaSq + nucSqSigma + entrySigmaSq));
+                }
+            } else if (mass > 1e-2f) {
+                res = rayWeight * (cumulDose - cumulDoseOld) / mass;
+            }
             cumulSpOld = cumulSp;
             cumulDoseOld = cumulDose;
             if (cumulSp > p.rangeStopDepth || static_cast<unsigned int>(stepNo) == afterLast) {
@@ -159,11 +211,17 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         if (!live || stepNo < firstIn - 1) {
             res = 0.0f;
             rSigmaEff = __int_as_float(0x7f800000);
+            nucRes = 0.0f;
+            nucRSigmaEff = __int_as_float(0x7f800000);
         }
         const int zr = stepNo - first;
         const size_t o = static_cast<size_t>(zr) * padPlane + static_cast<size_t>(y) * g.pitchX + x;
         iddL[o] = res;
         rsL[o] = rSigmaEff;
+        if (nucIdx >= 0) {
+            nucIddL[static_cast<size_t>(zr) * nucPlane + nucIdx] = nucRes;
+            nucRsL[static_cast<size_t>(zr) * nucPlane + nucIdx] = nucRSigmaEff;
+        }
 
         // Warp minimum on order-preserving unsigned keys of the floats; the device's
         // canonical NaN maps above +inf and drops out, as it does under fminf.
@@ -216,23 +274,37 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
 // and batching of sparse buckets into the radius above them
 // (complete_superposition.cu:476-483). Thread 0 then lays out the chunk's work list
 // in descending radius.
+//
+// With `primaryLs` set the kernel plans the nuclear halo of the chunk instead
+// (performNuclearTileBasedSuperposition, complete_superposition.cu:558-708): the
+// halo histogram already covers [first, calcPassive) of the primary layer, and a
+// radius above 32 is an error (the reference throws) rather than a merge.
 __global__ void __launch_bounds__(kMaxChunkLayers)
 layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restrict__ ls,
-                  BeamStateDev* __restrict__ beam, int workCapacity) {
+                  BeamStateDev* __restrict__ beam, int workCapacity, const LayerStateDev* __restrict__ primaryLs,
+                  const BeamStateDev* __restrict__ primaryBeam) {
     const int lc = threadIdx.x;
-    const int first = beam->firstInside;
+    const bool nuclear = primaryLs != nullptr;
+    const int first = nuclear ? primaryBeam->firstInside : beam->firstInside;
     const int tiles = g.tilesX * g.tilesY;
     if (lc < nLayers) {
         LayerStateDev& st = ls[layer0 + lc];
-        int calc = st.maxFirstPassive;
-        if (calc < first + 1) calc = first + 1;
-        if (calc < 0) calc = first + 1;
-        if (calc > st.afterLast) calc = st.afterLast;
-        if (calc > g.steps) calc = g.steps;
-        st.calcPassive = calc;
         int hist[kBuckets];
         for (int i = 0; i < kBuckets; ++i) hist[i] = st.histAll[i];
-        if (st.afterLast > calc && st.afterLast > first) hist[0] -= (st.afterLast - max(calc, first)) * tiles;
+        if (nuclear) {
+            const int calc = primaryLs[layer0 + lc].calcPassive;
+            st.afterLast = calc;
+            st.calcPassive = calc;
+            if (hist[kMaxR + 1] > 0) atomicOr(&beam->errorFlags, 4);
+        } else {
+            int calc = st.maxFirstPassive;
+            if (calc < first + 1) calc = first + 1;
+            if (calc < 0) calc = first + 1;
+            if (calc > st.afterLast) calc = st.afterLast;
+            if (calc > g.steps) calc = g.steps;
+            st.calcPassive = calc;
+            if (st.afterLast > calc && st.afterLast > first) hist[0] -= (st.afterLast - max(calc, first)) * tiles;
+        }
         for (int i = 0; i < kBuckets; ++i) st.hist[i] = hist[i];
         if (hist[kMaxR + 1] > 0) {
             hist[kMaxR] += hist[kMaxR + 1];
@@ -269,6 +341,11 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     }
     __syncthreads();
     if (lc == 0) {
+        if (nuclear) {
+            // The halo transfer spans the same steps as the primary one.
+            beam->firstInside = first;
+            beam->maxCalcPassive = primaryBeam->maxCalcPassive;
+        }
         int acc = 0;
         long long fma = 0;
         int mp = beam->maxCalcPassive;
@@ -320,31 +397,101 @@ __global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, cons
     }
 }
 
+// Halo cells start empty: IDD 0 and rSigmaEff +inf (wrapper.cu:4124-4135).
+__global__ void nuc_fill_kernel(float* __restrict__ idd, float* __restrict__ rs, size_t n) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        idd[i] = 0.0f;
+        rs[i] = __int_as_float(0x7f800000);
+    }
+}
+
+// One warp per (layer, step, halo tile) over [first, calcPassive) of the layer:
+// the tile's radius bucket and liveness (tileRadCalc, complete_superposition.cu:
+// 198-255, on the halo grid), its code, and its count in the halo histogram.
+__global__ void nuc_codes_kernel(BeamGeomDev gn, int layer0, int nLayers, const float* __restrict__ idd,
+                                 const float* __restrict__ rs, const LayerStateDev* __restrict__ primaryLs,
+                                 const BeamStateDev* __restrict__ primaryBeam, LayerStateDev* __restrict__ nucLs,
+                                 uint8_t* __restrict__ codes) {
+    const int lane = threadIdx.x & 31;
+    const int tiles = gn.tilesX * gn.tilesY;
+    const int first = primaryBeam->firstInside;
+    const size_t plane = static_cast<size_t>(gn.pitchX) * gn.pitchY;
+    const size_t perLayer = static_cast<size_t>(gn.steps) * tiles;
+    const size_t total = perLayer * nLayers;
+    const size_t warps = (size_t(gridDim.x) * blockDim.x) >> 5;
+    for (size_t i = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5; i < total; i += warps) {
+        const int lc = int(i / perLayer);
+        const int rem = int(i - size_t(lc) * perLayer);
+        const int zr = rem / tiles, tile = rem - zr * tiles;
+        if (zr >= primaryLs[layer0 + lc].calcPassive - first) continue;
+        const int tx = tile % gn.tilesX, ty = tile / gn.tilesX;
+        const float* ti = idd + (lc * static_cast<size_t>(gn.steps) + zr) * plane + size_t(ty * kTileY) * gn.pitchX +
+                          tx * kTileX + lane;
+        const float* tr = rs + (ti - idd);
+        unsigned key = 0xffffffffu;
+        bool live = false;
+#pragma unroll
+        for (int r = 0; r < kTileY; ++r) {
+            key = min(key, float_order_key(tr[size_t(r) * gn.pitchX]));
+            live |= ti[size_t(r) * gn.pitchX] > 0.0f;
+        }
+        key = __reduce_min_sync(0xffffffffu, key);
+        live = __any_sync(0xffffffffu, live);
+        if (lane == 0) {
+            const int R = tile_radius_bucket(float_from_order_key(key));
+            codes[i] = static_cast<uint8_t>(R | (live ? 0x80 : 0));
+            atomicAdd(&nucLs[layer0 + lc].histAll[R], 1);
+            if (live) atomicAdd(&nucLs[layer0 + lc].liveHist[R], 1);
+        }
+    }
+}
+
 }  // namespace
 
 size_t idd_smem_bytes(const BeamGeomDev& g, const LutsDev& luts) {
-    return (static_cast<size_t>(luts.nS) + luts.nRrl + 2 * static_cast<size_t>(g.steps)) * sizeof(float) +
+    const size_t rows = static_cast<size_t>(luts.nS) * (g.nucOn ? 3 : 1);
+    return (rows + luts.nRrl + 2 * static_cast<size_t>(g.steps)) * sizeof(float) +
            static_cast<size_t>(g.steps) * 8 * (sizeof(float) + sizeof(int));
+}
+
+cudaError_t launch_nuc_prepare(const BeamGeomDev& gn, int nLayers, float* idd, float* rsigma, cudaStream_t s) {
+    const size_t n = static_cast<size_t>(nLayers) * gn.steps * gn.pitchX * gn.pitchY;
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    nuc_fill_kernel<<<blocks, 256, 0, s>>>(idd, rsigma, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nuc_codes(const BeamGeomDev& gn, int layer0, int nLayers, const float* idd, const float* rsigma,
+                             const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, LayerStateDev* nucLs,
+                             uint8_t* codes, cudaStream_t s) {
+    const size_t warps = static_cast<size_t>(nLayers) * gn.steps * gn.tilesX * gn.tilesY;
+    const int blocks = int(std::min<size_t>((warps + 7) / 8, 148 * 16));
+    nuc_codes_kernel<<<blocks, 256, 0, s>>>(gn, layer0, nLayers, idd, rsigma, primaryLs, primaryBeam, nucLs, codes);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, int nLayers, const float* density,
                        const float* wepl, const int* firstInside, const int* firstOutside, const float* rayW,
                        const LayerParamsDev* lp, LayerStateDev* ls, const BeamStateDev* beam, float* idd,
-                       float* rsigma, uint8_t* codes, int* firstPassive, cudaStream_t s) {
+                       float* rsigma, uint8_t* codes, int* firstPassive, const int* rayToNuc, const float* lattice,
+                       float* nucIdd, float* nucRsigma, cudaStream_t s) {
     dim3 grid(g.tilesX, g.tilesY, nLayers);
     dim3 block(32, 8);
     const size_t smem = idd_smem_bytes(g, luts);
-    cudaError_t e = cudaFuncSetAttribute(idd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    auto k = g.nucOn ? idd_kernel<true> : idd_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    idd_kernel<<<grid, block, smem, s>>>(g, luts, layer0, density, wepl, firstInside, firstOutside, rayW, lp, ls, beam,
-                                         idd, rsigma, codes, firstPassive);
+    k<<<grid, block, smem, s>>>(g, luts, layer0, density, wepl, firstInside, firstOutside, rayW, lp, ls, beam, idd,
+                                rsigma, codes, firstPassive, rayToNuc, lattice, nucIdd, nucRsigma);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
-                            BeamStateDev* beam, int4* work, int workCapacity, cudaStream_t s) {
+                            BeamStateDev* beam, int4* work, int workCapacity, const LayerStateDev* primaryLs,
+                            const BeamStateDev* primaryBeam, cudaStream_t s) {
     if (nLayers > kMaxChunkLayers) return cudaErrorInvalidValue;
-    layer_plan_kernel<<<1, kMaxChunkLayers, 0, s>>>(g, layer0, nLayers, ls, beam, workCapacity);
+    layer_plan_kernel<<<1, kMaxChunkLayers, 0, s>>>(g, layer0, nLayers, ls, beam, workCapacity, primaryLs,
+                                                    primaryBeam);
     const size_t total = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY * nLayers;
     const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 8));
     work_scatter_kernel<<<blocks, 256, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work, workCapacity);

@@ -40,14 +40,27 @@ cudaError_t launch_conv_cpb(const BeamGeomDev& g, const float* subspots, int max
 size_t idd_smem_bytes(const BeamGeomDev& g, const LutsDev& luts);
 // fillIddAndSigmaKernel (src/algorithms/idd_sigma.cu:46-259) fused with the
 // per-tile radius reduction of tileRadCalc (complete_superposition.cu:198-255).
+// With g.nucOn it also writes the nuclear halo IDD and sigma of the rays under a
+// halo lattice cell (rayToNuc: [rays] -> cell or -1) into [layer][step][nucY][nucX].
 cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, int nLayers, const float* density,
                        const float* wepl, const int* firstInside, const int* firstOutside, const float* rayW,
                        const LayerParamsDev* lp, LayerStateDev* ls, const BeamStateDev* beam, float* idd,
-                       float* rsigma, uint8_t* codes, int* firstPassive, cudaStream_t s);
+                       float* rsigma, uint8_t* codes, int* firstPassive, const int* rayToNuc, const float* lattice,
+                       float* nucIdd, float* nucRsigma, cudaStream_t s);
 // Histogram, overflow merge and batching (complete_superposition.cu:358-490) plus
-// the radius-sorted work list of live tiles.
+// the radius-sorted work list of live tiles. With primaryLs/primaryBeam set it
+// plans the nuclear halo grid `g` instead (no merge: a radius above 32 sets error
+// flag 4).
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
-                            BeamStateDev* beam, int4* work, int workCapacity, cudaStream_t s);
+                            BeamStateDev* beam, int4* work, int workCapacity, const LayerStateDev* primaryLs,
+                            const BeamStateDev* primaryBeam, cudaStream_t s);
+// Nuclear halo: clear the chunk's halo IDD (0) and sigma (+inf) before the IDD
+// kernel, and the halo tile codes and histograms after the primary layer plan.
+// `gn` is the halo grid (pitch = nucX x nucY).
+cudaError_t launch_nuc_prepare(const BeamGeomDev& gn, int nLayers, float* idd, float* rsigma, cudaStream_t s);
+cudaError_t launch_nuc_codes(const BeamGeomDev& gn, int layer0, int nLayers, const float* idd, const float* rsigma,
+                             const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, LayerStateDev* nucLs,
+                             uint8_t* codes, cudaStream_t s);
 // kernelSuperposition<R> (complete_superposition.cu:264-335) over the work list,
 // summing all layers into one BEV dose: two persistent launches (radii 16..32,
 // then 0..15) sized for `numSMs` multiprocessors.

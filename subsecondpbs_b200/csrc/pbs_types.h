@@ -61,7 +61,7 @@ struct BeamStateDev {
     int transferMax[3];
     TransferParams transfer;
     int transferValid;
-    int errorFlags;
+    int errorFlags;         // 1 work list overflow, 2 radius outside a kernel instance, 4 nuclear radius > 32
 };
 
 // Everything a kernel needs to know about the beam geometry.
@@ -84,6 +84,18 @@ struct BeamGeomDev {
     int bevX, bevY;          // pitch + 64
     int doseX, doseY, doseZ;
     int compatBevZShift;
+    // Transport model (idd_sigma.cu:102-121): Highland reference energy, sigma
+    // offset and distal-dip suppression; the GAUSS_FIT nuclear model also narrows
+    // the entry sigma of the convolution (wrapper.cu:3788-3795).
+    float eRefSq;
+    float sigmaDelta;
+    int suppressDistalDip;
+    float entrySigmaScale;
+    // Nuclear halo: lattice padded to 32 x 8 and the device word that collects the
+    // beams' error flags until the host reads them.
+    int nucOn;
+    int nucX, nucY;
+    int* errWord;
 };
 
 // Lookup tables resident on the device.
@@ -99,6 +111,8 @@ struct LutsDev {
     const float* rrl;
     int nRrl;
     float rrlScale;
+    const float* nucWeight;  // [nE][nS] nuclear weight, or null
+    const float* nucSqSigma; // [nE][nS] nuclear sigma^2 (mm^2), or null
 };
 
 }  // namespace pbs

@@ -232,8 +232,8 @@ __global__ void beam_planner_kernel(BeamGeomDev g, float* __restrict__ weplMin,
             const float a = fdiv(0.00270f, fsub(p.convPeakDepth, 4.50f));
             const float b = fdiv(-4.39f, fsub(p.convPeakDepth, 3.86f));
             const float base = fadd(fmul(fmul(a, z), z), fmul(b, z));
-            st.entrySigmaX = fsqrt(fmaxf(0.0f, fadd(base, fmul(p.sigmaXmm, p.sigmaXmm))));
-            st.entrySigmaY = fsqrt(fmaxf(0.0f, fadd(base, fmul(p.sigmaYmm, p.sigmaYmm))));
+            st.entrySigmaX = fmul(fsqrt(fmaxf(0.0f, fadd(base, fmul(p.sigmaXmm, p.sigmaXmm)))), g.entrySigmaScale);
+            st.entrySigmaY = fmul(fsqrt(fmaxf(0.0f, fadd(base, fmul(p.sigmaYmm, p.sigmaYmm)))), g.entrySigmaScale);
         }
         // IDD entry variance (wrapper.cu:4309-4313).
         {

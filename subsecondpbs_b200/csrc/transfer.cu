@@ -44,6 +44,9 @@ __device__ __forceinline__ float bev_sample(const float* __restrict__ v, int nx,
 // the deepest superposed step of all layers.
 __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // Last kernel of the beam's work list with one thread: hand the beam's error
+    // flags to the context's error word, which outlives the beam state.
+    if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
     const int first = beam->firstInside;
     const int passive = beam->maxCalcPassive;
     const float xs[2] = {-float(kMaxR), float(g.pitchX + kMaxR - 1)};

@@ -89,7 +89,8 @@ class DoseEngine:
     on the device between calls). Wraps the pbs_context_* C ABI."""
 
     def __init__(self, gpu_id: int = 0, compat_bev_z_shift: bool = False, stage_timing: bool = False,
-                 keep_debug: bool = False, layer_budget_mib: int | None = None, ct_input_type: int | None = None):
+                 keep_debug: bool = False, layer_budget_mib: int | None = None, ct_input_type: int | None = None,
+                 nuclear_model: int | None = None):
         self._lib = _lib.load()
         h = C.c_void_p()
         _lib.check(self._lib.pbs_context_create(int(gpu_id), C.byref(h)))
@@ -102,6 +103,8 @@ class DoseEngine:
             self.set_option(_lib.PBS_OPT_LAYER_BUDGET_MIB, int(layer_budget_mib))
         if ct_input_type is not None:
             self.set_option(_lib.PBS_OPT_CT_INPUT_TYPE, int(ct_input_type))
+        if nuclear_model is not None:
+            self.set_option(_lib.PBS_OPT_NUCLEAR_MODEL, int(nuclear_model))
         self.dose_dims = None
 
     def close(self) -> None:

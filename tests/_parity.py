@@ -37,19 +37,72 @@ def gamma_pass_rate(dose, ref, spacing_mm, dd=0.01, dta_mm=1.0, thr=0.1):
     return float((best[mask] <= 1.0).mean())
 
 
-def run_gpu(case, beams=None, compat=False, keep_debug=True, initial=None, ct_input_type=None):
+def run_gpu(case, beams=None, compat=False, keep_debug=True, initial=None, ct_input_type=None, nuclear_model=None):
+    """Run the CUDA library on `case`; `nuclear_model` (0/1/2) adds the nuclear halo."""
     from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
 
-    eng = DoseEngine(0, keep_debug=keep_debug, compat_bev_z_shift=compat, ct_input_type=ct_input_type)
+    eng = DoseEngine(0, keep_debug=keep_debug, compat_bev_z_shift=compat, ct_input_type=ct_input_type,
+                     nuclear_model=nuclear_model)
     eng.set_energy(case["energy"])
     eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
     eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
     if initial is not None:
         eng.reset_dose(np.asarray(initial, np.float32))
     for b in beams or [case["beam"]]:
-        eng.add_beam(b)
+        eng.add_beam(b, nuclear_correction=nuclear_model is not None)
     eng.synchronize()
     return eng
+
+
+def nuclear_report(eng, cap) -> dict:
+    """Differences of the nuclear halo stages between the library and the oracle."""
+    pl = cap["plan"]
+    S, NX, NY = pl["steps"], pl["nuc_x"], pl["nuc_y"]
+    st = eng.beam_stats()
+    rep = {"nuc_dims": list(st["nuc_dims"]), "nuc_dims_oracle": [NX, NY],
+           "fma_gpu": st["nuc_superpose_fma"], "fma_oracle": cap["nuc_superpose_fma"]}
+    r2n = eng.debug(L.PBS_DBG_RAY_TO_NUC, 0, (pl["ray_y"], pl["ray_x"]), np.int32)
+    rep["ray_to_nuc_mismatch"] = int((r2n != cap["ray_to_nuc"]).sum())
+    layers = []
+    for l in range(pl["num_layers"]):
+        ls = eng.layer_stats(l)
+        lay = {"hist_equal": list(ls["nuc_tile_rad_counts"]) == [int(v) for v in cap["nuc_hist"][l]],
+               "batched_equal": list(ls["nuc_batched_counts"]) == [int(v) for v in cap["nuc_batched"][l]]}
+        if "nuc_idd" in cap:
+            idd = eng.debug(L.PBS_DBG_NUC_IDD, l, (S, NY, NX))
+            rs = eng.debug(L.PBS_DBG_NUC_RSIGMA, l, (S, NY, NX))
+            codes = eng.debug(L.PBS_DBG_NUC_TILE_BINS, l, (S, NY // 8, NX // 32), np.uint8)
+            oidd, ors, oc = cap["nuc_idd"][l], cap["nuc_rsigma"][l], cap["nuc_codes"][l]
+            lay["idd_rel"] = float(np.abs(idd - oidd).max() / max(oidd.max(), 1e-300))
+            fin = np.isfinite(rs) & np.isfinite(ors)
+            rel = np.abs(rs[fin] - ors[fin]) / np.maximum(ors[fin], 1e-30) if fin.any() else np.zeros(1)
+            lay["rsigma_rel_q999"] = float(np.quantile(rel, 0.999))
+            lay["rsigma_inf_mismatch"] = int((np.isfinite(rs) != np.isfinite(ors)).sum())
+            lay["code_mismatch"] = int(((codes != oc) & (oc != 255)).sum())
+        layers.append(lay)
+    rep["layers"] = layers
+    bev = eng.debug(L.PBS_DBG_NUC_BEV_DOSE, 0, (S, pl["nuc_bev_y"], pl["nuc_bev_x"]))
+    ob = cap["nuc_bev"]
+    bmax = max(float(ob.max()), 1e-300)
+    diff = np.abs(bev - ob) / bmax
+    rep["bev_rel"] = float(diff.max())
+    rep["bev_rel_q999"] = float(np.quantile(diff[ob > 1e-3 * bmax], 0.999)) if (ob > 1e-3 * bmax).any() else 0.0
+    return rep
+
+
+def assert_nuclear_parity(rep):
+    assert rep["nuc_dims"] == rep["nuc_dims_oracle"]
+    assert rep["ray_to_nuc_mismatch"] == 0
+    assert rep["fma_gpu"] == rep["fma_oracle"], (rep["fma_gpu"], rep["fma_oracle"])
+    for lay in rep["layers"]:
+        assert lay["hist_equal"] and lay["batched_equal"], lay
+        if "idd_rel" in lay:
+            assert lay["code_mismatch"] == 0, lay
+            assert lay["rsigma_inf_mismatch"] == 0, lay
+            assert lay["idd_rel"] < 1e-3, lay
+            assert lay["rsigma_rel_q999"] < 2e-3, lay
+    assert rep["bev_rel_q999"] < 1e-4, rep["bev_rel_q999"]
+    assert rep["bev_rel"] < DOSE_TOL_FRAC_DMAX, rep["bev_rel"]
 
 
 def stage_report(eng, cap) -> dict:
