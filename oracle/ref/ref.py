@@ -56,7 +56,20 @@ class _CaptureStdout:
 
 
 _BATCH = re.compile(r"Primary superposition batched launches:((?: \[rad=\d+:\d+\])*)")
+_NUC_BATCH = re.compile(r"Nuclear superposition batched launches:((?: \[rad=\d+:\d+\])*)")
 _ITEM = re.compile(r"\[rad=(\d+):(\d+)\]")
+
+
+def parse_batched(text: str, nuclear: bool = False) -> list:
+    """Per-layer batched radius counts (33 ints) the reference printed with verbose=1
+    (complete_superposition.cu:486-495 primary, 660-669 nuclear halo)."""
+    rows = []
+    for m in (_NUC_BATCH if nuclear else _BATCH).finditer(text):
+        row = [0] * 33
+        for r, n in _ITEM.findall(m.group(1)):
+            row[int(r)] = int(n)
+        rows.append(row)
+    return rows
 
 
 def run(case: dict, beams=None, nuclear: bool = False, verbose: int = 1, path: Path = REF_LIB):
@@ -85,11 +98,5 @@ def run(case: dict, beams=None, nuclear: bool = False, verbose: int = 1, path: P
                                        len(descs), C.byref(ed), 0, int(nuclear), int(verbose))
     if rc != 0:
         raise RuntimeError(f"reference returned {rc}:\n{cap.text[-2000:]}")
-    batched = []
-    for m in _BATCH.finditer(cap.text):
-        row = [0] * 33
-        for r, n in _ITEM.findall(m.group(1)):
-            row[int(r)] = int(n)
-        batched.append(row)
     del keep, ke
-    return dose, batched, cap.text
+    return dose, parse_batched(cap.text), cap.text

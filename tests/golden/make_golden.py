@@ -33,6 +33,10 @@ CASES = {
                                             "e_range": [80.0, 120.0]}, {"rotate": 30.0}),
     "hetero_legacy": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 2, "target_radius_mm": 12.0,
                                              "e_range": [90.0, 110.0]}, {"legacy": True}),
+    # Nuclear halo (reference built with NUCLEAR_CORR=GAUSS_FIT, oracle/_ref/librtd_nuc.so),
+    # synthetic halo tables on the proton axes (subsecondpbs_b200.tables.synthetic_nuclear_tables).
+    "halo_small": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                          "e_range": [80.0, 120.0]}, {"nuclear": "GAUSS_FIT"}),
 }
 
 
@@ -40,6 +44,11 @@ def build_case(name: str):
     builder, kw, tf = CASES[name]
     kw = {k: (tuple(v) if isinstance(v, list) else v) for k, v in kw.items()}
     case = getattr(phantoms, builder)(**kw)
+    if tf and "nuclear" in tf:
+        from subsecondpbs_b200 import tables
+
+        case = dict(case)
+        case["energy"] = tables.synthetic_nuclear_tables(case["energy"])
     beam = case["beam"]
     if tf and "rotate" in tf:
         beam = phantoms.rotate_beam(beam, tf["rotate"])
@@ -59,13 +68,19 @@ def main(argv=None) -> int:
     out.mkdir(parents=True, exist_ok=True)
     for name in a.cases:
         case, beam = build_case(name)
-        dose, batched, text = ref.run(case, beams=[beam], verbose=1)
         builder, kw, tf = CASES[name]
+        nuclear = bool(tf and "nuclear" in tf)
+        lib = ref.REF_LIB.parent / "librtd_nuc.so" if nuclear else ref.REF_LIB
+        dose, batched, text = ref.run(case, beams=[beam], nuclear=nuclear, verbose=1, path=lib)
+        build = f"NUCLEAR_CORR={tf['nuclear']}" if nuclear else "NUCLEAR_CORR=OFF"
         meta = {"case": name, "builder": builder, "kwargs": kw, "transform": tf,
-                "reference": "Nelgcis/subsecondPBS subsecondWrapper built by oracle/ref/build_ref.sh (NUCLEAR_CORR=OFF)",
+                "reference": f"Nelgcis/subsecondPBS subsecondWrapper built by oracle/ref/build_ref.sh ({build})",
                 "dose_max": float(dose.max()), "dose_sum": float(dose.sum())}
+        extra = {}
+        if nuclear:
+            extra["nuc_batched"] = np.asarray(ref.parse_batched(text, nuclear=True), np.int32).reshape(-1, 33)
         np.savez_compressed(out / f"{name}.npz", dose=dose.astype(np.float32),
-                            batched=np.asarray(batched, np.int32).reshape(-1, 33), meta=json.dumps(meta))
+                            batched=np.asarray(batched, np.int32).reshape(-1, 33), meta=json.dumps(meta), **extra)
         (out / f"{name}.log").write_text(text[-20000:])
         print(name, dose.shape, float(dose.max()), len(batched), flush=True)
     return 0

@@ -9,7 +9,9 @@ weights) with -use_fast_math; the oracle uses exact weights in double precision.
 Tolerances per case are the pinned agreement: max |dose - reference| over voxels
 above 10 % of Dmax, the 1 %/1 mm gamma pass rate, and the batched radius lists
 the reference prints (complete_superposition.cu:476-495), which must be identical
-up to single tiles that sit on a bucket boundary."""
+up to single tiles that sit on a bucket boundary. The nuclear-halo case was made by
+the reference built with NUCLEAR_CORR=GAUSS_FIT; its halo batched lists
+(complete_superposition.cu:660-669) are pinned the same way."""
 import json
 from pathlib import Path
 
@@ -29,7 +31,14 @@ PINS = {
     "hetero_small": (5e-3, 0.999, 1),
     "hetero_legacy": (2e-2, 0.999, 0),
     "hetero_rot30": (5e-2, 0.998, 0),
+    "halo_small": (5e-3, 0.999, 1),
 }
+
+
+def nuclear_model_of(meta):
+    """GAUSS_FIT (2) for the cases the reference ran with its nuclear halo, else None."""
+    tf = meta.get("transform") or {}
+    return {"SOUKUP": 0, "FLUKA": 1, "GAUSS_FIT": 2}[tf["nuclear"]] if "nuclear" in tf else None
 
 
 def load_case(name):
@@ -48,7 +57,9 @@ def load_case(name):
 def test_oracle_matches_reference_outputs(name):
     z, meta, case, beam = load_case(name)
     tol, gmin, flips = PINS[name]
-    r = O.dose(case, beams=[beam], compat_bev_z_shift=True, capture=True)
+    nuc = nuclear_model_of(meta)
+    r = O.dose(case, beams=[beam], compat_bev_z_shift=True, capture=True,
+               nuclear_model=-1 if nuc is None else nuc)
     ref = z["dose"].astype(np.float64)
     assert abs(float(ref.max()) - meta["dose_max"]) <= 1e-6 * meta["dose_max"]
     err = max_rel_err(r["dose"], ref)
@@ -60,6 +71,19 @@ def test_oracle_matches_reference_outputs(name):
     assert ob.shape[0] == rb.shape[0]
     moved = int(np.abs(ob - rb).sum()) // 2
     assert moved <= flips, (ob.tolist(), rb.tolist())
+    if nuc is not None:
+        on, rn = r["capture"]["nuc_batched"], z["nuc_batched"]
+        assert on.shape == rn.shape
+        assert int(np.abs(on - rn).sum()) // 2 <= flips, (on.tolist(), rn.tolist())
+
+
+def test_halo_is_what_the_reference_adds():
+    """The halo case differs from the same beam without the halo by far more than
+    its pinned tolerance: the halo branch itself is pinned."""
+    z, meta, case, beam = load_case("halo_small")
+    ref = z["dose"].astype(np.float64)
+    d = O.dose(case, beams=[beam], compat_bev_z_shift=True)["dose"]
+    assert max_rel_err(d, ref) > 0.05
 
 
 def test_bev_shift_is_what_the_reference_does():

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from _parity import gamma_pass_rate, max_rel_err, run_gpu
-from test_cpu_golden import PINS, load_case
+from test_cpu_golden import PINS, load_case, nuclear_model_of
 
 pytestmark = pytest.mark.gpu
 
@@ -14,12 +14,17 @@ pytestmark = pytest.mark.gpu
 def test_cuda_matches_reference_outputs(name):
     z, meta, case, beam = load_case(name)
     tol, gmin, flips = PINS[name]
-    eng = run_gpu(case, beams=[beam], compat=True, keep_debug=False)
+    nuc = nuclear_model_of(meta)
+    eng = run_gpu(case, beams=[beam], compat=True, keep_debug=False, nuclear_model=nuc)
     dose = eng.read_dose()
     ref = z["dose"].astype(np.float64)
     assert max_rel_err(dose, ref) < tol
     assert gamma_pass_rate(dose, ref, case["dose_resolution"]) >= gmin
-    moved = 0
+    moved = nuc_moved = 0
     for l in range(z["batched"].shape[0]):
-        moved += int(np.abs(np.asarray(eng.layer_stats(l)["batched_counts"]) - z["batched"][l]).sum()) // 2
+        ls = eng.layer_stats(l)
+        moved += int(np.abs(np.asarray(ls["batched_counts"]) - z["batched"][l]).sum()) // 2
+        if nuc is not None:
+            nuc_moved += int(np.abs(np.asarray(ls["nuc_batched_counts"]) - z["nuc_batched"][l]).sum()) // 2
     assert moved <= flips
+    assert nuc_moved <= flips
