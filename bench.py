@@ -148,7 +148,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    from subsecondpbs_b200 import _lib, phantoms
+    from subsecondpbs_b200 import _lib, phantoms, sharding
     from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine, fp32_peak_tflops
 
     world, rank, local = _dist()
@@ -161,7 +161,13 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     case = phantoms.heterogeneous_case()
-    beam = case["beam"] if world == 1 else phantoms.rotate_beam(case["beam"], 90.0 + 180.0 * (rank % 2))
+    # N > 1: a plan of one beam per rank (opposed gantry angles), divided by the
+    # sharding module's assignment; each rank computes its beam and the FP64 grids
+    # are reduced on rank 0.
+    plan = [case["beam"] if world == 1 else phantoms.rotate_beam(case["beam"], 90.0 + 180.0 * (k % 2))
+            for k in range(world)]
+    mine = sharding.assign_beams([sharding.beam_cost(b) for b in plan], world)[rank]
+    beam = plan[mine[0]]
     dims = case["dose_dims"]
     n_vox = int(np.prod(dims))
 
@@ -186,7 +192,7 @@ def run_ours(args):
         if d64 is not None:
             eng.read_dose64(d64)
             with torch.cuda.stream(stream):
-                dist.reduce(d64, dst=0)
+                sharding.reduce_dose(d64, dst=0)
 
     for _ in range(args.warmup):
         step()
