@@ -670,11 +670,11 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     }
     if ((rc = mark(7))) return rc;
     lastChunks = (L + chunk - 1) / chunk;
-    // trace, planner, two fluence kernels, five per chunk (IDD, layer plan, work
-    // scatter, two superposition ranges), transfer planner, transfer; the halo adds
-    // six per chunk (clear, codes, layer plan, scatter, two superposition ranges)
-    // and its transfer planner and transfer.
-    lastLaunches = 6 + 5 * lastChunks + (nuclear ? 6 * lastChunks + 2 : 0);
+    // trace, planner, two fluence kernels, six per chunk (IDD, layer plan, work
+    // scatter, three superposition ranges), transfer planner, transfer; the halo
+    // adds seven per chunk (clear, codes, layer plan, scatter, three superposition
+    // ranges) and its transfer planner and transfer.
+    lastLaunches = 6 + 6 * lastChunks + (nuclear ? 7 * lastChunks + 2 : 0);
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;

@@ -349,9 +349,10 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         int acc = 0;
         long long fma = 0;
         int mp = beam->maxCalcPassive;
-        int split = 0;
+        int split = 0, split2 = 0;
         for (int r = kMaxR; r >= 0; --r) {
             if (r == kSplitR) split = acc;
+            if (r == kSplitR2) split2 = acc;
             for (int q = 0; q < nLayers; ++q) {
                 LayerStateDev& st = ls[layer0 + q];
                 st.offR[r] = acc;
@@ -369,6 +370,8 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         beam->workNext = 0;
         beam->workSplit = min(split, acc);
         beam->workNextSmall = 0;
+        beam->workSplit2 = min(split2, acc);
+        beam->workNextTiny = 0;
         beam->liveTiles += acc;
         beam->superposeFma += fma;
     }

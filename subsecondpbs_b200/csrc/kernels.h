@@ -62,8 +62,8 @@ cudaError_t launch_nuc_codes(const BeamGeomDev& gn, int layer0, int nLayers, con
                              const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, LayerStateDev* nucLs,
                              uint8_t* codes, cudaStream_t s);
 // kernelSuperposition<R> (complete_superposition.cu:264-335) over the work list,
-// summing all layers into one BEV dose: two persistent launches (radii 16..32,
-// then 0..15) sized for `numSMs` multiprocessors.
+// summing all layers into one BEV dose: three persistent launches (radii 16..32,
+// 8..15, 0..7) sized for `numSMs` multiprocessors.
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                              BeamStateDev* beam, float* bev, int numSMs, cudaStream_t s);
 

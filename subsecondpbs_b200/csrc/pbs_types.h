@@ -52,9 +52,14 @@ struct BeamStateDev {
     float pxSpMultX, pxSpMultY;
     int maxCalcPassive;
     int workCount;          // superposition work items of the current layer chunk
-    int workNext;           // next unclaimed item of radius > 15 (dynamic scheduling)
-    int workSplit;          // items of radius > 15 (they lead the radius-sorted list)
-    int workNextSmall;      // next unclaimed item of radius <= 15, relative to workSplit
+    // The radius-sorted work list holds the wide (R > kSplitR), medium
+    // (kSplitR2 < R <= kSplitR) and narrow (R <= kSplitR2) items in that order;
+    // each range has its own claim counter (relative to the range start).
+    int workNext;
+    int workSplit;          // items with R > kSplitR
+    int workNextSmall;
+    int workSplit2;         // items with R > kSplitR2
+    int workNextTiny;
     long long liveTiles;
     long long superposeFma;
     int transferStart[3];

@@ -20,8 +20,9 @@
 //     depositing source are skipped;
 //   * the tile footprint is then added to the BEV dose of its step (all layers of
 //     the beam share one BEV volume).
-// Radii up to 15 and radii 16..32 run as two instances of the kernel: the small
-// one needs a third of the registers and shared memory and runs three CTAs per SM.
+// Radii 16..32, 8..15 and 0..7 run as three instances of the kernel with 128, 48
+// and 32 registers and 96, 43 and 21 KB of shared memory: 2, 5 and 8 CTAs per SM
+// (the narrower instances trade a few spilled registers for occupancy).
 #include "kernels.h"
 
 namespace pbs {
@@ -45,6 +46,18 @@ struct Shape {
 // source columns 4, 8 or 16 apart (read together by the lane groups of one
 // instruction) land in different banks.
 __device__ __forceinline__ int e4_col(int sx) { return sx ^ ((sx >> 3) & 3); }
+
+// erf(x), x >= 0, from Abramowitz & Stegun 7.1.26 (Hastings' rational
+// approximation, |error| <= 1.5e-7): 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e^{-x^2}
+// with t = 1 / (1 + p x). The caller supplies e^{-x^2}.
+__device__ __forceinline__ float erf_hastings(float x, float expNegX2) {
+    constexpr float p = 0.3275911f;
+    constexpr float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+                    a5 = 1.061405429f;
+    const float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
+    const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, a5, a4), a3), a2), a1);
+    return fmaf(-poly, expNegX2, 1.0f);
+}
 
 struct TileArgs {
     const float* idd;
@@ -78,12 +91,20 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         if (lane == 0) sMask[warp] = mask;
         float e[4 * Q];
         if (live) {
+            // erf at (k + 1/2) r, k = 0..R; e^{-((k+1/2) r)^2} follows the recurrence
+            // E_{k+1} = E_k G_k, G_k = e^{-2 (k+1) r^2} = G_{k-1} e^{-2 r^2}.
             const float rs = a.rsig[a.src];
-            float fPrev = erff(rs * 0.5f);
+            const float r2 = rs * rs;
+            const float step2 = __expf(-2.0f * r2);
+            float E = __expf(-0.25f * r2);
+            float G = step2;
+            float fPrev = erf_hastings(rs * 0.5f, E);
             e[0] = fPrev;
 #pragma unroll
             for (int k = 1; k <= R; ++k) {
-                const float f = erff(rs * (float(k) + 0.5f));
+                E *= G;
+                G *= step2;
+                const float f = erf_hastings(rs * (float(k) + 0.5f), E);
                 e[k] = 0.5f * (f - fPrev);
                 fPrev = f;
             }
@@ -160,9 +181,10 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                         }
                     }
                 }
-                // Keeps the next source's loads from being hoisted over this one's
-                // FMAs (which would hold every row of the column in registers).
-                asm volatile("" ::: "memory");
+                // Lets the loads of the next source overlap this pair's FMAs but keeps
+                // later sources' loads from being hoisted (which would hold every row
+                // of the column in registers).
+                if (sy & 1) asm volatile("" ::: "memory");
             }
             if (colLive) {
                 float* col = out + sx + R + d;
@@ -199,7 +221,7 @@ __device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, fl
 template <int RLo, int RHi, int MinBlocks>
 __global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
-                 const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev, int small) {
+                 const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev, int range) {
     extern __shared__ __align__(16) float sm[];
     float4* E4 = reinterpret_cast<float4*>(sm);                                  // [Q][256] e_s(4q..4q+3), slot sy*32+e4_col(sx)
     float* EW = sm + Shape<RHi>::kQ * kThreads * 4;                              // [256][EWS] idd_s e_s(k)
@@ -208,10 +230,10 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
     __shared__ unsigned sMask[kTileY];
 
     const int t = threadIdx.x;
-    const int split = beam->workSplit;
-    const int begin = small ? split : 0;
-    const int end = small ? beam->workCount : split;
-    int* counter = small ? &beam->workNextSmall : &beam->workNext;
+    // Range 0: R > kSplitR, 1: kSplitR2 < R <= kSplitR, 2: R <= kSplitR2.
+    const int begin = range == 0 ? 0 : (range == 1 ? beam->workSplit : beam->workSplit2);
+    const int end = range == 0 ? beam->workSplit : (range == 1 ? beam->workSplit2 : beam->workCount);
+    int* counter = range == 0 ? &beam->workNext : (range == 1 ? &beam->workNextSmall : &beam->workNextTiny);
     const size_t padPlane = static_cast<size_t>(g.pitchX) * g.pitchY;
     const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
     const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
@@ -247,12 +269,12 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
 
 template <int RLo, int RHi, int MinBlocks>
 cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                         BeamStateDev* beam, float* bev, int gridBlocks, int small, cudaStream_t s) {
+                         BeamStateDev* beam, float* bev, int gridBlocks, int range, cudaStream_t s) {
     auto k = superpose_kernel<RLo, RHi, MinBlocks>;
     const size_t smem = Shape<RHi>::kSmemBytes;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, small);
+    k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, range);
     return cudaGetLastError();
 }
 
@@ -263,7 +285,9 @@ cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float
     // Items are sorted by descending radius: the wide radii come first.
     cudaError_t e = launch_range<kSplitR + 1, kMaxR, 2>(g, idd, rsigma, work, beam, bev, numSMs * 2, 0, s);
     if (e != cudaSuccess) return e;
-    return launch_range<0, kSplitR, 3>(g, idd, rsigma, work, beam, bev, numSMs * 3, 1, s);
+    e = launch_range<kSplitR2 + 1, kSplitR, 5>(g, idd, rsigma, work, beam, bev, numSMs * 5, 1, s);
+    if (e != cudaSuccess) return e;
+    return launch_range<0, kSplitR2, 8>(g, idd, rsigma, work, beam, bev, numSMs * 8, 2, s);
 }
 
 }  // namespace pbs
