@@ -249,7 +249,10 @@ PBS_API int pbs_context_set_ct(PbsContext* ctx, const float* ct, int ct_on_devic
 /* Define the dose grid; allocates the FP64 accumulator. */
 PBS_API int pbs_context_set_dose_grid(PbsContext* ctx, const int dims[3], const float resolution[3],
                               const float corner[3]);
-/* Reset the accumulator to `initial` (float [Z][Y][X], host or device) or to 0. */
+/* Reset the accumulator to `initial` (float [Z][Y][X], host or device) or to 0.
+ * A host `initial` is copied on a side stream that overlaps the next beam's
+ * kernels; from pinned memory the copy is asynchronous, so the buffer must stay
+ * unchanged until the next add_beam, read or synchronize call has returned. */
 PBS_API int pbs_context_reset_dose(PbsContext* ctx, const float* initial, int initial_on_device);
 /* Plan the beam on the host and enqueue its whole pipeline on the context stream.
  * Returns without waiting for the device. */

@@ -222,6 +222,7 @@ int pbs_measure_fp32_peak(int gpu_id, double* tflops) {
 int pbs_context_synchronize(PbsContext* ctx) {
     if (int rc = guard(ctx)) return rc;
     cudaSetDevice(ctx->impl.device);
+    if (int rc = ctx->impl.flush_dose_init()) return rc;
     cudaError_t e = cudaStreamSynchronize(ctx->impl.stream);
     if (e != cudaSuccess) {
         pbs::set_error(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));

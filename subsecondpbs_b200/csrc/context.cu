@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -89,7 +90,11 @@ Context::~Context() {
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord})
         b->release();
     staging.release();
+    if (copyStream) cudaStreamSynchronize(copyStream);
     if (stagingEvent) cudaEventDestroy(stagingEvent);
+    if (copyStart) cudaEventDestroy(copyStart);
+    if (doseCopied) cudaEventDestroy(doseCopied);
+    if (copyStream) cudaStreamDestroy(copyStream);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -105,6 +110,9 @@ int Context::init(int gpu) {
     }
     PBS_CUDA(cudaSetDevice(gpu), "cudaSetDevice");
     PBS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    PBS_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
+    PBS_CUDA(cudaEventCreateWithFlags(&copyStart, cudaEventDisableTiming), "cudaEventCreate");
+    PBS_CUDA(cudaEventCreateWithFlags(&doseCopied, cudaEventDisableTiming), "cudaEventCreate");
     PBS_CUDA(cudaEventCreateWithFlags(&stagingEvent, cudaEventDisableTiming), "cudaEventCreate");
     for (auto& e : ev) PBS_CUDA(cudaEventCreate(&e), "cudaEventCreate");
     // Callers of the reference-shaped entry points cannot pass options: the
@@ -166,6 +174,29 @@ int Context::set_energy(const PbsEnergyDesc& e) {
         set_error("[RTD_ENTRY_ASSERT] density, stopping-power, and radiation-length LUTs are inconsistent");
         return PBS_ERR_INVALID_ARGUMENT;
     }
+    // The tables stay resident: a call with the same tables as the resident ones
+    // (the common case of repeated wrapper calls) uploads nothing.
+    auto same = [](const std::vector<float>& v, const float* p, size_t n) {
+        return v.size() == n && (n == 0 || std::memcmp(v.data(), p, n * sizeof(float)) == 0);
+    };
+    {
+        const size_t nTab = size_t(e.n_energies) * size_t(e.n_energy_samples);
+        const bool nucGiven = e.nuc_weight_matrix && e.nuc_sq_sigma_matrix && e.n_nuc_weight_matrix == nTab &&
+                              e.n_nuc_sq_sigma_matrix == nTab;
+        if (hasEnergy && energy.n_energies == e.n_energies && energy.n_energy_samples == e.n_energy_samples &&
+            energy.n_density_samples == e.n_density_samples && energy.n_sp_samples == e.n_sp_samples &&
+            energy.n_rrl_samples == e.n_rrl_samples && energy.density_scale_fact == e.density_scale_fact &&
+            energy.sp_scale_fact == e.sp_scale_fact && energy.rrl_scale_fact == e.rrl_scale_fact &&
+            same(energiesPerU, e.energies_per_u, e.n_energies) && same(peakDepths, e.peak_depths, e.n_energies) &&
+            same(scaleFacts, e.scale_facts, e.n_energies) && same(ciddHost, e.cidd_matrix, e.n_cidd_matrix) &&
+            same(densityHost, e.density_vector, e.n_density_vector) && same(spHost, e.sp_vector, e.n_sp_vector) &&
+            same(rrlHost, e.rrl_vector, e.n_rrl_vector) &&
+            (nucGiven ? same(nucWeightHost, e.nuc_weight_matrix, nTab) &&
+                            same(nucSqSigmaHost, e.nuc_sq_sigma_matrix, nTab) &&
+                            nucTablesAligned == (e.nuclear_tables_aligned_to_primary_axis != 0)
+                      : nucWeightHost.empty()))
+            return PBS_OK;
+    }
     energiesPerU.assign(e.energies_per_u, e.energies_per_u + e.n_energies);
     peakDepths.assign(e.peak_depths, e.peak_depths + e.n_energies);
     scaleFacts.assign(e.scale_facts, e.scale_facts + e.n_energies);
@@ -207,8 +238,9 @@ int Context::set_energy(const PbsEnergyDesc& e) {
     PBS_CUDA(cudaMemcpyAsync(density.ptr, densityHost.data(), densityHost.size() * 4, cudaMemcpyHostToDevice, stream),
              "LUT");
     PBS_CUDA(cudaMemcpyAsync(sp.ptr, spHost.data(), spHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
+    // The tables are copied from pageable host vectors, which cudaMemcpyAsync
+    // stages before it returns; no wait is needed before they are replaced.
     PBS_CUDA(cudaMemcpyAsync(rrl.ptr, rrlHost.data(), rrlHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
-    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     luts.cidd = static_cast<const float*>(cidd.ptr);
     luts.nS = e.n_energy_samples;
     luts.nE = e.n_energies;
@@ -225,6 +257,80 @@ int Context::set_energy(const PbsEnergyDesc& e) {
     luts.nucSqSigma = hasNuc ? static_cast<const float*>(nucSqSigma.ptr) : nullptr;
     hasEnergy = true;
     return PBS_OK;
+}
+
+namespace {
+// Copy of the voxel box [lo, hi] between two [Z][Y][X] float volumes of `dims`.
+cudaError_t copy_box(void* dst, const void* src, const int dims[3], const int lo[3], const int hi[3],
+                     cudaMemcpyKind kind, cudaStream_t s) {
+    cudaMemcpy3DParms p = {};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(src), size_t(dims[0]) * 4, size_t(dims[0]), size_t(dims[1]));
+    p.dstPtr = make_cudaPitchedPtr(dst, size_t(dims[0]) * 4, size_t(dims[0]), size_t(dims[1]));
+    p.srcPos = make_cudaPos(size_t(lo[0]) * 4, size_t(lo[1]), size_t(lo[2]));
+    p.dstPos = p.srcPos;
+    p.extent = make_cudaExtent(size_t(hi[0] - lo[0] + 1) * 4, size_t(hi[1] - lo[1] + 1), size_t(hi[2] - lo[2] + 1));
+    p.kind = kind;
+    return cudaMemcpy3DAsync(&p, s);
+}
+
+bool box_empty(const int lo[3], const int hi[3]) { return hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2]; }
+}  // namespace
+
+int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3], const int hi[3]) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!data || g.dims[0] <= 0 || g.dims[1] <= 0 || g.dims[2] <= 0 ||
+        !(g.res[0] > 0.0f && g.res[1] > 0.0f && g.res[2] > 0.0f)) {
+        set_error("[RTD_ENTRY_ASSERT] CT grid must have positive dims and resolution");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
+    int rc = ct.ensure(n * 4);
+    if (rc) return rc;
+    if (!box_empty(lo, hi)) PBS_CUDA(copy_box(ct.ptr, data, g.dims, lo, hi, cudaMemcpyHostToDevice, stream), "CT H2D");
+    // The CT type comes from the whole volume, as with a full upload.
+    int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
+    if (type == PBS_CT_AUTO) {
+        float mn, mx;
+        sample_ct_stats(data, n, mn, mx);
+        type = auto_detect_ct_type(mn, mx);
+    }
+    return convert_ct(type, g);
+}
+
+int Context::reset_dose_region(const float* init, const int lo[3], const int hi[3]) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    int rc = floatOut.ensure(n * 4);
+    if (rc) return rc;
+    if (box_empty(lo, hi)) return reset_dose(nullptr, 0);
+    // Voxels outside the box are initialised from stale values; no beam of the
+    // call writes them and read_dose_region does not copy them back.
+    PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
+    PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
+    PBS_CUDA(copy_box(floatOut.ptr, init, doseGrid.dims, lo, hi, cudaMemcpyHostToDevice, copyStream), "dose H2D");
+    PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
+    pendingDoseInit = true;
+    return PBS_OK;
+}
+
+int Context::read_dose_region(float* out, const int lo[3], const int hi[3]) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    int rc = flush_dose_init();
+    if (rc) return rc;
+    if ((rc = floatOut.ensure(n * 4))) return rc;
+    if (!box_empty(lo, hi)) {
+        PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), static_cast<float*>(floatOut.ptr), n,
+                                      stream),
+                 "dose_to_float");
+        PBS_CUDA(copy_box(out, floatOut.ptr, doseGrid.dims, lo, hi, cudaMemcpyDeviceToHost, stream), "dose D2H");
+    }
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    return take_device_errors();
 }
 
 int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
@@ -250,13 +356,20 @@ int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
             type = auto_detect_ct_type(mm[0], mm[1]);
         }
     } else {
+        // The copy goes first: the CT type is sampled on the host while it runs.
+        PBS_CUDA(cudaMemcpyAsync(ct.ptr, data, n * 4, cudaMemcpyHostToDevice, stream), "CT H2D");
         if (type == PBS_CT_AUTO) {
             float mn, mx;
             sample_ct_stats(data, n, mn, mx);
             type = auto_detect_ct_type(mn, mx);
         }
-        PBS_CUDA(cudaMemcpyAsync(ct.ptr, data, n * 4, cudaMemcpyHostToDevice, stream), "CT H2D");
     }
+    return convert_ct(type, g);
+}
+
+// CT adapter on the device (wrapper.cu:2290-2441): to HU+1000 in place.
+int Context::convert_ct(int type, const GridDesc& g) {
+    const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
     if (type == PBS_CT_DENSITY || type == PBS_CT_SPR) {
         if (!hasEnergy) {
             set_error("[CT_ADAPTER] density/SPR CT needs the lookup tables; call set_energy first");
@@ -303,18 +416,30 @@ int Context::reset_dose(const float* init, int onDevice) {
         return PBS_ERR_NOT_READY;
     }
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
-    const float* src = nullptr;
-    if (init) {
-        if (onDevice) {
-            src = init;
-        } else {
-            int rc = floatOut.ensure(n * 4);
-            if (rc) return rc;
-            PBS_CUDA(cudaMemcpyAsync(floatOut.ptr, init, n * 4, cudaMemcpyHostToDevice, stream), "dose H2D");
-            src = static_cast<const float*>(floatOut.ptr);
-        }
+    if (init && !onDevice) {
+        // The copy waits for the work already on the context stream (the CT upload
+        // among it, which the next beam needs first) and then overlaps that beam.
+        int rc = floatOut.ensure(n * 4);
+        if (rc) return rc;
+        PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
+        PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
+        PBS_CUDA(cudaMemcpyAsync(floatOut.ptr, init, n * 4, cudaMemcpyHostToDevice, copyStream), "dose H2D");
+        PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
+        pendingDoseInit = true;
+        return PBS_OK;
     }
-    PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), src, n, stream), "dose_init");
+    pendingDoseInit = false;
+    PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), init, n, stream), "dose_init");
+    return PBS_OK;
+}
+
+int Context::flush_dose_init() {
+    if (!pendingDoseInit) return PBS_OK;
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    PBS_CUDA(cudaStreamWaitEvent(stream, doseCopied, 0), "cudaStreamWaitEvent");
+    PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), static_cast<const float*>(floatOut.ptr), n, stream),
+             "dose_init");
+    pendingDoseInit = false;
     return PBS_OK;
 }
 
@@ -325,6 +450,8 @@ int Context::read_dose(float* out, int onDevice) {
         return PBS_ERR_NOT_READY;
     }
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    int frc = flush_dose_init();
+    if (frc) return frc;
     if (onDevice) {
         PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), out, n, stream), "dose_to_float");
         return PBS_OK;
@@ -345,6 +472,8 @@ int Context::read_dose64(double* out, int onDevice) {
         return PBS_ERR_NOT_READY;
     }
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    int frc = flush_dose_init();
+    if (frc) return frc;
     PBS_CUDA(cudaMemcpyAsync(out, dose64.ptr, n * 8, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                              stream),
              "dose64 copy");
@@ -621,8 +750,7 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
                  "conv_cpb");
     }
     if ((rc = mark(3))) return rc;
-    int smCount = 148;
-    cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
+    if (smCount <= 0) PBS_CUDA(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device), "SM count");
     const int workCap = int(size_t(chunk) * S * tiles);
     const int nucWorkCap = int(size_t(chunk) * S * nucTiles);
     float* dNucIdd = static_cast<float*>(nucIddBuf.ptr);
@@ -660,6 +788,7 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
                      "nuc_superpose");
     }
     if ((rc = mark(6))) return rc;
+    if ((rc = flush_dose_init())) return rc;
     PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
     if (nuclear) {
@@ -848,6 +977,9 @@ int Context::debug_copy(int which, int layer, void* out, size_t bytes) {
         case PBS_DBG_FIRST_PASSIVE: return copy(static_cast<char*>(firstPassive.ptr) + size_t(layer) * rays * 4, rays * 4);
         case PBS_DBG_DOSE64: {
             const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+            int frc = flush_dose_init();
+            if (frc) return frc;
+            PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
             return copy(dose64.ptr, n * 8);
         }
         case PBS_DBG_BEV_DOSE: {
@@ -956,6 +1088,69 @@ int Context::debug_copy(int which, int layer, void* out, size_t bytes) {
 namespace {
 std::mutex g_cacheMutex;
 std::map<int, Context*> g_cache;
+
+void merge_box(int lo[3], int hi[3], const int a[3], const int b[3]) {
+    if (b[0] < a[0] || b[1] < a[1] || b[2] < a[2]) return;
+    for (int i = 0; i < 3; ++i) {
+        lo[i] = std::min(lo[i], a[i]);
+        hi[i] = std::max(hi[i], b[i]);
+    }
+}
+
+// CT voxels the tracer of a beam can read: the sample points are multilinear in
+// (ray x, ray y, step), so the corner rays at the first and last step bound them;
+// two voxels of margin cover the trilinear footprint and the rounding of the
+// repeated step additions (trace_kernel).
+void ct_trace_box(const BeamPlan& P, const int dims[3], int lo[3], int hi[3]) {
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    const int xs[2] = {0, P.rayDims[0] - 1}, ys[2] = {0, P.rayDims[1] - 1};
+    const float ks[2] = {0.0f, float(P.tracerSteps - 1)};
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            const V3 st = tracer_start(P.tracer, xs[a], ys[b]);
+            const V3 inc = tracer_inc(P.tracer, xs[a], ys[b]);
+            for (int c = 0; c < 2; ++c) {
+                const float q[3] = {st.x + 0.5f + ks[c] * inc.x, st.y + 0.5f + ks[c] * inc.y,
+                                    st.z + 0.5f + ks[c] * inc.z};
+                for (int i = 0; i < 3; ++i) {
+                    mn[i] = std::min(mn[i], q[i]);
+                    mx[i] = std::max(mx[i], q[i]);
+                }
+            }
+        }
+    for (int i = 0; i < 3; ++i) {
+        lo[i] = std::max(int(std::floor(std::max(mn[i], -1e9f))) - 2, 0);
+        hi[i] = std::min(int(std::floor(std::min(mx[i], 1e9f))) + 2, dims[i] - 1);
+    }
+}
+
+// Dose voxels a beam's transfer can write (transfer_planner_kernel and the block
+// rounding of transfer_kernel), over all steps so that it bounds every layer.
+void dose_transfer_box(const FromFan& f, int pitchX, int pitchY, int steps, const int dims[3], int lo[3],
+                       int hi[3]) {
+    const float xs[2] = {-float(kMaxR), float(pitchX + kMaxR - 1)};
+    const float ys[2] = {-float(kMaxR), float(pitchY + kMaxR - 1)};
+    const float zs[2] = {0.0f, float(steps - 1)};
+    V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
+    for (int zi = 0; zi < 2; ++zi)
+        for (int yi = 0; yi < 2; ++yi)
+            for (int xi = 0; xi < 2; ++xi) {
+                const V3 p = apply(f, v3(xs[xi], ys[yi], zs[zi]));
+                mx.x = std::max(mx.x, p.x);
+                mx.y = std::max(mx.y, p.y);
+                mx.z = std::max(mx.z, p.z);
+                mn.x = std::min(mn.x, p.x);
+                mn.y = std::min(mn.y, p.y);
+                mn.z = std::min(mn.z, p.z);
+            }
+    lo[0] = std::max((int(std::floor(mn.x)) / 32) * 32, 0);
+    lo[1] = std::max(int(std::floor(mn.y)), 0);
+    lo[2] = std::max(int(std::floor(mn.z)), 0);
+    // The transfer rounds its x and y spans up to whole 32 x 8 blocks.
+    hi[0] = std::min(int(std::ceil(mx.x)) + 32, dims[0] - 1);
+    hi[1] = std::min(int(std::ceil(mx.y)) + 8, dims[1] - 1);
+    hi[2] = std::min(int(std::ceil(mx.z)), dims[2] - 1);
+}
 }  // namespace
 
 int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
@@ -995,9 +1190,36 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
     }
     int rc;
     if ((rc = ctx->set_energy(*energyData))) return rc;
-    if ((rc = ctx->set_ct(ctData, 0, cg))) return rc;
+    // Every beam is planned up front (add_beam plans it again; it is cheap): the CT
+    // voxels their tracers can sample and the dose voxels their transfers can write
+    // bound the host copies of this call.
+    int ctLo[3] = {INT_MAX, INT_MAX, INT_MAX}, ctHi[3] = {-1, -1, -1};
+    int dLo[3] = {INT_MAX, INT_MAX, INT_MAX}, dHi[3] = {-1, -1, -1};
+    for (size_t i = 0; i < numBeams; ++i) {
+        BeamPlan P;
+        std::string perr;
+        if ((rc = plan_beam(beams[i], ctx->energy, cg, dg, P, perr))) {
+            set_error(perr);
+            return rc;
+        }
+        int lo[3], hi[3];
+        ct_trace_box(P, cg.dims, lo, hi);
+        merge_box(ctLo, ctHi, lo, hi);
+        dose_transfer_box(P.rayIdxToDoseIdx, P.superpDims[0], P.superpDims[1], P.tracerSteps, dg.dims, lo, hi);
+        merge_box(dLo, dHi, lo, hi);
+        if (nuclear && P.hasLattice) {
+            FromFan nf = P.rayIdxToDoseIdx;
+            nf.fanIdxToFan = idxxf(v3(P.lattice.dx, P.lattice.dy, P.fanDelta.z),
+                                   v3(P.lattice.ox, P.lattice.oy, P.fanCorner.z));
+            const int nx = (P.lattice.nx + kTileX - 1) / kTileX * kTileX;
+            const int ny = (P.lattice.ny + kTileY - 1) / kTileY * kTileY;
+            dose_transfer_box(nf, nx, ny, P.tracerSteps, dg.dims, lo, hi);
+            merge_box(dLo, dHi, lo, hi);
+        }
+    }
+    if ((rc = ctx->set_ct_region(ctData, cg, ctLo, ctHi))) return rc;
     if ((rc = ctx->set_dose_grid(dg))) return rc;
-    if ((rc = ctx->reset_dose(doseData, 0))) return rc;
+    if ((rc = ctx->reset_dose_region(doseData, dLo, dHi))) return rc;
     for (size_t i = 0; i < numBeams; ++i) {
         if ((rc = ctx->add_beam(beams[i], nuclear))) return rc;
         if (verbose > 0) {
@@ -1009,7 +1231,7 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
                              st.guaranteed_passive, st.live_tiles);
         }
     }
-    return ctx->read_dose(doseData, 0);
+    return ctx->read_dose_region(doseData, dLo, dHi);
 }
 
 }  // namespace pbs

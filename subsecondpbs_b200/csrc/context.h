@@ -33,6 +33,12 @@ struct PinnedBuf {
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // Host -> device copies of an initial dose run on their own stream so that they
+    // overlap the beam's kernels; the FP64 grid is initialised from them just
+    // before the first kernel that needs it (flush_dose_init).
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t copyStart = nullptr, doseCopied = nullptr;
+    bool pendingDoseInit = false;
 
     // Options.
     int compatBevZShift = 0;
@@ -41,6 +47,7 @@ struct Context {
     int ctInputType = PBS_CT_AUTO;
     long long layerBudgetMiB = 2048;
     int nuclearModel = 2;  // GAUSS_FIT
+    int smCount = 0;       // multiprocessors of the device, read on first use
 
     // Lookup tables.
     bool hasEnergy = false;
@@ -88,7 +95,17 @@ struct Context {
     // Reads (and clears) the error flags the kernels raised since the last check;
     // the stream must be synchronised. PBS_OK when none.
     int take_device_errors();
+    // Enqueues the deferred initialisation of the FP64 grid from a host dose.
+    int flush_dose_init();
     int set_ct(const float* data, int onDevice, const GridDesc& g);
+    // Wrapper path, where every beam is known before any upload: host copies limited
+    // to boxes [lo, hi] (inclusive voxel indices) of the CT and of the dose grid.
+    // The rest of the device CT is not read by those beams; the rest of the dose
+    // grid is not written by them, so the caller's buffer keeps its values there.
+    int set_ct_region(const float* data, const GridDesc& g, const int lo[3], const int hi[3]);
+    int reset_dose_region(const float* init, const int lo[3], const int hi[3]);
+    int read_dose_region(float* out, const int lo[3], const int hi[3]);
+    int convert_ct(int type, const GridDesc& g);
     int set_dose_grid(const GridDesc& g);
     int reset_dose(const float* init, int onDevice);
     int read_dose(float* out, int onDevice);

@@ -8,6 +8,7 @@
 
 #include "device_util.cuh"
 #include "kernels.h"
+#include "launch_util.h"
 
 namespace pbs {
 
@@ -482,7 +483,7 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
     dim3 block(32, 8);
     const size_t smem = idd_smem_bytes(g, luts);
     auto k = g.nucOn ? idd_kernel<true> : idd_kernel<false>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<grid, block, smem, s>>>(g, luts, layer0, density, wepl, firstInside, firstOutside, rayW, lp, ls, beam, idd,
                                 rsigma, codes, firstPassive, rayToNuc, lattice, nucIdd, nucRsigma);

@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <string>
+#include <thread>
+#include <vector>
 
 namespace pbs {
 
@@ -359,10 +361,31 @@ void sample_ct_stats(const float* data, size_t n, float& mn, float& mx) {
     if (!data || n == 0) return;
     const size_t maxSamples = 100000;
     const size_t stride = (n > maxSamples) ? (n / maxSamples) : 1;
-    mn = mx = data[0];
-    for (size_t i = 0; i < n; i += stride) {
-        mn = std::min(mn, data[i]);
-        mx = std::max(mx, data[i]);
+    const size_t samples = (n + stride - 1) / stride;
+    // The samples are cache lines apart and memory bound: four threads split them
+    // (minimum and maximum do not depend on the order).
+    const int threads = samples < 4096 ? 1 : 4;
+    float lo[4], hi[4];
+    auto part = [&](int t) {
+        const size_t a = samples * t / threads, b = samples * (t + 1) / threads;
+        float l = data[0], h = data[0];
+        for (size_t k = a; k < b; ++k) {
+            const float v = data[k * stride];
+            l = std::min(l, v);
+            h = std::max(h, v);
+        }
+        lo[t] = l;
+        hi[t] = h;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(part, t);
+    part(0);
+    for (auto& th : pool) th.join();
+    mn = lo[0];
+    mx = hi[0];
+    for (int t = 1; t < threads; ++t) {
+        mn = std::min(mn, lo[t]);
+        mx = std::max(mx, hi[t]);
     }
 }
 

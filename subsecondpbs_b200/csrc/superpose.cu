@@ -24,6 +24,7 @@
 // and 32 registers and 96, 43 and 21 KB of shared memory: 2, 5 and 8 CTAs per SM
 // (the narrower instances trade a few spilled registers for occupancy).
 #include "kernels.h"
+#include "launch_util.h"
 
 namespace pbs {
 
@@ -272,7 +273,7 @@ cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rs
                          BeamStateDev* beam, float* bev, int gridBlocks, int range, cudaStream_t s) {
     auto k = superpose_kernel<RLo, RHi, MinBlocks>;
     const size_t smem = Shape<RHi>::kSmemBytes;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, range);
     return cudaGetLastError();

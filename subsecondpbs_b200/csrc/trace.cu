@@ -6,6 +6,7 @@
 
 #include "device_util.cuh"
 #include "kernels.h"
+#include "launch_util.h"
 #include "../../include/subsecondpbs.h"
 
 namespace pbs {
@@ -347,7 +348,7 @@ cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float*
     const size_t cache = static_cast<size_t>(kTraceSegments) * seg * 32 * sizeof(float);
     unsigned* mins = reinterpret_cast<unsigned*>(weplMin);
     if (cache <= kTraceCacheMaxBytes) {
-        e = cudaFuncSetAttribute(trace_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(cache));
+        e = set_smem_limit(reinterpret_cast<const void*>(trace_kernel<true>), cache);
         if (e != cudaSuccess) return e;
         trace_kernel<true><<<grid, block, cache, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside,
                                                       firstOutside, mins, beam);

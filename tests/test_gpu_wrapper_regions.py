@@ -1,0 +1,66 @@
+"""pbs_subsecond_wrapper copies only the CT voxels its beams trace and the dose
+voxels they write. Its result must equal the resident-context path, and the
+caller's dose must keep its values where the beams add nothing."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from subsecondpbs_b200 import _lib as L
+from subsecondpbs_b200 import phantoms, tables
+from subsecondpbs_b200.cudaCalDoseRTD import _with_luts
+from _parity import run_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _wrapper(case, beams, initial, nuclear=False):
+    lib = L.load()
+    descs, keep = [], []
+    for b in beams:
+        d, k = L.beam_desc(b)
+        descs.append(d)
+        keep.append(k)
+    arr = (L.PbsBeamDesc * len(descs))(*descs)
+    ed, ke = L.energy_desc(_with_luts(case["energy"], None))
+    ct = np.ascontiguousarray(case["ct"], dtype=np.float32)
+    dose = np.ascontiguousarray(initial, dtype=np.float32).copy()
+    fp = C.POINTER(C.c_float)
+    L.check(lib.pbs_subsecond_wrapper(ct.ctypes.data_as(fp), L.int3(case["ct_dims"]), L.float3(case["ct_resolution"]),
+                                      L.float3(case["ct_corner"]), dose.ctypes.data_as(fp), L.int3(case["dose_dims"]),
+                                      L.float3(case["dose_resolution"]), L.float3(case["dose_corner"]), arr,
+                                      len(descs), C.byref(ed), 0, int(nuclear), 0))
+    del keep, ke
+    return dose
+
+
+def _same(got, want, initial):
+    # Float atomics make repeated runs differ in the last bits inside the dose.
+    m = float(np.abs(want - initial).max())
+    assert m > 0
+    assert float(np.abs(got - want).max()) <= 1e-6 * m, float(np.abs(got - want).max()) / m
+    # Where the beams add nothing the caller's values come back exactly, and the
+    # beams reach only part of the grid.
+    idle = want == initial
+    assert np.array_equal(got[idle], initial[idle])
+    assert idle.mean() > 0.05
+
+
+@pytest.mark.parametrize("angles", [(90.0,), (30.0, 200.0)])
+def test_wrapper_regions_equal_the_context_path(hetero_small_case, angles):
+    case = hetero_small_case
+    beams = [phantoms.rotate_beam(case["beam"], a) for a in angles]
+    rng = np.random.default_rng(7)
+    initial = rng.uniform(0.0, 1e-9, size=case["ct"].shape).astype(np.float32)
+    got = _wrapper(case, beams, initial)
+    want = run_gpu(case, beams=beams, keep_debug=False, initial=initial).read_dose()
+    _same(got, want, initial)
+
+
+def test_wrapper_regions_with_the_halo(hetero_small_case):
+    case = dict(hetero_small_case)
+    case["energy"] = tables.synthetic_nuclear_tables(hetero_small_case["energy"])
+    initial = np.zeros(case["ct"].shape, np.float32)
+    got = _wrapper(case, [case["beam"]], initial, nuclear=True)
+    want = run_gpu(case, keep_debug=False, nuclear_model=L.NUCLEAR_GAUSS_FIT).read_dose()
+    _same(got, want, initial)
