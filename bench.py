@@ -45,6 +45,7 @@ def _args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the spot-weight adjoint timing")
     return ap.parse_args()
 
 
@@ -104,12 +105,13 @@ def _cpu_oracle_ms(case, budget_s=12.0, max_runs=20):
 
     threads = os.cpu_count() or 1
     times = []
+    dose = None
     t_end = time.perf_counter() + budget_s
     while len(times) < max_runs and (not times or time.perf_counter() < t_end):
         t = time.perf_counter()
-        O.dose(case, threads=threads)
+        dose = O.dose(case, threads=threads)["dose"]
         times.append((time.perf_counter() - t) * 1e3)
-    return statistics.median(times), threads, len(times)
+    return statistics.median(times), threads, len(times), dose
 
 
 def run_reference(args):
@@ -140,6 +142,74 @@ def run_reference(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _adjoint_cost(local: int, reps: int = 5) -> dict:
+    """Inverse-planning gradient: the forward dose of four ~8000-spot beams on the
+    64x64x128 water phantom and the FP64 least-squares objective (2 Gy in a 5 cm
+    sphere, 0 Gy in a 2 cm shell), against the spot-weight adjoint of the same
+    plan (all four beams), both synchronised wall-clock medians on one GPU."""
+    import torch
+
+    from subsecondpbs_b200 import phantoms
+    from subsecondpbs_b200.autograd import with_weights
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    case = phantoms.inverse_planning_case()
+    dev = torch.device("cuda", local)
+    eng = DoseEngine(local)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    dd = case["dose_dims"]
+    dose = torch.empty((dd[2], dd[1], dd[0]), dtype=torch.float64, device=dev)
+    tt = torch.from_numpy(case["target"]).to(dev)
+    ts = torch.from_numpy(case["shell"]).to(dev)
+    p = case["prescription"]
+    beams = [eng.prepare_beam(b) for b in case["beams"]]
+
+    def forward():
+        eng.reset_dose()
+        for b in beams:
+            eng.add_beam(b)
+        eng.read_dose64(dose)
+        eng.synchronize()
+        return dose
+
+    d = forward()
+    s = p / float(d[tt].mean())
+    beams = [eng.prepare_beam(with_weights(b, b["spot_weights"] * s)) for b in case["beams"]]
+    n_spots = [int(np.sum(b["layer_spot_counts"])) for b in case["beams"]]
+
+    def objective():
+        d = forward()
+        g = torch.zeros_like(d)
+        g[tt] = 2.0 * (d[tt] - p)
+        g[ts] = 2.0 * d[ts]
+        j = float(((d[tt] - p) ** 2).sum() + (d[ts] ** 2).sum())
+        torch.cuda.synchronize(dev)
+        return j, g
+
+    def adjoint(g):
+        return [eng.adjoint_beam(b, g, n) for b, n in zip(beams, n_spots)]
+
+    for _ in range(2):
+        _, g = objective()
+        adjoint(g)
+    tf, ta = [], []
+    for _ in range(reps):
+        t = time.perf_counter()
+        j, g = objective()
+        tf.append((time.perf_counter() - t) * 1e3)
+        t = time.perf_counter()
+        adjoint(g)
+        ta.append((time.perf_counter() - t) * 1e3)
+    fwd, adj = statistics.median(tf), statistics.median(ta)
+    return {"workload": "water 64x64x128 at 2 mm, 4 beams (gantry 0/90/180/270) x 36 layers x 225 spots",
+            "spots": int(sum(n_spots)), "objective": "FP64 least squares on the GPU", "objective_value": j,
+            "forward_ms": round(fwd, 3), "adjoint_ms": round(adj, 3), "adjoint_over_forward": round(adj / fwd, 3),
+            "timing": f"median of {reps} synchronised wall-clock runs; forward includes the FP64 readout and "
+                      "objective, adjoint includes the per-spot gradient readout"}
 
 
 def run_ours(args):
@@ -316,10 +386,19 @@ def run_ours(args):
 
     launches_per_step = int(stats["kernel_launches"]) + 2  # + dose reset and float readout
     cpu = None
+    precision = None
     if world == 1 and not args.no_cpu_baseline:
-        cms, threads, runs = _cpu_oracle_ms(case)
+        cms, threads, runs, ref_dose = _cpu_oracle_ms(case)
         cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "port",
                "sample": f"full workload (one 20-layer beam) x {runs} runs, OpenMP over rays and steps"}
+        # Error of the benchmarked result against the FP64 oracle on the same inputs.
+        from subsecondpbs_b200 import precision as prec
+
+        precision = dict(prec.report(out.cpu().numpy(), ref_dose, case["dose_resolution"]),
+                         reference="FP64 oracle, same inputs", arithmetic="FP32 rays/superposition, "
+                         "Kahan WEPL, FP64 dose accumulation")
+
+    adjoint = _adjoint_cost(local) if world == 1 and not args.no_adjoint else None
 
     line = {
         "metric": METRIC,
@@ -344,6 +423,8 @@ def run_ours(args):
         "roofline_stages": roof_stages,
         "stages_ms": stage_ms,
         "cpu_baseline": cpu,
+        "precision": precision,
+        "adjoint": adjoint,
         "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers"},
         "gpu_launches": launches_per_step * args.steps,

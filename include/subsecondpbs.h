@@ -257,6 +257,18 @@ PBS_API int pbs_context_reset_dose(PbsContext* ctx, const float* initial, int in
 /* Plan the beam on the host and enqueue its whole pipeline on the context stream.
  * Returns without waiting for the device. */
 PBS_API int pbs_context_add_beam(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction);
+/* Spot-weight adjoint of one beam (no counterpart in the reference; the inverse-
+ * planning gradient of the north-star additions). For a dose gradient G
+ * (double [Z][Y][X], host or device) it writes dJ/dw_s = <G, dD/dw_s> for every
+ * spot s of `beam` (n_weights floats, host, in the beam's spot order), at the
+ * beam's current weights: the transposes of the transfer, the tile superposition
+ * (with the forward's radii and weights), the IDD scaling and the spot -> ray
+ * convolution. Dose is linear in the weights except where a ray's total weight
+ * crosses the 1e-6 live threshold (idd_sigma.cu:78). Needs a raw spot lattice, no
+ * nuclear halo, and every layer in one chunk (PBS_ERR_UNSUPPORTED otherwise).
+ * The context's dose accumulator is not changed. Synchronous. */
+PBS_API int pbs_context_adjoint_beam(PbsContext* ctx, const PbsBeamDesc* beam, const double* grad_dose,
+                                     int grad_on_device, float* grad_weights, size_t n_weights);
 /* Convert the accumulator to float and copy it out (host or device pointer). */
 PBS_API int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device);
 /* Copy the FP64 accumulator [Z][Y][X] out (host or device pointer), e.g. for a

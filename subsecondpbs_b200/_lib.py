@@ -197,6 +197,7 @@ def load() -> C.CDLL:
         "pbs_context_set_dose_grid": (i, [vp, ip3, fp3, fp3]),
         "pbs_context_reset_dose": (i, [vp, vp, i]),
         "pbs_context_add_beam": (i, [vp, C.POINTER(PbsBeamDesc), i]),
+        "pbs_context_adjoint_beam": (i, [vp, C.POINTER(PbsBeamDesc), vp, i, fp, C.c_size_t]),
         "pbs_context_read_dose": (i, [vp, vp, i]),
         "pbs_context_read_dose64": (i, [vp, vp, i]),
         "pbs_measure_fp32_peak": (i, [i, C.POINTER(C.c_double)]),

@@ -1,0 +1,168 @@
+// Adjoint of the dose with respect to the beam's ray weights: the transposes of
+// the BEV -> dose transfer and of the tile superposition, followed by the IDD
+// scaling. Dose is linear in the spot weights: for a live ray
+//   idd[l][k][ray] = rayW[l][ray] * g[l][k][ray]      (idd_sigma.cu:194-201),
+//   BEV = S(idd)  (tile superposition, complete_superposition.cu:264-335),
+//   D  += T(BEV)  (divergent trilinear transfer, prim_transf_kernel.cu:11-44),
+// so for a dose gradient Gd the ray-weight gradient is
+//   rbar[l][ray] = sum_k g[l][k][ray] * (S^T T^T Gd)[l][k][ray]
+//               = (sum_k idd[l][k][ray] * (S^T T^T Gd)[l][k][ray]) / rayW[l][ray].
+// The tile radii, the live-ray mask and rSigmaEff do not depend on the weights'
+// values, so they come from the same IDD and binning kernels as the forward pass.
+#include "device_util.cuh"
+#include "kernels.h"
+#include "launch_util.h"
+
+namespace pbs {
+
+namespace {
+
+// T^T: every dose voxel of the transfer box spreads its gradient over the eight
+// BEV texels its forward sample interpolated (bev_sample in transfer.cu), with the
+// same weights. The forward adds a sample only where it is positive; a BEV sample
+// is a sum of non-negative terms, so it is zero only where every texel's
+// coefficient is zero and the linear transpose is exact.
+__global__ void __launch_bounds__(256)
+transfer_adjoint_kernel(BeamGeomDev g, const double* __restrict__ gradDose, const BeamStateDev* __restrict__ beam,
+                        float* __restrict__ gradBev) {
+    if (!beam->transferValid) return;
+    const int sx = beam->transferStart[0], sy = beam->transferStart[1], sz = beam->transferStart[2];
+    const int mx = beam->transferMax[0], my = beam->transferMax[1], mz = beam->transferMax[2];
+    const int spanX = ((mx - sx + 1 + 31) / 32) * 32, spanY = ((my - sy + 1 + 7) / 8) * 8;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x < sx || y < sy || x >= sx + spanX || y >= sy + spanY || x >= g.doseX || y >= g.doseY) return;
+    const int z0 = max(sz, int(blockIdx.z) * 8);
+    const int z1 = min(mz, int(blockIdx.z) * 8 + 7);
+    if (z0 > z1) return;
+    const TransferParams T = beam->transfer;
+    const V3 start = transfer_start(T, x, y);
+    const float zShift = g.compatBevZShift ? float(beam->firstInside) : 0.0f;
+    const size_t slice = static_cast<size_t>(g.doseX) * g.doseY;
+    const int nx = g.bevX, ny = g.bevY, nz = g.steps;
+    for (int z = z0; z <= z1; ++z) {
+        const V3 f = transfer_fan_idx(T, start, z);
+        if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
+        const float gd = float(gradDose[static_cast<size_t>(z) * slice + static_cast<size_t>(y) * g.doseX + x]);
+        if (gd == 0.0f) continue;
+        const float px = fminf(fmaxf(f.x, -2.0f), float(nx) + 1.0f);
+        const float py = fminf(fmaxf(f.y, -2.0f), float(ny) + 1.0f);
+        const float pz = fminf(fmaxf(f.z - zShift, -2.0f), float(nz) + 1.0f);
+        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+        const int x0 = int(fx), y0 = int(fy), z0i = int(fz);
+        const float tx = px - fx, ty = py - fy, tz = pz - fz;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int xi = x0 + (c & 1), yi = y0 + ((c >> 1) & 1), zi = z0i + (c >> 2);
+            if (xi < 0 || yi < 0 || zi < 0 || xi >= nx || yi >= ny || zi >= nz) continue;
+            const float w = ((c & 1) ? tx : 1.0f - tx) * (((c >> 1) & 1) ? ty : 1.0f - ty) * ((c >> 2) ? tz : 1.0f - tz);
+            atomicAdd(gradBev + (static_cast<size_t>(zi) * ny + yi) * nx + xi, w * gd);
+        }
+    }
+}
+
+constexpr int kAdjThreads = 256;
+constexpr int kAdjOutFloats = (kTileY + 2 * kMaxR) * (kTileX + 2 * kMaxR);
+
+// S^T for one tile at radius R: each source gathers the BEV gradient over its
+// footprint with the forward's weights e(|dy|) e(|dx|) and adds idd * that sum to
+// its ray's accumulator.
+constexpr int kAdjEStride = kMaxR + 1;  // 33: odd, the threads' rows fall in distinct banks
+
+template <int R>
+__device__ __forceinline__ void superpose_adjoint_tile(const float* __restrict__ tileG, float* __restrict__ eRow,
+                                                       float dose, float rs, float* __restrict__ rbarRay, int sy,
+                                                       int sx) {
+    constexpr int Wo = kTileX + 2 * R;
+    float e[R + 1];
+    superposition_row<R>(rs, e);
+#pragma unroll
+    for (int k = 0; k <= R; ++k) eRow[k] = e[k];
+    // Rows R-k and R+k share the weight e[k]; within a row the columns R-j and
+    // R+j share e[j] (kept in registers; the row weight comes from eRow).
+    auto row_sum = [&](int i) {
+        const float* row = tileG + (sy + i) * Wo + sx + R;
+        float v = e[0] * row[0];
+#pragma unroll
+        for (int j = 1; j <= R; ++j) v = fmaf(e[j], row[-j] + row[j], v);
+        return v;
+    };
+    float acc = e[0] * row_sum(R);
+#pragma unroll 1
+    for (int k = 1; k <= R; ++k) acc = fmaf(eRow[k], row_sum(R - k) + row_sum(R + k), acc);
+    atomicAdd(rbarRay, dose * acc);
+}
+
+template <int R, int RHi>
+__device__ __forceinline__ void adjoint_dispatch(int r, const float* tileG, float* eRow, float dose, float rs,
+                                                 float* rbarRay, int sy, int sx) {
+    if (r == R) {
+        superpose_adjoint_tile<R>(tileG, eRow, dose, rs, rbarRay, sy, sx);
+        return;
+    }
+    if constexpr (R < RHi) adjoint_dispatch<R + 1, RHi>(r, tileG, eRow, dose, rs, rbarRay, sy, sx);
+}
+
+// Persistent CTAs over the whole work list of the (single) layer chunk.
+__global__ void __launch_bounds__(kAdjThreads)
+superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
+                         const int4* __restrict__ work, BeamStateDev* __restrict__ beam, const float* __restrict__ gradBev,
+                         float* __restrict__ rbar) {
+    extern __shared__ float adjSm[];
+    float* tileG = adjSm;                        // [8+2R][32+2R] BEV gradient of the tile's footprint
+    float* eS = adjSm + kAdjOutFloats;           // [256][kAdjEStride] each source's weights
+    __shared__ int sItem;
+    const int t = threadIdx.x;
+    const int count = beam->workCount;
+    const size_t padPlane = static_cast<size_t>(g.pitchX) * g.pitchY;
+    const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
+    const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
+    const size_t rayPlane = static_cast<size_t>(g.rayX) * g.rayY;
+    for (;;) {
+        if (t == 0) sItem = atomicAdd(&beam->workNext, 1);
+        __syncthreads();
+        const int w = sItem;
+        if (w >= count) break;
+        const int4 it = work[w];
+        const int lc = it.x, tile = it.y, zRel = it.z, R = it.w;
+        const int tx = tile % g.tilesX, ty = tile / g.tilesX;
+        const int Ho = kTileY + 2 * R, Wo = kTileX + 2 * R;
+        const float* src = gradBev + static_cast<size_t>(zRel) * bevPlane +
+                           static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX + (tx * kTileX - R + kMaxR);
+        for (int i = t; i < Ho * Wo; i += kAdjThreads) {
+            const int oy = i / Wo, ox = i - oy * Wo;
+            tileG[i] = src[static_cast<size_t>(oy) * g.bevX + ox];
+        }
+        __syncthreads();
+        const int sy = t >> 5, sx = t & 31;
+        const int ry = ty * kTileY + sy, rx = tx * kTileX + sx;
+        const size_t s = lc * layerStride + zRel * padPlane + static_cast<size_t>(ry) * g.pitchX + rx;
+        const float dose = idd[s];
+        if (dose > 0.0f && ry < g.rayY && rx < g.rayX)
+            adjoint_dispatch<0, kMaxR>(R, tileG, eS + t * kAdjEStride, dose, rsig[s],
+                                       rbar + lc * rayPlane + static_cast<size_t>(ry) * g.rayX + rx, sy, sx);
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_transfer_adjoint(const BeamGeomDev& g, const double* gradDose, const BeamStateDev* beam,
+                                    float* gradBev, cudaStream_t s) {
+    dim3 block(32, 8);
+    dim3 grid((g.doseX + 31) / 32, (g.doseY + 7) / 8, (g.doseZ + 7) / 8);
+    transfer_adjoint_kernel<<<grid, block, 0, s>>>(g, gradDose, beam, gradBev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_superpose_adjoint(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                                     BeamStateDev* beam, const float* gradBev, float* rbar, int numSMs,
+                                     cudaStream_t s) {
+    const size_t smem = (size_t(kAdjOutFloats) + size_t(kAdjThreads) * kAdjEStride) * sizeof(float);
+    cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(superpose_adjoint_kernel), smem);
+    if (e != cudaSuccess) return e;
+    superpose_adjoint_kernel<<<numSMs * 3, kAdjThreads, smem, s>>>(g, idd, rsigma, work, beam, gradBev, rbar);
+    return cudaGetLastError();
+}
+
+}  // namespace pbs

@@ -202,6 +202,13 @@ int pbs_context_add_beam(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_c
     return ctx->impl.add_beam(*beam, nuclear_correction);
 }
 
+int pbs_context_adjoint_beam(PbsContext* ctx, const PbsBeamDesc* beam, const double* grad_dose, int grad_on_device,
+                             float* grad_weights, size_t n_weights) {
+    if (int rc = guard(ctx)) return rc;
+    if (!beam) return PBS_ERR_INVALID_ARGUMENT;
+    return ctx->impl.adjoint_beam(*beam, grad_dose, grad_on_device, grad_weights, n_weights);
+}
+
 int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device) {
     if (int rc = guard(ctx)) return rc;
     if (!out) return PBS_ERR_INVALID_ARGUMENT;

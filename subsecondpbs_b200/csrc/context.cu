@@ -87,7 +87,8 @@ Context::~Context() {
     for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
-                      &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord})
+                      &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad, &rbarBuf,
+                      &gradInterm, &gradLattice})
         b->release();
     staging.release();
     if (copyStream) cudaStreamSynchronize(copyStream);
@@ -484,7 +485,34 @@ int Context::read_dose64(double* out, int onDevice) {
     return PBS_OK;
 }
 
-int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
+int Context::add_beam(const PbsBeamDesc& b, int nuclear) { return run_beam(b, nuclear, nullptr); }
+
+int Context::adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int gradOnDevice, float* gradSpots,
+                          size_t nSpots) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    size_t total = 0;
+    for (size_t l = 0; l < b.n_layer_spot_counts && b.layer_spot_counts; ++l) total += size_t(b.layer_spot_counts[l]);
+    if (!gradDose || !gradSpots || nSpots != total) {
+        set_error("adjoint: the gradient output needs one float per spot of the beam");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    const double* dGrad = gradDose;
+    if (!gradOnDevice) {
+        int rc = gradDoseBuf.ensure(n * 8);
+        if (rc) return rc;
+        PBS_CUDA(cudaMemcpyAsync(gradDoseBuf.ptr, gradDose, n * 8, cudaMemcpyHostToDevice, stream), "grad H2D");
+        dGrad = static_cast<const double*>(gradDoseBuf.ptr);
+    }
+    AdjointArgs a{dGrad, gradSpots, nSpots};
+    return run_beam(b, 0, &a);
+}
+
+int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
     if (!hasEnergy || !hasCt || !hasDose) {
         set_error("context needs lookup tables, CT and dose grid before add_beam");
@@ -644,6 +672,11 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
         set_error("beam needs " + std::to_string(P.tracerSteps) + " tracer steps; at most ~3000 are supported");
         return PBS_ERR_UNSUPPORTED;
     }
+    if (adj && (chunk < L || nuclear || !P.hasLattice)) {
+        set_error(chunk < L ? "adjoint: every layer of the beam must fit one chunk; raise PBS_OPT_LAYER_BUDGET_MIB"
+                            : "adjoint: needs a beam with a raw spot lattice and no nuclear halo");
+        return PBS_ERR_UNSUPPORTED;
+    }
     if (keepDebug && chunk < L) {
         set_error("PBS_OPT_KEEP_DEBUG needs every layer of the beam in one chunk; raise PBS_OPT_LAYER_BUDGET_MIB");
         return PBS_ERR_OUT_OF_MEMORY;
@@ -779,6 +812,7 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
                      "nuc_bin_plan");
         }
         if (l0 == 0 && (rc = mark(5))) return rc;
+        if (adj) break;  // the adjoint's superposition runs after the transfer box is known
         PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
                                   static_cast<const int4*>(work.ptr), dbs, dBev, smCount, stream),
                  "superpose");
@@ -788,6 +822,7 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
                      "nuc_superpose");
     }
     if ((rc = mark(6))) return rc;
+    if (adj) return finish_adjoint(*adj, b);
     if ((rc = flush_dose_init())) return rc;
     PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
@@ -807,6 +842,52 @@ int Context::add_beam(const PbsBeamDesc& b, int nuclear) {
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;
+}
+
+// Dose gradient -> spot-weight gradient for the beam whose IDD, binning and work
+// list run_beam just enqueued: T^T, S^T with the IDD scaling, the transposed
+// convolution, then the lattice-cell shares of every spot on the host.
+int Context::finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b) {
+    const BeamGeomDev& g = geom;
+    BeamStateDev* dbs = static_cast<BeamStateDev*>(bs.ptr);
+    const size_t S = size_t(g.steps), rays = size_t(g.rayX) * g.rayY, L = size_t(g.numLayers);
+    const size_t bevN = S * g.bevX * g.bevY, latN = L * g.latNy * g.latNx;
+    int rc;
+    if ((rc = bevGrad.ensure(bevN * 4)) || (rc = rbarBuf.ensure(L * rays * 4)) ||
+        (rc = gradInterm.ensure(L * g.latNy * g.rayX * 4)) || (rc = gradLattice.ensure(latN * 4)))
+        return rc;
+    PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
+    PBS_CUDA(cudaMemsetAsync(bevGrad.ptr, 0, bevN * 4, stream), "memset");
+    PBS_CUDA(cudaMemsetAsync(rbarBuf.ptr, 0, L * rays * 4, stream), "memset");
+    PBS_CUDA(launch_transfer_adjoint(g, a.gradDose, dbs, static_cast<float*>(bevGrad.ptr), stream), "transfer_adjoint");
+    PBS_CUDA(launch_superpose_adjoint(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
+                                      static_cast<const int4*>(work.ptr), dbs, static_cast<const float*>(bevGrad.ptr),
+                                      static_cast<float*>(rbarBuf.ptr), smCount, stream),
+             "superpose_adjoint");
+    PBS_CUDA(launch_conv_lattice_adjoint(g, static_cast<const float*>(rbarBuf.ptr), static_cast<const float*>(rayW.ptr),
+                                         static_cast<float*>(gradInterm.ptr), static_cast<float*>(gradLattice.ptr),
+                                         static_cast<const LayerStateDev*>(ls.ptr), dbs, stream),
+             "conv_adjoint");
+    std::vector<float> hLat(latN);
+    PBS_CUDA(cudaMemcpyAsync(hLat.data(), gradLattice.ptr, latN * 4, cudaMemcpyDeviceToHost, stream), "grad D2H");
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    std::vector<int> cells;
+    std::vector<float> shares;
+    if (!lattice_spot_cells(b, plan.lattice, cells, shares)) {
+        set_error("adjoint: could not map the spots onto the lattice");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    for (size_t s = 0; s < a.nSpots; ++s) {
+        double v = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            const int c = cells[s * 4 + k];
+            if (c >= 0) v += double(shares[s * 4 + k]) * double(hLat[size_t(c)]);
+        }
+        a.gradSpots[s] = float(v);
+    }
+    lastLaunches = 0;
+    lastBeamValid = true;
+    return take_device_errors();
 }
 
 int Context::beam_stats(PbsBeamStats* out) {

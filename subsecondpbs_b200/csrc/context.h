@@ -75,6 +75,8 @@ struct Context {
     BeamGeomDev nucGeom{};
     bool lastNuclear = false;
     std::vector<float> layerSpotDist;
+    // Adjoint working set.
+    DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice;
     PinnedBuf staging;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
@@ -111,6 +113,16 @@ struct Context {
     int read_dose(float* out, int onDevice);
     int read_dose64(double* out, int onDevice);
     int add_beam(const PbsBeamDesc& b, int nuclear);
+    // Gradient of <gradDose, dose of the beam> with respect to the beam's spot
+    // weights (one float per spot, host memory); gradDose is FP64 [Z][Y][X].
+    int adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int gradOnDevice, float* gradSpots, size_t nSpots);
+    struct AdjointArgs {
+        const double* gradDose;
+        float* gradSpots;
+        size_t nSpots;
+    };
+    int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj);
+    int finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b);
     int beam_stats(PbsBeamStats* out);
     int layer_stats(int layer, PbsLayerStats* out);
     int stage_times(float* ms, int n);

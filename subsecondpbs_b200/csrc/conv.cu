@@ -133,7 +133,89 @@ __global__ void cpb_to_ray_kernel(BeamGeomDev g, const float* __restrict__ cpb, 
     rayW[(static_cast<size_t>(l) * g.rayY + ry) * g.rayX + rx] = acc;
 }
 
+// Transposes of the two gather passes for the spot-weight adjoint. A forward
+// output o takes tap i when i >= ceil((o - reach - off) / delta) and
+// dist = i * delta + off - o < reach; the transpose visits, for tap i, the
+// outputs o near i * delta + off and applies that same test and weight.
+__device__ __forceinline__ float conv_tap(int o, int i, float delta, float off, float reach, float rSigma,
+                                          bool& taken) {
+    const int i0 = int(ceilf((float(o) - reach - off) / delta));
+    const float dist = float(i) * delta + off - float(o);
+    taken = i >= i0 && dist < reach;
+    return taken ? 0.5f * (erff((dist + 0.5f) * rSigma) - erff((dist - 0.5f) * rSigma)) : 0.0f;
+}
+
+// y pass transposed: gradInterm[l][iy][x] = sum_y w(y, iy) * gradRay[l][y][x], where
+// gradRay is the ray-weight gradient (rbar / rayW on rays with weight).
+__global__ void conv_y_adjoint_kernel(BeamGeomDev g, const float* __restrict__ rbar, const float* __restrict__ rayW,
+                                      float* __restrict__ gradInterm, const LayerStateDev* __restrict__ ls,
+                                      const BeamStateDev* __restrict__ beam) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z;
+    if (x >= g.rayX || iy >= g.latNy) return;
+    const float pixelSp = g.cpbResY * beam->pxSpMultY;
+    const float delta = g.latDy / g.cpbResY;
+    const float off = (g.latOy - g.cpbCornerY) / g.cpbResY;
+    const float sigmaEff = ls[l].entrySigmaY / pixelSp;
+    const float rSigma = 0.70710678f / sigmaEff;
+    const float reach = kConvSigmaCutoff * sigmaEff + 0.5f;
+    float acc = 0.0f;
+    if (delta > 0.0f && sigmaEff > 0.0f) {
+        const float c = float(iy) * delta + off;
+        const int y0 = max(int(floorf(c - reach)) - 2, 0), y1 = min(int(ceilf(c + reach)) + 2, g.rayY - 1);
+        for (int y = y0; y <= y1; ++y) {
+            bool taken;
+            const float w = conv_tap(y, iy, delta, off, reach, rSigma, taken);
+            if (!taken) continue;
+            const size_t r = (static_cast<size_t>(l) * g.rayY + y) * g.rayX + x;
+            const float rw = rayW[r];
+            if (rw > 0.0f) acc += w * (rbar[r] / rw);
+        }
+    }
+    gradInterm[(static_cast<size_t>(l) * g.latNy + iy) * g.rayX + x] = acc;
+}
+
+// x pass transposed: gradLattice[l][iy][ix] = sum_x w(x, ix) * gradInterm[l][iy][x].
+__global__ void conv_x_adjoint_kernel(BeamGeomDev g, const float* __restrict__ gradInterm,
+                                      float* __restrict__ gradLattice, const LayerStateDev* __restrict__ ls,
+                                      const BeamStateDev* __restrict__ beam) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z;
+    if (ix >= g.latNx || iy >= g.latNy) return;
+    const float pixelSp = g.cpbResX * beam->pxSpMultX;
+    const float delta = g.latDx / g.cpbResX;
+    const float off = (g.latOx - g.cpbCornerX) / g.cpbResX;
+    const float sigmaEff = ls[l].entrySigmaX / pixelSp;
+    const float rSigma = 0.70710678f / sigmaEff;
+    const float reach = kConvSigmaCutoff * sigmaEff + 0.5f;
+    float acc = 0.0f;
+    if (delta > 0.0f && sigmaEff > 0.0f) {
+        const float c = float(ix) * delta + off;
+        const int x0 = max(int(floorf(c - reach)) - 2, 0), x1 = min(int(ceilf(c + reach)) + 2, g.rayX - 1);
+        const float* row = gradInterm + (static_cast<size_t>(l) * g.latNy + iy) * g.rayX;
+        for (int x = x0; x <= x1; ++x) {
+            bool taken;
+            const float w = conv_tap(x, ix, delta, off, reach, rSigma, taken);
+            if (taken) acc += w * row[x];
+        }
+    }
+    gradLattice[(static_cast<size_t>(l) * g.latNy + iy) * g.latNx + ix] = acc;
+}
+
 }  // namespace
+
+cudaError_t launch_conv_lattice_adjoint(const BeamGeomDev& g, const float* rbar, const float* rayW, float* gradInterm,
+                                        float* gradLattice, const LayerStateDev* ls, const BeamStateDev* beam,
+                                        cudaStream_t s) {
+    dim3 block(32, 8);
+    dim3 gy((g.rayX + 31) / 32, (g.latNy + 7) / 8, g.numLayers);
+    conv_y_adjoint_kernel<<<gy, block, 0, s>>>(g, rbar, rayW, gradInterm, ls, beam);
+    dim3 gx((g.latNx + 31) / 32, (g.latNy + 7) / 8, g.numLayers);
+    conv_x_adjoint_kernel<<<gx, block, 0, s>>>(g, gradInterm, gradLattice, ls, beam);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_conv_lattice(const BeamGeomDev& g, const float* lattice, float* interm, float* rayW,
                                 const LayerStateDev* ls, const BeamStateDev* beam, cudaStream_t s) {

@@ -49,4 +49,37 @@ __device__ __forceinline__ int tile_radius_bucket(float minRSigma) {
     return min(int(q), 33);
 }
 
+// erf(x), x >= 0, from Abramowitz & Stegun 7.1.26 (Hastings' rational
+// approximation, |error| <= 1.5e-7): 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e^{-x^2}
+// with t = 1 / (1 + p x). The caller supplies e^{-x^2}.
+__device__ __forceinline__ float erf_hastings(float x, float expNegX2) {
+    constexpr float p = 0.3275911f;
+    constexpr float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+                    a5 = 1.061405429f;
+    const float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
+    const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, a5, a4), a3), a2), a1);
+    return fmaf(-poly, expNegX2, 1.0f);
+}
+
+// Superposition weights of one source (complete_superposition.cu:298-307):
+// e[0] = erf(r/2), e[k] = (erf((k+1/2) r) - erf((k-1/2) r)) / 2 for k = 1..R. The
+// factor e^{-((k+1/2) r)^2} follows E_{k+1} = E_k G_k, G_k = e^{-2 (k+1) r^2}.
+template <int R>
+__device__ __forceinline__ void superposition_row(float rs, float (&e)[R + 1]) {
+    const float r2 = rs * rs;
+    const float step2 = __expf(-2.0f * r2);
+    float E = __expf(-0.25f * r2);
+    float G = step2;
+    float fPrev = erf_hastings(rs * 0.5f, E);
+    e[0] = fPrev;
+#pragma unroll
+    for (int k = 1; k <= R; ++k) {
+        E *= G;
+        G *= step2;
+        const float f = erf_hastings(rs * (float(k) + 0.5f), E);
+        e[k] = 0.5f * (f - fPrev);
+        fPrev = f;
+    }
+}
+
 }  // namespace pbs

@@ -74,6 +74,20 @@ cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cu
 cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,
                             cudaStream_t s);
 
+// ---- spot-weight adjoint (adjoint.cu, conv.cu) ----------------------------------------
+// T^T: the dose gradient (FP64 [Z][Y][X]) spread onto the BEV gradient with the
+// transfer's trilinear weights over the transfer box of `beam`.
+cudaError_t launch_transfer_adjoint(const BeamGeomDev& g, const double* gradDose, const BeamStateDev* beam,
+                                    float* gradBev, cudaStream_t s);
+// S^T and the IDD scaling over the chunk's work list: rbar[l][ray] += idd * (S^T gradBev).
+cudaError_t launch_superpose_adjoint(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                                     BeamStateDev* beam, const float* gradBev, float* rbar, int numSMs,
+                                     cudaStream_t s);
+// Transposed spot -> ray convolution (mode A): gradLattice[l][iy][ix] from rbar / rayW.
+cudaError_t launch_conv_lattice_adjoint(const BeamGeomDev& g, const float* rbar, const float* rayW, float* gradInterm,
+                                        float* gradLattice, const LayerStateDev* ls, const BeamStateDev* beam,
+                                        cudaStream_t s);
+
 // ---- dose grid -------------------------------------------------------------------
 cudaError_t launch_dose_init(double* dose, const float* init, size_t n, cudaStream_t s);
 cudaError_t launch_dose_to_float(const double* dose, float* out, size_t n, cudaStream_t s);

@@ -292,6 +292,51 @@ bool estimate_virtual_source_distances(const PbsBeamDesc& b, V3 bmX, V3 bmY, V3 
 
 }  // namespace
 
+// Lattice cells each spot feeds, with its share (the linear map spot weights ->
+// lattice of build_raw_lattice): one cell for spot positions in mm, the bilinear
+// splat for positions given as rayweq indices. Four (cell, share) slots per spot;
+// unused slots have cell -1.
+bool lattice_spot_cells(const PbsBeamDesc& b, const RawLattice& lat, std::vector<int>& cells,
+                        std::vector<float>& shares) {
+    const int L = static_cast<int>(b.n_energies);
+    int total = 0;
+    for (int l = 0; l < L; ++l) total += b.layer_spot_counts[l];
+    cells.assign(static_cast<size_t>(total) * 4, -1);
+    shares.assign(static_cast<size_t>(total) * 4, 0.0f);
+    size_t nh = 0;
+    const float* hdr = active_weq_header(b, nh);
+    int off = 0;
+    for (int l = 0; l < L; ++l) {
+        for (int i = 0; i < b.layer_spot_counts[l]; ++i) {
+            const int s = off + i;
+            auto put = [&](int slot, int ix, int iy, float share) {
+                if (!(share > 0.0f) || ix < 0 || ix >= lat.nx || iy < 0 || iy >= lat.ny) return;
+                cells[size_t(s) * 4 + slot] = (l * lat.ny + iy) * lat.nx + ix;
+                shares[size_t(s) * 4 + slot] = share;
+            };
+            if (b.spot_positions_are_indices) {
+                const float lx = b.spot_positions[2 * s] - 0.5f, ly = b.spot_positions[2 * s + 1] - 0.5f;
+                const int ix0 = static_cast<int>(std::floor(lx)), iy0 = static_cast<int>(std::floor(ly));
+                const float tx = lx - static_cast<float>(ix0), ty = ly - static_cast<float>(iy0);
+                put(0, ix0, iy0, (1.0f - tx) * (1.0f - ty));
+                put(1, ix0 + 1, iy0, tx * (1.0f - ty));
+                put(2, ix0, iy0 + 1, (1.0f - tx) * ty);
+                put(3, ix0 + 1, iy0 + 1, tx * ty);
+            } else {
+                float x, y;
+                if (!decode_spot_position(b, hdr, nh, b.spot_positions[2 * s], b.spot_positions[2 * s + 1], x, y))
+                    return false;
+                const float fx = (lat.dx != 0.0f) ? ((x - lat.ox) / lat.dx) : 0.0f;
+                const float fy = (lat.dy != 0.0f) ? ((y - lat.oy) / lat.dy) : 0.0f;
+                put(0, static_cast<int>(std::lround(fx)), static_cast<int>(std::lround(fy)), 1.0f);
+            }
+        }
+        off += b.layer_spot_counts[l];
+    }
+    return true;
+}
+
+
 // ---- reference host helpers ---------------------------------------------
 
 // include/utils/vector_find.h:61-82

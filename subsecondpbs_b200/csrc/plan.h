@@ -84,6 +84,11 @@ int plan_beam(const PbsBeamDesc& b, const PbsEnergyDesc& e, const GridDesc& ctGr
               BeamPlan& out, std::string& err);
 
 // Reference host helpers (include/utils/vector_find.h, vector_interpolate.h).
+// Lattice cells (four slots per spot, cell -1 unused) and shares each spot of the
+// beam feeds in the lattice that plan_beam builds for it.
+bool lattice_spot_cells(const PbsBeamDesc& b, const RawLattice& lat, std::vector<int>& cells,
+                        std::vector<float>& shares);
+
 int find_first_larger_ordered(const float* v, int n, float value);
 float find_decimal_ordered(const float* v, int n, float value);
 float vector_interpolate(const float* v, int n, float idx);

@@ -23,6 +23,7 @@
 // Radii 16..32, 8..15 and 0..7 run as three instances of the kernel with 128, 48
 // and 32 registers and 96, 43 and 21 KB of shared memory: 2, 5 and 8 CTAs per SM
 // (the narrower instances trade a few spilled registers for occupancy).
+#include "device_util.cuh"
 #include "kernels.h"
 #include "launch_util.h"
 
@@ -47,18 +48,6 @@ struct Shape {
 // source columns 4, 8 or 16 apart (read together by the lane groups of one
 // instruction) land in different banks.
 __device__ __forceinline__ int e4_col(int sx) { return sx ^ ((sx >> 3) & 3); }
-
-// erf(x), x >= 0, from Abramowitz & Stegun 7.1.26 (Hastings' rational
-// approximation, |error| <= 1.5e-7): 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e^{-x^2}
-// with t = 1 / (1 + p x). The caller supplies e^{-x^2}.
-__device__ __forceinline__ float erf_hastings(float x, float expNegX2) {
-    constexpr float p = 0.3275911f;
-    constexpr float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
-                    a5 = 1.061405429f;
-    const float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
-    const float poly = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, a5, a4), a3), a2), a1);
-    return fmaf(-poly, expNegX2, 1.0f);
-}
 
 struct TileArgs {
     const float* idd;
@@ -92,25 +81,13 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         if (lane == 0) sMask[warp] = mask;
         float e[4 * Q];
         if (live) {
-            // erf at (k + 1/2) r, k = 0..R; e^{-((k+1/2) r)^2} follows the recurrence
-            // E_{k+1} = E_k G_k, G_k = e^{-2 (k+1) r^2} = G_{k-1} e^{-2 r^2}.
-            const float rs = a.rsig[a.src];
-            const float r2 = rs * rs;
-            const float step2 = __expf(-2.0f * r2);
-            float E = __expf(-0.25f * r2);
-            float G = step2;
-            float fPrev = erf_hastings(rs * 0.5f, E);
-            e[0] = fPrev;
+            float row[R + 1];
+            superposition_row<R>(a.rsig[a.src], row);
 #pragma unroll
-            for (int k = 1; k <= R; ++k) {
-                E *= G;
-                G *= step2;
-                const float f = erf_hastings(rs * (float(k) + 0.5f), E);
-                e[k] = 0.5f * (f - fPrev);
-                fPrev = f;
+            for (int k = 0; k <= R; ++k) {
+                e[k] = row[k];
+                EW[t * EWS + k] = dose * row[k];
             }
-#pragma unroll
-            for (int k = 0; k <= R; ++k) EW[t * EWS + k] = dose * e[k];
         } else {
 #pragma unroll
             for (int k = 0; k <= R; ++k) {

@@ -152,6 +152,23 @@ class DoseEngine:
         _lib.check(self._lib.pbs_context_add_beam(self._h, C.byref(bd), int(bool(nuclear_correction))))
         del keep
 
+    def adjoint_beam(self, beam, grad_dose, n_spots: int | None = None) -> np.ndarray:
+        """Gradient of <grad_dose, dose of `beam`> with respect to the beam's spot
+        weights at their current values (float32 [n_spots], the beam's spot order).
+        `grad_dose` is a float64 [Z][Y][X] numpy array or CUDA tensor."""
+        if isinstance(beam, tuple):
+            bd, keep = beam
+        else:
+            bd, keep = _lib.beam_desc(beam)
+        if n_spots is None:
+            n_spots = int(sum(bd.layer_spot_counts[i] for i in range(bd.n_layer_spot_counts)))
+        out = np.zeros(n_spots, dtype=np.float32)
+        on_dev, ptr, gkeep = self._ptr(grad_dose, np.float64)
+        _lib.check(self._lib.pbs_context_adjoint_beam(self._h, C.byref(bd), ptr, on_dev,
+                                                      out.ctypes.data_as(C.POINTER(C.c_float)), n_spots))
+        del keep, gkeep
+        return out
+
     @staticmethod
     def prepare_beam(beam: dict):
         """Convert a beam dict to its C descriptor once (for repeated add_beam calls)."""

@@ -238,3 +238,46 @@ def heterogeneous_case(dims=(256, 256, 160), res=(2.0, 2.0, 2.0), n_layers=20, e
     return {"name": "heterogeneous", "ct": ct, "ct_dims": dims, "ct_resolution": res, "ct_corner": corner,
             "dose_dims": dims, "dose_resolution": res, "dose_corner": corner, "beam": beam,
             "energy": proton_tables()}
+
+
+def inverse_planning_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), n_beams=4, n_layers=36, e_range=(66.0, 112.0),
+                          field_mm=70.0, pitch_mm=5.0, sigma_mm=4.0, target_radius_mm=25.0, shell_mm=20.0,
+                          prescription_gy=2.0, sad_mm=10000.0, ray_spacing=1.0, n_sub=7,
+                          seed=SEED_BASE + 4) -> dict:
+    """Inverse-planning workload: the water box of `water_phantom_case`, `n_beams`
+    coplanar beams (gantry 0, 360/n, ...), each with `n_layers` energy layers of a
+    square spot grid over the field (36 x 225 = 8100 spots per beam by default) and
+    lognormal weights; a target sphere of `target_radius_mm` at the isocentre with a
+    `prescription_gy` prescription and a surrounding `shell_mm` shell with 0 Gy.
+    Adds `beams`, `target` and `shell` (bool [Z][Y][X]) and `prescription`."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    base = water_phantom_case(dims=dims, res=res, sigma_mm=sigma_mm, sad_mm=sad_mm, ray_spacing=ray_spacing,
+                              n_sub=n_sub, seed=seed)
+    n_side = int(round(field_mm / pitch_mm)) + 1
+    g = (np.arange(n_side) - (n_side - 1) / 2.0) * pitch_mm
+    px, py = np.meshgrid(g, g, indexing="xy")
+    spots = np.stack([px.reshape(-1), py.reshape(-1)], axis=1).astype(np.float32)
+    energies = np.linspace(e_range[0], e_range[1], n_layers).astype(np.float32)
+    counts = np.full(n_layers, spots.shape[0], dtype=np.int32)
+    beam = dict(base["beam"])
+    beam.update({
+        "energies": energies,
+        "spot_sigmas": np.tile(np.array([[sigma_mm, sigma_mm]], np.float32), (n_layers, 1)),
+        "spot_delta": (pitch_mm, pitch_mm, 0.0),
+        "layer_spot_counts": counts,
+        "spot_positions": np.tile(spots, (n_layers, 1)).reshape(-1),
+        "subspot_data": subspot_lut(n_layers, n_sub, np.full(n_layers, sigma_mm), rng),
+    })
+    beams = []
+    for k in range(n_beams):
+        b = rotate_beam(beam, 360.0 * k / n_beams)
+        b["spot_weights"] = rng.lognormal(0.0, 0.5, size=int(counts.sum())).astype(np.float32)
+        beams.append(b)
+    dims_, res_, corner = _grid(dims, res)
+    z, y, x = np.meshgrid(*(corner[i] + res_[i] * np.arange(dims_[i]) for i in (2, 1, 0)), indexing="ij")
+    r = np.sqrt(x * x + y * y + z * z)
+    out = dict(base)
+    out.update({"name": "inverse_planning", "beam": beams[0], "beams": beams, "target": r <= target_radius_mm,
+                "shell": (r > target_radius_mm) & (r <= target_radius_mm + shell_mm),
+                "prescription": float(prescription_gy)})
+    return out

@@ -13,28 +13,7 @@ DOSE_TOL_FRAC_DMAX = 5e-3
 GAMMA_PASS_MIN = 0.999
 
 
-def max_rel_err(dose, ref, thr=0.1):
-    dmax = float(ref.max())
-    mask = ref > thr * dmax
-    return float(np.abs(dose.astype(np.float64) - ref)[mask].max() / dmax)
-
-
-def gamma_pass_rate(dose, ref, spacing_mm, dd=0.01, dta_mm=1.0, thr=0.1):
-    """1 %/1 mm global gamma over voxels above `thr` of Dmax; the evaluated dose is
-    sampled at the voxel and at +-dta along each axis (linear interpolation)."""
-    ref = np.asarray(ref, np.float64)
-    ev = np.asarray(dose, np.float64)
-    dmax = ref.max()
-    mask = ref > thr * dmax
-    best = ((ev - ref) / (dd * dmax)) ** 2
-    for axis, sp in zip((2, 1, 0), spacing_mm):
-        f = min(dta_mm / sp, 1.0)
-        for sgn in (-1, 1):
-            nb = np.roll(ev, -sgn, axis=axis)
-            shifted = ev + f * (nb - ev)
-            g = ((shifted - ref) / (dd * dmax)) ** 2 + (f * sp / dta_mm) ** 2
-            best = np.minimum(best, g)
-    return float((best[mask] <= 1.0).mean())
+from subsecondpbs_b200.precision import gamma_pass_rate, max_rel_err  # noqa: E402,F401
 
 
 def run_gpu(case, beams=None, compat=False, keep_debug=True, initial=None, ct_input_type=None, nuclear_model=None):
