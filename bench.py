@@ -46,6 +46,9 @@ def _args():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the spot-weight adjoint timing")
+    ap.add_argument("--serving-requests", type=int, default=1000, help="served stream length (0: skip)")
+    ap.add_argument("--serving-slots", type=int, default=4)
+    ap.add_argument("--serving-budget-mib", type=int, default=0, help="server HBM budget (0: 90%% of free)")
     return ap.parse_args()
 
 
@@ -210,6 +213,57 @@ def _adjoint_cost(local: int, reps: int = 5) -> dict:
             "forward_ms": round(fwd, 3), "adjoint_ms": round(adj, 3), "adjoint_over_forward": round(adj / fwd, 3),
             "timing": f"median of {reps} synchronised wall-clock runs; forward includes the FP64 readout and "
                       "objective, adjoint includes the per-spot gradient readout"}
+
+
+def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
+    """Served mixed stream (seeded Poisson arrivals; CTs 128^3 and 256x256x160 at
+    2 mm and 512x512x200 at 1 mm; 1-4 beams; heavy-tailed 500-20000 spots per
+    field; 80/20 proton/carbon, carbon with the nuclear halo) through the
+    continuous-batching server, against the plain pipeline that runs one request
+    at a time through pbs_subsecond_wrapper."""
+    from subsecondpbs_b200 import _lib, phantoms, serving
+    from subsecondpbs_b200.precision import max_rel_err
+
+    w = phantoms.serving_workload(n_requests=n_requests)
+    prepared = [[_lib.beam_desc(b) for b in phantoms.request_beams(w, r)] for r in w["requests"]]
+    check = set(range(0, n_requests, max(1, n_requests // 16)))
+    warm = min(50, n_requests)
+    head = dict(w, requests=w["requests"][:warm])
+    serving.plain_pipeline(head, prepared[:warm], local)
+    plain = serving.plain_pipeline(w, prepared, local, keep=check)
+    ps = plain["service_s"] * 1e3
+    srv = serving.DoseServer(local, slots=slots, hbm_budget_mib=budget_mib)
+    srv.add_energy(0, w["energy"]["proton"])
+    srv.add_energy(1, w["energy"]["carbon"])
+    for p in w["patients"]:
+        srv.add_patient(p["id"], p["ct"], p["ct_dims"], p["ct_resolution"], p["ct_corner"])
+    serving.serve_workload(srv, head, prepared[:warm], arrivals=False)
+    sat = serving.serve_workload(srv, w, prepared, arrivals=False, keep=check)
+    rate = 0.8 * sat["plans_per_s"]
+    poi = serving.serve_workload(srv, serving.with_rate(w, rate), prepared, arrivals=True)
+    stats = srv.stats()
+    srv.close()
+    diffs = [max_rel_err(sat["doses"][i], plain["doses"][i], thr=0.0) for i in sorted(check)]
+
+    def pct(a, q):
+        return round(float(np.quantile(a, q)), 3)
+
+    sl, pl = sat["latency_s"] * 1e3, poi["latency_s"] * 1e3
+    return {
+        "workload": f"{n_requests} requests, {len(w['patients'])} patients (CT 128^3@2mm, 256x256x160@2mm, "
+                    "512x512x200@1mm), 1-4 beams of 500-20000 spots (Pareto 1.1), 80/20 proton/carbon+halo",
+        "slots": slots, "hbm_budget_mib": budget_mib or "90% of free",
+        "plain": {"plans_per_s": round(plain["plans_per_s"], 2), "p50_ms": pct(ps, 0.5), "p99_ms": pct(ps, 0.99),
+                  "api": "pbs_subsecond_wrapper per request, pinned host CT and dose"},
+        "saturated": {"plans_per_s": round(sat["plans_per_s"], 2), "p50_ms": pct(sl, 0.5), "p99_ms": pct(sl, 0.99),
+                      "arrivals": "all at t=0"},
+        "poisson": {"rate_hz": round(rate, 2), "plans_per_s": round(poi["plans_per_s"], 2), "p50_ms": pct(pl, 0.5),
+                    "p99_ms": pct(pl, 0.99)},
+        "served_over_plain": round(sat["plans_per_s"] / plain["plans_per_s"], 3),
+        "result_max_diff_vs_plain_frac_dmax": float(max(diffs)),
+        "server_stats": {k: v for k, v in stats.items() if k in ("completed", "failed", "patient_loads",
+                                                                  "evictions", "peak_bytes", "budget_bytes")},
+    }
 
 
 def run_ours(args):
@@ -399,6 +453,8 @@ def run_ours(args):
                          "Kahan WEPL, FP64 dose accumulation")
 
     adjoint = _adjoint_cost(local) if world == 1 and not args.no_adjoint else None
+    served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
+              if world == 1 and args.serving_requests > 0 else None)
 
     line = {
         "metric": METRIC,
@@ -425,6 +481,7 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "precision": precision,
         "adjoint": adjoint,
+        "serving": served,
         "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers"},
         "gpu_launches": launches_per_step * args.steps,

@@ -307,6 +307,68 @@ PBS_API void* pbs_context_dose_device_ptr(PbsContext* ctx);
 /* Stats of the last beam (synchronizes the context stream). */
 PBS_API int pbs_context_beam_stats(PbsContext* ctx, PbsBeamStats* out);
 PBS_API int pbs_context_layer_stats(PbsContext* ctx, int layer, PbsLayerStats* out);
+
+/* ---- dose-request server (no reference counterpart) ------------------------
+ * Continuous batching of dose requests on one GPU. `n_slots` execution slots,
+ * each a resident context with its own stream and host thread, take requests
+ * from one FIFO queue as they free up; a request is admitted when its device
+ * bytes (tables, dose grid, largest beam) fit `hbm_budget_mib` next to the
+ * resident patient CTs and the other slots (0: 90 % of the free memory). A
+ * queued request that fits overtakes an older one that does not, until the older
+ * one has waited `pbs_server_set_bypass_limit` seconds (default 0.5).
+ * Patients are registered once: their CT is copied to pinned host memory, then
+ * uploaded and converted to HU+1000 by the first request that needs it and kept
+ * on the device for later requests; idle patients are evicted least recently
+ * used first when the budget is short. Beams and tables are copied at submit and
+ * registration, so the caller may free its arrays on return.
+ * A result is the float [Z][Y][X] dose of the request's beams, computed as
+ * pbs_context_add_beam would on a zeroed grid; `pbs_server_wait` gives a pointer
+ * to it that stays valid until `pbs_server_release`. Times are seconds since the
+ * server was created (submitted, started on a slot, finished). */
+typedef struct PbsServer PbsServer;
+typedef struct PbsServerStats {
+    long long submitted, completed, failed, queued, running;
+    long long patient_loads;  /* CT uploads (first use and reloads after eviction) */
+    long long evictions;      /* patient CTs dropped to make room                   */
+    long long slot_releases;  /* idle slots that gave their buffers back           */
+    long long resident_bytes; /* patient CTs on the device                          */
+    long long slot_bytes;     /* device bytes held by the slots                     */
+    long long peak_bytes;     /* largest committed total at an admission            */
+    long long budget_bytes;
+} PbsServerStats;
+
+PBS_API int pbs_server_create(int gpu_id, int n_slots, long long hbm_budget_mib, PbsServer** out);
+/* Stops the slots after their current request; queued requests are dropped. */
+PBS_API int pbs_server_destroy(PbsServer* server);
+/* PBS_OPT_COMPAT_BEV_Z_SHIFT, PBS_OPT_LAYER_BUDGET_MIB, PBS_OPT_NUCLEAR_MODEL for
+ * every slot; only while no request is queued or running. */
+PBS_API int pbs_server_set_option(PbsServer* server, int option, long long value);
+PBS_API int pbs_server_set_bypass_limit(PbsServer* server, double seconds);
+PBS_API int pbs_server_add_energy(PbsServer* server, int energy_id, const PbsEnergyDesc* energy);
+PBS_API int pbs_server_add_patient(PbsServer* server, int patient_id, const float* ct, const int ct_dims[3],
+                                   const float ct_resolution[3], const float ct_corner[3], const int dose_dims[3],
+                                   const float dose_resolution[3], const float dose_corner[3]);
+/* PBS_ERR_NOT_READY while a request of the patient is queued or running. */
+PBS_API int pbs_server_remove_patient(PbsServer* server, int patient_id);
+/* Plans every beam on the calling thread (PBS_ERR_INVALID_ARGUMENT / _GEOMETRY
+ * for a beam that cannot be planned, PBS_ERR_OUT_OF_MEMORY for a request larger
+ * than the budget), then queues the request. */
+PBS_API int pbs_server_submit(PbsServer* server, int patient_id, int energy_id, const PbsBeamDesc* beams,
+                              size_t n_beams, int nuclear_correction, unsigned long long* ticket);
+/* PBS_ERR_TIMEOUT when the request is not finished within `timeout_s` (negative:
+ * no limit); otherwise the request's own status. */
+PBS_API int pbs_server_wait(PbsServer* server, unsigned long long ticket, double timeout_s, const float** dose,
+                            double times[3], int* slot);
+/* A finished request's phase times (submitted, started on a slot, all of its
+ * work enqueued on the slot's stream, finished), its slot and the device bytes
+ * its admission reserved on the slot. PBS_ERR_NOT_READY before it finishes. */
+PBS_API int pbs_server_request_info(PbsServer* server, unsigned long long ticket, double times[4], int* slot,
+                                    long long* est_bytes);
+PBS_API int pbs_server_release(PbsServer* server, unsigned long long ticket);
+/* Waits until nothing is queued or running. */
+PBS_API int pbs_server_drain(PbsServer* server, double timeout_s);
+PBS_API int pbs_server_stats(PbsServer* server, PbsServerStats* out);
+PBS_API double pbs_server_now(PbsServer* server);
 /* Milliseconds per stage (PBS_STAGE_*) of the last beam; needs PBS_OPT_STAGE_TIMING. */
 PBS_API int pbs_context_stage_times(PbsContext* ctx, float* ms, int n);
 /* Copy an intermediate buffer of the last beam (PBS_DBG_*) to host memory;

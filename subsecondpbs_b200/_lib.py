@@ -156,6 +156,12 @@ def struct_to_dict(s: C.Structure) -> dict:
     return out
 
 
+class PbsServerStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in ("submitted", "completed", "failed", "queued", "running", "patient_loads",
+                                            "evictions", "slot_releases", "resident_bytes", "slot_bytes",
+                                            "peak_bytes", "budget_bytes")]
+
+
 class PbsError(RuntimeError):
     """Raised for a non-zero status of the native library."""
 
@@ -208,6 +214,22 @@ def load() -> C.CDLL:
         "pbs_context_layer_stats": (i, [vp, i, C.POINTER(PbsLayerStats)]),
         "pbs_context_stage_times": (i, [vp, C.POINTER(C.c_float), i]),
         "pbs_context_debug_copy": (i, [vp, i, i, vp, C.c_size_t]),
+        "pbs_server_create": (i, [i, i, C.c_longlong, C.POINTER(vp)]),
+        "pbs_server_destroy": (i, [vp]),
+        "pbs_server_set_option": (i, [vp, i, C.c_longlong]),
+        "pbs_server_set_bypass_limit": (i, [vp, C.c_double]),
+        "pbs_server_add_energy": (i, [vp, i, C.POINTER(PbsEnergyDesc)]),
+        "pbs_server_add_patient": (i, [vp, i, fp, ip3, fp3, fp3, ip3, fp3, fp3]),
+        "pbs_server_remove_patient": (i, [vp, i]),
+        "pbs_server_submit": (i, [vp, i, i, C.POINTER(PbsBeamDesc), C.c_size_t, i, C.POINTER(C.c_ulonglong)]),
+        "pbs_server_wait": (i, [vp, C.c_ulonglong, C.c_double, C.POINTER(C.POINTER(C.c_float)),
+                                C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+        "pbs_server_release": (i, [vp, C.c_ulonglong]),
+        "pbs_server_request_info": (i, [vp, C.c_ulonglong, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_longlong)]),
+        "pbs_server_drain": (i, [vp, C.c_double]),
+        "pbs_server_stats": (i, [vp, C.POINTER(PbsServerStats)]),
+        "pbs_server_now": (C.c_double, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

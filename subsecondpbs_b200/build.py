@@ -22,7 +22,7 @@ LIB = PKG / "libsubsecondpbs_b200.so"
 BUILD_DIR = PKG / "_build"
 
 CU_SOURCES = ["trace.cu", "conv.cu", "idd.cu", "superpose.cu", "transfer.cu", "context.cu", "peak.cu", "noalloc.cu", "adjoint.cu"]
-CXX_SOURCES = ["plan.cpp", "capi.cpp", "final_dose.cpp"]
+CXX_SOURCES = ["plan.cpp", "capi.cpp", "final_dose.cpp", "server.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden"]

@@ -42,21 +42,24 @@ static int cuda_fail(cudaError_t e, const char* where) {
 
 int DevBuf::ensure(size_t b) {
     if (b <= bytes) return PBS_OK;
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
+    release();
     if (b == 0) return PBS_OK;
-    cudaError_t e = cudaMalloc(&ptr, b);
+    cudaError_t e = allocStream ? cudaMallocAsync(&ptr, b, allocStream) : cudaMalloc(&ptr, b);
     if (e != cudaSuccess) {
         ptr = nullptr;
-        return cuda_fail(e, "cudaMalloc");
+        return cuda_fail(e, allocStream ? "cudaMallocAsync" : "cudaMalloc");
     }
     bytes = b;
     return PBS_OK;
 }
 
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (allocStream)
+            cudaFreeAsync(ptr, allocStream);
+        else
+            cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
 }
@@ -91,6 +94,7 @@ Context::~Context() {
                       &gradInterm, &gradLattice})
         b->release();
     staging.release();
+    errHost.release();
     if (copyStream) cudaStreamSynchronize(copyStream);
     if (stagingEvent) cudaEventDestroy(stagingEvent);
     if (copyStart) cudaEventDestroy(copyStart);
@@ -132,10 +136,14 @@ int Context::init(int gpu) {
 }
 
 int Context::take_device_errors() {
-    int flags = 0;
-    PBS_CUDA(cudaMemcpy(&flags, errWord.ptr, sizeof(int), cudaMemcpyDeviceToHost), "error flags D2H");
+    int rc = errHost.ensure(sizeof(int));
+    if (rc) return rc;
+    volatile int* hostFlags = static_cast<volatile int*>(errHost.ptr);
+    PBS_CUDA(cudaMemcpyAsync(errHost.ptr, errWord.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream), "error flags D2H");
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    const int flags = *hostFlags;
     if (!flags) return PBS_OK;
-    PBS_CUDA(cudaMemset(errWord.ptr, 0, sizeof(int)), "cudaMemset");
+    PBS_CUDA(cudaMemsetAsync(errWord.ptr, 0, sizeof(int), stream), "cudaMemsetAsync");
     if (flags & 4) {
         // complete_superposition.cu:609-627 throws here.
         set_error("Nuclear superposition kernel radius exceeded kMaxSuperpR=32 (a halo sigma below the tile "
@@ -287,6 +295,7 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
     const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
     int rc = ct.ensure(n * 4);
     if (rc) return rc;
+    ctView = nullptr;
     if (!box_empty(lo, hi)) PBS_CUDA(copy_box(ct.ptr, data, g.dims, lo, hi, cudaMemcpyHostToDevice, stream), "CT H2D");
     // The CT type comes from the whole volume, as with a full upload.
     int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
@@ -344,6 +353,7 @@ int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
     const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
     int rc = ct.ensure(n * 4);
     if (rc) return rc;
+    ctView = nullptr;
     int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
     if (onDevice) {
         PBS_CUDA(cudaMemcpyAsync(ct.ptr, data, n * 4, cudaMemcpyDeviceToDevice, stream), "CT D2D");
@@ -371,6 +381,15 @@ int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
 // CT adapter on the device (wrapper.cu:2290-2441): to HU+1000 in place.
 int Context::convert_ct(int type, const GridDesc& g) {
     const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
+    int rc = convert_ct_buffer(static_cast<float*>(ct.ptr), n, type);
+    if (rc) return rc;
+    ctType = type;
+    ctGrid = g;
+    hasCt = true;
+    return PBS_OK;
+}
+
+int Context::convert_ct_buffer(float* data, size_t n, int type) {
     if (type == PBS_CT_DENSITY || type == PBS_CT_SPR) {
         if (!hasEnergy) {
             set_error("[CT_ADAPTER] density/SPR CT needs the lookup tables; call set_energy first");
@@ -383,15 +402,12 @@ int Context::convert_ct(int type, const GridDesc& g) {
             set_error("[CT_ADAPTER] LUT is empty or scale factor is 0; cannot convert");
             return PBS_ERR_INVALID_ARGUMENT;
         }
-        PBS_CUDA(launch_ct_convert(static_cast<float*>(ct.ptr), n, type,
-                                   static_cast<const float*>(useDensity ? density.ptr : sp.ptr), lutN, scale, stream),
+        PBS_CUDA(launch_ct_convert(data, n, type, static_cast<const float*>(useDensity ? density.ptr : sp.ptr), lutN,
+                                   scale, stream),
                  "ct_convert");
     } else {
-        PBS_CUDA(launch_ct_convert(static_cast<float*>(ct.ptr), n, type, nullptr, 0, 1.0f, stream), "ct_convert");
+        PBS_CUDA(launch_ct_convert(data, n, type, nullptr, 0, 1.0f, stream), "ct_convert");
     }
-    ctType = type;
-    ctGrid = g;
-    hasCt = true;
     return PBS_OK;
 }
 
@@ -482,6 +498,99 @@ int Context::read_dose64(double* out, int onDevice) {
         PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         return take_device_errors();
     }
+    return PBS_OK;
+}
+
+BeamBuffers beam_buffers(const BeamPlan& P, size_t nSubspotData, int nuclear, long long layerBudgetMiB) {
+    BeamBuffers z;
+    const size_t L = size_t(P.numLayers), S = size_t(P.tracerSteps);
+    const size_t rays = size_t(P.rayDims[0]) * P.rayDims[1];
+    const size_t pitchX = size_t(P.superpDims[0]), pitchY = size_t(P.superpDims[1]);
+    const size_t padPlane = pitchX * pitchY;
+    const size_t tiles = (pitchX / kTileX) * (pitchY / kTileY);
+    const size_t perLayer = S * padPlane * 8 + S * tiles * (1 + sizeof(int4));
+    const size_t budget = size_t(std::max<long long>(layerBudgetMiB, 1)) << 20;
+    z.chunk = int(std::max<size_t>(1, std::min<size_t>(budget / std::max<size_t>(perLayer, 1), L)));
+    z.chunk = std::min(z.chunk, 64);
+    const size_t chunk = size_t(z.chunk);
+    z.dens = z.wepl = S * rays * 4;
+    z.weplMin = S * 4;
+    z.firstIn = z.firstOut = rays * 4;
+    z.rayW = L * rays * 4;
+    z.bev = S * (pitchX + 2 * kMaxR) * (pitchY + 2 * kMaxR) * 4;
+    z.codes = chunk * S * tiles;
+    z.work = chunk * S * tiles * sizeof(int4);
+    z.idd = z.rs = chunk * S * padPlane * 4;
+    z.firstPassive = chunk * rays * 4;
+    z.lp = L * sizeof(LayerParamsDev);
+    z.ls = L * sizeof(LayerStateDev);
+    z.bs = sizeof(BeamStateDev);
+    if (P.hasLattice) {
+        z.lattice = P.lattice.weights.size() * 4;
+        z.interm = L * size_t(P.lattice.ny) * size_t(P.rayDims[0]) * 4;
+    } else {
+        z.subspots = nSubspotData * 4;
+        z.cpb = L * rays * 4;
+    }
+    if (nuclear) {
+        const size_t nucX = (size_t(P.lattice.nx) + kTileX - 1) / kTileX * kTileX;
+        const size_t nucY = (size_t(P.lattice.ny) + kTileY - 1) / kTileY * kTileY;
+        const size_t nucPlane = nucX * nucY, nucTiles = nucPlane / (kTileX * kTileY);
+        z.rayToNuc = rays * 4;
+        z.nucIdd = z.nucRs = chunk * S * nucPlane * 4;
+        z.nucCodes = chunk * S * nucTiles;
+        z.nucWork = chunk * S * nucTiles * sizeof(int4);
+        z.nucBev = S * (nucX + 2 * kMaxR) * (nucY + 2 * kMaxR) * 4;
+        z.nucLs = L * sizeof(LayerStateDev);
+        z.nucBs = sizeof(BeamStateDev);
+    }
+    return z;
+}
+
+size_t BeamBuffers::total() const {
+    return dens + wepl + weplMin + firstIn + firstOut + rayW + bev + codes + work + idd + rs + firstPassive + lp + ls +
+           bs + lattice + interm + subspots + cpb + rayToNuc + nucIdd + nucRs + nucCodes + nucWork + nucBev + nucLs +
+           nucBs;
+}
+
+void Context::use_stream_ordered_allocation() {
+    for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
+                      &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
+                      &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
+                      &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm,
+                      &gradLattice})
+        if (!b->ptr) b->allocStream = stream;
+}
+
+size_t Context::device_bytes() const {
+    size_t n = 0;
+    for (const DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
+                            &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive,
+                            &codes, &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf,
+                            &nucRsBuf, &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
+                            &rbarBuf, &gradInterm, &gradLattice})
+        n += b->bytes;
+    return n;
+}
+
+void Context::release_beam_buffers() {
+    for (DevBuf* b : {&dens, &wepl, &weplMin, &rayW, &interm, &lattice, &iddBuf, &rsBuf, &bev, &cpb, &subspots,
+                      &floatOut, &firstIn, &firstOut, &firstPassive, &codes, &work, &rayToNuc, &nucIddBuf, &nucRsBuf,
+                      &nucCodes, &nucWork, &nucBev, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64})
+        b->release();
+    hasDose = false;
+    lastBeamValid = false;
+}
+
+int Context::attach_ct(const float* deviceCt, const GridDesc& g, int type) {
+    if (!deviceCt) {
+        set_error("attach_ct: null CT");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    ctView = deviceCt;
+    ctGrid = g;
+    ctType = type;
+    hasCt = true;
     return PBS_OK;
 }
 
@@ -643,30 +752,22 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
 
     const int L = P.numLayers;
     const size_t S = size_t(P.tracerSteps);
-    const size_t rays = size_t(g.rayX) * g.rayY;
-    const size_t padPlane = size_t(g.pitchX) * g.pitchY;
     const size_t tiles = size_t(g.tilesX) * g.tilesY;
-    const size_t perLayer = S * padPlane * 8 + S * tiles * (1 + sizeof(int4));
-    const size_t budget = size_t(std::max<long long>(layerBudgetMiB, 1)) << 20;
-    int chunk = int(std::max<size_t>(1, std::min<size_t>(budget / std::max<size_t>(perLayer, 1), size_t(L))));
-    chunk = std::min(chunk, 64);
+    const BeamBuffers z = beam_buffers(P, b.n_subspot_data, nuclear, layerBudgetMiB);
+    const int chunk = z.chunk;
     chunkLayers = chunk;
 
-    if ((rc = dens.ensure(S * rays * 4)) || (rc = wepl.ensure(S * rays * 4)) || (rc = weplMin.ensure(S * 4)) ||
-        (rc = firstIn.ensure(rays * 4)) || (rc = firstOut.ensure(rays * 4)) || (rc = rayW.ensure(size_t(L) * rays * 4)) ||
-        (rc = bev.ensure(S * g.bevX * g.bevY * 4)) || (rc = codes.ensure(size_t(chunk) * S * tiles)) ||
-        (rc = work.ensure(size_t(chunk) * S * tiles * sizeof(int4))) ||
-        (rc = iddBuf.ensure(size_t(chunk) * S * padPlane * 4)) || (rc = rsBuf.ensure(size_t(chunk) * S * padPlane * 4)) ||
-        (rc = firstPassive.ensure(size_t(chunk) * rays * 4)) || (rc = lp.ensure(size_t(L) * sizeof(LayerParamsDev))) ||
-        (rc = ls.ensure(size_t(L) * sizeof(LayerStateDev))) || (rc = bs.ensure(sizeof(BeamStateDev))))
+    if ((rc = dens.ensure(z.dens)) || (rc = wepl.ensure(z.wepl)) || (rc = weplMin.ensure(z.weplMin)) ||
+        (rc = firstIn.ensure(z.firstIn)) || (rc = firstOut.ensure(z.firstOut)) || (rc = rayW.ensure(z.rayW)) ||
+        (rc = bev.ensure(z.bev)) || (rc = codes.ensure(z.codes)) || (rc = work.ensure(z.work)) ||
+        (rc = iddBuf.ensure(z.idd)) || (rc = rsBuf.ensure(z.rs)) || (rc = firstPassive.ensure(z.firstPassive)) ||
+        (rc = lp.ensure(z.lp)) || (rc = ls.ensure(z.ls)) || (rc = bs.ensure(z.bs)))
         return rc;
     const size_t nucPlane = size_t(g.nucX) * g.nucY, nucTiles = nucPlane / (kTileX * kTileY);
     if (nuclear &&
-        ((rc = rayToNuc.ensure(rays * 4)) || (rc = nucIddBuf.ensure(size_t(chunk) * S * nucPlane * 4)) ||
-         (rc = nucRsBuf.ensure(size_t(chunk) * S * nucPlane * 4)) || (rc = nucCodes.ensure(size_t(chunk) * S * nucTiles)) ||
-         (rc = nucWork.ensure(size_t(chunk) * S * nucTiles * sizeof(int4))) ||
-         (rc = nucBev.ensure(S * nucGeom.bevX * nucGeom.bevY * 4)) ||
-         (rc = nucLs.ensure(size_t(L) * sizeof(LayerStateDev))) || (rc = nucBs.ensure(sizeof(BeamStateDev)))))
+        ((rc = rayToNuc.ensure(z.rayToNuc)) || (rc = nucIddBuf.ensure(z.nucIdd)) || (rc = nucRsBuf.ensure(z.nucRs)) ||
+         (rc = nucCodes.ensure(z.nucCodes)) || (rc = nucWork.ensure(z.nucWork)) || (rc = nucBev.ensure(z.nucBev)) ||
+         (rc = nucLs.ensure(z.nucLs)) || (rc = nucBs.ensure(z.nucBs))))
         return rc;
     if (idd_smem_bytes(g, luts) > size_t(200) * 1024) {
         set_error("beam needs " + std::to_string(P.tracerSteps) + " tracer steps; at most ~3000 are supported");
@@ -727,13 +828,13 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
         PBS_CUDA(cudaMemcpyAsync(bs.ptr, p, sizeof(hbs), cudaMemcpyHostToDevice, stream), "H2D");
         p += sizeof(hbs);
         if (latBytes) {
-            if ((rc = lattice.ensure(latBytes)) || (rc = interm.ensure(size_t(L) * g.latNy * g.rayX * 4))) return rc;
+            if ((rc = lattice.ensure(z.lattice)) || (rc = interm.ensure(z.interm))) return rc;
             std::memcpy(p, P.lattice.weights.data(), latBytes);
             PBS_CUDA(cudaMemcpyAsync(lattice.ptr, p, latBytes, cudaMemcpyHostToDevice, stream), "H2D");
             p += latBytes;
         }
         if (subBytes) {
-            if ((rc = subspots.ensure(subBytes)) || (rc = cpb.ensure(size_t(L) * rays * 4))) return rc;
+            if ((rc = subspots.ensure(z.subspots)) || (rc = cpb.ensure(z.cpb))) return rc;
             std::memcpy(p, b.subspot_data, subBytes);
             PBS_CUDA(cudaMemcpyAsync(subspots.ptr, p, subBytes, cudaMemcpyHostToDevice, stream), "H2D");
             p += subBytes;
@@ -767,7 +868,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
 
     PBS_CUDA(cudaMemsetAsync(dBev, 0, S * g.bevX * g.bevY * 4, stream), "memset BEV");
     if ((rc = mark(0))) return rc;
-    PBS_CUDA(launch_trace(g, luts, static_cast<const float*>(ct.ptr), ctGrid.dims[0], ctGrid.dims[1], ctGrid.dims[2],
+    PBS_CUDA(launch_trace(g, luts, ctView ? ctView : static_cast<const float*>(ct.ptr), ctGrid.dims[0], ctGrid.dims[1], ctGrid.dims[2],
                           dDens, dWepl, dFi, dFo, static_cast<float*>(weplMin.ptr), dbs, stream),
              "trace");
     if ((rc = mark(1))) return rc;

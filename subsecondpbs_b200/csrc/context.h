@@ -14,10 +14,13 @@ namespace pbs {
 void set_error(const std::string& msg);
 const char* last_error();
 
-// Grow-only device allocation.
+// Grow-only device allocation; stream-ordered (cudaMallocAsync / cudaFreeAsync
+// on `allocStream`) when that stream is set, so that a resize or release does not
+// wait for the rest of the device.
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t allocStream = nullptr;
     int ensure(size_t b);
     void release();
 };
@@ -29,6 +32,17 @@ struct PinnedBuf {
     int ensure(size_t b);
     void release();
 };
+
+// Device bytes of every per-beam buffer run_beam sizes for one beam (the
+// context's buffers grow to the largest beam they have run).
+struct BeamBuffers {
+    int chunk = 1;
+    size_t dens = 0, wepl = 0, weplMin = 0, firstIn = 0, firstOut = 0, rayW = 0, bev = 0, codes = 0, work = 0, idd = 0,
+           rs = 0, firstPassive = 0, lp = 0, ls = 0, bs = 0, lattice = 0, interm = 0, subspots = 0, cpb = 0;
+    size_t rayToNuc = 0, nucIdd = 0, nucRs = 0, nucCodes = 0, nucWork = 0, nucBev = 0, nucLs = 0, nucBs = 0;
+    size_t total() const;
+};
+BeamBuffers beam_buffers(const BeamPlan& P, size_t nSubspotData, int nuclear, long long layerBudgetMiB);
 
 struct Context {
     int device = 0;
@@ -63,6 +77,9 @@ struct Context {
     int ctType = PBS_CT_AUTO;
     GridDesc ctGrid{};
     DevBuf ct;
+    // A CT owned elsewhere on the same device (a server's resident patient),
+    // used by the tracer in place of `ct` while set.
+    const float* ctView = nullptr;
     bool hasDose = false;
     GridDesc doseGrid{};
     DevBuf dose64;
@@ -77,7 +94,7 @@ struct Context {
     std::vector<float> layerSpotDist;
     // Adjoint working set.
     DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice;
-    PinnedBuf staging;
+    PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
 
@@ -108,7 +125,17 @@ struct Context {
     int reset_dose_region(const float* init, const int lo[3], const int hi[3]);
     int read_dose_region(float* out, const int lo[3], const int hi[3]);
     int convert_ct(int type, const GridDesc& g);
+    // HU+1000 conversion of `n` device floats in place, on the context stream.
+    int convert_ct_buffer(float* data, size_t n, int type);
+    // Per-beam buffers and the dose grid are allocated in stream order from here on.
+    void use_stream_ordered_allocation();
     int set_dose_grid(const GridDesc& g);
+    // Traces against a device CT (HU+1000) that the caller keeps alive.
+    int attach_ct(const float* deviceCt, const GridDesc& g, int type);
+    // Device bytes this context holds, and a release of the per-beam buffers and
+    // the dose grid (tables and the error word stay).
+    size_t device_bytes() const;
+    void release_beam_buffers();
     int reset_dose(const float* init, int onDevice);
     int read_dose(float* out, int onDevice);
     int read_dose64(double* out, int onDevice);

@@ -97,8 +97,11 @@ def heterogeneous_ct(dims, res, rng: np.random.Generator) -> np.ndarray:
     the extents) of HU N(0, 20); a lung slab N(-800, 50) and two bone cylinders
     U(700, 1200) inside it."""
     nx, ny, nz = dims
-    z, y, x = np.meshgrid(np.arange(nz, dtype=np.float32), np.arange(ny, dtype=np.float32),
-                          np.arange(nx, dtype=np.float32), indexing="ij")
+    # Broadcast coordinates ([Z][1][1], [1][Y][1], [1][1][X]) keep the masks the
+    # only full-size temporaries.
+    z = np.arange(nz, dtype=np.float32)[:, None, None]
+    y = np.arange(ny, dtype=np.float32)[None, :, None]
+    x = np.arange(nx, dtype=np.float32)[None, None, :]
     cx, cy, cz = (nx - 1) / 2.0, (ny - 1) / 2.0, (nz - 1) / 2.0
     ax, ay, az = 0.45 * nx, 0.45 * ny, 0.45 * nz
     body = ((x - cx) / ax) ** 2 + ((y - cy) / ay) ** 2 + ((z - cz) / az) ** 2 <= 1.0
@@ -280,4 +283,114 @@ def inverse_planning_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), n_beams=4, n_
     out.update({"name": "inverse_planning", "beam": beams[0], "beams": beams, "target": r <= target_radius_mm,
                 "shell": (r > target_radius_mm) & (r <= target_radius_mm + shell_mm),
                 "prescription": float(prescription_gy)})
+    return out
+
+
+# ---- serving stream (mixed CT sizes, beams, spot counts and ions) -------------
+
+SERVING_CT_CLASSES = (((128, 128, 128), (2.0, 2.0, 2.0)),
+                      ((256, 256, 160), (2.0, 2.0, 2.0)),
+                      ((512, 512, 200), (1.0, 1.0, 1.0)))
+
+
+def carbon_tables() -> dict:
+    """Synthetic carbon-ion tables (120-400 MeV/u) with their nuclear halo tables."""
+    from .tables import synthetic_carbon_tables, synthetic_nuclear_tables
+
+    if "carbon" not in _TABLE_CACHE:
+        _TABLE_CACHE["carbon"] = synthetic_nuclear_tables(synthetic_carbon_tables())
+    return _TABLE_CACHE["carbon"]
+
+
+def heavy_tailed_spots(rng: np.random.Generator, lo: int = 500, hi: int = 20000, alpha: float = 1.1) -> int:
+    """Pareto(alpha) spot count with minimum `lo`, clipped at `hi`."""
+    return int(min(hi, np.floor(lo * (1.0 - rng.uniform()) ** (-1.0 / alpha))))
+
+
+def field_beam(n_spots: int, ion: str, gantry_deg: float, rng: np.random.Generator, pitch_mm: float = 5.0,
+               sad_mm: float = 2000.0, ray_spacing: float = 1.0, n_sub: int = 7) -> dict:
+    """A coplanar field of about `n_spots` spots: n_spots/250 energy layers (4 to
+    40) of a hexagonal spot disc, proton 70-180 MeV (sigma 6 -> 3 mm) or carbon
+    120-400 MeV/u (sigma 4 -> 2 mm); unit weights (a request sets its own)."""
+    n_layers = int(np.clip(round(n_spots / 250.0), 4, 40))
+    per_layer = max(n_spots // n_layers, 7)
+    radius = float(np.sqrt(per_layer * pitch_mm * pitch_mm * np.sqrt(3.0) / 2.0 / np.pi))
+    spots = hex_spots(radius, pitch_mm)
+    e_range, s_range = ((70.0, 180.0), (6.0, 3.0)) if ion == "proton" else ((120.0, 400.0), (4.0, 2.0))
+    energies = np.linspace(e_range[0], e_range[1], n_layers).astype(np.float32)
+    sig = np.linspace(s_range[0], s_range[1], n_layers).astype(np.float32)
+    counts = np.full(n_layers, spots.shape[0], dtype=np.int32)
+    bmz = np.array([-1.0, 0.0, 0.0])
+    beam = {
+        "energies": energies,
+        "spot_sigmas": np.stack([sig, sig], axis=1),
+        "ray_spacing": (ray_spacing, ray_spacing),
+        "steps": 0,
+        "source_dist": (sad_mm, sad_mm),
+        "spot_offset": (0.0, 0.0, 0.0),
+        "spot_delta": (pitch_mm, pitch_mm * np.sqrt(3.0) / 2.0, 0.0),
+        "beam_direction": tuple(bmz),
+        "beam_xdir": (0.0, 1.0, 0.0),
+        "beam_ydir": (0.0, 0.0, 1.0),
+        "sad": sad_mm,
+        "source_position": tuple(-bmz * sad_mm),
+        "layer_spot_counts": counts,
+        "spot_positions": np.tile(spots, (n_layers, 1)).reshape(-1),
+        "spot_weights": np.ones(int(counts.sum()), np.float32),
+        "subspot_data": subspot_lut(n_layers, n_sub, sig, rng),
+    }
+    return rotate_beam(beam, gantry_deg)
+
+
+def serving_workload(n_requests: int = 1000, rate_hz: float = 100.0, patients_per_class: int = 4,
+                     fields_per_patient: int = 4, carbon_fraction: float = 0.2, seed: int = SEED_BASE + 5,
+                     ct_classes=SERVING_CT_CLASSES, max_spots: int = 20000) -> dict:
+    """Seeded stream of dose requests: patients with CTs uniform among the three
+    size classes of SERVING_CT_CLASSES (heterogeneous_ct recipe), each with
+    `fields_per_patient` coplanar fields of a heavy-tailed spot count (500-20000)
+    in a proton and a carbon variant; requests arrive as a Poisson process of
+    `rate_hz`, pick a patient uniformly, 1-4 of its fields and an ion (carbon with
+    `carbon_fraction`, with the nuclear halo). Spot weights are drawn per request
+    (`request_beams`)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    patients = []
+    for c, (dims, res) in enumerate(ct_classes):
+        for k in range(patients_per_class):
+            pid = len(patients)
+            prng = np.random.Generator(np.random.PCG64(seed + 1000 + pid))
+            dims_, res_, corner = _grid(dims, res)
+            gantries = (rng.uniform(0.0, 360.0) + 360.0 / fields_per_patient * np.arange(fields_per_patient)) % 360.0
+            fields = []
+            for g in gantries:
+                n = heavy_tailed_spots(rng, hi=max_spots)
+                fields.append({"spots": n, "gantry": float(g),
+                               "proton": field_beam(n, "proton", float(g), prng),
+                               "carbon": field_beam(n, "carbon", float(g), prng)})
+            patients.append({"id": pid, "size_class": c, "ct": heterogeneous_ct(dims_, res_, prng),
+                             "ct_dims": dims_, "ct_resolution": res_, "ct_corner": corner, "dose_dims": dims_,
+                             "dose_resolution": res_, "dose_corner": corner, "fields": fields})
+    gaps = rng.exponential(1.0 / rate_hz, size=n_requests)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    requests = []
+    for i in range(n_requests):
+        pid = int(rng.integers(len(patients)))
+        nb = int(rng.integers(1, 5))
+        nb = min(nb, fields_per_patient)
+        fids = sorted(int(f) for f in rng.choice(fields_per_patient, nb, replace=False))
+        ion = "carbon" if rng.uniform() < carbon_fraction else "proton"
+        requests.append({"index": i, "arrival_s": float(arrivals[i]), "patient": pid, "fields": fids, "ion": ion,
+                         "seed": seed + 100000 + i})
+    return {"patients": patients, "requests": requests, "rate_hz": rate_hz,
+            "energy": {"proton": proton_tables(), "carbon": carbon_tables()}}
+
+
+def request_beams(workload: dict, req: dict) -> list:
+    """The request's beams with their lognormal(0, 0.5) spot weights."""
+    rng = np.random.Generator(np.random.PCG64(req["seed"]))
+    p = workload["patients"][req["patient"]]
+    out = []
+    for f in req["fields"]:
+        b = dict(p["fields"][f][req["ion"]])
+        b["spot_weights"] = rng.lognormal(0.0, 0.5, size=b["spot_weights"].size).astype(np.float32)
+        out.append(b)
     return out

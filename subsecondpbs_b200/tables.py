@@ -205,7 +205,7 @@ def synthetic_carbon_tables(n_energies: int = 120, n_samples: int = 1024) -> dic
     e = np.linspace(120.0, 400.0, n_energies)
     ranges = alpha * e ** p
     t = _ion_tables(ranges, alpha=alpha, p=p, n_samples=n_samples, peak_index=819.0, straggle_coef=0.004,
-                    straggle_pow=0.935, fluence_loss=0.0045, tail=0.08, mev_scale=1.602e-7)
+                    straggle_pow=0.935, fluence_loss=0.002, tail=0.08, mev_scale=1.602e-7)
     t.update(hu_luts())
     return t
 
