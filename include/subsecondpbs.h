@@ -318,8 +318,9 @@ PBS_API int pbs_context_layer_stats(PbsContext* ctx, int layer, PbsLayerStats* o
  * one has waited `pbs_server_set_bypass_limit` seconds (default 0.5).
  * Patients are registered once: their CT is copied to pinned host memory, then
  * uploaded and converted to HU+1000 by the first request that needs it and kept
- * on the device for later requests; idle patients are evicted least recently
- * used first when the budget is short. Beams and tables are copied at submit and
+ * on the device for later requests, with the BEV traces of its beam geometries;
+ * idle CTs and traces are evicted least recently used first when the budget is
+ * short. Beams and tables are copied at submit and
  * registration, so the caller may free its arrays on return.
  * A result is the float [Z][Y][X] dose of the request's beams, computed as
  * pbs_context_add_beam would on a zeroed grid; `pbs_server_wait` gives a pointer
@@ -335,6 +336,9 @@ typedef struct PbsServerStats {
     long long slot_bytes;     /* device bytes held by the slots                     */
     long long peak_bytes;     /* largest committed total at an admission            */
     long long budget_bytes;
+    long long trace_hits;     /* beams that reused a resident trace                 */
+    long long trace_loads;    /* traces built and kept resident                     */
+    long long trace_evictions;
 } PbsServerStats;
 
 PBS_API int pbs_server_create(int gpu_id, int n_slots, long long hbm_budget_mib, PbsServer** out);
@@ -344,6 +348,11 @@ PBS_API int pbs_server_destroy(PbsServer* server);
  * every slot; only while no request is queued or running. */
 PBS_API int pbs_server_set_option(PbsServer* server, int option, long long value);
 PBS_API int pbs_server_set_bypass_limit(PbsServer* server, double seconds);
+/* Resident traces (on by default): the BEV trace of a beam geometry (density,
+ * WEPL, entry and exit steps) is kept per patient and reused by later beams of
+ * the same geometry and tracer tables; traces count against the budget and are
+ * evicted with the CTs, least recently used first. Only while idle. */
+PBS_API int pbs_server_set_trace_cache(PbsServer* server, int enabled);
 PBS_API int pbs_server_add_energy(PbsServer* server, int energy_id, const PbsEnergyDesc* energy);
 PBS_API int pbs_server_add_patient(PbsServer* server, int patient_id, const float* ct, const int ct_dims[3],
                                    const float ct_resolution[3], const float ct_corner[3], const int dose_dims[3],

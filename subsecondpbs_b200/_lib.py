@@ -159,7 +159,8 @@ def struct_to_dict(s: C.Structure) -> dict:
 class PbsServerStats(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in ("submitted", "completed", "failed", "queued", "running", "patient_loads",
                                             "evictions", "slot_releases", "resident_bytes", "slot_bytes",
-                                            "peak_bytes", "budget_bytes")]
+                                            "peak_bytes", "budget_bytes", "trace_hits", "trace_loads",
+                                            "trace_evictions")]
 
 
 class PbsError(RuntimeError):
@@ -218,6 +219,7 @@ def load() -> C.CDLL:
         "pbs_server_destroy": (i, [vp]),
         "pbs_server_set_option": (i, [vp, i, C.c_longlong]),
         "pbs_server_set_bypass_limit": (i, [vp, C.c_double]),
+        "pbs_server_set_trace_cache": (i, [vp, i]),
         "pbs_server_add_energy": (i, [vp, i, C.POINTER(PbsEnergyDesc)]),
         "pbs_server_add_patient": (i, [vp, i, fp, ip3, fp3, fp3, ip3, fp3, fp3]),
         "pbs_server_remove_patient": (i, [vp, i]),

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -547,10 +548,16 @@ BeamBuffers beam_buffers(const BeamPlan& P, size_t nSubspotData, int nuclear, lo
     return z;
 }
 
-size_t BeamBuffers::total() const {
-    return dens + wepl + weplMin + firstIn + firstOut + rayW + bev + codes + work + idd + rs + firstPassive + lp + ls +
-           bs + lattice + interm + subspots + cpb + rayToNuc + nucIdd + nucRs + nucCodes + nucWork + nucBev + nucLs +
-           nucBs;
+size_t BeamBuffers::total(bool withTrace) const {
+    return (withTrace ? dens + wepl + weplMin + firstIn + firstOut : 0) + rayW + bev + codes + work + idd + rs +
+           firstPassive + lp + ls + bs + lattice + interm + subspots + cpb + rayToNuc + nucIdd + nucRs + nucCodes +
+           nucWork + nucBev + nucLs + nucBs;
+}
+
+size_t trace_bytes(size_t steps, size_t rays) {
+    // dens, wepl | firstIn, firstOut | weplMin | inOut, each part 256-byte aligned
+    auto up = [](size_t n) { return (n + 255) / 256 * 256; };
+    return 2 * up(steps * rays * 4) + 2 * up(rays * 4) + up(steps * 4) + 256;
 }
 
 void Context::use_stream_ordered_allocation() {
@@ -757,11 +764,24 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
     const int chunk = z.chunk;
     chunkLayers = chunk;
 
-    if ((rc = dens.ensure(z.dens)) || (rc = wepl.ensure(z.wepl)) || (rc = weplMin.ensure(z.weplMin)) ||
-        (rc = firstIn.ensure(z.firstIn)) || (rc = firstOut.ensure(z.firstOut)) || (rc = rayW.ensure(z.rayW)) ||
-        (rc = bev.ensure(z.bev)) || (rc = codes.ensure(z.codes)) || (rc = work.ensure(z.work)) ||
-        (rc = iddBuf.ensure(z.idd)) || (rc = rsBuf.ensure(z.rs)) || (rc = firstPassive.ensure(z.firstPassive)) ||
-        (rc = lp.ensure(z.lp)) || (rc = ls.ensure(z.ls)) || (rc = bs.ensure(z.bs)))
+    // The trace's home: the store's resident copy for this geometry, else the
+    // context's own buffers.
+    trace = TraceSlot{};
+    if (traceStore && (rc = traceStore->acquire(*this, g, trace))) return rc;
+    if (!trace.dens) {
+        if ((rc = dens.ensure(z.dens)) || (rc = wepl.ensure(z.wepl)) || (rc = weplMin.ensure(z.weplMin)) ||
+            (rc = firstIn.ensure(z.firstIn)) || (rc = firstOut.ensure(z.firstOut)))
+            return rc;
+        trace.dens = static_cast<float*>(dens.ptr);
+        trace.wepl = static_cast<float*>(wepl.ptr);
+        trace.firstIn = static_cast<int*>(firstIn.ptr);
+        trace.firstOut = static_cast<int*>(firstOut.ptr);
+        trace.weplMin = static_cast<float*>(weplMin.ptr);
+    }
+    if ((rc = rayW.ensure(z.rayW)) || (rc = bev.ensure(z.bev)) || (rc = codes.ensure(z.codes)) ||
+        (rc = work.ensure(z.work)) || (rc = iddBuf.ensure(z.idd)) || (rc = rsBuf.ensure(z.rs)) ||
+        (rc = firstPassive.ensure(z.firstPassive)) || (rc = lp.ensure(z.lp)) || (rc = ls.ensure(z.ls)) ||
+        (rc = bs.ensure(z.bs)))
         return rc;
     const size_t nucPlane = size_t(g.nucX) * g.nucY, nucTiles = nucPlane / (kTileX * kTileY);
     if (nuclear &&
@@ -855,10 +875,10 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
     LayerParamsDev* dlp = static_cast<LayerParamsDev*>(lp.ptr);
     LayerStateDev* dls = static_cast<LayerStateDev*>(ls.ptr);
     BeamStateDev* dbs = static_cast<BeamStateDev*>(bs.ptr);
-    float* dDens = static_cast<float*>(dens.ptr);
-    float* dWepl = static_cast<float*>(wepl.ptr);
-    int* dFi = static_cast<int*>(firstIn.ptr);
-    int* dFo = static_cast<int*>(firstOut.ptr);
+    float* dDens = trace.dens;
+    float* dWepl = trace.wepl;
+    int* dFi = trace.firstIn;
+    int* dFo = trace.firstOut;
     float* dRayW = static_cast<float*>(rayW.ptr);
     float* dBev = static_cast<float*>(bev.ptr);
     auto mark = [&](int slot) -> int {
@@ -868,11 +888,26 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
 
     PBS_CUDA(cudaMemsetAsync(dBev, 0, S * g.bevX * g.bevY * 4, stream), "memset BEV");
     if ((rc = mark(0))) return rc;
-    PBS_CUDA(launch_trace(g, luts, ctView ? ctView : static_cast<const float*>(ct.ptr), ctGrid.dims[0], ctGrid.dims[1], ctGrid.dims[2],
-                          dDens, dWepl, dFi, dFo, static_cast<float*>(weplMin.ptr), dbs, stream),
-             "trace");
+    static_assert(offsetof(BeamStateDev, firstOutside) == offsetof(BeamStateDev, firstInside) + sizeof(int),
+                  "the trace's beam steps are two adjacent ints");
+    if (trace.traced) {
+        // A resident trace of this geometry: its beam steps replace the tracer's.
+        PBS_CUDA(cudaStreamWaitEvent(stream, trace.ready, 0), "cudaStreamWaitEvent");
+        PBS_CUDA(cudaMemcpyAsync(&dbs->firstInside, trace.inOut, 2 * sizeof(int), cudaMemcpyDeviceToDevice, stream),
+                 "trace steps D2D");
+    } else {
+        PBS_CUDA(launch_trace(g, luts, ctView ? ctView : static_cast<const float*>(ct.ptr), ctGrid.dims[0],
+                              ctGrid.dims[1], ctGrid.dims[2], dDens, dWepl, dFi, dFo, trace.weplMin, dbs, stream),
+                 "trace");
+        if (trace.inOut) {
+            PBS_CUDA(cudaMemcpyAsync(trace.inOut, &dbs->firstInside, 2 * sizeof(int), cudaMemcpyDeviceToDevice,
+                                     stream),
+                     "trace steps D2D");
+            if ((rc = traceStore->traced(*this, trace))) return rc;
+        }
+    }
     if ((rc = mark(1))) return rc;
-    PBS_CUDA(launch_beam_planner(g, static_cast<float*>(weplMin.ptr), dlp, dls, dbs, stream), "beam_planner");
+    PBS_CUDA(launch_beam_planner(g, trace.weplMin, dlp, dls, dbs, stream), "beam_planner");
     if ((rc = mark(2))) return rc;
     if (P.hasLattice) {
         PBS_CUDA(launch_conv_lattice(g, static_cast<const float*>(lattice.ptr), static_cast<float*>(interm.ptr), dRayW,
@@ -1150,11 +1185,11 @@ int Context::debug_copy(int which, int layer, void* out, size_t bytes) {
     PBS_CUDA(cudaMemcpy(&h, bs.ptr, sizeof(h), cudaMemcpyDeviceToHost), "debug D2H");
     const int first = h.firstInside;
     switch (which) {
-        case PBS_DBG_DENSITY: return copy(dens.ptr, S * rays * 4);
-        case PBS_DBG_WEPL: return copy(wepl.ptr, S * rays * 4);
-        case PBS_DBG_FIRST_INSIDE: return copy(firstIn.ptr, rays * 4);
-        case PBS_DBG_FIRST_OUTSIDE: return copy(firstOut.ptr, rays * 4);
-        case PBS_DBG_WEPL_MIN: return copy(weplMin.ptr, S * 4);
+        case PBS_DBG_DENSITY: return copy(trace.dens, S * rays * 4);
+        case PBS_DBG_WEPL: return copy(trace.wepl, S * rays * 4);
+        case PBS_DBG_FIRST_INSIDE: return copy(trace.firstIn, rays * 4);
+        case PBS_DBG_FIRST_OUTSIDE: return copy(trace.firstOut, rays * 4);
+        case PBS_DBG_WEPL_MIN: return copy(trace.weplMin, S * 4);
         case PBS_DBG_RAY_WEIGHTS: return copy(rayW.ptr, size_t(plan.numLayers) * rays * 4);
         case PBS_DBG_FIRST_PASSIVE: return copy(static_cast<char*>(firstPassive.ptr) + size_t(layer) * rays * 4, rays * 4);
         case PBS_DBG_DOSE64: {

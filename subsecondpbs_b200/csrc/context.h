@@ -40,9 +40,39 @@ struct BeamBuffers {
     size_t dens = 0, wepl = 0, weplMin = 0, firstIn = 0, firstOut = 0, rayW = 0, bev = 0, codes = 0, work = 0, idd = 0,
            rs = 0, firstPassive = 0, lp = 0, ls = 0, bs = 0, lattice = 0, interm = 0, subspots = 0, cpb = 0;
     size_t rayToNuc = 0, nucIdd = 0, nucRs = 0, nucCodes = 0, nucWork = 0, nucBev = 0, nucLs = 0, nucBs = 0;
-    size_t total() const;
+    size_t total(bool withTrace = true) const;
 };
 BeamBuffers beam_buffers(const BeamPlan& P, size_t nSubspotData, int nuclear, long long layerBudgetMiB);
+
+struct Context;
+
+// Where a beam's trace lives: density and WEPL [S][rays], per-ray entry and exit
+// steps, the per-step WEPL minimum and the beam's first-inside / first-outside
+// steps (two ints, in BeamStateDev order). A TraceStore keeps traces resident
+// across beams of the same geometry; without one the context's own buffers hold
+// the trace of its last beam.
+struct TraceSlot {
+    float* dens = nullptr;
+    float* wepl = nullptr;
+    int* firstIn = nullptr;
+    int* firstOut = nullptr;
+    float* weplMin = nullptr;
+    int* inOut = nullptr;
+    bool traced = false;          // holds the trace already: the tracer is skipped
+    cudaEvent_t ready = nullptr;  // recorded after the trace was enqueued
+};
+
+struct TraceStore {
+    virtual ~TraceStore() = default;
+    // Fills `slot` for a beam of geometry `g` (dens == nullptr: not cached, use the
+    // context's own buffers).
+    virtual int acquire(Context& c, const BeamGeomDev& g, TraceSlot& slot) = 0;
+    // The tracer into `slot` has been enqueued on the context stream.
+    virtual int traced(Context& c, TraceSlot& slot) = 0;
+};
+
+// Bytes of one beam's trace (the TraceSlot arrays).
+size_t trace_bytes(size_t steps, size_t rays);
 
 struct Context {
     int device = 0;
@@ -97,6 +127,10 @@ struct Context {
     PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
+
+    // Resident traces (a server's per-patient store), and the last beam's trace.
+    TraceStore* traceStore = nullptr;
+    TraceSlot trace;
 
     // Last beam.
     BeamPlan plan;

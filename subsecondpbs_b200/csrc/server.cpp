@@ -67,7 +67,36 @@ void OwnedEnergy::assign(const PbsEnergyDesc& e) {
     d.rrl_vector = copy_array(rrl, e.rrl_vector, e.n_rrl_vector);
     d.nuc_weight_matrix = copy_array(nucWeight, e.nuc_weight_matrix, e.n_nuc_weight_matrix);
     d.nuc_sq_sigma_matrix = copy_array(nucSqSigma, e.nuc_sq_sigma_matrix, e.n_nuc_sq_sigma_matrix);
+    // FNV-1a over everything the tracer reads from the tables.
+    unsigned long long h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    };
+    mix(density.data(), density.size() * 4);
+    mix(sp.data(), sp.size() * 4);
+    mix(&e.n_density_samples, sizeof(int));
+    mix(&e.n_sp_samples, sizeof(int));
+    mix(&e.density_scale_fact, sizeof(float));
+    mix(&e.sp_scale_fact, sizeof(float));
+    lutHash = h;
 }
+
+namespace {
+// Identity of a trace within one patient: the tracer geometry, the ray grid, the
+// step count and the tracer's tables.
+std::string trace_key(const TracerParams& t, int rayX, int rayY, int steps, unsigned long long lutHash) {
+    std::string k(reinterpret_cast<const char*>(&t), sizeof(TracerParams));
+    const int v[3] = {rayX, rayY, steps};
+    k.append(reinterpret_cast<const char*>(v), sizeof(v));
+    k.append(reinterpret_cast<const char*>(&lutHash), sizeof(lutHash));
+    return k;
+}
+}  // namespace
+
+int SlotTraces::acquire(Context&, const BeamGeomDev& g, TraceSlot& ts) { return server->trace_acquire(*slot, g, ts); }
+
+int SlotTraces::traced(Context&, TraceSlot& ts) { return server->trace_done(*slot, ts); }
 
 Server::~Server() {
     {
@@ -84,6 +113,10 @@ Server::~Server() {
         if (p.deviceCt) cudaFreeAsync(p.deviceCt, st);
         p.hostCt.release();
         if (p.ready) cudaEventDestroy(p.ready);
+        for (auto& tv : p.traces) {
+            if (tv.second->mem) cudaFreeAsync(tv.second->mem, st);
+            if (tv.second->ready) cudaEventDestroy(tv.second->ready);
+        }
     }
     if (st) cudaStreamSynchronize(st);
     for (auto& kv : requests_) kv.second->result.release();
@@ -115,6 +148,9 @@ int Server::init(int gpu, int nSlots, size_t budgetBytes) {
         int rc = s->ctx.init(gpu);
         if (rc) return rc;
         s->ctx.use_stream_ordered_allocation();
+        s->traces.server = this;
+        s->traces.slot = s.get();
+        s->ctx.traceStore = &s->traces;
         s->ctx.layerBudgetMiB = layerBudgetMiB_;
         s->ctx.nuclearModel = nuclearModel_;
         s->bytes = s->ctx.device_bytes();
@@ -142,6 +178,13 @@ int Server::set_option(int option, long long value) {
     if (option == PBS_OPT_LAYER_BUDGET_MIB) layerBudgetMiB_ = value;
     if (option == PBS_OPT_NUCLEAR_MODEL) nuclearModel_ = int(value);
     if (option == PBS_OPT_COMPAT_BEV_Z_SHIFT) compatBevZShift_ = value != 0;
+    return PBS_OK;
+}
+
+int Server::set_trace_cache(bool on) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (running_ > 0 || !queue_.empty()) return fail(PBS_ERR_NOT_READY, "server options change only while it is idle");
+    traceCache = on;
     return PBS_OK;
 }
 
@@ -205,10 +248,15 @@ int Server::remove_patient(int id) {
     if (p.pins > 0 || queued || p.state == Patient::Loading)
         return fail(PBS_ERR_NOT_READY, "patient " + std::to_string(id) + " has requests queued or running");
     cudaSetDevice(device_);
+    cudaStream_t st = slots_.front()->ctx.stream;
     if (p.deviceCt) {
         // No request uses the CT any more (every user's stream was synchronised).
-        cudaFreeAsync(p.deviceCt, slots_.front()->ctx.stream);
+        cudaFreeAsync(p.deviceCt, st);
         residentBytes_ -= p.ctBytes;
+    }
+    for (auto& tv : p.traces) {
+        if (tv.second->mem) evict_trace(*tv.second, st);
+        if (tv.second->ready) cudaEventDestroy(tv.second->ready);
     }
     p.hostCt.release();
     cudaEventDestroy(p.ready);
@@ -235,6 +283,7 @@ int Server::submit(int patientId, int energyId, const PbsBeamDesc* beams, size_t
     r->energyId = energyId;
     r->nuclear = nuclear != 0;
     r->patient = p;
+    r->energy = e;
     r->beams.resize(nBeams);
     // Device bytes of the request on a slot: tables, FP64 grid and its float copy,
     // and the largest beam's working set (the beams run one after another).
@@ -246,13 +295,20 @@ int Server::submit(int patientId, int energyId, const PbsBeamDesc* beams, size_t
         BeamPlan plan;
         int rc = plan_beam(r->beams[i].d, e->d, p->ctGrid, p->doseGrid, plan, err);
         if (rc) return fail(rc, err);
-        maxBeam = std::max(maxBeam, beam_buffers(plan, r->beams[i].d.n_subspot_data, r->nuclear, layerBudgetMiB_).total());
+        const BeamBuffers z = beam_buffers(plan, r->beams[i].d.n_subspot_data, r->nuclear, layerBudgetMiB_);
+        maxBeam = std::max(maxBeam, z.total(!traceCache));
+        if (traceCache) {
+            r->traceKeys.push_back(trace_key(plan.tracer, plan.rayDims[0], plan.rayDims[1], plan.tracerSteps, e->lutHash));
+            r->traceBytes.push_back(trace_bytes(size_t(plan.tracerSteps), size_t(plan.rayDims[0]) * plan.rayDims[1]));
+        }
     }
     const size_t tableBytes = (e->cidd.size() + e->density.size() + e->sp.size() + e->rrl.size() +
                                e->nucWeight.size() + e->nucSqSigma.size()) * 4;
     r->estBytes = maxBeam + grid_voxels(p->doseGrid) * 12 + tableBytes + 4096;
-    if (r->estBytes + p->ctBytes > budget_)
-        return fail(PBS_ERR_OUT_OF_MEMORY, "request needs " + std::to_string((r->estBytes + p->ctBytes) >> 20) +
+    size_t traceTotal = 0;
+    for (size_t b : r->traceBytes) traceTotal += b;
+    if (r->estBytes + p->ctBytes + traceTotal > budget_)
+        return fail(PBS_ERR_OUT_OF_MEMORY, "request needs " + std::to_string((r->estBytes + p->ctBytes + traceTotal) >> 20) +
                                                " MiB of device memory; the server budget is " +
                                                std::to_string(budget_ >> 20) + " MiB");
     std::lock_guard<std::mutex> lk(mu_);
@@ -273,22 +329,58 @@ size_t Server::committed_bytes() const {
     return n;
 }
 
-bool Server::make_room(size_t need, const Patient* keep, Slot& self) {
+void Server::evict_trace(TraceEntry& e, cudaStream_t st) {
+    // Every request that read the trace has completed and synchronised its stream.
+    cudaFreeAsync(e.mem, st);
+    e.mem = nullptr;
+    e.slot = TraceSlot{};
+    e.state = TraceEntry::Absent;
+    residentBytes_ -= e.bytes;
+}
+
+bool Server::make_room(size_t need, const Request& r, Slot& self) {
     size_t committed = committed_bytes();
+    const Patient* keep = r.patient;
+    auto wanted = [&](const Patient& p, const std::string& key) {
+        if (&p != keep) return false;
+        for (const std::string& k : r.traceKeys)
+            if (k == key) return true;
+        return false;
+    };
     while (committed + need > budget_) {
-        Patient* victim = nullptr;
+        // Least recently used idle CT or trace.
+        Patient* vp = nullptr;
+        TraceEntry* vt = nullptr;
+        unsigned long long oldest = ~0ull;
         for (auto& kv : patients_) {
             Patient* q = kv.second.get();
-            if (q != keep && q->state == Patient::Resident && q->pins == 0 && (!victim || q->lastUse < victim->lastUse))
-                victim = q;
+            if (q != keep && q->state == Patient::Resident && q->pins == 0 && q->lastUse < oldest) {
+                oldest = q->lastUse;
+                vp = q;
+                vt = nullptr;
+            }
+            for (auto& tv : q->traces) {
+                TraceEntry* e = tv.second.get();
+                if (e->state == TraceEntry::Ready && e->pins == 0 && e->lastUse < oldest && !wanted(*q, tv.first)) {
+                    oldest = e->lastUse;
+                    vt = e;
+                    vp = nullptr;
+                }
+            }
         }
-        if (!victim) break;
+        if (vt) {
+            committed -= vt->bytes;
+            evict_trace(*vt, self.ctx.stream);
+            ++traceEvictions_;
+            continue;
+        }
+        if (!vp) break;
         // Every request that read the CT has completed and synchronised its stream.
-        cudaFreeAsync(victim->deviceCt, self.ctx.stream);
-        victim->deviceCt = nullptr;
-        victim->state = Patient::Absent;
-        residentBytes_ -= victim->ctBytes;
-        committed -= victim->ctBytes;
+        cudaFreeAsync(vp->deviceCt, self.ctx.stream);
+        vp->deviceCt = nullptr;
+        vp->state = Patient::Absent;
+        residentBytes_ -= vp->ctBytes;
+        committed -= vp->ctBytes;
         ++evictions_;
     }
     for (auto& o : slots_) {
@@ -312,9 +404,16 @@ Request* Server::pick(Slot& s) {
         if (i > 0 && headBlocks) break;
         Request* r = queue_[i];
         Patient* p = r->patient;
+        size_t traceNeed = 0;
+        for (size_t k = 0; k < r->traceKeys.size(); ++k) {
+            bool dup = false;
+            for (size_t j = 0; j < k; ++j) dup = dup || r->traceKeys[j] == r->traceKeys[k];
+            auto it = p->traces.find(r->traceKeys[k]);
+            if (!dup && (it == p->traces.end() || it->second->state == TraceEntry::Absent)) traceNeed += r->traceBytes[k];
+        }
         const size_t need = (r->estBytes > s.bytes ? r->estBytes - s.bytes : 0) +
-                            (p->state == Patient::Absent ? p->ctBytes : 0);
-        if (committed_bytes() + need > budget_ && !make_room(need, p, s)) continue;
+                            (p->state == Patient::Absent ? p->ctBytes : 0) + traceNeed;
+        if (committed_bytes() + need > budget_ && !make_room(need, *r, s)) continue;
         queue_.erase(queue_.begin() + long(i));
         r->slot = s.index;
         r->state = 1;
@@ -326,6 +425,23 @@ Request* Server::pick(Slot& s) {
         }
         ++p->pins;
         p->lastUse = ++useClock_;
+        r->traces.assign(r->traceKeys.size(), nullptr);
+        for (size_t k = 0; k < r->traceKeys.size(); ++k) {
+            std::unique_ptr<TraceEntry>& e = p->traces[r->traceKeys[k]];
+            if (!e) {
+                e = std::make_unique<TraceEntry>();
+                e->bytes = r->traceBytes[k];
+                cudaEventCreateWithFlags(&e->ready, cudaEventDisableTiming);
+            }
+            if (e->state == TraceEntry::Absent) {
+                e->state = TraceEntry::Loading;
+                e->loader = r;
+                residentBytes_ += e->bytes;
+            }
+            ++e->pins;
+            e->lastUse = ++useClock_;
+            r->traces[k] = e.get();
+        }
         s.current = r;
         ++running_;
         peakBytes_ = std::max(peakBytes_, committed_bytes());
@@ -350,6 +466,21 @@ void Server::worker(Slot* s) {
         r->tDone = now();
         r->state = 2;
         --r->patient->pins;
+        for (TraceEntry* e : r->traces) {
+            if (!e) continue;
+            --e->pins;
+            if (e->loader == r) {
+                e->loader = nullptr;
+                if (e->state == TraceEntry::Loading) {  // the request failed before tracing
+                    if (e->mem) cudaFreeAsync(e->mem, s->ctx.stream);
+                    e->mem = nullptr;
+                    e->slot = TraceSlot{};
+                    e->state = TraceEntry::Absent;
+                    residentBytes_ -= e->bytes;
+                    cvLoad_.notify_all();
+                }
+            }
+        }
         s->current = nullptr;
         s->bytes = s->ctx.device_bytes();
         --running_;
@@ -360,6 +491,68 @@ void Server::worker(Slot* s) {
         cvDone_.notify_all();
         cvWork_.notify_all();
     }
+}
+
+int Server::trace_acquire(Slot& s, const BeamGeomDev& g, TraceSlot& ts) {
+    Request* r = s.current;
+    if (!traceCache || !r) return PBS_OK;
+    const std::string key = trace_key(g.tracer, g.rayX, g.rayY, g.steps, r->energy->lutHash);
+    TraceEntry* e = nullptr;
+    for (size_t k = 0; k < r->traceKeys.size() && !e; ++k)
+        if (r->traceKeys[k] == key) e = r->traces[k];
+    if (!e) return PBS_OK;  // not planned at submit: the context traces into its own buffers
+    std::unique_lock<std::mutex> lk(mu_);
+    if (e->state == TraceEntry::Loading && e->loader == r && !e->mem) {
+        lk.unlock();
+        const size_t rays = size_t(g.rayX) * g.rayY, S = size_t(g.steps);
+        void* mem = nullptr;
+        cudaError_t err = cudaMallocAsync(&mem, e->bytes, s.ctx.stream);
+        if (err != cudaSuccess)
+            return fail(err == cudaErrorMemoryAllocation ? PBS_ERR_OUT_OF_MEMORY : PBS_ERR_CUDA,
+                        std::string("trace allocation: ") + cudaGetErrorString(err));
+        auto up = [](size_t n) { return (n + 255) / 256 * 256; };
+        char* p = static_cast<char*>(mem);
+        TraceSlot t;
+        t.dens = reinterpret_cast<float*>(p);
+        p += up(S * rays * 4);
+        t.wepl = reinterpret_cast<float*>(p);
+        p += up(S * rays * 4);
+        t.firstIn = reinterpret_cast<int*>(p);
+        p += up(rays * 4);
+        t.firstOut = reinterpret_cast<int*>(p);
+        p += up(rays * 4);
+        t.weplMin = reinterpret_cast<float*>(p);
+        p += up(S * 4);
+        t.inOut = reinterpret_cast<int*>(p);
+        lk.lock();
+        e->mem = mem;
+        e->slot = t;
+        ++traceLoads_;
+        ts = t;
+        ts.traced = false;
+        return PBS_OK;
+    }
+    if (!cvLoad_.wait_for(lk, std::chrono::seconds(120), [&] { return e->state != TraceEntry::Loading; }))
+        return fail(PBS_ERR_TIMEOUT, "timed out waiting for a resident trace");
+    if (e->state != TraceEntry::Ready) return fail(PBS_ERR_CUDA, "a resident trace failed to build");
+    ts = e->slot;
+    ts.traced = true;
+    ts.ready = e->ready;
+    ++traceHits_;
+    return PBS_OK;
+}
+
+int Server::trace_done(Slot& s, TraceSlot& ts) {
+    Request* r = s.current;
+    TraceEntry* e = nullptr;
+    for (TraceEntry* q : r->traces)
+        if (q && q->slot.dens == ts.dens) e = q;
+    if (!e) return fail(PBS_ERR_CUDA, "trace_done: unknown trace");
+    if (cudaEventRecord(e->ready, s.ctx.stream) != cudaSuccess) return fail(PBS_ERR_CUDA, "cudaEventRecord failed");
+    std::lock_guard<std::mutex> lk(mu_);
+    e->state = TraceEntry::Ready;
+    cvLoad_.notify_all();
+    return PBS_OK;
 }
 
 int Server::ensure_resident(Slot& s, Request& r) {
@@ -535,6 +728,9 @@ void Server::stats(ServerStats* out) {
     out->patientLoads = loads_;
     out->evictions = evictions_;
     out->slotReleases = slotReleases_;
+    out->traceHits = traceHits_;
+    out->traceLoads = traceLoads_;
+    out->traceEvictions = traceEvictions_;
     out->residentBytes = residentBytes_;
     size_t sb = 0;
     for (const auto& s : slots_) sb += s->bytes;
@@ -609,6 +805,11 @@ PBS_API int pbs_server_set_bypass_limit(PbsServer* s, double seconds) {
     return PBS_OK;
 }
 
+PBS_API int pbs_server_set_trace_cache(PbsServer* s, int enabled) {
+    if (!s) return PBS_ERR_INVALID_ARGUMENT;
+    return guarded([&] { return s->server.set_trace_cache(enabled != 0); });
+}
+
 PBS_API int pbs_server_add_energy(PbsServer* s, int energy_id, const PbsEnergyDesc* energy) {
     if (!s || !energy) return PBS_ERR_INVALID_ARGUMENT;
     return guarded([&] { return s->server.add_energy(energy_id, *energy); });
@@ -674,6 +875,9 @@ PBS_API int pbs_server_stats(PbsServer* s, PbsServerStats* out) {
     out->slot_bytes = (long long)st.slotBytes;
     out->peak_bytes = (long long)st.peakBytes;
     out->budget_bytes = (long long)st.budgetBytes;
+    out->trace_hits = st.traceHits;
+    out->trace_loads = st.traceLoads;
+    out->trace_evictions = st.traceEvictions;
     return PBS_OK;
 }
 

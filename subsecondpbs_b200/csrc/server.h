@@ -38,11 +38,27 @@ struct OwnedBeam {
     void assign(const PbsBeamDesc& b);
 };
 
-// Deep copy of the lookup tables.
+// Deep copy of the lookup tables; `lutHash` identifies the HU -> density and
+// stopping-power tables the tracer uses.
 struct OwnedEnergy {
     PbsEnergyDesc d{};
     std::vector<float> energiesPerU, peakDepths, scaleFacts, cidd, density, sp, rrl, nucWeight, nucSqSigma;
+    unsigned long long lutHash = 0;
     void assign(const PbsEnergyDesc& e);
+};
+
+struct Request;
+
+// A beam geometry's trace kept resident for one patient (see TraceSlot).
+struct TraceEntry {
+    size_t bytes = 0;
+    void* mem = nullptr;
+    TraceSlot slot;
+    enum State { Absent, Loading, Ready } state = Absent;
+    cudaEvent_t ready = nullptr;
+    int pins = 0;
+    unsigned long long lastUse = 0;
+    const Request* loader = nullptr;
 };
 
 struct Patient {
@@ -57,6 +73,7 @@ struct Patient {
     int pins = 0;                   // admitted requests using the CT
     unsigned long long lastUse = 0;
     int loads = 0;
+    std::map<std::string, std::unique_ptr<TraceEntry>> traces;  // by trace_key
 };
 
 struct Request {
@@ -64,6 +81,10 @@ struct Request {
     int patientId = 0, energyId = 0, nuclear = 0;
     Patient* patient = nullptr;
     std::vector<OwnedBeam> beams;
+    const OwnedEnergy* energy = nullptr;
+    std::vector<std::string> traceKeys;   // per beam
+    std::vector<size_t> traceBytes;
+    std::vector<TraceEntry*> traces;      // pinned at admission
     size_t estBytes = 0;            // slot bytes the request needs (tables, dose grid, largest beam)
     bool loadsPatient = false;      // admitted while the patient's CT was absent
     double tSubmit = 0, tStart = 0, tEnqueued = 0, tDone = 0;
@@ -74,9 +95,20 @@ struct Request {
     PinnedBuf result;               // float [Z][Y][X] dose of the request
 };
 
+class Server;
+
+// The slot's view of the server's resident traces (Context::traceStore).
+struct SlotTraces : TraceStore {
+    Server* server = nullptr;
+    struct Slot* slot = nullptr;
+    int acquire(Context& c, const BeamGeomDev& g, TraceSlot& ts) override;
+    int traced(Context& c, TraceSlot& ts) override;
+};
+
 struct Slot {
     int index = 0;
     Context ctx;
+    SlotTraces traces;
     std::thread thread;
     Request* current = nullptr;
     size_t bytes = 0;               // device bytes the slot's context holds (updated between requests)
@@ -85,6 +117,7 @@ struct Slot {
 struct ServerStats {
     long long submitted = 0, completed = 0, failed = 0, queued = 0, running = 0;
     long long patientLoads = 0, evictions = 0, slotReleases = 0;
+    long long traceHits = 0, traceLoads = 0, traceEvictions = 0;
     size_t residentBytes = 0, slotBytes = 0, peakBytes = 0, budgetBytes = 0;
 };
 
@@ -93,6 +126,7 @@ class Server {
     ~Server();
     int init(int gpu, int nSlots, size_t budgetBytes);
     int set_option(int option, long long value);
+    int set_trace_cache(bool on);
     int add_energy(int id, const PbsEnergyDesc& e);
     int add_patient(int id, const float* ct, const GridDesc& ctGrid, const GridDesc& doseGrid);
     int remove_patient(int id);
@@ -110,11 +144,16 @@ class Server {
     double now() const;
 
     double maxBypassSec = 0.5;
+    bool traceCache = true;
+
+    int trace_acquire(Slot& s, const BeamGeomDev& g, TraceSlot& ts);
+    int trace_done(Slot& s, TraceSlot& ts);
 
    private:
     void worker(Slot* s);
     Request* pick(Slot& s);                       // mu held
-    bool make_room(size_t need, const Patient* keep, Slot& s);  // mu held
+    bool make_room(size_t need, const Request& r, Slot& s);  // mu held
+    void evict_trace(TraceEntry& e, cudaStream_t s);      // mu held
     size_t committed_bytes() const;               // mu held
     int execute(Slot& s, Request& r);
     int ensure_resident(Slot& s, Request& r);
@@ -136,7 +175,7 @@ class Server {
     unsigned long long nextTicket_ = 1, useClock_ = 0;
     size_t residentBytes_ = 0, peakBytes_ = 0;
     long long submitted_ = 0, completed_ = 0, failed_ = 0, running_ = 0, loads_ = 0, evictions_ = 0,
-              slotReleases_ = 0;
+              slotReleases_ = 0, traceHits_ = 0, traceLoads_ = 0, traceEvictions_ = 0;
     long long layerBudgetMiB_ = 2048;
     int nuclearModel_ = 2, compatBevZShift_ = 0;
 };

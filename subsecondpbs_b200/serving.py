@@ -23,13 +23,15 @@ class DoseServer:
     """Continuous-batching dose server on GPU `gpu_id` (see include/subsecondpbs.h)."""
 
     def __init__(self, gpu_id: int = 0, slots: int = 4, hbm_budget_mib: int = 0, bypass_limit_s: float | None = None,
-                 nuclear_model: int | None = None, layer_budget_mib: int | None = None):
+                 nuclear_model: int | None = None, layer_budget_mib: int | None = None, trace_cache: bool = True):
         self._lib = _lib.load()
         h = C.c_void_p()
         _lib.check(self._lib.pbs_server_create(gpu_id, slots, hbm_budget_mib, C.byref(h)))
         self._h = h
         self._patients: dict[int, tuple] = {}
         self._keep: dict[int, object] = {}
+        if not trace_cache:
+            _lib.check(self._lib.pbs_server_set_trace_cache(self._h, 0))
         if bypass_limit_s is not None:
             _lib.check(self._lib.pbs_server_set_bypass_limit(self._h, float(bypass_limit_s)))
         if nuclear_model is not None:

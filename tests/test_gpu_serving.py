@@ -80,6 +80,12 @@ def test_results_same_alone_and_in_the_mix(workload):
         st = srv.stats()
         assert st["failed"] == 0 and st["completed"] == 2 * len(w["requests"])
         assert st["patient_loads"] == len(w["patients"])  # loaded once, then resident
+        # Every field geometry (the ion changes the ray grid and the steps) is traced
+        # once; later beams reuse the resident trace.
+        n_fields = len({(r["patient"], f, r["ion"]) for r in w["requests"] for f in r["fields"]})
+        n_beams = sum(len(r["fields"]) for r in w["requests"])
+        assert st["trace_loads"] == n_fields
+        assert st["trace_hits"] == 2 * n_beams - n_fields
 
 
 def test_poisson_arrivals_overlap_on_the_device(workload):
@@ -90,23 +96,32 @@ def test_poisson_arrivals_overlap_on_the_device(workload):
     assert res["plans_per_s"] > 0 and np.all(res["latency_s"] > 0)
 
 
-def test_budget_evicts_idle_patients(workload):
+@pytest.mark.parametrize("trace_cache", [False, True])
+def test_budget_evicts_idle_patients(workload, trace_cache):
     w = workload
     prepared = [[_lib.beam_desc(b) for b in phantoms.request_beams(w, r)] for r in w["requests"]]
     ref = _alone(w)
-    # One slot and room for the largest request plus one or two patient CTs, not
-    # for all of them.
-    ct_bytes = max(int(np.prod(p["ct_dims"])) * 4 for p in w["patients"])
-    with _server(w, slots=1) as probe:
+    ct_all = sum(int(np.prod(p["ct_dims"])) * 4 for p in w["patients"])
+    ct_max = max(int(np.prod(p["ct_dims"])) * 4 for p in w["patients"])
+    with _server(w, slots=1, trace_cache=trace_cache) as probe:
         serving.serve_workload(probe, w, prepared, arrivals=False)
-        per_slot = probe.stats()["slot_bytes"]  # the slot grown to the largest request
-    budget_mib = int(np.ceil((per_slot + 1.6 * ct_bytes) / 2**20))
-    with _server(w, slots=1, hbm_budget_mib=budget_mib) as srv:
+        st0 = probe.stats()
+    per_slot = st0["slot_bytes"]  # the slot grown to the largest request
+    traces_all = st0["resident_bytes"] - ct_all
+    # One slot and room for the largest request plus part of the CTs and traces.
+    if trace_cache:
+        budget = per_slot + ct_all + 0.5 * traces_all
+    else:
+        budget = per_slot + 1.6 * ct_max
+    with _server(w, slots=1, hbm_budget_mib=int(np.ceil(budget / 2**20)), trace_cache=trace_cache) as srv:
         res = serving.serve_workload(srv, w, prepared, arrivals=False, keep=set(range(len(w["requests"]))))
         st = srv.stats()
     for i, d in res["doses"].items():
         _assert_same(d, ref[i], ("budget", i))
-    assert st["evictions"] > 0 and st["patient_loads"] > len(w["patients"]), st
+    if trace_cache:
+        assert st["trace_evictions"] > 0 and st["trace_loads"] > st0["trace_loads"], st
+    else:
+        assert st["evictions"] > 0 and st["patient_loads"] > len(w["patients"]), st
     assert st["peak_bytes"] <= st["budget_bytes"], st
 
 
