@@ -497,6 +497,10 @@ typedef struct {
     TracerP tracer;
     float volConst, volLin, volSq;
     float* lp; /* [L][8] */
+    /* Water-equivalence import (wrapper.cu:3316-3395, 3566-3640). */
+    int weq, weqNx, weqNy, weqSteps, weqActive;
+    float weqStepMm, weqX0, weqY0, weqDx, weqDy;
+    const float* weqBody;
 } Plan;
 
 static void free_plan(Plan* P) {
@@ -674,13 +678,44 @@ static int plan_beam(const PbsBeamDesc* b, const PbsEnergyDesc* e, const int* cd
                     maxGZ = fmaxf(maxGZ, g.z);
                 }
     }
-    if (nh >= 9 && b->water_equivalence && b->n_water_equivalence > 9)
-        return fail(PBS_ERR_UNSUPPORTED, "water-equivalence import transport is not modelled by the oracle");
-    float stepMm = cr[2] * lenToMm;
-    int steps = (int)ceilf((maxGZ - minGZ) / fabsf(stepMm)) + 1;
-    if (steps < 1) steps = 1;
+    const int hasWeq = nh >= 9 && b->water_equivalence && b->n_water_equivalence > 9;
+    float stepMm = hasWeq ? hdr[1] * lenToMm : cr[2] * lenToMm;
+    if (!(stepMm > 0.0f)) stepMm = cr[2] * lenToMm;
+    float startZ = maxGZ;
+    int steps;
+    P->weq = hasWeq;
+    if (hasWeq) {
+        /* BEV start plane at the exporter's projected WEQ origin when it is positive,
+         * finite and within max(WEQ depth span, 50 mm) of the CT start
+         * (wrapper.cu:3316-3364); steps from the header (wrapper.cu:3365-3367). */
+        float weqStart = hdr[0] * lenToMm;
+        float aligned = 0.5f * (distX + distY) - weqStart;
+        long hs = lroundf(hdr[2]);
+        float span = fabsf(hdr[1] * lenToMm) * (float)(hs > 0 ? hs : 0);
+        float maxDelta = span > 50.0f ? span : 50.0f;
+        if (isfinite(aligned) && isfinite(weqStart) && weqStart > 0.0f && fabsf(aligned - maxGZ) <= maxDelta)
+            startZ = aligned;
+        steps = (int)lroundf(hdr[2]);
+        if (steps < 1) steps = 1;
+        P->weqSteps = steps;
+        P->weqNy = (int)lroundf(hdr[5]); if (P->weqNy < 1) P->weqNy = 1;
+        P->weqNx = (int)lroundf(hdr[8]); if (P->weqNx < 1) P->weqNx = 1;
+        /* Only nx*ny*nStep samples are depths (wrapper.cu:3566-3590). */
+        if (b->n_water_equivalence - 9 < (size_t)P->weqNx * P->weqNy * P->weqSteps)
+            return fail(PBS_ERR_GEOMETRY, "water_equivalence payload is smaller than header-declared nx*ny*nStep");
+        P->weqActive = steps < P->weqSteps ? steps : P->weqSteps;
+        P->weqStepMm = fabsf(hdr[1] * lenToMm);
+        P->weqX0 = hdr[6] / lenToMm;
+        P->weqY0 = hdr[3] / lenToMm;
+        P->weqDx = hdr[7] / lenToMm;
+        P->weqDy = hdr[4] / lenToMm;
+        P->weqBody = b->water_equivalence + 9;
+    } else {
+        steps = (int)ceilf((maxGZ - minGZ) / fabsf(stepMm)) + 1;
+        if (steps < 1) steps = 1;
+    }
     P->p.steps = steps;
-    V3 fanCorner = v3(cpbCorner.x * lenToMm, cpbCorner.y * lenToMm, maxGZ);
+    V3 fanCorner = v3(cpbCorner.x * lenToMm, cpbCorner.y * lenToMm, startZ);
     V3 fanDelta = v3(cpbRes.x * lenToMm, cpbRes.y * lenToMm, -fabsf(stepMm));
     P->p.fan_corner[0] = fanCorner.x; P->p.fan_corner[1] = fanCorner.y; P->p.fan_corner[2] = fanCorner.z;
     P->p.fan_delta[0] = fanDelta.x; P->p.fan_delta[1] = fanDelta.y; P->p.fan_delta[2] = fanDelta.z;
@@ -987,6 +1022,42 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
     double* wepl = (double*)malloc(sizeof(double) * S * rays);
     int* fin = (int*)malloc(sizeof(int) * rays);
     int* fout = (int*)malloc(sizeof(int) * rays);
+    if (P->weq) {
+        /* fillBevFromWeqVolumeKernel (wrapper.cu:1923-1989): the ray at
+         * origin + index * spacing reads its nearest WEQ texel ([nx][ny][steps],
+         * depth fastest); density is the per-step depth increase over the WEQ step;
+         * entry/exit from the first/last step with density above 1e-4. */
+        const float safeStep = P->weqStepMm > 0.0f ? P->weqStepMm : 1.0f;
+        for (int y = 0; y < RY; ++y)
+            for (int x = 0; x < RX; ++x) {
+                const float rx = P->p.cpb_corner[0] + (float)x * P->p.cpb_res[0];
+                const float ry = P->p.cpb_corner[1] + (float)y * P->p.cpb_res[1];
+                const int wx = fabsf(P->weqDx) > 0.0f ? (int)lroundf((rx - P->weqX0) / P->weqDx) : -1;
+                const int wy = fabsf(P->weqDy) > 0.0f ? (int)lroundf((ry - P->weqY0) / P->weqDy) : -1;
+                const int inside = wx >= 0 && wx < P->weqNx && wy >= 0 && wy < P->weqNy;
+                float prev = 0.0f, last = 0.0f;
+                int firstMat = -1, lastMat = -1;
+                size_t idx = (size_t)y * RX + x;
+                for (int k = 0; k < S; ++k) {
+                    float w = last;
+                    if (inside && k < P->weqActive) {
+                        w = P->weqBody[((size_t)wx * P->weqNy + wy) * P->weqSteps + k];
+                        last = w;
+                    }
+                    const float d = fmaxf(0.0f, w - prev) / safeStep;
+                    wepl[idx] = w;
+                    dens[idx] = d;
+                    if (d > 1.0e-4f) {
+                        if (firstMat < 0) firstMat = k;
+                        lastMat = k;
+                    }
+                    prev = w;
+                    idx += rays;
+                }
+                fin[(size_t)y * RX + x] = firstMat >= 0 ? firstMat + 1 : S;
+                fout[(size_t)y * RX + x] = lastMat >= 0 ? lastMat + 1 : 0;
+            }
+    } else
     /* Trace (bev_ray_tracing.cu:65-159) with double sums; sample points advance by
      * repeated single-precision additions as in the reference. */
 #pragma omp parallel for schedule(dynamic, 4)

@@ -92,7 +92,7 @@ Context::~Context() {
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad, &rbarBuf,
-                      &gradInterm, &gradLattice})
+                      &gradInterm, &gradLattice, &weqBody})
         b->release();
     staging.release();
     errHost.release();
@@ -565,7 +565,7 @@ void Context::use_stream_ordered_allocation() {
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm,
-                      &gradLattice})
+                      &gradLattice, &weqBody})
         if (!b->ptr) b->allocStream = stream;
 }
 
@@ -575,7 +575,7 @@ size_t Context::device_bytes() const {
                             &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive,
                             &codes, &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf,
                             &nucRsBuf, &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
-                            &rbarBuf, &gradInterm, &gradLattice})
+                            &rbarBuf, &gradInterm, &gradLattice, &weqBody})
         n += b->bytes;
     return n;
 }
@@ -583,7 +583,8 @@ size_t Context::device_bytes() const {
 void Context::release_beam_buffers() {
     for (DevBuf* b : {&dens, &wepl, &weplMin, &rayW, &interm, &lattice, &iddBuf, &rsBuf, &bev, &cpb, &subspots,
                       &floatOut, &firstIn, &firstOut, &firstPassive, &codes, &work, &rayToNuc, &nucIddBuf, &nucRsBuf,
-                      &nucCodes, &nucWork, &nucBev, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64})
+                      &nucCodes, &nucWork, &nucBev, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64,
+                      &weqBody})
         b->release();
     hasDose = false;
     lastBeamValid = false;
@@ -767,7 +768,8 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
     // The trace's home: the store's resident copy for this geometry, else the
     // context's own buffers.
     trace = TraceSlot{};
-    if (traceStore && (rc = traceStore->acquire(*this, g, trace))) return rc;
+    // A WEQ beam's trace is its own input, not a function of the geometry: never shared.
+    if (traceStore && !P.hasWeqVolume && (rc = traceStore->acquire(*this, g, trace))) return rc;
     if (!trace.dens) {
         if ((rc = dens.ensure(z.dens)) || (rc = wepl.ensure(z.wepl)) || (rc = weplMin.ensure(z.weplMin)) ||
             (rc = firstIn.ensure(z.firstIn)) || (rc = firstOut.ensure(z.firstOut)))
@@ -895,6 +897,17 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
         PBS_CUDA(cudaStreamWaitEvent(stream, trace.ready, 0), "cudaStreamWaitEvent");
         PBS_CUDA(cudaMemcpyAsync(&dbs->firstInside, trace.inOut, 2 * sizeof(int), cudaMemcpyDeviceToDevice, stream),
                  "trace steps D2D");
+    } else if (P.hasWeqVolume) {
+        // Water-equivalence import: the exporter's depths replace the CT trace.
+        const size_t weqN = size_t(P.weqNx) * P.weqNy * P.weqSteps;
+        if ((rc = weqBody.ensure(weqN * 4))) return rc;
+        PBS_CUDA(cudaMemcpyAsync(weqBody.ptr, b.water_equivalence + 9, weqN * 4, cudaMemcpyHostToDevice, stream),
+                 "WEQ H2D");
+        PBS_CUDA(launch_weq_trace(g, static_cast<const float*>(weqBody.ptr), P.weqNx, P.weqNy, P.weqSteps,
+                                  P.weqActiveSteps, P.weqStepMm, P.cpbCorner.x, P.cpbCorner.y, P.cpbRes.x, P.cpbRes.y,
+                                  P.weqX0, P.weqY0, P.weqDx, P.weqDy, dDens, dWepl, dFi, dFo, trace.weplMin, dbs,
+                                  stream),
+                 "weq_trace");
     } else {
         PBS_CUDA(launch_trace(g, luts, ctView ? ctView : static_cast<const float*>(ct.ptr), ctGrid.dims[0],
                               ctGrid.dims[1], ctGrid.dims[2], dDens, dWepl, dFi, dFo, trace.weplMin, dbs, stream),

@@ -122,8 +122,8 @@ struct Context {
     BeamGeomDev nucGeom{};
     bool lastNuclear = false;
     std::vector<float> layerSpotDist;
-    // Adjoint working set.
-    DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice;
+    // Adjoint working set, and the imported water-equivalence volume of a beam.
+    DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice, weqBody;
     PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};

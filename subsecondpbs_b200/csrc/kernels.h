@@ -24,6 +24,13 @@ cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float*
                          BeamStateDev* beam, cudaStream_t s);
 // Beam planner: guaranteed passive step, entry plane, per-layer cut-off steps and
 // entry sigmas (wrapper.cu:3651-3700, 3733-3833, 4302-4313).
+// fillBevFromWeqVolumeKernel + sliceMinVarIgnoreNeverEnter (wrapper.cu:1923-2023):
+// the exporter's water-equivalent depths [nx][ny][storedSteps] in place of the CT
+// trace, with the per-step minimum over entering rays.
+cudaError_t launch_weq_trace(const BeamGeomDev& g, const float* body, int nx, int ny, int storedSteps,
+                             int activeSteps, float stepMm, float rayOriginX, float rayOriginY, float rayStepX,
+                             float rayStepY, float x0, float y0, float dx, float dy, float* density, float* wepl,
+                             int* firstInside, int* firstOutside, float* weplMin, BeamStateDev* beam, cudaStream_t s);
 cudaError_t launch_beam_planner(const BeamGeomDev& g, float* weplMin, const LayerParamsDev* lp,
                                 LayerStateDev* ls, BeamStateDev* beam, cudaStream_t s);
 

@@ -770,15 +770,43 @@ int plan_beam(const PbsBeamDesc& b, const PbsEnergyDesc& e, const GridDesc& ctGr
     P.minGZ = minGZ;
     P.maxGZ = maxGZ;
     const bool hasWeqVolume = hasHdr && b.water_equivalence && b.n_water_equivalence > 9;
-    if (hasWeqVolume) {
-        err = "water-equivalence (WEQ) import transport is not available in this build";
-        return PBS_ERR_UNSUPPORTED;
-    }
-    float stepMm = ctGrid.res[2] * lenToMm;
+    float stepMm = hasWeqVolume ? hdr[1] * lenToMm : ctGrid.res[2] * lenToMm;
     if (!(stepMm > 0.0f)) stepMm = ctGrid.res[2] * lenToMm;
     P.stepLengthMm = stepMm;
     P.startZ = maxGZ;
-    P.tracerSteps = std::max(1, static_cast<int>(std::ceil((maxGZ - minGZ) / std::fabs(stepMm))) + 1);
+    P.hasWeqVolume = hasWeqVolume;
+    if (hasWeqVolume) {
+        // The BEV start plane follows the exporter's projected WEQ origin when that
+        // origin is positive, finite and within the WEQ depth span (at least 5 cm)
+        // of the CT-derived start (wrapper.cu:3316-3364).
+        const float weqStartMm = hdr[0] * lenToMm;
+        const float aligned = 0.5f * (distX + distY) - weqStartMm;
+        const float span = std::fabs(hdr[1] * lenToMm) * static_cast<float>(std::max(0L, std::lround(hdr[2])));
+        if (std::isfinite(aligned) && std::isfinite(weqStartMm) && weqStartMm > 0.0f &&
+            std::fabs(aligned - maxGZ) <= std::max(span, 50.0f)) {
+            P.startZ = aligned;
+            P.startAlignedToWeq = true;
+        }
+        P.tracerSteps = std::max(1, static_cast<int>(std::lround(hdr[2])));
+        P.weqSteps = P.tracerSteps;
+        P.weqNy = std::max(1, static_cast<int>(std::lround(hdr[5])));
+        P.weqNx = std::max(1, static_cast<int>(std::lround(hdr[8])));
+        // Only the header's nx*ny*nStep samples are depths; a longer payload is
+        // preallocated capacity (wrapper.cu:3566-3590).
+        const size_t need = size_t(P.weqNx) * size_t(P.weqNy) * size_t(P.weqSteps);
+        if (b.n_water_equivalence - 9 < need) {
+            err = "water_equivalence payload is smaller than header-declared nx*ny*nStep";
+            return PBS_ERR_GEOMETRY;
+        }
+        P.weqActiveSteps = std::min(P.tracerSteps, P.weqSteps);
+        P.weqStepMm = std::fabs(hdr[1] * lenToMm);
+        P.weqX0 = hdr[6] / lenToMm;
+        P.weqY0 = hdr[3] / lenToMm;
+        P.weqDx = hdr[7] / lenToMm;
+        P.weqDy = hdr[4] / lenToMm;
+    } else {
+        P.tracerSteps = std::max(1, static_cast<int>(std::ceil((maxGZ - minGZ) / std::fabs(stepMm))) + 1);
+    }
 
     P.fanCorner = v3(P.cpbCorner.x * lenToMm, P.cpbCorner.y * lenToMm, P.startZ);
     P.fanDelta = v3(P.cpbRes.x * lenToMm, P.cpbRes.y * lenToMm, -std::fabs(stepMm));

@@ -71,6 +71,14 @@ struct BeamPlan {
     float volConst = 0.f, volLin = 0.f, volSq = 0.f;
     float maxPeakDepthMm = 0.f;
     std::vector<LayerHost> layers;
+    // Water-equivalence import transport (wrapper.cu:3316-3395, 3566-3640): the
+    // exporter's per-ray water-equivalent depths [weqNx][weqNy][weqSteps] replace
+    // the CT trace. Lattice origin and spacing are in beam length units.
+    bool hasWeqVolume = false;
+    bool startAlignedToWeq = false;
+    int weqNx = 0, weqNy = 0, weqSteps = 0, weqActiveSteps = 0;
+    float weqStepMm = 1.f;
+    float weqX0 = 0.f, weqY0 = 0.f, weqDx = 0.f, weqDy = 0.f;
 };
 
 // wrapper.cu:1025-1075 (+ the LUT sample counts the textures are built with).

@@ -297,7 +297,7 @@ int Server::submit(int patientId, int energyId, const PbsBeamDesc* beams, size_t
         if (rc) return fail(rc, err);
         const BeamBuffers z = beam_buffers(plan, r->beams[i].d.n_subspot_data, r->nuclear, layerBudgetMiB_);
         maxBeam = std::max(maxBeam, z.total(!traceCache));
-        if (traceCache) {
+        if (traceCache && !plan.hasWeqVolume) {
             r->traceKeys.push_back(trace_key(plan.tracer, plan.rayDims[0], plan.rayDims[1], plan.tracerSteps, e->lutHash));
             r->traceBytes.push_back(trace_bytes(size_t(plan.tracerSteps), size_t(plan.rayDims[0]) * plan.rayDims[1]));
         }

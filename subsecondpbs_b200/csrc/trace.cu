@@ -182,6 +182,144 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
     }
 }
 
+// ---- water-equivalence import transport -------------------------------------
+// fillBevFromWeqVolumeKernel (wrapper.cu:1923-1989): the exporter's per-ray water-
+// equivalent depths replace the CT trace. Ray (x, y) at (origin + index * ray
+// spacing) reads the WEQ texel nearest to it (body [nx][ny][steps], depth fastest);
+// WEPL is that depth, density its per-step increase divided by the WEQ step, and
+// the ray enters at its first step with density above 1e-4 (firstInside = that
+// step + 1, else `steps`) and leaves after its last (firstOutside = last + 1, else 0).
+// A ray outside the WEQ lattice keeps depth 0; steps beyond the active ones keep the
+// last depth read.
+//
+// Layout: one CTA per 32 consecutive rays (ray index y * rayX + x). Depths are read
+// depth-fastest (one warp per ray and 32-step chunk, coalesced) and written
+// ray-fastest ([step][ray], coalesced) through a 32 x 33 shared tile.
+struct WeqParams {
+    const float* body;
+    int nx, ny, storedSteps, activeSteps;
+    float stepMm;
+    float rayOriginX, rayOriginY, rayStepX, rayStepY;
+    float x0, y0, dx, dy;
+};
+
+constexpr int kWeqRaysPerCta = 32;
+
+__global__ void __launch_bounds__(256)
+weq_fill_kernel(BeamGeomDev g, WeqParams q, float* __restrict__ density, float* __restrict__ wepl,
+                int* __restrict__ firstInside, int* __restrict__ firstOutside, BeamStateDev* __restrict__ beam) {
+    __shared__ float tile[32][33];
+    __shared__ float carry[32];
+    __shared__ long long base[kWeqRaysPerCta];
+    __shared__ int sFirst[8][32], sLast[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int rays = g.rayX * g.rayY, S = g.steps;
+    const int r0 = blockIdx.x * kWeqRaysPerCta;
+    const float safeStep = q.stepMm > 0.0f ? q.stepMm : 1.0f;
+    if (w == 0) {
+        long long b = -1;
+        const int r = r0 + lane;
+        if (r < rays) {
+            const int x = r % g.rayX, y = r / g.rayX;
+            const float rx = fmaf(float(x), q.rayStepX, q.rayOriginX);
+            const float ry = fmaf(float(y), q.rayStepY, q.rayOriginY);
+            const int wx = fabsf(q.dx) > 0.0f ? int(lroundf((rx - q.x0) / q.dx)) : -1;
+            const int wy = fabsf(q.dy) > 0.0f ? int(lroundf((ry - q.y0) / q.dy)) : -1;
+            if (wx >= 0 && wx < q.nx && wy >= 0 && wy < q.ny)
+                b = (static_cast<long long>(wx) * q.ny + wy) * q.storedSteps;
+        }
+        base[lane] = b;
+        carry[lane] = 0.0f;
+    }
+    __syncthreads();
+    int first = INT_MAX, last = -1;
+    const size_t plane = static_cast<size_t>(rays);
+    for (int k0 = 0; k0 < S; k0 += 32) {
+#pragma unroll
+        for (int j = 0; j < kWeqRaysPerCta / 8; ++j) {
+            const int ray = w * (kWeqRaysPerCta / 8) + j;
+            const long long b = base[ray];
+            const int k = min(k0 + lane, q.activeSteps - 1);
+            tile[lane][ray] = (b >= 0 && k >= 0) ? q.body[b + k] : 0.0f;
+        }
+        __syncthreads();
+        const int r = r0 + lane;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int kk = w + 8 * i, k = k0 + kk;
+            if (k < S && r < rays) {
+                const float v = tile[kk][lane];
+                const float prev = kk > 0 ? tile[kk - 1][lane] : carry[lane];
+                const float d = fmaxf(0.0f, v - prev) / safeStep;
+                wepl[static_cast<size_t>(k) * plane + r] = v;
+                density[static_cast<size_t>(k) * plane + r] = d;
+                if (d > 1.0e-4f) {
+                    first = min(first, k);
+                    last = max(last, k);
+                }
+            }
+        }
+        __syncthreads();
+        if (w == 0) carry[lane] = tile[31][lane];
+        __syncthreads();
+    }
+    sFirst[w][lane] = first;
+    sLast[w][lane] = last;
+    __syncthreads();
+    if (w == 0) {
+        int fk = INT_MAX, lk = -1;
+        for (int q8 = 0; q8 < 8; ++q8) {
+            fk = min(fk, sFirst[q8][lane]);
+            lk = max(lk, sLast[q8][lane]);
+        }
+        const int r = r0 + lane;
+        const bool active = r < rays;
+        const int fi = fk == INT_MAX ? S : fk + 1;
+        const int fo = lk >= 0 ? lk + 1 : 0;
+        if (active) {
+            firstInside[r] = fi;
+            firstOutside[r] = fo;
+        }
+        int wmin = active ? fi : INT_MAX, wmax = active ? fo : INT_MIN;
+        for (int o = 16; o > 0; o >>= 1) {
+            wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+            wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+        }
+        if (lane == 0) {
+            atomicMin(&beam->firstInside, wmin);
+            atomicMax(&beam->firstOutside, wmax);
+        }
+    }
+}
+
+// sliceMinVarIgnoreNeverEnter (wrapper.cu:1991-2023): per step the minimum WEPL
+// over the rays that enter (firstOutside > 0), 1e20 where none does. One CTA per
+// step, reading the step's rays contiguously.
+__global__ void __launch_bounds__(256)
+weq_step_min_kernel(BeamGeomDev g, const float* __restrict__ wepl, const int* __restrict__ firstOutside,
+                    float* __restrict__ weplMin) {
+    __shared__ float red[8];
+    const int rays = g.rayX * g.rayY;
+    const float* row = wepl + static_cast<size_t>(blockIdx.x) * rays;
+    float m = kInf20;
+    for (int r = threadIdx.x; r < rays; r += blockDim.x)
+        if (firstOutside[r] > 0) {
+            const float v = row[r];
+            if (v < m) m = v;
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float other = __shfl_xor_sync(0xffffffffu, m, o);
+        if (other < m) m = other;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < 8; ++i)
+            if (red[i] < m) m = red[i];
+        weplMin[blockIdx.x] = m;
+    }
+}
+
 // include/utils/vector_find.h:61-82
 __device__ int find_first_larger_ordered_dev(const float* v, int n, float value) {
     int upper = n - 1, lower = 0;
@@ -356,6 +494,21 @@ cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float*
         trace_kernel<false><<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside,
                                                    firstOutside, mins, beam);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_weq_trace(const BeamGeomDev& g, const float* body, int nx, int ny, int storedSteps,
+                             int activeSteps, float stepMm, float rayOriginX, float rayOriginY, float rayStepX,
+                             float rayStepY, float x0, float y0, float dx, float dy, float* density, float* wepl,
+                             int* firstInside, int* firstOutside, float* weplMin, BeamStateDev* beam, cudaStream_t s) {
+    WeqParams q{body, nx, ny, storedSteps, activeSteps, stepMm, rayOriginX, rayOriginY, rayStepX, rayStepY,
+                x0, y0, dx, dy};
+    const int rays = g.rayX * g.rayY;
+    weq_fill_kernel<<<(rays + kWeqRaysPerCta - 1) / kWeqRaysPerCta, 256, 0, s>>>(g, q, density, wepl, firstInside,
+                                                                                  firstOutside, beam);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    weq_step_min_kernel<<<g.steps, 256, 0, s>>>(g, wepl, firstOutside, weplMin);
     return cudaGetLastError();
 }
 

@@ -394,3 +394,63 @@ def request_beams(workload: dict, req: dict) -> list:
         b["spot_weights"] = rng.lognormal(0.0, 0.5, size=b["spot_weights"].size).astype(np.float32)
         out.append(b)
     return out
+
+
+# ---- water-equivalence import (CarbonPBS rayweq) -------------------------------
+
+def weq_volume(n_xy: int, pitch_mm: float, n_steps: int, step_mm: float, rng: np.random.Generator) -> tuple:
+    """Synthetic exporter depths in beam's-eye coordinates: per lateral texel (u, v)
+    (pitch_mm apart, centred on the beam axis) and depth t = (k + 1) * step_mm from
+    the start plane, relative stopping power 0 in air before a curved skin surface
+    t_in = 30 mm + (u^2 + v^2) / 500 mm, 1.0 +- 1 % in tissue, 0.25 in a lung band
+    (v > 8 mm, 20 mm to 50 mm past the skin) and 1.7 in a bone slab (|u - 6| < 5 mm,
+    35 mm to 45 mm past the skin); the depth is the running sum of rsp * step_mm.
+    Returns (weq [nx][ny][steps] float32, lateral origin mm)."""
+    x0 = -0.5 * (n_xy - 1) * pitch_mm
+    u = (x0 + pitch_mm * np.arange(n_xy))[:, None, None]
+    v = (x0 + pitch_mm * np.arange(n_xy))[None, :, None]
+    t = ((np.arange(n_steps) + 1) * step_mm)[None, None, :]
+    t_in = 30.0 + (u * u + v * v) / 500.0
+    past = t - t_in
+    rsp = np.where(past >= 0.0, 1.0 + 0.01 * rng.standard_normal((n_xy, n_xy, 1)), 0.0)
+    rsp = np.where((v > 8.0) & (past >= 20.0) & (past < 50.0), 0.25, rsp)
+    rsp = np.where((np.abs(u - 6.0) < 5.0) & (past >= 35.0) & (past < 45.0), 1.7, rsp)
+    weq = np.cumsum(rsp * step_mm, axis=2).astype(np.float32)
+    return weq, float(x0)
+
+
+def weq_case(dims=(64, 64, 48), res=(2.0, 2.0, 2.0), n_layers=3, e_range=(80.0, 120.0), target_radius_mm=14.0,
+             hex_pitch_mm=5.0, sigma_range=(6.0, 3.0), sad_mm=2000.0, ray_mm=1.0, n_sub=7, index_positions=True,
+             seed=SEED_BASE + 6) -> dict:
+    """A beam driven by an imported water-equivalence volume (the CarbonPBS rayweq
+    contract): the heterogeneous_case CT fixes the dose grid and the beam geometry,
+    and `water_equivalence` = the 9-value header [depth0, step, nSteps, y0, dy, ny,
+    x0, dx, nx] followed by weq_volume's depths. The header's depth origin and step
+    are the CT plan's start plane and step, so the BEV start plane stays where the CT
+    would put it. With index_positions the spot positions are rayweq texel
+    coordinates (texel i centred at i + 0.5), as CarbonPBS exports them."""
+    from .cudaCalDoseRTD import plan_beam
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    case = heterogeneous_case(dims=dims, res=res, n_layers=n_layers, e_range=e_range,
+                              target_radius_mm=target_radius_mm, hex_pitch_mm=hex_pitch_mm, sigma_range=sigma_range,
+                              sad_mm=sad_mm, ray_spacing=ray_mm, n_sub=n_sub, seed=seed)
+    beam = dict(case["beam"])
+    st = plan_beam(beam, case["energy"], case["ct_dims"], case["ct_resolution"], case["ct_corner"],
+                   case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    step = abs(float(st["fan_delta"][2]))
+    n_steps = int(st["tracer_steps"])
+    depth0 = 0.5 * (float(st["source_dist"][0]) + float(st["source_dist"][1])) - float(st["fan_corner"][2])
+    half = target_radius_mm + 3.0 * max(sigma_range) + 8.0
+    n_xy = 2 * int(np.ceil(half / ray_mm)) + 1
+    weq, x0 = weq_volume(n_xy, ray_mm, n_steps, step, rng)
+    header = np.array([depth0, step, n_steps, x0, ray_mm, n_xy, x0, ray_mm, n_xy], np.float32)
+    beam["water_equivalence"] = np.concatenate([header, weq.reshape(-1)])
+    beam["ray_weq_header"] = header
+    if index_positions:
+        pos = np.asarray(beam["spot_positions"], np.float32).reshape(-1, 2)
+        beam["spot_positions"] = ((pos - np.array([x0, x0], np.float32)) / ray_mm + 0.5).astype(np.float32).reshape(-1)
+        beam["spot_positions_are_indices"] = True
+    out = dict(case)
+    out.update({"name": "weq", "beam": beam, "weq": weq})
+    return out

@@ -37,6 +37,9 @@ CASES = {
     # synthetic halo tables on the proton axes (subsecondpbs_b200.tables.synthetic_nuclear_tables).
     "halo_small": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
                                           "e_range": [80.0, 120.0]}, {"nuclear": "GAUSS_FIT"}),
+    # Water-equivalence import (the CarbonPBS rayweq contract): exporter depths in
+    # place of the CT trace, spot positions as rayweq texel coordinates.
+    "weq_small": ("weq_case", {}, None),
 }
 
 

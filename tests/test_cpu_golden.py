@@ -11,7 +11,9 @@ above 10 % of Dmax, the 1 %/1 mm gamma pass rate, and the batched radius lists
 the reference prints (complete_superposition.cu:476-495), which must be identical
 up to single tiles that sit on a bucket boundary. The nuclear-halo case was made by
 the reference built with NUCLEAR_CORR=GAUSS_FIT; its halo batched lists
-(complete_superposition.cu:660-669) are pinned the same way."""
+(complete_superposition.cu:660-669) are pinned the same way. The WEQ case drives
+the beam with an imported water-equivalence volume and rayweq texel spot
+coordinates (the CarbonPBS contract)."""
 import json
 from pathlib import Path
 
@@ -32,6 +34,7 @@ PINS = {
     "hetero_legacy": (2e-2, 0.999, 0),
     "hetero_rot30": (5e-2, 0.998, 0),
     "halo_small": (5e-3, 0.999, 1),
+    "weq_small": (5e-4, 1.0, 0),
 }
 
 
