@@ -21,7 +21,8 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["raytracedicom_wrapper", "DoseEngine"]
+__all__ = ["raytracedicom_wrapper", "DoseEngine", "cuFinalDose", "calcDose", "cuCalDose", "cuCalDose3",
+           "debug_build_carbonpbs_context"]
 
 
 def _with_luts(energy: dict, tables_dir: str | Path | None) -> dict:
@@ -269,3 +270,7 @@ def plan_beam(beam: dict, energy: dict, ct_dims, ct_resolution, ct_corner, dose_
         out["lattice"] = lat
     del keep_b, keep_e
     return out
+
+
+# CarbonPBS-contract entry points (raytracedicom_pybind.cpp:2088-2313).
+from .carbonpbs import calcDose, cuCalDose, cuCalDose3, cuFinalDose, debug_build_carbonpbs_context  # noqa: E402,F401

@@ -454,3 +454,52 @@ def weq_case(dims=(64, 64, 48), res=(2.0, 2.0, 2.0), n_layers=3, e_range=(80.0, 
     out = dict(case)
     out.update({"name": "weq", "beam": beam, "weq": weq})
     return out
+
+
+def carbonpbs_export(case: dict, idd_step_mm: float = 1.0, idd_samples: int = 400) -> dict:
+    """The arguments of a cuFinalDose call (the CarbonPBS export) for a weq_case
+    beam: the rayweq array, spot texel coordinates, weights and layer counts, per-
+    spot directions, the subspot table with the spot sigma in its sigma columns, and
+    an IDD table on one common depth axis (idd_step_mm spacing) taken from the
+    case's CIDD tables (the derivative of each energy's CIDD curve, resampled)."""
+    b = case["beam"]
+    e = case["energy"]
+    ne, ns = int(e["n_energies"]), int(e["n_energy_samples"])
+    cidd = np.asarray(e["cidd_matrix"], np.float64).reshape(ne, ns)
+    z = np.arange(idd_samples + 1) * idd_step_mm
+    idd = np.zeros((ne, idd_samples), np.float32)
+    for i in range(ne):
+        c = np.interp(z * float(e["scale_facts"][i]), np.arange(ns), cidd[i])
+        idd[i] = (np.diff(c) / idd_step_mm).astype(np.float32)
+    n = int(np.sum(b["layer_spot_counts"]))
+    d = np.asarray(b["beam_direction"], np.float32)
+    dims = case["dose_dims"]
+    # The contract reads each layer's spot sigma from its first subspot row
+    # (raytracedicom_pybind.cpp:640-657): the subspots carry the spot sigma.
+    sub = np.asarray(b["subspot_data"], np.float32).copy()
+    sub[:, :, 3:5] = np.asarray(b["spot_sigmas"], np.float32).reshape(-1, 1, 2)
+    return {
+        "rayweq": np.asarray(b["water_equivalence"], np.float32),
+        "roiIdx": np.zeros(0, np.int32),
+        "all_energies": np.repeat(np.asarray(b["energies"], np.float32), np.asarray(b["layer_spot_counts"])),
+        "sourcePos": np.asarray(b["source_position"], np.float32).reshape(3, 1),
+        "tmpBeamDir": np.tile(d, (n, 1)),
+        "bmxdir": np.asarray(b["beam_xdir"], np.float32),
+        "bmydir": np.asarray(b["beam_ydir"], np.float32),
+        "corner": np.asarray(case["dose_corner"], np.float32),
+        "resolution": np.asarray(case["dose_resolution"], np.float32),
+        "dims": np.asarray(dims, np.int32),
+        "longitudalCutoff": None,
+        "enelist": np.asarray(e["energies_per_u"], np.float32),
+        "idddata": idd,
+        "iddsetting": np.array([0.0, idd_step_mm, idd_samples], np.float32),
+        "profiledata": None,
+        "profilesetting": None,
+        "beamparadata": None,
+        "subspotdata": sub,
+        "layerInfo": np.asarray(b["layer_spot_counts"], np.int32),
+        "layerEnergy": np.asarray(b["energies"], np.float32),
+        "idbeamxy": np.asarray(b["spot_positions"], np.float32).reshape(-1, 2),
+        "nPar": np.asarray(b["spot_weights"], np.float32),
+        "sad": float(b["sad"]),
+    }

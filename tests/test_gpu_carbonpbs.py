@@ -1,0 +1,87 @@
+"""The CarbonPBS-contract entry points on the GPU: cuFinalDose (= calcDose =
+cuCalDose) and cuCalDose3 give the dose of the converted beam in every output
+layout, add onto the caller's dose, and agree with the oracle run on the same
+converted inputs."""
+import numpy as np
+import pytest
+
+from subsecondpbs_b200 import carbonpbs as cp
+from subsecondpbs_b200 import phantoms
+from subsecondpbs_b200.cudaCalDoseRTD import calcDose, cuCalDose3, cuFinalDose
+
+from _parity import oracle_run
+from test_gpu_parity import _dose_checks
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def export():
+    case = phantoms.weq_case()
+    ex = phantoms.carbonpbs_export(case)
+    ctx = cp.build_carbonpbs_context(**ex, tables_dir=None)
+    return case, ex, ctx
+
+
+def test_final_dose_layouts_and_accumulation(export):
+    case, ex, ctx = export
+    nx, ny, nz = ctx["dims"]
+    flat = cuFinalDose(np.zeros(nx * ny * nz, np.float32), **ex, tables_dir=None)
+    zyx = calcDose(np.zeros((nz, ny, nx), np.float32), **ex, tables_dir=None)
+    xyz = cuFinalDose(np.zeros((nx, ny, nz), np.float32), **ex, tables_dir=None)
+    ref = zyx.copy()
+    assert ref.max() > 0
+    scale = float(ref.max())
+    assert np.abs(flat.reshape(nz, ny, nx) - ref).max() <= 2e-5 * scale
+    assert np.abs(xyz.transpose(2, 1, 0) - ref).max() <= 2e-5 * scale
+    # The result is added to what the caller's array holds.
+    init = np.full((nz, ny, nx), 0.25 * scale, np.float32)
+    acc = cuFinalDose(init, **ex, tables_dir=None)
+    assert np.abs(acc - (ref + 0.25 * scale)).max() <= 2e-5 * scale
+    with pytest.raises(RuntimeError, match="size does not match dims"):
+        cuFinalDose(np.zeros(10, np.float32), **ex, tables_dir=None)
+    with pytest.raises(RuntimeError, match="float32"):
+        cuFinalDose(np.zeros((nz, ny, nx)), **ex, tables_dir=None)
+
+
+def test_final_dose_matches_the_oracle_on_the_converted_inputs(export):
+    case, ex, ctx = export
+    nx, ny, nz = ctx["dims"]
+    dose = cuFinalDose(np.zeros((nz, ny, nx), np.float32), **ex, tables_dir=None)
+    conv = dict(case, beam=ctx["beam"], energy=ctx["energy"], ct=np.full(nx * ny * nz, 1000.0, np.float32))
+    r = oracle_run(conv)
+    _dose_checks(dose, r["dose"], case["dose_resolution"])
+
+
+def test_cal_dose3_zeroes_the_sparse_outputs(export):
+    case, ex, ctx = export
+    nx, ny, nz = ctx["dims"]
+    data = np.ones(16, np.float32)
+    ptr = np.ones(8, np.int32)
+    rows = np.ones(16, np.int32)
+    nnz = np.ones(1, np.uint64)
+    args = dict(weq_data=ex["rayweq"], roi_index=ex["roiIdx"], source_energies=ex["all_energies"],
+                source=ex["sourcePos"], beam_dir=ex["tmpBeamDir"], beam_xdir=ex["bmxdir"], beam_ydir=ex["bmydir"],
+                corner=ex["corner"], resolution=ex["resolution"], dims=ex["dims"], longitudal_cutoff=None,
+                enelist=ex["enelist"], idddata=ex["idddata"], iddsetting=ex["iddsetting"], profiledata=None,
+                profilesetting=None, beamparadata=None, subspot_data=ex["subspotdata"], layer_info=ex["layerInfo"],
+                layer_energy=ex["layerEnergy"], outNNZ=nnz, idbeamxy=ex["idbeamxy"],
+                num_particles_per_beam=ex["nPar"], cutoff=None, sad=ex["sad"], beam_para_pos=None,
+                python_nnz_size=None, tables_dir=None)
+    out = cuCalDose3(data, ptr, rows, **args)
+    assert not data.any() and not ptr.any() and not rows.any() and not nnz.any()
+    ref = cuFinalDose(np.zeros((nz, ny, nx), np.float32), **ex, tables_dir=None)
+    assert out["dose_grid"].shape == (nx, ny, nz)
+    assert np.abs(out["dose_grid"].transpose(2, 1, 0) - ref).max() <= 2e-5 * float(ref.max())
+
+
+def test_roi_ct_changes_only_the_geometry_stand_in(export):
+    """With an ROI the stand-in CT is water on the ROI and air elsewhere; the WEQ
+    volume still carries the transport, so the dose is the same."""
+    case, ex, ctx = export
+    nx, ny, nz = ctx["dims"]
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    roi = np.stack([xx.reshape(-1), yy.reshape(-1), zz.reshape(-1)], axis=1)[::7].astype(np.int32)
+    a = cuFinalDose(np.zeros((nz, ny, nx), np.float32), **ex, tables_dir=None)
+    b = cuFinalDose(np.zeros((nz, ny, nx), np.float32), **dict(ex, roiIdx=roi), tables_dir=None)
+    assert np.abs(a - b).max() <= 2e-5 * float(a.max())
