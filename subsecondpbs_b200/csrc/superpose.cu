@@ -10,14 +10,14 @@
 //   * table phase: each thread builds its source's rows e_s(0..R) (float4 chunks,
 //     chunk-major so that the stores and the broadcast reads are conflict-free)
 //     and idd_s * e_s(0..R) (odd row stride); sources without dose get zero rows;
-//   * accumulation phase: a warp lane is one (source column, column offset d in
-//     [-R, R]) pair; a source column's eight sources share the lane's output
+//   * accumulation phase: a warp lane is one column offset d in [-R, R] of one
+//     source column; a source column's eight sources share the lane's output
 //     column, so the lane keeps the whole footprint height (8+2R rows) in
-//     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. The 32*(2R+1)
-//     pairs of a tile are dealt out 32 per warp instruction, so no lane idles
-//     whatever the footprint width. A pair ends with one shared-memory add per
-//     footprint row; pairs whose source column has no depositing source are
-//     skipped;
+//     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. When 2R+1 <= 32
+//     several source columns, spaced so that their footprints are disjoint, share
+//     one warp instruction; wider footprints split into 32-column chunks. A column
+//     ends with one shared-memory add per footprint row; columns without a
+//     depositing source are skipped;
 //   * the tile footprint is then added to the BEV dose of its step (all layers of
 //     the beam share one BEV volume).
 // Radii 16..32, 8..15 and 0..7 run as three instances of the kernel with 128, 48
@@ -106,20 +106,33 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
 
     // ---- accumulation phase --------------------------------------------------
     {
-        // The (source column, offset) pairs of the tile, 32 per warp instruction:
-        // every lane does useful work whatever the footprint width.
-        constexpr int kPairs = kTileX * W;
-        constexpr int kUnits = (kPairs + 31) / 32;
+        constexpr bool kGrouped = W <= 32;
+        constexpr int G = kGrouped ? 32 / W : 1;                   // source columns per instruction
+        constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing (>= W: disjoint)
+        constexpr int CH = kGrouped ? 1 : (W + 31) / 32;           // 32-lane chunks of one column
+        constexpr int kUnits = kGrouped ? S : 32 * CH;
         // Depositing sources of source column `lane`, as an 8-bit mask over sy.
         unsigned colBits = 0;
 #pragma unroll
         for (int sy = 0; sy < kTileY; ++sy) colBits |= ((sMask[sy] >> lane) & 1u) << sy;
 #pragma unroll 1
         for (int u = warp; u < kUnits; u += kWarps) {
-            const int pr = u * 32 + lane;
-            const bool valid = pr < kPairs;
-            const int sx = valid ? pr / W : 0;
-            const int d = valid ? pr - sx * W - R : 0;
+            int sx, d;
+            bool valid;
+            if (kGrouped) {
+                const int g = lane / W;
+                d = lane - g * W - R;
+                sx = u + g * S;
+                valid = g < G && sx < kTileX;
+            } else {
+                sx = u / CH;
+                d = (u - sx * CH) * 32 + lane - R;
+                valid = d <= R;
+            }
+            if (!valid) {
+                sx = 0;
+                d = 0;
+            }
             const int ad = d < 0 ? -d : d;
             const unsigned colAll = __shfl_sync(0xffffffffu, colBits, sx);
             const unsigned colLive = valid ? colAll : 0u;
