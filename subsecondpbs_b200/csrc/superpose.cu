@@ -15,7 +15,8 @@
 //     column, so the lane keeps the whole footprint height (8+2R rows) in
 //     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. When 2R+1 <= 32
 //     several source columns, spaced so that their footprints are disjoint, share
-//     one warp instruction; wider footprints split into 32-column chunks. A column
+//     one warp instruction; wider footprints deal the tile's (column, offset) pairs
+//     out 32 at a time. A column
 //     ends with one shared-memory add per footprint row; columns without a
 //     depositing source are skipped;
 //   * the tile footprint is then added to the BEV dose of its step (all layers of
@@ -109,8 +110,12 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         constexpr bool kGrouped = W <= 32;
         constexpr int G = kGrouped ? 32 / W : 1;                   // source columns per instruction
         constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing (>= W: disjoint)
-        constexpr int CH = kGrouped ? 1 : (W + 31) / 32;           // 32-lane chunks of one column
-        constexpr int kUnits = kGrouped ? S : 32 * CH;
+        // Wider footprints: the tile's 32 * (2R+1) (column, offset) pairs dealt out 32
+        // per instruction. A warp then spans at most two source columns whose
+        // footprints overlap in no output column it writes (their offsets lie about
+        // 2R apart), so the lanes stay conflict-free and none idles.
+        constexpr int kPairs = kTileX * W;
+        constexpr int kUnits = kGrouped ? S : (kPairs + 31) / 32;
         // Depositing sources of source column `lane`, as an 8-bit mask over sy.
         unsigned colBits = 0;
 #pragma unroll
@@ -125,9 +130,10 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                 sx = u + g * S;
                 valid = g < G && sx < kTileX;
             } else {
-                sx = u / CH;
-                d = (u - sx * CH) * 32 + lane - R;
-                valid = d <= R;
+                const int pr = u * 32 + lane;
+                sx = pr / W;
+                d = pr - sx * W - R;
+                valid = pr < kPairs;
             }
             if (!valid) {
                 sx = 0;
