@@ -503,3 +503,48 @@ def carbonpbs_export(case: dict, idd_step_mm: float = 1.0, idd_samples: int = 40
         "nPar": np.asarray(b["spot_weights"], np.float32),
         "sad": float(b["sad"]),
     }
+
+
+def carbon_case(dims=(512, 512, 200), res=(1.0, 1.0, 1.0), gantries=(0.0, 120.0, 240.0), n_layers=40,
+                e_range=(120.0, 400.0), spots_per_layer=125, pitch_mm=5.0, sigma_range=(4.0, 2.0), sad_mm=2000.0,
+                ray_spacing=1.0, n_sub=9, seed=SEED_BASE + 3) -> dict:
+    """Carbon-ion plan with the nuclear halo: the heterogeneous_ct recipe on
+    `dims` at `res`, one beam per gantry angle, `n_layers` layers spanning
+    `e_range` MeV/u with about `spots_per_layer` spots each on a hexagonal grid,
+    lognormal(0, 0.5) weights, sigma falling linearly over `sigma_range`,
+    n_sub x n_sub subspots, and the synthetic carbon tables with their nuclear
+    halo tables (carbon_tables)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dims_, res_, corner = _grid(dims, res)
+    ct = heterogeneous_ct(dims_, res_, rng)
+    radius = float(np.sqrt(spots_per_layer * pitch_mm * pitch_mm * np.sqrt(3.0) / 2.0 / np.pi))
+    spots = hex_spots(radius, pitch_mm)
+    energies = np.linspace(e_range[0], e_range[1], n_layers).astype(np.float32)
+    sig = np.linspace(sigma_range[0], sigma_range[1], n_layers).astype(np.float32)
+    counts = np.full(n_layers, spots.shape[0], dtype=np.int32)
+    bmz = np.array([-1.0, 0.0, 0.0])
+    base = {
+        "energies": energies,
+        "spot_sigmas": np.stack([sig, sig], axis=1),
+        "ray_spacing": (ray_spacing, ray_spacing),
+        "steps": 0,
+        "source_dist": (sad_mm, sad_mm),
+        "spot_offset": (0.0, 0.0, 0.0),
+        "spot_delta": (pitch_mm, pitch_mm * np.sqrt(3.0) / 2.0, 0.0),
+        "beam_direction": tuple(bmz),
+        "beam_xdir": (0.0, 1.0, 0.0),
+        "beam_ydir": (0.0, 0.0, 1.0),
+        "sad": sad_mm,
+        "source_position": tuple(-bmz * sad_mm),
+        "layer_spot_counts": counts,
+        "spot_positions": np.tile(spots, (n_layers, 1)).reshape(-1),
+        "subspot_data": subspot_lut(n_layers, n_sub, sig, rng),
+    }
+    beams = []
+    for g in gantries:
+        b = rotate_beam(base, float(g))
+        b["spot_weights"] = rng.lognormal(0.0, 0.5, size=int(counts.sum())).astype(np.float32)
+        beams.append(b)
+    return {"name": "carbon", "ct": ct, "ct_dims": dims_, "ct_resolution": res_, "ct_corner": corner,
+            "dose_dims": dims_, "dose_resolution": res_, "dose_corner": corner, "beam": beams[0], "beams": beams,
+            "energy": carbon_tables()}

@@ -40,6 +40,10 @@ CASES = {
     # Water-equivalence import (the CarbonPBS rayweq contract): exporter depths in
     # place of the CT trace, spot positions as rayweq texel coordinates.
     "weq_small": ("weq_case", {}, None),
+    # Carbon ions with the nuclear halo (synthetic carbon tables and their halo tables).
+    "carbon_halo_small": ("carbon_case", {"dims": [64, 64, 48], "res": [2.0, 2.0, 2.0], "gantries": [90.0],
+                                          "n_layers": 3, "e_range": [120.0, 200.0], "spots_per_layer": 40},
+                          {"nuclear": "GAUSS_FIT"}),
 }
 
 

@@ -35,6 +35,7 @@ PINS = {
     "hetero_rot30": (5e-2, 0.998, 0),
     "halo_small": (5e-3, 0.999, 1),
     "weq_small": (5e-4, 1.0, 0),
+    "carbon_halo_small": (2e-2, 0.999, 3),
 }
 
 
