@@ -45,7 +45,8 @@ def _args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-adjoint", action="store_true", help="skip the spot-weight adjoint timing")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the secondary timings (spot-weight adjoint, carbon plan)")
     ap.add_argument("--serving-requests", type=int, default=1000, help="served stream length (0: skip)")
     ap.add_argument("--serving-slots", type=int, default=4)
     ap.add_argument("--serving-budget-mib", type=int, default=0, help="server HBM budget (0: 90%% of free)")
@@ -266,6 +267,39 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
     }
 
 
+def _carbon_plan(local: int, reps: int = 3) -> dict:
+    """Carbon-ion plan with the nuclear halo (512x512x200 CT at 1 mm, three beams of
+    40 layers 120-400 MeV/u, ~15,000 spots): device time of the whole plan on the
+    context stream, median of `reps` after one warm-up."""
+    import torch
+
+    from subsecondpbs_b200 import phantoms
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    case = phantoms.carbon_case()
+    eng = DoseEngine(local, nuclear_model=2)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    beams = [eng.prepare_beam(b) for b in case["beams"]]
+    stream = torch.cuda.ExternalStream(eng.stream_handle, device=torch.device("cuda", local))
+    ms = []
+    for rep in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.reset_dose()
+        for b in beams:
+            eng.add_beam(b, nuclear_correction=True)
+        e1.record(stream)
+        eng.synchronize()
+        if rep:
+            ms.append(e0.elapsed_time(e1))
+    eng.close()
+    return {"workload": "carbon + nuclear halo (GAUSS_FIT), CT 512x512x200 at 1 mm, 3 beams (0/120/240 deg) x 40 "
+                        "layers 120-400 MeV/u, 14,520 spots, 9x9 subspots",
+            "ms_per_plan": round(statistics.median(ms), 3), "timing": f"CUDA events, median of {reps}"}
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -455,6 +489,7 @@ def run_ours(args):
     adjoint = _adjoint_cost(local) if world == 1 and not args.no_adjoint else None
     served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
               if world == 1 and args.serving_requests > 0 else None)
+    carbon = _carbon_plan(local) if world == 1 and not args.no_adjoint else None
 
     line = {
         "metric": METRIC,
@@ -482,6 +517,7 @@ def run_ours(args):
         "precision": precision,
         "adjoint": adjoint,
         "serving": served,
+        "carbon_plan": carbon,
         "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers"},
         "gpu_launches": launches_per_step * args.steps,
