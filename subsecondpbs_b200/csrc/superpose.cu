@@ -10,15 +10,17 @@
 //   * table phase: each thread builds its source's rows e_s(0..R) (float4 chunks,
 //     chunk-major so that the stores and the broadcast reads are conflict-free)
 //     and idd_s * e_s(0..R) (odd row stride); sources without dose get zero rows;
-//   * accumulation phase: a warp lane is one column offset d in [-R, R] of one
-//     source column; a source column's eight sources share the lane's output
-//     column, so the lane keeps the whole footprint height (8+2R rows) in
-//     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. When 2R+1 <= 32
-//     several source columns, spaced so that their footprints are disjoint, share
-//     one warp instruction; wider footprints deal the tile's (column, offset) pairs
-//     out 32 at a time. A column
-//     ends with one shared-memory add per footprint row; columns without a
-//     depositing source are skipped;
+//   * accumulation phase: a warp lane is one column distance |d| of one source
+//     column; a source column's eight sources share the lane's output
+//     columns, so the lane keeps the whole footprint height (8+2R rows) in
+//     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. The column at
+//     +d equals the one at -d, so up to radius 15 it is accumulated once and added
+//     to both: the FMAs and shared loads are (R+1)/(2R+1) of the direct (2R+1)^2
+//     formulation. Several source columns share one warp instruction; for radii
+//     16..32 a lane is one signed offset and the tile's (column, offset) pairs are
+//     dealt out 32 at a time. A pair ends with one
+//     shared-memory add per footprint row and output column; pairs whose source
+//     column has no depositing source are skipped;
 //   * the tile footprint is then added to the BEV dose of its step (all layers of
 //     the beam share one BEV volume).
 // Radii 16..32, 8..15 and 0..7 run as three instances of the kernel with 128, 48
@@ -64,7 +66,6 @@ template <int R, int RMax>
 __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* __restrict__ EW,
                                                float* __restrict__ out, unsigned* __restrict__ sMask,
                                                const TileArgs& a) {
-    constexpr int W = 2 * R + 1;
     constexpr int H = kTileY + 2 * R;
     constexpr int Wo = kTileX + 2 * R;
     constexpr int Q = (R + 1 + 3) / 4;
@@ -107,14 +108,18 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
 
     // ---- accumulation phase --------------------------------------------------
     {
-        constexpr bool kGrouped = W <= 32;
-        constexpr int G = kGrouped ? 32 / W : 1;                   // source columns per instruction
-        constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing (>= W: disjoint)
-        // Wider footprints: the tile's 32 * (2R+1) (column, offset) pairs dealt out 32
-        // per instruction. A warp then spans at most two source columns whose
-        // footprints overlap in no output column it writes (their offsets lie about
-        // 2R apart), so the lanes stay conflict-free and none idles.
-        constexpr int kPairs = kTileX * W;
+        // A source column's footprint is the same column vector at offsets +d and -d
+        // (the weights depend on |d| only). Up to radius kSplitR one lane per (source
+        // column, |d|) pair accumulates it once and adds it to both output columns;
+        // wider footprints keep one lane per signed offset (their doubled flushes
+        // cost more than the saved FMAs).
+        constexpr bool kMirror = R <= kSplitR;
+        constexpr int M = kMirror ? R + 1 : 2 * R + 1;             // pairs per source column
+        constexpr bool kGrouped = M <= 32;
+        constexpr int G = kGrouped ? 32 / M : 1;                   // source columns per instruction
+        constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing
+        // Otherwise the tile's 32 * M pairs are dealt out 32 per instruction.
+        constexpr int kPairs = kTileX * M;
         constexpr int kUnits = kGrouped ? S : (kPairs + 31) / 32;
         // Depositing sources of source column `lane`, as an 8-bit mask over sy.
         unsigned colBits = 0;
@@ -122,19 +127,20 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         for (int sy = 0; sy < kTileY; ++sy) colBits |= ((sMask[sy] >> lane) & 1u) << sy;
 #pragma unroll 1
         for (int u = warp; u < kUnits; u += kWarps) {
-            int sx, d;
+            int sx, d;  // d: |d| when mirrored, else the signed offset
             bool valid;
             if (kGrouped) {
-                const int g = lane / W;
-                d = lane - g * W - R;
+                const int g = lane / M;
+                d = lane - g * M;
                 sx = u + g * S;
                 valid = g < G && sx < kTileX;
             } else {
                 const int pr = u * 32 + lane;
-                sx = pr / W;
-                d = pr - sx * W - R;
+                sx = pr / M;
+                d = pr - sx * M;
                 valid = pr < kPairs;
             }
+            if (!kMirror) d -= R;
             if (!valid) {
                 sx = 0;
                 d = 0;
@@ -174,6 +180,11 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                 float* col = out + sx + R + d;
 #pragma unroll
                 for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, acc[i]);
+                if (kMirror && d > 0) {
+                    col = out + sx + R - d;
+#pragma unroll
+                    for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, acc[i]);
+                }
             }
         }
     }
