@@ -4,6 +4,8 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <cstdint>
+#include <cstring>
 #include <cctype>
 #include <cmath>
 #include <cstdlib>
@@ -158,6 +160,28 @@ bool build_raw_lattice(const PbsBeamDesc& b, RawLattice& out) {
             return fail("failed to decode spot position");
     }
     auto unique_axis = [](std::vector<float> v) {
+        // Exact duplicates (every layer repeats the spot grid) cannot change the
+        // tolerance merge below, so they are dropped before the sort (open
+        // addressing on the bit patterns; 0xffffffff, a NaN, marks a free slot).
+        size_t cap = 16;
+        while (cap < 2 * v.size()) cap <<= 1;
+        std::vector<uint32_t> table(cap, 0xffffffffu);
+        size_t n = 0;
+        for (float x : v) {
+            uint32_t bits;
+            std::memcpy(&bits, &x, sizeof(bits));
+            if (bits == 0xffffffffu) {
+                v[n++] = x;
+                continue;
+            }
+            size_t h = (bits * 2654435761u) & (cap - 1);
+            while (table[h] != 0xffffffffu && table[h] != bits) h = (h + 1) & (cap - 1);
+            if (table[h] == 0xffffffffu) {
+                table[h] = bits;
+                v[n++] = x;
+            }
+        }
+        v.resize(n);
         std::sort(v.begin(), v.end());
         std::vector<float> u;
         for (float x : v)
@@ -174,17 +198,58 @@ bool build_raw_lattice(const PbsBeamDesc& b, RawLattice& out) {
         // holds, so a single-column axis keeps the 1e20 step.
         return step;
     };
-    const std::vector<float> ux = unique_axis(xs), uy = unique_axis(ys);
+    // A layer that repeats the previous layer's positions bit for bit adds no new
+    // axis values: only the first of such a run enters the merge.
+    std::vector<float> axX, axY;
+    axX.reserve(xs.size());
+    axY.reserve(ys.size());
+    for (int l = 0, o = 0, po = -1, pc = -1; l < L; o += b.layer_spot_counts[l], ++l) {
+        const int c = b.layer_spot_counts[l];
+        if (c <= 0) return false;  // as the weight pass below refuses it
+        const bool rep = c == pc && std::memcmp(xs.data() + o, xs.data() + po, sizeof(float) * size_t(c)) == 0 &&
+                         std::memcmp(ys.data() + o, ys.data() + po, sizeof(float) * size_t(c)) == 0;
+        if (!rep) {
+            axX.insert(axX.end(), xs.begin() + o, xs.begin() + o + c);
+            axY.insert(axY.end(), ys.begin() + o, ys.begin() + o + c);
+        }
+        po = o;
+        pc = c;
+    }
+    const std::vector<float> ux = unique_axis(std::move(axX)), uy = unique_axis(std::move(axY));
     if (ux.empty() || uy.empty()) return fail("empty lattice axes");
     const float dx = grid_step(ux), dy = grid_step(uy);
     const float ox = ux.front(), oy = uy.front();
     const int nx = std::max(1, static_cast<int>(std::lround((ux.back() - ox) / dx)) + 1);
     const int ny = std::max(1, static_cast<int>(std::lround((uy.back() - oy) / dy)) + 1);
     std::vector<float> dense(static_cast<size_t>(nx) * ny * L, 0.0f);
-    int off = 0;
+    // Lattice cell of every spot (-1: outside, -2: off the lattice phase). A layer
+    // whose positions repeat the previous layer's bit for bit reuses its cells.
+    std::vector<int> cell(static_cast<size_t>(total));
+    int off = 0, prevOff = -1, prevCnt = -1;
     for (int l = 0; l < L; ++l) {
         const int cnt = b.layer_spot_counts[l];
         if (cnt <= 0) return false;
+        const bool same = cnt == prevCnt &&
+                          std::memcmp(xs.data() + off, xs.data() + prevOff, sizeof(float) * size_t(cnt)) == 0 &&
+                          std::memcmp(ys.data() + off, ys.data() + prevOff, sizeof(float) * size_t(cnt)) == 0;
+        for (int i = 0; i < cnt; ++i) {
+            const int s = off + i;
+            if (same) {
+                cell[s] = cell[prevOff + i];
+                continue;
+            }
+            const float x = xs[s], y = ys[s];
+            const float fx = (dx != 0.0f) ? ((x - ox) / dx) : 0.0f;
+            const float fy = (dy != 0.0f) ? ((y - oy) / dy) : 0.0f;
+            const int ix = static_cast<int>(std::lround(fx));
+            const int iy = static_cast<int>(std::lround(fy));
+            if (ix < 0 || ix >= nx || iy < 0 || iy >= ny)
+                cell[s] = -1;
+            else if (!(std::fabs(ox + ix * dx - x) <= 2e-2f) || !(std::fabs(oy + iy * dy - y) <= 2e-2f))
+                cell[s] = -2;
+            else
+                cell[s] = iy * nx + ix;
+        }
         for (int i = 0; i < cnt; ++i) {
             const int s = off + i;
             const float w = b.spot_weights[s];
@@ -194,16 +259,12 @@ bool build_raw_lattice(const PbsBeamDesc& b, RawLattice& out) {
                 out.skippedZeroWeightSpots++;
                 continue;
             }
-            const float x = xs[s], y = ys[s];
-            const float fx = (dx != 0.0f) ? ((x - ox) / dx) : 0.0f;
-            const float fy = (dy != 0.0f) ? ((y - oy) / dy) : 0.0f;
-            const int ix = static_cast<int>(std::lround(fx));
-            const int iy = static_cast<int>(std::lround(fy));
-            if (ix < 0 || ix >= nx || iy < 0 || iy >= ny) return fail("spot outside inferred lattice bounds");
-            if (!(std::fabs(ox + ix * dx - x) <= 2e-2f) || !(std::fabs(oy + iy * dy - y) <= 2e-2f))
-                return fail("spot does not align with inferred lattice phase");
-            dense[(static_cast<size_t>(l) * ny + iy) * nx + ix] += w;
+            if (cell[s] == -1) return fail("spot outside inferred lattice bounds");
+            if (cell[s] == -2) return fail("spot does not align with inferred lattice phase");
+            dense[static_cast<size_t>(l) * ny * nx + cell[s]] += w;
         }
+        prevOff = off;
+        prevCnt = cnt;
         off += cnt;
     }
     out.valid = true;
