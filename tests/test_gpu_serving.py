@@ -141,3 +141,38 @@ def test_submit_refuses_bad_requests(workload):
             srv.submit(big["id"], [big["fields"][0]["proton"]], 0)
         assert ex.value.code == _lib.PBS_ERR_OUT_OF_MEMORY
         assert srv.stats()["submitted"] == 0
+
+
+def test_a_failing_request_does_not_stop_the_server(workload):
+    """A carbon request with the halo against tables that carry no halo tables
+    passes submit, fails on its slot with PBS_ERR_UNSUPPORTED, and the requests
+    around it complete."""
+    w = workload
+    r0 = w["requests"][0]
+    beams = phantoms.request_beams(w, r0)
+    with _server(w, slots=2) as srv:
+        ok1 = srv.submit(r0["patient"], beams, 0)
+        bad = srv.submit(r0["patient"], beams, 0, nuclear_correction=True)  # proton tables: no halo tables
+        ok2 = srv.submit(r0["patient"], beams, 0)
+        d1, _ = srv.result(ok1)
+        with pytest.raises(_lib.PbsError) as ex:
+            srv.result(bad)
+        assert ex.value.code == _lib.PBS_ERR_UNSUPPORTED
+        srv.release(bad)
+        d2, _ = srv.result(ok2)
+        _assert_same(d2, d1, "around a failure")
+        st = srv.stats()
+        assert st["failed"] == 1 and st["completed"] == 2
+
+
+def test_patients_are_removed_only_when_idle(workload):
+    w = workload
+    r0 = w["requests"][0]
+    with _server(w, slots=1) as srv:
+        t = srv.submit(r0["patient"], phantoms.request_beams(w, r0), 0)
+        srv.drain()
+        srv.remove_patient(r0["patient"])
+        with pytest.raises(_lib.PbsError):
+            srv.submit(r0["patient"], phantoms.request_beams(w, r0), 0)
+        srv.release(t)
+        assert srv.stats()["resident_bytes"] >= 0
