@@ -48,7 +48,7 @@ def _args():
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the secondary timings (spot-weight adjoint, carbon plan)")
     ap.add_argument("--serving-requests", type=int, default=1000, help="served stream length (0: skip)")
-    ap.add_argument("--serving-slots", type=int, default=4)
+    ap.add_argument("--serving-slots", type=int, default=8)
     ap.add_argument("--serving-budget-mib", type=int, default=0, help="server HBM budget (0: 90%% of free)")
     return ap.parse_args()
 

@@ -148,6 +148,9 @@ int Server::init(int gpu, int nSlots, size_t budgetBytes) {
         int rc = s->ctx.init(gpu);
         if (rc) return rc;
         s->ctx.use_stream_ordered_allocation();
+        // Pinned staging for the beams' host inputs, sized up front for the same reason
+        // as the result buffers (see add_patient); larger beams still grow it.
+        if ((rc = s->ctx.staging.ensure(size_t(4) << 20))) return rc;
         s->traces.server = this;
         s->traces.slot = s.get();
         s->ctx.traceStore = &s->traces;
@@ -228,13 +231,30 @@ int Server::add_patient(int id, const float* ct, const GridDesc& ctGrid, const G
         p->hostCt.release();
         return fail(PBS_ERR_CUDA, "cudaEventCreate failed");
     }
-    std::lock_guard<std::mutex> lk(mu_);
-    if (patients_.count(id)) {
-        p->hostCt.release();
-        cudaEventDestroy(p->ready);
-        return fail(PBS_ERR_INVALID_ARGUMENT, "patient id " + std::to_string(id) + " exists");
+    const size_t resultBytes = grid_voxels(doseGrid) * 4;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (patients_.count(id)) {
+            p->hostCt.release();
+            cudaEventDestroy(p->ready);
+            return fail(PBS_ERR_INVALID_ARGUMENT, "patient id " + std::to_string(id) + " exists");
+        }
+        patients_[id] = std::move(p);
     }
-    patients_[id] = std::move(p);
+    // Pinned result buffers of this grid size for every slot and two in the
+    // caller's hands, allocated now: pinning host memory while requests run
+    // stalls the device.
+    const size_t want = slots_.size() + 2;
+    for (;;) {
+        {
+            std::lock_guard<std::mutex> lk(poolMu_);
+            if (freeResults_.count(resultBytes) >= want || freeResults_.size() >= kMaxPooledResults) break;
+        }
+        void* ptr = nullptr;
+        if (cudaMallocHost(&ptr, resultBytes) != cudaSuccess) break;  // the pool grows on demand instead
+        std::lock_guard<std::mutex> lk(poolMu_);
+        freeResults_.emplace(resultBytes, ptr);
+    }
     return PBS_OK;
 }
 
