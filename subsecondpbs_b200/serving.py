@@ -249,3 +249,59 @@ def with_rate(workload: dict, rate_hz: float) -> dict:
     f = workload["rate_hz"] / rate_hz
     reqs = [dict(r, arrival_s=r["arrival_s"] * f) for r in workload["requests"]]
     return dict(workload, requests=reqs, rate_hz=rate_hz)
+
+
+class ServerPool:
+    """One DoseServer per GPU of a node. Requests of a patient go to the GPU that
+    already holds its CT and traces (the least loaded one at its first request),
+    unless that GPU has `spill` more requests in flight than the least loaded one,
+    in which case the request goes there and the patient becomes resident on both.
+    Tickets are (gpu index, ticket) pairs."""
+
+    def __init__(self, gpu_ids=(0,), slots: int = 8, hbm_budget_mib: int = 0, spill: int = 16, **kw):
+        self.servers = [DoseServer(g, slots=slots, hbm_budget_mib=hbm_budget_mib, **kw) for g in gpu_ids]
+        self.gpu_ids = list(gpu_ids)
+        self.spill = spill
+        self._home: dict[int, int] = {}
+        self._inflight = [0] * len(self.servers)
+
+    def close(self) -> None:
+        for s in self.servers:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_energy(self, energy_id: int, energy: dict, tables_dir: str | None = None) -> None:
+        for s in self.servers:
+            s.add_energy(energy_id, energy, tables_dir)
+
+    def add_patient(self, patient_id: int, *args, **kw) -> None:
+        for s in self.servers:
+            s.add_patient(patient_id, *args, **kw)
+
+    def _route(self, patient_id: int) -> int:
+        least = min(range(len(self.servers)), key=lambda i: self._inflight[i])
+        home = self._home.setdefault(patient_id, least)
+        if self._inflight[home] - self._inflight[least] > self.spill:
+            return least
+        return home
+
+    def submit(self, patient_id: int, beams, energy_id: int = 0, nuclear_correction: bool = False) -> tuple:
+        i = self._route(patient_id)
+        t = self.servers[i].submit(patient_id, beams, energy_id, nuclear_correction)
+        self._inflight[i] += 1
+        return (i, t)
+
+    def result(self, ticket: tuple, timeout: float = 120.0):
+        i, t = ticket
+        try:
+            return self.servers[i].result(t, timeout)
+        finally:
+            self._inflight[i] -= 1
+
+    def stats(self) -> list:
+        return [s.stats() for s in self.servers]

@@ -176,3 +176,27 @@ def test_patients_are_removed_only_when_idle(workload):
             srv.submit(r0["patient"], phantoms.request_beams(w, r0), 0)
         srv.release(t)
         assert srv.stats()["resident_bytes"] >= 0
+
+
+def test_server_pool_keeps_patients_home_and_results_unchanged(workload):
+    """Two servers (both on GPU 0 here; one per GPU on a node): a patient's requests
+    stay on the server holding its CT, and the results are the requests' doses."""
+    w = workload
+    ref = _alone(w)
+    with serving.ServerPool(gpu_ids=(0, 0), slots=2) as pool:
+        pool.add_energy(0, w["energy"]["proton"])
+        pool.add_energy(1, w["energy"]["carbon"])
+        for p in w["patients"]:
+            pool.add_patient(p["id"], p["ct"], p["ct_dims"], p["ct_resolution"], p["ct_corner"])
+        tickets = [pool.submit(r["patient"], phantoms.request_beams(w, r), serving.ENERGY_IDS[r["ion"]],
+                               r["ion"] == "carbon") for r in w["requests"]]
+        for i, t in enumerate(tickets):
+            d, _ = pool.result(t)
+            _assert_same(d, ref[i], ("pool", i))
+        homes = {}
+        for r, (g, _) in zip(w["requests"], tickets):
+            homes.setdefault(r["patient"], set()).add(g)
+        assert all(len(v) == 1 for v in homes.values())
+        st = pool.stats()
+        assert sum(s["completed"] for s in st) == len(w["requests"])
+        assert min(s["completed"] for s in st) > 0
