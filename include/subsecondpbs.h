@@ -257,8 +257,8 @@ PBS_API int pbs_context_reset_dose(PbsContext* ctx, const float* initial, int in
 /* Plan the beam on the host and enqueue its whole pipeline on the context stream.
  * Returns without waiting for the device. */
 PBS_API int pbs_context_add_beam(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction);
-/* Spot-weight adjoint of one beam (no counterpart in the reference; the inverse-
- * planning gradient of the north-star additions). For a dose gradient G
+/* Spot-weight adjoint of one beam (no counterpart in the reference; the gradient
+ * an inverse-planning optimiser needs). For a dose gradient G
  * (double [Z][Y][X], host or device) it writes dJ/dw_s = <G, dD/dw_s> for every
  * spot s of `beam` (n_weights floats, host, in the beam's spot order), at the
  * beam's current weights: the transposes of the transfer, the tile superposition

@@ -1,5 +1,5 @@
-"""Nuclear halo branch (halo lattice IDD/sigma, halo tile
-superposition and halo transfer) against the oracle on the same inputs."""
+"""Nuclear halo branch (halo lattice IDD/sigma, halo tile superposition and halo
+transfer) against the oracle on the same inputs."""
 import numpy as np
 import pytest
 
