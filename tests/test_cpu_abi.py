@@ -94,3 +94,30 @@ def test_struct_layouts_match_header():
     assert members("PbsEnergyDesc") == len(_lib.PbsEnergyDesc._fields_)
     assert members("PbsBeamStats") == len(_lib.PbsBeamStats._fields_)
     assert members("PbsLayerStats") == len(_lib.PbsLayerStats._fields_)
+
+
+def test_server_stats_layout_matches_header():
+    text = (ROOT / "include" / "subsecondpbs.h").read_text()
+    body = re.search(r"typedef struct PbsServerStats \{(.*?)\} PbsServerStats;", text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if decl:
+            assert decl.startswith("long long ")
+            names += [n.strip() for n in decl[len("long long "):].split(",")]
+    assert names == [n for n, _ in _lib.PbsServerStats._fields_]
+
+
+def test_server_refuses_to_start_without_a_device():
+    """No GPU here: creating a server fails with a status, not a crash."""
+    lib = _lib.load()
+    h = C.c_void_p()
+    n = C.c_int(0)
+    lib.pbs_device_count(C.byref(n))
+    if n.value > 0:
+        pytest.skip("a GPU is visible")
+    rc = lib.pbs_server_create(0, 2, 0, C.byref(h))
+    assert rc != _lib.PBS_OK and not h.value
+    assert lib.pbs_server_destroy(None) == _lib.PBS_OK
+    assert lib.pbs_server_submit(None, 0, 0, None, 0, 0, None) == _lib.PBS_ERR_INVALID_ARGUMENT
