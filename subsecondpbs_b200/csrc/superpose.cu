@@ -21,6 +21,14 @@
 //     dealt out 32 at a time. A pair ends with one
 //     shared-memory add per footprint row and output column; pairs whose source
 //     column has no depositing source are skipped;
+//   * the footprint accumulates in 32-bit fixed point: a float add to shared memory
+//     has no native instruction on this part (it is a compare-and-swap loop, a
+//     third of the throughput of an integer add), while the integer add is native
+//     and order-independent. Every footprint value and every partial sum of it is at
+//     most the tile's total dose (each e_s(k) <= 1 and each source adds to a row of
+//     a pair once), so the power-of-two scale 2^30 / total keeps every sum inside
+//     int32 with a resolution of 2^-30 of the tile's dose, finer than FP32 near the
+//     footprint's peak;
 //   * the tile footprint is then added to the BEV dose of its step (all layers of
 //     the beam share one BEV volume).
 // Radii 16..32, 8..15 and 0..7 run as three instances of the kernel with 128, 48
@@ -64,8 +72,8 @@ struct TileArgs {
 // Table phase, accumulation phase and write-out of one tile at radius R.
 template <int R, int RMax>
 __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* __restrict__ EW,
-                                               float* __restrict__ out, unsigned* __restrict__ sMask,
-                                               const TileArgs& a) {
+                                               int* __restrict__ out, unsigned* __restrict__ sMask,
+                                               float* __restrict__ sSum, const TileArgs& a) {
     constexpr int H = kTileY + 2 * R;
     constexpr int Wo = kTileX + 2 * R;
     constexpr int Q = (R + 1 + 3) / 4;
@@ -75,12 +83,19 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
 
     // ---- table phase (complete_superposition.cu:298-307) --------------------
     // Sources without dose get zero rows, so the accumulation needs no per-source
-    // test; sColMask[sx] collects the depositing sources of every source column.
+    // test; sMask[sy] collects the depositing sources of every source row and
+    // sSum[sy] their dose.
     {
         const float dose = a.idd[a.src];
         const bool live = dose > 0.0f;
         const unsigned mask = __ballot_sync(0xffffffffu, live);
-        if (lane == 0) sMask[warp] = mask;
+        float rowDose = live ? dose : 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
+        if (lane == 0) {
+            sMask[warp] = mask;
+            sSum[warp] = rowDose;
+        }
         float e[4 * Q];
         if (live) {
             float row[R + 1];
@@ -102,9 +117,18 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         const int pt = warp * kTileX + e4_col(lane);
 #pragma unroll
         for (int q = 0; q < Q; ++q) E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
-        for (int i = t; i < H * Wo; i += kThreads) out[i] = 0.0f;
+        for (int i = t; i < H * Wo; i += kThreads) out[i] = 0;
     }
     __syncthreads();
+
+    // Fixed-point scale: 2^(30 - ex) with total < 2^ex, so total * scale < 2^30.
+    float total = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) total += sSum[w];
+    int ex;
+    frexpf(total, &ex);
+    const float scale = ldexpf(1.0f, min(30 - ex, 126));
+    const float invScale = 1.0f / scale;
 
     // ---- accumulation phase --------------------------------------------------
     {
@@ -177,13 +201,16 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                 if (sy & 1) asm volatile("" ::: "memory");
             }
             if (colLive) {
-                float* col = out + sx + R + d;
+                int q[H];
 #pragma unroll
-                for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, acc[i]);
+                for (int i = 0; i < H; ++i) q[i] = __float2int_rn(acc[i] * scale);
+                int* col = out + sx + R + d;
+#pragma unroll
+                for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, q[i]);
                 if (kMirror && d > 0) {
                     col = out + sx + R - d;
 #pragma unroll
-                    for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, acc[i]);
+                    for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, q[i]);
                 }
             }
         }
@@ -192,21 +219,21 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
 
     // ---- write-out -------------------------------------------------------------
     for (int i = t; i < H * Wo; i += kThreads) {
-        const float v = out[i];
+        const int q = out[i];
         const int oy = i / Wo, ox = i - oy * Wo;
-        if (v != 0.0f) atomicAdd(a.dst + static_cast<size_t>(oy) * a.bevX + ox, v);
+        if (q != 0) atomicAdd(a.dst + static_cast<size_t>(oy) * a.bevX + ox, float(q) * invScale);
     }
 }
 
 // Chain of compile-time radii RLo..RHi; returns false if r is outside it.
 template <int R, int RHi, int RMax>
-__device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, float* out, unsigned* sMask,
-                                                const TileArgs& a) {
+__device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, int* out, unsigned* sMask,
+                                                float* sSum, const TileArgs& a) {
     if (r == R) {
-        superpose_tile<R, RMax>(E4, EW, out, sMask, a);
+        superpose_tile<R, RMax>(E4, EW, out, sMask, sSum, a);
         return true;
     }
-    if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sMask, a);
+    if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sMask, sSum, a);
     return false;
 }
 
@@ -220,9 +247,10 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
     extern __shared__ __align__(16) float sm[];
     float4* E4 = reinterpret_cast<float4*>(sm);                                  // [Q][256] e_s(4q..4q+3), slot sy*32+e4_col(sx)
     float* EW = sm + Shape<RHi>::kQ * kThreads * 4;                              // [256][EWS] idd_s e_s(k)
-    float* out = EW + kThreads * Shape<RHi>::kEWStride;                          // [8+2R][32+2R] footprint
+    int* out = reinterpret_cast<int*>(EW + kThreads * Shape<RHi>::kEWStride);   // [8+2R][32+2R] fixed-point footprint
     __shared__ int sItem[2];
     __shared__ unsigned sMask[kTileY];
+    __shared__ float sSum[kTileY];
 
     const int t = threadIdx.x;
     // Range 0: R > kSplitR, 1: kSplitR2 < R <= kSplitR, 2: R <= kSplitR2.
@@ -252,7 +280,7 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
         a.dst = bev + static_cast<size_t>(zRel) * bevPlane + static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX +
                 (tx * kTileX - R + kMaxR);
         a.bevX = g.bevX;
-        if (!dispatch_radius<RLo, RHi, RHi>(R, E4, EW, out, sMask, a)) {
+        if (!dispatch_radius<RLo, RHi, RHi>(R, E4, EW, out, sMask, sSum, a)) {
             if (t == 0) atomicOr(&beam->errorFlags, 2);
         }
         // Every thread is past the tile (and has read sItem[buf]) before the
