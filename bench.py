@@ -484,7 +484,7 @@ def run_ours(args):
 
         precision = dict(prec.report(out.cpu().numpy(), ref_dose, case["dose_resolution"]),
                          reference="FP64 oracle, same inputs", arithmetic="FP32 rays/superposition, "
-                         "Kahan WEPL, FP64 dose accumulation")
+                         "int32 fixed-point tile footprints, Kahan WEPL, FP64 dose accumulation")
 
     adjoint = _adjoint_cost(local) if world == 1 and not args.no_adjoint else None
     served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
