@@ -158,7 +158,11 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         nextSp = wepl[idx];
         nextDens = density[idx];
     }
-    for (int stepNo = first; stepNo < afterLastL; ++stepNo) {
+    int stepNo = first;
+    for (; stepNo < afterLastL; ++stepNo) {
+        // Once no ray of the row is live, every later step is (0, +inf): the fill
+        // below writes those without the per-step walk.
+        if (!__any_sync(0xffffffffu, live)) break;
         float res = 0.0f;
         float rSigmaEff = __int_as_float(0x7f800000);
         float nucRes = 0.0f;
@@ -232,6 +236,21 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             partMin[zr * 8 + warp] = float_from_order_key(mk);
             partLive[zr * 8 + warp] = anyLive;
         }
+    }
+    // The row's remaining steps: no dose, rSigmaEff = +inf, nothing live.
+    for (int k = stepNo; k < afterLastL; ++k) {
+        const int zr = k - first;
+        const size_t o = static_cast<size_t>(zr) * padPlane + static_cast<size_t>(y) * g.pitchX + x;
+        iddL[o] = 0.0f;
+        rsL[o] = __int_as_float(0x7f800000);
+        if (nucIdx >= 0) {
+            nucIddL[static_cast<size_t>(zr) * nucPlane + nucIdx] = 0.0f;
+            nucRsL[static_cast<size_t>(zr) * nucPlane + nucIdx] = __int_as_float(0x7f800000);
+        }
+    }
+    for (int zr = stepNo - first + lane; zr < afterLastL - first; zr += 32) {
+        partMin[zr * 8 + warp] = __int_as_float(0x7f800000);
+        partLive[zr * 8 + warp] = 0;
     }
 
     int fp = real ? static_cast<int>(afterLast) : INT_MIN;
