@@ -302,7 +302,10 @@ PBS_API int pbs_cpb_fluence_no_alloc(const float* d_subspots, int max_subspots, 
 PBS_API int pbs_context_synchronize(PbsContext* ctx);
 /* cudaStream_t the context enqueues on. */
 PBS_API void* pbs_context_stream(PbsContext* ctx);
-/* Device pointer of the FP64 accumulator [Z][Y][X]. */
+/* Device pointer of the FP64 accumulator [Z][Y][X]. Until the pointer is handed
+ * out, a zeroing reset clears only the voxels the context's beams can have
+ * written and a float readout converts only those; afterwards the caller may
+ * write anywhere, so every reset and readout covers the whole grid. */
 PBS_API void* pbs_context_dose_device_ptr(PbsContext* ctx);
 /* Stats of the last beam (synchronizes the context stream). */
 PBS_API int pbs_context_beam_stats(PbsContext* ctx, PbsBeamStats* out);

@@ -240,7 +240,13 @@ int pbs_context_synchronize(PbsContext* ctx) {
 
 void* pbs_context_stream(PbsContext* ctx) { return ctx ? static_cast<void*>(ctx->impl.stream) : nullptr; }
 
-void* pbs_context_dose_device_ptr(PbsContext* ctx) { return ctx ? ctx->impl.dose64.ptr : nullptr; }
+void* pbs_context_dose_device_ptr(PbsContext* ctx) {
+    if (!ctx) return nullptr;
+    // The caller may now write anywhere in the grid: resets and readouts cover all of it.
+    ctx->impl.doseExposed = true;
+    ctx->impl.doseBoxed = false;
+    return ctx->impl.dose64.ptr;
+}
 
 int pbs_context_beam_stats(PbsContext* ctx, PbsBeamStats* out) {
     if (int rc = guard(ctx)) return rc;

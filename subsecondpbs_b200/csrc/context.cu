@@ -284,6 +284,42 @@ cudaError_t copy_box(void* dst, const void* src, const int dims[3], const int lo
 }
 
 bool box_empty(const int lo[3], const int hi[3]) { return hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2]; }
+
+void merge_box(int lo[3], int hi[3], const int a[3], const int b[3]) {
+    if (b[0] < a[0] || b[1] < a[1] || b[2] < a[2]) return;
+    for (int i = 0; i < 3; ++i) {
+        lo[i] = std::min(lo[i], a[i]);
+        hi[i] = std::max(hi[i], b[i]);
+    }
+}
+
+// Dose voxels a beam's transfer can write (transfer_planner_kernel and the block
+// rounding of transfer_kernel), over all steps so that it bounds every layer.
+void dose_transfer_box(const FromFan& f, int pitchX, int pitchY, int steps, const int dims[3], int lo[3],
+                       int hi[3]) {
+    const float xs[2] = {-float(kMaxR), float(pitchX + kMaxR - 1)};
+    const float ys[2] = {-float(kMaxR), float(pitchY + kMaxR - 1)};
+    const float zs[2] = {0.0f, float(steps - 1)};
+    V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
+    for (int zi = 0; zi < 2; ++zi)
+        for (int yi = 0; yi < 2; ++yi)
+            for (int xi = 0; xi < 2; ++xi) {
+                const V3 p = apply(f, v3(xs[xi], ys[yi], zs[zi]));
+                mx.x = std::max(mx.x, p.x);
+                mx.y = std::max(mx.y, p.y);
+                mx.z = std::max(mx.z, p.z);
+                mn.x = std::min(mn.x, p.x);
+                mn.y = std::min(mn.y, p.y);
+                mn.z = std::min(mn.z, p.z);
+            }
+    lo[0] = std::max((int(std::floor(mn.x)) / 32) * 32, 0);
+    lo[1] = std::max(int(std::floor(mn.y)), 0);
+    lo[2] = std::max(int(std::floor(mn.z)), 0);
+    // The transfer rounds its x and y spans up to whole 32 x 8 blocks.
+    hi[0] = std::min(int(std::ceil(mx.x)) + 32, dims[0] - 1);
+    hi[1] = std::min(int(std::ceil(mx.y)) + 8, dims[1] - 1);
+    hi[2] = std::min(int(std::ceil(mx.z)), dims[2] - 1);
+}
 }  // namespace
 
 int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3], const int hi[3]) {
@@ -320,6 +356,7 @@ int Context::reset_dose_region(const float* init, const int lo[3], const int hi[
     if (box_empty(lo, hi)) return reset_dose(nullptr, 0);
     // Voxels outside the box are initialised from stale values; no beam of the
     // call writes them and read_dose_region does not copy them back.
+    doseBoxed = false;
     PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
     PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
     PBS_CUDA(copy_box(floatOut.ptr, init, doseGrid.dims, lo, hi, cudaMemcpyHostToDevice, copyStream), "dose H2D");
@@ -335,8 +372,9 @@ int Context::read_dose_region(float* out, const int lo[3], const int hi[3]) {
     if (rc) return rc;
     if ((rc = floatOut.ensure(n * 4))) return rc;
     if (!box_empty(lo, hi)) {
-        PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), static_cast<float*>(floatOut.ptr), n,
-                                      stream),
+        // Only the region is copied back, so only the region is converted.
+        PBS_CUDA(launch_dose_box(static_cast<double*>(dose64.ptr), static_cast<float*>(floatOut.ptr), doseGrid.dims,
+                                 lo, hi, stream),
                  "dose_to_float");
         PBS_CUDA(copy_box(out, floatOut.ptr, doseGrid.dims, lo, hi, cudaMemcpyDeviceToHost, stream), "dose D2H");
     }
@@ -424,6 +462,7 @@ int Context::set_dose_grid(const GridDesc& g) {
     if (rc) return rc;
     doseGrid = g;
     hasDose = true;
+    doseBoxed = false;
     return reset_dose(nullptr, 0);
 }
 
@@ -444,11 +483,36 @@ int Context::reset_dose(const float* init, int onDevice) {
         PBS_CUDA(cudaMemcpyAsync(floatOut.ptr, init, n * 4, cudaMemcpyHostToDevice, copyStream), "dose H2D");
         PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
         pendingDoseInit = true;
+        doseBoxed = false;
         return PBS_OK;
     }
     pendingDoseInit = false;
-    PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), init, n, stream), "dose_init");
+    if (!init && doseBoxed && !doseExposed) {
+        // Zero outside the dirty box already: clearing the box clears the grid.
+        if (!box_empty(dirtyLo, dirtyHi))
+            PBS_CUDA(launch_dose_box(static_cast<double*>(dose64.ptr), nullptr, doseGrid.dims, dirtyLo, dirtyHi,
+                                     stream),
+                     "dose_box_zero");
+    } else {
+        PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), init, n, stream), "dose_init");
+    }
+    doseBoxed = !init && !doseExposed;
+    for (int i = 0; i < 3; ++i) {
+        dirtyLo[i] = INT_MAX;
+        dirtyHi[i] = -1;
+    }
     return PBS_OK;
+}
+
+void Context::mark_dose_written(const int lo[3], const int hi[3]) {
+    if (!doseBoxed || box_empty(lo, hi)) return;
+    // One voxel of margin around the host bound of the transfer's writes.
+    int a[3], b[3];
+    for (int i = 0; i < 3; ++i) {
+        a[i] = std::max(lo[i] - 1, 0);
+        b[i] = std::min(hi[i] + 1, doseGrid.dims[i] - 1);
+    }
+    merge_box(dirtyLo, dirtyHi, a, b);
 }
 
 int Context::flush_dose_init() {
@@ -470,14 +534,20 @@ int Context::read_dose(float* out, int onDevice) {
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
     int frc = flush_dose_init();
     if (frc) return frc;
-    if (onDevice) {
-        PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), out, n, stream), "dose_to_float");
-        return PBS_OK;
+    if (!onDevice) {
+        int rc = floatOut.ensure(n * 4);
+        if (rc) return rc;
     }
-    int rc = floatOut.ensure(n * 4);
-    if (rc) return rc;
-    PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), static_cast<float*>(floatOut.ptr), n, stream),
-             "dose_to_float");
+    float* dst = onDevice ? out : static_cast<float*>(floatOut.ptr);
+    if (doseBoxed && !doseExposed) {
+        PBS_CUDA(cudaMemsetAsync(dst, 0, n * 4, stream), "dose memset");
+        if (!box_empty(dirtyLo, dirtyHi))
+            PBS_CUDA(launch_dose_box(static_cast<double*>(dose64.ptr), dst, doseGrid.dims, dirtyLo, dirtyHi, stream),
+                     "dose_to_float");
+    } else {
+        PBS_CUDA(launch_dose_to_float(static_cast<const double*>(dose64.ptr), dst, n, stream), "dose_to_float");
+    }
+    if (onDevice) return PBS_OK;
     PBS_CUDA(cudaMemcpyAsync(out, floatOut.ptr, n * 4, cudaMemcpyDeviceToHost, stream), "dose D2H");
     PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     return take_device_errors();
@@ -587,6 +657,7 @@ void Context::release_beam_buffers() {
                       &weqBody})
         b->release();
     hasDose = false;
+    doseBoxed = false;
     lastBeamValid = false;
 }
 
@@ -973,6 +1044,17 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
     if ((rc = mark(6))) return rc;
     if (adj) return finish_adjoint(*adj, b);
     if ((rc = flush_dose_init())) return rc;
+    if (doseBoxed) {
+        int lo[3], hi[3];
+        dose_transfer_box(plan.rayIdxToDoseIdx, plan.superpDims[0], plan.superpDims[1], plan.tracerSteps,
+                          doseGrid.dims, lo, hi);
+        mark_dose_written(lo, hi);
+        if (nuclear) {
+            dose_transfer_box(nucGeom.rayIdxToDoseIdx, nucGeom.pitchX, nucGeom.pitchY, plan.tracerSteps,
+                              doseGrid.dims, lo, hi);
+            mark_dose_written(lo, hi);
+        }
+    }
     PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
     if (nuclear) {
@@ -1319,14 +1401,6 @@ namespace {
 std::mutex g_cacheMutex;
 std::map<int, Context*> g_cache;
 
-void merge_box(int lo[3], int hi[3], const int a[3], const int b[3]) {
-    if (b[0] < a[0] || b[1] < a[1] || b[2] < a[2]) return;
-    for (int i = 0; i < 3; ++i) {
-        lo[i] = std::min(lo[i], a[i]);
-        hi[i] = std::max(hi[i], b[i]);
-    }
-}
-
 // CT voxels the tracer of a beam can read: the sample points are multilinear in
 // (ray x, ray y, step), so the corner rays at the first and last step bound them;
 // two voxels of margin cover the trilinear footprint and the rounding of the
@@ -1354,33 +1428,6 @@ void ct_trace_box(const BeamPlan& P, const int dims[3], int lo[3], int hi[3]) {
     }
 }
 
-// Dose voxels a beam's transfer can write (transfer_planner_kernel and the block
-// rounding of transfer_kernel), over all steps so that it bounds every layer.
-void dose_transfer_box(const FromFan& f, int pitchX, int pitchY, int steps, const int dims[3], int lo[3],
-                       int hi[3]) {
-    const float xs[2] = {-float(kMaxR), float(pitchX + kMaxR - 1)};
-    const float ys[2] = {-float(kMaxR), float(pitchY + kMaxR - 1)};
-    const float zs[2] = {0.0f, float(steps - 1)};
-    V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
-    for (int zi = 0; zi < 2; ++zi)
-        for (int yi = 0; yi < 2; ++yi)
-            for (int xi = 0; xi < 2; ++xi) {
-                const V3 p = apply(f, v3(xs[xi], ys[yi], zs[zi]));
-                mx.x = std::max(mx.x, p.x);
-                mx.y = std::max(mx.y, p.y);
-                mx.z = std::max(mx.z, p.z);
-                mn.x = std::min(mn.x, p.x);
-                mn.y = std::min(mn.y, p.y);
-                mn.z = std::min(mn.z, p.z);
-            }
-    lo[0] = std::max((int(std::floor(mn.x)) / 32) * 32, 0);
-    lo[1] = std::max(int(std::floor(mn.y)), 0);
-    lo[2] = std::max(int(std::floor(mn.z)), 0);
-    // The transfer rounds its x and y spans up to whole 32 x 8 blocks.
-    hi[0] = std::min(int(std::ceil(mx.x)) + 32, dims[0] - 1);
-    hi[1] = std::min(int(std::ceil(mx.y)) + 8, dims[1] - 1);
-    hi[2] = std::min(int(std::ceil(mx.z)), dims[2] - 1);
-}
 }  // namespace
 
 int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],

@@ -83,6 +83,15 @@ struct Context {
     cudaStream_t copyStream = nullptr;
     cudaEvent_t copyStart = nullptr, doseCopied = nullptr;
     bool pendingDoseInit = false;
+    // While doseBoxed is set, the FP64 grid is exactly zero outside the inclusive
+    // voxel box [dirtyLo, dirtyHi]: the union of the transfer boxes of the beams
+    // added since the last zeroing reset. Such a reset then clears only that box,
+    // and a float readout zeroes its output and converts only that box. An
+    // initialised reset, a new grid or a handed-out device pointer (after which the
+    // caller may write anywhere) clear the flag: the whole grid is then used.
+    bool doseBoxed = false;
+    bool doseExposed = false;
+    int dirtyLo[3] = {0, 0, 0}, dirtyHi[3] = {-1, -1, -1};
 
     // Options.
     int compatBevZShift = 0;
@@ -171,6 +180,8 @@ struct Context {
     size_t device_bytes() const;
     void release_beam_buffers();
     int reset_dose(const float* init, int onDevice);
+    // Adds an inclusive voxel box a beam's transfer writes to the dirty box.
+    void mark_dose_written(const int lo[3], const int hi[3]);
     int read_dose(float* out, int onDevice);
     int read_dose64(double* out, int onDevice);
     int add_beam(const PbsBeamDesc& b, int nuclear);

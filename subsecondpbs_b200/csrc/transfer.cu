@@ -119,6 +119,23 @@ __global__ void dose_to_float_kernel(const double* dose, float* out, size_t n) {
         out[i] = float(dose[i]);
 }
 
+// Box [lo, lo + ext) of a [dims.z][dims.y][dims.x] grid: zeroes the FP64 dose there
+// (out == nullptr) or converts it to float into the same voxels of `out`.
+__global__ void dose_box_kernel(double* dose, float* out, int3 dims, int3 lo, int3 ext) {
+    const size_t total = size_t(ext.x) * ext.y * ext.z;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % size_t(ext.x));
+        const size_t r = i / size_t(ext.x);
+        const int y = int(r % size_t(ext.y));
+        const int z = int(r / size_t(ext.y));
+        const size_t v = (size_t(z + lo.z) * dims.y + (y + lo.y)) * size_t(dims.x) + (x + lo.x);
+        if (out)
+            out[v] = float(dose[v]);
+        else
+            dose[v] = 0.0;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cudaStream_t s) {
@@ -143,6 +160,19 @@ cudaError_t launch_dose_init(double* dose, const float* init, size_t n, cudaStre
 cudaError_t launch_dose_to_float(const double* dose, float* out, size_t n, cudaStream_t s) {
     const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 32));
     dose_to_float_kernel<<<blocks, 256, 0, s>>>(dose, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dose_box(double* dose, float* out, const int dims[3], const int lo[3], const int hi[3],
+                            cudaStream_t s) {
+    for (int i = 0; i < 3; ++i)
+        if (lo[i] < 0 || hi[i] >= dims[i] || hi[i] < lo[i]) return cudaErrorInvalidValue;
+    const int3 d = make_int3(dims[0], dims[1], dims[2]);
+    const int3 l = make_int3(lo[0], lo[1], lo[2]);
+    const int3 e = make_int3(hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1);
+    const size_t total = size_t(e.x) * e.y * e.z;
+    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 32));
+    dose_box_kernel<<<blocks, 256, 0, s>>>(dose, out, d, l, e);
     return cudaGetLastError();
 }
 
