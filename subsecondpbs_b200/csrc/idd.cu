@@ -303,10 +303,16 @@ __global__ void __launch_bounds__(kMaxChunkLayers)
 layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restrict__ ls,
                   BeamStateDev* __restrict__ beam, int workCapacity, const LayerStateDev* __restrict__ primaryLs,
                   const BeamStateDev* __restrict__ primaryBeam) {
+    __shared__ int sLive[kMaxChunkLayers][kMaxR + 1];   // live items per layer and batched radius
+    __shared__ int sCalc[kMaxChunkLayers];
+    __shared__ int sWarpSum[kMaxChunkLayers / 32];
+    __shared__ long long sWarpFma[kMaxChunkLayers / 32];
+    __shared__ int sSplit[2];
     const int lc = threadIdx.x;
     const bool nuclear = primaryLs != nullptr;
     const int first = nuclear ? primaryBeam->firstInside : beam->firstInside;
     const int tiles = g.tilesX * g.tilesY;
+    if (lc < 2) sSplit[lc] = 0;
     if (lc < nLayers) {
         LayerStateDev& st = ls[layer0 + lc];
         int hist[kBuckets];
@@ -349,15 +355,58 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         int live = 0;
         for (int i = 0; i <= kMaxR; ++i) {
             st.batchedCounts[i] = batched[i];
-            st.liveR[i] = 0;
             st.curR[i] = 0;
         }
+        int liveR[kMaxR + 1];
+        for (int i = 0; i <= kMaxR; ++i) liveR[i] = 0;
         for (int b = 0; b < kBuckets; ++b) {
             st.batchedR[b] = map[b];
-            st.liveR[map[b]] += st.liveHist[b];
+            liveR[map[b]] += st.liveHist[b];
             live += st.liveHist[b];
         }
+        for (int i = 0; i <= kMaxR; ++i) {
+            st.liveR[i] = liveR[i];
+            sLive[lc][i] = liveR[i];
+        }
         st.liveTiles = live;
+        sCalc[lc] = st.calcPassive;
+    }
+    __syncthreads();
+
+    // Work-list offsets: radius groups in descending radius, each with its layers in
+    // order, i.e. position p = (kMaxR - r) * nLayers + q. Each thread sums a run of
+    // positions, the block scans the runs, then each thread writes its offsets.
+    const int total = (kMaxR + 1) * nLayers;
+    const int per = (total + kMaxChunkLayers - 1) / kMaxChunkLayers;
+    const int p0 = min(lc * per, total), p1 = min(p0 + per, total);
+    int runSum = 0;
+    long long runFma = 0;
+    for (int p = p0; p < p1; ++p) {
+        const int r = kMaxR - p / nLayers, q = p % nLayers;
+        const int v = sLive[q][r];
+        runSum += v;
+        runFma += static_cast<long long>(v) * 256 * (2 * r + 1) * (2 * r + 1);
+    }
+    const int lane = lc & 31, warp = lc >> 5;
+    int incl = runSum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += n;
+    }
+    long long wf = runFma;
+    for (int o = 16; o > 0; o >>= 1) wf += __shfl_xor_sync(0xffffffffu, wf, o);
+    if (lane == 31) sWarpSum[warp] = incl;
+    if (lane == 0) sWarpFma[warp] = wf;
+    __syncthreads();
+    int acc = incl - runSum;
+    for (int w = 0; w < warp; ++w) acc += sWarpSum[w];
+    const int pSplit = (kMaxR - kSplitR) * nLayers, pSplit2 = (kMaxR - kSplitR2) * nLayers;
+    for (int p = p0; p < p1; ++p) {
+        const int r = kMaxR - p / nLayers, q = p % nLayers;
+        if (p == pSplit) sSplit[0] = acc;
+        if (p == pSplit2) sSplit[1] = acc;
+        ls[layer0 + q].offR[r] = acc;
+        acc += sLive[q][r];
     }
     __syncthreads();
     if (lc == 0) {
@@ -366,21 +415,15 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
             beam->firstInside = first;
             beam->maxCalcPassive = primaryBeam->maxCalcPassive;
         }
-        int acc = 0;
+        acc = 0;
         long long fma = 0;
-        int mp = beam->maxCalcPassive;
-        int split = 0, split2 = 0;
-        for (int r = kMaxR; r >= 0; --r) {
-            if (r == kSplitR) split = acc;
-            if (r == kSplitR2) split2 = acc;
-            for (int q = 0; q < nLayers; ++q) {
-                LayerStateDev& st = ls[layer0 + q];
-                st.offR[r] = acc;
-                acc += st.liveR[r];
-                fma += static_cast<long long>(st.liveR[r]) * 256 * (2 * r + 1) * (2 * r + 1);
-            }
+        for (int w = 0; w < kMaxChunkLayers / 32; ++w) {
+            acc += sWarpSum[w];
+            fma += sWarpFma[w];
         }
-        for (int q = 0; q < nLayers; ++q) mp = max(mp, ls[layer0 + q].calcPassive);
+        const int split = sSplit[0], split2 = sSplit[1];
+        int mp = beam->maxCalcPassive;
+        for (int q = 0; q < nLayers; ++q) mp = max(mp, sCalc[q]);
         beam->maxCalcPassive = mp;
         if (acc > workCapacity) {
             atomicOr(&beam->errorFlags, 1);
