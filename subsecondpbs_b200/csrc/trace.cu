@@ -14,7 +14,7 @@ namespace pbs {
 namespace {
 
 constexpr float kInf20 = 1.0e20f;  // the reference's INF stored in a float (Macro.cuh:7)
-constexpr int kTraceSegments = 8;  // warps per tracing CTA; each marches one depth segment
+constexpr int kTraceSegments = 16;  // warps per tracing CTA; each marches one depth segment
 constexpr int kNone = 0x7fffffff;
 constexpr size_t kTraceCacheMaxBytes = 160 * 1024;  // CT samples kept on chip up to ~1280 steps
 
@@ -46,6 +46,42 @@ __device__ __forceinline__ float ct_sample_border(const float* __restrict__ vol,
     return c0 + (c1 - c0) * tz;
 }
 
+
+struct CtCorners {
+    float c[8];
+    float tx, ty, tz;
+};
+
+// The loads of ct_sample_border, issued ahead of the arithmetic (ct_combine).
+__device__ __forceinline__ void ct_fetch(const float* __restrict__ vol, int dx, int dy, int dz, float x, float y,
+                                         float z, CtCorners& o) {
+    float fx = x - 0.5f, fy = y - 0.5f, fz = z - 0.5f;
+    fx = fminf(fmaxf(fx, -2.0f), float(dx) + 1.0f);
+    fy = fminf(fmaxf(fy, -2.0f), float(dy) + 1.0f);
+    fz = fminf(fmaxf(fz, -2.0f), float(dz) + 1.0f);
+    const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+    const int x0 = int(flx), y0 = int(fly), z0 = int(flz);
+    o.tx = fx - flx;
+    o.ty = fy - fly;
+    o.tz = fz - flz;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int xi = x0 + (i & 1), yi = y0 + ((i >> 1) & 1), zi = z0 + (i >> 2);
+        const bool in = xi >= 0 && yi >= 0 && zi >= 0 && xi < dx && yi < dy && zi < dz;
+        o.c[i] = in ? __ldg(vol + (static_cast<size_t>(zi) * dy + yi) * dx + xi) : 0.0f;
+    }
+}
+
+__device__ __forceinline__ float ct_combine(const CtCorners& o) {
+    const float c00 = o.c[0] + (o.c[1] - o.c[0]) * o.tx;
+    const float c10 = o.c[2] + (o.c[3] - o.c[2]) * o.tx;
+    const float c01 = o.c[4] + (o.c[5] - o.c[4]) * o.tx;
+    const float c11 = o.c[6] + (o.c[7] - o.c[6]) * o.tx;
+    const float c0 = c00 + (c10 - c00) * o.ty;
+    const float c1 = c01 + (c11 - c01) * o.ty;
+    return c0 + (c1 - c0) * o.tz;
+}
+
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
     const float y = v - comp;
     const float t = sum + y;
@@ -53,7 +89,9 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
     sum = t;
 }
 
-// One CTA traces 32 neighbouring rays of one ray row; warp w marches depth segment w.
+// One CTA traces 32 neighbouring rays of one ray row; warp w marches depth segment w
+// (16 segments). In pass 1 the eight CT corners of the next step are loaded while
+// the current step is combined, looked up and summed.
 // Pass 1 sums each segment, the segment sums are prefix-scanned per ray, and pass 2
 // re-marches the segment writing density and compensated cumulative WEPL.
 //
@@ -99,15 +137,20 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
     // Pass 1: segment sums of HU+1000 and of WEPL increments.
     float huSum = 0.f, spSum = 0.f, spComp = 0.f;
     float* myCache = shCache + static_cast<size_t>(w) * seg * 32 + lane;
-    if (active) {
+    if (active && s0 < s1) {
         V3 pos = pos0;
+        CtCorners cur, nxt;
+        ct_fetch(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z, cur);
         for (int k = s0; k < s1; ++k) {
-            const float hu = ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+            const V3 posN = add(pos, inc);
+            if (k + 1 < s1) ct_fetch(ct, ctX, ctY, ctZ, posN.x, posN.y, posN.z, nxt);
+            const float hu = ct_combine(cur);
             if (kCache) myCache[(k - s0) * 32] = hu;
             huSum += hu;
             const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
             kahan_add(spSum, spComp, stepLen * sp);
-            pos = add(pos, inc);
+            pos = posN;
+            cur = nxt;
         }
     }
     shHu[w][lane] = huSum;
