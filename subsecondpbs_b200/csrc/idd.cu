@@ -19,6 +19,11 @@ constexpr float kECoef = 8.639415f;   // (10 alpha)^(-1/p) (raytracedicom_integr
 constexpr float kSqrt2 = 1.41421356f;
 constexpr int kMaxChunkLayers = 64;
 
+// Divisions in the per-step walk use the approximate reciprocal (__fdividef, within
+// 2 ulp): the IEEE quotient's range check and slow path cost more ALU and branch
+// issue than the rest of a step's arithmetic. The tile radius bucket keeps its
+// IEEE division (tile_radius_bucket).
+//
 // One CTA = one 32x8 tile of rays for one layer. Each thread walks its ray from the
 // beam's first-inside step to the layer's cut-off step (fillIddAndSigmaKernel,
 // idd_sigma.cu:46-259). After every step each warp reduces min(rSigmaEff) and
@@ -178,9 +183,9 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             const float cumulDose = lut_linear_clamp_smem(ciddRow, luts.nS, cumulSp * p.energyScaleFact + 0.5f);
             if (cumulSp < p.peakDepth) {
                 const float resE = kECoef * __powf(p.peakDepth - 0.5f * (cumulSp + cumulSpOld), kPInv);
-                const float betaP = resE + 938.3f - 938.3f * 938.3f / (resE + 938.3f);
+                const float betaP = resE + 938.3f - __fdividef(938.3f * 938.3f, resE + 938.3f);
                 const float rRl = dens * lut_linear_clamp_smem(rrlTab, luts.nRrl, dens * luts.rrlScale + 0.5f);
-                const float thetaSq = eRefSq / (betaP * betaP) * stepLength * rRl;
+                const float thetaSq = __fdividef(eRefSq, betaP * betaP) * stepLength * rRl;
                 sigmaSq += incScat + incDiv;
                 incincScat += 2.0f * thetaSq * stepLength * stepLength;
                 incScat += incincScat;
@@ -188,15 +193,15 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             } else if (!suppressDip) {
                 sigmaSq -= 1.5f * (incScat + incDiv) * dens;
             }
-            rSigmaEff = stepNum[stepNo] / (kSqrt2 * (sqrtf(sigmaSq) + sigmaDelta));
+            rSigmaEff = __fdividef(stepNum[stepNo], kSqrt2 * (sqrtf(sigmaSq) + sigmaDelta));
             const float mass = dens * stepVolT[stepNo];
             if (nucOn) {
                 const float depthMidIdx = 0.5f * (cumulSp + cumulSpOld) * p.energyScaleFact + 0.5f;
                 if (mass > 1e-2f) {
                     const float nucWeight = lut_linear_clamp_smem(nucWRow, luts.nS, depthMidIdx);
-                    res = (1.0f - nucWeight) * rayWeight * (cumulDose - cumulDoseOld) / mass;
+                    res = __fdividef((1.0f - nucWeight) * rayWeight * (cumulDose - cumulDoseOld), mass);
                     if (nucIdx >= 0)
-                        nucRes = nucWeight * nucRayWeight * (cumulDose - cumulDoseOld) / (mass * spotDist * spotDist);
+                        nucRes = __fdividef(nucWeight * nucRayWeight * (cumulDose - cumulDoseOld), mass * spotDist * spotDist);
                 }
                 if (nucIdx >= 0) {
                     const float nucSqSigma = lut_linear_clamp_smem(nucSRow, luts.nS, depthMidIdx);
@@ -204,7 +209,7 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
                                    (kSqrt2 * sqrtf(sigmaSq + nucSqSigma + entrySigmaSq));
                 }
             } else if (mass > 1e-2f) {
-                res = rayWeight * (cumulDose - cumulDoseOld) / mass;
+                res = __fdividef(rayWeight * (cumulDose - cumulDoseOld), mass);
             }
             cumulSpOld = cumulSp;
             cumulDoseOld = cumulDose;
