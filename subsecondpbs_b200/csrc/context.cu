@@ -88,7 +88,7 @@ void PinnedBuf::release() {
 Context::~Context() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
-    for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
+    for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &ctQuad, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad, &rbarBuf,
@@ -333,6 +333,7 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
     int rc = ct.ensure(n * 4);
     if (rc) return rc;
     ctView = nullptr;
+    ctQuadValid = false;
     if (!box_empty(lo, hi)) PBS_CUDA(copy_box(ct.ptr, data, g.dims, lo, hi, cudaMemcpyHostToDevice, stream), "CT H2D");
     // The CT type comes from the whole volume, as with a full upload.
     int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
@@ -414,7 +415,19 @@ int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
             type = auto_detect_ct_type(mn, mx);
         }
     }
-    return convert_ct(type, g);
+    if ((rc = convert_ct(type, g))) return rc;
+    // The packed copy is an optimisation: without room for it the tracer samples
+    // the CT directly.
+    ctQuadValid = false;
+    if (ctQuad.ensure(ct_quad_bytes(g.dims)) == PBS_OK) {
+        PBS_CUDA(launch_ct_quad(static_cast<const float*>(ct.ptr), g.dims, static_cast<float4*>(ctQuad.ptr), stream),
+                 "ct_quad");
+        ctQuadValid = true;
+    } else {
+        cudaGetLastError();
+        set_error("");
+    }
+    return PBS_OK;
 }
 
 // CT adapter on the device (wrapper.cu:2290-2441): to HU+1000 in place.
@@ -631,7 +644,7 @@ size_t trace_bytes(size_t steps, size_t rays) {
 }
 
 void Context::use_stream_ordered_allocation() {
-    for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
+    for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &ctQuad, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm,
@@ -641,7 +654,7 @@ void Context::use_stream_ordered_allocation() {
 
 size_t Context::device_bytes() const {
     size_t n = 0;
-    for (const DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
+    for (const DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &ctQuad, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                             &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive,
                             &codes, &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf,
                             &nucRsBuf, &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
@@ -667,6 +680,7 @@ int Context::attach_ct(const float* deviceCt, const GridDesc& g, int type) {
         return PBS_ERR_INVALID_ARGUMENT;
     }
     ctView = deviceCt;
+    ctQuadValid = false;
     ctGrid = g;
     ctType = type;
     hasCt = true;
@@ -980,7 +994,8 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
                                   stream),
                  "weq_trace");
     } else {
-        PBS_CUDA(launch_trace(g, luts, ctView ? ctView : static_cast<const float*>(ct.ptr), ctGrid.dims[0],
+        const float4* quad = !ctView && ctQuadValid ? static_cast<const float4*>(ctQuad.ptr) : nullptr;
+        PBS_CUDA(launch_trace(g, luts, ctView ? ctView : static_cast<const float*>(ct.ptr), quad, ctGrid.dims[0],
                               ctGrid.dims[1], ctGrid.dims[2], dDens, dWepl, dFi, dFo, trace.weplMin, dbs, stream),
                  "trace");
         if (trace.inOut) {

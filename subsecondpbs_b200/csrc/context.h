@@ -116,6 +116,10 @@ struct Context {
     int ctType = PBS_CT_AUTO;
     GridDesc ctGrid{};
     DevBuf ct;
+    // Packed copy of `ct` for the tracer (launch_ct_quad), built by set_ct; a CT
+    // uploaded by region or attached from elsewhere is sampled directly.
+    DevBuf ctQuad;
+    bool ctQuadValid = false;
     // A CT owned elsewhere on the same device (a server's resident patient),
     // used by the tracer in place of `ct` while set.
     const float* ctView = nullptr;

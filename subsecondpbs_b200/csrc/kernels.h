@@ -19,9 +19,16 @@ cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStrea
 // rayTracingBEVKernel (src/core/bev_ray_tracing.cu:65-159) as a segmented scan,
 // with the per-step WEPL minimum of sliceMinVarIgnoreNeverEnter
 // (src/core/raytracedicom_wrapper.cu:1991-2023) folded into its second pass.
-cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ctHu1000, int ctX, int ctY, int ctZ,
-                         float* density, float* wepl, int* firstInside, int* firstOutside, float* weplMin,
-                         BeamStateDev* beam, cudaStream_t s);
+// `ctQuad` (or null) is the packed copy of the CT from launch_ct_quad: the same
+// samples from two 16-byte loads instead of eight scattered ones.
+cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ctHu1000, const float4* ctQuad,
+                         int ctX, int ctY, int ctZ, float* density, float* wepl, int* firstInside, int* firstOutside,
+                         float* weplMin, BeamStateDev* beam, cudaStream_t s);
+// Packed CT for the trace: entry (x, y, z) = the HU+1000 values at (x, y), (x+1, y),
+// (x, y+1), (x+1, y+1) of slice z, zero outside the CT, over a grid padded by two
+// voxels below and two or three above in every axis.
+size_t ct_quad_bytes(const int dims[3]);
+cudaError_t launch_ct_quad(const float* ctHu1000, const int dims[3], float4* quad, cudaStream_t s);
 // Beam planner: guaranteed passive step, entry plane, per-layer cut-off steps and
 // entry sigmas (wrapper.cu:3651-3700, 3733-3833, 4302-4313).
 // fillBevFromWeqVolumeKernel + sliceMinVarIgnoreNeverEnter (wrapper.cu:1923-2023):

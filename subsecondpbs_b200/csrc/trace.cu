@@ -17,42 +17,20 @@ constexpr float kInf20 = 1.0e20f;  // the reference's INF stored in a float (Mac
 constexpr int kTraceSegments = 16;  // warps per tracing CTA; each marches one depth segment
 constexpr int kNone = 0x7fffffff;
 constexpr size_t kTraceCacheMaxBytes = 160 * 1024;  // CT samples kept on chip up to ~1280 steps
-
-// Trilinear sample of a [Z][Y][X] volume, texel centres at i + 0.5, zero outside
-// (sample3DLinearBorder, src/core/bev_ray_tracing.cu:16-61).
-__device__ __forceinline__ float ct_sample_border(const float* __restrict__ vol, int dx, int dy, int dz, float x, float y,
-                                                  float z) {
-    float fx = x - 0.5f, fy = y - 0.5f, fz = z - 0.5f;
-    fx = fminf(fmaxf(fx, -2.0f), float(dx) + 1.0f);
-    fy = fminf(fmaxf(fy, -2.0f), float(dy) + 1.0f);
-    fz = fminf(fmaxf(fz, -2.0f), float(dz) + 1.0f);
-    const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
-    const int x0 = int(flx), y0 = int(fly), z0 = int(flz);
-    const float tx = fx - flx, ty = fy - fly, tz = fz - flz;
-    auto at = [&](int xi, int yi, int zi) -> float {
-        if (xi < 0 || yi < 0 || zi < 0 || xi >= dx || yi >= dy || zi >= dz) return 0.0f;
-        return __ldg(vol + (static_cast<size_t>(zi) * dy + yi) * dx + xi);
-    };
-    const float c000 = at(x0, y0, z0), c100 = at(x0 + 1, y0, z0);
-    const float c010 = at(x0, y0 + 1, z0), c110 = at(x0 + 1, y0 + 1, z0);
-    const float c001 = at(x0, y0, z0 + 1), c101 = at(x0 + 1, y0, z0 + 1);
-    const float c011 = at(x0, y0 + 1, z0 + 1), c111 = at(x0 + 1, y0 + 1, z0 + 1);
-    const float c00 = c000 + (c100 - c000) * tx;
-    const float c10 = c010 + (c110 - c010) * tx;
-    const float c01 = c001 + (c101 - c001) * tx;
-    const float c11 = c011 + (c111 - c011) * tx;
-    const float c0 = c00 + (c10 - c00) * ty;
-    const float c1 = c01 + (c11 - c01) * ty;
-    return c0 + (c1 - c0) * tz;
-}
-
+// Packed CT: entry (x, y, z) holds the corners (x, y), (x+1, y), (x, y+1), (x+1, y+1)
+// of slice z, for x in [-2, dx + 1], y in [-2, dy + 1], z in [-2, dz + 2] (zero
+// outside the CT): every floor index the clamped sample point can take.
+constexpr int kQuadPad = 2;
 
 struct CtCorners {
     float c[8];
     float tx, ty, tz;
 };
 
-// The loads of ct_sample_border, issued ahead of the arithmetic (ct_combine).
+// Trilinear sample of a [Z][Y][X] volume, texel centres at i + 0.5, zero outside
+// (sample3DLinearBorder, src/core/bev_ray_tracing.cu:16-61), split into its eight
+// corner loads (ct_fetch) and its arithmetic (ct_combine) so that the loads of the
+// next sample can be issued first.
 __device__ __forceinline__ void ct_fetch(const float* __restrict__ vol, int dx, int dy, int dz, float x, float y,
                                          float z, CtCorners& o) {
     float fx = x - 0.5f, fy = y - 0.5f, fz = z - 0.5f;
@@ -82,6 +60,41 @@ __device__ __forceinline__ float ct_combine(const CtCorners& o) {
     return c0 + (c1 - c0) * o.tz;
 }
 
+// The same eight corners from the packed CT (ct_quad_kernel): two aligned 16-byte
+// loads, the border zeros stored in the padding.
+__device__ __forceinline__ void ct_fetch_quad(const float4* __restrict__ quad, int dx, int dy, int dz, float x,
+                                              float y, float z, CtCorners& o) {
+    float fx = x - 0.5f, fy = y - 0.5f, fz = z - 0.5f;
+    fx = fminf(fmaxf(fx, -2.0f), float(dx) + 1.0f);
+    fy = fminf(fmaxf(fy, -2.0f), float(dy) + 1.0f);
+    fz = fminf(fmaxf(fz, -2.0f), float(dz) + 1.0f);
+    const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+    const int x0 = int(flx), y0 = int(fly), z0 = int(flz);
+    o.tx = fx - flx;
+    o.ty = fy - fly;
+    o.tz = fz - flz;
+    const size_t px = size_t(dx) + kQuadPad + 2, py = size_t(dy) + kQuadPad + 2;
+    const size_t i = (size_t(z0 + kQuadPad) * py + size_t(y0 + kQuadPad)) * px + size_t(x0 + kQuadPad);
+    const float4 a = __ldg(quad + i), b = __ldg(quad + i + px * py);
+    o.c[0] = a.x;
+    o.c[1] = a.y;
+    o.c[2] = a.z;
+    o.c[3] = a.w;
+    o.c[4] = b.x;
+    o.c[5] = b.y;
+    o.c[6] = b.z;
+    o.c[7] = b.w;
+}
+
+template <bool kQuad>
+__device__ __forceinline__ void ct_fetch_any(const float* __restrict__ ct, const float4* __restrict__ quad, int dx,
+                                             int dy, int dz, V3 p, CtCorners& o) {
+    if (kQuad)
+        ct_fetch_quad(quad, dx, dy, dz, p.x, p.y, p.z, o);
+    else
+        ct_fetch(ct, dx, dy, dz, p.x, p.y, p.z, o);
+}
+
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
     const float y = v - comp;
     const float t = sum + y;
@@ -104,9 +117,10 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
 // With kCache the first pass keeps every CT sample of the segment in shared memory
 // ([segment step][lane], 128 B per step and warp) and the second pass reads them
 // back instead of sampling the CT again.
-template <bool kCache>
+template <bool kCache, bool kQuad>
 __global__ void __launch_bounds__(32 * kTraceSegments)
-trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX, int ctY, int ctZ,
+trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, const float4* __restrict__ ctQuad, int ctX,
+             int ctY, int ctZ,
              float* __restrict__ density, float* __restrict__ wepl, int* __restrict__ firstInside,
              int* __restrict__ firstOutside, unsigned* __restrict__ weplMinBits, BeamStateDev* __restrict__ beam) {
     extern __shared__ float shCache[];  // [kTraceSegments][seg][32] with kCache
@@ -140,10 +154,10 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
     if (active && s0 < s1) {
         V3 pos = pos0;
         CtCorners cur, nxt;
-        ct_fetch(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z, cur);
+        ct_fetch_any<kQuad>(ct, ctQuad, ctX, ctY, ctZ, pos, cur);
         for (int k = s0; k < s1; ++k) {
             const V3 posN = add(pos, inc);
-            if (k + 1 < s1) ct_fetch(ct, ctX, ctY, ctZ, posN.x, posN.y, posN.z, nxt);
+            if (k + 1 < s1) ct_fetch_any<kQuad>(ct, ctQuad, ctX, ctY, ctZ, posN, nxt);
             const float hu = ct_combine(cur);
             if (kCache) myCache[(k - s0) * 32] = hu;
             huSum += hu;
@@ -177,8 +191,14 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
         for (int k = s0; k < s1; ++k) {
             unsigned bits = 0xffffffffu;
             if (active) {
-                const float hu =
-                    kCache ? myCache[(k - s0) * 32] : ct_sample_border(ct, ctX, ctY, ctZ, pos.x, pos.y, pos.z);
+                float hu;
+                if (kCache) {
+                    hu = myCache[(k - s0) * 32];
+                } else {
+                    CtCorners c;
+                    ct_fetch_any<kQuad>(ct, ctQuad, ctX, ctY, ctZ, pos, c);
+                    hu = ct_combine(c);
+                }
                 cumHu += hu;
                 density[idx] = lut_linear_clamp(luts.density, luts.nDensity, hu * luts.densityScale + 0.5f);
                 const float sp = lut_linear_clamp(luts.sp, luts.nSp, hu * luts.spScale + 0.5f);
@@ -222,6 +242,23 @@ trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, int ctX,
             atomicMin(&beam->firstInside, wmin);
             atomicMax(&beam->firstOutside, wmax);
         }
+    }
+}
+
+// Packed CT (kQuadPad): one thread per entry.
+__global__ void ct_quad_kernel(const float* __restrict__ ct, int dx, int dy, int dz, float4* __restrict__ quad) {
+    const size_t px = size_t(dx) + kQuadPad + 2, py = size_t(dy) + kQuadPad + 2, pz = size_t(dz) + kQuadPad + 3;
+    const size_t n = px * py * pz;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % px) - kQuadPad;
+        const size_t r = i / px;
+        const int y = int(r % py) - kQuadPad;
+        const int z = int(r / py) - kQuadPad;
+        auto at = [&](int xi, int yi) -> float {
+            if (xi < 0 || yi < 0 || z < 0 || xi >= dx || yi >= dy || z >= dz) return 0.0f;
+            return ct[(size_t(z) * dy + yi) * dx + xi];
+        };
+        quad[i] = make_float4(at(x, y), at(x + 1, y), at(x, y + 1), at(x + 1, y + 1));
     }
 }
 
@@ -517,9 +554,21 @@ cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStrea
     return cudaGetLastError();
 }
 
-cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ct, int ctX, int ctY, int ctZ,
-                         float* density, float* wepl, int* firstInside, int* firstOutside, float* weplMin,
-                         BeamStateDev* beam, cudaStream_t s) {
+size_t ct_quad_bytes(const int dims[3]) {
+    return (size_t(dims[0]) + kQuadPad + 2) * (size_t(dims[1]) + kQuadPad + 2) * (size_t(dims[2]) + kQuadPad + 3) *
+           sizeof(float4);
+}
+
+cudaError_t launch_ct_quad(const float* ct, const int dims[3], float4* quad, cudaStream_t s) {
+    const size_t n = ct_quad_bytes(dims) / sizeof(float4);
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    ct_quad_kernel<<<blocks, 256, 0, s>>>(ct, dims[0], dims[1], dims[2], quad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float* ct, const float4* ctQuad, int ctX,
+                         int ctY, int ctZ, float* density, float* wepl, int* firstInside, int* firstOutside,
+                         float* weplMin, BeamStateDev* beam, cudaStream_t s) {
     // 0xff bytes: the largest unsigned pattern, the identity of the atomic minimum.
     cudaError_t e = cudaMemsetAsync(weplMin, 0xff, sizeof(float) * size_t(g.steps), s);
     if (e != cudaSuccess) return e;
@@ -528,15 +577,15 @@ cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float*
     const int seg = (g.steps + kTraceSegments - 1) / kTraceSegments;
     const size_t cache = static_cast<size_t>(kTraceSegments) * seg * 32 * sizeof(float);
     unsigned* mins = reinterpret_cast<unsigned*>(weplMin);
-    if (cache <= kTraceCacheMaxBytes) {
-        e = set_smem_limit(reinterpret_cast<const void*>(trace_kernel<true>), cache);
+    auto k = cache <= kTraceCacheMaxBytes ? (ctQuad ? trace_kernel<true, true> : trace_kernel<true, false>)
+                                          : (ctQuad ? trace_kernel<false, true> : trace_kernel<false, false>);
+    const size_t smem = cache <= kTraceCacheMaxBytes ? cache : 0;
+    if (smem) {
+        e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
         if (e != cudaSuccess) return e;
-        trace_kernel<true><<<grid, block, cache, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside,
-                                                      firstOutside, mins, beam);
-    } else {
-        trace_kernel<false><<<grid, block, 0, s>>>(g, luts, ct, ctX, ctY, ctZ, density, wepl, firstInside,
-                                                   firstOutside, mins, beam);
     }
+    k<<<grid, block, smem, s>>>(g, luts, ct, ctQuad, ctX, ctY, ctZ, density, wepl, firstInside, firstOutside, mins,
+                                beam);
     return cudaGetLastError();
 }
 
