@@ -72,7 +72,7 @@ struct TileArgs {
 // Table phase, accumulation phase and write-out of one tile at radius R.
 template <int R, int RMax>
 __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* __restrict__ EW,
-                                               int* __restrict__ out, unsigned* __restrict__ sMask,
+                                               int* __restrict__ out, unsigned* __restrict__ sCol,
                                                float* __restrict__ sSum, const TileArgs& a) {
     constexpr int H = kTileY + 2 * R;
     constexpr int Wo = kTileX + 2 * R;
@@ -83,19 +83,16 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
 
     // ---- table phase (complete_superposition.cu:298-307) --------------------
     // Sources without dose get zero rows, so the accumulation needs no per-source
-    // test; sMask[sy] collects the depositing sources of every source row and
-    // sSum[sy] their dose.
+    // test; sCol[sx] collects the depositing sources of every source column (one
+    // shared OR per depositing source) and sSum[sy] the dose of every source row.
     {
         const float dose = a.idd[a.src];
         const bool live = dose > 0.0f;
-        const unsigned mask = __ballot_sync(0xffffffffu, live);
+        if (live) atomicOr(&sCol[lane], 1u << warp);
         float rowDose = live ? dose : 0.0f;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
-        if (lane == 0) {
-            sMask[warp] = mask;
-            sSum[warp] = rowDose;
-        }
+        if (lane == 0) sSum[warp] = rowDose;
         float e[4 * Q];
         if (live) {
             float row[R + 1];
@@ -117,7 +114,8 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         const int pt = warp * kTileX + e4_col(lane);
 #pragma unroll
         for (int q = 0; q < Q; ++q) E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
-        for (int i = t; i < H * Wo; i += kThreads) out[i] = 0;
+        // H and Wo are even and `out` is 16-byte aligned.
+        for (int i = t; i < H * Wo / 4; i += kThreads) reinterpret_cast<int4*>(out)[i] = make_int4(0, 0, 0, 0);
     }
     __syncthreads();
 
@@ -146,9 +144,7 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
         constexpr int kPairs = kTileX * M;
         constexpr int kUnits = kGrouped ? S : (kPairs + 31) / 32;
         // Depositing sources of source column `lane`, as an 8-bit mask over sy.
-        unsigned colBits = 0;
-#pragma unroll
-        for (int sy = 0; sy < kTileY; ++sy) colBits |= ((sMask[sy] >> lane) & 1u) << sy;
+        const unsigned colBits = sCol[lane];
 #pragma unroll 1
         for (int u = warp; u < kUnits; u += kWarps) {
             int sx, d;  // d: |d| when mirrored, else the signed offset
@@ -218,6 +214,8 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
     __syncthreads();
 
     // ---- write-out -------------------------------------------------------------
+    // The column masks were last read before the barrier: clear them for the next tile.
+    if (t < kTileX) sCol[t] = 0;
     for (int i = t; i < H * Wo; i += kThreads) {
         const int q = out[i];
         const int oy = i / Wo, ox = i - oy * Wo;
@@ -227,13 +225,13 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
 
 // Chain of compile-time radii RLo..RHi; returns false if r is outside it.
 template <int R, int RHi, int RMax>
-__device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, int* out, unsigned* sMask,
+__device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, int* out, unsigned* sCol,
                                                 float* sSum, const TileArgs& a) {
     if (r == R) {
-        superpose_tile<R, RMax>(E4, EW, out, sMask, sSum, a);
+        superpose_tile<R, RMax>(E4, EW, out, sCol, sSum, a);
         return true;
     }
-    if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sMask, sSum, a);
+    if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sCol, sSum, a);
     return false;
 }
 
@@ -249,7 +247,7 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
     float* EW = sm + Shape<RHi>::kQ * kThreads * 4;                              // [256][EWS] idd_s e_s(k)
     int* out = reinterpret_cast<int*>(EW + kThreads * Shape<RHi>::kEWStride);   // [8+2R][32+2R] fixed-point footprint
     __shared__ int sItem[2];
-    __shared__ unsigned sMask[kTileY];
+    __shared__ unsigned sCol[kTileX];     // per source column: depositing sources over sy
     __shared__ float sSum[kTileY];
 
     const int t = threadIdx.x;
@@ -262,6 +260,7 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
     const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
 
     if (t == 0) sItem[0] = atomicAdd(counter, 1);
+    if (t < kTileX) sCol[t] = 0;
     __syncthreads();
     int buf = 0;
     for (;;) {
@@ -280,7 +279,7 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
         a.dst = bev + static_cast<size_t>(zRel) * bevPlane + static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX +
                 (tx * kTileX - R + kMaxR);
         a.bevX = g.bevX;
-        if (!dispatch_radius<RLo, RHi, RHi>(R, E4, EW, out, sMask, sSum, a)) {
+        if (!dispatch_radius<RLo, RHi, RHi>(R, E4, EW, out, sCol, sSum, a)) {
             if (t == 0) atomicOr(&beam->errorFlags, 2);
         }
         // Every thread is past the tile (and has read sItem[buf]) before the
