@@ -452,6 +452,8 @@ def run_ours(args):
             traffic = None
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_source = ("MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)" if "hbm_gbs" in peaks
+                  else "fallback: 6.65 TB/s, an earlier copy-bandwidth measurement on this pool")
     rays = stats["ray_dims"][0] * stats["ray_dims"][1]
     pad = stats["superp_dims"][0] * stats["superp_dims"][1]
     S = stats["tracer_steps"]
@@ -470,7 +472,8 @@ def run_ours(args):
         if stage_ms[k] > 0:
             gbs = b / (stage_ms[k] * 1e-3) / 1e9
             roof_stages.append({"stage": k, "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak,
-                                "unit": "GB/s", "frac": round(gbs / hbm_peak, 4), "algorithmic_bytes": b})
+                                "unit": "GB/s", "frac": round(gbs / hbm_peak, 4), "algorithmic_bytes": b,
+                                "peak_source": hbm_source})
 
     launches_per_step = int(stats["kernel_launches"]) + 2  # + dose reset and float readout
     cpu = None
