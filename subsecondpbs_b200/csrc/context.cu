@@ -100,6 +100,8 @@ Context::~Context() {
     if (stagingEvent) cudaEventDestroy(stagingEvent);
     if (copyStart) cudaEventDestroy(copyStart);
     if (doseCopied) cudaEventDestroy(doseCopied);
+    if (doseZeroed) cudaEventDestroy(doseZeroed);
+    if (bevCleared) cudaEventDestroy(bevCleared);
     if (copyStream) cudaStreamDestroy(copyStream);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
@@ -119,6 +121,8 @@ int Context::init(int gpu) {
     PBS_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
     PBS_CUDA(cudaEventCreateWithFlags(&copyStart, cudaEventDisableTiming), "cudaEventCreate");
     PBS_CUDA(cudaEventCreateWithFlags(&doseCopied, cudaEventDisableTiming), "cudaEventCreate");
+    PBS_CUDA(cudaEventCreateWithFlags(&doseZeroed, cudaEventDisableTiming), "cudaEventCreate");
+    PBS_CUDA(cudaEventCreateWithFlags(&bevCleared, cudaEventDisableTiming), "cudaEventCreate");
     PBS_CUDA(cudaEventCreateWithFlags(&stagingEvent, cudaEventDisableTiming), "cudaEventCreate");
     for (auto& e : ev) PBS_CUDA(cudaEventCreate(&e), "cudaEventCreate");
     // Callers of the reference-shaped entry points cannot pass options: the
@@ -471,7 +475,9 @@ int Context::set_dose_grid(const GridDesc& g) {
         return PBS_ERR_INVALID_ARGUMENT;
     }
     const size_t n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
-    int rc = dose64.ensure(n * 8);
+    int rc = join_side_work();
+    if (rc) return rc;
+    rc = dose64.ensure(n * 8);
     if (rc) return rc;
     doseGrid = g;
     hasDose = true;
@@ -486,6 +492,7 @@ int Context::reset_dose(const float* init, int onDevice) {
         return PBS_ERR_NOT_READY;
     }
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    if (int rc = join_side_work()) return rc;
     if (init && !onDevice) {
         // The copy waits for the work already on the context stream (the CT upload
         // among it, which the next beam needs first) and then overlaps that beam.
@@ -501,11 +508,18 @@ int Context::reset_dose(const float* init, int onDevice) {
     }
     pendingDoseInit = false;
     if (!init && doseBoxed && !doseExposed) {
-        // Zero outside the dirty box already: clearing the box clears the grid.
-        if (!box_empty(dirtyLo, dirtyHi))
+        // Zero outside the dirty box already: clearing the box clears the grid. The
+        // clear waits for the work on the context stream (the last readout) and
+        // then runs beside the next beam's trace; flush_dose_init joins it.
+        if (!box_empty(dirtyLo, dirtyHi)) {
+            PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
+            PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
             PBS_CUDA(launch_dose_box(static_cast<double*>(dose64.ptr), nullptr, doseGrid.dims, dirtyLo, dirtyHi,
-                                     stream),
+                                     copyStream),
                      "dose_box_zero");
+            PBS_CUDA(cudaEventRecord(doseZeroed, copyStream), "cudaEventRecord");
+            pendingDoseZero = true;
+        }
     } else {
         PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), init, n, stream), "dose_init");
     }
@@ -528,7 +542,20 @@ void Context::mark_dose_written(const int lo[3], const int hi[3]) {
     merge_box(dirtyLo, dirtyHi, a, b);
 }
 
+int Context::join_side_work() {
+    if (pendingDoseZero) {
+        PBS_CUDA(cudaStreamWaitEvent(stream, doseZeroed, 0), "cudaStreamWaitEvent");
+        pendingDoseZero = false;
+    }
+    if (pendingBevClear) {
+        PBS_CUDA(cudaStreamWaitEvent(stream, bevCleared, 0), "cudaStreamWaitEvent");
+        pendingBevClear = false;
+    }
+    return PBS_OK;
+}
+
 int Context::flush_dose_init() {
+    if (int rc = join_side_work()) return rc;
     if (!pendingDoseInit) return PBS_OK;
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
     PBS_CUDA(cudaStreamWaitEvent(stream, doseCopied, 0), "cudaStreamWaitEvent");
@@ -664,6 +691,7 @@ size_t Context::device_bytes() const {
 }
 
 void Context::release_beam_buffers() {
+    join_side_work();
     for (DevBuf* b : {&dens, &wepl, &weplMin, &rayW, &interm, &lattice, &iddBuf, &rsBuf, &bev, &cpb, &subspots,
                       &floatOut, &firstIn, &firstOut, &firstPassive, &codes, &work, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64,
@@ -716,6 +744,8 @@ int Context::adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int grad
 
 int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    // Buffers may be resized below: nothing of an earlier beam may still be clearing them.
+    if (int jrc = join_side_work()) return jrc;
     if (!hasEnergy || !hasCt || !hasDose) {
         set_error("context needs lookup tables, CT and dose grid before add_beam");
         return PBS_ERR_NOT_READY;
@@ -973,7 +1003,13 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
         return PBS_OK;
     };
 
-    PBS_CUDA(cudaMemsetAsync(dBev, 0, S * g.bevX * g.bevY * 4, stream), "memset BEV");
+    // The BEV clear runs beside the trace, the planner and the fluence kernels;
+    // the superposition waits for it.
+    PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
+    PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
+    PBS_CUDA(cudaMemsetAsync(dBev, 0, S * g.bevX * g.bevY * 4, copyStream), "memset BEV");
+    PBS_CUDA(cudaEventRecord(bevCleared, copyStream), "cudaEventRecord");
+    pendingBevClear = true;
     if ((rc = mark(0))) return rc;
     static_assert(offsetof(BeamStateDev, firstOutside) == offsetof(BeamStateDev, firstInside) + sizeof(int),
                   "the trace's beam steps are two adjacent ints");
@@ -1025,6 +1061,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
     float* dNucRs = static_cast<float*>(nucRsBuf.ptr);
     LayerStateDev* dNucLs = static_cast<LayerStateDev*>(nucLs.ptr);
     BeamStateDev* dNucBs = static_cast<BeamStateDev*>(nucBs.ptr);
+    if ((rc = join_side_work())) return rc;
     for (int l0 = 0; l0 < L; l0 += chunk) {
         const int nl = std::min(chunk, L - l0);
         if (nuclear) PBS_CUDA(launch_nuc_prepare(nucGeom, nl, dNucIdd, dNucRs, stream), "nuc_prepare");

@@ -82,6 +82,11 @@ struct Context {
     // before the first kernel that needs it (flush_dose_init).
     cudaStream_t copyStream = nullptr;
     cudaEvent_t copyStart = nullptr, doseCopied = nullptr;
+    // Clears that no kernel needs until later in a beam run on copyStream as well:
+    // the zeroing of the dose grid's dirty box (joined before anything reads or
+    // rewrites the grid) and the BEV clear (joined before the superposition).
+    cudaEvent_t doseZeroed = nullptr, bevCleared = nullptr;
+    bool pendingDoseZero = false, pendingBevClear = false;
     bool pendingDoseInit = false;
     // While doseBoxed is set, the FP64 grid is exactly zero outside the inclusive
     // voxel box [dirtyLo, dirtyHi]: the union of the transfer boxes of the beams
@@ -163,6 +168,8 @@ struct Context {
     int take_device_errors();
     // Enqueues the deferred initialisation of the FP64 grid from a host dose.
     int flush_dose_init();
+    // Makes the context stream wait for the clears still running on copyStream.
+    int join_side_work();
     int set_ct(const float* data, int onDevice, const GridDesc& g);
     // Wrapper path, where every beam is known before any upload: host copies limited
     // to boxes [lo, hi] (inclusive voxel indices) of the CT and of the dose grid.
