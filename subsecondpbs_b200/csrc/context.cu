@@ -717,6 +717,10 @@ int Context::attach_ct(const float* deviceCt, const GridDesc& g, int type) {
 
 int Context::add_beam(const PbsBeamDesc& b, int nuclear) { return run_beam(b, nuclear, nullptr); }
 
+int Context::add_planned_beam(const PbsBeamDesc& b, int nuclear, BeamPlan&& planned) {
+    return run_beam(b, nuclear, nullptr, &planned);
+}
+
 int Context::adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int gradOnDevice, float* gradSpots,
                           size_t nSpots) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
@@ -742,7 +746,7 @@ int Context::adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int grad
     return run_beam(b, 0, &a);
 }
 
-int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj) {
+int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
     // Buffers may be resized below: nothing of an earlier beam may still be clearing them.
     if (int jrc = join_side_work()) return jrc;
@@ -767,8 +771,10 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj)
         return PBS_ERR_INVALID_ARGUMENT;
     }
     lastBeamValid = false;
-    int rc = plan_beam(b, energy, ctGrid, doseGrid, plan, err);
-    if (rc) {
+    int rc = PBS_OK;
+    if (planned) {
+        plan = std::move(*planned);
+    } else if ((rc = plan_beam(b, energy, ctGrid, doseGrid, plan, err))) {
         set_error(err);
         return rc;
     }
@@ -1519,13 +1525,14 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
     }
     int rc;
     if ((rc = ctx->set_energy(*energyData))) return rc;
-    // Every beam is planned up front (add_beam plans it again; it is cheap): the CT
+    // Every beam is planned up front, and the plan is handed to add_planned_beam: the CT
     // voxels their tracers can sample and the dose voxels their transfers can write
     // bound the host copies of this call.
     int ctLo[3] = {INT_MAX, INT_MAX, INT_MAX}, ctHi[3] = {-1, -1, -1};
     int dLo[3] = {INT_MAX, INT_MAX, INT_MAX}, dHi[3] = {-1, -1, -1};
+    std::vector<BeamPlan> plans(numBeams);
     for (size_t i = 0; i < numBeams; ++i) {
-        BeamPlan P;
+        BeamPlan& P = plans[i];
         std::string perr;
         if ((rc = plan_beam(beams[i], ctx->energy, cg, dg, P, perr))) {
             set_error(perr);
@@ -1550,7 +1557,8 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
     if ((rc = ctx->set_dose_grid(dg))) return rc;
     if ((rc = ctx->reset_dose_region(doseData, dLo, dHi))) return rc;
     for (size_t i = 0; i < numBeams; ++i) {
-        if ((rc = ctx->add_beam(beams[i], nuclear))) return rc;
+        // The plan made above used the same tables and grids as the context now holds.
+        if ((rc = ctx->add_planned_beam(beams[i], nuclear, std::move(plans[i])))) return rc;
         if (verbose > 0) {
             PbsBeamStats st;
             if (ctx->beam_stats(&st) == PBS_OK)

@@ -196,6 +196,9 @@ struct Context {
     int read_dose(float* out, int onDevice);
     int read_dose64(double* out, int onDevice);
     int add_beam(const PbsBeamDesc& b, int nuclear);
+    // add_beam with the beam's plan already made against this context's tables and
+    // grids (plan_beam); the plan is moved into the context.
+    int add_planned_beam(const PbsBeamDesc& b, int nuclear, BeamPlan&& planned);
     // Gradient of <gradDose, dose of the beam> with respect to the beam's spot
     // weights (one float per spot, host memory); gradDose is FP64 [Z][Y][X].
     int adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int gradOnDevice, float* gradSpots, size_t nSpots);
@@ -204,7 +207,7 @@ struct Context {
         float* gradSpots;
         size_t nSpots;
     };
-    int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj);
+    int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned = nullptr);
     int finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b);
     int beam_stats(PbsBeamStats* out);
     int layer_stats(int layer, PbsLayerStats* out);
