@@ -342,6 +342,24 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
     // The CT type comes from the whole volume, as with a full upload.
     int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
     if (type == PBS_CT_AUTO) {
+        // A page-locked host CT is visible to the device: the samples are read and the
+        // type detected there, and the conversion follows without a host pass. The
+        // caller's buffer outlives the call (the wrapper synchronises before returning).
+        cudaPointerAttributes at{};
+        const bool mapped = cudaPointerGetAttributes(&at, data) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+                            at.devicePointer != nullptr;
+        cudaGetLastError();
+        const int lutN = int(densityHost.size());
+        if (mapped && hasEnergy && lutN > 0 && energy.density_scale_fact != 0.0f && stats.ensure(64) == PBS_OK) {
+            PBS_CUDA(launch_ct_convert_detect(static_cast<float*>(ct.ptr), n, static_cast<const float*>(at.devicePointer),
+                                              static_cast<const float*>(density.ptr), lutN, energy.density_scale_fact,
+                                              static_cast<unsigned*>(stats.ptr), stream),
+                     "ct_convert_detect");
+            ctType = PBS_CT_AUTO;
+            ctGrid = g;
+            hasCt = true;
+            return PBS_OK;
+        }
         float mn, mx;
         sample_ct_stats(data, n, mn, mx);
         type = auto_detect_ct_type(mn, mx);

@@ -14,6 +14,12 @@ cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, i
                               cudaStream_t s);
 // min/max of a strided sample (the reference's ~100k-sample statistics).
 cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStream_t s);
+// The reference's ~100k-sample type detection and the conversion in one pass on
+// the device: the samples are read from the caller's page-locked host CT through
+// its device mapping (`hostCtMapped`, n values), the conversion runs on the
+// uploaded `ct`. `keys` is two words of device scratch.
+cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const float* densityLut,
+                                     int lutN, float lutScale, unsigned* keys, cudaStream_t s);
 
 // ---- tracing ------------------------------------------------------------------
 // rayTracingBEVKernel (src/core/bev_ray_tracing.cu:65-159) as a segmented scan,

@@ -473,8 +473,23 @@ __global__ void beam_planner_kernel(BeamGeomDev g, float* __restrict__ weplMin,
     }
 }
 
+// Type detection of the reference's CT adapter (wrapper.cu:2327-2337) on the sample
+// minimum and maximum.
+__device__ __forceinline__ int ct_type_from_range(float mn, float mx) {
+    if (mn < -200.0f) return PBS_CT_HU;
+    if (mx <= 20.0f && mn >= 0.0f) return PBS_CT_DENSITY;
+    return PBS_CT_HU_PLUS_1000;
+}
+
+// With `rangeKeys` (order keys of the sample minimum and maximum, from
+// ct_sample_range_kernel) the type is detected here; `lut` is then the density
+// table, the only one detection can call for.
 __global__ void ct_convert_kernel(float* ct, size_t n, int type, const float* __restrict__ lut, int lutN,
-                                  float lutScale) {
+                                  float lutScale, const unsigned* __restrict__ rangeKeys) {
+    if (rangeKeys) {
+        type = ct_type_from_range(float_from_order_key(rangeKeys[0]), float_from_order_key(rangeKeys[1]));
+        if (type == PBS_CT_HU_PLUS_1000) return;
+    }
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         const float v = ct[i];
         if (type == PBS_CT_HU) {
@@ -511,6 +526,25 @@ __global__ void ct_convert_kernel(float* ct, size_t n, int type, const float* __
     }
 }
 
+// The reference's strided sample (every `stride`-th value, wrapper.cu:2307-2325), one
+// thread per sample, reduced into order keys of its minimum and maximum (NaN is
+// left out, as under std::min / std::max). Used on the caller's page-locked host CT
+// through its device mapping, so that the CT type is known without a host pass.
+__global__ void ct_sample_range_kernel(const float* __restrict__ ct, size_t stride, size_t samples, unsigned* keys) {
+    const size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    unsigned lo = 0xffffffffu, hi = 0u;
+    if (k < samples) {
+        const float v = ct[k * stride];
+        if (v == v) lo = hi = float_order_key(v);
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        if (lo != 0xffffffffu) atomicMin(keys, lo);
+        if (hi != 0u) atomicMax(keys + 1, hi);
+    }
+}
+
 __global__ void ct_stats_kernel(const float* __restrict__ ct, size_t n, size_t stride, float* minmax) {
     float mn = ct[0], mx = ct[0];
     for (size_t i = size_t(threadIdx.x) * stride; i < n; i += size_t(blockDim.x) * stride) {
@@ -543,7 +577,22 @@ cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, i
                               cudaStream_t s) {
     if (type == PBS_CT_HU_PLUS_1000 || n == 0) return cudaSuccess;
     const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
-    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, type, lut, lutN, lutScale);
+    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, type, lut, lutN, lutScale, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const float* densityLut,
+                                     int lutN, float lutScale, unsigned* keys, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const size_t maxSamples = 100000;
+    const size_t stride = (n > maxSamples) ? (n / maxSamples) : 1;
+    const size_t samples = (n + stride - 1) / stride;
+    cudaError_t e = cudaMemsetAsync(keys, 0xff, sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(keys + 1, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    ct_sample_range_kernel<<<unsigned((samples + 255) / 256), 256, 0, s>>>(hostCtMapped, stride, samples, keys);
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, PBS_CT_AUTO, densityLut, lutN, lutScale, keys);
     return cudaGetLastError();
 }
 

@@ -64,3 +64,40 @@ def test_wrapper_regions_with_the_halo(hetero_small_case):
     got = _wrapper(case, [case["beam"]], initial, nuclear=True)
     want = run_gpu(case, keep_debug=False, nuclear_model=L.NUCLEAR_GAUSS_FIT).read_dose()
     _same(got, want, initial)
+
+
+def _wrapper_ct(case, beam, ct):
+    """The wrapper on one beam with `ct` given as a numpy array (pageable) or a
+    page-locked torch tensor; returns the dose."""
+    lib = L.load()
+    d, keep = L.beam_desc(beam)
+    ed, ke = L.energy_desc(_with_luts(case["energy"], None))
+    dose = np.zeros(tuple(reversed(case["dose_dims"])), dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    ptr = C.cast(C.c_void_p(ct.data_ptr()), fp) if hasattr(ct, "data_ptr") else ct.ctypes.data_as(fp)
+    L.check(lib.pbs_subsecond_wrapper(ptr, L.int3(case["ct_dims"]), L.float3(case["ct_resolution"]),
+                                      L.float3(case["ct_corner"]), dose.ctypes.data_as(fp), L.int3(case["dose_dims"]),
+                                      L.float3(case["dose_resolution"]), L.float3(case["dose_corner"]), C.byref(d), 1,
+                                      C.byref(ed), 0, 0, 0))
+    del keep, ke
+    return dose
+
+
+@pytest.mark.parametrize("form", ["hu+1000", "hu", "density"])
+def test_page_locked_ct_detects_the_same_type(hetero_small_case, form):
+    """A page-locked host CT has its type detected on the device from the same
+    samples: the dose equals the one from a pageable copy of the same CT, for
+    each of the three types detection can choose."""
+    import torch
+
+    case = hetero_small_case
+    ct = np.ascontiguousarray(case["ct"], dtype=np.float32)
+    if form == "hu":
+        ct = ct - 1000.0
+    elif form == "density":
+        ct = np.clip(ct / 1000.0, 0.0, 2.0).astype(np.float32)
+    want = _wrapper_ct(case, case["beam"], ct)
+    got = _wrapper_ct(case, case["beam"], torch.from_numpy(ct.copy()).pin_memory())
+    m = float(np.abs(want).max())
+    assert m > 0
+    assert float(np.abs(got - want).max()) <= 1e-6 * m
