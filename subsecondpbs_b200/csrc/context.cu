@@ -380,11 +380,24 @@ int Context::reset_dose_region(const float* init, const int lo[3], const int hi[
     // Voxels outside the box are initialised from stale values; no beam of the
     // call writes them and read_dose_region does not copy them back.
     doseBoxed = false;
+    deferredInit = init;
+    for (int i = 0; i < 3; ++i) {
+        deferredLo[i] = lo[i];
+        deferredHi[i] = hi[i];
+    }
+    pendingDoseInit = true;
+    return PBS_OK;
+}
+
+int Context::issue_dose_copy() {
+    if (!deferredInit) return PBS_OK;
     PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
     PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
-    PBS_CUDA(copy_box(floatOut.ptr, init, doseGrid.dims, lo, hi, cudaMemcpyHostToDevice, copyStream), "dose H2D");
+    PBS_CUDA(copy_box(floatOut.ptr, deferredInit, doseGrid.dims, deferredLo, deferredHi, cudaMemcpyHostToDevice,
+                      copyStream),
+             "dose H2D");
     PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
-    pendingDoseInit = true;
+    deferredInit = nullptr;
     return PBS_OK;
 }
 
@@ -500,6 +513,7 @@ int Context::set_dose_grid(const GridDesc& g) {
     doseGrid = g;
     hasDose = true;
     doseBoxed = false;
+    deferredInit = nullptr;
     return reset_dose(nullptr, 0);
 }
 
@@ -511,6 +525,7 @@ int Context::reset_dose(const float* init, int onDevice) {
     }
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
     if (int rc = join_side_work()) return rc;
+    deferredInit = nullptr;  // superseded
     if (init && !onDevice) {
         // The copy waits for the work already on the context stream (the CT upload
         // among it, which the next beam needs first) and then overlaps that beam.
@@ -575,6 +590,7 @@ int Context::join_side_work() {
 int Context::flush_dose_init() {
     if (int rc = join_side_work()) return rc;
     if (!pendingDoseInit) return PBS_OK;
+    if (int rc = issue_dose_copy()) return rc;
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
     PBS_CUDA(cudaStreamWaitEvent(stream, doseCopied, 0), "cudaStreamWaitEvent");
     PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), static_cast<const float*>(floatOut.ptr), n, stream),
@@ -1066,6 +1082,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         }
     }
     if ((rc = mark(1))) return rc;
+    if ((rc = issue_dose_copy())) return rc;
     PBS_CUDA(launch_beam_planner(g, trace.weplMin, dlp, dls, dbs, stream), "beam_planner");
     if ((rc = mark(2))) return rc;
     if (P.hasLattice) {

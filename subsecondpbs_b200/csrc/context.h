@@ -88,6 +88,12 @@ struct Context {
     cudaEvent_t doseZeroed = nullptr, bevCleared = nullptr;
     bool pendingDoseZero = false, pendingBevClear = false;
     bool pendingDoseInit = false;
+    // The wrapper path's initial-dose box copy, issued once the beam's own uploads and
+    // its trace are enqueued (issue_dose_copy) so that it does not hold them back on
+    // the copy engine; the caller's buffer outlives the wrapper call.
+    const float* deferredInit = nullptr;
+    int deferredLo[3] = {0, 0, 0}, deferredHi[3] = {-1, -1, -1};
+    int issue_dose_copy();
     // While doseBoxed is set, the FP64 grid is exactly zero outside the inclusive
     // voxel box [dirtyLo, dirtyHi]: the union of the transfer boxes of the beams
     // added since the last zeroing reset. Such a reset then clears only that box,
