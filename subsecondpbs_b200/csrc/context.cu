@@ -358,13 +358,31 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
             ctType = PBS_CT_AUTO;
             ctGrid = g;
             hasCt = true;
-            return PBS_OK;
+            return build_ct_quad_box(lo, hi);
         }
         float mn, mx;
         sample_ct_stats(data, n, mn, mx);
         type = auto_detect_ct_type(mn, mx);
     }
-    return convert_ct(type, g);
+    if ((rc = convert_ct(type, g))) return rc;
+    return build_ct_quad_box(lo, hi);
+}
+
+int Context::build_ct_quad_box(const int lo[3], const int hi[3]) {
+    // The packed copy is an optimisation: without room for it the tracer samples
+    // the CT directly.
+    ctQuadValid = false;
+    if (box_empty(lo, hi)) return PBS_OK;
+    if (ctQuad.ensure(ct_quad_bytes(ctGrid.dims)) != PBS_OK) {
+        cudaGetLastError();
+        set_error("");
+        return PBS_OK;
+    }
+    PBS_CUDA(launch_ct_quad_box(static_cast<const float*>(ct.ptr), ctGrid.dims, lo, hi,
+                                static_cast<float4*>(ctQuad.ptr), stream),
+             "ct_quad_box");
+    ctQuadValid = true;
+    return PBS_OK;
 }
 
 int Context::reset_dose_region(const float* init, const int lo[3], const int hi[3]) {

@@ -127,8 +127,9 @@ struct Context {
     int ctType = PBS_CT_AUTO;
     GridDesc ctGrid{};
     DevBuf ct;
-    // Packed copy of `ct` for the tracer (launch_ct_quad), built by set_ct; a CT
-    // uploaded by region or attached from elsewhere is sampled directly.
+    // Packed copy of `ct` for the tracer (launch_ct_quad), built by set_ct, and by
+    // set_ct_region over the uploaded box; a CT attached from elsewhere is sampled
+    // directly.
     DevBuf ctQuad;
     bool ctQuadValid = false;
     // A CT owned elsewhere on the same device (a server's resident patient),
@@ -182,6 +183,8 @@ struct Context {
     // The rest of the device CT is not read by those beams; the rest of the dose
     // grid is not written by them, so the caller's buffer keeps its values there.
     int set_ct_region(const float* data, const GridDesc& g, const int lo[3], const int hi[3]);
+    // Packed CT entries of the uploaded box only (set_ct_region).
+    int build_ct_quad_box(const int lo[3], const int hi[3]);
     int reset_dose_region(const float* init, const int lo[3], const int hi[3]);
     int read_dose_region(float* out, const int lo[3], const int hi[3]);
     int convert_ct(int type, const GridDesc& g);

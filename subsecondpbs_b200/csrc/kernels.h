@@ -35,6 +35,10 @@ cudaError_t launch_trace(const BeamGeomDev& g, const LutsDev& luts, const float*
 // voxels below and two or three above in every axis.
 size_t ct_quad_bytes(const int dims[3]);
 cudaError_t launch_ct_quad(const float* ctHu1000, const int dims[3], float4* quad, cudaStream_t s);
+// The packed entries of the voxels in the inclusive box [lo, hi] only (a CT uploaded
+// by region: its tracers sample inside the box, two voxels in from its faces).
+cudaError_t launch_ct_quad_box(const float* ctHu1000, const int dims[3], const int lo[3], const int hi[3],
+                               float4* quad, cudaStream_t s);
 // Beam planner: guaranteed passive step, entry plane, per-layer cut-off steps and
 // entry sigmas (wrapper.cu:3651-3700, 3733-3833, 4302-4313).
 // fillBevFromWeqVolumeKernel + sliceMinVarIgnoreNeverEnter (wrapper.cu:1923-2023):

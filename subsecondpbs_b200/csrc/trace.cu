@@ -608,6 +608,44 @@ size_t ct_quad_bytes(const int dims[3]) {
            sizeof(float4);
 }
 
+// Packed entries (x, y, z) for x, y, z in [lo, lo + ext) only; lo may reach into the
+// padding (negative, or past the CT), where the entries hold the border zeros.
+__global__ void ct_quad_box_kernel(const float* __restrict__ ct, int dx, int dy, int dz, int3 lo, int3 ext,
+                                   float4* __restrict__ quad) {
+    const size_t px = size_t(dx) + kQuadPad + 2, py = size_t(dy) + kQuadPad + 2;
+    const size_t total = size_t(ext.x) * ext.y * ext.z;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = lo.x + int(i % size_t(ext.x));
+        const size_t r = i / size_t(ext.x);
+        const int y = lo.y + int(r % size_t(ext.y));
+        const int z = lo.z + int(r / size_t(ext.y));
+        auto at = [&](int xi, int yi) -> float {
+            if (xi < 0 || yi < 0 || z < 0 || xi >= dx || yi >= dy || z >= dz) return 0.0f;
+            return ct[(size_t(z) * dy + yi) * dx + xi];
+        };
+        quad[(size_t(z + kQuadPad) * py + size_t(y + kQuadPad)) * px + size_t(x + kQuadPad)] =
+            make_float4(at(x, y), at(x + 1, y), at(x, y + 1), at(x + 1, y + 1));
+    }
+}
+
+cudaError_t launch_ct_quad_box(const float* ct, const int dims[3], const int lo[3], const int hi[3], float4* quad,
+                               cudaStream_t s) {
+    int a[3], b[3];
+    for (int i = 0; i < 3; ++i) {
+        if (lo[i] < 0 || hi[i] >= dims[i] || hi[i] < lo[i]) return cudaErrorInvalidValue;
+        // A box on a face of the CT takes the padding beyond that face along: the
+        // tracer clamps sample points outside the CT into it.
+        a[i] = lo[i] == 0 ? -kQuadPad : lo[i];
+        b[i] = hi[i] == dims[i] - 1 ? dims[i] - 1 + kQuadPad + (i == 2 ? 1 : 0) : hi[i];
+    }
+    const int3 l = make_int3(a[0], a[1], a[2]);
+    const int3 e = make_int3(b[0] - a[0] + 1, b[1] - a[1] + 1, b[2] - a[2] + 1);
+    const size_t total = size_t(e.x) * e.y * e.z;
+    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 16));
+    ct_quad_box_kernel<<<blocks, 256, 0, s>>>(ct, dims[0], dims[1], dims[2], l, e, quad);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ct_quad(const float* ct, const int dims[3], float4* quad, cudaStream_t s) {
     const size_t n = ct_quad_bytes(dims) / sizeof(float4);
     const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
