@@ -6,15 +6,16 @@
 namespace pbs {
 
 // tex1D with linear filtering, clamp addressing and unnormalised coordinates
-// (texel i centred at i + 0.5), evaluated with full-precision weights.
+// (texel i centred at i + 0.5), evaluated with full-precision weights. The texel
+// coordinate is clamped to [0, n - 1] before the split into index and weight: below
+// the table and past its end the filter returns the edge texel either way (the two
+// taps coincide or the weight is 0), and a NaN coordinate gives texel 0.
 __device__ __forceinline__ float lut_linear_clamp(const float* __restrict__ t, int n, float x) {
-    float xb = x - 0.5f;
-    xb = fminf(fmaxf(xb, -1.0f), float(n));
+    const float xb = fminf(fmaxf(x - 0.5f, 0.0f), float(n - 1));
     const float fl = floorf(xb);
-    const int i = int(fl);
+    const int i0 = int(fl);
+    const int i1 = min(i0 + 1, n - 1);
     const float a = xb - fl;
-    const int i0 = min(max(i, 0), n - 1);
-    const int i1 = min(max(i + 1, 0), n - 1);
     const float v0 = __ldg(t + i0), v1 = __ldg(t + i1);
     return v0 + (v1 - v0) * a;
 }
@@ -30,13 +31,11 @@ __device__ __forceinline__ float float_from_order_key(unsigned k) {
 
 // Same lookup on a table staged in shared memory.
 __device__ __forceinline__ float lut_linear_clamp_smem(const float* t, int n, float x) {
-    float xb = x - 0.5f;
-    xb = fminf(fmaxf(xb, -1.0f), float(n));
+    const float xb = fminf(fmaxf(x - 0.5f, 0.0f), float(n - 1));
     const float fl = floorf(xb);
-    const int i = int(fl);
+    const int i0 = int(fl);
+    const int i1 = min(i0 + 1, n - 1);
     const float a = xb - fl;
-    const int i0 = min(max(i, 0), n - 1);
-    const int i1 = min(max(i + 1, 0), n - 1);
     const float v0 = t[i0], v1 = t[i1];
     return v0 + (v1 - v0) * a;
 }
