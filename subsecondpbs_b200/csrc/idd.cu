@@ -50,7 +50,11 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
     int* partLive = reinterpret_cast<int*>(partMin + g.steps * 8);  // [steps][8]
     __shared__ int shHist[kBuckets], shLive[kBuckets], shPassive[8];
 
-    const int lc = blockIdx.z;
+    // Longest walks first: the layers are dispatched from the end of the chunk whose
+    // cut-off step is deeper, so that the long CTAs do not form the grid's tail.
+    const int nl = int(gridDim.z);
+    const bool deepLast = ls[layer0].afterLast < ls[layer0 + nl - 1].afterLast;
+    const int lc = deepLast ? nl - 1 - int(blockIdx.z) : int(blockIdx.z);
     const int l = layer0 + lc;
     const int tx = blockIdx.x, ty = blockIdx.y;
     const int lane = threadIdx.x, warp = threadIdx.y;
