@@ -228,9 +228,10 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
     w = phantoms.serving_workload(n_requests=n_requests)
     prepared = [[_lib.beam_desc(b) for b in phantoms.request_beams(w, r)] for r in w["requests"]]
     check = set(range(0, n_requests, max(1, n_requests // 16)))
-    warm = min(50, n_requests)
-    head = dict(w, requests=w["requests"][:warm])
-    serving.plain_pipeline(head, prepared[:warm], local)
+    # Both sides are measured warm, as a long-running service: one untimed pass of the
+    # whole stream first, so that the plain pipeline's context and the server's slots
+    # hold their largest buffers and the server its per-field traces.
+    serving.plain_pipeline(w, prepared, local)
     plain = serving.plain_pipeline(w, prepared, local, keep=check)
     ps = plain["service_s"] * 1e3
     srv = serving.DoseServer(local, slots=slots, hbm_budget_mib=budget_mib)
@@ -238,7 +239,7 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
     srv.add_energy(1, w["energy"]["carbon"])
     for p in w["patients"]:
         srv.add_patient(p["id"], p["ct"], p["ct_dims"], p["ct_resolution"], p["ct_corner"])
-    serving.serve_workload(srv, head, prepared[:warm], arrivals=False)
+    serving.serve_workload(srv, w, prepared, arrivals=False)
     sat = serving.serve_workload(srv, w, prepared, arrivals=False, keep=check)
     rate = 0.8 * sat["plans_per_s"]
     poi = serving.serve_workload(srv, serving.with_rate(w, rate), prepared, arrivals=True)
@@ -254,6 +255,7 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
         "workload": f"{n_requests} requests, {len(w['patients'])} patients (CT 128^3@2mm, 256x256x160@2mm, "
                     "512x512x200@1mm), 1-4 beams of 500-20000 spots (Pareto 1.1), 80/20 proton/carbon+halo",
         "slots": slots, "hbm_budget_mib": budget_mib or "90% of free",
+        "warmup": "one untimed pass of the whole stream on each side",
         "plain": {"plans_per_s": round(plain["plans_per_s"], 2), "p50_ms": pct(ps, 0.5), "p99_ms": pct(ps, 0.99),
                   "api": "pbs_subsecond_wrapper per request, pinned host CT and dose"},
         "saturated": {"plans_per_s": round(sat["plans_per_s"], 2), "p50_ms": pct(sl, 0.5), "p99_ms": pct(sl, 0.99),
