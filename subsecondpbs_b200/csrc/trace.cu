@@ -118,7 +118,9 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
 // ([segment step][lane], 128 B per step and warp) and the second pass reads them
 // back instead of sampling the CT again.
 template <bool kCache, bool kQuad>
-__global__ void __launch_bounds__(32 * kTraceSegments)
+// Three CTAs per SM (at most 42 registers): the headline grid of 416 row CTAs then
+// runs as one wave instead of 1.4.
+__global__ void __launch_bounds__(32 * kTraceSegments, 3)
 trace_kernel(BeamGeomDev g, LutsDev luts, const float* __restrict__ ct, const float4* __restrict__ ctQuad, int ctX,
              int ctY, int ctZ,
              float* __restrict__ density, float* __restrict__ wepl, int* __restrict__ firstInside,
