@@ -270,6 +270,46 @@ PBS_API int pbs_context_add_beam(PbsContext* ctx, const PbsBeamDesc* beam, int n
 PBS_API int pbs_context_adjoint_beam(PbsContext* ctx, const PbsBeamDesc* beam, const double* grad_dose,
                                      int grad_on_device, float* grad_weights, size_t n_weights);
 /* Convert the accumulator to float and copy it out (host or device pointer). */
+/* ---- operator mode (rtd_operator_mode.h) ---------------------------------- */
+/* Mirrors RTDOperatorLayerSpan / RTDOperatorBatch (include/core/rtd_operator_mode.h:18-32). */
+typedef struct PbsOperatorLayerSpan {
+    int layer_index;
+    int spot_begin;
+    int spot_count;
+    float energy;
+    float longitudinal_cutoff;
+} PbsOperatorLayerSpan;
+
+typedef struct PbsOperatorBatch {
+    int batch_index;
+    int spot_begin;
+    int spot_count;
+    int first_layer_index;
+    int last_layer_index;
+} PbsOperatorBatch;
+
+/* Replaces buildRTDOperatorBatchPlan (include/core/rtd_operator_mode.h:43-111).
+ * info[6] = {valid, total_layers, total_spots, max_spots_per_batch, n_spans,
+ * n_batches}; an invalid beam gives valid = 0 with the fields filled so far, as
+ * the reference does. NULL spans/batches query the counts only; otherwise the
+ * capacities must hold n_spans / n_batches (else PBS_ERR_INVALID_ARGUMENT).
+ * Host only: needs no GPU. */
+PBS_API int pbs_operator_batch_plan(const PbsBeamDesc* beam, int max_spots_per_batch, PbsOperatorLayerSpan* spans,
+                                    int span_capacity, PbsOperatorBatch* batches, int batch_capacity, int info[6]);
+
+/* Spot-preserving dose-influence matrix of spots [spot_begin, spot_begin +
+ * spot_count) of `beam` in compressed sparse columns, the export that
+ * rtd_operator_mode.h:1-8 plans and cuCalDose3 (raytracedicom_pybind.cpp:1955-2053)
+ * leaves zeroed. Column j = dose per unit weight of spot spot_begin + j with the
+ * beam's own plan; rows are linear voxel indices (z*Y + y)*X + x in ascending
+ * order; entries with |dose| > threshold (Gy per unit weight, >= 0). Host outputs:
+ * col_ptr[spot_count + 1] from 0, rows/values of `capacity` entries. *nnz is set
+ * even when it exceeds `capacity`, which returns PBS_ERR_INVALID_ARGUMENT (col_ptr
+ * filled, rows/values not). Replaces the context's dose with zero. */
+PBS_API int pbs_context_influence_csc(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction,
+                                      long long spot_begin, long long spot_count, double threshold,
+                                      long long* col_ptr, int* rows, float* values, long long capacity,
+                                      long long* nnz);
 PBS_API int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device);
 /* Copy the FP64 accumulator [Z][Y][X] out (host or device pointer), e.g. for a
  * cross-GPU reduction of beam doses. */

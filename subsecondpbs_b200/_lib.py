@@ -156,6 +156,16 @@ def struct_to_dict(s: C.Structure) -> dict:
     return out
 
 
+class PbsOperatorLayerSpan(C.Structure):
+    _fields_ = [("layer_index", C.c_int), ("spot_begin", C.c_int), ("spot_count", C.c_int),
+                ("energy", C.c_float), ("longitudinal_cutoff", C.c_float)]
+
+
+class PbsOperatorBatch(C.Structure):
+    _fields_ = [("batch_index", C.c_int), ("spot_begin", C.c_int), ("spot_count", C.c_int),
+                ("first_layer_index", C.c_int), ("last_layer_index", C.c_int)]
+
+
 class PbsServerStats(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in ("submitted", "completed", "failed", "queued", "running", "patient_loads",
                                             "evictions", "slot_releases", "resident_bytes", "slot_bytes",
@@ -205,6 +215,9 @@ def load() -> C.CDLL:
         "pbs_context_reset_dose": (i, [vp, vp, i]),
         "pbs_context_add_beam": (i, [vp, C.POINTER(PbsBeamDesc), i]),
         "pbs_context_adjoint_beam": (i, [vp, C.POINTER(PbsBeamDesc), vp, i, fp, C.c_size_t]),
+        "pbs_operator_batch_plan": (i, [C.POINTER(PbsBeamDesc), i, vp, i, vp, i, C.POINTER(C.c_int)]),
+        "pbs_context_influence_csc": (i, [vp, C.POINTER(PbsBeamDesc), i, C.c_longlong, C.c_longlong, C.c_double,
+                                          C.POINTER(C.c_longlong), vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
         "pbs_context_read_dose": (i, [vp, vp, i]),
         "pbs_context_read_dose64": (i, [vp, vp, i]),
         "pbs_measure_fp32_peak": (i, [i, C.POINTER(C.c_double)]),

@@ -209,6 +209,36 @@ int pbs_context_adjoint_beam(PbsContext* ctx, const PbsBeamDesc* beam, const dou
     return ctx->impl.adjoint_beam(*beam, grad_dose, grad_on_device, grad_weights, n_weights);
 }
 
+int pbs_operator_batch_plan(const PbsBeamDesc* beam, int max_spots_per_batch, PbsOperatorLayerSpan* spans,
+                            int span_capacity, PbsOperatorBatch* batches, int batch_capacity, int info[6]) {
+    if (!beam || !info) {
+        pbs::set_error("null beam or info");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    pbs::OperatorPlan plan;
+    if (int rc = pbs::operator_batch_plan(*beam, max_spots_per_batch, plan)) return rc;
+    const int nSpans = static_cast<int>(plan.spans.size()), nBatches = static_cast<int>(plan.batches.size());
+    const int vals[6] = {plan.valid ? 1 : 0, plan.totalLayers, plan.totalSpots, plan.maxSpotsPerBatch, nSpans, nBatches};
+    for (int i = 0; i < 6; ++i) info[i] = vals[i];
+    if ((spans && span_capacity < nSpans) || (batches && batch_capacity < nBatches)) {
+        pbs::set_error("operator batch plan: output capacity below " + std::to_string(nSpans) + " spans / " +
+                       std::to_string(nBatches) + " batches");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (spans) std::copy(plan.spans.begin(), plan.spans.end(), spans);
+    if (batches) std::copy(plan.batches.begin(), plan.batches.end(), batches);
+    return PBS_OK;
+}
+
+int pbs_context_influence_csc(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction, long long spot_begin,
+                              long long spot_count, double threshold, long long* col_ptr, int* rows, float* values,
+                              long long capacity, long long* nnz) {
+    if (int rc = guard(ctx)) return rc;
+    if (!beam) return PBS_ERR_INVALID_ARGUMENT;
+    return ctx->impl.influence_csc(*beam, nuclear_correction, spot_begin, spot_count, threshold, col_ptr, rows, values,
+                                   capacity, nnz);
+}
+
 int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device) {
     if (int rc = guard(ctx)) return rc;
     if (!out) return PBS_ERR_INVALID_ARGUMENT;

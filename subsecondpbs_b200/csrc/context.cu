@@ -92,7 +92,7 @@ Context::~Context() {
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad, &rbarBuf,
-                      &gradInterm, &gradLattice, &weqBody})
+                      &gradInterm, &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         b->release();
     staging.release();
     errHost.release();
@@ -727,7 +727,7 @@ void Context::use_stream_ordered_allocation() {
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm,
-                      &gradLattice, &weqBody})
+                      &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         if (!b->ptr) b->allocStream = stream;
 }
 
@@ -737,7 +737,7 @@ size_t Context::device_bytes() const {
                             &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive,
                             &codes, &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf,
                             &nucRsBuf, &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
-                            &rbarBuf, &gradInterm, &gradLattice, &weqBody})
+                            &rbarBuf, &gradInterm, &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         n += b->bytes;
     return n;
 }
@@ -747,7 +747,7 @@ void Context::release_beam_buffers() {
     for (DevBuf* b : {&dens, &wepl, &weplMin, &rayW, &interm, &lattice, &iddBuf, &rsBuf, &bev, &cpb, &subspots,
                       &floatOut, &firstIn, &firstOut, &firstPassive, &codes, &work, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64,
-                      &weqBody})
+                      &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         b->release();
     hasDose = false;
     doseBoxed = false;

@@ -149,6 +149,8 @@ struct Context {
     std::vector<float> layerSpotDist;
     // Adjoint working set, and the imported water-equivalence volume of a beam.
     DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice, weqBody;
+    // Influence export: column offsets, per-block offsets, and the entries.
+    DevBuf opColPtr, opBlockOff, opRows, opVals;
     PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
@@ -218,6 +220,13 @@ struct Context {
     };
     int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned = nullptr);
     int finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b);
+    // Dose-influence columns of spots [spotBegin, spotBegin + spotCount) in CSC:
+    // colPtr[spotCount + 1] (host, from 0), rows = linear voxel indices in ascending
+    // order, values = dose per unit spot weight with |value| > threshold. Entries
+    // past `capacity` are counted in *nnz but not copied (PBS_ERR_INVALID_ARGUMENT).
+    // Leaves the dose accumulator zeroed.
+    int influence_csc(const PbsBeamDesc& b, int nuclear, long long spotBegin, long long spotCount, double threshold,
+                      long long* colPtr, int* rows, float* vals, long long capacity, long long* nnz);
     int beam_stats(PbsBeamStats* out);
     int layer_stats(int layer, PbsLayerStats* out);
     int stage_times(float* ms, int n);
@@ -225,6 +234,17 @@ struct Context {
 };
 
 int measure_fp32_peak(int gpu, double* tflops);
+
+// The operator-mode batch plan of a beam (rtd_operator_mode.h:18-41).
+struct OperatorPlan {
+    bool valid = false;
+    int totalLayers = 0;
+    int totalSpots = 0;
+    int maxSpotsPerBatch = 0;
+    std::vector<PbsOperatorLayerSpan> spans;
+    std::vector<PbsOperatorBatch> batches;
+};
+int operator_batch_plan(const PbsBeamDesc& beam, int maxSpotsPerBatch, OperatorPlan& plan);
 
 int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
                       float* doseData, const int doseDims[3], const float doseRes[3], const float doseCorner[3],

@@ -1,0 +1,321 @@
+// Spot-preserving operator mode: the batch plan of the reference's operator-mode
+// helper (include/core/rtd_operator_mode.h:43-111), and a dose-influence export
+// in compressed sparse columns (one column per spot, one row per dose voxel) that
+// the reference plans for but does not compute (cuCalDose3 only zeroes its CSC
+// outputs, raytracedicom_pybind.cpp:1955-2053).
+//
+// Column j of the influence matrix is the dose of the beam with spot j at unit
+// weight and every other spot at zero: the same plan, ray grid and lattice as the
+// whole beam, so that A . w equals the forward dose of w up to the live-ray mask
+// (ray weight < 1e-6, idd_sigma.cu:78) and rounding. Each column is compacted on
+// the device from the FP64 grid's dirty box in ascending voxel order, with its
+// offsets scanned on the device, so a batch of columns needs one synchronisation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "../../include/subsecondpbs.h"
+
+namespace pbs {
+
+namespace {
+
+constexpr int kOpThreads = 256;
+constexpr int kOpPasses = 8;
+constexpr int kOpChunk = kOpThreads * kOpPasses;  // box voxels per block
+
+// An inclusive voxel box of the dose grid walked in grid order (x fastest).
+struct OpBox {
+    int lo[3];
+    int ext[3];
+    int X, Y;
+    long long n;  // voxels in the box
+};
+
+__device__ __forceinline__ long long box_to_grid(const OpBox& a, long long b) {
+    const int bx = int(b % a.ext[0]);
+    const long long r = b / a.ext[0];
+    const int by = int(r % a.ext[1]);
+    const int bz = int(r / a.ext[1]);
+    return (static_cast<long long>(a.lo[2] + bz) * a.Y + (a.lo[1] + by)) * a.X + (a.lo[0] + bx);
+}
+
+// Entries above the threshold in each block's chunk of the box.
+__global__ void __launch_bounds__(kOpThreads) influence_count_kernel(const double* __restrict__ dose, OpBox a,
+                                                                     double thr, long long* __restrict__ blockOff) {
+    const long long base = static_cast<long long>(blockIdx.x) * kOpChunk;
+    int c = 0;
+    for (int p = 0; p < kOpPasses; ++p) {
+        const long long b = base + p * kOpThreads + threadIdx.x;
+        const bool keep = b < a.n && fabs(dose[box_to_grid(a, b)]) > thr;
+        c += __syncthreads_count(keep);
+    }
+    if (threadIdx.x == 0) blockOff[blockIdx.x] = c;
+}
+
+// One block: block counts -> absolute exclusive offsets (starting at colPtr[col]),
+// and colPtr[col + 1] = colPtr[col] + entries of the column.
+__global__ void __launch_bounds__(1024) influence_scan_kernel(long long* __restrict__ blockOff, int nBlocks,
+                                                              long long* __restrict__ colPtr, int col) {
+    __shared__ long long carry;
+    __shared__ long long warpSums[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = colPtr[col];
+    __syncthreads();
+    for (int start = 0; start < nBlocks; start += 1024) {
+        const int i = start + threadIdx.x;
+        const long long v = i < nBlocks ? blockOff[i] : 0;
+        long long x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            long long s = warpSums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            warpSums[lane] = s;
+        }
+        __syncthreads();
+        const long long incl = x + (warp > 0 ? warpSums[warp - 1] : 0);
+        const long long c0 = carry;
+        if (i < nBlocks) blockOff[i] = c0 + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = c0 + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) colPtr[col + 1] = carry;
+}
+
+// Ordered compaction of each block's chunk: entries keep the box order, which is
+// ascending voxel order. Entries past `cap` are counted but not written.
+__global__ void __launch_bounds__(kOpThreads) influence_write_kernel(const double* __restrict__ dose, OpBox a,
+                                                                     double thr, const long long* __restrict__ blockOff,
+                                                                     int* __restrict__ rows, float* __restrict__ vals,
+                                                                     long long cap) {
+    __shared__ int warpCounts[kOpThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long pos = blockOff[blockIdx.x];
+    const long long base = static_cast<long long>(blockIdx.x) * kOpChunk;
+    for (int p = 0; p < kOpPasses; ++p) {
+        const long long b = base + p * kOpThreads + threadIdx.x;
+        long long g = 0;
+        double v = 0.0;
+        bool keep = false;
+        if (b < a.n) {
+            g = box_to_grid(a, b);
+            v = dose[g];
+            keep = fabs(v) > thr;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) warpCounts[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < kOpThreads / 32; ++w) {
+            const int c = warpCounts[w];
+            if (w < warp) before += c;
+            total += c;
+        }
+        if (keep) {
+            const long long at = pos + before + __popc(m & ((1u << lane) - 1u));
+            if (at < cap) {
+                rows[at] = static_cast<int>(g);
+                vals[at] = static_cast<float>(v);
+            }
+        }
+        pos += total;
+        __syncthreads();
+    }
+}
+
+int op_cuda(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return PBS_OK;
+    set_error(std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? PBS_ERR_OUT_OF_MEMORY : PBS_ERR_CUDA;
+}
+
+}  // namespace
+
+// rtd_operator_mode.h:43-111: the same validation (an invalid beam returns the
+// fields filled so far and valid = 0), spans in layer order, and batches of at most
+// max(1, maxSpotsPerBatch) consecutive spots with the layers of their first and
+// last spot (the first non-empty span holding the spot, -1 if none).
+int operator_batch_plan(const PbsBeamDesc& beam, int maxSpotsPerBatch, OperatorPlan& plan) {
+    plan = OperatorPlan{};
+    plan.totalLayers = static_cast<int>(beam.layer_spot_counts ? beam.n_layer_spot_counts : 0);
+    const size_t nEnergies = beam.energies ? beam.n_energies : 0;
+    if (plan.totalLayers <= 0 || static_cast<int>(nEnergies) != plan.totalLayers) return PBS_OK;
+    int totalSpots = 0;
+    for (int l = 0; l < plan.totalLayers; ++l) {
+        if (beam.layer_spot_counts[l] < 0) return PBS_OK;
+        totalSpots += beam.layer_spot_counts[l];
+    }
+    plan.totalSpots = totalSpots;
+    if (totalSpots <= 0) return PBS_OK;
+    const size_t nWeights = beam.spot_weights ? beam.n_spot_weights : 0;
+    const size_t nPositions = beam.spot_positions ? beam.n_spot_positions : 0;
+    const size_t nDirections = beam.spot_beam_directions ? beam.n_spot_beam_directions : 0;
+    if (nWeights != 0 && static_cast<int>(nWeights) != totalSpots) return PBS_OK;
+    if (nPositions != 0 && static_cast<int>(nPositions / 2u) != totalSpots) return PBS_OK;
+    if (nDirections != 0 && static_cast<int>(nDirections / 3u) != totalSpots) return PBS_OK;
+
+    const size_t nCutoffs = beam.layer_longitudinal_cutoffs ? beam.n_layer_longitudinal_cutoffs : 0;
+    int running = 0;
+    for (int l = 0; l < plan.totalLayers; ++l) {
+        PbsOperatorLayerSpan s{};
+        s.layer_index = l;
+        s.spot_begin = running;
+        s.spot_count = beam.layer_spot_counts[l];
+        s.energy = beam.energies[l];
+        s.longitudinal_cutoff = static_cast<size_t>(l) < nCutoffs ? beam.layer_longitudinal_cutoffs[l] : 0.0f;
+        plan.spans.push_back(s);
+        running += s.spot_count;
+    }
+    plan.maxSpotsPerBatch = std::max(1, maxSpotsPerBatch);
+    auto layerOf = [&](int spot) {
+        for (const PbsOperatorLayerSpan& s : plan.spans) {
+            if (s.spot_count <= 0) continue;
+            if (spot >= s.spot_begin && spot < s.spot_begin + s.spot_count) return s.layer_index;
+        }
+        return -1;
+    };
+    for (int begin = 0, index = 0; begin < totalSpots; begin += plan.maxSpotsPerBatch, ++index) {
+        PbsOperatorBatch b{};
+        b.batch_index = index;
+        b.spot_begin = begin;
+        b.spot_count = std::min(plan.maxSpotsPerBatch, totalSpots - begin);
+        b.first_layer_index = layerOf(b.spot_begin);
+        b.last_layer_index = layerOf(b.spot_begin + b.spot_count - 1);
+        plan.batches.push_back(b);
+        // A batch size that reaches past INT_MAX ends the walk instead of wrapping.
+        if (begin > INT_MAX - plan.maxSpotsPerBatch) break;
+    }
+    plan.valid = !plan.spans.empty() && !plan.batches.empty();
+    return PBS_OK;
+}
+
+int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotBegin, long long spotCount,
+                           double threshold, long long* colPtrHost, int* rowsHost, float* valsHost,
+                           long long capacity, long long* nnzOut) {
+    if (int rc = op_cuda(cudaSetDevice(device), "cudaSetDevice")) return rc;
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    if (!beam.layer_spot_counts || beam.n_layer_spot_counts == 0) {
+        set_error("influence export: the beam has no layer spot counts");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    long long nSpots = 0;
+    for (size_t l = 0; l < beam.n_layer_spot_counts; ++l) {
+        if (beam.layer_spot_counts[l] < 0) {
+            set_error("influence export: negative layer spot count");
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+        nSpots += beam.layer_spot_counts[l];
+    }
+    if (spotBegin < 0 || spotCount < 0 || spotBegin + spotCount > nSpots || spotCount > INT_MAX - 1) {
+        set_error("influence export: spot range [" + std::to_string(spotBegin) + ", " +
+                  std::to_string(spotBegin + spotCount) + ") outside the beam's " + std::to_string(nSpots) + " spots");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (!(threshold >= 0.0) || !std::isfinite(threshold)) {
+        set_error("influence export: the threshold must be finite and >= 0");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (!colPtrHost || !nnzOut || capacity < 0 || (capacity > 0 && (!rowsHost || !valsHost))) {
+        set_error("influence export: null output or negative capacity");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    const long long gridN = static_cast<long long>(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    if (gridN > INT_MAX) {
+        set_error("influence export: the dose grid has more voxels than an int32 row index holds");
+        return PBS_ERR_UNSUPPORTED;
+    }
+    const long long maxBlocks = (gridN + kOpChunk - 1) / kOpChunk;
+    if (int rc = opColPtr.ensure(static_cast<size_t>(spotCount + 1) * sizeof(long long))) return rc;
+    if (int rc = opBlockOff.ensure(static_cast<size_t>(std::max(maxBlocks, 1LL)) * sizeof(long long))) return rc;
+    if (capacity > 0) {
+        if (int rc = opRows.ensure(static_cast<size_t>(capacity) * sizeof(int))) return rc;
+        if (int rc = opVals.ensure(static_cast<size_t>(capacity) * sizeof(float))) return rc;
+    }
+    long long* dColPtr = static_cast<long long*>(opColPtr.ptr);
+    long long* dBlockOff = static_cast<long long*>(opBlockOff.ptr);
+    int* dRows = capacity > 0 ? static_cast<int*>(opRows.ptr) : nullptr;
+    float* dVals = capacity > 0 ? static_cast<float*>(opVals.ptr) : nullptr;
+    if (int rc = op_cuda(cudaMemsetAsync(dColPtr, 0, sizeof(long long), stream), "influence colPtr clear")) return rc;
+
+    std::vector<float> unit(static_cast<size_t>(nSpots), 0.0f);
+    PbsBeamDesc one = beam;
+    one.spot_weights = unit.data();
+    one.n_spot_weights = unit.size();
+    for (long long k = 0; k < spotCount; ++k) {
+        const size_t j = static_cast<size_t>(spotBegin + k);
+        unit[j] = 1.0f;
+        if (int rc = reset_dose(nullptr, 0)) return rc;
+        int rc = add_beam(one, nuclear);
+        unit[j] = 0.0f;
+        if (rc) return rc;
+        if (int rc2 = join_side_work()) return rc2;
+        OpBox a{};
+        int lo[3], hi[3];
+        for (int i = 0; i < 3; ++i) {
+            const bool boxed = doseBoxed && !doseExposed;
+            lo[i] = boxed ? dirtyLo[i] : 0;
+            hi[i] = boxed ? dirtyHi[i] : doseGrid.dims[i] - 1;
+        }
+        const bool empty = hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2];
+        for (int i = 0; i < 3; ++i) {
+            a.lo[i] = lo[i];
+            a.ext[i] = empty ? 0 : hi[i] - lo[i] + 1;
+        }
+        a.X = doseGrid.dims[0];
+        a.Y = doseGrid.dims[1];
+        a.n = empty ? 0 : static_cast<long long>(a.ext[0]) * a.ext[1] * a.ext[2];
+        const int nBlocks = static_cast<int>((a.n + kOpChunk - 1) / kOpChunk);
+        const double* d = static_cast<const double*>(dose64.ptr);
+        if (nBlocks > 0) influence_count_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, threshold, dBlockOff);
+        influence_scan_kernel<<<1, 1024, 0, stream>>>(dBlockOff, nBlocks, dColPtr, static_cast<int>(k));
+        if (nBlocks > 0)
+            influence_write_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, threshold, dBlockOff, dRows, dVals,
+                                                                       capacity);
+        if (int rc3 = op_cuda(cudaGetLastError(), "influence kernels")) return rc3;
+    }
+    if (int rc = op_cuda(cudaMemcpyAsync(colPtrHost, dColPtr, static_cast<size_t>(spotCount + 1) * sizeof(long long),
+                                         cudaMemcpyDeviceToHost, stream),
+                         "influence colPtr D2H"))
+        return rc;
+    if (int rc = op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return rc;
+    if (int rc = take_device_errors()) return rc;
+    const long long nnz = colPtrHost[spotCount];
+    *nnzOut = nnz;
+    if (nnz > capacity) {
+        reset_dose(nullptr, 0);
+        set_error("influence export: " + std::to_string(nnz) + " entries do not fit the capacity of " +
+                  std::to_string(capacity));
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (nnz > 0) {
+        if (int rc = op_cuda(cudaMemcpyAsync(rowsHost, dRows, static_cast<size_t>(nnz) * sizeof(int),
+                                             cudaMemcpyDeviceToHost, stream),
+                             "influence rows D2H"))
+            return rc;
+        if (int rc = op_cuda(cudaMemcpyAsync(valsHost, dVals, static_cast<size_t>(nnz) * sizeof(float),
+                                             cudaMemcpyDeviceToHost, stream),
+                             "influence values D2H"))
+            return rc;
+    }
+    if (int rc = reset_dose(nullptr, 0)) return rc;
+    return op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+}
+
+}  // namespace pbs

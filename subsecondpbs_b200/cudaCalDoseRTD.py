@@ -170,6 +170,40 @@ class DoseEngine:
         del keep, gkeep
         return out
 
+    def influence_csc(self, beam, spot_begin: int = 0, spot_count: int | None = None, threshold: float = 0.0,
+                      nuclear_correction: bool = False, capacity: int | None = None):
+        """Spot-preserving dose-influence matrix of spots [spot_begin, spot_begin +
+        spot_count) as a scipy CSC matrix of shape (voxels, spot_count): column j is
+        the dose per unit weight of spot spot_begin + j under the beam's own plan,
+        rows are linear voxel indices (z*Y + y)*X + x, entries |dose| > threshold.
+        The context's dose accumulator is left at zero. Without `capacity` the
+        export runs twice when the first guess of its size is short."""
+        import scipy.sparse as sp
+
+        bd, keep = beam if isinstance(beam, tuple) else _lib.beam_desc(beam)
+        n_spots = int(sum(bd.layer_spot_counts[i] for i in range(bd.n_layer_spot_counts)))
+        if spot_count is None:
+            spot_count = n_spots - int(spot_begin)
+        n_vox = int(np.prod(self.dose_dims))
+        cap = int(capacity) if capacity is not None else max(1 << 16, 4096 * int(spot_count))
+        col_ptr = np.zeros(int(spot_count) + 1, dtype=np.int64)
+        nnz = C.c_longlong(0)
+        while True:
+            rows = np.empty(cap, dtype=np.int32)
+            vals = np.empty(cap, dtype=np.float32)
+            rc = self._lib.pbs_context_influence_csc(
+                self._h, C.byref(bd), int(bool(nuclear_correction)), int(spot_begin), int(spot_count),
+                float(threshold), col_ptr.ctypes.data_as(C.POINTER(C.c_longlong)), rows.ctypes.data_as(C.c_void_p),
+                vals.ctypes.data_as(C.c_void_p), cap, C.byref(nnz))
+            if rc == _lib.PBS_ERR_INVALID_ARGUMENT and nnz.value > cap and capacity is None:
+                cap = int(nnz.value)
+                continue
+            _lib.check(rc)
+            break
+        del keep
+        n = int(nnz.value)
+        return sp.csc_matrix((vals[:n], rows[:n], col_ptr), shape=(n_vox, int(spot_count)))
+
     @staticmethod
     def prepare_beam(beam: dict):
         """Convert a beam dict to its C descriptor once (for repeated add_beam calls)."""

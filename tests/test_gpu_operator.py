@@ -1,0 +1,108 @@
+"""Dose-influence export (pbs_context_influence_csc) against the forward dose and
+the spot-weight adjoint on the same context.
+
+Dose is linear in the spot weights at a fixed set of live rays, so A . w must
+reproduce the forward dose of w, and A^T g the adjoint's gradient for any
+dose-grid vector g. Tolerance: 0.5 % of Dmax for the dose (the dose tolerance of
+the parity tests; the export's float32 values and the forward's few-ulp atomics
+noise are far below it); for A^T g, 1e-4 of the largest |A|^T |g|, the summed
+magnitude of the terms each gradient entry adds up (a signed g cancels inside the
+sums, so the entries themselves are no scale for float32 rounding)."""
+import numpy as np
+import pytest
+
+from subsecondpbs_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+SEED = 20261203
+DOSE_TOL = 5e-3
+
+
+def _engine(case):
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    eng = DoseEngine(0)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    return eng
+
+
+def _weighted(case):
+    beam = dict(case["beam"])
+    n = int(np.sum(beam["layer_spot_counts"]))
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    beam["spot_weights"] = rng.lognormal(0.0, 0.5, n).astype(np.float32)
+    return beam, n
+
+
+def _forward(eng, beam):
+    eng.reset_dose()
+    eng.add_beam(beam)
+    return eng.read_dose64().ravel()
+
+
+@pytest.fixture(scope="module")
+def exported(hetero_small_case):
+    eng = _engine(hetero_small_case)
+    beam, n = _weighted(hetero_small_case)
+    a = eng.influence_csc(beam)
+    return eng, beam, n, a
+
+
+def test_columns_reproduce_the_forward_dose(exported):
+    eng, beam, n, a = exported
+    assert a.shape == (int(np.prod(eng.dose_dims)), n)
+    d = _forward(eng, beam)
+    ad = a.astype(np.float64) @ beam["spot_weights"].astype(np.float64)
+    dmax = d.max()
+    assert dmax > 0
+    assert np.abs(ad - d).max() <= DOSE_TOL * dmax
+    # Rows ascend strictly inside every column; every stored value passes the threshold (0).
+    for j in range(n):
+        rows = a.indices[a.indptr[j]:a.indptr[j + 1]]
+        assert np.all(np.diff(rows) > 0)
+    assert np.all(a.data != 0)
+
+
+def test_column_is_the_one_hot_forward(exported):
+    eng, beam, n, a = exported
+    for j in (0, n // 2, n - 1):
+        one = dict(beam)
+        w = np.zeros(n, dtype=np.float32)
+        w[j] = 1.0
+        one["spot_weights"] = w
+        d = _forward(eng, one)
+        col = a[:, j].toarray().ravel()
+        scale = max(np.abs(d).max(), 1e-30)
+        assert np.abs(col - d).max() <= 1e-5 * scale
+
+
+def test_transpose_is_the_adjoint(exported):
+    eng, beam, n, a = exported
+    rng = np.random.Generator(np.random.PCG64(SEED + 1))
+    g = rng.standard_normal(tuple(reversed(eng.dose_dims)))
+    grad = eng.adjoint_beam(beam, g, n).astype(np.float64)
+    atg = a.T.astype(np.float64) @ g.ravel()
+    scale = (abs(a).T.astype(np.float64) @ np.abs(g).ravel()).max()
+    assert np.abs(atg - grad).max() <= 1e-4 * scale
+
+
+def test_batches_threshold_and_capacity(exported):
+    eng, beam, n, a = exported
+    begin, count = n // 3, min(17, n - n // 3)
+    part = eng.influence_csc(beam, spot_begin=begin, spot_count=count)
+    ref = a[:, begin:begin + count].toarray()
+    scale = np.abs(a.data).max()
+    assert np.abs(part.toarray() - ref).max() <= 1e-5 * scale
+    t = 1e-3 * scale
+    cut = eng.influence_csc(beam, threshold=t)
+    assert cut.nnz < a.nnz and np.all(np.abs(cut.data) > t)
+    assert np.abs(cut.toarray() - np.where(np.abs(a.toarray()) > t, a.toarray(), 0.0)).max() <= t * 1.001
+    with pytest.raises(_lib.PbsError, match="capacity"):
+        eng.influence_csc(beam, spot_count=2, capacity=1)
+    empty = eng.influence_csc(beam, spot_begin=n, spot_count=0)
+    assert empty.shape[1] == 0 and empty.nnz == 0
+    # The export leaves the accumulator at zero.
+    assert not eng.read_dose64().any()
