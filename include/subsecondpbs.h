@@ -305,7 +305,12 @@ PBS_API int pbs_operator_batch_plan(const PbsBeamDesc* beam, int max_spots_per_b
  * order; entries with |dose| > threshold (Gy per unit weight, >= 0). Host outputs:
  * col_ptr[spot_count + 1] from 0, rows/values of `capacity` entries. *nnz is set
  * even when it exceeds `capacity`, which returns PBS_ERR_INVALID_ARGUMENT (col_ptr
- * filled, rows/values not). Replaces the context's dose with zero. */
+ * filled, rows/values not). The beam is planned once, every spot at unit weight,
+ * and each column reuses that plan with only its spot's lattice cells set. A beam
+ * without a raw spot lattice (missing spot positions or weights, an empty layer, a
+ * spot off the lattice phase) would run the legacy CPB fluence, which ignores
+ * per-spot weights: it returns PBS_ERR_UNSUPPORTED. On return, success or error,
+ * the context's dose is zero. */
 PBS_API int pbs_context_influence_csc(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction,
                                       long long spot_begin, long long spot_count, double threshold,
                                       long long* col_ptr, int* rows, float* values, long long capacity,
@@ -330,10 +335,14 @@ PBS_API int pbs_measure_fp32_peak(int gpu_id, double* tflops);
  * call (a caller-managed memory pool, a process that must not grow its
  * footprint): the CPB grid is a fixed static device array of 2^20 floats
  * (4 MiB) per device, so ray_dims[0] * ray_dims[1] * n_layers must not exceed
- * 1048576 (PBS_ERR_INVALID_ARGUMENT otherwise). No memory is allocated; the
+ * 1048576, n_layers must not exceed 65535 and ray_dims[1] not 524280 (the
+ * kernels' launch limits; PBS_ERR_INVALID_ARGUMENT otherwise, before anything is
+ * launched). Devices 0..63 only. No memory is allocated; the
  * scratch cells used are cleared on `stream` before use. The first call on a
  * device looks up the scratch address (cudaGetSymbolAddress): make that first
- * call before any stream capture. All calls on one device share the scratch, so
+ * call before any stream capture. The address is kept for the life of the
+ * process: after a cudaDeviceReset of a device, do not call this entry point on
+ * that device again. All calls on one device share the scratch, so
  * calls that overlap in time (other streams or threads) race and corrupt each
  * other's result: serialise them. Launches are asynchronous on `stream`. */
 PBS_API int pbs_cpb_fluence_no_alloc(const float* d_subspots, int max_subspots, int n_layers, const int ray_dims[2],

@@ -1,11 +1,13 @@
 #!/usr/bin/env bash
 # Builds the reference's dose library from its own CUDA/C++ sources (read in place
-# under /root/reference) plus the C shim beside this script, into oracle/_ref/.
+# from the reference checkout) plus the C shim beside this script, into oracle/_ref/.
+# The checkout is $REFERENCE_DIR, else a sibling of this repository named
+# `reference` (<repo>/../reference); without either the script stops with a message.
 # Test infrastructure only: the result is run on the GPU box to pin the oracle.
 # Usage: bash oracle/ref/build_ref.sh [NUCLEAR_CORR value, e.g. GAUSS_FIT]
 set -euo pipefail
-REF=${REFERENCE_DIR:-/root/reference}
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF=${REFERENCE_DIR:-"$HERE/../../../reference"}
 OUT="$HERE/../_ref"
 NUC="${1:-OFF}"
 mkdir -p "$OUT"

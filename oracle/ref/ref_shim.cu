@@ -102,3 +102,44 @@ extern "C" int ref_subsecond_wrapper(const float* ct, const int* ctDims, const f
     }
     return 0;
 }
+
+// The reference's own table parser (src/utils/energy_reader.cpp:21-185) on `dir`.
+// Call once with null outputs to get the sizes: sizes[0..4] = nEnergySamples,
+// nEnergies, nDensitySamples, nSpSamples, nRRlSamples; sizes[5] = 1 when nuclear
+// tables were read (a NUCLEAR_CORR build). scales[0..2] = density, sp, rRl scale
+// factors. Then call again with buffers of those sizes: `energy` takes energiesPerU,
+// peakDepths and scaleFacts (3 x nEnergies), `cidd` nEnergies x nEnergySamples,
+// `luts` density | sp | rRl, `nuc` weights | sqSigmas (2 x nEnergies x nEnergySamples).
+#include "energy_reader.h"
+#include "energy_struct.h"
+#include <cstring>
+#include <string>
+
+extern "C" int ref_energy_reader(const char* dir, int* sizes, float* scales, float* energy, float* cidd, float* luts,
+                                 float* nuc) {
+    EnergyStruct es;
+    try {
+        es = energyReader(std::string(dir));
+    } catch (const std::exception& ex) {
+        std::fprintf(stderr, "reference energyReader threw: %s\n", ex.what());
+        return 2;
+    }
+    sizes[0] = es.nEnergySamples;
+    sizes[1] = es.nEnergies;
+    sizes[2] = es.nDensitySamples;
+    sizes[3] = es.nSpSamples;
+    sizes[4] = es.nRRlSamples;
+    sizes[5] = es.nucWeightMatrix.empty() ? 0 : 1;
+    scales[0] = es.densityScaleFact;
+    scales[1] = es.spScaleFact;
+    scales[2] = es.rRlScaleFact;
+    auto put = [](float* dst, const std::vector<float>& v) {
+        if (!v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(float));
+        return dst + v.size();
+    };
+    if (energy) put(put(put(energy, es.energiesPerU), es.peakDepths), es.scaleFacts);
+    if (cidd) put(cidd, es.ciddMatrix);
+    if (luts) put(put(put(luts, es.densityVector), es.spVector), es.rRlVector);
+    if (nuc && sizes[5]) put(put(nuc, es.nucWeightMatrix), es.nucSqSigmaMatrix);
+    return 0;
+}

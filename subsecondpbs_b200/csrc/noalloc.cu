@@ -24,7 +24,9 @@ std::mutex g_scratchMutex;
 float* g_scratchPtr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up once per
-// device (the first call on a device does it).
+// device (the first call on a device does it) and kept for the life of the process.
+// A cudaDeviceReset of that device unloads the module the address belongs to, so
+// the entry point must not be used on that device after such a reset.
 int scratch_for_current_device(int device, float** out) {
     std::lock_guard<std::mutex> lock(g_scratchMutex);
     if (!g_scratchPtr[device]) {
@@ -54,6 +56,13 @@ extern "C" PBS_API int pbs_cpb_fluence_no_alloc(const float* d_subspots, int max
         set_error("pbs_cpb_fluence_no_alloc: null pointer or non-positive size");
         return PBS_ERR_INVALID_ARGUMENT;
     }
+    // Launch limits of the two kernels: layers run on grid y / z (at most 65535) and
+    // ray rows in groups of 8 on grid y.
+    if (n_layers > 65535 || (ray_dims[1] + 7) / 8 > 65535) {
+        set_error("pbs_cpb_fluence_no_alloc: n_layers = " + std::to_string(n_layers) + " and ray_dims[1] = " +
+                  std::to_string(ray_dims[1]) + " exceed the launch limits (n_layers <= 65535, ray_dims[1] <= 524280)");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
     const size_t cells = size_t(ray_dims[0]) * size_t(ray_dims[1]) * size_t(n_layers);
     if (cells > kScratchCells) {
         set_error("pbs_cpb_fluence_no_alloc: ray_dims[0]*ray_dims[1]*n_layers = " + std::to_string(cells) +
@@ -63,9 +72,14 @@ extern "C" PBS_API int pbs_cpb_fluence_no_alloc(const float* d_subspots, int max
     }
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess || device < 0 || device >= kMaxDevices) {
+    if (e != cudaSuccess) {
         set_error(std::string("pbs_cpb_fluence_no_alloc: no usable current device: ") + cudaGetErrorString(e));
         return PBS_ERR_CUDA;
+    }
+    if (device < 0 || device >= kMaxDevices) {
+        set_error("pbs_cpb_fluence_no_alloc: current device " + std::to_string(device) +
+                  " is beyond the " + std::to_string(kMaxDevices) + " devices this entry point keeps scratch for");
+        return PBS_ERR_UNSUPPORTED;
     }
     float* scratch = nullptr;
     int rc = scratch_for_current_device(device, &scratch);

@@ -223,9 +223,10 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         }
         nSpots += beam.layer_spot_counts[l];
     }
-    if (spotBegin < 0 || spotCount < 0 || spotBegin + spotCount > nSpots || spotCount > INT_MAX - 1) {
-        set_error("influence export: spot range [" + std::to_string(spotBegin) + ", " +
-                  std::to_string(spotBegin + spotCount) + ") outside the beam's " + std::to_string(nSpots) + " spots");
+    if (spotBegin < 0 || spotCount < 0 || spotBegin > nSpots || spotCount > nSpots - spotBegin ||
+        spotCount > INT_MAX - 1) {
+        set_error("influence export: spot range of " + std::to_string(spotCount) + " spots from " +
+                  std::to_string(spotBegin) + " lies outside the beam's " + std::to_string(nSpots) + " spots");
         return PBS_ERR_INVALID_ARGUMENT;
     }
     if (!(threshold >= 0.0) || !std::isfinite(threshold)) {
@@ -241,31 +242,69 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         set_error("influence export: the dose grid has more voxels than an int32 row index holds");
         return PBS_ERR_UNSUPPORTED;
     }
+
+    // One plan for every column. The beam geometry, ray grid and spot lattice do not
+    // depend on the weights, so the plan is made once with every spot at unit weight
+    // and a column only replaces the lattice weights by its spot's shares. A beam
+    // without a raw spot lattice would fall back to the legacy CPB fluence, which
+    // reads the subspot table and ignores per-spot weights: it has no columns.
+    std::vector<float> unit(static_cast<size_t>(nSpots), 1.0f);
+    PbsBeamDesc one = beam;
+    one.spot_weights = unit.data();
+    one.n_spot_weights = unit.size();
+    BeamPlan base;
+    {
+        std::string err;
+        if (int rc = plan_beam(one, energy, ctGrid, doseGrid, base, err)) {
+            set_error("influence export: " + err);
+            return rc;
+        }
+    }
+    if (!base.hasLattice) {
+        set_error("influence export: needs a beam with a raw spot lattice (spot positions, weights and layer counts "
+                  "on one lattice phase); the legacy CPB fluence it would fall back to ignores per-spot weights" +
+                  (base.lattice.failure.empty() ? std::string() : " (" + base.lattice.failure + ")"));
+        return PBS_ERR_UNSUPPORTED;
+    }
+    std::vector<int> cells;
+    std::vector<float> shares;
+    if (!lattice_spot_cells(one, base.lattice, cells, shares)) {
+        set_error("influence export: failed to map the spots onto the beam's lattice");
+        return PBS_ERR_GEOMETRY;
+    }
+
+    // Any failure below leaves the dose grid zeroed, as a finished export does.
+    auto fail = [&](int rc) {
+        const std::string msg = last_error();
+        reset_dose(nullptr, 0);
+        set_error(msg);
+        return rc;
+    };
     const long long maxBlocks = (gridN + kOpChunk - 1) / kOpChunk;
-    if (int rc = opColPtr.ensure(static_cast<size_t>(spotCount + 1) * sizeof(long long))) return rc;
-    if (int rc = opBlockOff.ensure(static_cast<size_t>(std::max(maxBlocks, 1LL)) * sizeof(long long))) return rc;
+    if (int rc = opColPtr.ensure(static_cast<size_t>(spotCount + 1) * sizeof(long long))) return fail(rc);
+    if (int rc = opBlockOff.ensure(static_cast<size_t>(std::max(maxBlocks, 1LL)) * sizeof(long long))) return fail(rc);
     if (capacity > 0) {
-        if (int rc = opRows.ensure(static_cast<size_t>(capacity) * sizeof(int))) return rc;
-        if (int rc = opVals.ensure(static_cast<size_t>(capacity) * sizeof(float))) return rc;
+        if (int rc = opRows.ensure(static_cast<size_t>(capacity) * sizeof(int))) return fail(rc);
+        if (int rc = opVals.ensure(static_cast<size_t>(capacity) * sizeof(float))) return fail(rc);
     }
     long long* dColPtr = static_cast<long long*>(opColPtr.ptr);
     long long* dBlockOff = static_cast<long long*>(opBlockOff.ptr);
     int* dRows = capacity > 0 ? static_cast<int*>(opRows.ptr) : nullptr;
     float* dVals = capacity > 0 ? static_cast<float*>(opVals.ptr) : nullptr;
-    if (int rc = op_cuda(cudaMemsetAsync(dColPtr, 0, sizeof(long long), stream), "influence colPtr clear")) return rc;
+    if (int rc = op_cuda(cudaMemsetAsync(dColPtr, 0, sizeof(long long), stream), "influence colPtr clear"))
+        return fail(rc);
 
-    std::vector<float> unit(static_cast<size_t>(nSpots), 0.0f);
-    PbsBeamDesc one = beam;
-    one.spot_weights = unit.data();
-    one.n_spot_weights = unit.size();
     for (long long k = 0; k < spotCount; ++k) {
         const size_t j = static_cast<size_t>(spotBegin + k);
-        unit[j] = 1.0f;
-        if (int rc = reset_dose(nullptr, 0)) return rc;
-        int rc = add_beam(one, nuclear);
-        unit[j] = 0.0f;
-        if (rc) return rc;
-        if (int rc2 = join_side_work()) return rc2;
+        BeamPlan P = base;
+        std::fill(P.lattice.weights.begin(), P.lattice.weights.end(), 0.0f);
+        for (int slot = 0; slot < 4; ++slot) {
+            const int c = cells[j * 4 + slot];
+            if (c >= 0) P.lattice.weights[static_cast<size_t>(c)] += shares[j * 4 + slot];
+        }
+        if (int rc = reset_dose(nullptr, 0)) return fail(rc);
+        if (int rc = add_planned_beam(one, nuclear, std::move(P))) return fail(rc);
+        if (int rc = join_side_work()) return fail(rc);
         OpBox a{};
         int lo[3], hi[3];
         for (int i = 0; i < 3; ++i) {
@@ -288,14 +327,14 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         if (nBlocks > 0)
             influence_write_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, threshold, dBlockOff, dRows, dVals,
                                                                        capacity);
-        if (int rc3 = op_cuda(cudaGetLastError(), "influence kernels")) return rc3;
+        if (int rc3 = op_cuda(cudaGetLastError(), "influence kernels")) return fail(rc3);
     }
     if (int rc = op_cuda(cudaMemcpyAsync(colPtrHost, dColPtr, static_cast<size_t>(spotCount + 1) * sizeof(long long),
                                          cudaMemcpyDeviceToHost, stream),
                          "influence colPtr D2H"))
-        return rc;
-    if (int rc = op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return rc;
-    if (int rc = take_device_errors()) return rc;
+        return fail(rc);
+    if (int rc = op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return fail(rc);
+    if (int rc = take_device_errors()) return fail(rc);
     const long long nnz = colPtrHost[spotCount];
     *nnzOut = nnz;
     if (nnz > capacity) {
@@ -308,11 +347,11 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         if (int rc = op_cuda(cudaMemcpyAsync(rowsHost, dRows, static_cast<size_t>(nnz) * sizeof(int),
                                              cudaMemcpyDeviceToHost, stream),
                              "influence rows D2H"))
-            return rc;
+            return fail(rc);
         if (int rc = op_cuda(cudaMemcpyAsync(valsHost, dVals, static_cast<size_t>(nnz) * sizeof(float),
                                              cudaMemcpyDeviceToHost, stream),
                              "influence values D2H"))
-            return rc;
+            return fail(rc);
     }
     if (int rc = reset_dose(nullptr, 0)) return rc;
     return op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");

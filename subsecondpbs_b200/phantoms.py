@@ -57,9 +57,11 @@ def _grid(dims, res):
 
 
 def water_phantom_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), energy_mev=150.0, n_side=11, spacing_mm=5.0,
-                       sigma_mm=4.0, sad_mm=10000.0, ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 1) -> dict:
+                       sigma_mm=4.0, sad_mm=10000.0, ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 1,
+                       energy: dict | None = None) -> dict:
     """Homogeneous water: all HU = 0 passed as HU+1000 = 1000 (an all-zero HU volume
-    would be auto-detected as density by the reference, raytracedicom_wrapper.cu:2333)."""
+    would be auto-detected as density by the reference, raytracedicom_wrapper.cu:2333).
+    `energy` is the table dict (default: the synthetic proton tables)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     dims, res, corner = _grid(dims, res)
     ct = np.full((dims[2], dims[1], dims[0]), 1000.0, dtype=np.float32)
@@ -89,7 +91,7 @@ def water_phantom_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), energy_mev=150.0
     }
     return {"name": "water_phantom", "ct": ct, "ct_dims": dims, "ct_resolution": res, "ct_corner": corner,
             "dose_dims": dims, "dose_resolution": res, "dose_corner": corner, "beam": beam,
-            "energy": proton_tables()}
+            "energy": proton_tables() if energy is None else energy}
 
 
 def heterogeneous_ct(dims, res, rng: np.random.Generator) -> np.ndarray:
@@ -208,7 +210,9 @@ def with_spot_directions(beam: dict, sad_x: float, sad_y: float) -> dict:
 
 def heterogeneous_case(dims=(256, 256, 160), res=(2.0, 2.0, 2.0), n_layers=20, e_range=(70.0, 180.0),
                        target_radius_mm=32.0, hex_pitch_mm=5.0, sigma_range=(6.0, 3.0), sad_mm=2000.0,
-                       ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 2) -> dict:
+                       ray_spacing=1.0, n_sub=7, seed=SEED_BASE + 2, energy: dict | None = None) -> dict:
+    """The heterogeneous phantom and its hexagonal-grid beam; `energy` is the table
+    dict (default: the synthetic proton tables)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     dims, res, corner = _grid(dims, res)
     ct = heterogeneous_ct(dims, res, rng)
@@ -240,13 +244,13 @@ def heterogeneous_case(dims=(256, 256, 160), res=(2.0, 2.0, 2.0), n_layers=20, e
     }
     return {"name": "heterogeneous", "ct": ct, "ct_dims": dims, "ct_resolution": res, "ct_corner": corner,
             "dose_dims": dims, "dose_resolution": res, "dose_corner": corner, "beam": beam,
-            "energy": proton_tables()}
+            "energy": proton_tables() if energy is None else energy}
 
 
 def inverse_planning_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), n_beams=4, n_layers=36, e_range=(66.0, 112.0),
                           field_mm=70.0, pitch_mm=5.0, sigma_mm=4.0, target_radius_mm=25.0, shell_mm=20.0,
                           prescription_gy=2.0, sad_mm=10000.0, ray_spacing=1.0, n_sub=7,
-                          seed=SEED_BASE + 4) -> dict:
+                          seed=SEED_BASE + 4, energy: dict | None = None) -> dict:
     """Inverse-planning workload: the water box of `water_phantom_case`, `n_beams`
     coplanar beams (gantry 0, 360/n, ...), each with `n_layers` energy layers of a
     square spot grid over the field (36 x 225 = 8100 spots per beam by default) and
@@ -255,7 +259,7 @@ def inverse_planning_case(dims=(64, 64, 128), res=(2.0, 2.0, 2.0), n_beams=4, n_
     Adds `beams`, `target` and `shell` (bool [Z][Y][X]) and `prescription`."""
     rng = np.random.Generator(np.random.PCG64(seed))
     base = water_phantom_case(dims=dims, res=res, sigma_mm=sigma_mm, sad_mm=sad_mm, ray_spacing=ray_spacing,
-                              n_sub=n_sub, seed=seed)
+                              n_sub=n_sub, seed=seed, energy=energy)
     n_side = int(round(field_mm / pitch_mm)) + 1
     g = (np.arange(n_side) - (n_side - 1) / 2.0) * pitch_mm
     px, py = np.meshgrid(g, g, indexing="xy")

@@ -11,6 +11,12 @@
   nuclear_weights_and_sigmas_fit.txt (optional) nS nE, energies, peaks, scales,
                                weight[nE][nS], sqSigma[nE][nS]
 
+On the reference's own tables/ files the result is bit-identical to what the
+reference's energyReader stores (decimal text to float32).
+
+`save_table_npz` / `load_table_npz` keep a parsed energy dict as one compressed
+numpy archive, so the tables can travel where the text files are not present.
+
 `synthetic_proton_tables` / `synthetic_carbon_tables` generate tables of the same
 layout from analytic models (Bragg-Kleeman range-energy relation with Gaussian
 range straggling and a linear primary-fluence loss), so the pipeline can run
@@ -44,8 +50,18 @@ def _read_lut(path: Path):
     return n, scale, v[2:2 + n].astype(np.float32)
 
 
-def energy_reader(tables_dir: str | Path, nuclear: bool = False) -> dict:
-    """Parse the reference's LUT text files into the pybind energy dict."""
+NUCLEAR_FILES = {"GAUSS_FIT": NUCLEAR_FILE, "FLUKA": "nuclear_weights_and_sigmas_Fluka.txt",
+                 "SOUKUP": "nuclear_weights_and_sigmas_Soukup.txt"}
+
+
+def energy_reader(tables_dir: str | Path, nuclear: bool = False, nuclear_file: str = NUCLEAR_FILE) -> dict:
+    """Parse the reference's LUT text files into the pybind energy dict.
+
+    With `nuclear`, the halo weight and squared-sigma tables come from
+    `nuclear_file` (the reference reads nuclear_weights_and_sigmas_fit.txt,
+    energy_reader.cpp:136; the Fluka and Soukup files share its layout). Their
+    energy, peak-depth and scale rows must agree with the proton file's within
+    0.01, the reference's own check (energy_reader.cpp:148-167)."""
     d = Path(tables_dir)
     v = _read_numbers(d / PROTON_FILE)
     ns, ne = int(v[0]), int(v[1])
@@ -70,14 +86,47 @@ def energy_reader(tables_dir: str | Path, nuclear: bool = False) -> dict:
         out[f"{key}_scale_fact"] = scale
         out[f"{key}_vector"] = vec
     if nuclear:
-        w = _read_numbers(d / NUCLEAR_FILE)
+        w = _read_numbers(d / nuclear_file)
         nns, nne = int(w[0]), int(w[1])
         if nns != ns or nne != ne:
-            raise ValueError(f"{NUCLEAR_FILE}: sample/energy counts differ from {PROTON_FILE}")
+            raise ValueError(f"{nuclear_file}: sample/energy counts differ from {PROTON_FILE}")
+        for k, (name, ref) in enumerate((("energies", energies), ("peak depths", peaks), ("scale facts", scales))):
+            row = w[2 + k * ne:2 + (k + 1) * ne].astype(np.float32)
+            if np.any(np.abs(row - ref.astype(np.float32)) > 0.01):
+                raise ValueError(f"{nuclear_file}: {name} differ from {PROTON_FILE}")
         o = 2 + 3 * ne
+        if w.size < o + 2 * ns * ne:
+            raise ValueError(f"{nuclear_file}: truncated weight/sigma matrices")
         out["nuc_weight_matrix"] = w[o:o + ns * ne].reshape(ne, ns).astype(np.float32)
         out["nuc_sq_sigma_matrix"] = w[o + ns * ne:o + 2 * ns * ne].reshape(ne, ns).astype(np.float32)
         out["nuclear_tables_aligned_to_primary_axis"] = True
+    return out
+
+
+def save_table_npz(path: str | Path, energy: dict, **meta: str) -> None:
+    """Store an energy dict (arrays and scalars) in one compressed archive; string
+    keyword arguments are kept beside it as metadata (`meta_<name>`)."""
+    arrays = {}
+    for k, v in energy.items():
+        arrays[k] = np.asarray(v)
+    for k, v in meta.items():
+        arrays[f"meta_{k}"] = np.asarray(str(v))
+    np.savez_compressed(path, **arrays)
+
+
+def load_table_npz(path: str | Path) -> dict:
+    """The energy dict stored by `save_table_npz` (metadata keys left out)."""
+    z = np.load(path)
+    out = {}
+    for k in z.files:
+        if k.startswith("meta_"):
+            continue
+        v = z[k]
+        if v.ndim == 0:
+            v = v.item()
+            if isinstance(v, float) and k.startswith("n_"):
+                v = int(v)
+        out[k] = v
     return out
 
 

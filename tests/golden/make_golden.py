@@ -44,14 +44,44 @@ CASES = {
     "carbon_halo_small": ("carbon_case", {"dims": [64, 64, 48], "res": [2.0, 2.0, 2.0], "gantries": [90.0],
                                           "n_layers": 3, "e_range": [120.0, 200.0], "spots_per_layer": 40},
                           {"nuclear": "GAUSS_FIT"}),
+    # The reference's own tables (reference_tables.npz, made by make_tables.py from
+    # the reference's tables/ with its energyReader): configs 1 and 2 in small form,
+    # a gantry of 30 deg, and the nuclear halo with the reference's
+    # nuclear_weights_and_sigmas_fit.txt.
+    "water_config1_rt": ("water_phantom_case", {}, {"tables": "reference"}),
+    "hetero_small_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                               "e_range": [80.0, 120.0]}, {"tables": "reference"}),
+    "hetero_rot30_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                               "e_range": [80.0, 120.0]}, {"tables": "reference", "rotate": 30.0}),
+    "hetero_mid_rt": ("heterogeneous_case", {"dims": [96, 96, 64], "n_layers": 6, "target_radius_mm": 20.0,
+                                             "e_range": [70.0, 150.0]}, {"tables": "reference"}),
+    "halo_small_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                             "e_range": [80.0, 120.0]}, {"tables": "reference", "nuclear": "GAUSS_FIT"}),
 }
+
+REFERENCE_TABLES = Path(__file__).resolve().parent / "reference_tables.npz"
+
+
+def reference_tables(nuclear: bool) -> dict:
+    """The reference's tables (reference_tables.npz); without `nuclear` the halo
+    tables are left out."""
+    from subsecondpbs_b200 import tables
+
+    t = tables.load_table_npz(REFERENCE_TABLES)
+    if not nuclear:
+        for k in ("nuc_weight_matrix", "nuc_sq_sigma_matrix", "nuclear_tables_aligned_to_primary_axis"):
+            t.pop(k, None)
+    return t
 
 
 def build_case(name: str):
     builder, kw, tf = CASES[name]
     kw = {k: (tuple(v) if isinstance(v, list) else v) for k, v in kw.items()}
     case = getattr(phantoms, builder)(**kw)
-    if tf and "nuclear" in tf:
+    if tf and tf.get("tables") == "reference":
+        case = dict(case)
+        case["energy"] = reference_tables("nuclear" in tf)
+    elif tf and "nuclear" in tf:
         from subsecondpbs_b200 import tables
 
         case = dict(case)

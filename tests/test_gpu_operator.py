@@ -106,3 +106,28 @@ def test_batches_threshold_and_capacity(exported):
     assert empty.shape[1] == 0 and empty.nnz == 0
     # The export leaves the accumulator at zero.
     assert not eng.read_dose64().any()
+
+
+def test_beam_without_a_lattice_is_refused(exported):
+    """A spot off the lattice phase leaves the beam without a raw spot lattice; its
+    dose would come from the legacy CPB fluence, which ignores per-spot weights, so
+    the export refuses it and leaves the dose grid at zero."""
+    eng, beam, n, a = exported
+    off = dict(beam)
+    pos = np.asarray(beam["spot_positions"], np.float32).reshape(-1, 2).copy()
+    pos[n // 3, 0] += 0.3
+    off["spot_positions"] = pos.reshape(-1)
+    with pytest.raises(_lib.PbsError) as e:
+        eng.influence_csc(off, spot_count=2)
+    assert e.value.code == _lib.PBS_ERR_UNSUPPORTED
+    assert "raw spot lattice" in str(e.value)
+    assert not np.any(eng.read_dose64())
+
+
+def test_spot_range_past_the_beam_is_refused(exported):
+    eng, beam, n, a = exported
+    with pytest.raises(_lib.PbsError) as e:
+        eng.influence_csc(beam, spot_begin=n - 1, spot_count=2)
+    assert e.value.code == _lib.PBS_ERR_INVALID_ARGUMENT
+    with pytest.raises(_lib.PbsError):
+        eng.influence_csc(beam, spot_begin=2, spot_count=n)

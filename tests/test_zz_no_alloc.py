@@ -64,3 +64,15 @@ def test_cpb_fluence_no_alloc_rejects_oversized_grid():
     msg = L.load().pbs_last_error()
     msg = msg.decode() if isinstance(msg, bytes) else str(msg)
     assert "static scratch" in msg
+
+
+def test_cpb_fluence_no_alloc_rejects_launch_limits():
+    f = _entry()
+    corner = (C.c_float * 2)(0.0, 0.0)
+    res = (C.c_float * 2)(1.0, 1.0)
+    # 70000 layers of one ray fit the scratch but not the kernels' grid: refused before any launch.
+    rc = f(C.c_void_p(16), 1, 70000, (C.c_int * 2)(1, 1), corner, res, C.c_void_p(16), None)
+    assert rc == L.PBS_ERR_INVALID_ARGUMENT
+    msg = L.load().pbs_last_error()
+    msg = msg.decode() if isinstance(msg, bytes) else str(msg)
+    assert "launch limits" in msg
