@@ -10,6 +10,12 @@ buffers, host<->device copies included. Under torchrun every rank computes one
 beam of an opposed-beam plan (gantry 90/270) and the FP64 beam doses are summed
 to rank 0 with one NCCL reduce per step (weak scaling).
 
+The lookup tables are the reference's own (its tables/ files as its energyReader
+reads them, kept in tests/golden/reference_tables.npz). On one GPU the line also
+carries `reference_gpu`: the reference's own subsecondWrapper, built from its
+sources by oracle/ref/build_ref.sh, timed on the same beam in a child process,
+and its dose against this library's in the reference's BEV depth convention.
+
 `--impl reference` times the reference path's CPU restatement (the oracle port)
 on the host cores; the reference ships no CPU implementation of this path.
 """
@@ -35,6 +41,23 @@ METRIC = "ms per beam dose (256²×160, 3k spots); served plans/s, p50/p99 laten
 WORKLOAD = ("heterogeneous CT 256x256x160 at 2 mm (body ellipsoid, lung slab, 2 bone cylinders), "
             "1 proton beam at gantry 90 deg, 20 layers 70-180 MeV, 3020 spots on a 5 mm hex grid, "
             "7x7 subspots, 1 mm rays")
+DATA = ("synthetic seeded phantom; the reference's own proton lookup tables (tables/ as read by its "
+        "energyReader)")
+TABLES = ROOT / "tests" / "golden" / "reference_tables.npz"
+REF_LIB = ROOT / "oracle" / "_ref" / "librtd.so"
+
+
+def _proton_tables() -> dict:
+    """The reference's proton tables without its nuclear halo tables."""
+    from subsecondpbs_b200 import tables
+
+    return {k: v for k, v in tables.load_table_npz(TABLES).items() if not k.startswith("nuc")}
+
+
+def _headline_case() -> dict:
+    from subsecondpbs_b200 import phantoms
+
+    return phantoms.heterogeneous_case(energy=_proton_tables())
 
 
 def _args():
@@ -45,6 +68,8 @@ def _args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU path (oracle/_ref/librtd.so)")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the secondary timings (spot-weight adjoint, carbon plan)")
     ap.add_argument("--serving-requests", type=int, default=1000, help="served stream length (0: skip)")
@@ -122,10 +147,9 @@ def run_reference(args):
     world, rank, _ = _dist()
     if rank != 0:
         return 0
-    from subsecondpbs_b200 import phantoms
     from oracle import oracle as O
 
-    case = phantoms.heterogeneous_case()
+    case = _headline_case()
     threads = os.cpu_count() or 1
     for _ in range(max(args.warmup, 1)):
         O.dose(case, threads=threads)
@@ -138,7 +162,7 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantom, analytic LUTs in the reference format)",
+        "vs_baseline": None, "dtype": "f64", "data": DATA,
         "config": {"workload": WORKLOAD, "l2": "not applicable (CPU)"},
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
                          "sample": f"full workload: {args.steps} beams after {args.warmup} warm-up beams"},
@@ -159,7 +183,7 @@ def _adjoint_cost(local: int, reps: int = 5) -> dict:
     from subsecondpbs_b200.autograd import with_weights
     from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
 
-    case = phantoms.inverse_planning_case()
+    case = phantoms.inverse_planning_case(energy=_proton_tables())
     dev = torch.device("cuda", local)
     eng = DoseEngine(local)
     eng.set_energy(case["energy"])
@@ -225,7 +249,7 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
     from subsecondpbs_b200 import _lib, phantoms, serving
     from subsecondpbs_b200.precision import max_rel_err
 
-    w = phantoms.serving_workload(n_requests=n_requests)
+    w = phantoms.serving_workload(n_requests=n_requests, proton_energy=_proton_tables())
     prepared = [[_lib.beam_desc(b) for b in phantoms.request_beams(w, r)] for r in w["requests"]]
     check = set(range(0, n_requests, max(1, n_requests // 16)))
     # Both sides are measured warm, as a long-running service: one untimed pass of the
@@ -302,6 +326,44 @@ def _carbon_plan(local: int, reps: int = 3) -> dict:
             "ms_per_plan": round(statistics.median(ms), 3), "timing": f"CUDA events, median of {reps}"}
 
 
+def _reference_gpu(local: int, case: dict, our_e2e_ms: float) -> dict | None:
+    """The reference's own GPU path on the same beam and tables: its subsecondWrapper
+    (built from its sources into oracle/_ref/librtd.so) timed in a child process,
+    host buffers in and out as its callers use it. Its dose is then compared with
+    this library's dose computed in the reference's BEV depth convention
+    (PBS_OPT_COMPAT_BEV_Z_SHIFT), the one deliberate difference of the default path."""
+    if not REF_LIB.exists():
+        return {"unavailable": "oracle/_ref/librtd.so not built (oracle/ref/build_ref.sh needs the reference sources)"}
+    from subsecondpbs_b200 import precision as prec
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    with tempfile.TemporaryDirectory() as d:
+        dose_path = Path(d) / "ref_dose.npy"
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+        r = subprocess.run([sys.executable, "-m", "oracle.ref.ref", "--calls", "10", "--budget-s", "90",
+                            "--dose-out", str(dose_path)], cwd=str(ROOT), capture_output=True, text=True,
+                           timeout=600, env=env)
+        if r.returncode != 0:
+            return {"unavailable": f"reference run failed (rc {r.returncode}): {r.stderr.strip()[-300:]}"}
+        timing = json.loads(r.stdout.strip().splitlines()[-1])
+        ref_dose = np.load(dose_path)
+    eng = DoseEngine(local, compat_bev_z_shift=True)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    eng.add_beam(case["beam"])
+    ours = eng.read_dose()
+    eng.close()
+    agreement = prec.report(ours, ref_dose.astype(np.float64), case["dose_resolution"])
+    return {"api": "reference subsecondWrapper (raytracedicom_wrapper.cu:2446) built from its sources for sm_100a "
+                   "by oracle/ref/build_ref.sh, host buffers, verbose=0",
+            "e2e_ms_median": round(timing["median_ms"], 3), "calls": timing["calls"],
+            "ours_e2e_ms": round(our_e2e_ms, 4),
+            "speedup_e2e": round(timing["median_ms"] / our_e2e_ms, 1),
+            "dose_agreement": dict(agreement, against="this library with the reference's BEV depth shift, "
+                                                      "same inputs (voxels above 10 % of Dmax)")}
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -320,7 +382,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    case = phantoms.heterogeneous_case()
+    case = _headline_case()
     # N > 1: a plan of one beam per rank (opposed gantry angles), divided by the
     # sharding module's assignment; each rank computes its beam and the FP64 grids
     # are reduced on rank 0.
@@ -424,18 +486,13 @@ def run_ours(args):
         e2e_call()
         e2e_times.append((time.perf_counter() - t) * 1e3)
     e2e_ms = float(np.mean(e2e_times))
+    copied = (C.c_ulonglong * 2)()
+    _lib.check(lib.pbs_wrapper_copy_bytes(copied))
+    h2d, d2h = int(copied[0]), int(copied[1])
     if world > 1:
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    lut_bytes = sum(np.asarray(energy[k]).nbytes for k in
-                    ("energies_per_u", "peak_depths", "scale_facts", "cidd_matrix", "density_vector", "sp_vector",
-                     "rrl_vector"))
-    beam_bytes = sum(np.asarray(beam[k]).nbytes for k in
-                     ("energies", "spot_sigmas", "layer_spot_counts", "spot_positions", "spot_weights",
-                      "subspot_data"))
-    h2d = int(ct_pin.numel() * 4 + dose_pin.numel() * 4 + lut_bytes + beam_bytes)
-    d2h = int(dose_pin.numel() * 4)
 
     if rank != 0:
         dist.destroy_process_group()
@@ -495,6 +552,7 @@ def run_ours(args):
     served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
               if world == 1 and args.serving_requests > 0 else None)
     carbon = _carbon_plan(local) if world == 1 and not args.no_adjoint else None
+    reference_gpu = _reference_gpu(local, case, e2e_ms) if world == 1 and not args.no_reference_gpu else None
 
     line = {
         "metric": METRIC,
@@ -508,7 +566,7 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded phantom, analytic proton LUTs in the reference format)",
+        "data": DATA,
         "config": {"workload": WORKLOAD, "beams_per_step": world, "parallelism": f"beam-sharded x{world}",
                    "l2": "flushed between timed steps (256 MiB write outside the step events)",
                    "accumulation": "FP64 dose grid", "total_ms_incl_flush": total_ms},
@@ -524,7 +582,10 @@ def run_ours(args):
         "serving": served,
         "carbon_plan": carbon,
         "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers"},
+                "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers",
+                "bytes": "measured by the library (pbs_wrapper_copy_bytes): traced CT box, initial and final dose "
+                         "box, beam inputs, strided CT type samples; tables resident after the first call"},
+        "reference_gpu": reference_gpu,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "plan": {"ray_dims": stats["ray_dims"], "tracer_steps": S, "live_tiles": stats["live_tiles"],

@@ -222,6 +222,13 @@ PBS_API int pbs_subsecond_wrapper(const float* ct_data, const int ct_dims[3], co
                           const PbsBeamDesc* beams, size_t num_beams, const PbsEnergyDesc* energy,
                           int gpu_id, int nuclear_correction, int verbose);
 
+/* Bytes the calling thread's last completed pbs_subsecond_wrapper call moved
+ * between host and device: out[0] host->device (CT box, initial dose box, tables
+ * that differed from the resident ones, beam inputs, and the strided CT samples
+ * the device reads from a page-locked CT for the type detection), out[1]
+ * device->host (dose box, status words). No counterpart in the reference. */
+PBS_API int pbs_wrapper_copy_bytes(unsigned long long out[2]);
+
 /* Host-side planning of one beam only (no device work): validation, gantry frame,
  * spot lattice, ray grid, tracer steps and per-layer energy parameters. Fills the
  * host-known fields of `out` (device-derived fields are left 0). When

@@ -100,3 +100,69 @@ def run(case: dict, beams=None, nuclear: bool = False, verbose: int = 1, path: P
         raise RuntimeError(f"reference returned {rc}:\n{cap.text[-2000:]}")
     del keep, ke
     return dose, parse_batched(cap.text), cap.text
+
+
+def _headline_case():
+    """The 256x256x160 heterogeneous CT with one 20-layer beam of 3020 spots on the
+    reference's own proton tables (tests/golden/reference_tables.npz)."""
+    from subsecondpbs_b200 import phantoms, tables
+
+    t = tables.load_table_npz(HERE.parents[1] / "tests" / "golden" / "reference_tables.npz")
+    t = {k: v for k, v in t.items() if not k.startswith("nuc")}
+    return phantoms.heterogeneous_case(energy=t)
+
+
+def time_reference(calls: int = 10, budget_s: float = 90.0, dose_out: str | None = None) -> dict:
+    """Wall time of the reference's subsecondWrapper (host buffers in and out, as its
+    callers use it) on the headline beam: one untimed call (module load, first-use
+    set-up), then up to `calls` timed calls within `budget_s`; the median is reported.
+    With `dose_out` the last call's dose is saved there (.npy)."""
+    import time
+
+    from subsecondpbs_b200 import _lib as P
+    from subsecondpbs_b200.cudaCalDoseRTD import _with_luts
+
+    case = _headline_case()
+    lib = _load()
+    bd, kb = P.beam_desc(case["beam"])
+    ed, ke = P.energy_desc(_with_luts(case["energy"], None))
+    ct = np.ascontiguousarray(case["ct"], dtype=np.float32)
+    dd = case["dose_dims"]
+    dose = np.zeros((dd[2], dd[1], dd[0]), dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+
+    def call():
+        dose[...] = 0.0
+        with _CaptureStdout():
+            rc = lib.ref_subsecond_wrapper(ct.ctypes.data_as(fp), P.int3(case["ct_dims"]),
+                                           P.float3(case["ct_resolution"]), P.float3(case["ct_corner"]),
+                                           dose.ctypes.data_as(fp), P.int3(dd), P.float3(case["dose_resolution"]),
+                                           P.float3(case["dose_corner"]), C.byref(bd), 1, C.byref(ed), 0, 0, 0)
+        if rc != 0:
+            raise RuntimeError(f"reference returned {rc}")
+
+    call()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < calls and (len(times) < 3 or time.perf_counter() < t_end):
+        t = time.perf_counter()
+        call()
+        times.append((time.perf_counter() - t) * 1e3)
+    if dose_out:
+        np.save(dose_out, dose)
+    del kb, ke
+    return {"median_ms": float(np.median(times)), "calls": len(times), "times_ms": [round(x, 2) for x in times]}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    import sys
+
+    sys.path.insert(0, str(HERE.parents[1]))
+    ap = argparse.ArgumentParser(description="time the reference's subsecondWrapper on the headline beam")
+    ap.add_argument("--calls", type=int, default=10)
+    ap.add_argument("--budget-s", type=float, default=90.0)
+    ap.add_argument("--dose-out", default=None)
+    a = ap.parse_args()
+    print(json.dumps(time_reference(a.calls, a.budget_s, a.dose_out)), flush=True)

@@ -20,48 +20,51 @@ float3 f3(const float* v) { return make_float3(v[0], v[1], v[2]); }
 
 }  // namespace
 
+// RTDBeamSettings of the reference from the flat descriptor.
+static RTDBeamSettings to_reference(const PbsBeamDesc& d) {
+    RTDBeamSettings b;
+    b.energies = vec(d.energies, d.n_energies);
+    b.spotSigmas.clear();
+    for (size_t k = 0; 2 * k + 1 < d.n_spot_sigmas; ++k)
+        b.spotSigmas.push_back(make_float2(d.spot_sigmas[2 * k], d.spot_sigmas[2 * k + 1]));
+    b.raySpacing = make_float2(d.ray_spacing[0], d.ray_spacing[1]);
+    b.steps = d.steps;
+    b.sourceDist = make_float2(d.source_dist[0], d.source_dist[1]);
+    b.spotOffset = f3(d.spot_offset);
+    b.spotDelta = f3(d.spot_delta);
+    b.gantryToImOffset = make_float3(0, 0, 0);
+    b.gantryToImMatrix = make_float3(0, 0, 0);
+    b.gantryToDoseOffset = make_float3(0, 0, 0);
+    b.gantryToDoseMatrix = make_float3(0, 0, 0);
+    b.maxSubspotsPerLayer = d.max_subspots_per_layer;
+    b.subspotData = vec(d.subspot_data, d.n_subspot_data);
+    b.layerSpotCounts = vec(d.layer_spot_counts, d.n_layer_spot_counts);
+    b.spotPositions = vec(d.spot_positions, d.n_spot_positions);
+    b.spotPositionsAreIndices = d.spot_positions_are_indices != 0;
+    b.spotWeights = vec(d.spot_weights, d.n_spot_weights);
+    b.spotBeamDirections = vec(d.spot_beam_directions, d.n_spot_beam_directions);
+    b.layerLongitudinalCutoffs = vec(d.layer_longitudinal_cutoffs, d.n_layer_longitudinal_cutoffs);
+    b.waterEquivalence = vec(d.water_equivalence, d.n_water_equivalence);
+    b.rayWeqHeader = vec(d.ray_weq_header, d.n_ray_weq_header);
+    b.profileData = vec(d.profile_data, d.n_profile_data);
+    b.profileSetting = vec(d.profile_setting, d.n_profile_setting);
+    b.beamParaData = vec(d.beam_para_data, d.n_beam_para_data);
+    b.beamDirection = f3(d.beam_direction);
+    b.bmXDirection = f3(d.bm_x_direction);
+    b.bmYDirection = f3(d.bm_y_direction);
+    b.sourcePosition = f3(d.source_position);
+    b.sad = d.sad;
+    b.refPlaneZ = d.ref_plane_z;
+    b.roiLinearIndices = vec(d.roi_linear_indices, d.n_roi_linear_indices);
+    return b;
+}
+
 extern "C" int ref_subsecond_wrapper(const float* ct, const int* ctDims, const float* ctRes, const float* ctCorner,
                                      float* dose, const int* doseDims, const float* doseRes, const float* doseCorner,
                                      const PbsBeamDesc* beams, size_t nBeams, const PbsEnergyDesc* e, int gpuId,
                                      int nuclear, int verbose) {
     std::vector<RTDBeamSettings> bs(nBeams);
-    for (size_t i = 0; i < nBeams; ++i) {
-        const PbsBeamDesc& d = beams[i];
-        RTDBeamSettings& b = bs[i];
-        b.energies = vec(d.energies, d.n_energies);
-        b.spotSigmas.clear();
-        for (size_t k = 0; 2 * k + 1 < d.n_spot_sigmas; ++k)
-            b.spotSigmas.push_back(make_float2(d.spot_sigmas[2 * k], d.spot_sigmas[2 * k + 1]));
-        b.raySpacing = make_float2(d.ray_spacing[0], d.ray_spacing[1]);
-        b.steps = d.steps;
-        b.sourceDist = make_float2(d.source_dist[0], d.source_dist[1]);
-        b.spotOffset = f3(d.spot_offset);
-        b.spotDelta = f3(d.spot_delta);
-        b.gantryToImOffset = make_float3(0, 0, 0);
-        b.gantryToImMatrix = make_float3(0, 0, 0);
-        b.gantryToDoseOffset = make_float3(0, 0, 0);
-        b.gantryToDoseMatrix = make_float3(0, 0, 0);
-        b.maxSubspotsPerLayer = d.max_subspots_per_layer;
-        b.subspotData = vec(d.subspot_data, d.n_subspot_data);
-        b.layerSpotCounts = vec(d.layer_spot_counts, d.n_layer_spot_counts);
-        b.spotPositions = vec(d.spot_positions, d.n_spot_positions);
-        b.spotPositionsAreIndices = d.spot_positions_are_indices != 0;
-        b.spotWeights = vec(d.spot_weights, d.n_spot_weights);
-        b.spotBeamDirections = vec(d.spot_beam_directions, d.n_spot_beam_directions);
-        b.layerLongitudinalCutoffs = vec(d.layer_longitudinal_cutoffs, d.n_layer_longitudinal_cutoffs);
-        b.waterEquivalence = vec(d.water_equivalence, d.n_water_equivalence);
-        b.rayWeqHeader = vec(d.ray_weq_header, d.n_ray_weq_header);
-        b.profileData = vec(d.profile_data, d.n_profile_data);
-        b.profileSetting = vec(d.profile_setting, d.n_profile_setting);
-        b.beamParaData = vec(d.beam_para_data, d.n_beam_para_data);
-        b.beamDirection = f3(d.beam_direction);
-        b.bmXDirection = f3(d.bm_x_direction);
-        b.bmYDirection = f3(d.bm_y_direction);
-        b.sourcePosition = f3(d.source_position);
-        b.sad = d.sad;
-        b.refPlaneZ = d.ref_plane_z;
-        b.roiLinearIndices = vec(d.roi_linear_indices, d.n_roi_linear_indices);
-    }
+    for (size_t i = 0; i < nBeams; ++i) bs[i] = to_reference(beams[i]);
     RTDEnergyStruct es;
     es.nEnergySamples = e->n_energy_samples;
     es.nEnergies = e->n_energies;
@@ -141,5 +144,39 @@ extern "C" int ref_energy_reader(const char* dir, int* sizes, float* scales, flo
     if (cidd) put(cidd, es.ciddMatrix);
     if (luts) put(put(put(luts, es.densityVector), es.spVector), es.rRlVector);
     if (nuc && sizes[5]) put(put(nuc, es.nucWeightMatrix), es.nucSqSigmaMatrix);
+    return 0;
+}
+
+// The reference's spot batch plan (include/core/rtd_operator_mode.h:43-111) for
+// the beam, in the output form of pbs_operator_batch_plan: info = {valid,
+// total_layers, total_spots, max_spots_per_batch, n_spans, n_batches}; spans and
+// batches receive up to the given capacities.
+#include "rtd_operator_mode.h"
+
+extern "C" int ref_operator_batch_plan(const PbsBeamDesc* beam, int maxSpotsPerBatch, PbsOperatorLayerSpan* spans,
+                                       int spanCapacity, PbsOperatorBatch* batches, int batchCapacity, int* info) {
+    const RTDOperatorBatchPlan p = buildRTDOperatorBatchPlan(to_reference(*beam), maxSpotsPerBatch);
+    info[0] = p.valid ? 1 : 0;
+    info[1] = p.totalLayers;
+    info[2] = p.totalSpots;
+    info[3] = p.maxSpotsPerBatch;
+    info[4] = static_cast<int>(p.layerSpans.size());
+    info[5] = static_cast<int>(p.batches.size());
+    for (int i = 0; i < info[4] && i < spanCapacity; ++i) {
+        const RTDOperatorLayerSpan& a = p.layerSpans[static_cast<size_t>(i)];
+        spans[i].layer_index = a.layerIndex;
+        spans[i].spot_begin = a.spotBegin;
+        spans[i].spot_count = a.spotCount;
+        spans[i].energy = a.energy;
+        spans[i].longitudinal_cutoff = a.longitudinalCutoff;
+    }
+    for (int i = 0; i < info[5] && i < batchCapacity; ++i) {
+        const RTDOperatorBatch& a = p.batches[static_cast<size_t>(i)];
+        batches[i].batch_index = a.batchIndex;
+        batches[i].spot_begin = a.spotBegin;
+        batches[i].spot_count = a.spotCount;
+        batches[i].first_layer_index = a.firstLayerIndex;
+        batches[i].last_layer_index = a.lastLayerIndex;
+    }
     return 0;
 }

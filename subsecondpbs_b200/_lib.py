@@ -204,6 +204,7 @@ def load() -> C.CDLL:
         "pbs_device_count": (i, [C.POINTER(C.c_int)]),
         "pbs_subsecond_wrapper": (i, [fp, ip3, fp3, fp3, fp, ip3, fp3, fp3, C.POINTER(PbsBeamDesc), C.c_size_t,
                                       C.POINTER(PbsEnergyDesc), i, i, i]),
+        "pbs_wrapper_copy_bytes": (i, [C.POINTER(C.c_ulonglong)]),
         "pbs_plan_beam": (i, [C.POINTER(PbsBeamDesc), C.POINTER(PbsEnergyDesc), ip3, fp3, fp3, ip3, fp3, fp3,
                               C.POINTER(PbsBeamStats), fp, fp, C.c_size_t]),
         "pbs_context_create": (i, [i, C.POINTER(vp)]),

@@ -65,6 +65,14 @@ int pbs_subsecond_wrapper(const float* ct_data, const int ct_dims[3], const floa
                                   dose_corner, beams, num_beams, energy, gpu_id, nuclear_correction, verbose);
 }
 
+int pbs_wrapper_copy_bytes(unsigned long long out[2]) {
+    if (!out) {
+        pbs::set_error("null argument");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    return pbs::wrapper_copy_bytes(out);
+}
+
 int pbs_plan_beam(const PbsBeamDesc* beam, const PbsEnergyDesc* energy, const int ct_dims[3],
                   const float ct_resolution[3], const float ct_corner[3], const int dose_dims[3],
                   const float dose_resolution[3], const float dose_corner[3], PbsBeamStats* out, float* layer_params,

@@ -145,6 +145,7 @@ int Context::take_device_errors() {
     if (rc) return rc;
     volatile int* hostFlags = static_cast<volatile int*>(errHost.ptr);
     PBS_CUDA(cudaMemcpyAsync(errHost.ptr, errWord.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream), "error flags D2H");
+    copiedD2H += sizeof(int);
     PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     const int flags = *hostFlags;
     if (!flags) return PBS_OK;
@@ -169,6 +170,7 @@ int Context::upload(void* dst, const void* src, size_t n) {
     if (rc) return rc;
     std::memcpy(staging.ptr, src, n);
     PBS_CUDA(cudaMemcpyAsync(dst, staging.ptr, n, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+    copiedH2D += n;
     PBS_CUDA(cudaEventRecord(stagingEvent, stream), "cudaEventRecord");
     return PBS_OK;
 }
@@ -255,6 +257,8 @@ int Context::set_energy(const PbsEnergyDesc& e) {
     // The tables are copied from pageable host vectors, which cudaMemcpyAsync
     // stages before it returns; no wait is needed before they are replaced.
     PBS_CUDA(cudaMemcpyAsync(rrl.ptr, rrlHost.data(), rrlHost.size() * 4, cudaMemcpyHostToDevice, stream), "LUT");
+    copiedH2D += (ciddHost.size() + densityHost.size() + spHost.size() + rrlHost.size()) * 4 +
+                 (hasNuc ? 2 * nTab * 4 : 0);
     luts.cidd = static_cast<const float*>(cidd.ptr);
     luts.nS = e.n_energy_samples;
     luts.nE = e.n_energies;
@@ -288,6 +292,11 @@ cudaError_t copy_box(void* dst, const void* src, const int dims[3], const int lo
 }
 
 bool box_empty(const int lo[3], const int hi[3]) { return hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2]; }
+
+unsigned long long box_bytes(const int lo[3], const int hi[3]) {
+    if (box_empty(lo, hi)) return 0;
+    return 4ull * (unsigned long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+}
 
 void merge_box(int lo[3], int hi[3], const int a[3], const int b[3]) {
     if (b[0] < a[0] || b[1] < a[1] || b[2] < a[2]) return;
@@ -338,7 +347,10 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
     if (rc) return rc;
     ctView = nullptr;
     ctQuadValid = false;
-    if (!box_empty(lo, hi)) PBS_CUDA(copy_box(ct.ptr, data, g.dims, lo, hi, cudaMemcpyHostToDevice, stream), "CT H2D");
+    if (!box_empty(lo, hi)) {
+        PBS_CUDA(copy_box(ct.ptr, data, g.dims, lo, hi, cudaMemcpyHostToDevice, stream), "CT H2D");
+        copiedH2D += box_bytes(lo, hi);
+    }
     // The CT type comes from the whole volume, as with a full upload.
     int type = ctInputType != PBS_CT_AUTO ? ctInputType : parse_ct_input_type_env();
     if (type == PBS_CT_AUTO) {
@@ -355,6 +367,7 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
                                               static_cast<const float*>(density.ptr), lutN, energy.density_scale_fact,
                                               static_cast<unsigned*>(stats.ptr), stream),
                      "ct_convert_detect");
+            copiedH2D += ct_type_sample_count(n) * sizeof(float);
             ctType = PBS_CT_AUTO;
             ctGrid = g;
             hasCt = true;
@@ -414,6 +427,7 @@ int Context::issue_dose_copy() {
     PBS_CUDA(copy_box(floatOut.ptr, deferredInit, doseGrid.dims, deferredLo, deferredHi, cudaMemcpyHostToDevice,
                       copyStream),
              "dose H2D");
+    copiedH2D += box_bytes(deferredLo, deferredHi);
     PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
     deferredInit = nullptr;
     return PBS_OK;
@@ -431,6 +445,7 @@ int Context::read_dose_region(float* out, const int lo[3], const int hi[3]) {
                                  lo, hi, stream),
                  "dose_to_float");
         PBS_CUDA(copy_box(out, floatOut.ptr, doseGrid.dims, lo, hi, cudaMemcpyDeviceToHost, stream), "dose D2H");
+        copiedD2H += box_bytes(lo, hi);
     }
     PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     return take_device_errors();
@@ -462,6 +477,7 @@ int Context::set_ct(const float* data, int onDevice, const GridDesc& g) {
     } else {
         // The copy goes first: the CT type is sampled on the host while it runs.
         PBS_CUDA(cudaMemcpyAsync(ct.ptr, data, n * 4, cudaMemcpyHostToDevice, stream), "CT H2D");
+        copiedH2D += n * 4;
         if (type == PBS_CT_AUTO) {
             float mn, mx;
             sample_ct_stats(data, n, mn, mx);
@@ -552,6 +568,7 @@ int Context::reset_dose(const float* init, int onDevice) {
         PBS_CUDA(cudaEventRecord(copyStart, stream), "cudaEventRecord");
         PBS_CUDA(cudaStreamWaitEvent(copyStream, copyStart, 0), "cudaStreamWaitEvent");
         PBS_CUDA(cudaMemcpyAsync(floatOut.ptr, init, n * 4, cudaMemcpyHostToDevice, copyStream), "dose H2D");
+        copiedH2D += n * 4;
         PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
         pendingDoseInit = true;
         doseBoxed = false;
@@ -641,6 +658,7 @@ int Context::read_dose(float* out, int onDevice) {
     }
     if (onDevice) return PBS_OK;
     PBS_CUDA(cudaMemcpyAsync(out, floatOut.ptr, n * 4, cudaMemcpyDeviceToHost, stream), "dose D2H");
+    copiedD2H += n * 4;
     PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     return take_device_errors();
 }
@@ -1541,6 +1559,14 @@ void ct_trace_box(const BeamPlan& P, const int dims[3], int lo[3], int hi[3]) {
 
 }  // namespace
 
+namespace {
+// Host<->device bytes of the calling thread's last completed wrapper call.
+thread_local unsigned long long g_lastWrapperCopies[2] = {0, 0};
+int wrapper_body(Context* ctx, const float* ctData, const GridDesc& cg, float* doseData, const GridDesc& dg,
+                 const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* energyData, int nuclear,
+                 int verbose);
+}  // namespace
+
 int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
                       float* doseData, const int doseDims[3], const float doseRes[3], const float doseCorner[3],
                       const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* energyData, int gpuId,
@@ -1576,6 +1602,24 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
         }
         ctx = c;
     }
+    ctx->copiedH2D = ctx->copiedD2H = 0;
+    int rc = wrapper_body(ctx, ctData, cg, doseData, dg, beams, numBeams, energyData, nuclear, verbose);
+    g_lastWrapperCopies[0] = ctx->copiedH2D;
+    g_lastWrapperCopies[1] = ctx->copiedD2H;
+    return rc;
+}
+
+int wrapper_copy_bytes(unsigned long long out[2]) {
+    out[0] = g_lastWrapperCopies[0];
+    out[1] = g_lastWrapperCopies[1];
+    return PBS_OK;
+}
+
+namespace {
+
+int wrapper_body(Context* ctx, const float* ctData, const GridDesc& cg, float* doseData, const GridDesc& dg,
+                 const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* energyData, int nuclear,
+                 int verbose) {
     int rc;
     if ((rc = ctx->set_energy(*energyData))) return rc;
     // Every beam is planned up front, and the plan is handed to add_planned_beam: the CT
@@ -1623,5 +1667,7 @@ int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRe
     }
     return ctx->read_dose_region(doseData, dLo, dHi);
 }
+
+}  // namespace
 
 }  // namespace pbs

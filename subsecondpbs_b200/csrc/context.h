@@ -171,6 +171,9 @@ struct Context {
     ~Context();
     int init(int gpu);
     int upload(void* dst, const void* src, size_t n);
+    // Bytes this context copied between host and device memory (host-visible
+    // reads of a page-locked CT by the device included), for the end-to-end figures.
+    unsigned long long copiedH2D = 0, copiedD2H = 0;
     int set_energy(const PbsEnergyDesc& e);
     // Reads (and clears) the error flags the kernels raised since the last check;
     // the stream must be synchronised. PBS_OK when none.
@@ -246,6 +249,9 @@ struct OperatorPlan {
 };
 int operator_batch_plan(const PbsBeamDesc& beam, int maxSpotsPerBatch, OperatorPlan& plan);
 
+// Host->device and device->host bytes of the calling thread's last completed
+// subsecond_wrapper call.
+int wrapper_copy_bytes(unsigned long long out[2]);
 int subsecond_wrapper(const float* ctData, const int ctDims[3], const float ctRes[3], const float ctCorner[3],
                       float* doseData, const int doseDims[3], const float doseRes[3], const float doseCorner[3],
                       const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* energyData, int gpuId,

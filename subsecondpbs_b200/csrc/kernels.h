@@ -18,6 +18,8 @@ cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStrea
 // the device: the samples are read from the caller's page-locked host CT through
 // its device mapping (`hostCtMapped`, n values), the conversion runs on the
 // uploaded `ct`. `keys` is two words of device scratch.
+// Number of strided CT samples the type detection reads (the reference's ~100k).
+size_t ct_type_sample_count(size_t n);
 cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const float* densityLut,
                                      int lutN, float lutScale, unsigned* keys, cudaStream_t s);
 

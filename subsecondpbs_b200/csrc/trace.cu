@@ -583,12 +583,18 @@ cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, i
     return cudaGetLastError();
 }
 
+size_t ct_type_sample_count(size_t n) {
+    const size_t maxSamples = 100000;
+    const size_t stride = (n > maxSamples) ? (n / maxSamples) : 1;
+    return n == 0 ? 0 : (n + stride - 1) / stride;
+}
+
 cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const float* densityLut,
                                      int lutN, float lutScale, unsigned* keys, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const size_t maxSamples = 100000;
     const size_t stride = (n > maxSamples) ? (n / maxSamples) : 1;
-    const size_t samples = (n + stride - 1) / stride;
+    const size_t samples = ct_type_sample_count(n);
     cudaError_t e = cudaMemsetAsync(keys, 0xff, sizeof(unsigned), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(keys + 1, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;

@@ -348,14 +348,16 @@ def field_beam(n_spots: int, ion: str, gantry_deg: float, rng: np.random.Generat
 
 def serving_workload(n_requests: int = 1000, rate_hz: float = 100.0, patients_per_class: int = 4,
                      fields_per_patient: int = 4, carbon_fraction: float = 0.2, seed: int = SEED_BASE + 5,
-                     ct_classes=SERVING_CT_CLASSES, max_spots: int = 20000) -> dict:
+                     ct_classes=SERVING_CT_CLASSES, max_spots: int = 20000,
+                     proton_energy: dict | None = None) -> dict:
     """Seeded stream of dose requests: patients with CTs uniform among the three
     size classes of SERVING_CT_CLASSES (heterogeneous_ct recipe), each with
     `fields_per_patient` coplanar fields of a heavy-tailed spot count (500-20000)
     in a proton and a carbon variant; requests arrive as a Poisson process of
     `rate_hz`, pick a patient uniformly, 1-4 of its fields and an ion (carbon with
     `carbon_fraction`, with the nuclear halo). Spot weights are drawn per request
-    (`request_beams`)."""
+    (`request_beams`). `proton_energy` is the proton table dict (default: the
+    synthetic proton tables); carbon uses the synthetic carbon tables."""
     rng = np.random.Generator(np.random.PCG64(seed))
     patients = []
     for c, (dims, res) in enumerate(ct_classes):
@@ -385,7 +387,8 @@ def serving_workload(n_requests: int = 1000, rate_hz: float = 100.0, patients_pe
         requests.append({"index": i, "arrival_s": float(arrivals[i]), "patient": pid, "fields": fids, "ion": ion,
                          "seed": seed + 100000 + i})
     return {"patients": patients, "requests": requests, "rate_hz": rate_hz,
-            "energy": {"proton": proton_tables(), "carbon": carbon_tables()}}
+            "energy": {"proton": proton_tables() if proton_energy is None else proton_energy,
+                       "carbon": carbon_tables()}}
 
 
 def request_beams(workload: dict, req: dict) -> list:

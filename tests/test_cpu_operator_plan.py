@@ -1,7 +1,12 @@
-"""`pbs_operator_batch_plan` (host only, no GPU) against the CPU restatement of
-buildRTDOperatorBatchPlan (include/core/rtd_operator_mode.h:43-111): bit-exact
-spans and batches on seeded beams and on every early-return case of the
-reference's validation."""
+"""`pbs_operator_batch_plan` (host only, no GPU) against buildRTDOperatorBatchPlan
+(include/core/rtd_operator_mode.h:43-111): bit-exact spans and batches on seeded
+beams and on every early-return case of the reference's validation, checked
+against the CPU restatement (oracle/operator_plan.py) and, where the reference
+library built by oracle/ref/build_ref.sh is present, against the reference's own
+header compiled into it (ref_operator_batch_plan of oracle/ref/ref_shim.cu)."""
+import ctypes as C
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -25,10 +30,38 @@ def _beam(counts, n_energies=None, weights=None, positions=None, directions=None
     return b
 
 
+REF_LIB = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "librtd.so"
+
+
+def _reference_plan(beam, m):
+    """The reference header's plan through the shim, in operator_batch_plan's form."""
+    from subsecondpbs_b200 import _lib
+
+    lib = C.CDLL(str(REF_LIB))
+    f = lib.ref_operator_batch_plan
+    f.restype = C.c_int
+    bd, keep = _lib.beam_desc(beam)
+    info = (C.c_int * 6)()
+    spans = (_lib.PbsOperatorLayerSpan * 4096)()
+    batches = (_lib.PbsOperatorBatch * 4096)()
+    assert f(C.byref(bd), int(m), spans, 4096, batches, 4096, info) == 0
+    del keep
+    return {
+        "valid": bool(info[0]),
+        "total_layers": info[1],
+        "total_spots": info[2],
+        "max_spots_per_batch": info[3],
+        "layer_spans": [_lib.struct_to_dict(spans[i]) for i in range(info[4])],
+        "batches": [_lib.struct_to_dict(batches[i]) for i in range(info[5])],
+    }
+
+
 def _check(beam, m):
     got = operator_batch_plan(beam, m)
     want = oracle_plan(beam, m)
     assert got == want
+    if REF_LIB.exists():
+        assert got == _reference_plan(beam, m)
     return got
 
 
