@@ -74,6 +74,14 @@ extern "C" {
  * 1 FLUKA, 2 GAUSS_FIT (default). These are the reference's NUCLEAR_CORR build
  * choices (idd_sigma.cu:102-121, wrapper.cu:3788-3795), selected at run time here. */
 #define PBS_OPT_NUCLEAR_MODEL 6
+/* CarbonPBS lateral profile model of a beam's profile_data (bitmask; default 0).
+ * 1: the effective sigma of every step with dose is replaced by the profile's
+ * (overrideRSigmaFromCarbonProfileKernel, raytracedicom_wrapper.cu:2080-2152),
+ * 2: the IDD is scaled by the profile's overall-weight channel
+ * (applyCarbonProfileOverallWeightKernel, raytracedicom_wrapper.cu:2154-2187).
+ * The reference compiles both but keeps them off (raytracedicom_wrapper.cu:2813-2814);
+ * the wrapper entry points read PBS_CARBON_PROFILE from the environment. */
+#define PBS_OPT_CARBON_PROFILE 7
 
 /* ---- stage timer slots -------------------------------------------------- */
 #define PBS_STAGE_TRACE 0
@@ -137,6 +145,14 @@ typedef struct PbsBeamDesc {
     float sad;
     float ref_plane_z;
     const int* roi_linear_indices;     size_t n_roi_linear_indices;
+    /* CarbonPBS lateral profile model (raytracedicom_integration.h:71-76): the
+     * energy axis of the profile / beam-parameter rows (profileEnergies) and the
+     * beam-parameter reference position (beamParaPos). profile_data is
+     * [rows][depth][channels] (nGauss weights, nGauss sigmas, overall weight),
+     * profile_setting = [depth0, depthStep, depthN], beam_para_data = [rows][3]
+     * (2 sigmaIso^2, rtheta, theta^2). Used only with PBS_OPT_CARBON_PROFILE. */
+    const float* profile_energies;     size_t n_profile_energies;
+    float beam_para_pos;
 } PbsBeamDesc;
 
 /* Mirrors RTDEnergyStruct (include/core/raytracedicom_integration.h:99-128). */
@@ -322,6 +338,18 @@ PBS_API int pbs_context_influence_csc(PbsContext* ctx, const PbsBeamDesc* beam, 
                                       long long spot_begin, long long spot_count, double threshold,
                                       long long* col_ptr, int* rows, float* values, long long capacity,
                                       long long* nnz);
+/* Row norms of the same influence matrix, the quantity CarbonPBS's cuCalDoseNorm
+ * returns (carbonPBS/cudaCalDose.cpp:347-500, calDoseSumSquareKernel,
+ * carbonPBS/deviceCalDose.cu:123-229): for every requested voxel the sum over the
+ * spots [spot_begin, spot_begin + spot_count) of its squared dose per unit spot
+ * weight, accumulated in FP64 on the device without forming the matrix. `voxels`
+ * holds n_voxels linear indices (z*Y + y)*X + x and `out` receives one float each;
+ * with voxels == NULL, `out` receives the whole grid [Z][Y][X]. Same plan, lattice
+ * requirement and error behaviour as pbs_context_influence_csc; the context's dose
+ * is zero on return. */
+PBS_API int pbs_context_influence_row_norms(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction,
+                                            long long spot_begin, long long spot_count, const long long* voxels,
+                                            long long n_voxels, float* out);
 PBS_API int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device);
 /* Copy the FP64 accumulator [Z][Y][X] out (host or device pointer), e.g. for a
  * cross-GPU reduction of beam doses. */
@@ -329,6 +357,67 @@ PBS_API int pbs_context_read_dose64(PbsContext* ctx, double* out, int out_on_dev
 /* Measure the FP32 FMA throughput of `gpu_id` with a register-resident FFMA loop
  * (TFLOP/s, 2 flops per FMA): the denominator of the superposition roofline. */
 PBS_API int pbs_measure_fp32_peak(int gpu_id, double* tflops);
+
+/* ---- biological maps on top of the physical dose --------------------------
+ * CarbonPBS computes, with its own point-kernel engine, the dose-averaged linear-
+ * quadratic parameters of every voxel and an RBE map from them
+ * (cuCalFinalDoseAndRBEKernel and LQRBEKernel, carbonPBS/deviceCalDose.cu:587-772;
+ * the LEM variant lemRBEMapKernel, :1027-1057, has the same RBE arithmetic; the MKM
+ * variant mkmRBEMapKernel, :1060-1126). Here the same quantities ride on this
+ * library's pencil-beam dose: every step of every ray carries its IDD times the
+ * step's biological factors, superposed and transferred like the dose itself.
+ *
+ * LET at a step: the dose-averaged LET of `let_samples` depth samples
+ * t_j = LET(weq + range_shifter + (j - (n-1)/2) * est_dimension / n) of the layer's
+ * energy row (let = sum t_j^2 / sum t_j, deviceCalDose.cu:686-692), from the table
+ * let_table [let_rows][let_depths] (keV/um) on the depth axis let_depth0 +
+ * i * let_depth_step (mm water-equivalent) and the energy axis let_energies
+ * (ascending MeV/u; a layer's row is its fractional position on that axis).
+ * LQ model: alpha and beta of the step from lq_alpha / lq_beta [n_lq] at
+ * log10(LET) on the axis lq_log0 + i * lq_log_step (the reference's lqData is
+ * indexed by log10(LET) * 100, lq_log0 = 0, lq_log_step = 0.01); the voxel mixes
+ * alpha and sqrt(beta) dose-weighted. MKM: z1D [n_lq] on the same axis, mixed
+ * dose-weighted, with the photon reference (alpha0, beta0). Tables are linearly
+ * interpolated and clamped at their ends. Beams with the nuclear halo are refused
+ * (PBS_ERR_UNSUPPORTED) while a model is set. */
+#define PBS_BIO_OFF 0
+#define PBS_BIO_LQ 1
+#define PBS_BIO_MKM 2
+typedef struct PbsBioModel {
+    int model;                                    /* PBS_BIO_* */
+    const float* let_table; int let_rows, let_depths;
+    const float* let_energies;                    /* [let_rows] */
+    float let_depth0, let_depth_step;
+    int let_samples;
+    float est_dimension, range_shifter;
+    const float* lq_alpha;                        /* [n_lq], LQ */
+    const float* lq_beta;                         /* [n_lq], LQ */
+    const float* z1d;                             /* [n_lq], MKM */
+    int n_lq;
+    float lq_log0, lq_log_step;
+    float alpha0, beta0;                          /* MKM photon reference */
+} PbsBioModel;
+
+/* Maps over the beams added since the last dose reset (an initial dose passed to
+ * the reset is not part of them). DOSE: their physical dose. LETD: dose-averaged
+ * LET. RBE: LQ, 3.988565 / D10 with D10 the dose of the mixed alpha, beta at 10 %
+ * survival, 1 where the dose, alpha or beta is 0 (LQRBEKernel); MKM, the
+ * mkmRBEMapKernel expression, 1 at or below 1e-3 Gy. RBE_DOSE: RBE x DOSE.
+ * ALPHA / BETA: the mixed LQ parameters (LQ only). Z1D: 0.172 + beta0 x the mixed
+ * z1D (MKM only, the reference's second MKM map). */
+#define PBS_BIO_MAP_DOSE 0
+#define PBS_BIO_MAP_LETD 1
+#define PBS_BIO_MAP_RBE 2
+#define PBS_BIO_MAP_RBE_DOSE 3
+#define PBS_BIO_MAP_ALPHA 4
+#define PBS_BIO_MAP_BETA 5
+#define PBS_BIO_MAP_Z1D 6
+
+/* Sets (model != PBS_BIO_OFF, tables copied to the device) or clears the model;
+ * the biological accumulators start at zero and are cleared with every dose reset. */
+PBS_API int pbs_context_set_bio_model(PbsContext* ctx, const PbsBioModel* model);
+/* One map as float [Z][Y][X] into host (out_on_device = 0) or device memory. */
+PBS_API int pbs_context_read_bio_map(PbsContext* ctx, int map, float* out, int out_on_device);
 
 /* ---- allocation-free stage entry (no counterpart in the reference) ---------
  * Legacy CPB fluence of `n_layers` layers on the calling thread's current

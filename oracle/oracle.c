@@ -213,6 +213,154 @@ static int g_texq = 0;
 static double texw(double a) { return g_texq == 1 ? rint(a * 256.0) / 256.0 : (g_texq == 2 ? floor(a * 256.0) / 256.0 : a); }
 void oracle_set_texture_quantization(int on) { g_texq = on; }
 
+static float frac_index_monotonic(const float* v, int n, float value);
+
+/* CarbonPBS lateral profile model (off by default, as in the reference): bit 1
+ * overrideRSigmaFromCarbonProfileKernel (raytracedicom_wrapper.cu:2080-2152), bit 2
+ * applyCarbonProfileOverallWeightKernel (raytracedicom_wrapper.cu:2154-2187). */
+static int g_profile = 0;
+void oracle_set_carbon_profile(int mode) { g_profile = mode; }
+
+typedef struct ProfileC {
+    int table, beamPara, rows, depthN, channels;
+    float depth0, depthStep;
+} ProfileC;
+
+/* Table shape the reference infers (raytracedicom_wrapper.cu:2816-2862). */
+static void profile_shape(const PbsBeamDesc* b, int L, ProfileC* o) {
+    memset(o, 0, sizeof(*o));
+    const size_t nData = b->profile_data ? b->n_profile_data : 0;
+    const size_t nPara = b->beam_para_data ? b->n_beam_para_data : 0;
+    const size_t nProfE = b->profile_energies ? b->n_profile_energies : 0;
+    o->beamPara = nPara >= (size_t)L * 3u;
+    if (!(b->profile_setting && b->n_profile_setting >= 3 && lroundf(b->profile_setting[2]) > 0 && nData > 0)) return;
+    o->depth0 = b->profile_setting[0];
+    o->depthStep = b->profile_setting[1];
+    o->depthN = (int)lroundf(b->profile_setting[2]);
+    if (o->depthN < 1) o->depthN = 1;
+    const size_t plane = (size_t)o->depthN;
+    const int paraRows = (int)(nPara / 3u);
+    if (paraRows > 0 && nPara == (size_t)paraRows * 3u && nData % ((size_t)paraRows * plane) == 0)
+        o->rows = paraRows;
+    else if (nProfE > 0 && nData % (nProfE * plane) == 0)
+        o->rows = (int)nProfE;
+    else if (L > 0 && nData % ((size_t)L * plane) == 0)
+        o->rows = L;
+    else if (nData % plane == 0 && (nData / plane) % 11u == 0)
+        o->rows = (int)((nData / plane) / 11u);
+    const size_t perRow = o->rows > 0 ? nData / (size_t)o->rows : 0;
+    if (o->rows > 0 && perRow >= plane) {
+        o->channels = (int)(perRow / plane);
+        o->table = o->channels > 0 && (size_t)o->rows * plane * (size_t)o->channels == nData;
+    }
+}
+
+/* Fractional table row of layer l (raytracedicom_wrapper.cu:4577-4590). */
+static float profile_row(const PbsBeamDesc* b, const PbsEnergyDesc* e, const ProfileC* pc, int L, int l, float eIdx) {
+    const int lastRow = pc->rows - 1 > 0 ? pc->rows - 1 : 0;
+    const size_t nProfE = b->profile_energies ? b->n_profile_energies : 0;
+    float r;
+    if (pc->rows == L)
+        r = (float)l;
+    else if (nProfE > 0 && pc->rows == (int)nProfE)
+        r = frac_index_monotonic(b->profile_energies, (int)nProfE, b->energies[l]);
+    else if (pc->rows == e->n_energies && e->energies_per_u && e->n_energies_per_u > 0)
+        r = fminf(fmaxf(eIdx, 0.0f), (float)(pc->rows - 1));
+    else
+        r = fminf(fmaxf((float)l, 0.0f), (float)lastRow);
+    return fminf(fmaxf(r, 0.0f), (float)lastRow);
+}
+
+/* Linear filter of the profile texture at channel c, depth index d, row index r
+ * (both clamped to the table), in double. */
+static double profile_at(const float* t, const ProfileC* pc, int c, double d, double r) {
+    double fd = floor(d), fr = floor(r);
+    int d0 = (int)fd, r0 = (int)fr;
+    int d1 = d0 + 1 < pc->depthN ? d0 + 1 : pc->depthN - 1, r1 = r0 + 1 < pc->rows ? r0 + 1 : pc->rows - 1;
+    double ad = texw(d - fd), ar = texw(r - fr);
+    double a0 = t[((size_t)r0 * pc->depthN + d0) * pc->channels + c], a1 = t[((size_t)r0 * pc->depthN + d1) * pc->channels + c];
+    double b0 = t[((size_t)r1 * pc->depthN + d0) * pc->channels + c], b1 = t[((size_t)r1 * pc->depthN + d1) * pc->channels + c];
+    double lo = a0 + (a1 - a0) * ad, hi = b0 + (b1 - b0) * ad;
+    return lo + (hi - lo) * ar;
+}
+
+/* Biological model (pbs_context_set_bio_model): when set, every layer's IDD is
+ * also scaled by the steps' biological factors, superposed and transferred into
+ * the accumulators [4][Z][Y][X]: dose, dose x alpha (LQ) or z1D (MKM), dose x
+ * sqrt(beta) (LQ), dose x LET. */
+static const PbsBioModel* g_bio = NULL;
+static double* g_bioAcc = NULL;
+void oracle_set_bio(const PbsBioModel* m, double* acc) {
+    g_bio = (m && m->model != PBS_BIO_OFF) ? m : NULL;
+    g_bioAcc = acc;
+}
+
+static double table_at_d(const float* t, int n, double x) {
+    if (x < 0.0) x = 0.0;
+    if (x > n - 1) x = n - 1;
+    double f = floor(x);
+    int i0 = (int)f, i1 = i0 + 1 < n ? i0 + 1 : n - 1;
+    return t[i0] + ((double)t[i1] - t[i0]) * (x - f);
+}
+
+/* Dose-averaged LET of a step over the model's depth samples (deviceCalDose.cu:686-692). */
+static double bio_let(const PbsBioModel* m, double row, double weq) {
+    if (row < 0.0) row = 0.0;
+    if (row > m->let_rows - 1) row = m->let_rows - 1;
+    double fr = floor(row);
+    int r0 = (int)fr, r1 = r0 + 1 < m->let_rows ? r0 + 1 : m->let_rows - 1;
+    double ar = row - fr, s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < m->let_samples; ++j) {
+        double depth = weq + m->range_shifter + (j - 0.5 * (m->let_samples - 1)) * m->est_dimension / m->let_samples;
+        double x = (depth - m->let_depth0) / m->let_depth_step;
+        double a = table_at_d(m->let_table + (size_t)r0 * m->let_depths, m->let_depths, x);
+        double b = table_at_d(m->let_table + (size_t)r1 * m->let_depths, m->let_depths, x);
+        double t = a + (b - a) * ar;
+        s1 += t;
+        s2 += t * t;
+    }
+    return s1 > 0.0 ? s2 / s1 : 0.0;
+}
+
+/* Factor of channel c (0: alpha or z1D, 1: sqrt(beta), 2: LET) at LET `let`. */
+static double bio_factor(const PbsBioModel* m, int c, double let) {
+    if (c == 2) return let;
+    double li = let > 0.0 ? (log10(let) - m->lq_log0) / m->lq_log_step : 0.0;
+    if (m->model == PBS_BIO_MKM) return table_at_d(m->z1d, m->n_lq, li);
+    if (c == 0) return table_at_d(m->lq_alpha, m->n_lq, li);
+    double b = table_at_d(m->lq_beta, m->n_lq, li);
+    return sqrt(b > 0.0 ? b : 0.0);
+}
+
+/* The maps of pbs_context_read_bio_map from the accumulators (LQRBEKernel,
+ * deviceCalDose.cu:738-772; mkmRBEMapKernel, :1060-1126). */
+void oracle_bio_map(const PbsBioModel* m, const double* acc, size_t n, int map, double* out) {
+    const double *D = acc, *c0 = acc + n, *c1 = acc + 2 * n, *c2 = acc + 3 * n;
+    for (size_t i = 0; i < n; ++i) {
+        double d = D[i], v = 0.0;
+        if (map == PBS_BIO_MAP_DOSE) v = d;
+        else if (map == PBS_BIO_MAP_LETD) v = d > 0.0 ? c2[i] / d : 0.0;
+        else if (map == PBS_BIO_MAP_ALPHA) v = d > 0.0 ? c0[i] / d : 0.0;
+        else if (map == PBS_BIO_MAP_BETA) { double sb = d > 0.0 ? c1[i] / d : 0.0; v = sb * sb; }
+        else if (map == PBS_BIO_MAP_Z1D) v = 0.172 + (double)m->beta0 * (d > 0.0 ? c0[i] / d : 0.0);
+        else {
+            double rbe = 1.0;
+            if (m->model == PBS_BIO_MKM) {
+                double a = 0.172 + (double)m->beta0 * (d > 0.0 ? c0[i] / d : 0.0);
+                double b0 = m->beta0, t2 = (double)m->alpha0 / 2.0 / b0;
+                double dx = -t2 + sqrt(t2 * t2 + (a * d + b0 * d * d) / b0);
+                rbe = d > 1e-3 ? dx / d : 1.0;
+            } else if (d != 0.0 && c0[i] != 0.0 && c1[i] != 0.0) {
+                double a = c0[i] / d, sb = c1[i] / d, b = sb * sb;
+                double d10 = (-a + sqrt(a * a - 4.0 * -2.302585 * b)) / b * 0.5;
+                rbe = 3.988565 / d10;
+            }
+            v = map == PBS_BIO_MAP_RBE ? rbe : rbe * d;
+        }
+        out[i] = v;
+    }
+}
+
 /* tex1D linear/clamp/unnormalised evaluated in double. */
 static double lut1(const float* t, int n, double x) {
     double xb = x - 0.5;
@@ -1239,6 +1387,28 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
         const int nucOn = nuc && spotDist > 0.0f;
         const double rEref = nucOn ? eRefSq : 198.81, rDelta = nucOn ? sigDelta : 0.21;
         const int rSuppress = nucOn ? suppressDip : 0;
+        /* CarbonPBS profile model of the layer: what each switch runs on this beam
+         * (raytracedicom_wrapper.cu:4656-4660, 4814-4818, and the kernels' own early
+         * returns), the table row and the interpolated beam parameters (4592-4606). */
+        ProfileC pc;
+        profile_shape(b, L, &pc);
+        const int pOverride = (g_profile & 1) && pc.table && pc.beamPara && pc.channels >= 3 &&
+                              (pc.channels - 1) / 2 > 0 && pc.depthStep > 0.0f;
+        const int pWeight = (g_profile & 2) && pc.table && pc.channels > 0 && pc.depthStep > 0.0f;
+        const float pRow = profile_row(b, e, &pc, L, l, eIdx);
+        double bp[3] = {0.0, 0.0, 0.0};
+        if (pc.rows > 0 && b->beam_para_data && b->n_beam_para_data >= (size_t)pc.rows * 3u) {
+            const float cr = fminf(fmaxf(pRow, 0.0f), (float)(pc.rows - 1));
+            int i0 = (int)floorf(cr);
+            if (i0 < 0) i0 = 0;
+            if (i0 > pc.rows - 1) i0 = pc.rows - 1;
+            const int i1 = i0 + 1 < pc.rows ? i0 + 1 : pc.rows - 1;
+            const float t = cr - (float)i0;
+            for (int k = 0; k < 3; ++k) {
+                const float v0 = b->beam_para_data[(size_t)i0 * 3 + k], v1 = b->beam_para_data[(size_t)i1 * 3 + k];
+                bp[k] = v0 + (v1 - v0) * t;
+            }
+        }
         for (size_t i = 0; i < (size_t)S * pad; ++i) { idd[i] = 0.0; rsg[i] = NaNinf; }
         if (nucOn)
             for (size_t i = 0; i < (size_t)S * nucPad; ++i) { nIdd[i] = 0.0; nRsg[i] = NaNinf; }
@@ -1309,6 +1479,48 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
                         if (sp > (double)rangeStop || (unsigned)k == afterLast) { live = 0; afterLast = (unsigned)k; }
                     }
                     if (!live || k < firstIn - 1) { res = 0.0; rs = NaNinf; nRes = 0.0; nRs = NaNinf; }
+                    if (pOverride || pWeight) {
+                        const double sp = wepl[(size_t)k * rays + r];
+                        double dI = (sp - pc.depth0) / pc.depthStep;
+                        if (dI < 0.0) dI = 0.0;
+                        if (dI > pc.depthN - 1) dI = pc.depthN - 1;
+                        if (pOverride) {
+                            if (!(res > 0.0)) {
+                                rs = NaNinf;
+                            } else {
+                                const int nG = (pc.channels - 1) / 2;
+                                double sumW = 0.0, sumS2 = 0.0;
+                                for (int gi = 0; gi < nG; ++gi) {
+                                    const double wv = profile_at(b->profile_data, &pc, gi, dI, pRow);
+                                    const double sv = profile_at(b->profile_data, &pc, gi + nG, dI, pRow);
+                                    sumW += wv;
+                                    sumS2 += wv * sv * sv;
+                                }
+                                if (!(sumW > 1.0e-8)) {
+                                    rs = NaNinf;
+                                } else {
+                                    const double sad = 0.5 * ((double)P->p.source_dist[0] + P->p.source_dist[1]);
+                                    const double fx = (double)P->p.fan_corner[0] + x * (double)P->p.fan_delta[0];
+                                    const double fy = (double)P->p.fan_corner[1] + y * (double)P->p.fan_delta[1];
+                                    const double fz = (double)P->p.fan_corner[2] + k * (double)P->p.fan_delta[2];
+                                    const double sdx = P->p.source_dist[0], sdy = P->p.source_dist[1];
+                                    const double proj = (sad - fz) * sqrt(1.0 + fx * fx / (sdx * sdx) + fy * fy / (sdy * sdy));
+                                    const double phy = proj - (sad - (double)b->beam_para_pos);
+                                    const double r2 = bp[0] + 2.0 * bp[1] * phy + bp[2] * phy * phy;
+                                    double ax2 = r2 + sumS2 / sumW;
+                                    ax2 = 0.5 * (ax2 > 0.0 ? ax2 : 0.0);
+                                    const double zk = (double)P->p.fan_corner[2] + (double)k * P->p.fan_delta[2];
+                                    const double vx = P->p.fan_delta[0] * (1.0 - zk / P->p.source_dist[0]);
+                                    const double vy = P->p.fan_delta[1] * (1.0 - zk / P->p.source_dist[1]);
+                                    rs = 0.5 * (0.5 * (vx + vy)) / (sqrt(2.0) * (sqrt(ax2) + 0.21));
+                                }
+                            }
+                        }
+                        if (pWeight && res > 0.0) {
+                            const double ow = profile_at(b->profile_data, &pc, pc.channels - 1, dI, pRow);
+                            res *= ow > 0.0 ? ow : 0.0;
+                        }
+                    }
                     idd[(size_t)k * pad + (size_t)y * PX + x] = res;
                     rsg[(size_t)k * pad + (size_t)y * PX + x] = rs;
                     if (nIdx >= 0) {
@@ -1351,6 +1563,38 @@ static int run_beam(const float* ct, const int* cd, double* dose, const int* dd,
             for (size_t i = 0; i < (size_t)S * bevPlane; ++i) bevSum[i] += bevL[i];
         int box[6];
         transfer_layer(&P->fanToDose, PX, PY, first, calc, passive, compat, bevL, BX, BY, dose, dd, box);
+        if (g_bio && g_bioAcc) {
+            /* Biological channels with the layer's radii: IDD x factor, superposed
+             * and transferred like the dose; the layer's dose into accumulator 0. */
+            const size_t nGrid = (size_t)dd[0] * dd[1] * dd[2];
+            int bbox[6];
+            transfer_layer(&P->fanToDose, PX, PY, first, calc, passive, compat, bevL, BX, BY, g_bioAcc, dd, bbox);
+            const double bioRow = frac_index_monotonic(g_bio->let_energies, g_bio->let_rows, b->energies[l]);
+            double* cIdd = (double*)malloc(sizeof(double) * S * pad);
+            double* cBev = (double*)malloc(sizeof(double) * S * bevPlane);
+            for (int c = 0; c < 3; ++c) {
+                if (c == 1 && g_bio->model != PBS_BIO_LQ) continue;
+                for (size_t i = 0; i < (size_t)S * pad; ++i) cIdd[i] = 0.0;
+#pragma omp parallel for schedule(static)
+                for (int k = first; k < afterLastL; ++k)
+                    for (int y = 0; y < RY; ++y)
+                        for (int x = 0; x < RX; ++x) {
+                            const size_t o = (size_t)k * pad + (size_t)y * PX + x;
+                            if (!(idd[o] > 0.0)) continue;
+                            const double let = bio_let(g_bio, bioRow, wepl[(size_t)k * rays + (size_t)y * RX + x]);
+                            cIdd[o] = idd[o] * bio_factor(g_bio, c, let);
+                        }
+                memset(cBev, 0, sizeof(double) * S * bevPlane);
+#pragma omp parallel for schedule(dynamic, 1)
+                for (int k = first; k < calc; ++k)
+                    superpose_step(cIdd + (size_t)k * pad, rsg + (size_t)k * pad, codes + (size_t)k * tiles, map, PX,
+                                   TX, TY, cBev + (size_t)k * bevPlane, BX);
+                transfer_layer(&P->fanToDose, PX, PY, first, calc, passive, compat, cBev, BX, BY,
+                               g_bioAcc + (size_t)(c + 1) * nGrid, dd, bbox);
+            }
+            free(cIdd);
+            free(cBev);
+        }
         /* Nuclear halo: tile radii over [first, calc) with no overflow merge
          * (complete_superposition.cu:558-708), superposition on the halo grid and
          * its own transfer (wrapper.cu:5510-5600, prim_transf_kernel.cu:46-78). */

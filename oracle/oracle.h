@@ -115,6 +115,16 @@ void oracle_set_texture_quantization(int on);
 
 const char* oracle_last_error(void);
 
+/* CarbonPBS lateral profile model on the beams' profile_data (bitmask, default 0
+ * as in the reference): 1 effective-sigma override, 2 overall IDD weight. */
+void oracle_set_carbon_profile(int mode);
+
+/* Biological model for the next oracle_dose calls (NULL clears it) and the
+ * accumulators [4][Z][Y][X] they add to (dose, dose x factor 0, 1, 2); and the
+ * maps of pbs_context_read_bio_map from such accumulators. */
+void oracle_set_bio(const PbsBioModel* m, double* acc);
+void oracle_bio_map(const PbsBioModel* m, const double* acc, size_t n, int map, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,12 @@ def load() -> C.CDLL:
     lib.oracle_batch.restype = None
     lib.oracle_batch.argtypes = [_IP, _IP, _IP]
     lib.oracle_last_error.restype = C.c_char_p
+    lib.oracle_set_carbon_profile.restype = None
+    lib.oracle_set_carbon_profile.argtypes = [C.c_int]
+    lib.oracle_set_bio.restype = None
+    lib.oracle_set_bio.argtypes = [C.POINTER(P.PbsBioModel), _DP]
+    lib.oracle_bio_map.restype = None
+    lib.oracle_bio_map.argtypes = [C.POINTER(P.PbsBioModel), _DP, C.c_size_t, C.c_int, _DP]
     _lib = lib
     return lib
 
@@ -113,10 +119,15 @@ def plan(case: dict, beam: dict | None = None, with_lattice: bool = False) -> di
 
 
 def dose(case: dict, beams: list | None = None, initial=None, ct_type: int = 0, compat_bev_z_shift: bool = False,
-         threads: int = 0, capture: bool = False, capture_layers: bool = False, nuclear_model: int = -1) -> dict:
+         threads: int = 0, capture: bool = False, capture_layers: bool = False, nuclear_model: int = -1,
+         carbon_profile: int = 0, bio: dict | None = None) -> dict:
     """Run the oracle; returns {'dose': float64 [Z][Y][X], 'capture': {...}}.
     `nuclear_model` -1 runs without the nuclear halo; 0/1/2 select SOUKUP, FLUKA
-    and GAUSS_FIT (the energy dict then carries the nuclear tables)."""
+    and GAUSS_FIT (the energy dict then carries the nuclear tables).
+    `carbon_profile` switches on the CarbonPBS lateral profile model of the beams'
+    profile_data (bits: 1 sigma override, 2 overall weight). With a biological
+    model `bio` (the dict of subsecondpbs_b200._lib.bio_desc) the result also holds
+    'bio_acc', its accumulators float64 [4][Z][Y][X]."""
     from subsecondpbs_b200 import _lib as P
     from subsecondpbs_b200.cudaCalDoseRTD import _with_luts
 
@@ -172,17 +183,44 @@ def dose(case: dict, beams: list | None = None, initial=None, ct_type: int = 0, 
         for name, a in bufs.items():
             setattr(cap, name, a.ctypes.data_as(types[name]))
         bufs["plan"] = pl
+    lib.oracle_set_carbon_profile(int(carbon_profile))
+    bio_acc = None
+    if bio:
+        bd_bio, keep_bio = P.bio_desc(bio)
+        bio_acc = np.zeros((4, dd[2], dd[1], dd[0]), np.float64)
+        lib.oracle_set_bio(C.byref(bd_bio), bio_acc.ctypes.data_as(_DP))
     rc = lib.oracle_dose_nuclear(ct.ctypes.data_as(_FP), P.int3(case["ct_dims"]), P.float3(case["ct_resolution"]),
                                  P.float3(case["ct_corner"]), dose_arr.ctypes.data_as(_DP), P.int3(dd),
                                  P.float3(case["dose_resolution"]), P.float3(case["dose_corner"]), arr, len(descs),
                                  C.byref(ed), int(ct_type), int(bool(compat_bev_z_shift)), int(nuclear_model),
                                  int(threads), C.byref(cap) if cap is not None else None)
+    lib.oracle_set_carbon_profile(0)
+    lib.oracle_set_bio(None, None)
     _err(rc)
     if cap is not None:
         bufs["superpose_fma"] = cap.superpose_fma
         bufs["nuc_superpose_fma"] = cap.nuc_superpose_fma
     del keep, ke
-    return {"dose": dose_arr, "capture": bufs}
+    out = {"dose": dose_arr, "capture": bufs}
+    if bio_acc is not None:
+        out["bio_acc"] = bio_acc
+        del keep_bio
+    return out
+
+
+def bio_map(bio: dict, acc: np.ndarray, name: str) -> np.ndarray:
+    """The map `name` ('dose', 'letd', 'rbe', 'rbe_dose', 'alpha', 'beta', 'z1d') of the
+    oracle's biological accumulators, float64 [Z][Y][X]."""
+    from subsecondpbs_b200 import _lib as P
+
+    lib = load()
+    m, keep = P.bio_desc(bio)
+    acc = np.ascontiguousarray(acc, np.float64)
+    n = acc[0].size
+    out = np.zeros(acc.shape[1:], np.float64)
+    lib.oracle_bio_map(C.byref(m), acc.ctypes.data_as(_DP), n, P.BIO_MAPS[name], out.ctypes.data_as(_DP))
+    del keep
+    return out
 
 
 def radius_bucket(m: float) -> int:

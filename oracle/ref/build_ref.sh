@@ -4,18 +4,36 @@
 # The checkout is $REFERENCE_DIR, else a sibling of this repository named
 # `reference` (<repo>/../reference); without either the script stops with a message.
 # Test infrastructure only: the result is run on the GPU box to pin the oracle.
-# Usage: bash oracle/ref/build_ref.sh [NUCLEAR_CORR value, e.g. GAUSS_FIT]
+# Usage: bash oracle/ref/build_ref.sh [NUCLEAR_CORR value, e.g. GAUSS_FIT | OFF] [profile]
+# With `profile` the wrapper is compiled from a copy (made under oracle/_ref/, the
+# checkout is never written) in which the CarbonPBS lateral profile model's two
+# switches (useCarbonProfileSigmaOverride, useCarbonProfileOverallWeight,
+# raytracedicom_wrapper.cu:2813-2814) are turned on: oracle/_ref/librtd_profile.so.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF=${REFERENCE_DIR:-"$HERE/../../../reference"}
 OUT="$HERE/../_ref"
 NUC="${1:-OFF}"
+PROFILE="${2:-}"
 mkdir -p "$OUT"
 if [ ! -d "$REF/src" ]; then echo "reference sources not found at $REF" >&2; exit 1; fi
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
 TAG=rtd
 DEFS="-DSOUKUP=0 -DFLUKA=1 -DGAUSS_FIT=2"
 if [ "$NUC" != "OFF" ]; then DEFS="$DEFS -DNUCLEAR_CORR=$NUC"; TAG="rtd_nuc"; fi
+WRAPPER_SRC="$REF/src/core/raytracedicom_wrapper.cu"
+if [ "$PROFILE" = "profile" ]; then
+  TAG="${TAG}_profile"
+  mkdir -p "$OUT/profile_src"
+  WRAPPER_SRC="$OUT/profile_src/raytracedicom_wrapper.cu"
+  sed -e 's/const bool useCarbonProfileSigmaOverride = false;/const bool useCarbonProfileSigmaOverride = true;/' \
+      -e 's/const bool useCarbonProfileOverallWeight = false;/const bool useCarbonProfileOverallWeight = true;/' \
+      "$REF/src/core/raytracedicom_wrapper.cu" > "$WRAPPER_SRC.tmp"
+  if [ "$(grep -c 'useCarbonProfile[A-Za-z]* = true;' "$WRAPPER_SRC.tmp")" != "2" ]; then
+    echo "profile switches not found in raytracedicom_wrapper.cu" >&2; exit 1
+  fi
+  if [ ! -f "$WRAPPER_SRC" ] || ! cmp -s "$WRAPPER_SRC.tmp" "$WRAPPER_SRC"; then mv "$WRAPPER_SRC.tmp" "$WRAPPER_SRC"; else rm "$WRAPPER_SRC.tmp"; fi
+fi
 INC="-I$REF/include -I$REF/include/core -I$REF/include/algorithms -I$REF/include/utils"
 # The reference's own compile options (CMakeLists.txt:180-187, separable compilation).
 FLAGS="-O3 -use_fast_math -std=c++17 -rdc=true -Xcompiler -fPIC -gencode arch=compute_100a,code=sm_100a -w"
@@ -29,8 +47,10 @@ mkdir -p "$OBJ"
 objs=()
 for s in $SRCS; do
   o="$OBJ/$(echo "$s" | tr '/' '_').o"
-  if [ ! -f "$o" ] || [ "$REF/$s" -nt "$o" ]; then
-    "$NVCC" $FLAGS $DEFS $INC -c "$REF/$s" -o "$o"
+  src="$REF/$s"
+  if [ "$s" = "src/core/raytracedicom_wrapper.cu" ]; then src="$WRAPPER_SRC"; fi
+  if [ ! -f "$o" ] || [ "$src" -nt "$o" ]; then
+    "$NVCC" $FLAGS $DEFS $INC -c "$src" -o "$o"
   fi
   objs+=("$o")
 done

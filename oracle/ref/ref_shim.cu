@@ -49,6 +49,8 @@ static RTDBeamSettings to_reference(const PbsBeamDesc& d) {
     b.profileData = vec(d.profile_data, d.n_profile_data);
     b.profileSetting = vec(d.profile_setting, d.n_profile_setting);
     b.beamParaData = vec(d.beam_para_data, d.n_beam_para_data);
+    b.profileEnergies = vec(d.profile_energies, d.n_profile_energies);
+    b.beamParaPos = d.beam_para_pos;
     b.beamDirection = f3(d.beam_direction);
     b.bmXDirection = f3(d.bm_x_direction);
     b.bmYDirection = f3(d.bm_y_direction);

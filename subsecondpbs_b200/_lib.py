@@ -30,6 +30,9 @@ PBS_OPT_LAYER_BUDGET_MIB = 3
 PBS_OPT_CT_INPUT_TYPE = 4
 PBS_OPT_KEEP_DEBUG = 5
 PBS_OPT_NUCLEAR_MODEL = 6
+PBS_OPT_CARBON_PROFILE = 7
+PBS_BIO_OFF, PBS_BIO_LQ, PBS_BIO_MKM = 0, 1, 2
+BIO_MAPS = {"dose": 0, "letd": 1, "rbe": 2, "rbe_dose": 3, "alpha": 4, "beta": 5, "z1d": 6}
 NUCLEAR_SOUKUP, NUCLEAR_FLUKA, NUCLEAR_GAUSS_FIT = 0, 1, 2
 
 STAGES = ("trace", "plan", "conv", "idd", "bin", "superpose", "transfer")
@@ -89,6 +92,23 @@ class PbsBeamDesc(C.Structure):
         ("sad", C.c_float),
         ("ref_plane_z", C.c_float),
         ("roi_linear_indices", _IP), ("n_roi_linear_indices", C.c_size_t),
+        ("profile_energies", _FP), ("n_profile_energies", C.c_size_t),
+        ("beam_para_pos", C.c_float),
+    ]
+
+
+class PbsBioModel(C.Structure):
+    _fields_ = [
+        ("model", C.c_int),
+        ("let_table", _FP), ("let_rows", C.c_int), ("let_depths", C.c_int),
+        ("let_energies", _FP),
+        ("let_depth0", C.c_float), ("let_depth_step", C.c_float),
+        ("let_samples", C.c_int),
+        ("est_dimension", C.c_float), ("range_shifter", C.c_float),
+        ("lq_alpha", _FP), ("lq_beta", _FP), ("z1d", _FP),
+        ("n_lq", C.c_int),
+        ("lq_log0", C.c_float), ("lq_log_step", C.c_float),
+        ("alpha0", C.c_float), ("beta0", C.c_float),
     ]
 
 
@@ -219,6 +239,10 @@ def load() -> C.CDLL:
         "pbs_operator_batch_plan": (i, [C.POINTER(PbsBeamDesc), i, vp, i, vp, i, C.POINTER(C.c_int)]),
         "pbs_context_influence_csc": (i, [vp, C.POINTER(PbsBeamDesc), i, C.c_longlong, C.c_longlong, C.c_double,
                                           C.POINTER(C.c_longlong), vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "pbs_context_influence_row_norms": (i, [vp, C.POINTER(PbsBeamDesc), i, C.c_longlong, C.c_longlong, vp,
+                                                C.c_longlong, vp]),
+        "pbs_context_set_bio_model": (i, [vp, C.POINTER(PbsBioModel)]),
+        "pbs_context_read_bio_map": (i, [vp, i, vp, i]),
         "pbs_context_read_dose": (i, [vp, vp, i]),
         "pbs_context_read_dose64": (i, [vp, vp, i]),
         "pbs_measure_fp32_peak": (i, [i, C.POINTER(C.c_double)]),
@@ -333,7 +357,56 @@ def beam_desc(beam: dict) -> tuple[PbsBeamDesc, list]:
     d.sad = float(beam.get("sad", 0.0))
     d.ref_plane_z = float(beam.get("ref_plane_z", 0.0))
     put("roi_linear_indices", "roi_linear_indices", np.int32)
+    put("profile_energies", "profile_energies")
+    d.beam_para_pos = float(beam.get("beam_para_pos", 0.0))
     return d, keep
+
+
+def bio_desc(model: dict | None) -> tuple[PbsBioModel, list]:
+    """PbsBioModel from a dict: model ("lq" | "mkm" | None), let_table [rows][depths],
+    let_energies, let_depth0, let_depth_step, let_samples, est_dimension,
+    range_shifter, lq_alpha / lq_beta (LQ) or z1d (MKM) on the log10(LET) axis
+    lq_log0 + i * lq_log_step, alpha0, beta0."""
+    keep: list = []
+    m = PbsBioModel()
+    if not model or model.get("model") in (None, "off"):
+        m.model = PBS_BIO_OFF
+        return m, keep
+    m.model = {"lq": PBS_BIO_LQ, "mkm": PBS_BIO_MKM}[model["model"]]
+    let = np.ascontiguousarray(np.asarray(model["let_table"], np.float32))
+    if let.ndim != 2:
+        raise ValueError("let_table must be [rows][depths]")
+    keep.append(let)
+    m.let_table = let.ctypes.data_as(_FP)
+    m.let_rows, m.let_depths = int(let.shape[0]), int(let.shape[1])
+
+    def arr(key):
+        a = np.ascontiguousarray(np.asarray(model[key], np.float32).reshape(-1))
+        keep.append(a)
+        return a
+
+    e = arr("let_energies")
+    if e.size != m.let_rows:
+        raise ValueError("let_energies must have one entry per let_table row")
+    m.let_energies = e.ctypes.data_as(_FP)
+    m.let_depth0 = float(model.get("let_depth0", 0.0))
+    m.let_depth_step = float(model["let_depth_step"])
+    m.let_samples = int(model.get("let_samples", 5))
+    m.est_dimension = float(model.get("est_dimension", 0.0))
+    m.range_shifter = float(model.get("range_shifter", 0.0))
+    if m.model == PBS_BIO_LQ:
+        a, b = arr("lq_alpha"), arr("lq_beta")
+        if a.size != b.size:
+            raise ValueError("lq_alpha and lq_beta must have the same length")
+        m.lq_alpha, m.lq_beta, m.n_lq = a.ctypes.data_as(_FP), b.ctypes.data_as(_FP), int(a.size)
+    else:
+        z = arr("z1d")
+        m.z1d, m.n_lq = z.ctypes.data_as(_FP), int(z.size)
+    m.lq_log0 = float(model.get("lq_log0", 0.0))
+    m.lq_log_step = float(model.get("lq_log_step", 0.01))
+    m.alpha0 = float(model.get("alpha0", 0.0))
+    m.beta0 = float(model.get("beta0", 0.0))
+    return m, keep
 
 
 def energy_desc(energy: dict) -> tuple[PbsEnergyDesc, list]:

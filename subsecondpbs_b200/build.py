@@ -21,7 +21,7 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "libsubsecondpbs_b200.so"
 BUILD_DIR = PKG / "_build"
 
-CU_SOURCES = ["trace.cu", "conv.cu", "idd.cu", "superpose.cu", "transfer.cu", "context.cu", "peak.cu", "noalloc.cu", "adjoint.cu", "operator.cu"]
+CU_SOURCES = ["trace.cu", "conv.cu", "idd.cu", "superpose.cu", "transfer.cu", "context.cu", "peak.cu", "noalloc.cu", "adjoint.cu", "operator.cu", "bio.cu"]
 CXX_SOURCES = ["plan.cpp", "capi.cpp", "final_dose.cpp", "server.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -386,9 +386,11 @@ def build_carbonpbs_context(rayweq, roiIdx, all_energies, sourcePos, tmpBeamDir,
             if per_spot.size != int(counts.sum()):
                 raise RuntimeError("longitudal_cutoff length must match total spot count")
             beam["layer_longitudinal_cutoffs"] = _layer_cutoffs(per_spot, counts)
+    prof_rows = 0
     if profiledata is not None:
         prof = np.asarray(profiledata, dtype=np.float32)
         beam["profile_data"] = prof.reshape(-1)
+        prof_rows = int(prof.shape[0]) if prof.ndim >= 1 else 0
         depth_n = prof.shape[1] if prof.ndim >= 2 else 0
         if profilesetting is not None:
             ps = _floats(profilesetting).copy()
@@ -400,8 +402,15 @@ def build_carbonpbs_context(rayweq, roiIdx, all_energies, sourcePos, tmpBeamDir,
             beam["profile_setting"] = ps
     elif profilesetting is not None:
         beam["profile_setting"] = _floats(profilesetting)
+    # The profile rows' energy axis: the machine energy list, sliced to the row count
+    # when they differ (raytracedicom_pybind.cpp:1291-1294, RTD_PROFILE_SLICE_MODE).
+    beam["profile_energies"] = lut_energies
+    if prof_rows > 0 and lut_energies.size and prof_rows != lut_energies.size:
+        beam["profile_energies"] = _slice(lut_energies, prof_rows, _slice_mode("RTD_PROFILE_SLICE_MODE"))
     if beamparadata is not None:
         beam["beam_para_data"] = np.asarray(beamparadata, dtype=np.float32).reshape(-1)
+    if beamParaPos is not None:
+        beam["beam_para_pos"] = float(np.asarray(beamParaPos, dtype=np.float32).reshape(-1)[0])
     sub = np.asarray(subspotdata, dtype=np.float32)
     if sub.ndim != 3 or sub.shape[2] != 5:
         raise RuntimeError("subspotdata must have shape (num_layers, max_subspots_per_layer, 5)")
@@ -526,18 +535,52 @@ calcDose = cuFinalDose
 cuCalDose = cuFinalDose
 
 
+def _influence(ctx, gpu_id, nuclear):
+    """Dose-influence matrix of the export's spots on its (Nx, Ny, Nz) grid: scipy
+    CSC of shape (voxels, spots) with rows as x-major linear indices
+    (ix*Ny + iy)*Nz + iz, the CarbonPBS voxel order (deviceCalDose.cu:167-168)."""
+    import scipy.sparse as sp
+
+    from .cudaCalDoseRTD import DoseEngine
+
+    dims = ctx["dims"]
+    ct = _ct_for(dims, ctx["beam"]["roi_linear_indices"])
+    eng = DoseEngine(gpu_id)
+    try:
+        eng.set_energy(ctx["energy"])
+        eng.set_ct(ct.reshape(dims[2], dims[1], dims[0]), dims, ctx["resolution"], ctx["corner"])
+        eng.set_dose_grid(dims, ctx["resolution"], ctx["corner"])
+        a = eng.influence_csc(ctx["beam"], nuclear_correction=nuclear).tocoo()
+    finally:
+        eng.close()
+    nx, ny, nz = dims
+    v = a.row.astype(np.int64)
+    x, y, z = v % nx, (v // nx) % ny, v // (nx * ny)
+    rows = (x * ny + y) * nz + z
+    return sp.csc_matrix((a.data, (rows, a.col)), shape=a.shape)
+
+
 def cuCalDose3(out_cscdata, out_cscptr, out_cscrowind, weq_data, roi_index, source_energies, source, beam_dir,
                beam_xdir, beam_ydir, corner, resolution, dims, longitudal_cutoff, enelist, idddata, iddsetting,
                profiledata, profilesetting, beamparadata, subspot_data, layer_info, layer_energy, outNNZ, idbeamxy,
                num_particles_per_beam, cutoff, sad, beam_para_pos, python_nnz_size, gpu_id=0,
                nuclear_correction=False, verbose=0, tables_dir="tables/"):
-    """The reference's cuCalDose3 (raytracedicom_pybind.cpp:1955-2053): zeroes the
-    CSC outputs and nnz, computes the beam's dose into a new (Nx,Ny,Nz) grid and
-    returns {'dose_grid', 'out_cscdata', 'out_cscptr', 'out_cscrowind', 'outNNZ'}."""
+    """The reference's cuCalDose3 (raytracedicom_pybind.cpp:1955-2053) computes the
+    beam's dose into a new (Nx,Ny,Nz) grid and zeroes its sparse outputs; here the
+    sparse outputs carry the spot-preserving dose-influence matrix the operator mode
+    plans for (include/core/rtd_operator_mode.h:1-8), in the layout its CarbonPBS
+    caller reads (tps_py/dosecal.py:1520-1530): `out_cscdata` / `out_cscrowind` hold
+    the values and x-major voxel rows (ascending within a column), `out_cscptr[0]` = 0
+    and `out_cscptr[1 + j]` the entry count of spot j (the caller takes the cumulative
+    sum), `outNNZ[0]` the total. Columns are per unit spot weight (the matrix times
+    num_particles_per_beam is the dose). Entries that do not fit the arrays (their
+    capacity is their size) are not written; outNNZ still reports the total, as the
+    caller's retry loop expects. Returns {'dose_grid', 'out_cscdata', 'out_cscptr',
+    'out_cscrowind', 'outNNZ'}."""
     del cutoff, python_nnz_size
     for a in (out_cscdata, out_cscptr, out_cscrowind, outNNZ):
         if isinstance(a, np.ndarray) and a.size:
-            if a.dtype not in (np.float32, np.int32, np.uint64):
+            if a.dtype not in (np.float32, np.int32, np.int64, np.uint64):
                 raise RuntimeError("Unsupported dtype for zero fill")
             a[...] = 0
     d = [int(v) for v in np.asarray(dims).reshape(-1)]
@@ -550,5 +593,60 @@ def cuCalDose3(out_cscdata, out_cscptr, out_cscrowind, weq_data, roi_index, sour
                                   num_particles_per_beam, sad, beam_para_pos, tables_dir)
     ct = _ct_for(ctx["dims"], ctx["beam"]["roi_linear_indices"])
     _run(dose, ct, ctx, gpu_id, nuclear_correction, verbose)
+    a = _influence(ctx, gpu_id, nuclear_correction)
+    a.sort_indices()
+    nnz = int(a.nnz)
+    if isinstance(outNNZ, np.ndarray) and outNNZ.size:
+        outNNZ.reshape(-1)[0] = nnz
+    data, rowind, ptr = (np.asarray(v).reshape(-1) if isinstance(v, np.ndarray) else None
+                         for v in (out_cscdata, out_cscrowind, out_cscptr))
+    if ptr is not None and ptr.size >= a.shape[1] + 1:
+        ptr[0] = 0
+        ptr[1:a.shape[1] + 1] = np.diff(a.indptr)
+    if data is not None and rowind is not None and nnz <= min(data.size, rowind.size):
+        data[:nnz] = a.data
+        rowind[:nnz] = a.indices
     return {"dose_grid": dose, "out_cscdata": out_cscdata, "out_cscptr": out_cscptr, "out_cscrowind": out_cscrowind,
             "outNNZ": outNNZ}
+
+
+def cuCalDoseNorm(doseNorm, weqData, roiIndex, sourceEne, source, bmdir, bmxdir, bmydir, corner, resolution, dims,
+                  longitudalCutoff, enelist, idddata, iddsetting, profiledata, profilesetting, beamparadata,
+                  subSpotData, layerInfo, layerEnergy, idbeamxy, sad, cutoff, beamParaPos, gpuId=0,
+                  nuclear_correction=False, tables_dir="tables/"):
+    """CarbonPBS's cuCalDoseNorm (carbonPBS/cudaCalDose.cpp:347-500, registered at
+    :1975, called by tps_py/dosecal.py:1504): `doseNorm[i]` = sum over the spots of
+    the squared dose per unit spot weight at ROI voxel i (calDoseSumSquareKernel,
+    carbonPBS/deviceCalDose.cu:123-229), the row norms of the dose-influence matrix.
+    The ROI is given as in the other faces ((N,3), (3,N) or flat triplets, x-major
+    layout); computed on the device without forming the matrix
+    (pbs_context_influence_row_norms). Returns 1, the reference's success flag."""
+    del cutoff
+    from .cudaCalDoseRTD import DoseEngine
+
+    d = [int(v) for v in np.asarray(dims).reshape(-1)]
+    if len(d) != 3:
+        raise RuntimeError("dims must contain exactly 3 integers")
+    n_spots = np.asarray(idbeamxy).size // 2
+    ctx = build_carbonpbs_context(weqData, roiIndex, sourceEne, source, bmdir, bmxdir, bmydir, corner, resolution,
+                                  dims, longitudalCutoff, enelist, idddata, iddsetting, profiledata, profilesetting,
+                                  beamparadata, subSpotData, layerInfo, layerEnergy, idbeamxy,
+                                  np.ones(n_spots, np.float32), sad, beamParaPos, tables_dir)
+    roi = ctx["beam"]["roi_linear_indices"]
+    out = np.asarray(doseNorm).reshape(-1) if isinstance(doseNorm, np.ndarray) else None
+    if out is None or out.dtype != np.float32 or out.size != roi.size:
+        raise RuntimeError("doseNorm must be a float32 array with one entry per ROI voxel")
+    nx, ny, nz = d
+    ix, rem = roi // (ny * nz), roi % (ny * nz)
+    iy, iz = rem // nz, rem % nz
+    voxels = (iz.astype(np.int64) * ny + iy) * nx + ix
+    ct = _ct_for(d, roi)
+    eng = DoseEngine(gpuId)
+    try:
+        eng.set_energy(ctx["energy"])
+        eng.set_ct(ct.reshape(nz, ny, nx), d, ctx["resolution"], ctx["corner"])
+        eng.set_dose_grid(d, ctx["resolution"], ctx["corner"])
+        out[...] = eng.influence_row_norms(ctx["beam"], voxels=voxels, nuclear_correction=nuclear_correction)
+    finally:
+        eng.close()
+    return 1

@@ -176,6 +176,10 @@ int pbs_context_set_option(PbsContext* ctx, int option, long long value) {
             if (value < 0 || value > 2) break;
             ctx->impl.nuclearModel = int(value);
             return PBS_OK;
+        case PBS_OPT_CARBON_PROFILE:
+            if (value < 0 || value > 3) break;
+            ctx->impl.carbonProfile = int(value);
+            return PBS_OK;
         default: break;
     }
     pbs::set_error("unknown option or value");
@@ -245,6 +249,25 @@ int pbs_context_influence_csc(PbsContext* ctx, const PbsBeamDesc* beam, int nucl
     if (!beam) return PBS_ERR_INVALID_ARGUMENT;
     return ctx->impl.influence_csc(*beam, nuclear_correction, spot_begin, spot_count, threshold, col_ptr, rows, values,
                                    capacity, nnz);
+}
+
+int pbs_context_influence_row_norms(PbsContext* ctx, const PbsBeamDesc* beam, int nuclear_correction,
+                                    long long spot_begin, long long spot_count, const long long* voxels,
+                                    long long n_voxels, float* out) {
+    if (int rc = guard(ctx)) return rc;
+    if (!beam) return PBS_ERR_INVALID_ARGUMENT;
+    return ctx->impl.influence_row_norms(*beam, nuclear_correction, spot_begin, spot_count, voxels, n_voxels, out);
+}
+
+int pbs_context_set_bio_model(PbsContext* ctx, const PbsBioModel* model) {
+    if (int rc = guard(ctx)) return rc;
+    return ctx->impl.set_bio_model(model);
+}
+
+int pbs_context_read_bio_map(PbsContext* ctx, int map, float* out, int out_on_device) {
+    if (int rc = guard(ctx)) return rc;
+    if (!out) return PBS_ERR_INVALID_ARGUMENT;
+    return ctx->impl.read_bio_map(map, out, out_on_device);
 }
 
 int pbs_context_read_dose(PbsContext* ctx, float* out, int out_on_device) {
@@ -371,6 +394,9 @@ void subsecondWrapper(const float* ctData, const int3& ctDims, const float3& ctR
         d.ref_plane_z = s.refPlaneZ;
         d.roi_linear_indices = s.roiLinearIndices.data();
         d.n_roi_linear_indices = s.roiLinearIndices.size();
+        d.profile_energies = s.profileEnergies.data();
+        d.n_profile_energies = s.profileEnergies.size();
+        d.beam_para_pos = s.beamParaPos;
     }
     PbsEnergyDesc e{};
     if (energyData) {

@@ -134,6 +134,12 @@ int Context::init(int gpu) {
         const int m = std::atoi(v);
         if (m >= 0 && m <= 2) nuclearModel = m;
     }
+    // The CarbonPBS lateral profile model is off in the reference; the environment
+    // switches it on for the wrapper entry points (bits of PBS_OPT_CARBON_PROFILE).
+    if (const char* v = std::getenv("PBS_CARBON_PROFILE")) {
+        const int m = std::atoi(v);
+        if (m >= 0 && m <= 3) carbonProfile = m;
+    }
     int rc = errWord.ensure(sizeof(int));
     if (rc) return rc;
     PBS_CUDA(cudaMemset(errWord.ptr, 0, sizeof(int)), "cudaMemset");
@@ -572,9 +578,12 @@ int Context::reset_dose(const float* init, int onDevice) {
         PBS_CUDA(cudaEventRecord(doseCopied, copyStream), "cudaEventRecord");
         pendingDoseInit = true;
         doseBoxed = false;
-        return PBS_OK;
+        return bioModel ? clear_bio() : PBS_OK;
     }
     pendingDoseInit = false;
+    if (bioModel) {
+        if (int rc = clear_bio()) return rc;
+    }
     if (!init && doseBoxed && !doseExposed) {
         // Zero outside the dirty box already: clearing the box clears the grid. The
         // clear waits for the work on the context stream (the last readout) and
@@ -852,6 +861,11 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         set_error("nuclear_correction=true requires raw spot lattice inputs; legacy CPB fallback cannot drive halo mode");
         return PBS_ERR_UNSUPPORTED;
     }
+    if (bioModel && (nuclear || adj)) {
+        set_error(nuclear ? "biological maps: beams with the nuclear halo are not supported while a model is set"
+                          : "biological maps: clear the model (PBS_BIO_OFF) before the spot-weight adjoint");
+        return PBS_ERR_UNSUPPORTED;
+    }
     const BeamPlan& P = plan;
     BeamGeomDev& g = geom;
     std::memset(&g, 0, sizeof(g));
@@ -996,6 +1010,41 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         return PBS_ERR_OUT_OF_MEMORY;
     }
 
+    // Biological model: the layers' fractional rows on the LET table's energy axis.
+    const bool bio = bioModel != 0;
+    if (bio) {
+        std::vector<float> rows(L);
+        for (int l = 0; l < L; ++l)
+            rows[l] = find_fractional_index_monotonic(bioLetEnergies.data(), int(bioLetEnergies.size()),
+                                                      b.energies[l]);
+        const size_t bevN = S * size_t(g.bevX) * g.bevY;
+        const int nCh = bioModel == PBS_BIO_LQ ? 3 : 2;
+        if ((rc = bioLayerRow.ensure(size_t(L) * 4)) || (rc = bioIdd.ensure(z.idd)) ||
+            (rc = bioBev.ensure(size_t(nCh) * bevN * 4)))
+            return rc;
+        if ((rc = upload(bioLayerRow.ptr, rows.data(), size_t(L) * 4))) return rc;
+        PBS_CUDA(cudaMemsetAsync(bioBev.ptr, 0, size_t(nCh) * bevN * 4, stream), "memset bio BEV");
+    }
+
+    // CarbonPBS lateral profile model: which of its two parts this beam runs.
+    ProfilePlan prof;
+    if (carbonProfile) {
+        plan_carbon_profile(b, energy, P, prof);
+        if ((carbonProfile & 1) && prof.sigmaOverride()) g.profileMode |= 1;
+        if ((carbonProfile & 2) && prof.overallWeight()) g.profileMode |= 2;
+    }
+    const size_t profBytes = g.profileMode ? b.n_profile_data * 4 : 0;
+    if (profBytes) {
+        if ((rc = profileBuf.ensure(profBytes))) return rc;
+        g.profile = static_cast<const float*>(profileBuf.ptr);
+        g.profileRows = prof.rows;
+        g.profileDepthN = prof.depthN;
+        g.profileChannels = prof.channels;
+        g.profileDepth0 = prof.depth0;
+        g.profileDepthStep = prof.depthStep;
+        g.beamParaPos = b.beam_para_pos;
+    }
+
     // Host -> device inputs of the beam: layer parameters, initial beam state and
     // the fluence source (dense spot lattice or legacy subspot table).
     std::vector<LayerParamsDev> hlp(L);
@@ -1012,6 +1061,12 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         d.sigmaXmm = H.sigmaXmm;
         d.sigmaYmm = H.sigmaYmm;
         d.spotDist = H.spotDist;
+        if (g.profileMode) {
+            d.profileRow = prof.row[l];
+            d.bp0 = prof.bp0[l];
+            d.bp1 = prof.bp1[l];
+            d.bp2 = prof.bp2[l];
+        }
         // With the halo the lattice spacing is taken as mm when the beam gives no
         // explicit spot spacing (wrapper.cu:4333-4347).
         if (nuclear && std::fabs(P.fanDelta.x) > 1e-6f) {
@@ -1028,8 +1083,8 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     const size_t latBytes = P.hasLattice ? P.lattice.weights.size() * 4 : 0;
     const size_t subBytes = P.hasLattice ? 0 : b.n_subspot_data * 4;
     const size_t nucMapBytes = nuclear ? hRayToNuc.size() * 4 : 0;
-    const size_t upBytes =
-        hlp.size() * sizeof(LayerParamsDev) + 2 * sizeof(BeamStateDev) + latBytes + subBytes + nucMapBytes;
+    const size_t upBytes = hlp.size() * sizeof(LayerParamsDev) + 2 * sizeof(BeamStateDev) + latBytes + subBytes +
+                           nucMapBytes + profBytes;
     {
         PBS_CUDA(cudaEventSynchronize(stagingEvent), "cudaEventSynchronize");
         if ((rc = staging.ensure(upBytes + 256))) return rc;
@@ -1062,7 +1117,13 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             PBS_CUDA(cudaMemsetAsync(nucLs.ptr, 0, size_t(L) * sizeof(LayerStateDev), stream), "memset");
             PBS_CUDA(cudaMemsetAsync(nucBev.ptr, 0, S * nucGeom.bevX * nucGeom.bevY * 4, stream), "memset");
         }
+        if (profBytes) {
+            std::memcpy(p, b.profile_data, profBytes);
+            PBS_CUDA(cudaMemcpyAsync(profileBuf.ptr, p, profBytes, cudaMemcpyHostToDevice, stream), "H2D");
+            p += profBytes;
+        }
         PBS_CUDA(cudaEventRecord(stagingEvent, stream), "cudaEventRecord");
+        copiedH2D += upBytes;
     }
 
     LayerParamsDev* dlp = static_cast<LayerParamsDev*>(lp.ptr);
@@ -1100,6 +1161,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         if ((rc = weqBody.ensure(weqN * 4))) return rc;
         PBS_CUDA(cudaMemcpyAsync(weqBody.ptr, b.water_equivalence + 9, weqN * 4, cudaMemcpyHostToDevice, stream),
                  "WEQ H2D");
+        copiedH2D += weqN * 4;
         PBS_CUDA(launch_weq_trace(g, static_cast<const float*>(weqBody.ptr), P.weqNx, P.weqNy, P.weqSteps,
                                   P.weqActiveSteps, P.weqStepMm, P.cpbCorner.x, P.cpbCorner.y, P.cpbRes.x, P.cpbRes.y,
                                   P.weqX0, P.weqY0, P.weqDx, P.weqDy, dDens, dWepl, dFi, dFo, trace.weplMin, dbs,
@@ -1169,6 +1231,26 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             PBS_CUDA(launch_superpose(nucGeom, dNucIdd, dNucRs, static_cast<const int4*>(nucWork.ptr), dNucBs,
                                       static_cast<float*>(nucBev.ptr), smCount, stream),
                      "nuc_superpose");
+        if (bio) {
+            // Every biological channel: the IDD scaled by the channel's factor,
+            // superposed with the same radii and work list into its own BEV volume.
+            const size_t bevN = S * size_t(g.bevX) * g.bevY;
+            const int channels[3] = {0, 1, 2};
+            int slot = 0;
+            for (int c : channels) {
+                if (c == 1 && bioModel != PBS_BIO_LQ) continue;
+                PBS_CUDA(launch_bio_channel(g, bioDev, l0, nl, static_cast<const float*>(iddBuf.ptr), dWepl, dls, dbs,
+                                            static_cast<const float*>(bioLayerRow.ptr), c,
+                                            static_cast<float*>(bioIdd.ptr), stream),
+                         "bio_channel");
+                PBS_CUDA(launch_reset_work_claims(dbs, stream), "reset work claims");
+                PBS_CUDA(launch_superpose(g, static_cast<const float*>(bioIdd.ptr),
+                                          static_cast<const float*>(rsBuf.ptr), static_cast<const int4*>(work.ptr),
+                                          dbs, static_cast<float*>(bioBev.ptr) + size_t(slot) * bevN, smCount, stream),
+                         "bio_superpose");
+                ++slot;
+            }
+        }
     }
     if ((rc = mark(6))) return rc;
     if (adj) return finish_adjoint(*adj, b);
@@ -1186,6 +1268,21 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     }
     PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
     PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
+    if (bio) {
+        // The beam's own dose and the channels into the biological accumulators.
+        const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+        const size_t bevN = S * size_t(g.bevX) * g.bevY;
+        double* acc = static_cast<double*>(bioAcc.ptr);
+        PBS_CUDA(launch_transfer(g, dBev, dbs, acc, stream), "bio transfer");
+        const int nCh = bioModel == PBS_BIO_LQ ? 3 : 2;
+        for (int slot = 0; slot < nCh; ++slot) {
+            // Slots are channels 0, 1, 2 (LQ) or 0, 2 (MKM); accumulator c + 1.
+            const int c = bioModel == PBS_BIO_LQ ? slot : (slot == 0 ? 0 : 2);
+            PBS_CUDA(launch_transfer(g, static_cast<const float*>(bioBev.ptr) + size_t(slot) * bevN, dbs,
+                                     acc + size_t(c + 1) * n, stream),
+                     "bio transfer");
+        }
+    }
     if (nuclear) {
         PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, stream), "nuc_transfer_planner");
         PBS_CUDA(launch_transfer(nucGeom, static_cast<const float*>(nucBev.ptr), dNucBs,
@@ -1199,6 +1296,9 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     // adds seven per chunk (clear, codes, layer plan, scatter, three superposition
     // ranges) and its transfer planner and transfer.
     lastLaunches = 6 + 6 * lastChunks + (nuclear ? 7 * lastChunks + 2 : 0);
+    // The biological channels: per chunk and channel, the scaling, a claim reset and
+    // four superposition ranges; then one transfer per accumulator.
+    if (bio) lastLaunches += (bioModel == PBS_BIO_LQ ? 3 : 2) * 6 * lastChunks + (bioModel == PBS_BIO_LQ ? 4 : 3);
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;
@@ -1669,5 +1769,102 @@ int wrapper_body(Context* ctx, const float* ctData, const GridDesc& cg, float* d
 }
 
 }  // namespace
+
+// ---- biological maps -----------------------------------------------------
+
+int Context::clear_bio() {
+    if (!hasDose) return PBS_OK;
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    if (int rc = bioAcc.ensure(4 * n * sizeof(double))) return rc;
+    PBS_CUDA(cudaMemsetAsync(bioAcc.ptr, 0, 4 * n * sizeof(double), stream), "memset bio accumulators");
+    return PBS_OK;
+}
+
+int Context::set_bio_model(const PbsBioModel* m) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!m || m->model == PBS_BIO_OFF) {
+        bioModel = 0;
+        return PBS_OK;
+    }
+    const bool lq = m->model == PBS_BIO_LQ, mkm = m->model == PBS_BIO_MKM;
+    if (!lq && !mkm) {
+        set_error("biological maps: unknown model");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (!m->let_table || !m->let_energies || m->let_rows <= 0 || m->let_depths <= 0 || !(m->let_depth_step > 0.0f) ||
+        m->let_samples <= 0 || m->n_lq <= 0 || !(m->lq_log_step > 0.0f) ||
+        (lq && (!m->lq_alpha || !m->lq_beta)) || (mkm && (!m->z1d || !(m->beta0 > 0.0f)))) {
+        set_error("biological maps: missing or empty table, or a non-positive axis step");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    for (int r = 1; r < m->let_rows; ++r)
+        if (!(m->let_energies[r] > m->let_energies[r - 1])) {
+            set_error("biological maps: let_energies must ascend");
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+    const size_t nLet = size_t(m->let_rows) * m->let_depths, nLq = size_t(m->n_lq);
+    std::vector<float> host(nLet + 2 * nLq);
+    std::memcpy(host.data(), m->let_table, nLet * 4);
+    if (lq) {
+        std::memcpy(host.data() + nLet, m->lq_alpha, nLq * 4);
+        std::memcpy(host.data() + nLet + nLq, m->lq_beta, nLq * 4);
+    } else {
+        std::memcpy(host.data() + nLet, m->z1d, nLq * 4);
+    }
+    if (int rc = bioTables.ensure(host.size() * 4)) return rc;
+    if (int rc = upload(bioTables.ptr, host.data(), host.size() * 4)) return rc;
+    const float* t = static_cast<const float*>(bioTables.ptr);
+    BioDev& d = bioDev;
+    d = BioDev{};
+    d.model = m->model;
+    d.letTable = t;
+    d.letRows = m->let_rows;
+    d.letDepths = m->let_depths;
+    d.letDepth0 = m->let_depth0;
+    d.letDepthStep = m->let_depth_step;
+    d.letSamples = m->let_samples;
+    d.estDimension = m->est_dimension;
+    d.rangeShifter = m->range_shifter;
+    d.alpha = lq ? t + nLet : nullptr;
+    d.beta = lq ? t + nLet + nLq : nullptr;
+    d.z1d = mkm ? t + nLet : nullptr;
+    d.nLq = m->n_lq;
+    d.lqLog0 = m->lq_log0;
+    d.lqLogStep = m->lq_log_step;
+    d.alpha0 = m->alpha0;
+    d.beta0 = m->beta0;
+    bioLetEnergies.assign(m->let_energies, m->let_energies + m->let_rows);
+    bioModel = m->model;
+    return clear_bio();
+}
+
+int Context::read_bio_map(int map, float* out, int onDevice) {
+    PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (!bioModel) {
+        set_error("biological maps: no model set");
+        return PBS_ERR_NOT_READY;
+    }
+    if (!hasDose) {
+        set_error("dose grid not set");
+        return PBS_ERR_NOT_READY;
+    }
+    if (map < PBS_BIO_MAP_DOSE || map > PBS_BIO_MAP_Z1D ||
+        ((map == PBS_BIO_MAP_ALPHA || map == PBS_BIO_MAP_BETA) && bioModel != PBS_BIO_LQ) ||
+        (map == PBS_BIO_MAP_Z1D && bioModel != PBS_BIO_MKM)) {
+        set_error("biological maps: unknown map, or a map of the other model");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    if (int rc = join_side_work()) return rc;
+    const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    if (int rc = floatOut.ensure(n * 4)) return rc;
+    const double* acc = static_cast<const double*>(bioAcc.ptr);
+    float* dst = onDevice ? out : static_cast<float*>(floatOut.ptr);
+    PBS_CUDA(launch_bio_map(acc, acc + n, acc + 2 * n, acc + 3 * n, n, bioDev, map, dst, stream), "bio_map");
+    if (onDevice) return PBS_OK;
+    PBS_CUDA(cudaMemcpyAsync(out, floatOut.ptr, n * 4, cudaMemcpyDeviceToHost, stream), "bio map D2H");
+    copiedD2H += n * 4;
+    PBS_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    return take_device_errors();
+}
 
 }  // namespace pbs

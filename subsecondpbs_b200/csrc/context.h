@@ -111,6 +111,7 @@ struct Context {
     int ctInputType = PBS_CT_AUTO;
     long long layerBudgetMiB = 2048;
     int nuclearModel = 2;  // GAUSS_FIT
+    int carbonProfile = 0; // PBS_OPT_CARBON_PROFILE bits
     int smCount = 0;       // multiprocessors of the device, read on first use
 
     // Lookup tables.
@@ -120,6 +121,19 @@ struct Context {
     std::vector<float> nucWeightHost, nucSqSigmaHost;
     bool nucTablesAligned = false;
     DevBuf cidd, density, sp, rrl, nucWeight, nucSqSigma;
+    DevBuf profileBuf;     // the beam's CarbonPBS profile table
+
+    // Biological model (pbs_context_set_bio_model): tables on the device, the
+    // layer rows of the current beam, the scaled IDD of one channel, the channels'
+    // BEV volumes and the FP64 accumulators [4][Z][Y][X] (dose, dose x factor 0,
+    // 1, 2) of the beams added since the last dose reset.
+    int bioModel = 0;
+    BioDev bioDev{};
+    std::vector<float> bioLetEnergies;
+    DevBuf bioTables, bioLayerRow, bioIdd, bioBev, bioAcc;
+    int set_bio_model(const PbsBioModel* m);
+    int read_bio_map(int map, float* out, int onDevice);
+    int clear_bio();
     LutsDev luts{};
 
     // CT (HU+1000) and dose accumulator.
@@ -150,7 +164,7 @@ struct Context {
     // Adjoint working set, and the imported water-equivalence volume of a beam.
     DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice, weqBody;
     // Influence export: column offsets, per-block offsets, and the entries.
-    DevBuf opColPtr, opBlockOff, opRows, opVals;
+    DevBuf opColPtr, opBlockOff, opRows, opVals, opNorm, opVoxels;
     PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
@@ -228,6 +242,23 @@ struct Context {
     // order, values = dose per unit spot weight with |value| > threshold. Entries
     // past `capacity` are counted in *nnz but not copied (PBS_ERR_INVALID_ARGUMENT).
     // Leaves the dose accumulator zeroed.
+    // Row norms of the influence matrix of spots [spotBegin, spotBegin + spotCount):
+    // sum over the spots of each voxel's squared dose per unit weight, at the
+    // voxels listed (linear indices) or, with voxels == nullptr, the whole grid.
+    int influence_row_norms(const PbsBeamDesc& b, int nuclear, long long spotBegin, long long spotCount,
+                            const long long* voxels, long long nVoxels, float* out);
+    // Shared by the influence exports: the beam planned once at unit weights and
+    // each spot's lattice cells; run_column computes one spot's dose (box: OpBox).
+    struct ColumnPlan {
+        std::vector<float> unit;
+        PbsBeamDesc beam{};
+        BeamPlan base;
+        std::vector<int> cells;
+        std::vector<float> shares;
+    };
+    int plan_columns(const PbsBeamDesc& b, long long spotBegin, long long spotCount, const char* what,
+                     ColumnPlan& cp);
+    int run_column(ColumnPlan& cp, size_t spot, int nuclear, void* box);
     int influence_csc(const PbsBeamDesc& b, int nuclear, long long spotBegin, long long spotCount, double threshold,
                       long long* colPtr, int* rows, float* vals, long long capacity, long long* nnz);
     int beam_stats(PbsBeamStats* out);

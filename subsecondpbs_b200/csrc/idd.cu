@@ -31,7 +31,23 @@ constexpr int kMaxChunkLayers = 64;
 // turns the eight warp partials of every step into the tile's radius bucket
 // (tileRadCalc, complete_superposition.cu:198-255), stores the code and adds the
 // tile's bucket counts to the layer histogram.
-template <bool kNuclear>
+// Profile table value of channel c at a fractional depth and row index, both
+// already clamped to the table: the linear filter of the reference's profile
+// texture (wrapper.cu:2858-2860, unnormalised coordinates at texel centres) with
+// exact weights.
+__device__ __forceinline__ float profile_sample(const float* __restrict__ t, int depthN, int channels, int rows,
+                                                int c, float depth, float row) {
+    const float fd = floorf(depth), fr = floorf(row);
+    const int d0 = int(fd), r0 = int(fr);
+    const int d1 = min(d0 + 1, depthN - 1), r1 = min(r0 + 1, rows - 1);
+    const float ad = depth - fd, ar = row - fr;
+    auto at = [&](int r, int d) { return __ldg(t + (static_cast<size_t>(r) * depthN + d) * channels + c); };
+    const float a0 = at(r0, d0), a1 = at(r0, d1), b0 = at(r1, d0), b1 = at(r1, d1);
+    const float lo = a0 + (a1 - a0) * ad, hi = b0 + (b1 - b0) * ad;
+    return lo + (hi - lo) * ar;
+}
+
+template <bool kNuclear, bool kProfile>
 __global__ void __launch_bounds__(256)
 idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ density,
            const float* __restrict__ wepl, const int* __restrict__ firstInside, const int* __restrict__ firstOutside,
@@ -176,6 +192,9 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         float rSigmaEff = __int_as_float(0x7f800000);
         float nucRes = 0.0f;
         float nucRSigmaEff = __int_as_float(0x7f800000);
+        // WEPL of this step for the profile model (the reference reads the traced
+        // value of every step, live or not).
+        const float nextProfileSp = kProfile && real ? wepl[static_cast<size_t>(stepNo) * rayPlane + ridx] : 0.0f;
         if (live) {
             const float cumulSp = nextSp;
             const float dens = nextDens;
@@ -227,6 +246,53 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
             rSigmaEff = __int_as_float(0x7f800000);
             nucRes = 0.0f;
             nucRSigmaEff = __int_as_float(0x7f800000);
+        }
+        if (kProfile && real) {
+            // CarbonPBS lateral profile model on the filled step, in the reference's
+            // order: the sigma override (overrideRSigmaFromCarbonProfileKernel,
+            // wrapper.cu:2080-2152), then the overall weight
+            // (applyCarbonProfileOverallWeightKernel, wrapper.cu:2154-2187).
+            const int nGauss = (g.profileChannels - 1) / 2;
+            const float depthIdx = (nextProfileSp - g.profileDepth0) / g.profileDepthStep;
+            const float dIdx = fminf(fmaxf(depthIdx, 0.0f), float(g.profileDepthN - 1));
+            const float rIdx = p.profileRow;
+            if (g.profileMode & 1) {
+                if (!(res > 0.0f)) {
+                    rSigmaEff = __int_as_float(0x7f800000);
+                } else {
+                    float sumW = 0.0f, sumS2 = 0.0f;
+                    for (int gi = 0; gi < nGauss; ++gi) {
+                        const float w = profile_sample(g.profile, g.profileDepthN, g.profileChannels, g.profileRows,
+                                                       gi, dIdx, rIdx);
+                        const float sr = profile_sample(g.profile, g.profileDepthN, g.profileChannels, g.profileRows,
+                                                        gi + nGauss, dIdx, rIdx);
+                        sumW += w;
+                        sumS2 += w * sr * sr;
+                    }
+                    if (!(sumW > 1.0e-8f)) {
+                        rSigmaEff = __int_as_float(0x7f800000);
+                    } else {
+                        // CarbonPBS geometric depth: distance from the virtual source along
+                        // this divergent ray minus the source-to-beam-parameter distance.
+                        const float sad = 0.5f * (g.sourceDist.x + g.sourceDist.y);
+                        const float fanX = g.fanCorner.x + float(x) * g.fanDelta.x;
+                        const float fanY = g.fanCorner.y + float(y) * g.fanDelta.y;
+                        const float fanZ = g.fanCorner.z + float(stepNo) * g.fanDelta.z;
+                        const float proj = (sad - fanZ) * sqrtf(1.0f + (fanX * fanX) / (g.sourceDist.x * g.sourceDist.x) +
+                                                                (fanY * fanY) / (g.sourceDist.y * g.sourceDist.y));
+                        const float phy = proj - (sad - g.beamParaPos);
+                        const float initR2 = p.bp0 + 2.0f * p.bp1 * phy + p.bp2 * phy * phy;
+                        const float axisSq = 0.5f * fmaxf(0.0f, initR2 + sumS2 / sumW);
+                        const float axis = sqrtf(fmaxf(0.0f, axisSq));
+                        rSigmaEff = 0.5f * stepNum[stepNo] / (kSqrt2 * (axis + 0.21f));
+                    }
+                }
+            }
+            if ((g.profileMode & 2) && res > 0.0f) {
+                const float ow = profile_sample(g.profile, g.profileDepthN, g.profileChannels, g.profileRows,
+                                                g.profileChannels - 1, dIdx, rIdx);
+                res *= fmaxf(0.0f, ow);
+            }
         }
         const int zr = stepNo - first;
         const size_t o = static_cast<size_t>(zr) * padPlane + static_cast<size_t>(y) * g.pitchX + x;
@@ -316,12 +382,12 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     __shared__ int sCalc[kMaxChunkLayers];
     __shared__ int sWarpSum[kMaxChunkLayers / 32];
     __shared__ long long sWarpFma[kMaxChunkLayers / 32];
-    __shared__ int sSplit[2];
+    __shared__ int sSplit[3];
     const int lc = threadIdx.x;
     const bool nuclear = primaryLs != nullptr;
     const int first = nuclear ? primaryBeam->firstInside : beam->firstInside;
     const int tiles = g.tilesX * g.tilesY;
-    if (lc < 2) sSplit[lc] = 0;
+    if (lc < 3) sSplit[lc] = 0;
     if (lc < nLayers) {
         LayerStateDev& st = ls[layer0 + lc];
         int hist[kBuckets];
@@ -409,11 +475,13 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     __syncthreads();
     int acc = incl - runSum;
     for (int w = 0; w < warp; ++w) acc += sWarpSum[w];
-    const int pSplit = (kMaxR - kSplitR) * nLayers, pSplit2 = (kMaxR - kSplitR2) * nLayers;
+    const int pSplit = (kMaxR - kSplitR) * nLayers, pSplit2 = (kMaxR - kSplitR2) * nLayers,
+              pSplit3 = (kMaxR - kSplitR3) * nLayers;
     for (int p = p0; p < p1; ++p) {
         const int r = kMaxR - p / nLayers, q = p % nLayers;
         if (p == pSplit) sSplit[0] = acc;
         if (p == pSplit2) sSplit[1] = acc;
+        if (p == pSplit3) sSplit[2] = acc;
         ls[layer0 + q].offR[r] = acc;
         acc += sLive[q][r];
     }
@@ -430,7 +498,7 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
             acc += sWarpSum[w];
             fma += sWarpFma[w];
         }
-        const int split = sSplit[0], split2 = sSplit[1];
+        const int split = sSplit[0], split2 = sSplit[1], split3 = sSplit[2];
         int mp = beam->maxCalcPassive;
         for (int q = 0; q < nLayers; ++q) mp = max(mp, sCalc[q]);
         beam->maxCalcPassive = mp;
@@ -444,6 +512,8 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         beam->workNextSmall = 0;
         beam->workSplit2 = min(split2, acc);
         beam->workNextTiny = 0;
+        beam->workSplit3 = min(split3, acc);
+        beam->workNextMid = 0;
         beam->liveTiles += acc;
         beam->superposeFma += fma;
     }
@@ -553,7 +623,8 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
     dim3 grid(g.tilesX, g.tilesY, nLayers);
     dim3 block(32, 8);
     const size_t smem = idd_smem_bytes(g, luts);
-    auto k = g.nucOn ? idd_kernel<true> : idd_kernel<false>;
+    auto k = g.nucOn ? (g.profileMode ? idd_kernel<true, true> : idd_kernel<true, false>)
+                     : (g.profileMode ? idd_kernel<false, true> : idd_kernel<false, false>);
     cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<grid, block, smem, s>>>(g, luts, layer0, density, wepl, firstInside, firstOutside, rayW, lp, ls, beam, idd,

@@ -122,4 +122,13 @@ cudaError_t launch_dose_to_float(const double* dose, float* out, size_t n, cudaS
 cudaError_t launch_dose_box(double* dose, float* out, const int dims[3], const int lo[3], const int hi[3],
                             cudaStream_t s);
 
+// Biological maps (bio.cu).
+cudaError_t launch_bio_channel(const BeamGeomDev& g, const BioDev& m, int layer0, int nLayers, const float* idd,
+                               const float* wepl, const LayerStateDev* ls, const BeamStateDev* beam,
+                               const float* layerRow, int channel, float* out, cudaStream_t s);
+cudaError_t launch_bio_map(const double* dose, const double* c0, const double* c1, const double* c2, size_t n,
+                           const BioDev& m, int map, float* out, cudaStream_t s);
+// Resets the superposition work list's claim counters so that the list can be run again.
+cudaError_t launch_reset_work_claims(BeamStateDev* beam, cudaStream_t s);
+
 }  // namespace pbs

@@ -143,6 +143,27 @@ int op_cuda(cudaError_t e, const char* where) {
     return e == cudaErrorMemoryAllocation ? PBS_ERR_OUT_OF_MEMORY : PBS_ERR_CUDA;
 }
 
+// Row norms of the influence matrix: the squared dose of one column added to the
+// FP64 norm grid over the column's dirty box.
+__global__ void __launch_bounds__(kOpThreads) row_norm_add_kernel(const double* __restrict__ dose, OpBox a,
+                                                                  double* __restrict__ norm) {
+    for (long long b = blockIdx.x * static_cast<long long>(kOpThreads) + threadIdx.x; b < a.n;
+         b += static_cast<long long>(gridDim.x) * kOpThreads) {
+        const long long g = box_to_grid(a, b);
+        const double v = dose[g];
+        norm[g] += v * v;
+    }
+}
+
+// Float copy of the norm grid at the requested voxels (all voxels when null).
+__global__ void __launch_bounds__(kOpThreads) row_norm_gather_kernel(const double* __restrict__ norm,
+                                                                     const long long* __restrict__ voxels,
+                                                                     long long n, float* __restrict__ out) {
+    for (long long i = blockIdx.x * static_cast<long long>(kOpThreads) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * kOpThreads)
+        out[i] = float(norm[voxels ? voxels[i] : i]);
+}
+
 }  // namespace
 
 // rtd_operator_mode.h:43-111: the same validation (an invalid beam returns the
@@ -203,32 +224,156 @@ int operator_batch_plan(const PbsBeamDesc& beam, int maxSpotsPerBatch, OperatorP
     return PBS_OK;
 }
 
-int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotBegin, long long spotCount,
-                           double threshold, long long* colPtrHost, int* rowsHost, float* valsHost,
-                           long long capacity, long long* nnzOut) {
+// Validation and the one plan shared by every column of an influence export.
+int Context::plan_columns(const PbsBeamDesc& beam, long long spotBegin, long long spotCount, const char* what,
+                          ColumnPlan& cp) {
     if (int rc = op_cuda(cudaSetDevice(device), "cudaSetDevice")) return rc;
     if (!hasDose) {
         set_error("dose grid not set");
         return PBS_ERR_NOT_READY;
     }
+    const std::string tag = std::string(what) + ": ";
     if (!beam.layer_spot_counts || beam.n_layer_spot_counts == 0) {
-        set_error("influence export: the beam has no layer spot counts");
+        set_error(tag + "the beam has no layer spot counts");
         return PBS_ERR_INVALID_ARGUMENT;
     }
     long long nSpots = 0;
     for (size_t l = 0; l < beam.n_layer_spot_counts; ++l) {
         if (beam.layer_spot_counts[l] < 0) {
-            set_error("influence export: negative layer spot count");
+            set_error(tag + "negative layer spot count");
             return PBS_ERR_INVALID_ARGUMENT;
         }
         nSpots += beam.layer_spot_counts[l];
     }
     if (spotBegin < 0 || spotCount < 0 || spotBegin > nSpots || spotCount > nSpots - spotBegin ||
         spotCount > INT_MAX - 1) {
-        set_error("influence export: spot range of " + std::to_string(spotCount) + " spots from " +
-                  std::to_string(spotBegin) + " lies outside the beam's " + std::to_string(nSpots) + " spots");
+        set_error(tag + "spot range of " + std::to_string(spotCount) + " spots from " + std::to_string(spotBegin) +
+                  " lies outside the beam's " + std::to_string(nSpots) + " spots");
         return PBS_ERR_INVALID_ARGUMENT;
     }
+    // One plan for every column. The beam geometry, ray grid and spot lattice do not
+    // depend on the weights, so the plan is made once with every spot at unit weight
+    // and a column only replaces the lattice weights by its spot's shares. A beam
+    // without a raw spot lattice would fall back to the legacy CPB fluence, which
+    // reads the subspot table and ignores per-spot weights: it has no columns.
+    cp.unit.assign(static_cast<size_t>(nSpots), 1.0f);
+    cp.beam = beam;
+    cp.beam.spot_weights = cp.unit.data();
+    cp.beam.n_spot_weights = cp.unit.size();
+    {
+        std::string err;
+        if (int rc = plan_beam(cp.beam, energy, ctGrid, doseGrid, cp.base, err)) {
+            set_error(tag + err);
+            return rc;
+        }
+    }
+    if (!cp.base.hasLattice) {
+        set_error(tag + "needs a beam with a raw spot lattice (spot positions, weights and layer counts on one "
+                        "lattice phase); the legacy CPB fluence it would fall back to ignores per-spot weights" +
+                  (cp.base.lattice.failure.empty() ? std::string() : " (" + cp.base.lattice.failure + ")"));
+        return PBS_ERR_UNSUPPORTED;
+    }
+    if (!lattice_spot_cells(cp.beam, cp.base.lattice, cp.cells, cp.shares)) {
+        set_error(tag + "failed to map the spots onto the beam's lattice");
+        return PBS_ERR_GEOMETRY;
+    }
+    return PBS_OK;
+}
+
+// Dose of spot j alone at unit weight into the (zeroed) FP64 grid, with the box of
+// voxels it can have written.
+int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut) {
+    BeamPlan P = cp.base;
+    std::fill(P.lattice.weights.begin(), P.lattice.weights.end(), 0.0f);
+    for (int slot = 0; slot < 4; ++slot) {
+        const int c = cp.cells[j * 4 + slot];
+        if (c >= 0) P.lattice.weights[static_cast<size_t>(c)] += cp.shares[j * 4 + slot];
+    }
+    if (int rc = reset_dose(nullptr, 0)) return rc;
+    if (int rc = add_planned_beam(cp.beam, nuclear, std::move(P))) return rc;
+    if (int rc = join_side_work()) return rc;
+    OpBox& a = *static_cast<OpBox*>(boxOut);
+    int lo[3], hi[3];
+    for (int i = 0; i < 3; ++i) {
+        const bool boxed = doseBoxed && !doseExposed;
+        lo[i] = boxed ? dirtyLo[i] : 0;
+        hi[i] = boxed ? dirtyHi[i] : doseGrid.dims[i] - 1;
+    }
+    const bool empty = hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2];
+    for (int i = 0; i < 3; ++i) {
+        a.lo[i] = lo[i];
+        a.ext[i] = empty ? 0 : hi[i] - lo[i] + 1;
+    }
+    a.X = doseGrid.dims[0];
+    a.Y = doseGrid.dims[1];
+    a.n = empty ? 0 : static_cast<long long>(a.ext[0]) * a.ext[1] * a.ext[2];
+    return PBS_OK;
+}
+
+int Context::influence_row_norms(const PbsBeamDesc& beam, int nuclear, long long spotBegin, long long spotCount,
+                                 const long long* voxelsHost, long long nVoxels, float* outHost) {
+    const long long gridN = hasDose ? static_cast<long long>(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2]
+                                    : 0;
+    if (!outHost || nVoxels < 0 || (nVoxels > 0 && !voxelsHost)) {
+        set_error("influence row norms: null output or negative voxel count");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
+    for (long long i = 0; i < nVoxels; ++i)
+        if (voxelsHost[i] < 0 || voxelsHost[i] >= gridN) {
+            set_error("influence row norms: voxel index " + std::to_string(voxelsHost[i]) + " outside the dose grid");
+            return PBS_ERR_INVALID_ARGUMENT;
+        }
+    ColumnPlan cp;
+    if (int rc = plan_columns(beam, spotBegin, spotCount, "influence row norms", cp)) return rc;
+    auto fail = [&](int rc) {
+        const std::string msg = last_error();
+        reset_dose(nullptr, 0);
+        set_error(msg);
+        return rc;
+    };
+    const long long nOut = voxelsHost ? nVoxels : gridN;
+    if (int rc = opNorm.ensure(static_cast<size_t>(gridN) * sizeof(double))) return fail(rc);
+    if (int rc = opVals.ensure(static_cast<size_t>(std::max(nOut, 1LL)) * sizeof(float))) return fail(rc);
+    if (voxelsHost && nVoxels > 0) {
+        if (int rc = opVoxels.ensure(static_cast<size_t>(nVoxels) * sizeof(long long))) return fail(rc);
+        if (int rc = upload(opVoxels.ptr, voxelsHost, static_cast<size_t>(nVoxels) * sizeof(long long)))
+            return fail(rc);
+    }
+    double* norm = static_cast<double*>(opNorm.ptr);
+    if (int rc = op_cuda(cudaMemsetAsync(norm, 0, static_cast<size_t>(gridN) * sizeof(double), stream),
+                         "row norm clear"))
+        return fail(rc);
+    const double* d = static_cast<const double*>(dose64.ptr);
+    for (long long k = 0; k < spotCount; ++k) {
+        OpBox a{};
+        if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a)) return fail(rc);
+        if (a.n > 0) {
+            const int blocks = static_cast<int>(std::min<long long>((a.n + kOpThreads - 1) / kOpThreads, 148 * 8));
+            row_norm_add_kernel<<<blocks, kOpThreads, 0, stream>>>(d, a, norm);
+        }
+        if (int rc = op_cuda(cudaGetLastError(), "row norm kernel")) return fail(rc);
+    }
+    if (nOut > 0) {
+        const int blocks = static_cast<int>(std::min<long long>((nOut + kOpThreads - 1) / kOpThreads, 148 * 8));
+        row_norm_gather_kernel<<<blocks, kOpThreads, 0, stream>>>(
+            norm, voxelsHost ? static_cast<const long long*>(opVoxels.ptr) : nullptr, nOut,
+            static_cast<float*>(opVals.ptr));
+        if (int rc = op_cuda(cudaGetLastError(), "row norm gather")) return fail(rc);
+        if (int rc = op_cuda(cudaMemcpyAsync(outHost, opVals.ptr, static_cast<size_t>(nOut) * sizeof(float),
+                                             cudaMemcpyDeviceToHost, stream),
+                             "row norms D2H"))
+            return fail(rc);
+        copiedD2H += static_cast<unsigned long long>(nOut) * sizeof(float);
+    }
+    if (int rc = op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return fail(rc);
+    if (int rc = take_device_errors()) return fail(rc);
+    if (int rc = reset_dose(nullptr, 0)) return rc;
+    return op_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+}
+
+int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotBegin, long long spotCount,
+                           double threshold, long long* colPtrHost, int* rowsHost, float* valsHost,
+                           long long capacity, long long* nnzOut) {
     if (!(threshold >= 0.0) || !std::isfinite(threshold)) {
         set_error("influence export: the threshold must be finite and >= 0");
         return PBS_ERR_INVALID_ARGUMENT;
@@ -237,41 +382,14 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         set_error("influence export: null output or negative capacity");
         return PBS_ERR_INVALID_ARGUMENT;
     }
-    const long long gridN = static_cast<long long>(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+    const long long gridN =
+        hasDose ? static_cast<long long>(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2] : 0;
     if (gridN > INT_MAX) {
         set_error("influence export: the dose grid has more voxels than an int32 row index holds");
         return PBS_ERR_UNSUPPORTED;
     }
-
-    // One plan for every column. The beam geometry, ray grid and spot lattice do not
-    // depend on the weights, so the plan is made once with every spot at unit weight
-    // and a column only replaces the lattice weights by its spot's shares. A beam
-    // without a raw spot lattice would fall back to the legacy CPB fluence, which
-    // reads the subspot table and ignores per-spot weights: it has no columns.
-    std::vector<float> unit(static_cast<size_t>(nSpots), 1.0f);
-    PbsBeamDesc one = beam;
-    one.spot_weights = unit.data();
-    one.n_spot_weights = unit.size();
-    BeamPlan base;
-    {
-        std::string err;
-        if (int rc = plan_beam(one, energy, ctGrid, doseGrid, base, err)) {
-            set_error("influence export: " + err);
-            return rc;
-        }
-    }
-    if (!base.hasLattice) {
-        set_error("influence export: needs a beam with a raw spot lattice (spot positions, weights and layer counts "
-                  "on one lattice phase); the legacy CPB fluence it would fall back to ignores per-spot weights" +
-                  (base.lattice.failure.empty() ? std::string() : " (" + base.lattice.failure + ")"));
-        return PBS_ERR_UNSUPPORTED;
-    }
-    std::vector<int> cells;
-    std::vector<float> shares;
-    if (!lattice_spot_cells(one, base.lattice, cells, shares)) {
-        set_error("influence export: failed to map the spots onto the beam's lattice");
-        return PBS_ERR_GEOMETRY;
-    }
+    ColumnPlan cp;
+    if (int rc = plan_columns(beam, spotBegin, spotCount, "influence export", cp)) return rc;
 
     // Any failure below leaves the dose grid zeroed, as a finished export does.
     auto fail = [&](int rc) {
@@ -295,31 +413,8 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         return fail(rc);
 
     for (long long k = 0; k < spotCount; ++k) {
-        const size_t j = static_cast<size_t>(spotBegin + k);
-        BeamPlan P = base;
-        std::fill(P.lattice.weights.begin(), P.lattice.weights.end(), 0.0f);
-        for (int slot = 0; slot < 4; ++slot) {
-            const int c = cells[j * 4 + slot];
-            if (c >= 0) P.lattice.weights[static_cast<size_t>(c)] += shares[j * 4 + slot];
-        }
-        if (int rc = reset_dose(nullptr, 0)) return fail(rc);
-        if (int rc = add_planned_beam(one, nuclear, std::move(P))) return fail(rc);
-        if (int rc = join_side_work()) return fail(rc);
         OpBox a{};
-        int lo[3], hi[3];
-        for (int i = 0; i < 3; ++i) {
-            const bool boxed = doseBoxed && !doseExposed;
-            lo[i] = boxed ? dirtyLo[i] : 0;
-            hi[i] = boxed ? dirtyHi[i] : doseGrid.dims[i] - 1;
-        }
-        const bool empty = hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2];
-        for (int i = 0; i < 3; ++i) {
-            a.lo[i] = lo[i];
-            a.ext[i] = empty ? 0 : hi[i] - lo[i] + 1;
-        }
-        a.X = doseGrid.dims[0];
-        a.Y = doseGrid.dims[1];
-        a.n = empty ? 0 : static_cast<long long>(a.ext[0]) * a.ext[1] * a.ext[2];
+        if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a)) return fail(rc);
         const int nBlocks = static_cast<int>((a.n + kOpChunk - 1) / kOpChunk);
         const double* d = static_cast<const double*>(dose64.ptr);
         if (nBlocks > 0) influence_count_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, threshold, dBlockOff);

@@ -22,6 +22,10 @@ struct LayerParamsDev {
     float sigmaXmm;
     float sigmaYmm;
     float spotDist;
+    // CarbonPBS lateral profile model: fractional table row and beam parameters
+    // (2 sigmaIso^2, rtheta, theta^2) of the layer (wrapper.cu:4577-4606).
+    float profileRow;
+    float bp0, bp1, bp2;
 };
 
 // Per-layer values produced on the device.
@@ -53,13 +57,16 @@ struct BeamStateDev {
     int maxCalcPassive;
     int workCount;          // superposition work items of the current layer chunk
     // The radius-sorted work list holds the wide (R > kSplitR), medium
-    // (kSplitR2 < R <= kSplitR) and narrow (R <= kSplitR2) items in that order;
-    // each range has its own claim counter (relative to the range start).
+    // (kSplitR3 < R <= kSplitR), medium-narrow (kSplitR2 < R <= kSplitR3) and
+    // narrow (R <= kSplitR2) items in that order; each range has its own claim
+    // counter (relative to the range start).
     int workNext;
     int workSplit;          // items with R > kSplitR
     int workNextSmall;
     int workSplit2;         // items with R > kSplitR2
     int workNextTiny;
+    int workSplit3;         // items with R > kSplitR3
+    int workNextMid;
     long long liveTiles;
     long long superposeFma;
     int transferStart[3];
@@ -101,6 +108,30 @@ struct BeamGeomDev {
     int nucOn;
     int nucX, nucY;
     int* errWord;
+    // CarbonPBS lateral profile model (PBS_OPT_CARBON_PROFILE bits active for this
+    // beam): table [rows][depthN][channels], its depth axis and the beam-parameter
+    // position (raytracedicom_integration.h:71-76).
+    int profileMode;
+    const float* profile;
+    int profileRows, profileDepthN, profileChannels;
+    float profileDepth0, profileDepthStep;
+    float beamParaPos;
+};
+
+// Biological model tables resident on the device (PbsBioModel of subsecondpbs.h).
+struct BioDev {
+    int model;
+    const float* letTable;  // [letRows][letDepths]
+    int letRows, letDepths;
+    float letDepth0, letDepthStep;
+    int letSamples;
+    float estDimension, rangeShifter;
+    const float* alpha;     // [nLq] (LQ)
+    const float* beta;      // [nLq] (LQ)
+    const float* z1d;       // [nLq] (MKM)
+    int nLq;
+    float lqLog0, lqLogStep;
+    float alpha0, beta0;
 };
 
 // Lookup tables resident on the device.

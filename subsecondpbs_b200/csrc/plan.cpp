@@ -531,6 +531,72 @@ float find_fractional_index_monotonic(const float* v, int n, float value) {
     return static_cast<float>(lo) + t;
 }
 
+// ---- CarbonPBS lateral profile model ----------------------------------------
+
+void plan_carbon_profile(const PbsBeamDesc& b, const PbsEnergyDesc& e, const BeamPlan& P, ProfilePlan& out) {
+    out = ProfilePlan{};
+    const int L = P.numLayers;
+    const size_t nData = b.profile_data ? b.n_profile_data : 0;
+    const size_t nPara = b.beam_para_data ? b.n_beam_para_data : 0;
+    const size_t nProfE = b.profile_energies ? b.n_profile_energies : 0;
+    out.beamPara = nPara >= size_t(L) * 3u;
+    const bool model = b.profile_setting && b.n_profile_setting >= 3 &&
+                       std::lround(b.profile_setting[2]) > 0 && nData > 0;
+    if (model) {
+        out.depth0 = b.profile_setting[0];
+        out.depthStep = b.profile_setting[1];
+        out.depthN = std::max(1, static_cast<int>(std::lround(b.profile_setting[2])));
+        const size_t plane = size_t(out.depthN);
+        const int paraRows = static_cast<int>(nPara / 3u);
+        // The row count: beam-parameter rows, else the profile energy axis, else the
+        // layers, else a 11-channel export (wrapper.cu:2830-2849).
+        if (paraRows > 0 && nPara == size_t(paraRows) * 3u && nData % (size_t(paraRows) * plane) == 0)
+            out.rows = paraRows;
+        else if (nProfE > 0 && nData % (nProfE * plane) == 0)
+            out.rows = static_cast<int>(nProfE);
+        else if (L > 0 && nData % (size_t(L) * plane) == 0)
+            out.rows = L;
+        else if (nData % plane == 0 && (nData / plane) % 11u == 0)
+            out.rows = static_cast<int>((nData / plane) / 11u);
+        const size_t perRow = out.rows > 0 ? nData / size_t(out.rows) : 0;
+        if (out.rows > 0 && perRow >= plane) {
+            out.channels = static_cast<int>(perRow / plane);
+            out.table = out.channels > 0 && size_t(out.rows) * plane * size_t(out.channels) == nData;
+        }
+    }
+    out.row.assign(L, 0.0f);
+    out.bp0.assign(L, 0.0f);
+    out.bp1.assign(L, 0.0f);
+    out.bp2.assign(L, 0.0f);
+    const int lastRow = std::max(0, out.rows - 1);
+    for (int l = 0; l < L; ++l) {
+        const float energy = b.energies[l];
+        float r;
+        if (out.rows == L)
+            r = float(l);
+        else if (nProfE > 0 && out.rows == static_cast<int>(nProfE))
+            r = find_fractional_index_monotonic(b.profile_energies, static_cast<int>(nProfE), energy);
+        else if (out.rows == e.n_energies && e.energies_per_u && e.n_energies_per_u > 0)
+            r = std::fmin(std::fmax(P.layers[l].energyIdx, 0.0f), float(out.rows - 1));
+        else
+            r = std::fmin(std::fmax(float(l), 0.0f), float(lastRow));
+        r = std::fmin(std::fmax(r, 0.0f), float(lastRow));
+        out.row[l] = r;
+        // interpBeamParaCoeff (wrapper.cu:4592-4603).
+        if (out.rows > 0 && nPara >= size_t(out.rows) * 3u) {
+            const float c = std::fmin(std::fmax(r, 0.0f), float(out.rows - 1));
+            const int i0 = std::max(0, std::min(out.rows - 1, static_cast<int>(std::floor(c))));
+            const int i1 = std::max(0, std::min(out.rows - 1, i0 + 1));
+            const float t = c - float(i0);
+            float* dst[3] = {&out.bp0[l], &out.bp1[l], &out.bp2[l]};
+            for (int k = 0; k < 3; ++k) {
+                const float v0 = b.beam_para_data[size_t(i0) * 3u + k], v1 = b.beam_para_data[size_t(i1) * 3u + k];
+                *dst[k] = v0 + (v1 - v0) * t;
+            }
+        }
+    }
+}
+
 // ---- validation -------------------------------------------------------------
 
 bool validate_global(const float* ct, const GridDesc& ctGrid, const void* dose, const GridDesc& doseGrid,

@@ -81,6 +81,25 @@ struct BeamPlan {
     float weqX0 = 0.f, weqY0 = 0.f, weqDx = 0.f, weqDy = 0.f;
 };
 
+// CarbonPBS lateral profile model of one beam: the table shape the reference infers
+// from profile_setting / profile_data / beam_para_data (wrapper.cu:2816-2862) and,
+// per layer, the fractional table row and the interpolated beam parameters
+// (wrapper.cu:4577-4606).
+struct ProfilePlan {
+    bool table = false;          // profile_data has the inferred [rows][depthN][channels] shape
+    bool beamPara = false;       // beam_para_data holds at least 3 values per layer
+    int rows = 0, depthN = 0, channels = 0;
+    float depth0 = 0.f, depthStep = 0.f;
+    std::vector<float> row, bp0, bp1, bp2;  // per layer
+    // What the reference's two switches would run on this beam (wrapper.cu:4656-4660,
+    // 4814-4818) and their kernels' own early returns (wrapper.cu:2103-2104, 2171).
+    bool sigmaOverride() const {
+        return table && beamPara && depthN > 0 && channels >= 3 && (channels - 1) / 2 > 0 && depthStep > 0.0f;
+    }
+    bool overallWeight() const { return table && depthN > 0 && channels > 0 && depthStep > 0.0f; }
+};
+void plan_carbon_profile(const PbsBeamDesc& b, const PbsEnergyDesc& e, const BeamPlan& P, ProfilePlan& out);
+
 // wrapper.cu:1025-1075 (+ the LUT sample counts the textures are built with).
 bool validate_global(const float* ct, const GridDesc& ctGrid, const void* dose, const GridDesc& doseGrid,
                      const PbsBeamDesc* beams, size_t numBeams, const PbsEnergyDesc* e, std::string& err);

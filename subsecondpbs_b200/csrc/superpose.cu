@@ -44,6 +44,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+// Resident CTAs per SM of the paired instances (radii 12..15, 8..11, 0..7).
+constexpr int kMidBlocks = 2;
+constexpr int kMidNarrowBlocks = 3;
+constexpr int kNarrowBlocks = 4;
+constexpr int kPairs = kTileX / 2;                 // column pairs per tile row
+constexpr int kPairSlots = kTileY * kPairs;        // (row, pair) slots per tile
 
 template <int RMax>
 struct Shape {
@@ -53,6 +59,24 @@ struct Shape {
     static constexpr size_t kSmemBytes =
         (size_t(kQ) * kThreads * 4 + size_t(kThreads) * kEWStride + kOutFloats) * sizeof(float);
 };
+
+// Paired layout (instances with radii up to kSplitR): the sources of source columns
+// 2p and 2p+1 (a column pair p) are stored interleaved, so that one 16-byte load
+// gives e(k) and e(k+1) of both columns as two register pairs and one 8-byte load
+// gives idd * e(d) of both; the accumulation then runs on packed FP32x2 FMAs, one
+// instruction per footprint row for the two columns.
+template <int RMax>
+struct PairShape {
+    static constexpr int kQ2 = (RMax + 2) / 2;                // float4 = (e_a(k), e_b(k), e_a(k+1), e_b(k+1))
+    static constexpr int kEW2 = (RMax + 1) | 1;               // float2 stride per (row, pair), odd
+    static constexpr int kOutInts = (kTileY + 2 * RMax) * (kTileX + 2 * RMax);
+    static constexpr size_t kSmemBytes =
+        size_t(kQ2) * kPairSlots * 16 + size_t(kPairSlots) * kEW2 * 8 + size_t(kOutInts) * 4;
+};
+
+// Slot of column pair p (0..15) within a source row: pairs 8 apart, read together by
+// the lane groups of one instruction, land in different banks.
+__device__ __forceinline__ int pair_slot(int p) { return p ^ ((p >> 3) & 1); }
 
 // Column part of the slot of source (sy, sx) in the chunk-major e_s table
 // (slot = sy * 32 + e4_col(sx)): the low bits are XORed with bits 3..4 so that
@@ -223,12 +247,148 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
     }
 }
 
+// Paired variant of superpose_tile for radii up to kSplitR. A lane is one column
+// distance |d| of one column pair (2p, 2p+1): it keeps both columns' footprint
+// heights as register pairs and adds (idd_a e_a(d), idd_b e_b(d)) * (e_a(k), e_b(k))
+// to rows sy+R+-k with one packed FP32x2 FMA per row. The table phase, fixed-point
+// flush and write-out are those of superpose_tile.
+template <int R, int RMax>
+__device__ __forceinline__ void superpose_tile_paired(float4* __restrict__ E2, float2* __restrict__ EW2,
+                                                      int* __restrict__ out, unsigned* __restrict__ sCol,
+                                                      float* __restrict__ sSum, const TileArgs& a) {
+    constexpr int H = kTileY + 2 * R;
+    constexpr int Wo = kTileX + 2 * R;
+    constexpr int Q2 = (R + 2) / 2;
+    constexpr int EWS = PairShape<RMax>::kEW2;
+    const int t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31;
+
+    // ---- table phase (complete_superposition.cu:298-307) --------------------
+    {
+        const float dose = a.idd[a.src];
+        const bool live = dose > 0.0f;
+        if (live) atomicOr(&sCol[lane], 1u << warp);
+        float rowDose = live ? dose : 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
+        if (lane == 0) sSum[warp] = rowDose;
+        float e[R + 1];
+        if (live) {
+            superposition_row<R>(a.rsig[a.src], e);
+        } else {
+#pragma unroll
+            for (int k = 0; k <= R; ++k) e[k] = 0.0f;
+        }
+        // This source is half h of column pair p: its e(k) goes to component
+        // (k & 1) * 2 + h of float4 k / 2 of its (row, pair) slot, its idd * e(k) to
+        // component h of float2 k of its (row, pair) row.
+        const int pr = lane >> 1, h = lane & 1;
+        float* e2 = reinterpret_cast<float*>(E2 + warp * kPairs + pair_slot(pr)) + h;
+        float* ew = reinterpret_cast<float*>(EW2 + (warp * kPairs + pr) * EWS) + h;
+#pragma unroll
+        for (int k = 0; k <= R; ++k) {
+            e2[(k >> 1) * kPairSlots * 4 + (k & 1) * 2] = e[k];
+            ew[2 * k] = dose * e[k];
+        }
+        if ((R & 1) == 0) e2[(R >> 1) * kPairSlots * 4 + 2] = 0.0f;  // k = R + 1 of the last float4
+        // H and Wo are even and `out` is 16-byte aligned.
+        for (int i = t; i < H * Wo / 4; i += kThreads) reinterpret_cast<int4*>(out)[i] = make_int4(0, 0, 0, 0);
+    }
+    __syncthreads();
+
+    // Fixed-point scale: 2^(30 - ex) with total < 2^ex, so total * scale < 2^30.
+    float total = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) total += sSum[w];
+    int ex;
+    frexpf(total, &ex);
+    const float scale = ldexpf(1.0f, min(30 - ex, 126));
+    const float invScale = 1.0f / scale;
+
+    // ---- accumulation phase --------------------------------------------------
+    {
+        constexpr int M = R + 1;                         // distances |d| per column pair
+        constexpr int G = (32 / M) < kPairs ? (32 / M) : kPairs;  // column pairs per instruction
+        constexpr int S = (kPairs + G - 1) / G;          // pair spacing = units per tile
+        const unsigned colBits = sCol[lane];
+#pragma unroll 1
+        for (int u = warp; u < S; u += kWarps) {
+            const int g = lane / M;
+            int d = lane - g * M;
+            int pr = u + g * S;
+            const bool valid = g < G && pr < kPairs;
+            if (!valid) {
+                pr = 0;
+                d = 0;
+            }
+            const unsigned colA = __shfl_sync(0xffffffffu, colBits, 2 * pr);
+            const unsigned colB = __shfl_sync(0xffffffffu, colBits, 2 * pr + 1);
+            const bool liveA = valid && colA != 0u, liveB = valid && colB != 0u;
+            if (!__any_sync(0xffffffffu, liveA || liveB)) continue;
+            // Lanes outside the footprint read pair 0 and are never flushed.
+            const float2* ewCol = EW2 + pr * EWS + d;
+            const float4* eCol = E2 + pair_slot(pr);
+            float2 acc[H];
+#pragma unroll
+            for (int i = 0; i < H; ++i) acc[i] = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int sy = 0; sy < kTileY; ++sy) {
+                const float2 w = ewCol[sy * kPairs * EWS];
+#pragma unroll
+                for (int q = 0; q < Q2; ++q) {
+                    const float4 v = eCol[q * kPairSlots + sy * kPairs];
+                    const float2 ev[2] = {make_float2(v.x, v.y), make_float2(v.z, v.w)};
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int k = 2 * q + c;
+                        if (k <= R) {
+                            acc[sy + R + k] = __ffma2_rn(w, ev[c], acc[sy + R + k]);
+                            if (k > 0) acc[sy + R - k] = __ffma2_rn(w, ev[c], acc[sy + R - k]);
+                        }
+                    }
+                }
+                if (sy & 1) asm volatile("" ::: "memory");
+            }
+            if (liveA) {
+                int* col = out + 2 * pr + R + d;
+#pragma unroll
+                for (int i = 0; i < H; ++i) {
+                    const int q = __float2int_rn(acc[i].x * scale);
+                    atomicAdd(col + i * Wo, q);
+                    if (d > 0) atomicAdd(col - 2 * d + i * Wo, q);
+                }
+            }
+            if (liveB) {
+                int* col = out + 2 * pr + 1 + R + d;
+#pragma unroll
+                for (int i = 0; i < H; ++i) {
+                    const int q = __float2int_rn(acc[i].y * scale);
+                    atomicAdd(col + i * Wo, q);
+                    if (d > 0) atomicAdd(col - 2 * d + i * Wo, q);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- write-out -------------------------------------------------------------
+    if (t < kTileX) sCol[t] = 0;
+    for (int i = t; i < H * Wo; i += kThreads) {
+        const int q = out[i];
+        const int oy = i / Wo, ox = i - oy * Wo;
+        if (q != 0) atomicAdd(a.dst + static_cast<size_t>(oy) * a.bevX + ox, float(q) * invScale);
+    }
+}
+
 // Chain of compile-time radii RLo..RHi; returns false if r is outside it.
 template <int R, int RHi, int RMax>
 __device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, int* out, unsigned* sCol,
                                                 float* sSum, const TileArgs& a) {
     if (r == R) {
-        superpose_tile<R, RMax>(E4, EW, out, sCol, sSum, a);
+        if constexpr (RMax <= kSplitR)
+            superpose_tile_paired<R, RMax>(E4, reinterpret_cast<float2*>(EW), out, sCol, sSum, a);
+        else
+            superpose_tile<R, RMax>(E4, EW, out, sCol, sSum, a);
         return true;
     }
     if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sCol, sSum, a);
@@ -243,18 +403,35 @@ __global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
                  const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev, int range) {
     extern __shared__ __align__(16) float sm[];
-    float4* E4 = reinterpret_cast<float4*>(sm);                                  // [Q][256] e_s(4q..4q+3), slot sy*32+e4_col(sx)
-    float* EW = sm + Shape<RHi>::kQ * kThreads * 4;                              // [256][EWS] idd_s e_s(k)
-    int* out = reinterpret_cast<int*>(EW + kThreads * Shape<RHi>::kEWStride);   // [8+2R][32+2R] fixed-point footprint
+    constexpr bool kPaired = RHi <= kSplitR;
+    // Wide radii: E4 = [Q][256] e_s(4q..4q+3) at slot sy*32+e4_col(sx), EW = [256][EWS]
+    // idd_s e_s(k). Paired radii: E4 = [Q2][128] pair float4s at slot sy*16+pair_slot(p),
+    // EW = [128][EW2] float2 (idd_a e_a(k), idd_b e_b(k)). Then the [8+2R][32+2R]
+    // fixed-point footprint.
+    constexpr size_t kE4Floats = kPaired ? size_t(PairShape<RHi>::kQ2) * kPairSlots * 4
+                                         : size_t(Shape<RHi>::kQ) * kThreads * 4;
+    constexpr size_t kEWFloats = kPaired ? size_t(kPairSlots) * PairShape<RHi>::kEW2 * 2
+                                         : size_t(kThreads) * Shape<RHi>::kEWStride;
+    float4* E4 = reinterpret_cast<float4*>(sm);
+    float* EW = sm + kE4Floats;
+    int* out = reinterpret_cast<int*>(EW + kEWFloats);
     __shared__ int sItem[2];
     __shared__ unsigned sCol[kTileX];     // per source column: depositing sources over sy
     __shared__ float sSum[kTileY];
 
     const int t = threadIdx.x;
-    // Range 0: R > kSplitR, 1: kSplitR2 < R <= kSplitR, 2: R <= kSplitR2.
-    const int begin = range == 0 ? 0 : (range == 1 ? beam->workSplit : beam->workSplit2);
-    const int end = range == 0 ? beam->workSplit : (range == 1 ? beam->workSplit2 : beam->workCount);
-    int* counter = range == 0 ? &beam->workNext : (range == 1 ? &beam->workNextSmall : &beam->workNextTiny);
+    // Range 0: R > kSplitR, 1: kSplitR3 < R <= kSplitR, 3: kSplitR2 < R <= kSplitR3,
+    // 2: R <= kSplitR2 (the work list holds them in the order 0, 1, 3, 2).
+    int begin, end, *counter;
+    if (range == 0) {
+        begin = 0, end = beam->workSplit, counter = &beam->workNext;
+    } else if (range == 1) {
+        begin = beam->workSplit, end = beam->workSplit3, counter = &beam->workNextSmall;
+    } else if (range == 3) {
+        begin = beam->workSplit3, end = beam->workSplit2, counter = &beam->workNextMid;
+    } else {
+        begin = beam->workSplit2, end = beam->workCount, counter = &beam->workNextTiny;
+    }
     const size_t padPlane = static_cast<size_t>(g.pitchX) * g.pitchY;
     const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
     const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
@@ -293,7 +470,7 @@ template <int RLo, int RHi, int MinBlocks>
 cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                          BeamStateDev* beam, float* bev, int gridBlocks, int range, cudaStream_t s) {
     auto k = superpose_kernel<RLo, RHi, MinBlocks>;
-    const size_t smem = Shape<RHi>::kSmemBytes;
+    const size_t smem = RHi <= kSplitR ? PairShape<RHi>::kSmemBytes : Shape<RHi>::kSmemBytes;
     cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, range);
@@ -307,9 +484,12 @@ cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float
     // Items are sorted by descending radius: the wide radii come first.
     cudaError_t e = launch_range<kSplitR + 1, kMaxR, 2>(g, idd, rsigma, work, beam, bev, numSMs * 2, 0, s);
     if (e != cudaSuccess) return e;
-    e = launch_range<kSplitR2 + 1, kSplitR, 5>(g, idd, rsigma, work, beam, bev, numSMs * 5, 1, s);
+    e = launch_range<kSplitR3 + 1, kSplitR, kMidBlocks>(g, idd, rsigma, work, beam, bev, numSMs * kMidBlocks, 1, s);
     if (e != cudaSuccess) return e;
-    return launch_range<0, kSplitR2, 8>(g, idd, rsigma, work, beam, bev, numSMs * 8, 2, s);
+    e = launch_range<kSplitR2 + 1, kSplitR3, kMidNarrowBlocks>(g, idd, rsigma, work, beam, bev,
+                                                                numSMs * kMidNarrowBlocks, 3, s);
+    if (e != cudaSuccess) return e;
+    return launch_range<0, kSplitR2, kNarrowBlocks>(g, idd, rsigma, work, beam, bev, numSMs * kNarrowBlocks, 2, s);
 }
 
 }  // namespace pbs

@@ -80,8 +80,13 @@ __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam) {
 // primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44). The reference launches
 // ceil(width/32) x ceil(height/8) blocks from the box start, so columns up to the
 // next block boundary inside the dose grid are transferred too. Every voxel is
-// independent, so the z range of a column is split across blockIdx.z.
+// independent: the box (known only on the device) is cut into items of one dose
+// column (x, y) and kTransferZChunk consecutive z, x fastest so that a warp's FP64
+// read-modify-writes are coalesced, and a persistent grid strides over the items.
+// The chunk's voxels are sampled with independent loads (unrolled loop), so the
+// latency of the BEV samples and of the dose reads overlaps.
 constexpr int kTransferZChunk = 8;
+constexpr int kTransferBlocksPerSM = 8;
 
 __global__ void __launch_bounds__(256)
 transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, const BeamStateDev* __restrict__ beam,
@@ -89,23 +94,37 @@ transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, const BeamStateDev
     if (!beam->transferValid) return;
     const int sx = beam->transferStart[0], sy = beam->transferStart[1], sz = beam->transferStart[2];
     const int mx = beam->transferMax[0], my = beam->transferMax[1], mz = beam->transferMax[2];
-    const int spanX = ((mx - sx + 1 + 31) / 32) * 32, spanY = ((my - sy + 1 + 7) / 8) * 8;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x < sx || y < sy || x >= sx + spanX || y >= sy + spanY || x >= g.doseX || y >= g.doseY) return;
-    const int z0 = max(sz, int(blockIdx.z) * kTransferZChunk);
-    const int z1 = min(mz, int(blockIdx.z) * kTransferZChunk + kTransferZChunk - 1);
-    if (z0 > z1) return;
+    // Columns of the launch box that lie inside the dose grid.
+    const int nx = min(((mx - sx + 1 + 31) / 32) * 32, g.doseX - sx);
+    const int ny = min(((my - sy + 1 + 7) / 8) * 8, g.doseY - sy);
+    const int nzc = (mz - sz + kTransferZChunk) / kTransferZChunk;
+    if (nx <= 0 || ny <= 0 || nzc <= 0) return;
+    const long long items = static_cast<long long>(nx) * ny * nzc;
     const TransferParams T = beam->transfer;
-    const V3 start = transfer_start(T, x, y);
     const float zShift = g.compatBevZShift ? float(beam->firstInside) : 0.0f;
     const size_t slice = static_cast<size_t>(g.doseX) * g.doseY;
-    double* col = dose + static_cast<size_t>(y) * g.doseX + x;
-    for (int z = z0; z <= z1; ++z) {
-        const V3 f = transfer_fan_idx(T, start, z);
-        if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
-        const float v = bev_sample(bev, g.bevX, g.bevY, g.steps, f.x, f.y, f.z - zShift);
-        if (v > 0.0f) col[z * slice] += double(v);
+    for (long long it = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = sx + static_cast<int>(it % nx);
+        const long long r = it / nx;
+        const int y = sy + static_cast<int>(r % ny);
+        const int z0 = sz + static_cast<int>(r / ny) * kTransferZChunk;
+        const V3 start = transfer_start(T, x, y);
+        double* col = dose + static_cast<size_t>(y) * g.doseX + x;
+        float v[kTransferZChunk];
+#pragma unroll
+        for (int k = 0; k < kTransferZChunk; ++k) {
+            const int z = z0 + k;
+            v[k] = 0.0f;
+            if (z <= mz) {
+                const V3 f = transfer_fan_idx(T, start, z);
+                if (!(f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f))
+                    v[k] = bev_sample(bev, g.bevX, g.bevY, g.steps, f.x, f.y, f.z - zShift);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kTransferZChunk; ++k)
+            if (v[k] > 0.0f) col[static_cast<size_t>(z0 + k) * slice] += double(v[k]);
     }
 }
 
@@ -145,9 +164,13 @@ cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cu
 
 cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,
                             cudaStream_t s) {
-    dim3 block(32, 8);
-    dim3 grid((g.doseX + 31) / 32, (g.doseY + 7) / 8, (g.doseZ + kTransferZChunk - 1) / kTransferZChunk);
-    transfer_kernel<<<grid, block, 0, s>>>(g, bev, beam, dose);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // No more CTAs than the whole grid could need (small grids).
+    const long long cap = ((static_cast<long long>(g.doseX) * g.doseY) * ((g.doseZ + kTransferZChunk - 1) / kTransferZChunk) +
+                           255) / 256;
+    const int blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(cap, sms * kTransferBlocksPerSM)));
+    transfer_kernel<<<blocks, 256, 0, s>>>(g, bev, beam, dose);
     return cudaGetLastError();
 }
 

@@ -91,7 +91,7 @@ class DoseEngine:
 
     def __init__(self, gpu_id: int = 0, compat_bev_z_shift: bool = False, stage_timing: bool = False,
                  keep_debug: bool = False, layer_budget_mib: int | None = None, ct_input_type: int | None = None,
-                 nuclear_model: int | None = None):
+                 nuclear_model: int | None = None, carbon_profile: int = 0):
         self._lib = _lib.load()
         h = C.c_void_p()
         _lib.check(self._lib.pbs_context_create(int(gpu_id), C.byref(h)))
@@ -106,6 +106,8 @@ class DoseEngine:
             self.set_option(_lib.PBS_OPT_CT_INPUT_TYPE, int(ct_input_type))
         if nuclear_model is not None:
             self.set_option(_lib.PBS_OPT_NUCLEAR_MODEL, int(nuclear_model))
+        if carbon_profile:
+            self.set_option(_lib.PBS_OPT_CARBON_PROFILE, int(carbon_profile))
         self.dose_dims = None
 
     def close(self) -> None:
@@ -168,6 +170,51 @@ class DoseEngine:
         _lib.check(self._lib.pbs_context_adjoint_beam(self._h, C.byref(bd), ptr, on_dev,
                                                       out.ctypes.data_as(C.POINTER(C.c_float)), n_spots))
         del keep, gkeep
+        return out
+
+    def set_bio_model(self, model: dict | None) -> None:
+        """Biological model for the maps on top of the dose (see _lib.bio_desc for
+        the dict); None clears it. The accumulators restart at zero."""
+        m, keep = _lib.bio_desc(model)
+        _lib.check(self._lib.pbs_context_set_bio_model(self._h, C.byref(m)))
+        del keep
+
+    def read_bio_map(self, name: str, out=None) -> np.ndarray:
+        """One biological map ('dose', 'letd', 'rbe', 'rbe_dose', 'alpha', 'beta',
+        'z1d') as float32 [Z][Y][X]; a CUDA float32 tensor `out` is filled on the
+        device instead."""
+        code = _lib.BIO_MAPS[name]
+        if out is not None and hasattr(out, "data_ptr"):
+            _lib.check(self._lib.pbs_context_read_bio_map(self._h, code, C.c_void_p(out.data_ptr()), 1))
+            return out
+        dd = self.dose_dims
+        res = np.empty((dd[2], dd[1], dd[0]), np.float32)
+        _lib.check(self._lib.pbs_context_read_bio_map(self._h, code, res.ctypes.data_as(C.c_void_p), 0))
+        return res
+
+    def influence_row_norms(self, beam, voxels=None, spot_begin: int = 0, spot_count: int | None = None,
+                            nuclear_correction: bool = False) -> np.ndarray:
+        """Row norms of the dose-influence matrix (CarbonPBS cuCalDoseNorm): for each
+        voxel the sum over the spots of its squared dose per unit spot weight.
+        `voxels` are linear indices (z*Y + y)*X + x (float32 [n] result); without
+        them the result is the whole grid, float32 [Z][Y][X]. The context's dose
+        accumulator is left at zero."""
+        bd, keep = beam if isinstance(beam, tuple) else _lib.beam_desc(beam)
+        n_spots = int(sum(bd.layer_spot_counts[i] for i in range(bd.n_layer_spot_counts)))
+        if spot_count is None:
+            spot_count = n_spots - int(spot_begin)
+        if voxels is None:
+            dd = self.dose_dims
+            out = np.empty((dd[2], dd[1], dd[0]), np.float32)
+            vptr, nv = None, 0
+        else:
+            vox = np.ascontiguousarray(np.asarray(voxels, np.int64).reshape(-1))
+            out = np.empty(vox.size, np.float32)
+            vptr, nv = vox.ctypes.data_as(C.c_void_p), vox.size
+        _lib.check(self._lib.pbs_context_influence_row_norms(
+            self._h, C.byref(bd), int(bool(nuclear_correction)), int(spot_begin), int(spot_count), vptr, nv,
+            out.ctypes.data_as(C.c_void_p)))
+        del keep
         return out
 
     def influence_csc(self, beam, spot_begin: int = 0, spot_count: int | None = None, threshold: float = 0.0,

@@ -555,3 +555,77 @@ def carbon_case(dims=(512, 512, 200), res=(1.0, 1.0, 1.0), gantries=(0.0, 120.0,
     return {"name": "carbon", "ct": ct, "ct_dims": dims_, "ct_resolution": res_, "ct_corner": corner,
             "dose_dims": dims_, "dose_resolution": res_, "dose_corner": corner, "beam": beams[0], "beams": beams,
             "energy": carbon_tables()}
+
+
+def with_carbon_profile(beam: dict, n_gauss: int = 2, depth_n: int = 96, depth_step_mm: float = 2.0,
+                        rows: str = "layers", seed: int = SEED_BASE + 7) -> dict:
+    """The beam with a seeded CarbonPBS lateral profile model in the layout of the
+    reference's RTDBeamSettings (raytracedicom_integration.h:71-76):
+    profile_data [rows][depth_n][2 n_gauss + 1] (n_gauss weights, n_gauss sigmas in
+    mm, one overall weight), profile_setting [depth0, step, depth_n], beam_para_data
+    [rows][3] = (2 sigmaIso^2, rtheta, theta^2) and beam_para_pos. `rows` = "layers"
+    gives one row per energy layer; "energies" gives rows on a separate energy axis
+    (profile_energies) of 1.5x as many rows spanning the layers' energies, and no
+    beam-parameter rows of that count (the reference then reads the rows from the
+    energy axis)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    energies = np.asarray(beam["energies"], np.float32)
+    L = energies.size
+    if rows == "energies":
+        n_rows = max(2, int(round(1.5 * L)))
+        axis = np.linspace(float(energies.min()) - 2.0, float(energies.max()) + 2.0, n_rows).astype(np.float32)
+    else:
+        n_rows = L
+        axis = None
+    d = np.arange(depth_n, dtype=np.float64) * depth_step_mm
+    ch = 2 * n_gauss + 1
+    prof = np.zeros((n_rows, depth_n, ch), np.float64)
+    for r in range(n_rows):
+        w = rng.uniform(0.5, 1.0, n_gauss)
+        w[1:] *= 0.3
+        for g in range(n_gauss):
+            prof[r, :, g] = w[g] * (1.0 + 0.1 * np.sin(d / (40.0 + 10.0 * g)))
+            prof[r, :, n_gauss + g] = (1.2 + 2.5 * g) * (1.0 + d / 300.0) + rng.uniform(0.0, 0.3)
+        prof[r, :, ch - 1] = np.clip(1.0 - 0.25 * d / d[-1] + rng.uniform(-0.02, 0.02), 0.0, None)
+    sig_iso = np.linspace(4.0, 3.0, L if axis is None else L + 1)
+    para = np.stack([2.0 * sig_iso ** 2, np.full_like(sig_iso, 0.002), np.full_like(sig_iso, 2.5e-5)], axis=1)
+    out = dict(beam)
+    out["profile_data"] = prof.astype(np.float32).reshape(-1)
+    out["profile_setting"] = np.array([0.0, depth_step_mm, depth_n], np.float32)
+    out["beam_para_data"] = para.astype(np.float32).reshape(-1)
+    out["beam_para_pos"] = float(beam.get("sad", 0.0)) * 0.0
+    if axis is not None:
+        out["profile_energies"] = axis
+    return out
+
+
+def bio_model(model: str = "lq", energies=(60.0, 240.0), n_rows: int = 12, depth_step_mm: float = 0.5,
+              max_depth_mm: float = 320.0) -> dict:
+    """A seeded-free analytic biological model in the layout of PbsBioModel: a LET
+    table (keV/um) that rises from an entrance plateau towards each energy's range
+    (Bragg-Kleeman, R = 0.022 E^1.77 mm) and falls off behind it, and LQ alpha /
+    beta (or MKM z1D) tables on a log10(LET) axis of 0.01 steps (the reference's
+    lqData indexing, carbonPBS/deviceCalDose.cu:694-695). Synthetic: the reference
+    ships no LET or LQ tables."""
+    e = np.linspace(energies[0], energies[1], n_rows)
+    depth = np.arange(0.0, max_depth_mm, depth_step_mm)
+    let = np.zeros((n_rows, depth.size))
+    for i, en in enumerate(e):
+        r = 0.022 * en ** 1.77
+        resid = np.clip(r - depth, 0.3, None)
+        let[i] = np.where(depth <= r + 2.0, 0.4 + 12.0 / np.sqrt(resid + 0.5), 0.5)
+    logl = np.arange(0.0, 3.0, 0.01)
+    L = 10.0 ** logl
+    out = {"model": model, "let_table": let.astype(np.float32), "let_energies": e.astype(np.float32),
+           "let_depth0": 0.0, "let_depth_step": depth_step_mm, "let_samples": 5, "est_dimension": 2.0,
+           "range_shifter": 0.0, "lq_log0": 0.0, "lq_log_step": 0.01}
+    if model == "lq":
+        # RBE near 1 at low LET: alpha 0.33 / Gy, beta 0.06 / Gy^2 give the reference's
+        # 10 % survival photon dose of 3.99 Gy (LQRBEKernel's constant).
+        out["lq_alpha"] = (0.33 + 0.05 * L / (1.0 + L / 150.0)).astype(np.float32)
+        out["lq_beta"] = (0.06 * np.ones_like(L) / (1.0 + L / 500.0)).astype(np.float32)
+    else:
+        # MKM's photon reference of mkmRBEMapKernel (alphar, betar = 0.3312, 0.0593).
+        out["z1d"] = (0.2 * L / (1.0 + L / 80.0)).astype(np.float32)
+        out["alpha0"], out["beta0"] = 0.3312, 0.0593
+    return out

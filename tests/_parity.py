@@ -16,12 +16,14 @@ GAMMA_PASS_MIN = 0.999
 from subsecondpbs_b200.precision import gamma_pass_rate, max_rel_err  # noqa: E402,F401
 
 
-def run_gpu(case, beams=None, compat=False, keep_debug=True, initial=None, ct_input_type=None, nuclear_model=None):
-    """Run the CUDA library on `case`; `nuclear_model` (0/1/2) adds the nuclear halo."""
+def run_gpu(case, beams=None, compat=False, keep_debug=True, initial=None, ct_input_type=None, nuclear_model=None,
+            carbon_profile=0):
+    """Run the CUDA library on `case`; `nuclear_model` (0/1/2) adds the nuclear halo,
+    `carbon_profile` (bits 1, 2) the CarbonPBS lateral profile model."""
     from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
 
     eng = DoseEngine(0, keep_debug=keep_debug, compat_bev_z_shift=compat, ct_input_type=ct_input_type,
-                     nuclear_model=nuclear_model)
+                     nuclear_model=nuclear_model, carbon_profile=carbon_profile)
     eng.set_energy(case["energy"])
     eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
     eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])

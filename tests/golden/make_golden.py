@@ -57,6 +57,16 @@ CASES = {
                                              "e_range": [70.0, 150.0]}, {"tables": "reference"}),
     "halo_small_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
                                              "e_range": [80.0, 120.0]}, {"tables": "reference", "nuclear": "GAUSS_FIT"}),
+    # CarbonPBS lateral profile model (sigma override and overall weight), which the
+    # reference compiles but keeps off: made by the reference built with both switches
+    # on (oracle/ref/build_ref.sh OFF profile, oracle/_ref/librtd_profile.so), with a
+    # seeded profile table per layer (phantoms.with_carbon_profile), and with the
+    # profile rows on their own energy axis.
+    "profile_small_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                                "e_range": [80.0, 120.0]}, {"tables": "reference", "profile": "layers"}),
+    "profile_energy_rows_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
+                                                      "e_range": [80.0, 120.0]},
+                               {"tables": "reference", "profile": "energies"}),
 }
 
 REFERENCE_TABLES = Path(__file__).resolve().parent / "reference_tables.npz"
@@ -89,6 +99,8 @@ def build_case(name: str):
     beam = case["beam"]
     if tf and "rotate" in tf:
         beam = phantoms.rotate_beam(beam, tf["rotate"])
+    if tf and "profile" in tf:
+        beam = phantoms.with_carbon_profile(beam, rows=tf["profile"])
     if tf and tf.get("legacy"):
         beam = phantoms.legacy_beam(beam)
     return case, beam
@@ -108,8 +120,12 @@ def main(argv=None) -> int:
         builder, kw, tf = CASES[name]
         nuclear = bool(tf and "nuclear" in tf)
         lib = ref.REF_LIB.parent / "librtd_nuc.so" if nuclear else ref.REF_LIB
+        if tf and "profile" in tf:
+            lib = ref.REF_LIB.parent / "librtd_profile.so"
         dose, batched, text = ref.run(case, beams=[beam], nuclear=nuclear, verbose=1, path=lib)
         build = f"NUCLEAR_CORR={tf['nuclear']}" if nuclear else "NUCLEAR_CORR=OFF"
+        if tf and "profile" in tf:
+            build += ", CarbonPBS profile switches on"
         meta = {"case": name, "builder": builder, "kwargs": kw, "transform": tf,
                 "reference": f"Nelgcis/subsecondPBS subsecondWrapper built by oracle/ref/build_ref.sh ({build})",
                 "dose_max": float(dose.max()), "dose_sum": float(dose.sum())}

@@ -45,6 +45,12 @@ def nuclear_model_of(meta):
     return {"SOUKUP": 0, "FLUKA": 1, "GAUSS_FIT": 2}[tf["nuclear"]] if "nuclear" in tf else None
 
 
+def carbon_profile_of(meta):
+    """Both profile switches (3) for the cases the reference ran with its CarbonPBS
+    lateral profile model on, else 0."""
+    return 3 if "profile" in (meta.get("transform") or {}) else 0
+
+
 def load_case(name):
     import sys
 
@@ -63,7 +69,7 @@ def test_oracle_matches_reference_outputs(name):
     tol, gmin, flips = PINS[name]
     nuc = nuclear_model_of(meta)
     r = O.dose(case, beams=[beam], compat_bev_z_shift=True, capture=True,
-               nuclear_model=-1 if nuc is None else nuc)
+               nuclear_model=-1 if nuc is None else nuc, carbon_profile=carbon_profile_of(meta))
     ref = z["dose"].astype(np.float64)
     assert abs(float(ref.max()) - meta["dose_max"]) <= 1e-6 * meta["dose_max"]
     err = max_rel_err(r["dose"], ref)

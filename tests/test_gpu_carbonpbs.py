@@ -53,14 +53,8 @@ def test_final_dose_matches_the_oracle_on_the_converted_inputs(export):
     _dose_checks(dose, r["dose"], case["dose_resolution"])
 
 
-def test_cal_dose3_zeroes_the_sparse_outputs(export):
-    case, ex, ctx = export
-    nx, ny, nz = ctx["dims"]
-    data = np.ones(16, np.float32)
-    ptr = np.ones(8, np.int32)
-    rows = np.ones(16, np.int32)
-    nnz = np.ones(1, np.uint64)
-    args = dict(weq_data=ex["rayweq"], roi_index=ex["roiIdx"], source_energies=ex["all_energies"],
+def _dose3_args(ex, nnz):
+    return dict(weq_data=ex["rayweq"], roi_index=ex["roiIdx"], source_energies=ex["all_energies"],
                 source=ex["sourcePos"], beam_dir=ex["tmpBeamDir"], beam_xdir=ex["bmxdir"], beam_ydir=ex["bmydir"],
                 corner=ex["corner"], resolution=ex["resolution"], dims=ex["dims"], longitudal_cutoff=None,
                 enelist=ex["enelist"], idddata=ex["idddata"], iddsetting=ex["iddsetting"], profiledata=None,
@@ -68,11 +62,65 @@ def test_cal_dose3_zeroes_the_sparse_outputs(export):
                 layer_energy=ex["layerEnergy"], outNNZ=nnz, idbeamxy=ex["idbeamxy"],
                 num_particles_per_beam=ex["nPar"], cutoff=None, sad=ex["sad"], beam_para_pos=None,
                 python_nnz_size=None, tables_dir=None)
-    out = cuCalDose3(data, ptr, rows, **args)
-    assert not data.any() and not ptr.any() and not rows.any() and not nnz.any()
-    ref = cuFinalDose(np.zeros((nz, ny, nx), np.float32), **ex, tables_dir=None)
-    assert out["dose_grid"].shape == (nx, ny, nz)
-    assert np.abs(out["dose_grid"].transpose(2, 1, 0) - ref).max() <= 2e-5 * float(ref.max())
+
+
+def test_cal_dose3_exports_the_influence_matrix(export):
+    """cuCalDose3's sparse outputs hold the spot-preserving influence matrix in the
+    CarbonPBS caller's layout (x-major rows, per-column counts after a leading 0):
+    weighted by the spot weights it gives the dose grid; a short buffer is left
+    unwritten with the needed size in outNNZ."""
+    case, ex, ctx = export
+    nx, ny, nz = ctx["dims"]
+    n_spots = ex["nPar"].size
+    nnz = np.zeros(1, np.uint64)
+    small = cuCalDose3(np.ones(16, np.float32), np.ones(n_spots + 1, np.int32), np.ones(16, np.int32),
+                       **_dose3_args(ex, nnz))
+    need = int(nnz[0])
+    assert need > 16 and not small["out_cscdata"].any() and not small["out_cscrowind"].any()
+    data, rows = np.zeros(need, np.float32), np.zeros(need, np.int32)
+    ptr = np.zeros(n_spots + 1, np.int32)
+    out = cuCalDose3(data, ptr, rows, **_dose3_args(ex, nnz))
+    assert int(nnz[0]) == need and int(ptr.sum()) == need and ptr[0] == 0
+    offs = np.cumsum(ptr.astype(np.int64))
+    for j in range(0, n_spots, max(1, n_spots // 7)):
+        assert np.all(np.diff(rows[offs[j]:offs[j + 1]]) > 0)
+    import scipy.sparse as sp
+
+    a = sp.csc_matrix((data, rows, offs), shape=(nx * ny * nz, n_spots))
+    dose_xyz = out["dose_grid"]
+    ad = (a @ ex["nPar"].astype(np.float64)).reshape(nx, ny, nz)
+    dmax = float(dose_xyz.max())
+    assert dmax > 0
+    assert np.abs(ad - dose_xyz).max() <= 5e-3 * dmax
+
+
+def test_dose_norm_is_the_row_norm_of_the_influence_matrix(export):
+    """cuCalDoseNorm (CarbonPBS) = sum over spots of the squared unit-weight dose at
+    each ROI voxel, computed on the device: equal to the squared row norms of the
+    matrix cuCalDose3 exports."""
+    case, ex, ctx = export
+    nx, ny, nz = ctx["dims"]
+    n_spots = ex["nPar"].size
+    nnz = np.zeros(1, np.uint64)
+    cuCalDose3(np.zeros(1, np.float32), np.zeros(n_spots + 1, np.int32), np.zeros(1, np.int32),
+               **_dose3_args(ex, nnz))
+    need = int(nnz[0])
+    data, rows, ptr = np.zeros(need, np.float32), np.zeros(need, np.int32), np.zeros(n_spots + 1, np.int32)
+    cuCalDose3(data, ptr, rows, **_dose3_args(ex, nnz))
+    import scipy.sparse as sp
+
+    a = sp.csc_matrix((data.astype(np.float64), rows, np.cumsum(ptr.astype(np.int64))),
+                      shape=(nx * ny * nz, n_spots))
+    want = np.asarray(a.multiply(a).sum(axis=1)).reshape(-1)
+    hot = np.flatnonzero(want > 0.05 * want.max())
+    roi = np.stack([hot // (ny * nz), (hot // nz) % ny, hot % nz], axis=1).astype(np.int32)
+    norm = np.zeros(hot.size, np.float32)
+    assert cp.cuCalDoseNorm(norm, ex["rayweq"], roi, ex["all_energies"], ex["sourcePos"], ex["tmpBeamDir"],
+                            ex["bmxdir"], ex["bmydir"], ex["corner"], ex["resolution"], ex["dims"], None,
+                            ex["enelist"], ex["idddata"], ex["iddsetting"], None, None, None, ex["subspotdata"],
+                            ex["layerInfo"], ex["layerEnergy"], ex["idbeamxy"], ex["sad"], None, None,
+                            tables_dir=None) == 1
+    np.testing.assert_allclose(norm, want[hot], rtol=2e-5)
 
 
 def test_roi_ct_changes_only_the_geometry_stand_in(export):

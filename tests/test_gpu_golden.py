@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from _parity import gamma_pass_rate, max_rel_err, run_gpu
-from test_cpu_golden import PINS, load_case, nuclear_model_of
+from test_cpu_golden import PINS, carbon_profile_of, load_case, nuclear_model_of
 
 pytestmark = pytest.mark.gpu
 
@@ -15,7 +15,8 @@ def test_cuda_matches_reference_outputs(name):
     z, meta, case, beam = load_case(name)
     tol, gmin, flips = PINS[name]
     nuc = nuclear_model_of(meta)
-    eng = run_gpu(case, beams=[beam], compat=True, keep_debug=False, nuclear_model=nuc)
+    eng = run_gpu(case, beams=[beam], compat=True, keep_debug=False, nuclear_model=nuc,
+                  carbon_profile=carbon_profile_of(meta))
     dose = eng.read_dose()
     ref = z["dose"].astype(np.float64)
     assert max_rel_err(dose, ref) < tol
