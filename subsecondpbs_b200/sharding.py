@@ -6,6 +6,13 @@ beams are divided among the ranks, every rank computes its beams into its own
 FP64 dose grid, and a single reduction sums the grids on the destination rank.
 No other data crosses ranks: this is the only collective of the path.
 
+A single beam shards by energy layer in the same way: the layers of a beam are
+independent once the beam is traced (raytracedicom_wrapper.cu:3917-5625 loops
+over them into one grid), so each rank traces the whole beam (the cheap part),
+computes only its share of the layers (the other layers' spots at zero weight,
+which leaves their rays dead and their tiles out of the superposition) and the
+same single reduction sums the shares.
+
 The functions take any engine with `reset_dose()`, `add_beam(beam)` and
 `read_dose64(out)` (`cudaCalDoseRTD.DoseEngine` on a GPU) and any
 `torch.distributed` process group (NCCL between GPUs; gloo works for CPU
@@ -48,6 +55,41 @@ def assign_beams(costs: Sequence[float], world: int) -> list[list[int]]:
     for lst in out:
         lst.sort()
     return out
+
+
+def assign_layers(beam: dict, world: int) -> list[list[int]]:
+    """Layers of `beam` per rank: longest-processing-time on the layers' spot counts
+    (every layer costs at least 1), deterministic as assign_beams."""
+    counts = np.asarray(beam["layer_spot_counts"]).reshape(-1)
+    return assign_beams([max(float(c), 1.0) for c in counts], world)
+
+
+def layer_share(beam: dict, layers: Sequence[int]) -> dict:
+    """The beam with only `layers` carrying spot weight. Spot positions, energies and
+    everything the plan is made from stay, so every share has the whole beam's ray
+    grid, lattice and cut-off steps, and the shares' doses add up to the beam's."""
+    counts = np.asarray(beam["layer_spot_counts"]).astype(np.int64).reshape(-1)
+    keep = np.zeros(int(counts.sum()), bool)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    for l in layers:
+        keep[starts[l]:starts[l + 1]] = True
+    out = dict(beam)
+    out["spot_weights"] = np.where(keep, np.asarray(beam["spot_weights"], np.float32), np.float32(0.0))
+    return out
+
+
+def beam_layers_dose(engine, beam: dict, dose64, rank: int, world: int, dst: int = 0, group=None):
+    """This rank's share of one beam's layers, reduced on `dst`. A rank without
+    layers (more ranks than layers) adds nothing and still joins the reduction.
+    Returns (tensor, assigned layer indices)."""
+    mine = assign_layers(beam, world)[rank]
+    engine.reset_dose()
+    if mine:
+        engine.add_beam(layer_share(beam, mine))
+    engine.read_dose64(dose64)
+    if world > 1:
+        reduce_dose(dose64, dst=dst, group=group)
+    return dose64, mine
 
 
 def reduce_dose(dose64, dst: int = 0, group=None):

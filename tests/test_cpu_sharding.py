@@ -55,7 +55,7 @@ def _free_port():
     return port
 
 
-def _worker(rank, world, port, result_path, fail_rank):
+def _worker(rank, world, port, result_path, fail_rank, mode="beams"):
     import sys
     from datetime import timedelta
     from pathlib import Path
@@ -78,7 +78,10 @@ def _worker(rank, world, port, result_path, fail_rank):
     try:
         if rank == fail_rank:
             raise RuntimeError("rank failed before its collective")
-        out, mine = sharding.plan_dose(OracleEngine(case), beams, dose, rank, world)
+        if mode == "layers":
+            out, mine = sharding.beam_layers_dose(OracleEngine(case), beams[1], dose, rank, world)
+        else:
+            out, mine = sharding.plan_dose(OracleEngine(case), beams, dose, rank, world)
         if rank == 0:
             np.save(result_path, out.numpy())
     except Exception as e:  # recorded for the parent; a peer's failure must surface as an error here
@@ -88,11 +91,11 @@ def _worker(rank, world, port, result_path, fail_rank):
         dist.destroy_process_group()
 
 
-def _spawn(tmp_path, fail_rank):
+def _spawn(tmp_path, fail_rank, mode="beams"):
     import torch.multiprocessing as mp
 
     result = str(tmp_path / "dose.npy")
-    mp.start_processes(_worker, args=(2, _free_port(), result, fail_rank), nprocs=2, join=True,
+    mp.start_processes(_worker, args=(2, _free_port(), result, fail_rank, mode), nprocs=2, join=True,
                        start_method="spawn")
     return result
 
@@ -114,3 +117,38 @@ def test_a_failed_rank_surfaces_as_an_error(tmp_path):
     _spawn(tmp_path, fail_rank=1)
     assert (tmp_path / "dose.npy.rank1").read_text().startswith("error")
     assert (tmp_path / "dose.npy.rank0").read_text().startswith("error")
+
+
+def test_layer_assignment_covers_every_layer_once(hetero_small_case):
+    beam = hetero_small_case["beam"]
+    L = len(beam["energies"])
+    for world in (1, 2, 3, 5):
+        parts = sharding.assign_layers(beam, world)
+        assert sorted(l for p in parts for l in p) == list(range(L))
+
+
+def test_layer_shares_sum_to_the_beam():
+    """The shares' doses add up to the whole beam's: layers are independent once the
+    beam is traced, and a layer without weight deposits nothing."""
+    from oracle import oracle as O
+    from subsecondpbs_b200 import phantoms
+
+    case = phantoms.heterogeneous_case(dims=(48, 48, 32), n_layers=3, target_radius_mm=10.0)
+    beam = case["beam"]
+    whole = O.dose(case, threads=2)["dose"]
+    parts = [O.dose(case, beams=[sharding.layer_share(beam, [l])], threads=2)["dose"] for l in range(3)]
+    assert np.abs(sum(parts) - whole).max() <= 1e-12 * whole.max()
+    assert all(p.max() > 0 for p in parts)
+
+
+def test_two_ranks_shard_one_beam_by_layer(tmp_path):
+    from oracle import oracle as O
+    from subsecondpbs_b200 import phantoms
+
+    result = _spawn(tmp_path, fail_rank=-1, mode="layers")
+    case = phantoms.heterogeneous_case(dims=(48, 48, 32), n_layers=2, target_radius_mm=10.0)
+    beam = phantoms.rotate_beam(case["beam"], 90.0)
+    whole = O.dose(case, beams=[beam], threads=2)["dose"]
+    got = np.load(result)
+    assert np.abs(got - whole).max() <= 1e-12 * whole.max()
+    assert (tmp_path / "dose.npy.rank1").read_text() == "ok"
