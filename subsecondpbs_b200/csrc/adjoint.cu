@@ -9,6 +9,8 @@
 //               = (sum_k idd[l][k][ray] * (S^T T^T Gd)[l][k][ray]) / rayW[l][ray].
 // The tile radii, the live-ray mask and rSigmaEff do not depend on the weights'
 // values, so they come from the same IDD and binning kernels as the forward pass.
+#include <algorithm>
+
 #include "device_util.cuh"
 #include "kernels.h"
 #include "launch_util.h"
@@ -22,41 +24,50 @@ namespace {
 // same weights. The forward adds a sample only where it is positive; a BEV sample
 // is a sum of non-negative terms, so it is zero only where every texel's
 // coefficient is zero and the linear transpose is exact.
+// Items of one dose column and 8 consecutive z, x fastest, strided over by a
+// persistent grid (the box is known only on the device; see transfer_kernel).
 __global__ void __launch_bounds__(256)
 transfer_adjoint_kernel(BeamGeomDev g, const double* __restrict__ gradDose, const BeamStateDev* __restrict__ beam,
                         float* __restrict__ gradBev) {
     if (!beam->transferValid) return;
     const int sx = beam->transferStart[0], sy = beam->transferStart[1], sz = beam->transferStart[2];
     const int mx = beam->transferMax[0], my = beam->transferMax[1], mz = beam->transferMax[2];
-    const int spanX = ((mx - sx + 1 + 31) / 32) * 32, spanY = ((my - sy + 1 + 7) / 8) * 8;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x < sx || y < sy || x >= sx + spanX || y >= sy + spanY || x >= g.doseX || y >= g.doseY) return;
-    const int z0 = max(sz, int(blockIdx.z) * 8);
-    const int z1 = min(mz, int(blockIdx.z) * 8 + 7);
-    if (z0 > z1) return;
+    const int nxCols = min(((mx - sx + 1 + 31) / 32) * 32, g.doseX - sx);
+    const int nyCols = min(((my - sy + 1 + 7) / 8) * 8, g.doseY - sy);
+    const int nzc = (mz - sz + 8) / 8;
+    if (nxCols <= 0 || nyCols <= 0 || nzc <= 0) return;
+    const long long items = static_cast<long long>(nxCols) * nyCols * nzc;
     const TransferParams T = beam->transfer;
-    const V3 start = transfer_start(T, x, y);
     const float zShift = g.compatBevZShift ? float(beam->firstInside) : 0.0f;
     const size_t slice = static_cast<size_t>(g.doseX) * g.doseY;
     const int nx = g.bevX, ny = g.bevY, nz = g.steps;
-    for (int z = z0; z <= z1; ++z) {
-        const V3 f = transfer_fan_idx(T, start, z);
-        if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
-        const float gd = float(gradDose[static_cast<size_t>(z) * slice + static_cast<size_t>(y) * g.doseX + x]);
-        if (gd == 0.0f) continue;
-        const float px = fminf(fmaxf(f.x, -2.0f), float(nx) + 1.0f);
-        const float py = fminf(fmaxf(f.y, -2.0f), float(ny) + 1.0f);
-        const float pz = fminf(fmaxf(f.z - zShift, -2.0f), float(nz) + 1.0f);
-        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
-        const int x0 = int(fx), y0 = int(fy), z0i = int(fz);
-        const float tx = px - fx, ty = py - fy, tz = pz - fz;
+    for (long long it = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = sx + static_cast<int>(it % nxCols);
+        const long long r = it / nxCols;
+        const int y = sy + static_cast<int>(r % nyCols);
+        const int z0 = sz + static_cast<int>(r / nyCols) * 8;
+        const int z1 = min(mz, z0 + 7);
+        const V3 start = transfer_start(T, x, y);
+        for (int z = z0; z <= z1; ++z) {
+            const V3 f = transfer_fan_idx(T, start, z);
+            if (f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f) continue;
+            const float gd = float(gradDose[static_cast<size_t>(z) * slice + static_cast<size_t>(y) * g.doseX + x]);
+            if (gd == 0.0f) continue;
+            const float px = fminf(fmaxf(f.x, -2.0f), float(nx) + 1.0f);
+            const float py = fminf(fmaxf(f.y, -2.0f), float(ny) + 1.0f);
+            const float pz = fminf(fmaxf(f.z - zShift, -2.0f), float(nz) + 1.0f);
+            const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+            const int x0 = int(fx), y0 = int(fy), z0i = int(fz);
+            const float tx = px - fx, ty = py - fy, tz = pz - fz;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int xi = x0 + (c & 1), yi = y0 + ((c >> 1) & 1), zi = z0i + (c >> 2);
-            if (xi < 0 || yi < 0 || zi < 0 || xi >= nx || yi >= ny || zi >= nz) continue;
-            const float w = ((c & 1) ? tx : 1.0f - tx) * (((c >> 1) & 1) ? ty : 1.0f - ty) * ((c >> 2) ? tz : 1.0f - tz);
-            atomicAdd(gradBev + (static_cast<size_t>(zi) * ny + yi) * nx + xi, w * gd);
+            for (int c = 0; c < 8; ++c) {
+                const int xi = x0 + (c & 1), yi = y0 + ((c >> 1) & 1), zi = z0i + (c >> 2);
+                if (xi < 0 || yi < 0 || zi < 0 || xi >= nx || yi >= ny || zi >= nz) continue;
+                const float w =
+                    ((c & 1) ? tx : 1.0f - tx) * (((c >> 1) & 1) ? ty : 1.0f - ty) * ((c >> 2) ? tz : 1.0f - tz);
+                atomicAdd(gradBev + (static_cast<size_t>(zi) * ny + yi) * nx + xi, w * gd);
+            }
         }
     }
 }
@@ -149,9 +160,11 @@ superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const flo
 
 cudaError_t launch_transfer_adjoint(const BeamGeomDev& g, const double* gradDose, const BeamStateDev* beam,
                                     float* gradBev, cudaStream_t s) {
-    dim3 block(32, 8);
-    dim3 grid((g.doseX + 31) / 32, (g.doseY + 7) / 8, (g.doseZ + 7) / 8);
-    transfer_adjoint_kernel<<<grid, block, 0, s>>>(g, gradDose, beam, gradBev);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long cap = (static_cast<long long>(g.doseX) * g.doseY * ((g.doseZ + 7) / 8) + 255) / 256;
+    const int blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(cap, sms * 8)));
+    transfer_adjoint_kernel<<<blocks, 256, 0, s>>>(g, gradDose, beam, gradBev);
     return cudaGetLastError();
 }
 

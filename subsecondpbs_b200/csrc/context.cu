@@ -370,9 +370,11 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
         const int lutN = int(densityHost.size());
         if (mapped && hasEnergy && lutN > 0 && energy.density_scale_fact != 0.0f && stats.ensure(64) == PBS_OK) {
             PBS_CUDA(launch_ct_convert_detect(static_cast<float*>(ct.ptr), n, static_cast<const float*>(at.devicePointer),
-                                              static_cast<const float*>(density.ptr), lutN, energy.density_scale_fact,
-                                              static_cast<unsigned*>(stats.ptr), stream),
+                                              g.dims, lo, hi, static_cast<const float*>(density.ptr), lutN,
+                                              energy.density_scale_fact, static_cast<unsigned*>(stats.ptr), stream),
                      "ct_convert_detect");
+            // At most the samples outside the box cross the host link (none when the
+            // box already holds a value below -200); counted as all samples.
             copiedH2D += ct_type_sample_count(n) * sizeof(float);
             ctType = PBS_CT_AUTO;
             ctGrid = g;

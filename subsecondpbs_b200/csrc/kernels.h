@@ -20,8 +20,12 @@ cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStrea
 // uploaded `ct`. `keys` is two words of device scratch.
 // Number of strided CT samples the type detection reads (the reference's ~100k).
 size_t ct_type_sample_count(size_t n);
-cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const float* densityLut,
-                                     int lutN, float lutScale, unsigned* keys, cudaStream_t s);
+// CT type detection from the reference's strided samples, with the samples inside
+// the uploaded box [boxLo, boxHi] read from `ct` and the others from the mapped
+// host CT only when needed, then the conversion in place.
+cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const int dims[3],
+                                     const int boxLo[3], const int boxHi[3], const float* densityLut, int lutN,
+                                     float lutScale, unsigned* keys, cudaStream_t s);
 
 // ---- tracing ------------------------------------------------------------------
 // rayTracingBEVKernel (src/core/bev_ray_tracing.cu:65-159) as a segmented scan,

@@ -532,18 +532,35 @@ __global__ void ct_convert_kernel(float* ct, size_t n, int type, const float* __
 // thread per sample, reduced into order keys of its minimum and maximum (NaN is
 // left out, as under std::min / std::max). Used on the caller's page-locked host CT
 // through its device mapping, so that the CT type is known without a host pass.
-__global__ void ct_sample_range_kernel(const float* __restrict__ ct, size_t stride, size_t samples, unsigned* keys) {
+// Range of the CT type samples (every `stride`-th voxel, wrapper.cu:2307-2337) in two
+// passes. Pass 0 reads the samples inside the uploaded box from the device copy
+// (raw values: the conversion runs after both passes). Pass 1 reads the samples
+// outside the box from the caller's page-locked host CT through its device mapping
+// (latency-bound reads over the host link), unless pass 0 already found a value
+// below -200: the type is then HU whatever the other samples hold, since the
+// detection tests the minimum against -200 first (ct_type_from_range).
+__global__ void ct_sample_range_kernel(const float* __restrict__ hostCt, const float* __restrict__ devCt, int3 dims,
+                                       int3 lo, int3 hi, size_t stride, size_t samples, unsigned* keys, int pass) {
+    if (pass == 1 && float_from_order_key(*(volatile unsigned*)keys) < -200.0f) return;
     const size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-    unsigned lo = 0xffffffffu, hi = 0u;
+    unsigned kl = 0xffffffffu, kh = 0u;
     if (k < samples) {
-        const float v = ct[k * stride];
-        if (v == v) lo = hi = float_order_key(v);
+        const size_t idx = k * stride;
+        const size_t plane = size_t(dims.x) * dims.y;
+        const int z = int(idx / plane);
+        const size_t r = idx - size_t(z) * plane;
+        const int y = int(r / dims.x), x = int(r - size_t(y) * dims.x);
+        const bool inBox = x >= lo.x && x <= hi.x && y >= lo.y && y <= hi.y && z >= lo.z && z <= hi.z;
+        if (inBox == (pass == 0)) {
+            const float v = inBox ? devCt[idx] : hostCt[idx];
+            if (v == v) kl = kh = float_order_key(v);
+        }
     }
-    lo = __reduce_min_sync(0xffffffffu, lo);
-    hi = __reduce_max_sync(0xffffffffu, hi);
+    kl = __reduce_min_sync(0xffffffffu, kl);
+    kh = __reduce_max_sync(0xffffffffu, kh);
     if ((threadIdx.x & 31) == 0) {
-        if (lo != 0xffffffffu) atomicMin(keys, lo);
-        if (hi != 0u) atomicMax(keys + 1, hi);
+        if (kl != 0xffffffffu) atomicMin(keys, kl);
+        if (kh != 0u) atomicMax(keys + 1, kh);
     }
 }
 
@@ -589,8 +606,9 @@ size_t ct_type_sample_count(size_t n) {
     return n == 0 ? 0 : (n + stride - 1) / stride;
 }
 
-cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const float* densityLut,
-                                     int lutN, float lutScale, unsigned* keys, cudaStream_t s) {
+cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMapped, const int dims[3],
+                                     const int boxLo[3], const int boxHi[3], const float* densityLut, int lutN,
+                                     float lutScale, unsigned* keys, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const size_t maxSamples = 100000;
     const size_t stride = (n > maxSamples) ? (n / maxSamples) : 1;
@@ -598,7 +616,11 @@ cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMap
     cudaError_t e = cudaMemsetAsync(keys, 0xff, sizeof(unsigned), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(keys + 1, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    ct_sample_range_kernel<<<unsigned((samples + 255) / 256), 256, 0, s>>>(hostCtMapped, stride, samples, keys);
+    const int3 d = make_int3(dims[0], dims[1], dims[2]);
+    const int3 lo = make_int3(boxLo[0], boxLo[1], boxLo[2]), hi = make_int3(boxHi[0], boxHi[1], boxHi[2]);
+    for (int pass = 0; pass < 2; ++pass)
+        ct_sample_range_kernel<<<unsigned((samples + 255) / 256), 256, 0, s>>>(hostCtMapped, ct, d, lo, hi, stride,
+                                                                               samples, keys, pass);
     const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
     ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, PBS_CT_AUTO, densityLut, lutN, lutScale, keys);
     return cudaGetLastError();
