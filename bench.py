@@ -44,6 +44,10 @@ WORKLOAD = ("heterogeneous CT 256x256x160 at 2 mm (body ellipsoid, lung slab, 2 
 DATA = ("synthetic seeded phantom; the reference's own proton lookup tables (tables/ as read by its "
         "energyReader)")
 TABLES = ROOT / "tests" / "golden" / "reference_tables.npz"
+# The same `config` on both arms (the workload and how the L2 is treated between
+# timed steps); run details of either arm go under `run`.
+L2_NOTE = "GPU arm: L2 flushed between timed steps (256 MiB write outside the step events); CPU arm: not applicable"
+CONFIG = {"workload": WORKLOAD, "l2": L2_NOTE}
 REF_LIB = ROOT / "oracle" / "_ref" / "librtd.so"
 
 
@@ -163,7 +167,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": DATA,
-        "config": {"workload": WORKLOAD, "l2": "not applicable (CPU)"},
+        "config": dict(CONFIG),
+        "run": {"arm": "CPU restatement of the reference's dose path (the oracle port), all host threads"},
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
                          "sample": f"full workload: {args.steps} beams after {args.warmup} warm-up beams"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -258,6 +263,7 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
     serving.plain_pipeline(w, prepared, local)
     plain = serving.plain_pipeline(w, prepared, local, keep=check)
     ps = plain["service_s"] * 1e3
+    device = serving.device_pipeline(w, prepared, local)
     srv = serving.DoseServer(local, slots=slots, hbm_budget_mib=budget_mib)
     srv.add_energy(0, w["energy"]["proton"])
     srv.add_energy(1, w["energy"]["carbon"])
@@ -286,7 +292,11 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
                       "arrivals": "all at t=0"},
         "poisson": {"rate_hz": round(rate, 2), "plans_per_s": round(poi["plans_per_s"], 2), "p50_ms": pct(pl, 0.5),
                     "p99_ms": pct(pl, 0.99)},
+        "device_serial": {"plans_per_s": round(device["plans_per_s"], 2),
+                          "what": "the same requests' kernels back to back on one resident context per ion, "
+                                  "CUDA-event device time per request (no host planning, uploads or copies)"},
         "served_over_plain": round(sat["plans_per_s"] / plain["plans_per_s"], 3),
+        "served_over_device_serial": round(sat["plans_per_s"] / device["plans_per_s"], 3),
         "result_max_diff_vs_plain_frac_dmax": float(max(diffs)),
         "server_stats": {k: v for k, v in stats.items() if k in ("completed", "failed", "patient_loads",
                                                                   "evictions", "peak_bytes", "budget_bytes")},
@@ -326,6 +336,80 @@ def _carbon_plan(local: int, reps: int = 3) -> dict:
             "ms_per_plan": round(statistics.median(ms), 3), "timing": f"CUDA events, median of {reps}"}
 
 
+def _operator_export(local: int, n_spots: int = 256) -> dict:
+    """Influence-matrix export (pbs_context_influence_csc) of a batch of the headline
+    beam's spots: wall time of the call (all columns, entries compacted on the device
+    and copied to host memory), after one warm-up batch."""
+    import time
+
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    case = _headline_case()
+    eng = DoseEngine(local)
+    eng.set_energy(case["energy"])
+    eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
+    eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
+    beam = eng.prepare_beam(case["beam"])
+    begin = 1500
+    cap = 40000 * n_spots
+    eng.influence_csc(beam, spot_begin=begin - n_spots, spot_count=n_spots, capacity=cap)
+    t = time.perf_counter()
+    a = eng.influence_csc(beam, spot_begin=begin, spot_count=n_spots, capacity=cap)
+    ms = (time.perf_counter() - t) * 1e3
+    eng.close()
+    return {"workload": f"{n_spots} spots of the headline beam (from spot {begin}), threshold 0",
+            "ms": round(ms, 2), "ms_per_spot": round(ms / n_spots, 4), "entries": int(a.nnz),
+            "timing": "wall time of one pbs_context_influence_csc call after a warm-up batch"}
+
+
+def _upstream_cpu_conv(eng, stats: dict, spacing_mm: float, our_conv_ms: float, budget_s: float = 10.0) -> dict:
+    """Stage-level CPU baseline of the spot-to-ray convolution: the upstream
+    RayTraceDicom CPU Gaussian convolution (xConvCpu then yConvCpu,
+    RayTraceDicom-main/src/cpu_convolution_1d.cpp, built from its sources into
+    oracle/_ref/librtd_cpuconv.so by oracle/ref/build_upstream_conv.sh), single
+    threaded as shipped, over a dense weight map of the headline beam's ray grid for
+    each of its layers with the layer's entry sigma in ray pixels (3-sigma radius)."""
+    lib_path = ROOT / "oracle" / "_ref" / "librtd_cpuconv.so"
+    if not lib_path.exists():
+        return {"unavailable": "oracle/_ref/librtd_cpuconv.so not built (oracle/ref/build_upstream_conv.sh needs the "
+                               "reference sources)"}
+    import ctypes as C
+    import time
+
+    lib = C.CDLL(str(lib_path))
+    fp = C.POINTER(C.c_float)
+    lib.upstream_x_conv_cpu.argtypes = [fp, fp, C.c_float, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int]
+    lib.upstream_y_conv_cpu.argtypes = [fp, fp, C.c_float, C.c_uint, C.c_uint, C.c_uint, C.c_int]
+    rx, ry = stats["ray_dims"]
+    layers = []
+    for l in range(stats["num_layers"]):
+        sig = max(float(eng.layer_stats(l)["entry_sigma"][0]) / spacing_mm, 1e-3)
+        layers.append((1.0 / (np.sqrt(2.0) * sig), int(np.ceil(3.0 * sig))))
+    rng = np.random.Generator(np.random.PCG64(7))
+    src = rng.random((ry, rx), dtype=np.float32)
+    mid = np.zeros((ry, rx), np.float32)
+    outs = [np.zeros((ry + 2 * rad, rx), np.float32) for _, rad in layers]
+
+    def one_beam():
+        for (rs, rad), out in zip(layers, outs):
+            out[...] = 0.0
+            lib.upstream_x_conv_cpu(src.ctypes.data_as(fp), mid.ctypes.data_as(fp), rs, rad, rx, rx, ry, 0)
+            lib.upstream_y_conv_cpu(mid.ctypes.data_as(fp), out.ctypes.data_as(fp), rs, rad, ry, rx, rad)
+
+    one_beam()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < 3 or (len(times) < 50 and time.perf_counter() < t_end):
+        t = time.perf_counter()
+        one_beam()
+        times.append((time.perf_counter() - t) * 1e3)
+    ms = float(np.median(times))
+    return {"stage": "spot-to-ray convolution", "impl": "upstream RayTraceDicom xConvCpu + yConvCpu "
+            "(cpu_convolution_1d.cpp) built from its sources, 1 thread", "ms_per_beam": round(ms, 3),
+            "ours_conv_ms": round(our_conv_ms, 4), "ratio": round(ms / max(our_conv_ms, 1e-9), 1),
+            "sample": f"{len(layers)} layers on the {rx}x{ry} ray grid, median of {len(times)} beams"}
+
+
 def _reference_gpu(local: int, case: dict, our_e2e_ms: float) -> dict | None:
     """The reference's own GPU path on the same beam and tables: its subsecondWrapper
     (built from its sources into oracle/_ref/librtd.so) timed in a child process,
@@ -358,6 +442,7 @@ def _reference_gpu(local: int, case: dict, our_e2e_ms: float) -> dict | None:
     return {"api": "reference subsecondWrapper (raytracedicom_wrapper.cu:2446) built from its sources for sm_100a "
                    "by oracle/ref/build_ref.sh, host buffers, verbose=0",
             "e2e_ms_median": round(timing["median_ms"], 3), "calls": timing["calls"],
+            "reference_last_vs_first_call_max_diff_frac_dmax": timing.get("last_vs_first_call_max_diff_frac_dmax"),
             "ours_e2e_ms": round(our_e2e_ms, 4),
             "speedup_e2e": round(timing["median_ms"] / our_e2e_ms, 1),
             "dose_agreement": dict(agreement, against="this library with the reference's BEV depth shift, "
@@ -552,7 +637,10 @@ def run_ours(args):
     served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
               if world == 1 and args.serving_requests > 0 else None)
     carbon = _carbon_plan(local) if world == 1 and not args.no_adjoint else None
+    operator = _operator_export(local) if world == 1 and not args.no_adjoint else None
     reference_gpu = _reference_gpu(local, case, e2e_ms) if world == 1 and not args.no_reference_gpu else None
+    upstream_conv = (_upstream_cpu_conv(eng, stats, float(case["beam"]["ray_spacing"][0]), stage_ms["conv"])
+                     if world == 1 and not args.no_cpu_baseline else None)
 
     line = {
         "metric": METRIC,
@@ -567,9 +655,9 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": DATA,
-        "config": {"workload": WORKLOAD, "beams_per_step": world, "parallelism": f"beam-sharded x{world}",
-                   "l2": "flushed between timed steps (256 MiB write outside the step events)",
-                   "accumulation": "FP64 dose grid", "total_ms_incl_flush": total_ms},
+        "config": dict(CONFIG),
+        "run": {"beams_per_step": world, "parallelism": f"beam-sharded x{world}", "accumulation": "FP64 dose grid",
+                "total_ms_incl_flush": total_ms},
         "roofline": {"kernel": "superpose_kernel", "bound": "fp32", "achieved": round(achieved, 3),
                      "peak": round(peak_fp32, 3), "unit": "TFLOP/s", "frac": round(achieved / peak_fp32, 4),
                      "traffic": traffic, "peak_source": "in-run FFMA microbenchmark (FP32 pipe, no tensor cores)",
@@ -577,10 +665,12 @@ def run_ours(args):
         "roofline_stages": roof_stages,
         "stages_ms": stage_ms,
         "cpu_baseline": cpu,
+        "cpu_stage_baseline": upstream_conv,
         "precision": precision,
         "adjoint": adjoint,
         "serving": served,
         "carbon_plan": carbon,
+        "operator_export": operator,
         "e2e": {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "pbs_subsecond_wrapper (C ABI), pinned host buffers",
                 "bytes": "measured by the library (pbs_wrapper_copy_bytes): traced CT box, initial and final dose "

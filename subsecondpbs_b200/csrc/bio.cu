@@ -154,7 +154,6 @@ cudaError_t launch_bio_map(const double* dose, const double* c0, const double* c
 __global__ void reset_work_claims_kernel(BeamStateDev* beam) {
     beam->workNext = 0;
     beam->workNextSmall = 0;
-    beam->workNextMid = 0;
     beam->workNextTiny = 0;
 }
 

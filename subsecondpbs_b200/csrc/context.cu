@@ -91,7 +91,7 @@ Context::~Context() {
     for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &ctQuad, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
-                      &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad, &rbarBuf,
+                      &nucCodes, &nucWork, &nucBev, &bevFixed, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad, &rbarBuf,
                       &gradInterm, &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         b->release();
     staging.release();
@@ -736,13 +736,14 @@ BeamBuffers beam_buffers(const BeamPlan& P, size_t nSubspotData, int nuclear, lo
         z.nucLs = L * sizeof(LayerStateDev);
         z.nucBs = sizeof(BeamStateDev);
     }
+    z.bevFixed = std::max(z.bev, z.nucBev) * 2;
     return z;
 }
 
 size_t BeamBuffers::total(bool withTrace) const {
     return (withTrace ? dens + wepl + weplMin + firstIn + firstOut : 0) + rayW + bev + codes + work + idd + rs +
            firstPassive + lp + ls + bs + lattice + interm + subspots + cpb + rayToNuc + nucIdd + nucRs + nucCodes +
-           nucWork + nucBev + nucLs + nucBs;
+           nucWork + nucBev + nucLs + nucBs + bevFixed;
 }
 
 size_t trace_bytes(size_t steps, size_t rays) {
@@ -755,7 +756,7 @@ void Context::use_stream_ordered_allocation() {
     for (DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &ctQuad, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                       &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive, &codes,
                       &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf, &nucRsBuf,
-                      &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm,
+                      &nucCodes, &nucWork, &nucBev, &bevFixed, &nucLs, &nucBs, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm,
                       &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         if (!b->ptr) b->allocStream = stream;
 }
@@ -765,7 +766,7 @@ size_t Context::device_bytes() const {
     for (const DevBuf* b : {&cidd, &density, &sp, &rrl, &ct, &ctQuad, &dose64, &dens, &wepl, &weplMin, &rayW, &interm, &lattice,
                             &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive,
                             &codes, &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf,
-                            &nucRsBuf, &nucCodes, &nucWork, &nucBev, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
+                            &nucRsBuf, &nucCodes, &nucWork, &nucBev, &bevFixed, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
                             &rbarBuf, &gradInterm, &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         n += b->bytes;
     return n;
@@ -775,7 +776,7 @@ void Context::release_beam_buffers() {
     join_side_work();
     for (DevBuf* b : {&dens, &wepl, &weplMin, &rayW, &interm, &lattice, &iddBuf, &rsBuf, &bev, &cpb, &subspots,
                       &floatOut, &firstIn, &firstOut, &firstPassive, &codes, &work, &rayToNuc, &nucIddBuf, &nucRsBuf,
-                      &nucCodes, &nucWork, &nucBev, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64,
+                      &nucCodes, &nucWork, &nucBev, &bevFixed, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64,
                       &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
         b->release();
     hasDose = false;
@@ -969,7 +970,12 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     const size_t S = size_t(P.tracerSteps);
     const size_t tiles = size_t(g.tilesX) * g.tilesY;
     const BeamBuffers z = beam_buffers(P, b.n_subspot_data, nuclear, layerBudgetMiB);
-    const int chunk = z.chunk;
+    // The reference transfers every layer on its own, with the box of that layer's
+    // steps [first, calcPassive) (wrapper.cu:5343-5505). With its BEV depth indexing
+    // (compat) a layer's dose lands deeper than its own steps and that box cuts it
+    // off, so in that mode the layers are superposed and transferred one at a time.
+    const bool perLayerTransfer = compatBevZShift && !adj;
+    const int chunk = perLayerTransfer ? 1 : z.chunk;
     chunkLayers = chunk;
 
     // The trace's home: the store's resident copy for this geometry, else the
@@ -998,8 +1004,21 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
          (rc = nucCodes.ensure(z.nucCodes)) || (rc = nucWork.ensure(z.nucWork)) || (rc = nucBev.ensure(z.nucBev)) ||
          (rc = nucLs.ensure(z.nucLs)) || (rc = nucBs.ensure(z.nucBs))))
         return rc;
+    if (!adj) {
+        const size_t had = bevFixed.bytes;
+        if ((rc = bevFixed.ensure(z.bevFixed))) return rc;
+        if (bevFixed.bytes != had || !bevFixedClean) {
+            PBS_CUDA(cudaMemsetAsync(bevFixed.ptr, 0, bevFixed.bytes, stream), "memset fixed BEV");
+            bevFixedClean = true;
+        }
+    }
     if (idd_smem_bytes(g, luts) > size_t(200) * 1024) {
         set_error("beam needs " + std::to_string(P.tracerSteps) + " tracer steps; at most ~3000 are supported");
+        return PBS_ERR_UNSUPPORTED;
+    }
+    if (adj && compatBevZShift) {
+        // The forward of that mode transfers each layer with its own box.
+        set_error("adjoint: not available with PBS_OPT_COMPAT_BEV_Z_SHIFT");
         return PBS_ERR_UNSUPPORTED;
     }
     if (adj && (chunk < L || nuclear || !P.hasLattice)) {
@@ -1008,6 +1027,10 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         return PBS_ERR_UNSUPPORTED;
     }
     if (keepDebug && chunk < L) {
+        if (perLayerTransfer) {
+            set_error("PBS_OPT_KEEP_DEBUG with PBS_OPT_COMPAT_BEV_Z_SHIFT needs a beam of one layer");
+            return PBS_ERR_UNSUPPORTED;
+        }
         set_error("PBS_OPT_KEEP_DEBUG needs every layer of the beam in one chunk; raise PBS_OPT_LAYER_BUDGET_MIB");
         return PBS_ERR_OUT_OF_MEMORY;
     }
@@ -1203,6 +1226,52 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     LayerStateDev* dNucLs = static_cast<LayerStateDev*>(nucLs.ptr);
     BeamStateDev* dNucBs = static_cast<BeamStateDev*>(nucBs.ptr);
     if ((rc = join_side_work())) return rc;
+    // BEV -> dose: the box over the steps of every layer, or of `layer` (and of
+    // `nucLayer` for the halo) alone; the dose grid's pending initialisation and
+    // dirty box are settled before the first transfer.
+    bool doseReady = false;
+    auto transfer_layers = [&](const LayerStateDev* layer, const LayerStateDev* nucLayer) -> int {
+        int trc;
+        if (!doseReady) {
+            if ((trc = flush_dose_init())) return trc;
+            if (doseBoxed) {
+                int lo[3], hi[3];
+                dose_transfer_box(plan.rayIdxToDoseIdx, plan.superpDims[0], plan.superpDims[1], plan.tracerSteps,
+                                  doseGrid.dims, lo, hi);
+                mark_dose_written(lo, hi);
+                if (nuclear) {
+                    dose_transfer_box(nucGeom.rayIdxToDoseIdx, nucGeom.pitchX, nucGeom.pitchY, plan.tracerSteps,
+                                      doseGrid.dims, lo, hi);
+                    mark_dose_written(lo, hi);
+                }
+            }
+            doseReady = true;
+        }
+        PBS_CUDA(launch_transfer_planner(g, dbs, layer, stream), "transfer_planner");
+        PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
+        if (bio) {
+            // The beam's own dose and the channels into the biological accumulators.
+            const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
+            const size_t bevN = S * size_t(g.bevX) * g.bevY;
+            double* acc = static_cast<double*>(bioAcc.ptr);
+            PBS_CUDA(launch_transfer(g, dBev, dbs, acc, stream), "bio transfer");
+            const int nCh = bioModel == PBS_BIO_LQ ? 3 : 2;
+            for (int slot = 0; slot < nCh; ++slot) {
+                // Slots are channels 0, 1, 2 (LQ) or 0, 2 (MKM); accumulator c + 1.
+                const int c = bioModel == PBS_BIO_LQ ? slot : (slot == 0 ? 0 : 2);
+                PBS_CUDA(launch_transfer(g, static_cast<const float*>(bioBev.ptr) + size_t(slot) * bevN, dbs,
+                                         acc + size_t(c + 1) * n, stream),
+                         "bio transfer");
+            }
+        }
+        if (nuclear) {
+            PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, nucLayer, stream), "nuc_transfer_planner");
+            PBS_CUDA(launch_transfer(nucGeom, static_cast<const float*>(nucBev.ptr), dNucBs,
+                                     static_cast<double*>(dose64.ptr), stream),
+                     "nuc_transfer");
+        }
+        return PBS_OK;
+    };
     for (int l0 = 0; l0 < L; l0 += chunk) {
         const int nl = std::min(chunk, L - l0);
         if (nuclear) PBS_CUDA(launch_nuc_prepare(nucGeom, nl, dNucIdd, dNucRs, stream), "nuc_prepare");
@@ -1214,24 +1283,26 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
                  "idd");
         if (l0 == 0 && (rc = mark(4))) return rc;
         PBS_CUDA(launch_bin_plan(g, l0, nl, static_cast<const uint8_t*>(codes.ptr), dls, dbs,
-                                 static_cast<int4*>(work.ptr), workCap, nullptr, nullptr, stream),
+                                 static_cast<int4*>(work.ptr), workCap, adj == nullptr, nullptr, nullptr, stream),
                  "bin_plan");
         if (nuclear) {
             PBS_CUDA(launch_nuc_codes(nucGeom, l0, nl, dNucIdd, dNucRs, dls, dbs, dNucLs,
                                       static_cast<uint8_t*>(nucCodes.ptr), stream),
                      "nuc_codes");
             PBS_CUDA(launch_bin_plan(nucGeom, l0, nl, static_cast<const uint8_t*>(nucCodes.ptr), dNucLs, dNucBs,
-                                     static_cast<int4*>(nucWork.ptr), nucWorkCap, dls, dbs, stream),
+                                     static_cast<int4*>(nucWork.ptr), nucWorkCap, adj == nullptr, dls, dbs, stream),
                      "nuc_bin_plan");
         }
         if (l0 == 0 && (rc = mark(5))) return rc;
         if (adj) break;  // the adjoint's superposition runs after the transfer box is known
+        unsigned long long* dFixed = static_cast<unsigned long long*>(bevFixed.ptr);
+        bevFixedClean = false;
         PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
-                                  static_cast<const int4*>(work.ptr), dbs, dBev, smCount, stream),
+                                  static_cast<const int4*>(work.ptr), dbs, dBev, dFixed, 0, smCount, stream),
                  "superpose");
         if (nuclear)
             PBS_CUDA(launch_superpose(nucGeom, dNucIdd, dNucRs, static_cast<const int4*>(nucWork.ptr), dNucBs,
-                                      static_cast<float*>(nucBev.ptr), smCount, stream),
+                                      static_cast<float*>(nucBev.ptr), dFixed, 0, smCount, stream),
                      "nuc_superpose");
         if (bio) {
             // Every biological channel: the IDD scaled by the channel's factor,
@@ -1248,59 +1319,49 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
                 PBS_CUDA(launch_reset_work_claims(dbs, stream), "reset work claims");
                 PBS_CUDA(launch_superpose(g, static_cast<const float*>(bioIdd.ptr),
                                           static_cast<const float*>(rsBuf.ptr), static_cast<const int4*>(work.ptr),
-                                          dbs, static_cast<float*>(bioBev.ptr) + size_t(slot) * bevN, smCount, stream),
+                                          dbs, static_cast<float*>(bioBev.ptr) + size_t(slot) * bevN, dFixed,
+                                          bioShiftOffset[c], smCount, stream),
                          "bio_superpose");
                 ++slot;
             }
         }
+        bevFixedClean = true;
+        if (perLayerTransfer) {
+            // This layer alone, then empty BEV volumes for the next one (the last
+            // layer's BEV stays for the debug readouts).
+            if ((rc = transfer_layers(dls + l0, nuclear ? dNucLs + l0 : nullptr))) return rc;
+        }
+        if (perLayerTransfer && l0 + nl < L) {
+            PBS_CUDA(cudaMemsetAsync(dBev, 0, S * size_t(g.bevX) * g.bevY * 4, stream), "memset BEV");
+            if (nuclear)
+                PBS_CUDA(cudaMemsetAsync(nucBev.ptr, 0, S * size_t(nucGeom.bevX) * nucGeom.bevY * 4, stream),
+                         "memset BEV");
+            if (bio)
+                PBS_CUDA(cudaMemsetAsync(bioBev.ptr, 0,
+                                         size_t(bioModel == PBS_BIO_LQ ? 3 : 2) * S * size_t(g.bevX) * g.bevY * 4,
+                                         stream),
+                         "memset BEV");
+        }
     }
     if ((rc = mark(6))) return rc;
     if (adj) return finish_adjoint(*adj, b);
-    if ((rc = flush_dose_init())) return rc;
-    if (doseBoxed) {
-        int lo[3], hi[3];
-        dose_transfer_box(plan.rayIdxToDoseIdx, plan.superpDims[0], plan.superpDims[1], plan.tracerSteps,
-                          doseGrid.dims, lo, hi);
-        mark_dose_written(lo, hi);
-        if (nuclear) {
-            dose_transfer_box(nucGeom.rayIdxToDoseIdx, nucGeom.pitchX, nucGeom.pitchY, plan.tracerSteps,
-                              doseGrid.dims, lo, hi);
-            mark_dose_written(lo, hi);
-        }
-    }
-    PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
-    PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
-    if (bio) {
-        // The beam's own dose and the channels into the biological accumulators.
-        const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
-        const size_t bevN = S * size_t(g.bevX) * g.bevY;
-        double* acc = static_cast<double*>(bioAcc.ptr);
-        PBS_CUDA(launch_transfer(g, dBev, dbs, acc, stream), "bio transfer");
-        const int nCh = bioModel == PBS_BIO_LQ ? 3 : 2;
-        for (int slot = 0; slot < nCh; ++slot) {
-            // Slots are channels 0, 1, 2 (LQ) or 0, 2 (MKM); accumulator c + 1.
-            const int c = bioModel == PBS_BIO_LQ ? slot : (slot == 0 ? 0 : 2);
-            PBS_CUDA(launch_transfer(g, static_cast<const float*>(bioBev.ptr) + size_t(slot) * bevN, dbs,
-                                     acc + size_t(c + 1) * n, stream),
-                     "bio transfer");
-        }
-    }
-    if (nuclear) {
-        PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, stream), "nuc_transfer_planner");
-        PBS_CUDA(launch_transfer(nucGeom, static_cast<const float*>(nucBev.ptr), dNucBs,
-                                 static_cast<double*>(dose64.ptr), stream),
-                 "nuc_transfer");
-    }
+    if (!perLayerTransfer && (rc = transfer_layers(nullptr, nullptr))) return rc;
     if ((rc = mark(7))) return rc;
     lastChunks = (L + chunk - 1) / chunk;
-    // trace, planner, two fluence kernels, six per chunk (IDD, layer plan, work
-    // scatter, three superposition ranges), transfer planner, transfer; the halo
-    // adds seven per chunk (clear, codes, layer plan, scatter, three superposition
-    // ranges) and its transfer planner and transfer.
-    lastLaunches = 6 + 6 * lastChunks + (nuclear ? 7 * lastChunks + 2 : 0);
-    // The biological channels: per chunk and channel, the scaling, a claim reset and
-    // four superposition ranges; then one transfer per accumulator.
-    if (bio) lastLaunches += (bioModel == PBS_BIO_LQ ? 3 : 2) * 6 * lastChunks + (bioModel == PBS_BIO_LQ ? 4 : 3);
+    // trace, planner, two fluence kernels, seven per chunk (IDD, layer plan, work
+    // list, three superposition ranges, fixed-point write-out), and per transfer (one,
+    // or one per layer in the per-layer mode) the transfer planner and transfer; the
+    // halo adds eight per chunk (clear, codes, layer plan, work list, three
+    // superposition ranges, write-out) and its own transfer planner and transfer.
+    const int transfers = perLayerTransfer ? lastChunks : 1;
+    lastLaunches = 4 + 7 * lastChunks + 2 * transfers + (nuclear ? 8 * lastChunks + 2 * transfers : 0);
+    // The biological channels: per chunk and channel, the scaling, a claim reset,
+    // three superposition ranges and the write-out; per transfer one transfer per
+    // accumulator.
+    if (bio) {
+        const int nCh = bioModel == PBS_BIO_LQ ? 3 : 2;
+        lastLaunches += nCh * 6 * lastChunks + (nCh + 1) * transfers;
+    }
     lastBeamValid = true;
     lastStageTimed = stageTiming != 0;
     return PBS_OK;
@@ -1318,7 +1379,7 @@ int Context::finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b) {
     if ((rc = bevGrad.ensure(bevN * 4)) || (rc = rbarBuf.ensure(L * rays * 4)) ||
         (rc = gradInterm.ensure(L * g.latNy * g.rayX * 4)) || (rc = gradLattice.ensure(latN * 4)))
         return rc;
-    PBS_CUDA(launch_transfer_planner(g, dbs, stream), "transfer_planner");
+    PBS_CUDA(launch_transfer_planner(g, dbs, nullptr, stream), "transfer_planner");
     PBS_CUDA(cudaMemsetAsync(bevGrad.ptr, 0, bevN * 4, stream), "memset");
     PBS_CUDA(cudaMemsetAsync(rbarBuf.ptr, 0, L * rays * 4, stream), "memset");
     PBS_CUDA(launch_transfer_adjoint(g, a.gradDose, dbs, static_cast<float*>(bevGrad.ptr), stream), "transfer_adjoint");
@@ -1805,6 +1866,16 @@ int Context::set_bio_model(const PbsBioModel* m) {
             return PBS_ERR_INVALID_ARGUMENT;
         }
     const size_t nLet = size_t(m->let_rows) * m->let_depths, nLq = size_t(m->n_lq);
+    auto finite = [](const float* p, size_t n) {
+        for (size_t i = 0; i < n; ++i)
+            if (!std::isfinite(p[i])) return false;
+        return true;
+    };
+    if (!finite(m->let_table, nLet) || (lq && (!finite(m->lq_alpha, nLq) || !finite(m->lq_beta, nLq))) ||
+        (mkm && !finite(m->z1d, nLq))) {
+        set_error("biological maps: a table holds a NaN or an infinity");
+        return PBS_ERR_INVALID_ARGUMENT;
+    }
     std::vector<float> host(nLet + 2 * nLq);
     std::memcpy(host.data(), m->let_table, nLet * 4);
     if (lq) {
@@ -1835,6 +1906,22 @@ int Context::set_bio_model(const PbsBioModel* m) {
     d.lqLogStep = m->lq_log_step;
     d.alpha0 = m->alpha0;
     d.beta0 = m->beta0;
+    // A channel scales the IDD by at most its table's largest factor f < 2^e: its
+    // fixed-point superposition runs e bits lower than the dose's.
+    auto largest = [](const float* p, size_t n) {
+        float v = 0.0f;
+        for (size_t i = 0; i < n; ++i) v = std::max(v, p[i]);
+        return v;
+    };
+    auto bits = [](float f) {
+        int e = 0;
+        std::frexp(f, &e);
+        return f > 0.0f ? -std::max(e, 0) : 0;
+    };
+    const float* lqHost = host.data() + nLet;
+    bioShiftOffset[0] = bits(largest(lqHost, nLq));
+    bioShiftOffset[1] = lq ? bits(std::sqrt(largest(lqHost + nLq, nLq))) : 0;
+    bioShiftOffset[2] = bits(largest(host.data(), nLet));
     bioLetEnergies.assign(m->let_energies, m->let_energies + m->let_rows);
     bioModel = m->model;
     return clear_bio();

@@ -40,6 +40,7 @@ struct BeamBuffers {
     size_t dens = 0, wepl = 0, weplMin = 0, firstIn = 0, firstOut = 0, rayW = 0, bev = 0, codes = 0, work = 0, idd = 0,
            rs = 0, firstPassive = 0, lp = 0, ls = 0, bs = 0, lattice = 0, interm = 0, subspots = 0, cpb = 0;
     size_t rayToNuc = 0, nucIdd = 0, nucRs = 0, nucCodes = 0, nucWork = 0, nucBev = 0, nucLs = 0, nucBs = 0;
+    size_t bevFixed = 0;  // int64 accumulator of the larger of the two BEV volumes
     size_t total(bool withTrace = true) const;
 };
 BeamBuffers beam_buffers(const BeamPlan& P, size_t nSubspotData, int nuclear, long long layerBudgetMiB);
@@ -130,6 +131,7 @@ struct Context {
     int bioModel = 0;
     BioDev bioDev{};
     std::vector<float> bioLetEnergies;
+    int bioShiftOffset[3] = {0, 0, 0};  // fixed-point exponent offset of channels 0, 1, 2
     DevBuf bioTables, bioLayerRow, bioIdd, bioBev, bioAcc;
     int set_bio_model(const PbsBioModel* m);
     int read_bio_map(int map, float* out, int onDevice);
@@ -158,6 +160,10 @@ struct Context {
     DevBuf firstIn, firstOut, firstPassive, codes, work, lp, ls, bs, stats;
     // Nuclear halo working set and the device word collecting error flags.
     DevBuf rayToNuc, nucIddBuf, nucRsBuf, nucCodes, nucWork, nucBev, nucLs, nucBs, errWord;
+    // Fixed-point superposition accumulator; zero between superpositions unless a
+    // run stopped between a superposition and its write-out (bevFixedClean false).
+    DevBuf bevFixed;
+    bool bevFixedClean = false;
     BeamGeomDev nucGeom{};
     bool lastNuclear = false;
     std::vector<float> layerSpotDist;

@@ -81,46 +81,4 @@ __device__ __forceinline__ void superposition_row(float rs, float (&e)[R + 1]) {
     }
 }
 
-// superposition_row with two k per packed FP32x2 instruction: the erf arguments
-// x_k, x_{k+1} and the factors E_k, E_{k+1} advance together, E_{k+2} = E_k
-// G_k G_{k+1} with G_k G_{k+1} = e^{-2 (2k+3) r^2}; the erf differences are scalar.
-template <int R>
-__device__ __forceinline__ void superposition_row_x2(float rs, float (&e)[R + 1]) {
-    constexpr float p = 0.3275911f;
-    constexpr float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
-                    a5 = 1.061405429f;
-    const float r2 = rs * rs;
-    const float step2 = __expf(-2.0f * r2);
-    const float s2 = step2 * step2, s3 = s2 * step2;
-    float2 E = make_float2(__expf(-0.25f * r2), 0.0f);
-    E.y = E.x * step2;
-    float2 M = make_float2(s3, s3 * s2);
-    const float2 s4 = make_float2(s2 * s2, s2 * s2);
-    float2 x = make_float2(0.5f * rs, 1.5f * rs);
-    const float2 dx = make_float2(2.0f * rs, 2.0f * rs);
-    const float2 one = make_float2(1.0f, 1.0f), pp = make_float2(p, p);
-    float fPrev = 0.0f;
-#pragma unroll
-    for (int k = 0; k <= R; k += 2) {
-        const float2 den = __ffma2_rn(pp, x, one);
-        const float2 t = make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
-        float2 poly = __ffma2_rn(t, make_float2(a5, a5), make_float2(a4, a4));
-        poly = __ffma2_rn(t, poly, make_float2(a3, a3));
-        poly = __ffma2_rn(t, poly, make_float2(a2, a2));
-        poly = __ffma2_rn(t, poly, make_float2(a1, a1));
-        poly = __fmul2_rn(t, poly);
-        const float2 f = __ffma2_rn(make_float2(-poly.x, -poly.y), E, one);
-        if (k == 0) {
-            e[0] = f.x;
-        } else {
-            e[k] = 0.5f * (f.x - fPrev);
-        }
-        if (k + 1 <= R) e[k + 1] = 0.5f * (f.y - f.x);
-        fPrev = f.y;
-        E = __fmul2_rn(E, M);
-        M = __fmul2_rn(M, s4);
-        x = __fadd2_rn(x, dx);
-    }
-}
-
 }  // namespace pbs

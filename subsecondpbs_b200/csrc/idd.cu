@@ -183,6 +183,7 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         nextSp = wepl[idx];
         nextDens = density[idx];
     }
+    float runMax = 0.0f;  // largest IDD of this ray (fixed-point range of the superposition)
     int stepNo = first;
     for (; stepNo < afterLastL; ++stepNo) {
         // Once no ray of the row is live, every later step is (0, +inf): the fill
@@ -294,6 +295,7 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
                 res *= fmaxf(0.0f, ow);
             }
         }
+        runMax = fmaxf(runMax, res);
         const int zr = stepNo - first;
         const size_t o = static_cast<size_t>(zr) * padPlane + static_cast<size_t>(y) * g.pitchX + x;
         iddL[o] = res;
@@ -328,6 +330,10 @@ idd_kernel(BeamGeomDev g, LutsDev luts, int layer0, const float* __restrict__ de
         partLive[zr * 8 + warp] = 0;
     }
 
+    {
+        const unsigned mb = __reduce_max_sync(0xffffffffu, __float_as_uint(fmaxf(runMax, 0.0f)));
+        if (lane == 0 && mb) atomicMax(&ls[l].maxIddBits, mb);
+    }
     int fp = real ? static_cast<int>(afterLast) : INT_MIN;
     if (real && firstPassiveOut) firstPassiveOut[static_cast<size_t>(lc) * rayPlane + ridx] = fp;
     for (int off = 16; off > 0; off >>= 1) fp = max(fp, __shfl_xor_sync(0xffffffffu, fp, off));
@@ -382,12 +388,12 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     __shared__ int sCalc[kMaxChunkLayers];
     __shared__ int sWarpSum[kMaxChunkLayers / 32];
     __shared__ long long sWarpFma[kMaxChunkLayers / 32];
-    __shared__ int sSplit[3];
+    __shared__ int sSplit[2];
     const int lc = threadIdx.x;
     const bool nuclear = primaryLs != nullptr;
     const int first = nuclear ? primaryBeam->firstInside : beam->firstInside;
     const int tiles = g.tilesX * g.tilesY;
-    if (lc < 3) sSplit[lc] = 0;
+    if (lc < 2) sSplit[lc] = 0;
     if (lc < nLayers) {
         LayerStateDev& st = ls[layer0 + lc];
         int hist[kBuckets];
@@ -475,14 +481,13 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     __syncthreads();
     int acc = incl - runSum;
     for (int w = 0; w < warp; ++w) acc += sWarpSum[w];
-    const int pSplit = (kMaxR - kSplitR) * nLayers, pSplit2 = (kMaxR - kSplitR2) * nLayers,
-              pSplit3 = (kMaxR - kSplitR3) * nLayers;
+    const int pSplit = (kMaxR - kSplitR) * nLayers, pSplit2 = (kMaxR - kSplitR2) * nLayers;
     for (int p = p0; p < p1; ++p) {
         const int r = kMaxR - p / nLayers, q = p % nLayers;
         if (p == pSplit) sSplit[0] = acc;
         if (p == pSplit2) sSplit[1] = acc;
-        if (p == pSplit3) sSplit[2] = acc;
         ls[layer0 + q].offR[r] = acc;
+        if (q == 0) beam->rStart[r] = acc;
         acc += sLive[q][r];
     }
     __syncthreads();
@@ -498,7 +503,7 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
             acc += sWarpSum[w];
             fma += sWarpFma[w];
         }
-        const int split = sSplit[0], split2 = sSplit[1], split3 = sSplit[2];
+        const int split = sSplit[0], split2 = sSplit[1];
         int mp = beam->maxCalcPassive;
         for (int q = 0; q < nLayers; ++q) mp = max(mp, sCalc[q]);
         beam->maxCalcPassive = mp;
@@ -512,8 +517,18 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         beam->workNextSmall = 0;
         beam->workSplit2 = min(split2, acc);
         beam->workNextTiny = 0;
-        beam->workSplit3 = min(split3, acc);
-        beam->workNextMid = 0;
+        for (int r = 0; r <= kMaxR; ++r) beam->mergedR[r] = 0;
+        // Fixed-point range of the chunk's BEV: a cell sums at most `acc` tile
+        // footprints (merged items sum several of them), each at most 256 x the
+        // largest IDD of the chunk, so with that IDD below 2^ex every cell stays below
+        // 2^(ex + 8 + ceil(log2 acc)); the shift puts that bound at 2^61.
+        unsigned mb = 0;
+        for (int q = 0; q < nLayers; ++q) mb = max(mb, ls[layer0 + q].maxIddBits);
+        int ex = 0;
+        frexpf(__uint_as_float(mb), &ex);
+        int lg = 0;
+        while ((1LL << lg) < static_cast<long long>(max(acc, 1))) ++lg;
+        beam->fixedShift = mb ? min(61 - ex - 8 - lg, 120) : 0;
         beam->liveTiles += acc;
         beam->superposeFma += fma;
     }
@@ -539,6 +554,68 @@ __global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, cons
         const int R = st.batchedR[c & 0x3f];
         const int slot = st.offR[R] + atomicAdd(&st.curR[R], 1);
         if (slot < workCapacity) work[slot] = make_int4(lc, rem - zr * tiles, zr, R);
+    }
+}
+
+// Appends a merged item to the block of its radius. Merging only joins items of one
+// radius, so the merged items of R fit in the block its unmerged items occupy.
+__device__ __forceinline__ void emit_merged(BeamStateDev* beam, int4* work, unsigned layers, int tile, int zr,
+                                            int R) {
+    const int begin = beam->rStart[R];
+    const int end = R > 0 ? beam->rStart[R - 1] : beam->workCount;
+    const int slot = begin + atomicAdd(&beam->mergedR[R], 1);
+    if (slot < end) work[slot] = make_int4(static_cast<int>(layers), tile, zr, R);
+}
+
+// The forward superposition's work list: one warp per (step, tile) of the chunk,
+// a lane per chunk layer (two passes for chunks of more than 32 layers), takes the
+// tile's live items at that step (the same items, radii and step ranges as
+// work_scatter_kernel) and groups the layers with equal batched radius, in layer
+// order, into items of up to kMergeLayers layers (x = the chunk layers as bytes,
+// 0xff: none); radii above kSplitR stay one layer per item. Each item goes to the
+// block of its radius (so the superposition's CTAs run one radius at a time); the
+// order within a block is arbitrary, and the superposition's fixed-point BEV makes
+// the dose independent of it.
+__global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restrict__ codes,
+                                  const LayerStateDev* __restrict__ ls, BeamStateDev* __restrict__ beam,
+                                  int4* __restrict__ work) {
+    const int lane = threadIdx.x & 31;
+    const int tiles = g.tilesX * g.tilesY;
+    const int first = beam->firstInside;
+    const size_t perLayer = static_cast<size_t>(g.steps) * tiles;
+    const size_t warps = (size_t(gridDim.x) * blockDim.x) >> 5;
+    for (size_t i = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5; i < perLayer; i += warps) {
+        const int zr = int(i / tiles);
+        const int tile = int(i - size_t(zr) * tiles);
+        for (int base = 0; base < nLayers; base += 32) {
+            const int lc = base + lane;
+            int R = -1;
+            if (lc < nLayers) {
+                const LayerStateDev& st = ls[layer0 + lc];
+                const int c = codes[size_t(lc) * perLayer + i];
+                if (zr < st.afterLast - first && (c & 0x80)) R = st.batchedR[c & 0x3f];
+            }
+            const bool merge = R >= 0 && R <= kSplitR;
+            const unsigned mergeLanes = __ballot_sync(0xffffffffu, merge);
+            if (R > kSplitR) emit_merged(beam, work, 0xffffff00u | unsigned(lc), tile, zr, R);
+            if (merge) {
+                // Lanes with this radius; every kMergeLayers-th of them (in lane
+                // order) writes the item of itself and the next ones.
+                const unsigned same = __match_any_sync(mergeLanes, R);
+                const unsigned below = (1u << lane) - 1u;
+                const int rank = __popc(same & below);
+                if (rank % kMergeLayers == 0) {
+                    unsigned layers = 0xffffffffu;
+                    unsigned rest = same & ~below;
+                    for (int n = 0; n < kMergeLayers && rest; ++n) {
+                        const int l = __ffs(rest) - 1;
+                        rest &= rest - 1u;
+                        layers = (layers & ~(0xffu << (8 * n))) | (unsigned(base + l) << (8 * n));
+                    }
+                    emit_merged(beam, work, layers, tile, zr, R);
+                }
+            }
+        }
     }
 }
 
@@ -575,13 +652,18 @@ __global__ void nuc_codes_kernel(BeamGeomDev gn, int layer0, int nLayers, const 
         const float* tr = rs + (ti - idd);
         unsigned key = 0xffffffffu;
         bool live = false;
+        float mx = 0.0f;
 #pragma unroll
         for (int r = 0; r < kTileY; ++r) {
             key = min(key, float_order_key(tr[size_t(r) * gn.pitchX]));
-            live |= ti[size_t(r) * gn.pitchX] > 0.0f;
+            const float v = ti[size_t(r) * gn.pitchX];
+            live |= v > 0.0f;
+            mx = fmaxf(mx, v);
         }
         key = __reduce_min_sync(0xffffffffu, key);
         live = __any_sync(0xffffffffu, live);
+        const unsigned mb = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
+        if (lane == 0 && mb) atomicMax(&nucLs[layer0 + lc].maxIddBits, mb);
         if (lane == 0) {
             const int R = tile_radius_bucket(float_from_order_key(key));
             codes[i] = static_cast<uint8_t>(R | (live ? 0x80 : 0));
@@ -633,14 +715,20 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
 }
 
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
-                            BeamStateDev* beam, int4* work, int workCapacity, const LayerStateDev* primaryLs,
-                            const BeamStateDev* primaryBeam, cudaStream_t s) {
+                            BeamStateDev* beam, int4* work, int workCapacity, bool merged,
+                            const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, cudaStream_t s) {
     if (nLayers > kMaxChunkLayers) return cudaErrorInvalidValue;
     layer_plan_kernel<<<1, kMaxChunkLayers, 0, s>>>(g, layer0, nLayers, ls, beam, workCapacity, primaryLs,
                                                     primaryBeam);
-    const size_t total = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY * nLayers;
-    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 8));
-    work_scatter_kernel<<<blocks, 256, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work, workCapacity);
+    if (merged) {
+        const size_t warps = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY;
+        const int blocks = int(std::min<size_t>((warps + 7) / 8, 148 * 16));
+        work_merge_kernel<<<blocks, 256, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work);
+    } else {
+        const size_t total = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY * nLayers;
+        const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 8));
+        work_scatter_kernel<<<blocks, 256, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work, workCapacity);
+    }
     return cudaGetLastError();
 }
 

@@ -80,10 +80,12 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
 // Histogram, overflow merge and batching (complete_superposition.cu:358-490) plus
 // the radius-sorted work list of live tiles. With primaryLs/primaryBeam set it
 // plans the nuclear halo grid `g` instead (no merge: a radius above 32 sets error
-// flag 4).
+// flag 4). `merged` selects the forward superposition's list (items of up to
+// kMergeLayers layers of one tile and step with one radius, x = the layers as bytes)
+// over the one-layer items {layer, tile, step, radius} the adjoint gathers from.
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
-                            BeamStateDev* beam, int4* work, int workCapacity, const LayerStateDev* primaryLs,
-                            const BeamStateDev* primaryBeam, cudaStream_t s);
+                            BeamStateDev* beam, int4* work, int workCapacity, bool merged,
+                            const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, cudaStream_t s);
 // Nuclear halo: clear the chunk's halo IDD (0) and sigma (+inf) before the IDD
 // kernel, and the halo tile codes and histograms after the primary layer plan.
 // `gn` is the halo grid (pitch = nucX x nucY).
@@ -93,13 +95,19 @@ cudaError_t launch_nuc_codes(const BeamGeomDev& gn, int layer0, int nLayers, con
                              uint8_t* codes, cudaStream_t s);
 // kernelSuperposition<R> (complete_superposition.cu:264-335) over the work list,
 // summing all layers into one BEV dose: three persistent launches (radii 16..32,
-// 8..15, 0..7) sized for `numSMs` multiprocessors.
+// 8..15, 0..7) sized for `numSMs` multiprocessors accumulate the chunk in
+// `bevFixed` (int64 fixed point at 2^(fixedShift + shiftOffset), all zero on entry),
+// and a fifth adds it to the float `bev` and clears it again. Integer adds commute,
+// so the BEV does not depend on the order in which tiles land.
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                             BeamStateDev* beam, float* bev, int numSMs, cudaStream_t s);
+                             BeamStateDev* beam, float* bev, unsigned long long* bevFixed, int shiftOffset,
+                             int numSMs, cudaStream_t s);
 
 // ---- BEV -> dose ---------------------------------------------------------------
-// Transfer bounding box and parameters (wrapper.cu:5343-5403).
-cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cudaStream_t s);
+// Transfer bounding box and parameters (wrapper.cu:5343-5403): over the steps of
+// every layer, or of `layer` alone (non-null).
+cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer,
+                                    cudaStream_t s);
 // primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44) accumulating in FP64.
 cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,
                             cudaStream_t s);

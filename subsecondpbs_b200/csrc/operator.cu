@@ -283,11 +283,38 @@ int Context::plan_columns(const PbsBeamDesc& beam, long long spotBegin, long lon
 // Dose of spot j alone at unit weight into the (zeroed) FP64 grid, with the box of
 // voxels it can have written.
 int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut) {
-    BeamPlan P = cp.base;
-    std::fill(P.lattice.weights.begin(), P.lattice.weights.end(), 0.0f);
+    // The column is the dose of spot j's layer alone: the other layers' weights are
+    // zero, so they add nothing, and every per-layer decision (steps, radii, work
+    // items) depends on the layer's own parameters and the beam's geometry only. The
+    // plan is cut down to that layer unless the biological or CarbonPBS profile
+    // models, which index the beam's layers, are on.
+    const size_t plane = static_cast<size_t>(cp.base.lattice.nx) * cp.base.lattice.ny;
+    int layer = -1;
+    for (int slot = 0; slot < 4; ++slot)
+        if (cp.cells[j * 4 + slot] >= 0) layer = static_cast<int>(cp.cells[j * 4 + slot] / plane);
+    const bool oneLayer = layer >= 0 && !bioModel && !carbonProfile;
+    BeamPlan P;
+    if (oneLayer) {
+        // Copy the plan without its per-layer vectors, then give it the one layer.
+        std::vector<float> weights;
+        std::vector<LayerHost> layers;
+        std::swap(cp.base.lattice.weights, weights);
+        std::swap(cp.base.layers, layers);
+        P = cp.base;
+        std::swap(cp.base.lattice.weights, weights);
+        std::swap(cp.base.layers, layers);
+        P.numLayers = 1;
+        P.layers.assign(1, cp.base.layers[static_cast<size_t>(layer)]);
+        P.lattice.nl = 1;
+        P.lattice.weights.assign(plane, 0.0f);
+    } else {
+        P = cp.base;
+        std::fill(P.lattice.weights.begin(), P.lattice.weights.end(), 0.0f);
+    }
+    const size_t cellBase = oneLayer ? static_cast<size_t>(layer) * plane : 0;
     for (int slot = 0; slot < 4; ++slot) {
         const int c = cp.cells[j * 4 + slot];
-        if (c >= 0) P.lattice.weights[static_cast<size_t>(c)] += cp.shares[j * 4 + slot];
+        if (c >= 0) P.lattice.weights[static_cast<size_t>(c) - cellBase] += cp.shares[j * 4 + slot];
     }
     if (int rc = reset_dose(nullptr, 0)) return rc;
     if (int rc = add_planned_beam(cp.beam, nuclear, std::move(P))) return rc;

@@ -30,9 +30,11 @@ namespace pbs {
 constexpr int kTileX = 32;               // SUPERP_TILE_X, include/core/Macro.cuh:65
 constexpr int kTileY = 8;                // SUPERP_TILE_Y, include/core/Macro.cuh:66
 constexpr int kMaxR = 32;                // MAX_SUPERP_RADIUS, include/core/Macro.cuh:64
-constexpr int kSplitR = 15;              // radii <= kSplitR run in the paired superposition instances
-constexpr int kSplitR3 = 11;             // radii kSplitR3 + 1 .. kSplitR: first paired instance; kSplitR2 + 1 .. kSplitR3: second
+constexpr int kSplitR = 15;              // radii <= kSplitR run in the medium and narrow superposition instances
 constexpr int kSplitR2 = 7;              // radii <= kSplitR2 run in the narrow instance
+// Up to kMergeLayers layers of one tile at one step with the same radius (<= kSplitR)
+// share one superposition item: their footprints land on the same BEV cells.
+constexpr int kMergeLayers = 4;
 constexpr int kMinTilesInBatch = 16;     // MIN_TILES_IN_BATCH, include/core/Macro.cuh:67
 constexpr float kBpDepthCutoff = 1.05f;  // BP_DEPTH_CUTOFF, include/core/Macro.cuh:46
 

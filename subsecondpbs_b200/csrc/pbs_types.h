@@ -41,6 +41,7 @@ struct LayerStateDev {
     int batchedCounts[33];
     int liveTiles;
     int histAll[kBuckets];      // histogram over [first, afterLast) accumulated by the IDD kernel
+    unsigned maxIddBits;        // bits of the layer's largest IDD value (non-negative floats order as ints)
     int liveHist[kBuckets];     // live tiles per raw bucket
     int liveR[33];              // live tiles per processing radius
     int offR[33];               // first work-list slot of this layer's radius-R items
@@ -57,16 +58,22 @@ struct BeamStateDev {
     int maxCalcPassive;
     int workCount;          // superposition work items of the current layer chunk
     // The radius-sorted work list holds the wide (R > kSplitR), medium
-    // (kSplitR3 < R <= kSplitR), medium-narrow (kSplitR2 < R <= kSplitR3) and
-    // narrow (R <= kSplitR2) items in that order; each range has its own claim
-    // counter (relative to the range start).
+    // (kSplitR2 < R <= kSplitR) and narrow (R <= kSplitR2) items in that order;
+    // each range has its own claim counter (relative to the range start).
     int workNext;
     int workSplit;          // items with R > kSplitR
     int workNextSmall;
     int workSplit2;         // items with R > kSplitR2
     int workNextTiny;
-    int workSplit3;         // items with R > kSplitR3
-    int workNextMid;
+    // The work list holds each radius R in one block, the wide radii first; block R
+    // starts at rStart[R] (layer_plan_kernel). The layer-merged list of the forward
+    // superposition (work_merge_kernel) keeps mergedR[R] items at the start of R's
+    // block, so the items of one radius stay together.
+    int rStart[kMaxR + 1];
+    int mergedR[kMaxR + 1];
+    // Fixed-point exponent of the chunk's BEV accumulation: a value v is added to the
+    // int64 BEV as v * 2^fixedShift. Every BEV cell stays below 2^62 (layer_plan_kernel).
+    int fixedShift;
     long long liveTiles;
     long long superposeFma;
     int transferStart[3];

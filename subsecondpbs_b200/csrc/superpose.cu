@@ -1,39 +1,43 @@
 // Tile-based Gaussian superposition of the per-ray IDD into the padded BEV dose.
 //
-// Work items come from the radius-sorted list built on the device; each item is one
-// 32x8 tile of source rays at one step of one layer with its batched radius R
-// (kernelSuperposition<R>, complete_superposition.cu:264-335). Every source s
-// spreads idd_s * e_s(dy) * e_s(dx) over a (2R+1)^2 footprint, where
+// Each work item is one 32x8 tile of source rays at one step with its batched radius
+// R (kernelSuperposition<R>, complete_superposition.cu:264-335), for one layer or,
+// for R <= kSplitR, for up to kMergeLayers layers whose tile has the same radius at
+// that step (their footprints land on the same BEV cells). Every source s spreads
+// idd_s * e_s(dy) * e_s(dx) over a (2R+1)^2 footprint, where
 // e_s(0) = erf(r/2) and e_s(k) = (erf((k+1/2) r) - erf((k-1/2) r)) / 2.
 //
-// Formulation on the FP32 FMA pipe (one CTA per tile, persistent grid):
-//   * table phase: each thread builds its source's rows e_s(0..R) (float4 chunks,
-//     chunk-major so that the stores and the broadcast reads are conflict-free)
-//     and idd_s * e_s(0..R) (odd row stride); sources without dose get zero rows;
+// Formulation on the FP32 FMA pipe (one CTA per item, persistent grid):
+//   * table phase (per layer of the item): each thread builds its source's rows
+//     e_s(0..R) (float4 chunks, chunk-major so that the stores and the broadcast
+//     reads are conflict-free) and idd_s * e_s(0..R) (odd row stride); sources
+//     without dose get zero rows;
 //   * accumulation phase: a warp lane is one column distance |d| of one source
-//     column; a source column's eight sources share the lane's output
-//     columns, so the lane keeps the whole footprint height (8+2R rows) in
-//     registers and adds idd_s e_s(|d|) * e_s(k) to rows sy+R+-k. The column at
-//     +d equals the one at -d, so up to radius 15 it is accumulated once and added
-//     to both: the FMAs and shared loads are (R+1)/(2R+1) of the direct (2R+1)^2
-//     formulation. Several source columns share one warp instruction; for radii
-//     16..32 a lane is one signed offset and the tile's (column, offset) pairs are
-//     dealt out 32 at a time. A pair ends with one
-//     shared-memory add per footprint row and output column; pairs whose source
-//     column has no depositing source are skipped;
+//     column (radii 0..15) or one signed offset (radii 16..32); a source column's
+//     eight sources share the lane's output columns, so the lane keeps the whole
+//     footprint height (8+2R rows) in registers and adds idd_s e_s(|d|) * e_s(k) to
+//     rows sy+R+-k. Up to radius 15 the column at +d, equal to the one at -d, is
+//     accumulated once and added to both: the FMAs and shared loads are
+//     (R+1)/(2R+1) of the direct (2R+1)^2 formulation. Several source columns share
+//     one warp instruction; for radii 16..32 the tile's (column, offset) pairs are
+//     dealt out 32 at a time. A pair ends with one shared-memory add per footprint
+//     row and output column; pairs whose source column has no depositing source are
+//     skipped;
 //   * the footprint accumulates in 32-bit fixed point: a float add to shared memory
 //     has no native instruction on this part (it is a compare-and-swap loop, a
 //     third of the throughput of an integer add), while the integer add is native
 //     and order-independent. Every footprint value and every partial sum of it is at
-//     most the tile's total dose (each e_s(k) <= 1 and each source adds to a row of
+//     most the item's total dose (each e_s(k) <= 1 and each source adds to a row of
 //     a pair once), so the power-of-two scale 2^30 / total keeps every sum inside
-//     int32 with a resolution of 2^-30 of the tile's dose, finer than FP32 near the
-//     footprint's peak;
-//   * the tile footprint is then added to the BEV dose of its step (all layers of
-//     the beam share one BEV volume).
-// Radii 16..32, 8..15 and 0..7 run as three instances of the kernel with 128, 48
-// and 32 registers and 96, 43 and 21 KB of shared memory: 2, 5 and 8 CTAs per SM
-// (the narrower instances trade a few spilled registers for occupancy).
+//     int32 with a resolution of 2^-30 of the item's dose;
+//   * the footprint of all the item's layers is then added to the BEV dose of its
+//     step (all layers of the beam share one BEV volume) in 64-bit fixed point: a
+//     BEV cell sums many items, and integer adds commute, so the dose does not depend
+//     on the order in which the items land. The chunk's exponent
+//     (layer_plan_kernel) bounds every cell below 2^62; a last pass adds the chunk
+//     to the float BEV and clears it.
+// Radii 16..32, 8..15 and 0..7 run as three persistent instances with 128, 48 and
+// 32 registers: 2, 5 and 8 CTAs per SM.
 #include "device_util.cuh"
 #include "kernels.h"
 #include "launch_util.h"
@@ -44,39 +48,59 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-// Resident CTAs per SM of the paired instances (radii 12..15, 8..11, 0..7).
-constexpr int kMidBlocks = 2;
-constexpr int kMidNarrowBlocks = 3;
-constexpr int kNarrowBlocks = 4;
-constexpr int kPairs = kTileX / 2;                 // column pairs per tile row
-constexpr int kPairSlots = kTileY * kPairs;        // (row, pair) slots per tile
 
-template <int RMax>
-struct Shape {
-    static constexpr int kQ = (RMax + 1 + 3) / 4;            // float4 chunks of e_s(k), k <= RMax
-    static constexpr int kEWStride = (RMax + 1) | 1;          // odd: lanes of one row hit distinct banks
-    static constexpr int kOutFloats = (kTileY + 2 * RMax) * (kTileX + 2 * RMax);
-    static constexpr size_t kSmemBytes =
-        (size_t(kQ) * kThreads * 4 + size_t(kThreads) * kEWStride + kOutFloats) * sizeof(float);
+// A footprint value q * 2^-sc as a BEV fixed-point value at 2^shift (truncated
+// below the BEV's resolution). q >= 0; the chunk's shift leaves headroom for items
+// of up to kMergeLayers tiles, so the result stays below 2^62.
+__device__ __forceinline__ unsigned long long to_bev_fixed(int q, int sc, int shift) {
+    const int e = shift - sc;
+    if (e >= 0) return static_cast<unsigned long long>(q) << min(e, 62);
+    return e > -63 ? static_cast<unsigned long long>(q) >> (-e) : 0ull;
+}
+
+// Fixed-point exponent of an item of total dose `total`: 2^(30 - ex) with
+// total < 2^ex, so total * 2^sc < 2^30.
+__device__ __forceinline__ int footprint_exponent(float total) {
+    int ex;
+    frexpf(total, &ex);
+    return min(30 - ex, 126);
+}
+
+// Adds the item's fixed-point footprint [H][Wo] to the BEV.
+template <int H, int Wo>
+__device__ __forceinline__ void write_footprint(const int* __restrict__ out, unsigned long long* __restrict__ dst,
+                                                int bevX, int sc, int shift) {
+    for (int i = threadIdx.x; i < H * Wo; i += kThreads) {
+        const int q = out[i];
+        const int oy = i / Wo, ox = i - oy * Wo;
+        if (q != 0) atomicAdd(dst + static_cast<size_t>(oy) * bevX + ox, to_bev_fixed(q, sc, shift));
+    }
+}
+
+struct ItemArgs {
+    const float* idd;
+    const float* rsig;
+    size_t layerStride;         // IDD elements per chunk layer
+    size_t src;                 // this thread's source ray within a layer
+    unsigned long long* dst;    // footprint origin in the fixed-point BEV dose
+    unsigned layers;            // chunk layers of the item, one per byte (0xff: none)
+    int bevX;
+    int shift;                  // BEV fixed-point exponent
 };
 
-// Paired layout (instances with radii up to kSplitR): the sources of source columns
-// 2p and 2p+1 (a column pair p) are stored interleaved, so that one 16-byte load
-// gives e(k) and e(k+1) of both columns as two register pairs and one 8-byte load
-// gives idd * e(d) of both; the accumulation then runs on packed FP32x2 FMAs, one
-// instruction per footprint row for the two columns.
+// ============================================================================
+// Radii 0..15: lanes over (source column, |d|) pairs, layer by layer of a merged
+// item into one fixed-point footprint.
+// ============================================================================
+
 template <int RMax>
 struct PairShape {
-    static constexpr int kQ2 = (RMax + 2) / 2;                // float4 = (e_a(k), e_b(k), e_a(k+1), e_b(k+1))
-    static constexpr int kEW2 = (RMax + 1) | 1;               // float2 stride per (row, pair), odd
+    static constexpr int kQ = (RMax + 1 + 3) / 4;            // float4 chunks of e_s(k), k <= RMax
+    static constexpr int kEWStride = (RMax + 1) | 1;          // odd: lanes of one row hit distinct banks
     static constexpr int kOutInts = (kTileY + 2 * RMax) * (kTileX + 2 * RMax);
     static constexpr size_t kSmemBytes =
-        size_t(kQ2) * kPairSlots * 16 + size_t(kPairSlots) * kEW2 * 8 + size_t(kOutInts) * 4;
+        (size_t(kQ) * kThreads * 4 + size_t(kThreads) * kEWStride + kOutInts) * sizeof(float);
 };
-
-// Slot of column pair p (0..15) within a source row: pairs 8 apart, read together by
-// the lane groups of one instruction, land in different banks.
-__device__ __forceinline__ int pair_slot(int p) { return p ^ ((p >> 3) & 1); }
 
 // Column part of the slot of source (sy, sx) in the chunk-major e_s table
 // (slot = sy * 32 + e4_col(sx)): the low bits are XORed with bits 3..4 so that
@@ -84,117 +108,107 @@ __device__ __forceinline__ int pair_slot(int p) { return p ^ ((p >> 3) & 1); }
 // instruction) land in different banks.
 __device__ __forceinline__ int e4_col(int sx) { return sx ^ ((sx >> 3) & 3); }
 
-struct TileArgs {
-    const float* idd;
-    const float* rsig;
-    float* bev;
-    size_t src;        // this thread's source ray in the IDD / rSigma arrays
-    float* dst;        // footprint origin in the BEV dose
-    int bevX;
-};
-
-// Table phase, accumulation phase and write-out of one tile at radius R.
 template <int R, int RMax>
-__device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* __restrict__ EW,
-                                               int* __restrict__ out, unsigned* __restrict__ sCol,
-                                               float* __restrict__ sSum, const TileArgs& a) {
+__device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __restrict__ EW, int* __restrict__ out,
+                                          unsigned* __restrict__ sCol, float* __restrict__ sSum,
+                                          const ItemArgs& a) {
     constexpr int H = kTileY + 2 * R;
     constexpr int Wo = kTileX + 2 * R;
     constexpr int Q = (R + 1 + 3) / 4;
-    constexpr int EWS = Shape<RMax>::kEWStride;
+    constexpr int EWS = PairShape<RMax>::kEWStride;
+    // A source column's footprint is the same column vector at offsets +d and -d (the
+    // weights depend on |d| only): one lane per (source column, |d|) pair adds it to
+    // both output columns. floor(32 / (R+1)) source columns, spaced so that their
+    // pairs fill distinct lanes, share one warp instruction.
+    constexpr int M = R + 1;
+    constexpr int G = 32 / M;                   // source columns per instruction
+    constexpr int S = (32 + G - 1) / G;         // column spacing
+    constexpr int kUnits = S;
     const int t = threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
 
-    // ---- table phase (complete_superposition.cu:298-307) --------------------
-    // Sources without dose get zero rows, so the accumulation needs no per-source
-    // test; sCol[sx] collects the depositing sources of every source column (one
-    // shared OR per depositing source) and sSum[sy] the dose of every source row.
+    // H and Wo are even and `out` is 16-byte aligned.
+    for (int i = t; i < H * Wo / 4; i += kThreads) reinterpret_cast<int4*>(out)[i] = make_int4(0, 0, 0, 0);
+    // Fixed-point scale from the dose of every layer of the item.
     {
-        const float dose = a.idd[a.src];
-        const bool live = dose > 0.0f;
-        if (live) atomicOr(&sCol[lane], 1u << warp);
-        float rowDose = live ? dose : 0.0f;
+        float rowDose = 0.0f;
+#pragma unroll 1
+        for (int j = 0; j < kMergeLayers; ++j) {
+            const unsigned lc = (a.layers >> (8 * j)) & 0xffu;
+            if (lc == 0xffu) break;
+            rowDose += fmaxf(a.idd[lc * a.layerStride + a.src], 0.0f);
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
         if (lane == 0) sSum[warp] = rowDose;
-        float e[4 * Q];
-        if (live) {
-            float row[R + 1];
-            superposition_row<R>(a.rsig[a.src], row);
-#pragma unroll
-            for (int k = 0; k <= R; ++k) {
-                e[k] = row[k];
-                EW[t * EWS + k] = dose * row[k];
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k <= R; ++k) {
-                e[k] = 0.0f;
-                EW[t * EWS + k] = 0.0f;
-            }
-        }
-#pragma unroll
-        for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
-        const int pt = warp * kTileX + e4_col(lane);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
-        // H and Wo are even and `out` is 16-byte aligned.
-        for (int i = t; i < H * Wo / 4; i += kThreads) reinterpret_cast<int4*>(out)[i] = make_int4(0, 0, 0, 0);
     }
     __syncthreads();
-
-    // Fixed-point scale: 2^(30 - ex) with total < 2^ex, so total * scale < 2^30.
     float total = 0.0f;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) total += sSum[w];
-    int ex;
-    frexpf(total, &ex);
-    const float scale = ldexpf(1.0f, min(30 - ex, 126));
-    const float invScale = 1.0f / scale;
+    const int sc = footprint_exponent(total);
+    const float scale = ldexpf(1.0f, sc);
 
-    // ---- accumulation phase --------------------------------------------------
-    {
-        // A source column's footprint is the same column vector at offsets +d and -d
-        // (the weights depend on |d| only). Up to radius kSplitR one lane per (source
-        // column, |d|) pair accumulates it once and adds it to both output columns;
-        // wider footprints keep one lane per signed offset (their doubled flushes
-        // cost more than the saved FMAs).
-        constexpr bool kMirror = R <= kSplitR;
-        constexpr int M = kMirror ? R + 1 : 2 * R + 1;             // pairs per source column
-        constexpr bool kGrouped = M <= 32;
-        constexpr int G = kGrouped ? 32 / M : 1;                   // source columns per instruction
-        constexpr int S = kGrouped ? (32 + G - 1) / G : 1;         // column spacing
-        // Otherwise the tile's 32 * M pairs are dealt out 32 per instruction.
-        constexpr int kPairs = kTileX * M;
-        constexpr int kUnits = kGrouped ? S : (kPairs + 31) / 32;
-        // Depositing sources of source column `lane`, as an 8-bit mask over sy.
-        const unsigned colBits = sCol[lane];
+#pragma unroll 1
+    for (int j = 0; j < kMergeLayers; ++j) {
+        const unsigned lc = (a.layers >> (8 * j)) & 0xffu;
+        if (lc == 0xffu) break;
+        // The layers alternate between two column-mask buffers: a buffer is cleared
+        // after the barrier that ends its layer's accumulation, and refilled two
+        // layers later.
+        unsigned* colMask = sCol + (j & 1) * kTileX;
+        // ---- table phase (complete_superposition.cu:298-307) ----------------
+        // Thread t is source (sy, sx) = (warp, lane): its rows e_s(0..R) in float4
+        // chunks (chunk-major) and idd_s e_s(0..R); sources without dose get zero
+        // rows, and colMask[sx] collects the depositing sources of every column.
+        {
+            const size_t src = lc * a.layerStride + a.src;
+            const float dose = a.idd[src];
+            const bool live = dose > 0.0f;
+            if (live) atomicOr(&colMask[lane], 1u << warp);
+            float e[4 * Q];
+            if (live) {
+                float row[R + 1];
+                superposition_row<R>(a.rsig[src], row);
+#pragma unroll
+                for (int k = 0; k <= R; ++k) {
+                    e[k] = row[k];
+                    EW[t * EWS + k] = dose * row[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k <= R; ++k) {
+                    e[k] = 0.0f;
+                    EW[t * EWS + k] = 0.0f;
+                }
+            }
+#pragma unroll
+            for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
+            const int pt = warp * kTileX + e4_col(lane);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
+        }
+        __syncthreads();
+
+        // ---- accumulation phase ---------------------------------------------
+        // Lanes outside the footprint read source column 0 and are never flushed;
+        // pairs whose source column has no depositing source are skipped.
+        const unsigned colBits = colMask[lane];
 #pragma unroll 1
         for (int u = warp; u < kUnits; u += kWarps) {
-            int sx, d;  // d: |d| when mirrored, else the signed offset
-            bool valid;
-            if (kGrouped) {
-                const int g = lane / M;
-                d = lane - g * M;
-                sx = u + g * S;
-                valid = g < G && sx < kTileX;
-            } else {
-                const int pr = u * 32 + lane;
-                sx = pr / M;
-                d = pr - sx * M;
-                valid = pr < kPairs;
-            }
-            if (!kMirror) d -= R;
+            const int g = lane / M;
+            int d = lane - g * M;
+            int sx = u + g * S;
+            const bool valid = g < G && sx < kTileX;
             if (!valid) {
                 sx = 0;
                 d = 0;
             }
-            const int ad = d < 0 ? -d : d;
             const unsigned colAll = __shfl_sync(0xffffffffu, colBits, sx);
             const unsigned colLive = valid ? colAll : 0u;
             if (!__any_sync(0xffffffffu, colLive != 0)) continue;
-            // Lanes outside the footprint read source column 0 and are never flushed.
-            const float* ewCol = EW + sx * EWS + ad;
+            const float* ewCol = EW + sx * EWS + d;
             const float4* eCol = E4 + e4_col(sx);
             float acc[H];
 #pragma unroll
@@ -221,275 +235,331 @@ __device__ __forceinline__ void superpose_tile(float4* __restrict__ E4, float* _
                 if (sy & 1) asm volatile("" ::: "memory");
             }
             if (colLive) {
-                int q[H];
+                int qv[H];
 #pragma unroll
-                for (int i = 0; i < H; ++i) q[i] = __float2int_rn(acc[i] * scale);
+                for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(acc[i] * scale);
                 int* col = out + sx + R + d;
 #pragma unroll
-                for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, q[i]);
-                if (kMirror && d > 0) {
+                for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
+                if (d > 0) {
                     col = out + sx + R - d;
 #pragma unroll
-                    for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, q[i]);
+                    for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
                 }
             }
         }
+        // The next layer's tables overwrite these.
+        __syncthreads();
+        if (t < kTileX) colMask[t] = 0;
     }
     __syncthreads();
 
     // ---- write-out -------------------------------------------------------------
-    // The column masks were last read before the barrier: clear them for the next tile.
-    if (t < kTileX) sCol[t] = 0;
-    for (int i = t; i < H * Wo; i += kThreads) {
-        const int q = out[i];
-        const int oy = i / Wo, ox = i - oy * Wo;
-        if (q != 0) atomicAdd(a.dst + static_cast<size_t>(oy) * a.bevX + ox, float(q) * invScale);
-    }
+    write_footprint<H, Wo>(out, a.dst, a.bevX, sc, a.shift);
 }
 
-// Paired variant of superpose_tile for radii up to kSplitR. A lane is one column
-// distance |d| of one column pair (2p, 2p+1): it keeps both columns' footprint
-// heights as register pairs and adds (idd_a e_a(d), idd_b e_b(d)) * (e_a(k), e_b(k))
-// to rows sy+R+-k with one packed FP32x2 FMA per row. The table phase, fixed-point
-// flush and write-out are those of superpose_tile.
+template <int R, int RHi, int RMax>
+__device__ __forceinline__ bool dispatch_pair(int r, float4* E4, float* EW, int* out, unsigned* sCol, float* sSum,
+                                              const ItemArgs& a) {
+    if (r == R) {
+        pair_item<R, RMax>(E4, EW, out, sCol, sSum, a);
+        return true;
+    }
+    if constexpr (R < RHi) return dispatch_pair<R + 1, RHi, RMax>(r, E4, EW, out, sCol, sSum, a);
+    return false;
+}
+
+// ============================================================================
+// Radii 16..32: one layer per item, lanes over (source column, signed offset).
+// ============================================================================
+
+template <int RMax>
+struct WideShape {
+    static constexpr int kQ = (RMax + 1 + 3) / 4;            // float4 chunks of e_s(k), k <= RMax
+    static constexpr int kEWStride = (RMax + 1) | 1;          // odd: lanes of one row hit distinct banks
+    static constexpr int kOutFloats = (kTileY + 2 * RMax) * (kTileX + 2 * RMax);
+    static constexpr size_t kSmemBytes =
+        (size_t(kQ) * kThreads * 4 + size_t(kThreads) * kEWStride + kOutFloats) * sizeof(float);
+};
+
 template <int R, int RMax>
-__device__ __forceinline__ void superpose_tile_paired(float4* __restrict__ E2, float2* __restrict__ EW2,
-                                                      int* __restrict__ out, unsigned* __restrict__ sCol,
-                                                      float* __restrict__ sSum, const TileArgs& a) {
+__device__ __forceinline__ void wide_item(float4* __restrict__ E4, float* __restrict__ EW, int* __restrict__ out,
+                                          unsigned* __restrict__ sCol, float* __restrict__ sSum,
+                                          const ItemArgs& a) {
     constexpr int H = kTileY + 2 * R;
     constexpr int Wo = kTileX + 2 * R;
-    constexpr int Q2 = (R + 2) / 2;
-    constexpr int EWS = PairShape<RMax>::kEW2;
+    constexpr int Q = (R + 1 + 3) / 4;
+    constexpr int EWS = WideShape<RMax>::kEWStride;
+    constexpr int M = 2 * R + 1;                 // signed offsets per source column
+    constexpr int kPairs = kTileX * M;
+    constexpr int kUnits = (kPairs + 31) / 32;
     const int t = threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
+    const size_t src = (a.layers & 0xffu) * a.layerStride + a.src;
 
-    // ---- table phase (complete_superposition.cu:298-307) --------------------
+    // ---- table phase ----------------------------------------------------------
     {
-        const float dose = a.idd[a.src];
+        const float dose = a.idd[src];
         const bool live = dose > 0.0f;
         if (live) atomicOr(&sCol[lane], 1u << warp);
         float rowDose = live ? dose : 0.0f;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
         if (lane == 0) sSum[warp] = rowDose;
-        float e[R + 1];
+        float e[4 * Q];
         if (live) {
-            superposition_row<R>(a.rsig[a.src], e);
+            float row[R + 1];
+            superposition_row<R>(a.rsig[src], row);
+#pragma unroll
+            for (int k = 0; k <= R; ++k) {
+                e[k] = row[k];
+                EW[t * EWS + k] = dose * row[k];
+            }
         } else {
 #pragma unroll
-            for (int k = 0; k <= R; ++k) e[k] = 0.0f;
+            for (int k = 0; k <= R; ++k) {
+                e[k] = 0.0f;
+                EW[t * EWS + k] = 0.0f;
+            }
         }
-        // This source is half h of column pair p: its e(k) goes to component
-        // (k & 1) * 2 + h of float4 k / 2 of its (row, pair) slot, its idd * e(k) to
-        // component h of float2 k of its (row, pair) row.
-        const int pr = lane >> 1, h = lane & 1;
-        float* e2 = reinterpret_cast<float*>(E2 + warp * kPairs + pair_slot(pr)) + h;
-        float* ew = reinterpret_cast<float*>(EW2 + (warp * kPairs + pr) * EWS) + h;
 #pragma unroll
-        for (int k = 0; k <= R; ++k) {
-            e2[(k >> 1) * kPairSlots * 4 + (k & 1) * 2] = e[k];
-            ew[2 * k] = dose * e[k];
-        }
-        if ((R & 1) == 0) e2[(R >> 1) * kPairSlots * 4 + 2] = 0.0f;  // k = R + 1 of the last float4
-        // H and Wo are even and `out` is 16-byte aligned.
+        for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
+        const int pt = warp * kTileX + e4_col(lane);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
         for (int i = t; i < H * Wo / 4; i += kThreads) reinterpret_cast<int4*>(out)[i] = make_int4(0, 0, 0, 0);
     }
     __syncthreads();
 
-    // Fixed-point scale: 2^(30 - ex) with total < 2^ex, so total * scale < 2^30.
     float total = 0.0f;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) total += sSum[w];
-    int ex;
-    frexpf(total, &ex);
-    const float scale = ldexpf(1.0f, min(30 - ex, 126));
-    const float invScale = 1.0f / scale;
+    const int sc = footprint_exponent(total);
+    const float scale = ldexpf(1.0f, sc);
 
-    // ---- accumulation phase --------------------------------------------------
-    {
-        constexpr int M = R + 1;                         // distances |d| per column pair
-        constexpr int G = (32 / M) < kPairs ? (32 / M) : kPairs;  // column pairs per instruction
-        constexpr int S = (kPairs + G - 1) / G;          // pair spacing = units per tile
-        const unsigned colBits = sCol[lane];
+    // ---- accumulation phase -----------------------------------------------------
+    const unsigned colBits = sCol[lane];
 #pragma unroll 1
-        for (int u = warp; u < S; u += kWarps) {
-            const int g = lane / M;
-            int d = lane - g * M;
-            int pr = u + g * S;
-            const bool valid = g < G && pr < kPairs;
-            if (!valid) {
-                pr = 0;
-                d = 0;
-            }
-            const unsigned colA = __shfl_sync(0xffffffffu, colBits, 2 * pr);
-            const unsigned colB = __shfl_sync(0xffffffffu, colBits, 2 * pr + 1);
-            const bool liveA = valid && colA != 0u, liveB = valid && colB != 0u;
-            if (!__any_sync(0xffffffffu, liveA || liveB)) continue;
-            // Lanes outside the footprint read pair 0 and are never flushed.
-            const float2* ewCol = EW2 + pr * EWS + d;
-            const float4* eCol = E2 + pair_slot(pr);
-            float2 acc[H];
+    for (int u = warp; u < kUnits; u += kWarps) {
+        const int pr = u * 32 + lane;
+        const bool valid = pr < kPairs;
+        int sx = pr / M;
+        int d = pr - sx * M - R;
+        if (!valid) {
+            sx = 0;
+            d = 0;
+        }
+        const int ad = d < 0 ? -d : d;
+        const unsigned colAll = __shfl_sync(0xffffffffu, colBits, sx);
+        const unsigned colLive = valid ? colAll : 0u;
+        if (!__any_sync(0xffffffffu, colLive != 0)) continue;
+        // Lanes outside the footprint read source column 0 and are never flushed.
+        const float* ewCol = EW + sx * EWS + ad;
+        const float4* eCol = E4 + e4_col(sx);
+        float acc[H];
 #pragma unroll
-            for (int i = 0; i < H; ++i) acc[i] = make_float2(0.0f, 0.0f);
+        for (int i = 0; i < H; ++i) acc[i] = 0.0f;
 #pragma unroll
-            for (int sy = 0; sy < kTileY; ++sy) {
-                const float2 w = ewCol[sy * kPairs * EWS];
+        for (int sy = 0; sy < kTileY; ++sy) {
+            const float w = ewCol[sy * kTileX * EWS];
 #pragma unroll
-                for (int q = 0; q < Q2; ++q) {
-                    const float4 v = eCol[q * kPairSlots + sy * kPairs];
-                    const float2 ev[2] = {make_float2(v.x, v.y), make_float2(v.z, v.w)};
+            for (int q = 0; q < Q; ++q) {
+                const float4 v = eCol[q * kThreads + sy * kTileX];
+                const float ev[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
-                        const int k = 2 * q + c;
-                        if (k <= R) {
-                            acc[sy + R + k] = __ffma2_rn(w, ev[c], acc[sy + R + k]);
-                            if (k > 0) acc[sy + R - k] = __ffma2_rn(w, ev[c], acc[sy + R - k]);
-                        }
+                for (int c = 0; c < 4; ++c) {
+                    const int k = 4 * q + c;
+                    if (k <= R) {
+                        acc[sy + R + k] = fmaf(w, ev[c], acc[sy + R + k]);
+                        if (k > 0) acc[sy + R - k] = fmaf(w, ev[c], acc[sy + R - k]);
                     }
                 }
-                if (sy & 1) asm volatile("" ::: "memory");
             }
-            if (liveA) {
-                int* col = out + 2 * pr + R + d;
+            if (sy & 1) asm volatile("" ::: "memory");
+        }
+        if (colLive) {
+            int* col = out + sx + R + d;
 #pragma unroll
-                for (int i = 0; i < H; ++i) {
-                    const int q = __float2int_rn(acc[i].x * scale);
-                    atomicAdd(col + i * Wo, q);
-                    if (d > 0) atomicAdd(col - 2 * d + i * Wo, q);
-                }
-            }
-            if (liveB) {
-                int* col = out + 2 * pr + 1 + R + d;
-#pragma unroll
-                for (int i = 0; i < H; ++i) {
-                    const int q = __float2int_rn(acc[i].y * scale);
-                    atomicAdd(col + i * Wo, q);
-                    if (d > 0) atomicAdd(col - 2 * d + i * Wo, q);
-                }
-            }
+            for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, __float2int_rn(acc[i] * scale));
         }
     }
     __syncthreads();
 
-    // ---- write-out -------------------------------------------------------------
+    // ---- write-out ---------------------------------------------------------------
     if (t < kTileX) sCol[t] = 0;
-    for (int i = t; i < H * Wo; i += kThreads) {
-        const int q = out[i];
-        const int oy = i / Wo, ox = i - oy * Wo;
-        if (q != 0) atomicAdd(a.dst + static_cast<size_t>(oy) * a.bevX + ox, float(q) * invScale);
-    }
+    write_footprint<H, Wo>(out, a.dst, a.bevX, sc, a.shift);
 }
 
-// Chain of compile-time radii RLo..RHi; returns false if r is outside it.
 template <int R, int RHi, int RMax>
-__device__ __forceinline__ bool dispatch_radius(int r, float4* E4, float* EW, int* out, unsigned* sCol,
-                                                float* sSum, const TileArgs& a) {
+__device__ __forceinline__ bool dispatch_wide(int r, float4* E4, float* EW, int* out, unsigned* sCol, float* sSum,
+                                              const ItemArgs& a) {
     if (r == R) {
-        if constexpr (RMax <= kSplitR)
-            superpose_tile_paired<R, RMax>(E4, reinterpret_cast<float2*>(EW), out, sCol, sSum, a);
-        else
-            superpose_tile<R, RMax>(E4, EW, out, sCol, sSum, a);
+        wide_item<R, RMax>(E4, EW, out, sCol, sSum, a);
         return true;
     }
-    if constexpr (R < RHi) return dispatch_radius<R + 1, RHi, RMax>(r, E4, EW, out, sCol, sSum, a);
+    if constexpr (R < RHi) return dispatch_wide<R + 1, RHi, RMax>(r, E4, EW, out, sCol, sSum, a);
     return false;
 }
 
-// Persistent CTA loop over the work items [begin, end) of radii RLo..RHi, claimed
-// one at a time through `counter` (the next claim is issued before the current
-// tile runs so that its latency is hidden).
-template <int RLo, int RHi, int MinBlocks>
+// ============================================================================
+// The persistent kernel.
+// ============================================================================
+
+// Radius blocks of an instance: claim c of the instance is item c of the
+// concatenated merged items of radii RHi, RHi - 1, ..., RLo.
+template <int RLo, int RHi>
+struct RadiusBlocks {
+    int start[RHi - RLo + 1];
+    int count[RHi - RLo + 1];
+    int total;
+};
+
+template <int RLo, int RHi>
+__device__ __forceinline__ void load_blocks(const BeamStateDev* beam, RadiusBlocks<RLo, RHi>& b) {
+    const int t = threadIdx.x;
+    if (t <= RHi - RLo) {
+        const int R = RHi - t;
+        const int end = R > 0 ? beam->rStart[R - 1] : beam->workCount;
+        b.start[t] = beam->rStart[R];
+        b.count[t] = max(min(beam->mergedR[R], end - beam->rStart[R]), 0);
+    }
+    __syncthreads();
+    if (t == 0) {
+        int n = 0;
+        for (int i = 0; i <= RHi - RLo; ++i) n += b.count[i];
+        b.total = n;
+    }
+}
+
+template <int RLo, int RHi>
+__device__ __forceinline__ int block_slot(const RadiusBlocks<RLo, RHi>& b, int c) {
+#pragma unroll 1
+    for (int i = 0; i <= RHi - RLo; ++i) {
+        if (c < b.count[i]) return b.start[i] + c;
+        c -= b.count[i];
+    }
+    return -1;
+}
+
+// Persistent CTA loop over the merged items of radii RLo..RHi, claimed one at a
+// time through the range's counter (the next claim is issued before the current
+// item runs so that its latency is hidden). Items are taken radius block by radius
+// block, so the CTAs of the SM mostly run the code of one radius at a time.
+template <bool kWide, int RLo, int RHi, int MinBlocks>
 __global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
-                 const int4* __restrict__ work, BeamStateDev* __restrict__ beam, float* __restrict__ bev, int range) {
+                 const int4* __restrict__ work, BeamStateDev* __restrict__ beam, unsigned long long* __restrict__ bev,
+                 int shiftOffset, int range) {
     extern __shared__ __align__(16) float sm[];
-    constexpr bool kPaired = RHi <= kSplitR;
-    // Wide radii: E4 = [Q][256] e_s(4q..4q+3) at slot sy*32+e4_col(sx), EW = [256][EWS]
-    // idd_s e_s(k). Paired radii: E4 = [Q2][128] pair float4s at slot sy*16+pair_slot(p),
-    // EW = [128][EW2] float2 (idd_a e_a(k), idd_b e_b(k)). Then the [8+2R][32+2R]
-    // fixed-point footprint.
-    constexpr size_t kE4Floats = kPaired ? size_t(PairShape<RHi>::kQ2) * kPairSlots * 4
-                                         : size_t(Shape<RHi>::kQ) * kThreads * 4;
-    constexpr size_t kEWFloats = kPaired ? size_t(kPairSlots) * PairShape<RHi>::kEW2 * 2
-                                         : size_t(kThreads) * Shape<RHi>::kEWStride;
-    float4* E4 = reinterpret_cast<float4*>(sm);
-    float* EW = sm + kE4Floats;
-    int* out = reinterpret_cast<int*>(EW + kEWFloats);
     __shared__ int sItem[2];
-    __shared__ unsigned sCol[kTileX];     // per source column: depositing sources over sy
+    // Per source column, its depositing sources over sy (radii 0..15: two buffers).
+    __shared__ unsigned sCol[2 * kTileX];
     __shared__ float sSum[kTileY];
+    __shared__ RadiusBlocks<RLo, RHi> sBlocks;
 
     const int t = threadIdx.x;
-    // Range 0: R > kSplitR, 1: kSplitR3 < R <= kSplitR, 3: kSplitR2 < R <= kSplitR3,
-    // 2: R <= kSplitR2 (the work list holds them in the order 0, 1, 3, 2).
-    int begin, end, *counter;
-    if (range == 0) {
-        begin = 0, end = beam->workSplit, counter = &beam->workNext;
-    } else if (range == 1) {
-        begin = beam->workSplit, end = beam->workSplit3, counter = &beam->workNextSmall;
-    } else if (range == 3) {
-        begin = beam->workSplit3, end = beam->workSplit2, counter = &beam->workNextMid;
-    } else {
-        begin = beam->workSplit2, end = beam->workCount, counter = &beam->workNextTiny;
-    }
+    // Range 0: R > kSplitR, 1: kSplitR2 < R <= kSplitR, 2: R <= kSplitR2.
+    int* counter = range == 0 ? &beam->workNext : (range == 1 ? &beam->workNextSmall : &beam->workNextTiny);
     const size_t padPlane = static_cast<size_t>(g.pitchX) * g.pitchY;
-    const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
     const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
 
+    load_blocks<RLo, RHi>(beam, sBlocks);
     if (t == 0) sItem[0] = atomicAdd(counter, 1);
-    if (t < kTileX) sCol[t] = 0;
+    if (t < 2 * kTileX) sCol[t] = 0;
+    if (t < kTileY) sSum[t] = 0.0f;
     __syncthreads();
+    ItemArgs a;
+    a.idd = idd;
+    a.rsig = rsig;
+    a.layerStride = static_cast<size_t>(g.steps) * padPlane;
+    a.bevX = g.bevX;
+    a.shift = beam->fixedShift + shiftOffset;
     int buf = 0;
     for (;;) {
-        const int w = begin + sItem[buf];
-        if (w >= end) break;
+        const int c = sItem[buf];
+        if (c >= sBlocks.total) break;
         if (t == 0) sItem[buf ^ 1] = atomicAdd(counter, 1);
-        const int4 it = work[w];
-        const int lc = it.x, tile = it.y, zRel = it.z, R = it.w;
+        const int4 it = work[block_slot<RLo, RHi>(sBlocks, c)];
+        const int tile = it.y, zRel = it.z, R = it.w;
         const int tx = tile % g.tilesX, ty = tile / g.tilesX;
-        TileArgs a;
-        a.idd = idd;
-        a.rsig = rsig;
-        a.bev = bev;
-        a.src = lc * layerStride + zRel * padPlane + static_cast<size_t>(ty * kTileY + (t >> 5)) * g.pitchX +
-                tx * kTileX + (t & 31);
+        a.layers = static_cast<unsigned>(it.x);
+        a.src = zRel * padPlane + static_cast<size_t>(ty * kTileY + (t >> 5)) * g.pitchX + tx * kTileX + (t & 31);
         a.dst = bev + static_cast<size_t>(zRel) * bevPlane + static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX +
                 (tx * kTileX - R + kMaxR);
-        a.bevX = g.bevX;
-        if (!dispatch_radius<RLo, RHi, RHi>(R, E4, EW, out, sCol, sSum, a)) {
-            if (t == 0) atomicOr(&beam->errorFlags, 2);
+        bool ok;
+        if constexpr (kWide) {
+            float4* E4 = reinterpret_cast<float4*>(sm);                                       // [Q][256] e_s(4q..4q+3)
+            float* EW = sm + WideShape<RHi>::kQ * kThreads * 4;                               // [256][EWS] idd_s e_s(k)
+            int* out = reinterpret_cast<int*>(EW + kThreads * WideShape<RHi>::kEWStride);   // [8+2R][32+2R]
+            ok = dispatch_wide<RLo, RHi, RHi>(R, E4, EW, out, sCol, sSum, a);
+        } else {
+            float4* E4 = reinterpret_cast<float4*>(sm);                                       // [Q][256] e_s(4q..4q+3)
+            float* EW = sm + PairShape<RHi>::kQ * kThreads * 4;                               // [256][EWS] idd_s e_s(k)
+            int* out = reinterpret_cast<int*>(EW + kThreads * PairShape<RHi>::kEWStride);   // [8+2R][32+2R]
+            ok = dispatch_pair<RLo, RHi, RHi>(R, E4, EW, out, sCol, sSum, a);
         }
-        // Every thread is past the tile (and has read sItem[buf]) before the
-        // next claim lands in that slot.
+        if (!ok && t == 0) atomicOr(&beam->errorFlags, 2);
+        // Every thread is past the item (and has read sItem[buf]) before the next
+        // claim lands in that slot.
         __syncthreads();
         buf ^= 1;
     }
 }
 
-template <int RLo, int RHi, int MinBlocks>
+template <bool kWide, int RLo, int RHi, int MinBlocks>
 cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                         BeamStateDev* beam, float* bev, int gridBlocks, int range, cudaStream_t s) {
-    auto k = superpose_kernel<RLo, RHi, MinBlocks>;
-    const size_t smem = RHi <= kSplitR ? PairShape<RHi>::kSmemBytes : Shape<RHi>::kSmemBytes;
+                         BeamStateDev* beam, unsigned long long* bev, int shiftOffset, int gridBlocks, int range,
+                         cudaStream_t s) {
+    auto k = superpose_kernel<kWide, RLo, RHi, MinBlocks>;
+    const size_t smem = kWide ? WideShape<RHi>::kSmemBytes : PairShape<RHi>::kSmemBytes;
     cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
-    k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, range);
+    k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, shiftOffset, range);
     return cudaGetLastError();
 }
+
+// Adds the fixed-point BEV of the chunk (the planes written so far,
+// [0, maxCalcPassive - firstInside)) to the float BEV and clears it for the next
+// superposition. Every cell is converted once, so the float BEV is the same on
+// every run.
+__global__ void __launch_bounds__(256) bev_fixed_to_float_kernel(BeamGeomDev g, const BeamStateDev* __restrict__ beam,
+                                                                 unsigned long long* __restrict__ fixed,
+                                                                 float* __restrict__ bev, int shiftOffset) {
+    const int planes = min(beam->maxCalcPassive - beam->firstInside, g.steps);
+    if (planes <= 0) return;
+    const size_t n = static_cast<size_t>(planes) * g.bevX * g.bevY;
+    const int shift = beam->fixedShift + shiftOffset;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const unsigned long long v = fixed[i];
+        if (v) {
+            bev[i] += float(ldexp(double(v), -shift));
+            fixed[i] = 0ull;
+        }
+    }
+}
+
+// Resident CTAs per SM of the instances.
+constexpr int kWideBlocks = 2;
+constexpr int kMidBlocks = 5;
+constexpr int kNarrowBlocks = 8;
 
 }  // namespace
 
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
-                             BeamStateDev* beam, float* bev, int numSMs, cudaStream_t s) {
-    // Items are sorted by descending radius: the wide radii come first.
-    cudaError_t e = launch_range<kSplitR + 1, kMaxR, 2>(g, idd, rsigma, work, beam, bev, numSMs * 2, 0, s);
+                             BeamStateDev* beam, float* bev, unsigned long long* bevFixed, int shiftOffset, int numSMs,
+                             cudaStream_t s) {
+    // Items are sorted by range: the wide radii come first.
+    cudaError_t e = launch_range<true, kSplitR + 1, kMaxR, kWideBlocks>(g, idd, rsigma, work, beam, bevFixed,
+                                                                        shiftOffset, numSMs * kWideBlocks, 0, s);
     if (e != cudaSuccess) return e;
-    e = launch_range<kSplitR3 + 1, kSplitR, kMidBlocks>(g, idd, rsigma, work, beam, bev, numSMs * kMidBlocks, 1, s);
+    e = launch_range<false, kSplitR2 + 1, kSplitR, kMidBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
+                                                               numSMs * kMidBlocks, 1, s);
     if (e != cudaSuccess) return e;
-    e = launch_range<kSplitR2 + 1, kSplitR3, kMidNarrowBlocks>(g, idd, rsigma, work, beam, bev,
-                                                                numSMs * kMidNarrowBlocks, 3, s);
+    e = launch_range<false, 0, kSplitR2, kNarrowBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
+                                                        numSMs * kNarrowBlocks, 2, s);
     if (e != cudaSuccess) return e;
-    return launch_range<0, kSplitR2, kNarrowBlocks>(g, idd, rsigma, work, beam, bev, numSMs * kNarrowBlocks, 2, s);
+    bev_fixed_to_float_kernel<<<numSMs * 8, 256, 0, s>>>(g, beam, bevFixed, bev, shiftOffset);
+    return cudaGetLastError();
 }
 
 }  // namespace pbs

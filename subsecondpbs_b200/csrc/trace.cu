@@ -465,6 +465,7 @@ __global__ void beam_planner_kernel(BeamGeomDev g, float* __restrict__ weplMin,
         st.maxFirstPassive = INT_MIN;
         st.calcPassive = 0;
         st.liveTiles = 0;
+        st.maxIddBits = 0;
         for (int i = 0; i < kBuckets; ++i) {
             st.hist[i] = 0;
             st.batchedR[i] = 0;

@@ -41,14 +41,14 @@ __device__ __forceinline__ float bev_sample(const float* __restrict__ v, int nx,
 }
 
 // Transfer box from the eight BEV corners (wrapper.cu:5343-5394); the z range spans
-// the deepest superposed step of all layers.
-__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam) {
+// the deepest superposed step of all layers, or of `layer` alone when it is given.
+__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const LayerStateDev* layer) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     // Last kernel of the beam's work list with one thread: hand the beam's error
     // flags to the context's error word, which outlives the beam state.
     if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
     const int first = beam->firstInside;
-    const int passive = beam->maxCalcPassive;
+    const int passive = layer ? layer->calcPassive : beam->maxCalcPassive;
     const float xs[2] = {-float(kMaxR), float(g.pitchX + kMaxR - 1)};
     const float ys[2] = {-float(kMaxR), float(g.pitchY + kMaxR - 1)};
     const float zs[2] = {float(first), float(passive - 1)};
@@ -157,8 +157,9 @@ __global__ void dose_box_kernel(double* dose, float* out, int3 dims, int3 lo, in
 
 }  // namespace
 
-cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, cudaStream_t s) {
-    transfer_planner_kernel<<<1, 32, 0, s>>>(g, beam);
+cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer,
+                                    cudaStream_t s) {
+    transfer_planner_kernel<<<1, 32, 0, s>>>(g, beam, layer);
     return cudaGetLastError();
 }
 

@@ -244,6 +244,57 @@ def plain_pipeline(workload: dict, prepared: list, gpu_id: int = 0, keep: set | 
     return {"service_s": times, "plans_per_s": len(times) / float(times.sum()), "doses": kept}
 
 
+def device_pipeline(workload: dict, prepared: list, gpu_id: int = 0, passes: int = 2) -> dict:
+    """The stream's GPU work alone, one request after the other: every request's beams
+    and its float dose readout on one resident context per ion (the patient's CT and
+    dose grid set outside the timed region when the patient changes), timed with CUDA
+    events on the context's stream. Host planning, CT uploads and copies are not in
+    the per-request times; plans/s = requests / the sum of those times. The last of
+    `passes` passes over the stream is reported (the first grows the buffers)."""
+    import torch
+
+    from .cudaCalDoseRTD import DoseEngine
+
+    dev = torch.device("cuda", gpu_id)
+    engines: dict[str, DoseEngine] = {}
+    current: dict[str, int] = {}
+    outs: dict[tuple, torch.Tensor] = {}
+    times = []
+    for _ in range(passes):
+        times = []
+        for r, beams in zip(workload["requests"], prepared):
+            ion = r["ion"]
+            carbon = ion == "carbon"
+            eng = engines.get(ion)
+            if eng is None:
+                eng = engines[ion] = DoseEngine(gpu_id)
+                eng.set_energy(workload["energy"][ion])
+                current[ion] = -1
+            p = workload["patients"][r["patient"]]
+            if current[ion] != r["patient"]:
+                eng.set_ct(p["ct"], p["ct_dims"], p["ct_resolution"], p["ct_corner"])
+                eng.set_dose_grid(p["dose_dims"], p["dose_resolution"], p["dose_corner"])
+                eng.synchronize()
+                current[ion] = r["patient"]
+            dd = tuple(p["dose_dims"])
+            if dd not in outs:
+                outs[dd] = torch.empty((dd[2], dd[1], dd[0]), dtype=torch.float32, device=dev)
+            stream = torch.cuda.ExternalStream(eng.stream_handle, device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.reset_dose()
+            for b in beams:
+                eng.add_beam(b, nuclear_correction=carbon)
+            eng.read_dose(outs[dd])
+            e1.record(stream)
+            eng.synchronize()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+    for eng in engines.values():
+        eng.close()
+    times = np.array(times)
+    return {"device_s": times, "plans_per_s": len(times) / float(times.sum())}
+
+
 def with_rate(workload: dict, rate_hz: float) -> dict:
     """The same requests with their Poisson arrival times rescaled to `rate_hz`."""
     f = workload["rate_hz"] / rate_hz

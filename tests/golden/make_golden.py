@@ -55,6 +55,8 @@ CASES = {
                                                "e_range": [80.0, 120.0]}, {"tables": "reference", "rotate": 30.0}),
     "hetero_mid_rt": ("heterogeneous_case", {"dims": [96, 96, 64], "n_layers": 6, "target_radius_mm": 20.0,
                                              "e_range": [70.0, 150.0]}, {"tables": "reference"}),
+    # The bench's headline beam (config 2): 256x256x160 CT, 20 layers 70-180 MeV, 3020 spots.
+    "headline_rt": ("heterogeneous_case", {}, {"tables": "reference"}),
     "halo_small_rt": ("heterogeneous_case", {"dims": [64, 64, 48], "n_layers": 3, "target_radius_mm": 14.0,
                                              "e_range": [80.0, 120.0]}, {"tables": "reference", "nuclear": "GAUSS_FIT"}),
     # CarbonPBS lateral profile model (sigma override and overall weight), which the

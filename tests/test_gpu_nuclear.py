@@ -33,7 +33,7 @@ def test_gauss_fit_halo_stage_parity(hetero_small_case):
     rep = nuclear_report(eng, cap)
     assert rep["fma_oracle"] > 0
     assert_nuclear_parity(rep)
-    assert eng.beam_stats()["kernel_launches"] == 6 + 6 + 7 + 2
+    assert eng.beam_stats()["kernel_launches"] == 6 + 7 + 8 + 2
     _dose_checks(eng.read_dose(), r["dose"], case["dose_resolution"])
 
 

@@ -53,6 +53,21 @@ def test_heterogeneous_headline_dose(hetero_case):
     _dose_checks(eng.read_dose(), r["dose"], hetero_case["dose_resolution"])
 
 
+def test_headline_on_reference_tables_in_the_reference_convention():
+    """The bench's headline beam on the reference's own proton tables, with the
+    reference's BEV depth indexing (the form in which the bench compares this
+    library's dose with the reference's)."""
+    from pathlib import Path
+
+    from subsecondpbs_b200 import tables
+
+    t = tables.load_table_npz(Path(__file__).resolve().parent / "golden" / "reference_tables.npz")
+    case = phantoms.heterogeneous_case(energy={k: v for k, v in t.items() if not k.startswith("nuc")})
+    eng = run_gpu(case, compat=True, keep_debug=False)
+    r = oracle_run(case, compat_bev_z_shift=True)
+    _dose_checks(eng.read_dose(), r["dose"], case["dose_resolution"])
+
+
 @pytest.mark.parametrize("angle", [0.0, 120.0, 240.0])
 def test_rotated_gantry(hetero_small_case, angle):
     beam = phantoms.rotate_beam(hetero_small_case["beam"], angle)
@@ -123,6 +138,23 @@ def test_wrapper_matches_engine_and_is_repeatable(water_case):
     m = d3.max()
     assert np.abs(d1 - d3).max() <= 1e-6 * m
     assert np.abs(d1 - d2).max() <= 1e-6 * m
+
+
+def test_dose_is_bit_identical_across_runs(hetero_small_case):
+    """The superposition adds tile footprints to the BEV in integer fixed point and
+    the transfer gathers per dose voxel, so the dose does not depend on the order in
+    which the device schedules the tiles: repeated runs give the same bits, with the
+    nuclear halo as well."""
+    from subsecondpbs_b200 import tables
+
+    for nuclear in (None, L.NUCLEAR_GAUSS_FIT):
+        case = dict(hetero_small_case)
+        if nuclear is not None:
+            case["energy"] = tables.synthetic_nuclear_tables(case["energy"])
+        doses = [run_gpu(case, keep_debug=False, nuclear_model=nuclear).read_dose() for _ in range(3)]
+        assert doses[0].max() > 0
+        for d in doses[1:]:
+            assert np.array_equal(d.view(np.uint32), doses[0].view(np.uint32))
 
 
 def test_invalid_input_raises_without_touching_the_gpu_state(water_case):
