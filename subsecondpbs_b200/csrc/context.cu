@@ -1105,6 +1105,10 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     std::memset(&hbs, 0, sizeof(hbs));
     hbs.firstInside = INT32_MAX;
     hbs.firstOutside = INT32_MIN;
+    for (int i = 0; i < 3; ++i) {
+        hbs.liveLo[i] = INT32_MAX;
+        hbs.liveHi[i] = INT32_MIN;
+    }
     const size_t latBytes = P.hasLattice ? P.lattice.weights.size() * 4 : 0;
     const size_t subBytes = P.hasLattice ? 0 : b.n_subspot_data * 4;
     const size_t nucMapBytes = nuclear ? hRayToNuc.size() * 4 : 0;
@@ -1247,7 +1251,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             }
             doseReady = true;
         }
-        PBS_CUDA(launch_transfer_planner(g, dbs, layer, stream), "transfer_planner");
+        PBS_CUDA(launch_transfer_planner(g, dbs, layer, !perLayerTransfer, stream), "transfer_planner");
         PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
         if (bio) {
             // The beam's own dose and the channels into the biological accumulators.
@@ -1265,7 +1269,8 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             }
         }
         if (nuclear) {
-            PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, nucLayer, stream), "nuc_transfer_planner");
+            PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, nucLayer, !perLayerTransfer, stream),
+                     "nuc_transfer_planner");
             PBS_CUDA(launch_transfer(nucGeom, static_cast<const float*>(nucBev.ptr), dNucBs,
                                      static_cast<double*>(dose64.ptr), stream),
                      "nuc_transfer");
@@ -1379,7 +1384,7 @@ int Context::finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b) {
     if ((rc = bevGrad.ensure(bevN * 4)) || (rc = rbarBuf.ensure(L * rays * 4)) ||
         (rc = gradInterm.ensure(L * g.latNy * g.rayX * 4)) || (rc = gradLattice.ensure(latN * 4)))
         return rc;
-    PBS_CUDA(launch_transfer_planner(g, dbs, nullptr, stream), "transfer_planner");
+    PBS_CUDA(launch_transfer_planner(g, dbs, nullptr, 0, stream), "transfer_planner");
     PBS_CUDA(cudaMemsetAsync(bevGrad.ptr, 0, bevN * 4, stream), "memset");
     PBS_CUDA(cudaMemsetAsync(rbarBuf.ptr, 0, L * rays * 4, stream), "memset");
     PBS_CUDA(launch_transfer_adjoint(g, a.gradDose, dbs, static_cast<float*>(bevGrad.ptr), stream), "transfer_adjoint");

@@ -264,7 +264,9 @@ struct Context {
     };
     int plan_columns(const PbsBeamDesc& b, long long spotBegin, long long spotCount, const char* what,
                      ColumnPlan& cp);
-    int run_column(ColumnPlan& cp, size_t spot, int nuclear, void* box);
+    // Dose of one spot at unit weight into the FP64 grid (zeroed first unless
+    // `gridZero` says it is zero already), with the box of voxels it can have written.
+    int run_column(ColumnPlan& cp, size_t spot, int nuclear, void* box, bool gridZero = false);
     int influence_csc(const PbsBeamDesc& b, int nuclear, long long spotBegin, long long spotCount, double threshold,
                       long long* colPtr, int* rows, float* vals, long long capacity, long long* nnz);
     int beam_stats(PbsBeamStats* out);

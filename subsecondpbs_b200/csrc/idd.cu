@@ -579,6 +579,10 @@ __device__ __forceinline__ void emit_merged(BeamStateDev* beam, int4* work, unsi
 __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restrict__ codes,
                                   const LayerStateDev* __restrict__ ls, BeamStateDev* __restrict__ beam,
                                   int4* __restrict__ work) {
+    // The block's extent of the cells its items write (min x, y, z; max x, y, z).
+    __shared__ int sExt[6];
+    if (threadIdx.x < 6) sExt[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int tiles = g.tilesX * g.tilesY;
     const int first = beam->firstInside;
@@ -587,6 +591,7 @@ __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const 
     for (size_t i = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5; i < perLayer; i += warps) {
         const int zr = int(i / tiles);
         const int tile = int(i - size_t(zr) * tiles);
+        int rMax = -1;
         for (int base = 0; base < nLayers; base += 32) {
             const int lc = base + lane;
             int R = -1;
@@ -595,6 +600,7 @@ __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const 
                 const int c = codes[size_t(lc) * perLayer + i];
                 if (zr < st.afterLast - first && (c & 0x80)) R = st.batchedR[c & 0x3f];
             }
+            rMax = max(rMax, R);
             const bool merge = R >= 0 && R <= kSplitR;
             const unsigned mergeLanes = __ballot_sync(0xffffffffu, merge);
             if (R > kSplitR) emit_merged(beam, work, 0xffffff00u | unsigned(lc), tile, zr, R);
@@ -616,7 +622,21 @@ __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const 
                 }
             }
         }
+        rMax = __reduce_max_sync(0xffffffffu, rMax);
+        if (lane == 0 && rMax >= 0) {
+            const int tx = tile % g.tilesX, ty = tile / g.tilesX;
+            atomicMin(&sExt[0], tx * kTileX - rMax + kMaxR);
+            atomicMin(&sExt[1], ty * kTileY - rMax + kMaxR);
+            atomicMin(&sExt[2], zr);
+            atomicMax(&sExt[3], tx * kTileX + kTileX - 1 + rMax + kMaxR);
+            atomicMax(&sExt[4], ty * kTileY + kTileY - 1 + rMax + kMaxR);
+            atomicMax(&sExt[5], zr);
+        }
     }
+    __syncthreads();
+    if (threadIdx.x < 3 && sExt[threadIdx.x] != INT_MAX) atomicMin(&beam->liveLo[threadIdx.x], sExt[threadIdx.x]);
+    if (threadIdx.x >= 3 && threadIdx.x < 6 && sExt[threadIdx.x] != INT_MIN)
+        atomicMax(&beam->liveHi[threadIdx.x - 3], sExt[threadIdx.x]);
 }
 
 // Halo cells start empty: IDD 0 and rSigmaEff +inf (wrapper.cu:4124-4135).

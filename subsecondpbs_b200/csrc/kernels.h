@@ -105,8 +105,9 @@ cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float
 
 // ---- BEV -> dose ---------------------------------------------------------------
 // Transfer bounding box and parameters (wrapper.cu:5343-5403): over the steps of
-// every layer, or of `layer` alone (non-null).
-cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer,
+// every layer, or of `layer` alone (non-null); with `live` over the BEV cells the
+// forward's superposition items can have written.
+cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer, int live,
                                     cudaStream_t s);
 // primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44) accumulating in FP64.
 cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamStateDev* beam, double* dose,

@@ -29,6 +29,65 @@ constexpr int kOpThreads = 256;
 constexpr int kOpPasses = 8;
 constexpr int kOpChunk = kOpThreads * kOpPasses;  // box voxels per block
 
+// The columns of one export share the beam's geometry and so its trace: the first
+// column traces into this store's buffer and the others skip the tracer and wait
+// on its event (the TraceStore contract of Context::run_beam).
+struct ColumnTraces : TraceStore {
+    DevBuf mem;
+    cudaEvent_t ready = nullptr;
+    TraceSlot slot{};
+    bool have = false;
+
+    ~ColumnTraces() override {
+        if (ready) cudaEventDestroy(ready);
+        mem.release();
+    }
+    int acquire(Context&, const BeamGeomDev& g, TraceSlot& ts) override {
+        if (!have) {
+            const size_t rays = size_t(g.rayX) * g.rayY, S = size_t(g.steps);
+            if (int rc = mem.ensure(trace_bytes(S, rays))) return rc;
+            if (!ready && cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess)
+                return PBS_ERR_CUDA;
+            auto up = [](size_t n) { return (n + 255) / 256 * 256; };
+            char* p = static_cast<char*>(mem.ptr);
+            slot.dens = reinterpret_cast<float*>(p);
+            p += up(S * rays * 4);
+            slot.wepl = reinterpret_cast<float*>(p);
+            p += up(S * rays * 4);
+            slot.firstIn = reinterpret_cast<int*>(p);
+            p += up(rays * 4);
+            slot.firstOut = reinterpret_cast<int*>(p);
+            p += up(rays * 4);
+            slot.weplMin = reinterpret_cast<float*>(p);
+            p += up(S * 4);
+            slot.inOut = reinterpret_cast<int*>(p);
+            slot.ready = ready;
+        }
+        ts = slot;
+        ts.traced = have;
+        return PBS_OK;
+    }
+    int traced(Context& c, TraceSlot&) override {
+        if (cudaEventRecord(ready, c.stream) != cudaSuccess) return PBS_ERR_CUDA;
+        have = true;
+        return PBS_OK;
+    }
+};
+
+// Installs a ColumnTraces on a context without a trace store of its own for the
+// lifetime of the guard.
+struct ColumnTraceGuard {
+    Context& c;
+    ColumnTraces traces;
+    bool installed;
+    explicit ColumnTraceGuard(Context& ctx) : c(ctx), installed(ctx.traceStore == nullptr) {
+        if (installed) c.traceStore = &traces;
+    }
+    ~ColumnTraceGuard() {
+        if (installed) c.traceStore = nullptr;
+    }
+};
+
 // An inclusive voxel box of the dose grid walked in grid order (x fastest).
 struct OpBox {
     int lo[3];
@@ -45,9 +104,44 @@ __device__ __forceinline__ long long box_to_grid(const OpBox& a, long long b) {
     return (static_cast<long long>(a.lo[2] + bz) * a.Y + (a.lo[1] + by)) * a.X + (a.lo[0] + bx);
 }
 
-// Entries above the threshold in each block's chunk of the box.
-__global__ void __launch_bounds__(kOpThreads) influence_count_kernel(const double* __restrict__ dose, OpBox a,
+// The voxels a beam's transfer can have written: its device-side transfer box with
+// the launch's block rounding in x (32) and y (8), as transfer_kernel walks it.
+__device__ __forceinline__ void written_box(const BeamStateDev* bs, int X, int Y, int lo[3], int hi[3]) {
+    if (!bs || !bs->transferValid) {
+        lo[0] = lo[1] = lo[2] = INT_MAX;
+        hi[0] = hi[1] = hi[2] = INT_MIN;
+        return;
+    }
+    for (int i = 0; i < 3; ++i) lo[i] = bs->transferStart[i];
+    hi[0] = lo[0] + min(((bs->transferMax[0] - lo[0] + 1 + 31) / 32) * 32, X - lo[0]) - 1;
+    hi[1] = lo[1] + min(((bs->transferMax[1] - lo[1] + 1 + 7) / 8) * 8, Y - lo[1]) - 1;
+    hi[2] = bs->transferMax[2];
+}
+
+// The part of the column's host box `a` that the primary and halo transfers can
+// have written; every other voxel of `a` is zero.
+__device__ __forceinline__ OpBox column_box(const OpBox& a, const BeamStateDev* pb, const BeamStateDev* nb) {
+    int l0[3], h0[3], l1[3], h1[3];
+    written_box(pb, a.X, a.Y, l0, h0);
+    written_box(nb, a.X, a.Y, l1, h1);
+    OpBox e = a;
+    e.n = 1;
+    for (int i = 0; i < 3; ++i) {
+        const int lo = max(min(l0[i], l1[i]), a.lo[i]);
+        const int hi = min(max(h0[i], h1[i]), a.lo[i] + a.ext[i] - 1);
+        e.lo[i] = lo;
+        e.ext[i] = hi >= lo ? hi - lo + 1 : 0;
+        e.n *= e.ext[i];
+    }
+    return e;
+}
+
+// Entries above the threshold in each block's chunk of the column's box.
+__global__ void __launch_bounds__(kOpThreads) influence_count_kernel(const double* __restrict__ dose, OpBox host,
+                                                                     const BeamStateDev* __restrict__ pb,
+                                                                     const BeamStateDev* __restrict__ nb,
                                                                      double thr, long long* __restrict__ blockOff) {
+    const OpBox a = column_box(host, pb, nb);
     const long long base = static_cast<long long>(blockIdx.x) * kOpChunk;
     int c = 0;
     for (int p = 0; p < kOpPasses; ++p) {
@@ -97,12 +191,16 @@ __global__ void __launch_bounds__(1024) influence_scan_kernel(long long* __restr
 }
 
 // Ordered compaction of each block's chunk: entries keep the box order, which is
-// ascending voxel order. Entries past `cap` are counted but not written.
-__global__ void __launch_bounds__(kOpThreads) influence_write_kernel(const double* __restrict__ dose, OpBox a,
+// ascending voxel order. Entries past `cap` are counted but not written. Every voxel
+// of the box is zeroed once read, so the grid is zero again for the next column.
+__global__ void __launch_bounds__(kOpThreads) influence_write_kernel(double* __restrict__ dose, OpBox host,
+                                                                     const BeamStateDev* __restrict__ pb,
+                                                                     const BeamStateDev* __restrict__ nb,
                                                                      double thr, const long long* __restrict__ blockOff,
                                                                      int* __restrict__ rows, float* __restrict__ vals,
                                                                      long long cap) {
     __shared__ int warpCounts[kOpThreads / 32];
+    const OpBox a = column_box(host, pb, nb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long pos = blockOff[blockIdx.x];
     const long long base = static_cast<long long>(blockIdx.x) * kOpChunk;
@@ -114,6 +212,7 @@ __global__ void __launch_bounds__(kOpThreads) influence_write_kernel(const doubl
         if (b < a.n) {
             g = box_to_grid(a, b);
             v = dose[g];
+            dose[g] = 0.0;
             keep = fabs(v) > thr;
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -282,7 +381,7 @@ int Context::plan_columns(const PbsBeamDesc& beam, long long spotBegin, long lon
 
 // Dose of spot j alone at unit weight into the (zeroed) FP64 grid, with the box of
 // voxels it can have written.
-int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut) {
+int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut, bool gridZero) {
     // The column is the dose of spot j's layer alone: the other layers' weights are
     // zero, so they add nothing, and every per-layer decision (steps, radii, work
     // items) depends on the layer's own parameters and the beam's geometry only. The
@@ -316,7 +415,15 @@ int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut) {
         const int c = cp.cells[j * 4 + slot];
         if (c >= 0) P.lattice.weights[static_cast<size_t>(c) - cellBase] += cp.shares[j * 4 + slot];
     }
-    if (int rc = reset_dose(nullptr, 0)) return rc;
+    // A grid known to be zero only needs its dirty box forgotten.
+    if (gridZero && doseBoxed && !doseExposed && !pendingDoseInit && !bioModel) {
+        for (int i = 0; i < 3; ++i) {
+            dirtyLo[i] = INT_MAX;
+            dirtyHi[i] = -1;
+        }
+    } else if (int rc = reset_dose(nullptr, 0)) {
+        return rc;
+    }
     if (int rc = add_planned_beam(cp.beam, nuclear, std::move(P))) return rc;
     if (int rc = join_side_work()) return rc;
     OpBox& a = *static_cast<OpBox*>(boxOut);
@@ -352,6 +459,7 @@ int Context::influence_row_norms(const PbsBeamDesc& beam, int nuclear, long long
         }
     ColumnPlan cp;
     if (int rc = plan_columns(beam, spotBegin, spotCount, "influence row norms", cp)) return rc;
+    ColumnTraceGuard sharedTrace(*this);
     auto fail = [&](int rc) {
         const std::string msg = last_error();
         reset_dose(nullptr, 0);
@@ -417,6 +525,7 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
     }
     ColumnPlan cp;
     if (int rc = plan_columns(beam, spotBegin, spotCount, "influence export", cp)) return rc;
+    ColumnTraceGuard sharedTrace(*this);
 
     // Any failure below leaves the dose grid zeroed, as a finished export does.
     auto fail = [&](int rc) {
@@ -441,14 +550,18 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
 
     for (long long k = 0; k < spotCount; ++k) {
         OpBox a{};
-        if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a)) return fail(rc);
+        // The previous column's compaction zeroed what its transfers wrote.
+        if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a, k > 0)) return fail(rc);
         const int nBlocks = static_cast<int>((a.n + kOpChunk - 1) / kOpChunk);
-        const double* d = static_cast<const double*>(dose64.ptr);
-        if (nBlocks > 0) influence_count_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, threshold, dBlockOff);
+        double* d = static_cast<double*>(dose64.ptr);
+        const BeamStateDev* pb = static_cast<const BeamStateDev*>(bs.ptr);
+        const BeamStateDev* nb = lastNuclear ? static_cast<const BeamStateDev*>(nucBs.ptr) : nullptr;
+        if (nBlocks > 0)
+            influence_count_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, pb, nb, threshold, dBlockOff);
         influence_scan_kernel<<<1, 1024, 0, stream>>>(dBlockOff, nBlocks, dColPtr, static_cast<int>(k));
         if (nBlocks > 0)
-            influence_write_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, threshold, dBlockOff, dRows, dVals,
-                                                                       capacity);
+            influence_write_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, pb, nb, threshold, dBlockOff, dRows,
+                                                                       dVals, capacity);
         if (int rc3 = op_cuda(cudaGetLastError(), "influence kernels")) return fail(rc3);
     }
     if (int rc = op_cuda(cudaMemcpyAsync(colPtrHost, dColPtr, static_cast<size_t>(spotCount + 1) * sizeof(long long),

@@ -71,6 +71,10 @@ struct BeamStateDev {
     // block, so the items of one radius stay together.
     int rStart[kMaxR + 1];
     int mergedR[kMaxR + 1];
+    // Padded BEV cells (x, y) and steps relative to firstInside (z) the forward's
+    // superposition items can write, over all chunks (work_merge_kernel); lo > hi
+    // while none. The transfer box is taken over these cells.
+    int liveLo[3], liveHi[3];
     // Fixed-point exponent of the chunk's BEV accumulation: a value v is added to the
     // int64 BEV as v * 2^fixedShift. Every BEV cell stays below 2^62 (layer_plan_kernel).
     int fixedShift;

@@ -36,8 +36,10 @@
 //     on the order in which the items land. The chunk's exponent
 //     (layer_plan_kernel) bounds every cell below 2^62; a last pass adds the chunk
 //     to the float BEV and clears it.
+// Up to radius 7 a warp has at most one (column, distance) unit, so its column sums
+// stay in registers over all the item's layers and are flushed once per item.
 // Radii 16..32, 8..15 and 0..7 run as three persistent instances with 128, 48 and
-// 32 registers: 2, 5 and 8 CTAs per SM.
+// 40 registers: 2, 5 and 6 CTAs per SM.
 #include "device_util.cuh"
 #include "kernels.h"
 #include "launch_util.h"
@@ -149,108 +151,149 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
     const int sc = footprint_exponent(total);
     const float scale = ldexpf(1.0f, sc);
 
-#pragma unroll 1
-    for (int j = 0; j < kMergeLayers; ++j) {
-        const unsigned lc = (a.layers >> (8 * j)) & 0xffu;
-        if (lc == 0xffu) break;
-        // The layers alternate between two column-mask buffers: a buffer is cleared
-        // after the barrier that ends its layer's accumulation, and refilled two
-        // layers later.
-        unsigned* colMask = sCol + (j & 1) * kTileX;
-        // ---- table phase (complete_superposition.cu:298-307) ----------------
-        // Thread t is source (sy, sx) = (warp, lane): its rows e_s(0..R) in float4
-        // chunks (chunk-major) and idd_s e_s(0..R); sources without dose get zero
-        // rows, and colMask[sx] collects the depositing sources of every column.
-        {
-            const size_t src = lc * a.layerStride + a.src;
-            const float dose = a.idd[src];
-            const bool live = dose > 0.0f;
-            if (live) atomicOr(&colMask[lane], 1u << warp);
-            float e[4 * Q];
-            if (live) {
-                float row[R + 1];
-                superposition_row<R>(a.rsig[src], row);
+    // Table phase of one layer (complete_superposition.cu:298-307): thread t is source
+    // (sy, sx) = (warp, lane); its rows e_s(0..R) go in float4 chunks (chunk-major)
+    // and idd_s e_s(0..R); sources without dose get zero rows, and colMask[sx]
+    // collects the depositing sources of every column.
+    auto table = [&](unsigned lc, unsigned* colMask) {
+        const size_t src = lc * a.layerStride + a.src;
+        const float dose = a.idd[src];
+        const bool live = dose > 0.0f;
+        if (live) atomicOr(&colMask[lane], 1u << warp);
+        float e[4 * Q];
+        if (live) {
+            float row[R + 1];
+            superposition_row<R>(a.rsig[src], row);
 #pragma unroll
-                for (int k = 0; k <= R; ++k) {
-                    e[k] = row[k];
-                    EW[t * EWS + k] = dose * row[k];
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k <= R; ++k) {
-                    e[k] = 0.0f;
-                    EW[t * EWS + k] = 0.0f;
-                }
+            for (int k = 0; k <= R; ++k) {
+                e[k] = row[k];
+                EW[t * EWS + k] = dose * row[k];
             }
+        } else {
 #pragma unroll
-            for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
-            const int pt = warp * kTileX + e4_col(lane);
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-                E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
+            for (int k = 0; k <= R; ++k) {
+                e[k] = 0.0f;
+                EW[t * EWS + k] = 0.0f;
+            }
         }
-        __syncthreads();
-
-        // ---- accumulation phase ---------------------------------------------
-        // Lanes outside the footprint read source column 0 and are never flushed;
-        // pairs whose source column has no depositing source are skipped.
-        const unsigned colBits = colMask[lane];
-#pragma unroll 1
-        for (int u = warp; u < kUnits; u += kWarps) {
-            const int g = lane / M;
-            int d = lane - g * M;
-            int sx = u + g * S;
-            const bool valid = g < G && sx < kTileX;
-            if (!valid) {
-                sx = 0;
-                d = 0;
-            }
-            const unsigned colAll = __shfl_sync(0xffffffffu, colBits, sx);
-            const unsigned colLive = valid ? colAll : 0u;
-            if (!__any_sync(0xffffffffu, colLive != 0)) continue;
-            const float* ewCol = EW + sx * EWS + d;
-            const float4* eCol = E4 + e4_col(sx);
-            float acc[H];
 #pragma unroll
-            for (int i = 0; i < H; ++i) acc[i] = 0.0f;
+        for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
+        const int pt = warp * kTileX + e4_col(lane);
 #pragma unroll
-            for (int sy = 0; sy < kTileY; ++sy) {
-                const float w = ewCol[sy * kTileX * EWS];
+        for (int q = 0; q < Q; ++q)
+            E4[q * kThreads + pt] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
+    };
+    // Adds the eight sources of source column sx at distance d to the column sums.
+    auto accumulate = [&](int sx, int d, float (&acc)[H]) {
+        const float* ewCol = EW + sx * EWS + d;
+        const float4* eCol = E4 + e4_col(sx);
 #pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    const float4 v = eCol[q * kThreads + sy * kTileX];
-                    const float ev[4] = {v.x, v.y, v.z, v.w};
+        for (int sy = 0; sy < kTileY; ++sy) {
+            const float w = ewCol[sy * kTileX * EWS];
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const int k = 4 * q + c;
-                        if (k <= R) {
-                            acc[sy + R + k] = fmaf(w, ev[c], acc[sy + R + k]);
-                            if (k > 0) acc[sy + R - k] = fmaf(w, ev[c], acc[sy + R - k]);
-                        }
+            for (int q = 0; q < Q; ++q) {
+                const float4 v = eCol[q * kThreads + sy * kTileX];
+                const float ev[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int k = 4 * q + c;
+                    if (k <= R) {
+                        acc[sy + R + k] = fmaf(w, ev[c], acc[sy + R + k]);
+                        if (k > 0) acc[sy + R - k] = fmaf(w, ev[c], acc[sy + R - k]);
                     }
                 }
-                // Lets the loads of the next source overlap this pair's FMAs but keeps
-                // later sources' loads from being hoisted (which would hold every row
-                // of the column in registers).
-                if (sy & 1) asm volatile("" ::: "memory");
             }
-            if (colLive) {
-                int qv[H];
-#pragma unroll
-                for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(acc[i] * scale);
-                int* col = out + sx + R + d;
-#pragma unroll
-                for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
-                if (d > 0) {
-                    col = out + sx + R - d;
-#pragma unroll
-                    for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
-                }
-            }
+            // Lets the loads of the next source overlap this pair's FMAs but keeps
+            // later sources' loads from being hoisted (which would hold every row
+            // of the column in registers).
+            if (sy & 1) asm volatile("" ::: "memory");
         }
-        // The next layer's tables overwrite these.
+    };
+    // Adds a pair's column sums to both of its output columns.
+    auto flush = [&](int sx, int d, const float (&acc)[H]) {
+        int qv[H];
+#pragma unroll
+        for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(acc[i] * scale);
+        int* col = out + sx + R + d;
+#pragma unroll
+        for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
+        if (d > 0) {
+            col = out + sx + R - d;
+#pragma unroll
+            for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
+        }
+    };
+
+    if constexpr (kUnits <= kWarps) {
+        // One pair unit per warp: its column sums stay in registers over all the
+        // item's layers and are flushed once. The column masks OR over the layers.
+        const int g = lane / M;
+        int d = lane - g * M;
+        int sx = warp + g * S;
+        const bool valid = warp < kUnits && g < G && sx < kTileX;
+        if (!valid) {
+            sx = 0;
+            d = 0;
+        }
+        float acc[H];
+#pragma unroll
+        for (int i = 0; i < H; ++i) acc[i] = 0.0f;
+#pragma unroll 1
+        for (int j = 0; j < kMergeLayers; ++j) {
+            const unsigned lc = (a.layers >> (8 * j)) & 0xffu;
+            if (lc == 0xffu) break;
+            table(lc, sCol);
+            __syncthreads();
+            // Lanes outside the footprint read source column 0 and are never flushed.
+            // Every lane takes part in the shuffle.
+            const unsigned colAll = __shfl_sync(0xffffffffu, sCol[lane], sx);
+            const unsigned colLive = valid ? colAll : 0u;
+            if (__any_sync(0xffffffffu, colLive != 0)) accumulate(sx, d, acc);
+            // The next layer's tables overwrite these.
+            __syncthreads();
+        }
+        const unsigned colAll = __shfl_sync(0xffffffffu, sCol[lane], sx);
+        const unsigned colLive = valid ? colAll : 0u;
+        if (colLive) flush(sx, d, acc);
         __syncthreads();
-        if (t < kTileX) colMask[t] = 0;
+        if (t < kTileX) sCol[t] = 0;
+    } else {
+#pragma unroll 1
+        for (int j = 0; j < kMergeLayers; ++j) {
+            const unsigned lc = (a.layers >> (8 * j)) & 0xffu;
+            if (lc == 0xffu) break;
+            // The layers alternate between two column-mask buffers: a buffer is
+            // cleared after the barrier that ends its layer's accumulation, and
+            // refilled two layers later.
+            unsigned* colMask = sCol + (j & 1) * kTileX;
+            table(lc, colMask);
+            __syncthreads();
+            // Lanes outside the footprint read source column 0 and are never flushed;
+            // pairs whose source column has no depositing source are skipped.
+            const unsigned colBits = colMask[lane];
+#pragma unroll 1
+            for (int u = warp; u < kUnits; u += kWarps) {
+                const int g = lane / M;
+                int d = lane - g * M;
+                int sx = u + g * S;
+                const bool valid = g < G && sx < kTileX;
+                if (!valid) {
+                    sx = 0;
+                    d = 0;
+                }
+                const unsigned colAll = __shfl_sync(0xffffffffu, colBits, sx);
+                const unsigned colLive = valid ? colAll : 0u;
+                if (!__any_sync(0xffffffffu, colLive != 0)) continue;
+                float acc[H];
+#pragma unroll
+                for (int i = 0; i < H; ++i) acc[i] = 0.0f;
+                accumulate(sx, d, acc);
+                if (colLive) flush(sx, d, acc);
+            }
+            // The next layer's tables overwrite these.
+            __syncthreads();
+            if (t < kTileX) colMask[t] = 0;
+        }
     }
     __syncthreads();
 
@@ -527,13 +570,19 @@ __global__ void __launch_bounds__(256) bev_fixed_to_float_kernel(BeamGeomDev g, 
                                                                  float* __restrict__ bev, int shiftOffset) {
     const int planes = min(beam->maxCalcPassive - beam->firstInside, g.steps);
     if (planes <= 0) return;
-    const size_t n = static_cast<size_t>(planes) * g.bevX * g.bevY;
-    const int shift = beam->fixedShift + shiftOffset;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
-        const unsigned long long v = fixed[i];
-        if (v) {
-            bev[i] += float(ldexp(double(v), -shift));
-            fixed[i] = 0ull;
+    // bevX is even (the padded ray pitch plus 2 kMaxR), so cells go in aligned pairs.
+    const size_t pairs = static_cast<size_t>(planes) * g.bevX * g.bevY / 2;
+    const double unit = ldexp(1.0, -(beam->fixedShift + shiftOffset));
+    ulonglong2* f2 = reinterpret_cast<ulonglong2*>(fixed);
+    float2* b2 = reinterpret_cast<float2*>(bev);
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < pairs; i += size_t(gridDim.x) * blockDim.x) {
+        const ulonglong2 v = f2[i];
+        if (v.x | v.y) {
+            float2 o = b2[i];
+            o.x += float(double(v.x) * unit);
+            o.y += float(double(v.y) * unit);
+            b2[i] = o;
+            f2[i] = make_ulonglong2(0ull, 0ull);
         }
     }
 }
@@ -541,7 +590,7 @@ __global__ void __launch_bounds__(256) bev_fixed_to_float_kernel(BeamGeomDev g, 
 // Resident CTAs per SM of the instances.
 constexpr int kWideBlocks = 2;
 constexpr int kMidBlocks = 5;
-constexpr int kNarrowBlocks = 8;
+constexpr int kNarrowBlocks = 6;
 
 }  // namespace
 

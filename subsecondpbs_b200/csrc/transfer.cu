@@ -42,16 +42,35 @@ __device__ __forceinline__ float bev_sample(const float* __restrict__ v, int nx,
 
 // Transfer box from the eight BEV corners (wrapper.cu:5343-5394); the z range spans
 // the deepest superposed step of all layers, or of `layer` alone when it is given.
-__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const LayerStateDev* layer) {
+// With `live` the corners are those of the cells the superposition items can have
+// written (BeamStateDev::liveLo/liveHi, one cell of trilinear reach added): every
+// voxel outside samples only zero cells, so the transfer and the box's readers skip
+// it. No live cell gives an empty box.
+__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const LayerStateDev* layer, int live) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     // Last kernel of the beam's work list with one thread: hand the beam's error
     // flags to the context's error word, which outlives the beam state.
     if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
     const int first = beam->firstInside;
     const int passive = layer ? layer->calcPassive : beam->maxCalcPassive;
-    const float xs[2] = {-float(kMaxR), float(g.pitchX + kMaxR - 1)};
-    const float ys[2] = {-float(kMaxR), float(g.pitchY + kMaxR - 1)};
-    const float zs[2] = {float(first), float(passive - 1)};
+    float xs[2] = {-float(kMaxR), float(g.pitchX + kMaxR - 1)};
+    float ys[2] = {-float(kMaxR), float(g.pitchY + kMaxR - 1)};
+    float zs[2] = {float(first), float(passive - 1)};
+    if (live) {
+        if (beam->liveLo[0] > beam->liveHi[0]) {
+            beam->transferValid = 0;
+            beam->transferStart[0] = beam->transferStart[1] = beam->transferStart[2] = 0;
+            beam->transferMax[0] = beam->transferMax[1] = beam->transferMax[2] = -1;
+            return;
+        }
+        // Padded BEV cell c is ray coordinate c - kMaxR.
+        xs[0] = fmaxf(xs[0], float(beam->liveLo[0] - kMaxR - 1));
+        xs[1] = fminf(xs[1], float(beam->liveHi[0] - kMaxR + 1));
+        ys[0] = fmaxf(ys[0], float(beam->liveLo[1] - kMaxR - 1));
+        ys[1] = fminf(ys[1], float(beam->liveHi[1] - kMaxR + 1));
+        zs[0] = fmaxf(zs[0], float(first + beam->liveLo[2] - 1));
+        zs[1] = fminf(zs[1], float(first + beam->liveHi[2] + 1));
+    }
     V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
     for (int zi = 0; zi < 2; ++zi)
         for (int yi = 0; yi < 2; ++yi)
@@ -157,9 +176,9 @@ __global__ void dose_box_kernel(double* dose, float* out, int3 dims, int3 lo, in
 
 }  // namespace
 
-cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer,
+cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer, int live,
                                     cudaStream_t s) {
-    transfer_planner_kernel<<<1, 32, 0, s>>>(g, beam, layer);
+    transfer_planner_kernel<<<1, 32, 0, s>>>(g, beam, layer, live);
     return cudaGetLastError();
 }
 
