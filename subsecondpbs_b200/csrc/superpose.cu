@@ -153,8 +153,10 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
 
     // Table phase of one layer (complete_superposition.cu:298-307): thread t is source
     // (sy, sx) = (warp, lane); its rows e_s(0..R) go in float4 chunks (chunk-major)
-    // and idd_s e_s(0..R); sources without dose get zero rows, and colMask[sx]
-    // collects the depositing sources of every column.
+    // and idd_s e_s(0..R) 2^sc (the fixed-point scale is a power of two, so the column
+    // sums come out scaled exactly as if each were scaled at the flush); sources
+    // without dose get zero rows, and colMask[sx] collects the depositing sources of
+    // every column.
     auto table = [&](unsigned lc, unsigned* colMask) {
         const size_t src = lc * a.layerStride + a.src;
         const float dose = a.idd[src];
@@ -164,10 +166,11 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
         if (live) {
             float row[R + 1];
             superposition_row<R>(a.rsig[src], row);
+            const float doseScaled = dose * scale;
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 e[k] = row[k];
-                EW[t * EWS + k] = dose * row[k];
+                EW[t * EWS + k] = doseScaled * row[k];
             }
         } else {
 #pragma unroll
@@ -213,7 +216,7 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
     auto flush = [&](int sx, int d, const float (&acc)[H]) {
         int qv[H];
 #pragma unroll
-        for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(acc[i] * scale);
+        for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(acc[i]);
         int* col = out + sx + R + d;
 #pragma unroll
         for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
@@ -488,6 +491,14 @@ __device__ __forceinline__ int block_slot(const RadiusBlocks<RLo, RHi>& b, int c
 // time through the range's counter (the next claim is issued before the current
 // item runs so that its latency is hidden). Items are taken radius block by radius
 // block, so the CTAs of the SM mostly run the code of one radius at a time.
+//
+// The three instances of a beam are launched back to back with programmatic
+// dependent launch: every CTA lets the next instance start at once (its items are
+// independent of this instance's: both only add to the fixed-point BEV), so the next
+// instance's CTAs take the SMs this instance's CTAs leave at its tail. Before it
+// exits a CTA waits for the previous instance to complete, so an instance is complete
+// only once all earlier ones are, and the kernel after the last one (launched
+// normally) sees every item's adds.
 template <bool kWide, int RLo, int RHi, int MinBlocks>
 __global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
@@ -500,6 +511,7 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
     __shared__ float sSum[kTileY];
     __shared__ RadiusBlocks<RLo, RHi> sBlocks;
 
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int t = threadIdx.x;
     // Range 0: R > kSplitR, 1: kSplitR2 < R <= kSplitR, 2: R <= kSplitR2.
     int* counter = range == 0 ? &beam->workNext : (range == 1 ? &beam->workNextSmall : &beam->workNextTiny);
@@ -547,18 +559,30 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
         __syncthreads();
         buf ^= 1;
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// `overlap`: launch as a programmatic dependent of the previous kernel on `s` (the
+// previous superposition instance).
 template <bool kWide, int RLo, int RHi, int MinBlocks>
 cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                          BeamStateDev* beam, unsigned long long* bev, int shiftOffset, int gridBlocks, int range,
-                         cudaStream_t s) {
+                         bool overlap, cudaStream_t s) {
     auto k = superpose_kernel<kWide, RLo, RHi, MinBlocks>;
     const size_t smem = kWide ? WideShape<RHi>::kSmemBytes : PairShape<RHi>::kSmemBytes;
     cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
-    k<<<gridBlocks, kThreads, smem, s>>>(g, idd, rsigma, work, beam, bev, shiftOffset, range);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(gridBlocks);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, g, idd, rsigma, work, beam, bev, shiftOffset, range);
 }
 
 // Adds the fixed-point BEV of the chunk (the planes written so far,
@@ -599,13 +623,13 @@ cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float
                              cudaStream_t s) {
     // Items are sorted by range: the wide radii come first.
     cudaError_t e = launch_range<true, kSplitR + 1, kMaxR, kWideBlocks>(g, idd, rsigma, work, beam, bevFixed,
-                                                                        shiftOffset, numSMs * kWideBlocks, 0, s);
+                                                                        shiftOffset, numSMs * kWideBlocks, 0, false, s);
     if (e != cudaSuccess) return e;
     e = launch_range<false, kSplitR2 + 1, kSplitR, kMidBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
-                                                               numSMs * kMidBlocks, 1, s);
+                                                               numSMs * kMidBlocks, 1, true, s);
     if (e != cudaSuccess) return e;
     e = launch_range<false, 0, kSplitR2, kNarrowBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
-                                                        numSMs * kNarrowBlocks, 2, s);
+                                                        numSMs * kNarrowBlocks, 2, true, s);
     if (e != cudaSuccess) return e;
     bev_fixed_to_float_kernel<<<numSMs * 8, 256, 0, s>>>(g, beam, bevFixed, bev, shiftOffset);
     return cudaGetLastError();

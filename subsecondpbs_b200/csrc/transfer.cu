@@ -23,14 +23,33 @@ __device__ __forceinline__ float bev_sample(const float* __restrict__ v, int nx,
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
     const int x0 = int(fx), y0 = int(fy), z0 = int(fz);
     const float tx = x - fx, ty = y - fy, tz = z - fz;
-    auto at = [&](int xi, int yi, int zi) -> float {
-        if (xi < 0 || yi < 0 || zi < 0 || xi >= nx || yi >= ny || zi >= nz) return 0.0f;
-        return __ldg(v + (static_cast<size_t>(zi) * ny + yi) * nx + xi);
-    };
-    const float c000 = at(x0, y0, z0), c100 = at(x0 + 1, y0, z0);
-    const float c010 = at(x0, y0 + 1, z0), c110 = at(x0 + 1, y0 + 1, z0);
-    const float c001 = at(x0, y0, z0 + 1), c101 = at(x0 + 1, y0, z0 + 1);
-    const float c011 = at(x0, y0 + 1, z0 + 1), c111 = at(x0 + 1, y0 + 1, z0 + 1);
+    float c000, c100, c010, c110, c001, c101, c011, c111;
+    if (x0 >= 0 && y0 >= 0 && z0 >= 0 && x0 + 1 < nx && y0 + 1 < ny && z0 + 1 < nz) {
+        // All eight texels inside: one base address.
+        const size_t plane = static_cast<size_t>(nx) * ny;
+        const float* p = v + (static_cast<size_t>(z0) * ny + y0) * nx + x0;
+        c000 = __ldg(p);
+        c100 = __ldg(p + 1);
+        c010 = __ldg(p + nx);
+        c110 = __ldg(p + nx + 1);
+        c001 = __ldg(p + plane);
+        c101 = __ldg(p + plane + 1);
+        c011 = __ldg(p + plane + nx);
+        c111 = __ldg(p + plane + nx + 1);
+    } else {
+        auto at = [&](int xi, int yi, int zi) -> float {
+            if (xi < 0 || yi < 0 || zi < 0 || xi >= nx || yi >= ny || zi >= nz) return 0.0f;
+            return __ldg(v + (static_cast<size_t>(zi) * ny + yi) * nx + xi);
+        };
+        c000 = at(x0, y0, z0);
+        c100 = at(x0 + 1, y0, z0);
+        c010 = at(x0, y0 + 1, z0);
+        c110 = at(x0 + 1, y0 + 1, z0);
+        c001 = at(x0, y0, z0 + 1);
+        c101 = at(x0 + 1, y0, z0 + 1);
+        c011 = at(x0, y0 + 1, z0 + 1);
+        c111 = at(x0 + 1, y0 + 1, z0 + 1);
+    }
     const float c00 = c000 + (c100 - c000) * tx;
     const float c10 = c010 + (c110 - c010) * tx;
     const float c01 = c001 + (c101 - c001) * tx;
@@ -104,7 +123,7 @@ __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const
 // read-modify-writes are coalesced, and a persistent grid strides over the items.
 // The chunk's voxels are sampled with independent loads (unrolled loop), so the
 // latency of the BEV samples and of the dose reads overlaps.
-constexpr int kTransferZChunk = 8;
+constexpr int kTransferZChunk = 4;
 constexpr int kTransferBlocksPerSM = 8;
 
 __global__ void __launch_bounds__(256)
