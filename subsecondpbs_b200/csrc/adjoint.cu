@@ -104,24 +104,120 @@ __device__ __forceinline__ void superpose_adjoint_tile(const float* __restrict__
     atomicAdd(rbarRay, dose * acc);
 }
 
-template <int R, int RHi>
-__device__ __forceinline__ void adjoint_dispatch(int r, const float* tileG, float* eRow, float dose, float rs,
-                                                 float* rbarRay, int sy, int sx) {
-    if (r == R) {
-        superpose_adjoint_tile<R>(tileG, eRow, dose, rs, rbarRay, sy, sx);
-        return;
+// S^T for one tile at radius R <= kSplitR, in the forward's (source column, |d|)
+// pair form. A source's gradient is
+//   sum_d e(d) P_d,  P_d = sum_k e(|k|) c_d[sy + R + k],
+// where c_d is the sum of the footprint's gradient columns sx + R + d and
+// sx + R - d (one column for d = 0), the same for the eight sources of the column.
+// A lane is one (column, |d|) pair: it sums its two gradient columns once into
+// registers, then forms P_d for the column's eight sources with their weights read
+// as broadcast float4 chunks, and stores them; each source thread then sums
+// e(d) P_d over d. The shared-memory reads per source drop from (2R+1)^2 scalars
+// to about (2H + 8 Q)/8 per pair.
+template <int R>
+__device__ __forceinline__ void superpose_adjoint_pairs(const float* __restrict__ tileG, float4* __restrict__ E4,
+                                                        float* __restrict__ P, float dose, float rs,
+                                                        float* __restrict__ rbarRay) {
+    constexpr int H = kTileY + 2 * R;
+    constexpr int Wo = kTileX + 2 * R;
+    constexpr int Q = (R + 1 + 3) / 4;
+    constexpr int PS = (R + 1) | 1;             // odd row stride of P
+    constexpr int M = R + 1;
+    constexpr int G = 32 / M;                   // source columns per warp instruction
+    constexpr int S = (32 + G - 1) / G;         // column spacing, units
+    const int t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31;
+    const bool live = rbarRay != nullptr;
+    // Weights of source t = (sy, sx) = (warp, lane), chunk-major with the column
+    // swizzle of the forward kernel.
+    float e[4 * Q];
+    if (live) {
+        float row[R + 1];
+        superposition_row<R>(rs, row);
+#pragma unroll
+        for (int k = 0; k <= R; ++k) e[k] = row[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k <= R; ++k) e[k] = 0.0f;
     }
-    if constexpr (R < RHi) adjoint_dispatch<R + 1, RHi>(r, tileG, eRow, dose, rs, rbarRay, sy, sx);
+#pragma unroll
+    for (int k = R + 1; k < 4 * Q; ++k) e[k] = 0.0f;
+    const int col = lane ^ ((lane >> 3) & 3);
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        E4[q * kAdjThreads + warp * kTileX + col] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
+    __syncthreads();
+#pragma unroll 1
+    for (int u = warp; u < S; u += kAdjThreads / 32) {
+        const int g = lane / M;
+        int d = lane - g * M;
+        int sx = u + g * S;
+        const bool valid = g < G && sx < kTileX;
+        if (!valid) {
+            sx = 0;
+            d = 0;
+        }
+        float c[H];
+        const float* ca = tileG + sx + R + d;
+        const float* cb = tileG + sx + R - d;
+#pragma unroll
+        for (int i = 0; i < H; ++i) c[i] = ca[i * Wo] + (d > 0 ? cb[i * Wo] : 0.0f);
+        const float4* eCol = E4 + (sx ^ ((sx >> 3) & 3));
+#pragma unroll
+        for (int sy = 0; sy < kTileY; ++sy) {
+            float ev[4 * Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const float4 v = eCol[q * kAdjThreads + sy * kTileX];
+                ev[4 * q] = v.x;
+                ev[4 * q + 1] = v.y;
+                ev[4 * q + 2] = v.z;
+                ev[4 * q + 3] = v.w;
+            }
+            float pd = ev[0] * c[sy + R];
+#pragma unroll
+            for (int k = 1; k <= R; ++k) pd = fmaf(ev[k], c[sy + R - k] + c[sy + R + k], pd);
+            if (valid) P[(sy * kTileX + sx) * PS + d] = pd;
+        }
+    }
+    __syncthreads();
+    if (live) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k <= R; ++k) acc = fmaf(e[k], P[t * PS + k], acc);
+        atomicAdd(rbarRay, dose * acc);
+    }
 }
 
-// Persistent CTAs over the whole work list of the (single) layer chunk.
-__global__ void __launch_bounds__(kAdjThreads)
+// Radii above kSplitR gather per source (superpose_adjoint_tile); the others run
+// in pair form with every thread of the CTA (rbarRay null: no live source).
+template <int R, int RHi>
+__device__ __forceinline__ void adjoint_dispatch(int r, const float* tileG, float* eRow, float4* E4, float* P,
+                                                 float dose, float rs, float* rbarRay, int sy, int sx) {
+    if (r == R) {
+        if constexpr (R <= kSplitR) {
+            superpose_adjoint_pairs<R>(tileG, E4, P, dose, rs, rbarRay);
+        } else {
+            if (rbarRay) superpose_adjoint_tile<R>(tileG, eRow, dose, rs, rbarRay, sy, sx);
+        }
+        return;
+    }
+    if constexpr (R < RHi) adjoint_dispatch<R + 1, RHi>(r, tileG, eRow, E4, P, dose, rs, rbarRay, sy, sx);
+}
+
+// Persistent CTAs over the whole work list of the (single) layer chunk; three per
+// SM, as many as their shared memory allows.
+__global__ void __launch_bounds__(kAdjThreads, 3)
 superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
                          const int4* __restrict__ work, BeamStateDev* __restrict__ beam, const float* __restrict__ gradBev,
                          float* __restrict__ rbar) {
-    extern __shared__ float adjSm[];
+    extern __shared__ __align__(16) float adjSm[];
     float* tileG = adjSm;                        // [8+2R][32+2R] BEV gradient of the tile's footprint
-    float* eS = adjSm + kAdjOutFloats;           // [256][kAdjEStride] each source's weights
+    float* eS = adjSm + kAdjOutFloats;           // [256][kAdjEStride] each source's weights (R > kSplitR)
+    // Pair form (R <= kSplitR): the weights as float4 chunks [4][256] and the pair
+    // sums P [256][17], over the same space.
+    float4* E4 = reinterpret_cast<float4*>(eS);
+    float* P = eS + 4 * 4 * kAdjThreads;
     __shared__ int sItem;
     const int t = threadIdx.x;
     const int count = beam->workCount;
@@ -149,9 +245,10 @@ superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const flo
         const int ry = ty * kTileY + sy, rx = tx * kTileX + sx;
         const size_t s = lc * layerStride + zRel * padPlane + static_cast<size_t>(ry) * g.pitchX + rx;
         const float dose = idd[s];
-        if (dose > 0.0f && ry < g.rayY && rx < g.rayX)
-            adjoint_dispatch<0, kMaxR>(R, tileG, eS + t * kAdjEStride, dose, rsig[s],
-                                       rbar + lc * rayPlane + static_cast<size_t>(ry) * g.rayX + rx, sy, sx);
+        const bool live = dose > 0.0f && ry < g.rayY && rx < g.rayX;
+        adjoint_dispatch<0, kMaxR>(R, tileG, eS + t * kAdjEStride, E4, P, dose, live ? rsig[s] : 0.0f,
+                                   live ? rbar + lc * rayPlane + static_cast<size_t>(ry) * g.rayX + rx : nullptr,
+                                   sy, sx);
         __syncthreads();
     }
 }
