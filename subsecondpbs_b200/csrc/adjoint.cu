@@ -231,7 +231,7 @@ superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const flo
         const int w = sItem;
         if (w >= count) break;
         const int4 it = work[w];
-        const int lc = it.x, tile = it.y, zRel = it.z, R = it.w;
+        const int lc = it.x & 0xff, tile = it.y, zRel = it.z, R = it.w;
         const int tx = tile % g.tilesX, ty = tile / g.tilesX;
         const int Ho = kTileY + 2 * R, Wo = kTileX + 2 * R;
         const float* src = gradBev + static_cast<size_t>(zRel) * bevPlane +

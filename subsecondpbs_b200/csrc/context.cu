@@ -828,8 +828,13 @@ int Context::adjoint_beam(const PbsBeamDesc& b, const double* gradDose, int grad
     return run_beam(b, 0, &a);
 }
 
-int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned) {
+int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned,
+                      ColumnSink* cols) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    if (cols && (nuclear || adj || bioModel)) {
+        set_error("batched influence columns: not available with the nuclear halo, the adjoint or biological maps");
+        return PBS_ERR_UNSUPPORTED;
+    }
     // Buffers may be resized below: nothing of an earlier beam may still be clearing them.
     if (int jrc = join_side_work()) return jrc;
     if (!hasEnergy || !hasCt || !hasDose) {
@@ -977,6 +982,9 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     const bool perLayerTransfer = compatBevZShift && !adj;
     const int chunk = perLayerTransfer ? 1 : z.chunk;
     chunkLayers = chunk;
+    // Batched influence columns (a sink): each layer of a chunk is superposed from its
+    // own work list, selected from the chunk's one-layer list, and transferred alone.
+    const bool columnLists = cols && !perLayerTransfer;
 
     // The trace's home: the store's resident copy for this geometry, else the
     // context's own buffers.
@@ -1251,7 +1259,11 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             }
             doseReady = true;
         }
-        PBS_CUDA(launch_transfer_planner(g, dbs, layer, !perLayerTransfer, stream), "transfer_planner");
+        // The box over the cells the items wrote: the whole beam's (work_merge_kernel),
+        // or a column's layer (work_layer_view_kernel); the per-layer transfers of the
+        // reference's depth convention take the box over the layer's steps.
+        PBS_CUDA(launch_transfer_planner(g, dbs, layer, layer == nullptr || columnLists, stream),
+                 "transfer_planner");
         PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
         if (bio) {
             // The beam's own dose and the channels into the biological accumulators.
@@ -1269,7 +1281,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             }
         }
         if (nuclear) {
-            PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, nucLayer, !perLayerTransfer, stream),
+            PBS_CUDA(launch_transfer_planner(nucGeom, dNucBs, nucLayer, nucLayer == nullptr, stream),
                      "nuc_transfer_planner");
             PBS_CUDA(launch_transfer(nucGeom, static_cast<const float*>(nucBev.ptr), dNucBs,
                                      static_cast<double*>(dose64.ptr), stream),
@@ -1288,7 +1300,8 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
                  "idd");
         if (l0 == 0 && (rc = mark(4))) return rc;
         PBS_CUDA(launch_bin_plan(g, l0, nl, static_cast<const uint8_t*>(codes.ptr), dls, dbs,
-                                 static_cast<int4*>(work.ptr), workCap, adj == nullptr, nullptr, nullptr, stream),
+                                 static_cast<int4*>(work.ptr), workCap, adj == nullptr && !columnLists, nullptr,
+                                 nullptr, stream),
                  "bin_plan");
         if (nuclear) {
             PBS_CUDA(launch_nuc_codes(nucGeom, l0, nl, dNucIdd, dNucRs, dls, dbs, dNucLs,
@@ -1301,6 +1314,22 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         if (l0 == 0 && (rc = mark(5))) return rc;
         if (adj) break;  // the adjoint's superposition runs after the transfer box is known
         unsigned long long* dFixed = static_cast<unsigned long long*>(bevFixed.ptr);
+        if (columnLists) {
+            // One column per layer: its items, superposition and transfer, the sink's
+            // compaction, then an empty BEV for the next layer.
+            for (int q = 0; q < nl; ++q) {
+                PBS_CUDA(launch_work_layer_view(l0, q, dls, dbs, workCap, stream), "work_layer_view");
+                bevFixedClean = false;
+                PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
+                                          static_cast<const int4*>(work.ptr), dbs, dBev, dFixed, 0, smCount, stream),
+                         "superpose");
+                bevFixedClean = true;
+                if ((rc = transfer_layers(dls + l0 + q, nullptr))) return rc;
+                if ((rc = cols->column(l0 + q))) return rc;
+                PBS_CUDA(cudaMemsetAsync(dBev, 0, S * size_t(g.bevX) * g.bevY * 4, stream), "memset BEV");
+            }
+            continue;
+        }
         bevFixedClean = false;
         PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
                                   static_cast<const int4*>(work.ptr), dbs, dBev, dFixed, 0, smCount, stream),
@@ -1335,6 +1364,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             // This layer alone, then empty BEV volumes for the next one (the last
             // layer's BEV stays for the debug readouts).
             if ((rc = transfer_layers(dls + l0, nuclear ? dNucLs + l0 : nullptr))) return rc;
+            if (cols && (rc = cols->column(l0))) return rc;
         }
         if (perLayerTransfer && l0 + nl < L) {
             PBS_CUDA(cudaMemsetAsync(dBev, 0, S * size_t(g.bevX) * g.bevY * 4, stream), "memset BEV");
@@ -1350,7 +1380,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     }
     if ((rc = mark(6))) return rc;
     if (adj) return finish_adjoint(*adj, b);
-    if (!perLayerTransfer && (rc = transfer_layers(nullptr, nullptr))) return rc;
+    if (!perLayerTransfer && !cols && (rc = transfer_layers(nullptr, nullptr))) return rc;
     if ((rc = mark(7))) return rc;
     lastChunks = (L + chunk - 1) / chunk;
     // trace, planner, two fluence kernels, seven per chunk (IDD, layer plan, work

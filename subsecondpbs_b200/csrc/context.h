@@ -171,6 +171,7 @@ struct Context {
     DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice, weqBody;
     // Influence export: column offsets, per-block offsets, and the entries.
     DevBuf opColPtr, opBlockOff, opRows, opVals, opNorm, opVoxels;
+
     PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
     cudaEvent_t ev[8] = {};
@@ -241,7 +242,17 @@ struct Context {
         float* gradSpots;
         size_t nSpots;
     };
-    int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned = nullptr);
+    // Receives the columns of a batched influence export. With a sink, run_beam gives
+    // every layer of the plan its own superposition and transfer (each layer of the
+    // plan is one column: one spot at unit weight) and calls column(layer) once that
+    // layer's dose is in the FP64 grid and before the next layer's transfer; a column
+    // must leave the grid zero again (the compaction does).
+    struct ColumnSink {
+        virtual ~ColumnSink() = default;
+        virtual int column(int layer) = 0;
+    };
+    int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned = nullptr,
+                 ColumnSink* cols = nullptr);
     int finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b);
     // Dose-influence columns of spots [spotBegin, spotBegin + spotCount) in CSC:
     // colPtr[spotCount + 1] (host, from 0), rows = linear voxel indices in ascending
@@ -267,6 +278,11 @@ struct Context {
     // Dose of one spot at unit weight into the FP64 grid (zeroed first unless
     // `gridZero` says it is zero already), with the box of voxels it can have written.
     int run_column(ColumnPlan& cp, size_t spot, int nuclear, void* box, bool gridZero = false);
+    // Doses of spots [firstSpot, firstSpot + count) at unit weight, one column at a
+    // time into the FP64 grid (zeroed first unless `gridZero`), from one pass over a
+    // plan with one layer per spot; sink.column(q) receives spot firstSpot + q.
+    // Not for the nuclear halo, biological maps or the CarbonPBS profile model.
+    int run_column_batch(ColumnPlan& cp, size_t firstSpot, int count, ColumnSink& sink, bool gridZero);
     int influence_csc(const PbsBeamDesc& b, int nuclear, long long spotBegin, long long spotCount, double threshold,
                       long long* colPtr, int* rows, float* vals, long long capacity, long long* nnz);
     int beam_stats(PbsBeamStats* out);

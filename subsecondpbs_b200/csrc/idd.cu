@@ -535,7 +535,11 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
 }
 
 // One thread per (layer, step, tile) code of the chunk: live tiles are written to
-// their layer's radius group of the work list.
+// their layer's radius group of the work list as one-layer items in the forward
+// superposition's format (x = the chunk layer in the low byte, 0xff above it). Each
+// layer's box of the cells its items can write (LayerStateDev::liveLo/liveHi) is
+// reduced per warp (a warp's 32 consecutive codes span at most a few layers) before
+// its atomics.
 __global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restrict__ codes,
                                     LayerStateDev* __restrict__ ls, const BeamStateDev* __restrict__ beam,
                                     int4* __restrict__ work, int workCapacity) {
@@ -543,17 +547,49 @@ __global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, cons
     const int first = beam->firstInside;
     const size_t perLayer = static_cast<size_t>(g.steps) * tiles;
     const size_t total = perLayer * nLayers;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
-        const int lc = int(i / perLayer);
-        const int rem = int(i - size_t(lc) * perLayer);
-        const int zr = rem / tiles;
-        LayerStateDev& st = ls[layer0 + lc];
-        if (zr >= st.afterLast - first) continue;
-        const int c = codes[i];
-        if (!(c & 0x80)) continue;
-        const int R = st.batchedR[c & 0x3f];
-        const int slot = st.offR[R] + atomicAdd(&st.curR[R], 1);
-        if (slot < workCapacity) work[slot] = make_int4(lc, rem - zr * tiles, zr, R);
+    const int lane = threadIdx.x & 31;
+    // Warp-uniform trip count: every lane takes part in the reductions.
+    for (size_t i0 = blockIdx.x * size_t(blockDim.x) + threadIdx.x - lane; i0 < total;
+         i0 += size_t(gridDim.x) * blockDim.x) {
+        const size_t i = i0 + lane;
+        int key = -1, R = 0, tile = 0, zr = 0;
+        if (i < total) {
+            const int lc = int(i / perLayer);
+            const int rem = int(i - size_t(lc) * perLayer);
+            zr = rem / tiles;
+            tile = rem - zr * tiles;
+            LayerStateDev& st = ls[layer0 + lc];
+            const int c = codes[i];
+            if (zr < st.afterLast - first && (c & 0x80)) {
+                R = st.batchedR[c & 0x3f];
+                const int slot = st.offR[R] + atomicAdd(&st.curR[R], 1);
+                if (slot < workCapacity)
+                    work[slot] = make_int4(static_cast<int>(0xffffff00u | static_cast<unsigned>(lc)), tile, zr, R);
+                key = lc;
+            }
+        }
+        if (!__any_sync(0xffffffffu, key >= 0)) continue;
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        const int tx = tile % g.tilesX, ty = tile / g.tilesX;
+        const int lo0 = key >= 0 ? tx * kTileX - R + kMaxR : INT_MAX;
+        const int lo1 = key >= 0 ? ty * kTileY - R + kMaxR : INT_MAX;
+        const int lo2 = key >= 0 ? zr : INT_MAX;
+        const int hi0 = key >= 0 ? tx * kTileX + kTileX - 1 + R + kMaxR : INT_MIN;
+        const int hi1 = key >= 0 ? ty * kTileY + kTileY - 1 + R + kMaxR : INT_MIN;
+        const int hi2 = key >= 0 ? zr : INT_MIN;
+        const int mlo0 = __reduce_min_sync(same, lo0), mlo1 = __reduce_min_sync(same, lo1);
+        const int mlo2 = __reduce_min_sync(same, lo2);
+        const int mhi0 = __reduce_max_sync(same, hi0), mhi1 = __reduce_max_sync(same, hi1);
+        const int mhi2 = __reduce_max_sync(same, hi2);
+        if (key >= 0 && lane == __ffs(same) - 1) {
+            LayerStateDev& st = ls[layer0 + key];
+            atomicMin(&st.liveLo[0], mlo0);
+            atomicMin(&st.liveLo[1], mlo1);
+            atomicMin(&st.liveLo[2], mlo2);
+            atomicMax(&st.liveHi[0], mhi0);
+            atomicMax(&st.liveHi[1], mhi1);
+            atomicMax(&st.liveHi[2], mhi2);
+        }
     }
 }
 
@@ -731,6 +767,36 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
     if (e != cudaSuccess) return e;
     k<<<grid, block, smem, s>>>(g, luts, layer0, density, wepl, firstInside, firstOutside, rayW, lp, ls, beam, idd,
                                 rsigma, codes, firstPassive, rayToNuc, lattice, nucIdd, nucRsigma);
+    return cudaGetLastError();
+}
+
+// Points the forward superposition at one layer of the chunk's one-layer work list
+// (work_scatter_kernel): the layer's radius-R items are the block at ls.offR[R]
+// (the next block of the list starts at or after its end, so superpose_kernel's
+// block bounds hold), the claim counters restart, and the live-cell box is the
+// layer's, for the transfer planner.
+__global__ void work_layer_view_kernel(int layer0, int lc, const LayerStateDev* __restrict__ ls,
+                                       BeamStateDev* __restrict__ beam, int workCapacity) {
+    const LayerStateDev& st = ls[layer0 + lc];
+    const int t = threadIdx.x;
+    if (t <= kMaxR) {
+        beam->rStart[t] = st.offR[t];
+        beam->mergedR[t] = max(min(st.liveR[t], workCapacity - st.offR[t]), 0);
+    }
+    if (t < 3) {
+        beam->liveLo[t] = st.liveLo[t];
+        beam->liveHi[t] = st.liveHi[t];
+    }
+    if (t == 0) {
+        beam->workNext = 0;
+        beam->workNextSmall = 0;
+        beam->workNextTiny = 0;
+    }
+}
+
+cudaError_t launch_work_layer_view(int layer0, int lc, const LayerStateDev* ls, BeamStateDev* beam, int workCapacity,
+                                   cudaStream_t s) {
+    work_layer_view_kernel<<<1, 64, 0, s>>>(layer0, lc, ls, beam, workCapacity);
     return cudaGetLastError();
 }
 

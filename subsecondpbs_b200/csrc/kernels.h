@@ -82,10 +82,15 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
 // plans the nuclear halo grid `g` instead (no merge: a radius above 32 sets error
 // flag 4). `merged` selects the forward superposition's list (items of up to
 // kMergeLayers layers of one tile and step with one radius, x = the layers as bytes)
-// over the one-layer items {layer, tile, step, radius} the adjoint gathers from.
+// over the one-layer items {layer | 0xffffff00, tile, step, radius} the adjoint
+// gathers from, with each layer's box of live cells.
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
                             BeamStateDev* beam, int4* work, int workCapacity, bool merged,
                             const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, cudaStream_t s);
+// Points the forward superposition at chunk layer `lc`'s items of the one-layer list
+// (merged == false above) and the transfer planner's live box at that layer's.
+cudaError_t launch_work_layer_view(int layer0, int lc, const LayerStateDev* ls, BeamStateDev* beam, int workCapacity,
+                                   cudaStream_t s);
 // Nuclear halo: clear the chunk's halo IDD (0) and sigma (+inf) before the IDD
 // kernel, and the halo tile codes and histograms after the primary layer plan.
 // `gn` is the halo grid (pitch = nucX x nucY).

@@ -27,7 +27,8 @@ namespace {
 
 constexpr int kOpThreads = 256;
 constexpr int kOpPasses = 8;
-constexpr int kOpChunk = kOpThreads * kOpPasses;  // box voxels per block
+constexpr int kOpChunk = kOpThreads * kOpPasses;  // box voxels per chunk
+constexpr int kOpGridBlocks = 148 * 4;              // blocks striding over a column's chunks
 
 // The columns of one export share the beam's geometry and so its trace: the first
 // column traces into this store's buffer and the others skip the tracer and wait
@@ -136,28 +137,37 @@ __device__ __forceinline__ OpBox column_box(const OpBox& a, const BeamStateDev* 
     return e;
 }
 
-// Entries above the threshold in each block's chunk of the column's box.
+// Entries above the threshold in each kOpChunk-voxel chunk of the column's box
+// (column_box: known on the device only), the blocks striding over the chunks; block
+// 0 also stores the number of chunks for the scan.
 __global__ void __launch_bounds__(kOpThreads) influence_count_kernel(const double* __restrict__ dose, OpBox host,
                                                                      const BeamStateDev* __restrict__ pb,
                                                                      const BeamStateDev* __restrict__ nb,
-                                                                     double thr, long long* __restrict__ blockOff) {
+                                                                     double thr, long long* __restrict__ blockOff,
+                                                                     long long* __restrict__ nChunksOut) {
     const OpBox a = column_box(host, pb, nb);
-    const long long base = static_cast<long long>(blockIdx.x) * kOpChunk;
-    int c = 0;
-    for (int p = 0; p < kOpPasses; ++p) {
-        const long long b = base + p * kOpThreads + threadIdx.x;
-        const bool keep = b < a.n && fabs(dose[box_to_grid(a, b)]) > thr;
-        c += __syncthreads_count(keep);
+    const long long nChunks = (a.n + kOpChunk - 1) / kOpChunk;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nChunksOut = nChunks;
+    for (long long ch = blockIdx.x; ch < nChunks; ch += gridDim.x) {
+        const long long base = ch * kOpChunk;
+        int c = 0;
+        for (int p = 0; p < kOpPasses; ++p) {
+            const long long b = base + p * kOpThreads + threadIdx.x;
+            const bool keep = b < a.n && fabs(dose[box_to_grid(a, b)]) > thr;
+            c += __syncthreads_count(keep);
+        }
+        if (threadIdx.x == 0) blockOff[ch] = c;
     }
-    if (threadIdx.x == 0) blockOff[blockIdx.x] = c;
 }
 
-// One block: block counts -> absolute exclusive offsets (starting at colPtr[col]),
+// One block: chunk counts -> absolute exclusive offsets (starting at colPtr[col]),
 // and colPtr[col + 1] = colPtr[col] + entries of the column.
-__global__ void __launch_bounds__(1024) influence_scan_kernel(long long* __restrict__ blockOff, int nBlocks,
+__global__ void __launch_bounds__(1024) influence_scan_kernel(long long* __restrict__ blockOff,
+                                                              const long long* __restrict__ nChunksIn,
                                                               long long* __restrict__ colPtr, int col) {
     __shared__ long long carry;
     __shared__ long long warpSums[32];
+    const int nBlocks = static_cast<int>(*nChunksIn);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) carry = colPtr[col];
     __syncthreads();
@@ -190,9 +200,10 @@ __global__ void __launch_bounds__(1024) influence_scan_kernel(long long* __restr
     if (threadIdx.x == 0) colPtr[col + 1] = carry;
 }
 
-// Ordered compaction of each block's chunk: entries keep the box order, which is
-// ascending voxel order. Entries past `cap` are counted but not written. Every voxel
-// of the box is zeroed once read, so the grid is zero again for the next column.
+// Ordered compaction of each chunk, the blocks striding over the chunks as in the
+// count: entries keep the box order, which is ascending voxel order. Entries past
+// `cap` are counted but not written. Every voxel of the box is zeroed once read, so
+// the grid is zero again for the next column.
 __global__ void __launch_bounds__(kOpThreads) influence_write_kernel(double* __restrict__ dose, OpBox host,
                                                                      const BeamStateDev* __restrict__ pb,
                                                                      const BeamStateDev* __restrict__ nb,
@@ -201,40 +212,68 @@ __global__ void __launch_bounds__(kOpThreads) influence_write_kernel(double* __r
                                                                      long long cap) {
     __shared__ int warpCounts[kOpThreads / 32];
     const OpBox a = column_box(host, pb, nb);
+    const long long nChunks = (a.n + kOpChunk - 1) / kOpChunk;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    long long pos = blockOff[blockIdx.x];
-    const long long base = static_cast<long long>(blockIdx.x) * kOpChunk;
-    for (int p = 0; p < kOpPasses; ++p) {
-        const long long b = base + p * kOpThreads + threadIdx.x;
-        long long g = 0;
-        double v = 0.0;
-        bool keep = false;
-        if (b < a.n) {
-            g = box_to_grid(a, b);
-            v = dose[g];
-            dose[g] = 0.0;
-            keep = fabs(v) > thr;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) warpCounts[warp] = __popc(m);
-        __syncthreads();
-        int before = 0, total = 0;
-        for (int w = 0; w < kOpThreads / 32; ++w) {
-            const int c = warpCounts[w];
-            if (w < warp) before += c;
-            total += c;
-        }
-        if (keep) {
-            const long long at = pos + before + __popc(m & ((1u << lane) - 1u));
-            if (at < cap) {
-                rows[at] = static_cast<int>(g);
-                vals[at] = static_cast<float>(v);
+    for (long long ch = blockIdx.x; ch < nChunks; ch += gridDim.x) {
+        long long pos = blockOff[ch];
+        const long long base = ch * kOpChunk;
+        for (int p = 0; p < kOpPasses; ++p) {
+            const long long b = base + p * kOpThreads + threadIdx.x;
+            long long g = 0;
+            double v = 0.0;
+            bool keep = false;
+            if (b < a.n) {
+                g = box_to_grid(a, b);
+                v = dose[g];
+                dose[g] = 0.0;
+                keep = fabs(v) > thr;
             }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) warpCounts[warp] = __popc(m);
+            __syncthreads();
+            int before = 0, total = 0;
+            for (int w = 0; w < kOpThreads / 32; ++w) {
+                const int c = warpCounts[w];
+                if (w < warp) before += c;
+                total += c;
+            }
+            if (keep) {
+                const long long at = pos + before + __popc(m & ((1u << lane) - 1u));
+                if (at < cap) {
+                    rows[at] = static_cast<int>(g);
+                    vals[at] = static_cast<float>(v);
+                }
+            }
+            pos += total;
+            __syncthreads();
         }
-        pos += total;
-        __syncthreads();
     }
 }
+
+// The voxels the column just transferred can have written: the grid's dirty box,
+// or the whole grid when the context does not track one.
+OpBox dirty_op_box(const Context& c) {
+    OpBox a{};
+    int lo[3], hi[3];
+    const bool boxed = c.doseBoxed && !c.doseExposed;
+    for (int i = 0; i < 3; ++i) {
+        lo[i] = boxed ? c.dirtyLo[i] : 0;
+        hi[i] = boxed ? c.dirtyHi[i] : c.doseGrid.dims[i] - 1;
+    }
+    const bool empty = hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2];
+    for (int i = 0; i < 3; ++i) {
+        a.lo[i] = lo[i];
+        a.ext[i] = empty ? 0 : hi[i] - lo[i] + 1;
+    }
+    a.X = c.doseGrid.dims[0];
+    a.Y = c.doseGrid.dims[1];
+    a.n = empty ? 0 : static_cast<long long>(a.ext[0]) * a.ext[1] * a.ext[2];
+    return a;
+}
+
+// Spots per batched pass of an influence export (one plan layer each; at most the
+// layers of one chunk's layer plan).
+constexpr int kColumnBatch = 64;
 
 int op_cuda(cudaError_t e, const char* where) {
     if (e == cudaSuccess) return PBS_OK;
@@ -243,13 +282,19 @@ int op_cuda(cudaError_t e, const char* where) {
 }
 
 // Row norms of the influence matrix: the squared dose of one column added to the
-// FP64 norm grid over the column's dirty box.
-__global__ void __launch_bounds__(kOpThreads) row_norm_add_kernel(const double* __restrict__ dose, OpBox a,
+// Squares of the column's dose added into the FP64 norm grid, over the part of the
+// column's host box its transfers can have written (column_box); every voxel read is
+// zeroed, so the grid is zero again for the next column.
+__global__ void __launch_bounds__(kOpThreads) row_norm_add_kernel(double* __restrict__ dose, OpBox host,
+                                                                  const BeamStateDev* __restrict__ pb,
+                                                                  const BeamStateDev* __restrict__ nb,
                                                                   double* __restrict__ norm) {
+    const OpBox a = column_box(host, pb, nb);
     for (long long b = blockIdx.x * static_cast<long long>(kOpThreads) + threadIdx.x; b < a.n;
          b += static_cast<long long>(gridDim.x) * kOpThreads) {
         const long long g = box_to_grid(a, b);
         const double v = dose[g];
+        dose[g] = 0.0;
         norm[g] += v * v;
     }
 }
@@ -444,6 +489,50 @@ int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut, boo
     return PBS_OK;
 }
 
+int Context::run_column_batch(ColumnPlan& cp, size_t firstSpot, int count, ColumnSink& sink, bool gridZero) {
+    if (count <= 0) return PBS_OK;
+    const size_t plane = static_cast<size_t>(cp.base.lattice.nx) * cp.base.lattice.ny;
+    // The plan without its per-layer vectors, then one layer per spot: the spot's own
+    // layer's parameters and, as that layer's lattice weights, the spot's shares.
+    BeamPlan P;
+    {
+        std::vector<float> weights;
+        std::vector<LayerHost> layers;
+        std::swap(cp.base.lattice.weights, weights);
+        std::swap(cp.base.layers, layers);
+        P = cp.base;
+        std::swap(cp.base.lattice.weights, weights);
+        std::swap(cp.base.layers, layers);
+    }
+    P.numLayers = count;
+    P.lattice.nl = count;
+    P.layers.resize(static_cast<size_t>(count));
+    P.lattice.weights.assign(plane * static_cast<size_t>(count), 0.0f);
+    for (int q = 0; q < count; ++q) {
+        const size_t j = firstSpot + static_cast<size_t>(q);
+        int layer = -1;
+        for (int slot = 0; slot < 4; ++slot)
+            if (cp.cells[j * 4 + slot] >= 0) layer = static_cast<int>(cp.cells[j * 4 + slot] / plane);
+        // A spot on no lattice cell keeps an all-zero layer: an empty column.
+        P.layers[static_cast<size_t>(q)] = cp.base.layers[static_cast<size_t>(std::max(layer, 0))];
+        for (int slot = 0; slot < 4; ++slot) {
+            const int c = cp.cells[j * 4 + slot];
+            if (c >= 0)
+                P.lattice.weights[static_cast<size_t>(q) * plane + (static_cast<size_t>(c) - size_t(layer) * plane)] +=
+                    cp.shares[j * 4 + slot];
+        }
+    }
+    if (gridZero && doseBoxed && !doseExposed && !pendingDoseInit) {
+        for (int i = 0; i < 3; ++i) {
+            dirtyLo[i] = INT_MAX;
+            dirtyHi[i] = -1;
+        }
+    } else if (int rc = reset_dose(nullptr, 0)) {
+        return rc;
+    }
+    return run_beam(cp.beam, 0, nullptr, &P, &sink);
+}
+
 int Context::influence_row_norms(const PbsBeamDesc& beam, int nuclear, long long spotBegin, long long spotCount,
                                  const long long* voxelsHost, long long nVoxels, float* outHost) {
     const long long gridN = hasDose ? static_cast<long long>(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2]
@@ -478,15 +567,35 @@ int Context::influence_row_norms(const PbsBeamDesc& beam, int nuclear, long long
     if (int rc = op_cuda(cudaMemsetAsync(norm, 0, static_cast<size_t>(gridN) * sizeof(double), stream),
                          "row norm clear"))
         return fail(rc);
-    const double* d = static_cast<const double*>(dose64.ptr);
-    for (long long k = 0; k < spotCount; ++k) {
-        OpBox a{};
-        if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a)) return fail(rc);
+    double* d = static_cast<double*>(dose64.ptr);
+    auto add = [&](const OpBox& a, bool nuc) {
         if (a.n > 0) {
             const int blocks = static_cast<int>(std::min<long long>((a.n + kOpThreads - 1) / kOpThreads, 148 * 8));
-            row_norm_add_kernel<<<blocks, kOpThreads, 0, stream>>>(d, a, norm);
+            row_norm_add_kernel<<<blocks, kOpThreads, 0, stream>>>(
+                d, a, static_cast<const BeamStateDev*>(bs.ptr),
+                nuc ? static_cast<const BeamStateDev*>(nucBs.ptr) : nullptr, norm);
         }
-        if (int rc = op_cuda(cudaGetLastError(), "row norm kernel")) return fail(rc);
+        return op_cuda(cudaGetLastError(), "row norm kernel");
+    };
+    if (!nuclear && !bioModel && !carbonProfile) {
+        struct Sink : ColumnSink {
+            Context& c;
+            decltype(add)& run;
+            Sink(Context& ctx, decltype(add)& f) : c(ctx), run(f) {}
+            int column(int) override { return run(dirty_op_box(c), false); }
+        } sink(*this, add);
+        for (long long k0 = 0; k0 < spotCount; k0 += kColumnBatch) {
+            const int kb = static_cast<int>(std::min<long long>(kColumnBatch, spotCount - k0));
+            if (int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, k0 > 0))
+                return fail(rc);
+        }
+    } else {
+        for (long long k = 0; k < spotCount; ++k) {
+            OpBox a{};
+            // The previous column's norm pass zeroed what its transfers wrote.
+            if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a, k > 0)) return fail(rc);
+            if (int rc = add(a, lastNuclear)) return fail(rc);
+        }
     }
     if (nOut > 0) {
         const int blocks = static_cast<int>(std::min<long long>((nOut + kOpThreads - 1) / kOpThreads, 148 * 8));
@@ -536,7 +645,8 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
     };
     const long long maxBlocks = (gridN + kOpChunk - 1) / kOpChunk;
     if (int rc = opColPtr.ensure(static_cast<size_t>(spotCount + 1) * sizeof(long long))) return fail(rc);
-    if (int rc = opBlockOff.ensure(static_cast<size_t>(std::max(maxBlocks, 1LL)) * sizeof(long long))) return fail(rc);
+    // Chunk offsets, and after them the chunk count of the column being compacted.
+    if (int rc = opBlockOff.ensure(static_cast<size_t>(maxBlocks + 1) * sizeof(long long))) return fail(rc);
     if (capacity > 0) {
         if (int rc = opRows.ensure(static_cast<size_t>(capacity) * sizeof(int))) return fail(rc);
         if (int rc = opVals.ensure(static_cast<size_t>(capacity) * sizeof(float))) return fail(rc);
@@ -548,21 +658,50 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
     if (int rc = op_cuda(cudaMemsetAsync(dColPtr, 0, sizeof(long long), stream), "influence colPtr clear"))
         return fail(rc);
 
-    for (long long k = 0; k < spotCount; ++k) {
-        OpBox a{};
-        // The previous column's compaction zeroed what its transfers wrote.
-        if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a, k > 0)) return fail(rc);
-        const int nBlocks = static_cast<int>((a.n + kOpChunk - 1) / kOpChunk);
+    // Column k: its entries compacted from the FP64 grid (which the compaction zeroes
+    // again) into the CSC arrays after column k - 1's.
+    auto compact = [&](long long k, const OpBox& a, bool nuc) {
+        // The host box bounds the device box (column_box) the kernels walk: at most
+        // kOpGridBlocks blocks stride over its chunks.
+        const int nBlocks = static_cast<int>(std::min<long long>((a.n + kOpChunk - 1) / kOpChunk, kOpGridBlocks));
         double* d = static_cast<double*>(dose64.ptr);
         const BeamStateDev* pb = static_cast<const BeamStateDev*>(bs.ptr);
-        const BeamStateDev* nb = lastNuclear ? static_cast<const BeamStateDev*>(nucBs.ptr) : nullptr;
-        if (nBlocks > 0)
-            influence_count_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, pb, nb, threshold, dBlockOff);
-        influence_scan_kernel<<<1, 1024, 0, stream>>>(dBlockOff, nBlocks, dColPtr, static_cast<int>(k));
+        const BeamStateDev* nb = nuc ? static_cast<const BeamStateDev*>(nucBs.ptr) : nullptr;
+        long long* dChunks = dBlockOff + maxBlocks;
+        if (nBlocks > 0) {
+            influence_count_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, pb, nb, threshold, dBlockOff, dChunks);
+        } else if (int rc = op_cuda(cudaMemsetAsync(dChunks, 0, sizeof(long long), stream), "influence count clear")) {
+            return rc;
+        }
+        influence_scan_kernel<<<1, 1024, 0, stream>>>(dBlockOff, dChunks, dColPtr, static_cast<int>(k));
         if (nBlocks > 0)
             influence_write_kernel<<<nBlocks, kOpThreads, 0, stream>>>(d, a, pb, nb, threshold, dBlockOff, dRows,
                                                                        dVals, capacity);
-        if (int rc3 = op_cuda(cudaGetLastError(), "influence kernels")) return fail(rc3);
+        return op_cuda(cudaGetLastError(), "influence kernels");
+    };
+    if (!nuclear && !bioModel && !carbonProfile) {
+        // Batched: kColumnBatch spots per pass, each compacted as soon as its layer's
+        // transfer is enqueued.
+        struct Sink : ColumnSink {
+            Context& c;
+            decltype(compact)& run;
+            long long first = 0;
+            Sink(Context& ctx, decltype(compact)& f) : c(ctx), run(f) {}
+            int column(int layer) override { return run(first + layer, dirty_op_box(c), false); }
+        } sink(*this, compact);
+        for (long long k0 = 0; k0 < spotCount; k0 += kColumnBatch) {
+            const int kb = static_cast<int>(std::min<long long>(kColumnBatch, spotCount - k0));
+            sink.first = k0;
+            if (int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, k0 > 0))
+                return fail(rc);
+        }
+    } else {
+        for (long long k = 0; k < spotCount; ++k) {
+            OpBox a{};
+            // The previous column's compaction zeroed what its transfers wrote.
+            if (int rc = run_column(cp, static_cast<size_t>(spotBegin + k), nuclear, &a, k > 0)) return fail(rc);
+            if (int rc = compact(k, a, lastNuclear)) return fail(rc);
+        }
     }
     if (int rc = op_cuda(cudaMemcpyAsync(colPtrHost, dColPtr, static_cast<size_t>(spotCount + 1) * sizeof(long long),
                                          cudaMemcpyDeviceToHost, stream),

@@ -46,6 +46,9 @@ struct LayerStateDev {
     int liveR[33];              // live tiles per processing radius
     int offR[33];               // first work-list slot of this layer's radius-R items
     int curR[33];               // scatter cursors
+    // Padded BEV cells (x, y) and steps relative to firstInside (z) this layer's
+    // one-layer items (work_scatter_kernel) can write; lo > hi while none.
+    int liveLo[3], liveHi[3];
 };
 
 // Beam-level values produced on the device.

@@ -585,28 +585,40 @@ cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rs
     return cudaLaunchKernelEx(&cfg, k, g, idd, rsigma, work, beam, bev, shiftOffset, range);
 }
 
-// Adds the fixed-point BEV of the chunk (the planes written so far,
-// [0, maxCalcPassive - firstInside)) to the float BEV and clears it for the next
-// superposition. Every cell is converted once, so the float BEV is the same on
-// every run.
+// Adds the fixed-point BEV of the chunk to the float BEV and clears it for the next
+// superposition, over the cells the items can have written: the box of live cells
+// (BeamStateDev::liveLo/liveHi, from work_merge_kernel or, for one layer,
+// work_layer_view_kernel) within the planes written so far,
+// [0, maxCalcPassive - firstInside). Every cell is converted once, so the float BEV is
+// the same on every run.
 __global__ void __launch_bounds__(256) bev_fixed_to_float_kernel(BeamGeomDev g, const BeamStateDev* __restrict__ beam,
                                                                  unsigned long long* __restrict__ fixed,
                                                                  float* __restrict__ bev, int shiftOffset) {
     const int planes = min(beam->maxCalcPassive - beam->firstInside, g.steps);
-    if (planes <= 0) return;
+    if (planes <= 0 || beam->liveLo[0] > beam->liveHi[0]) return;
     // bevX is even (the padded ray pitch plus 2 kMaxR), so cells go in aligned pairs.
-    const size_t pairs = static_cast<size_t>(planes) * g.bevX * g.bevY / 2;
+    const int x0 = max(beam->liveLo[0], 0) & ~1, x1 = min(beam->liveHi[0], g.bevX - 1) | 1;
+    const int y0 = max(beam->liveLo[1], 0), y1 = min(beam->liveHi[1], g.bevY - 1);
+    const int z0 = max(beam->liveLo[2], 0), z1 = min(beam->liveHi[2], planes - 1);
+    if (x1 < x0 || y1 < y0 || z1 < z0) return;
+    const int pw = (x1 - x0 + 1) / 2, rows = y1 - y0 + 1;
+    const size_t n = static_cast<size_t>(pw) * rows * (z1 - z0 + 1);
     const double unit = ldexp(1.0, -(beam->fixedShift + shiftOffset));
     ulonglong2* f2 = reinterpret_cast<ulonglong2*>(fixed);
     float2* b2 = reinterpret_cast<float2*>(bev);
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < pairs; i += size_t(gridDim.x) * blockDim.x) {
-        const ulonglong2 v = f2[i];
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const int xp = static_cast<int>(i % pw);
+        const size_t r = i / pw;
+        const int y = y0 + static_cast<int>(r % rows);
+        const int z = z0 + static_cast<int>(r / rows);
+        const size_t pr = ((static_cast<size_t>(z) * g.bevY + y) * g.bevX + x0) / 2 + xp;
+        const ulonglong2 v = f2[pr];
         if (v.x | v.y) {
-            float2 o = b2[i];
+            float2 o = b2[pr];
             o.x += float(double(v.x) * unit);
             o.y += float(double(v.y) * unit);
-            b2[i] = o;
-            f2[i] = make_ulonglong2(0ull, 0ull);
+            b2[pr] = o;
+            f2[pr] = make_ulonglong2(0ull, 0ull);
         }
     }
 }

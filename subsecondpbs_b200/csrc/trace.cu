@@ -473,6 +473,10 @@ __global__ void beam_planner_kernel(BeamGeomDev g, float* __restrict__ weplMin,
             st.liveHist[i] = 0;
         }
         for (int i = 0; i < 33; ++i) st.batchedCounts[i] = 0;
+        for (int i = 0; i < 3; ++i) {
+            st.liveLo[i] = INT_MAX;
+            st.liveHi[i] = INT_MIN;
+        }
     }
 }
 
