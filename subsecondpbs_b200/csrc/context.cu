@@ -341,6 +341,19 @@ void dose_transfer_box(const FromFan& f, int pitchX, int pitchY, int steps, cons
 }
 }  // namespace
 
+void Context::column_layout(const BeamPlan& P, ColBox& fb, size_t& bevCells, size_t& bytesPerColumn) const {
+    int lo[3], hi[3];
+    dose_transfer_box(P.rayIdxToDoseIdx, P.superpDims[0], P.superpDims[1], P.tracerSteps, doseGrid.dims, lo, hi);
+    size_t voxels = 1;
+    for (int i = 0; i < 3; ++i) {
+        fb.lo[i] = lo[i];
+        fb.ext[i] = std::max(hi[i] - lo[i] + 1, 0);
+        voxels *= size_t(fb.ext[i]);
+    }
+    bevCells = size_t(P.tracerSteps) * size_t(P.superpDims[0] + 2 * kMaxR) * size_t(P.superpDims[1] + 2 * kMaxR);
+    bytesPerColumn = bevCells * (sizeof(float) + sizeof(unsigned long long)) + voxels * sizeof(double);
+}
+
 int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3], const int hi[3]) {
     PBS_CUDA(cudaSetDevice(device), "cudaSetDevice");
     if (!data || g.dims[0] <= 0 || g.dims[1] <= 0 || g.dims[2] <= 0 ||
@@ -985,6 +998,25 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     // Batched influence columns (a sink): each layer of a chunk is superposed from its
     // own work list, selected from the chunk's one-layer list, and transferred alone.
     const bool columnLists = cols && !perLayerTransfer;
+    size_t colCells = 0;
+    if (columnLists) {
+        size_t perColumn = 0;
+        column_layout(P, colBox, colCells, perColumn);
+        const size_t fbN = size_t(colBox.ext[0]) * colBox.ext[1] * colBox.ext[2];
+        const size_t c = size_t(chunk);
+        const bool had = colBev.bytes >= c * colCells * 4 && colFixed.bytes >= c * colCells * 8 &&
+                         colDose.bytes >= c * fbN * 8;
+        if ((rc = colBev.ensure(c * colCells * 4)) || (rc = colFixed.ensure(c * colCells * 8)) ||
+            (rc = colDose.ensure(c * fbN * 8)))
+            return rc;
+        if (!had || !colClean) {
+            PBS_CUDA(cudaMemsetAsync(colBev.ptr, 0, colBev.bytes, stream), "memset column BEV");
+            PBS_CUDA(cudaMemsetAsync(colFixed.ptr, 0, colFixed.bytes, stream), "memset column BEV");
+            PBS_CUDA(cudaMemsetAsync(colDose.ptr, 0, colDose.bytes, stream), "memset column dose");
+        }
+        // Clean again once every chunk's columns are compacted and cleared.
+        colClean = false;
+    }
 
     // The trace's home: the store's resident copy for this geometry, else the
     // context's own buffers.
@@ -1315,19 +1347,20 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
         if (adj) break;  // the adjoint's superposition runs after the transfer box is known
         unsigned long long* dFixed = static_cast<unsigned long long*>(bevFixed.ptr);
         if (columnLists) {
-            // One column per layer: its items, superposition and transfer, the sink's
-            // compaction, then an empty BEV for the next layer.
-            for (int q = 0; q < nl; ++q) {
-                PBS_CUDA(launch_work_layer_view(l0, q, dls, dbs, workCap, stream), "work_layer_view");
-                bevFixedClean = false;
-                PBS_CUDA(launch_superpose(g, static_cast<const float*>(iddBuf.ptr), static_cast<const float*>(rsBuf.ptr),
-                                          static_cast<const int4*>(work.ptr), dbs, dBev, dFixed, 0, smCount, stream),
-                         "superpose");
-                bevFixedClean = true;
-                if ((rc = transfer_layers(dls + l0 + q, nullptr))) return rc;
-                if ((rc = cols->column(l0 + q))) return rc;
-                PBS_CUDA(cudaMemsetAsync(dBev, 0, S * size_t(g.bevX) * g.bevY * 4, stream), "memset BEV");
-            }
+            // One column per layer of the chunk: the whole one-layer list superposed at
+            // once, layer q into BEV volume q, transferred into dose buffer q; the sink
+            // compacts the columns, then the volumes' live cells are cleared.
+            float* cBev = static_cast<float*>(colBev.ptr);
+            unsigned long long* cFixed = static_cast<unsigned long long*>(colFixed.ptr);
+            PBS_CUDA(launch_superpose_columns(g, static_cast<const float*>(iddBuf.ptr),
+                                              static_cast<const float*>(rsBuf.ptr), static_cast<const int4*>(work.ptr),
+                                              dbs, dls + l0, nl, cBev, cFixed, colCells, smCount, stream),
+                     "superpose_columns");
+            PBS_CUDA(launch_column_transfer(g, cBev, colCells, dbs, dls + l0, nl, colBox,
+                                            static_cast<double*>(colDose.ptr), stream),
+                     "column_transfer");
+            if ((rc = cols->columns(l0, nl))) return rc;
+            PBS_CUDA(launch_column_bev_clear(g, cBev, colCells, dls + l0, nl, stream), "column_bev_clear");
             continue;
         }
         bevFixedClean = false;
@@ -1364,7 +1397,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             // This layer alone, then empty BEV volumes for the next one (the last
             // layer's BEV stays for the debug readouts).
             if ((rc = transfer_layers(dls + l0, nuclear ? dNucLs + l0 : nullptr))) return rc;
-            if (cols && (rc = cols->column(l0))) return rc;
+            if (cols && (rc = cols->columns(l0, 1))) return rc;
         }
         if (perLayerTransfer && l0 + nl < L) {
             PBS_CUDA(cudaMemsetAsync(dBev, 0, S * size_t(g.bevX) * g.bevY * 4, stream), "memset BEV");
@@ -1380,6 +1413,7 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
     }
     if ((rc = mark(6))) return rc;
     if (adj) return finish_adjoint(*adj, b);
+    if (columnLists) colClean = true;
     if (!perLayerTransfer && !cols && (rc = transfer_layers(nullptr, nullptr))) return rc;
     if ((rc = mark(7))) return rc;
     lastChunks = (L + chunk - 1) / chunk;

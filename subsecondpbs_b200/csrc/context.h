@@ -171,6 +171,12 @@ struct Context {
     DevBuf gradDoseBuf, bevGrad, rbarBuf, gradInterm, gradLattice, weqBody;
     // Influence export: column offsets, per-block offsets, and the entries.
     DevBuf opColPtr, opBlockOff, opRows, opVals, opNorm, opVoxels;
+    // Batched influence columns: per chunk layer (column) a BEV volume as float and as
+    // int64 fixed point, and an FP64 dose buffer over colBox; all zero between
+    // batches while colClean.
+    DevBuf colBev, colFixed, colDose;
+    ColBox colBox{};
+    bool colClean = false;
 
     PinnedBuf staging, errHost;
     cudaEvent_t stagingEvent = nullptr;
@@ -242,15 +248,20 @@ struct Context {
         float* gradSpots;
         size_t nSpots;
     };
-    // Receives the columns of a batched influence export. With a sink, run_beam gives
-    // every layer of the plan its own superposition and transfer (each layer of the
-    // plan is one column: one spot at unit weight) and calls column(layer) once that
-    // layer's dose is in the FP64 grid and before the next layer's transfer; a column
-    // must leave the grid zero again (the compaction does).
+    // Receives the columns of a batched influence export. With a sink, every layer of
+    // the plan is one column (one spot at unit weight) with its own BEV volume and
+    // transfer: run_beam calls columns(first, count) once the doses of layers
+    // [first, first + count) are in colDose (buffer q = layer first + q, over colBox).
+    // The sink must leave those buffers zero (the compaction does). In the reference's
+    // depth convention the layers are transferred one at a time into the FP64 grid
+    // instead, with columns(layer, 1) after each; the sink reads and zeroes the grid.
     struct ColumnSink {
         virtual ~ColumnSink() = default;
-        virtual int column(int layer) = 0;
+        virtual int columns(int first, int count) = 0;
     };
+    // Batched influence columns of plan P: the box every column's dose buffer is laid
+    // out over, the cells of one BEV volume, and the device bytes of one column.
+    void column_layout(const BeamPlan& P, ColBox& fb, size_t& bevCells, size_t& bytesPerColumn) const;
     int run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj, BeamPlan* planned = nullptr,
                  ColumnSink* cols = nullptr);
     int finish_adjoint(const AdjointArgs& a, const PbsBeamDesc& b);

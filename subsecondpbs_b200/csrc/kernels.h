@@ -87,6 +87,14 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
                             BeamStateDev* beam, int4* work, int workCapacity, bool merged,
                             const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, cudaStream_t s);
+// Batched influence columns (one chunk layer per column, layers [0, nCols) of `ls`):
+// each column's transfer box over its layer's live cells, then the transfer of BEV
+// volume q (bev + q * bevStride) into dose buffer q (colDose + q * |fb|, laid out
+// over fb). The BEV clear zeroes each volume's live cells afterwards.
+cudaError_t launch_column_transfer(const BeamGeomDev& g, const float* bev, size_t bevStride, BeamStateDev* beam,
+                                   LayerStateDev* ls, int nCols, const ColBox& fb, double* colDose, cudaStream_t s);
+cudaError_t launch_column_bev_clear(const BeamGeomDev& g, float* bev, size_t bevStride, const LayerStateDev* ls,
+                                    int nCols, cudaStream_t s);
 // Points the forward superposition at chunk layer `lc`'s items of the one-layer list
 // (merged == false above) and the transfer planner's live box at that layer's.
 cudaError_t launch_work_layer_view(int layer0, int lc, const LayerStateDev* ls, BeamStateDev* beam, int workCapacity,
@@ -107,6 +115,12 @@ cudaError_t launch_nuc_codes(const BeamGeomDev& gn, int layer0, int nLayers, con
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                              BeamStateDev* beam, float* bev, unsigned long long* bevFixed, int shiftOffset,
                              int numSMs, cudaStream_t s);
+// Batched influence columns: the chunk's whole one-layer work list (layers
+// [0, nCols) of `ls`), item layer q into BEV volume q (bev / bevFixed + q * stride
+// cells), each volume converted over its layer's live cells.
+cudaError_t launch_superpose_columns(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                                     BeamStateDev* beam, const LayerStateDev* ls, int nCols, float* bev,
+                                     unsigned long long* bevFixed, size_t stride, int numSMs, cudaStream_t s);
 
 // ---- BEV -> dose ---------------------------------------------------------------
 // Transfer bounding box and parameters (wrapper.cu:5343-5403): over the steps of

@@ -250,6 +250,197 @@ __global__ void __launch_bounds__(kOpThreads) influence_write_kernel(double* __r
     }
 }
 
+// ---- Batched columns: buffer q (blockIdx.y) of colDose, laid out over fb --------
+
+// Voxel b of a column box [lo, hi] (x fastest): its linear grid index and its index
+// in a column buffer over fb.
+__device__ __forceinline__ void col_voxel(const int lo[3], const int ext[3], const ColBox& fb, int X, int Y,
+                                          long long b, long long& g, size_t& at) {
+    const int bx = int(b % ext[0]);
+    const long long r = b / ext[0];
+    const int by = int(r % ext[1]);
+    const int bz = int(r / ext[1]);
+    const int x = lo[0] + bx, y = lo[1] + by, z = lo[2] + bz;
+    g = (static_cast<long long>(z) * Y + y) * X + x;
+    at = (static_cast<size_t>(z - fb.lo[2]) * fb.ext[1] + (y - fb.lo[1])) * fb.ext[0] + (x - fb.lo[0]);
+}
+
+__device__ __forceinline__ long long col_box(const LayerStateDev& st, const ColBox& fb, int X, int Y, int lo[3],
+                                             int ext[3]) {
+    int hi[3];
+    if (!column_written_box(st, X, Y, fb, lo, hi)) return 0;
+    long long n = 1;
+    for (int i = 0; i < 3; ++i) {
+        ext[i] = hi[i] - lo[i] + 1;
+        n *= ext[i];
+    }
+    return n;
+}
+
+// Entries above the threshold per kOpChunk-voxel chunk of each column's box; the
+// column's chunk count goes to nChunks[q].
+__global__ void __launch_bounds__(kOpThreads) col_count_kernel(const double* __restrict__ colDose, ColBox fb,
+                                                               const LayerStateDev* __restrict__ ls, int X, int Y,
+                                                               double thr, long long* __restrict__ blockOff,
+                                                               int maxChunks, long long* __restrict__ nChunks) {
+    const int q = blockIdx.y;
+    int lo[3], ext[3];
+    const long long n = col_box(ls[q], fb, X, Y, lo, ext);
+    const long long nCh = (n + kOpChunk - 1) / kOpChunk;
+    if (blockIdx.x == 0 && threadIdx.x == 0) nChunks[q] = nCh;
+    const size_t fbN = static_cast<size_t>(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+    const double* d = colDose + static_cast<size_t>(q) * fbN;
+    for (long long ch = blockIdx.x; ch < nCh; ch += gridDim.x) {
+        int c = 0;
+        for (int p = 0; p < kOpPasses; ++p) {
+            const long long b = ch * kOpChunk + p * kOpThreads + threadIdx.x;
+            bool keep = false;
+            if (b < n) {
+                long long g;
+                size_t at;
+                col_voxel(lo, ext, fb, X, Y, b, g, at);
+                keep = fabs(d[at]) > thr;
+            }
+            c += __syncthreads_count(keep);
+        }
+        if (threadIdx.x == 0) blockOff[static_cast<size_t>(q) * maxChunks + ch] = c;
+    }
+}
+
+// One block: the columns' chunk counts -> absolute offsets, column after column
+// (colPtr[col0 + q + 1] = colPtr[col0 + q] + entries of column q).
+__global__ void __launch_bounds__(1024) col_scan_kernel(long long* __restrict__ blockOff, int maxChunks,
+                                                        const long long* __restrict__ nChunks, int nCols,
+                                                        long long* __restrict__ colPtr, int col0) {
+    __shared__ long long carry;
+    __shared__ long long warpSums[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = 0; q < nCols; ++q) {
+        long long* off = blockOff + static_cast<size_t>(q) * maxChunks;
+        const int nBlocks = static_cast<int>(nChunks[q]);
+        if (threadIdx.x == 0) carry = colPtr[col0 + q];
+        __syncthreads();
+        for (int start = 0; start < nBlocks; start += 1024) {
+            const int i = start + threadIdx.x;
+            const long long v = i < nBlocks ? off[i] : 0;
+            long long x = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) warpSums[warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                long long t = warpSums[lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const long long y = __shfl_up_sync(0xffffffffu, t, o);
+                    if (lane >= o) t += y;
+                }
+                warpSums[lane] = t;
+            }
+            __syncthreads();
+            const long long incl = x + (warp > 0 ? warpSums[warp - 1] : 0);
+            const long long c0 = carry;
+            if (i < nBlocks) off[i] = c0 + incl - v;
+            __syncthreads();
+            if (threadIdx.x == 1023) carry = c0 + incl;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) colPtr[col0 + q + 1] = carry;
+        __syncthreads();
+    }
+}
+
+// Ordered compaction of each column's chunks (rows = linear grid indices, ascending);
+// every voxel read is zeroed, so the buffers are zero for the next batch.
+__global__ void __launch_bounds__(kOpThreads) col_write_kernel(double* __restrict__ colDose, ColBox fb,
+                                                               const LayerStateDev* __restrict__ ls, int X, int Y,
+                                                               double thr, const long long* __restrict__ blockOff,
+                                                               int maxChunks, int* __restrict__ rows,
+                                                               float* __restrict__ vals, long long cap) {
+    __shared__ int warpCounts[kOpThreads / 32];
+    const int q = blockIdx.y;
+    int lo[3], ext[3];
+    const long long n = col_box(ls[q], fb, X, Y, lo, ext);
+    const long long nCh = (n + kOpChunk - 1) / kOpChunk;
+    const size_t fbN = static_cast<size_t>(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+    double* d = colDose + static_cast<size_t>(q) * fbN;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (long long ch = blockIdx.x; ch < nCh; ch += gridDim.x) {
+        long long pos = blockOff[static_cast<size_t>(q) * maxChunks + ch];
+        for (int p = 0; p < kOpPasses; ++p) {
+            const long long b = ch * kOpChunk + p * kOpThreads + threadIdx.x;
+            long long g = 0;
+            double v = 0.0;
+            bool keep = false;
+            if (b < n) {
+                size_t at;
+                col_voxel(lo, ext, fb, X, Y, b, g, at);
+                v = d[at];
+                d[at] = 0.0;
+                keep = fabs(v) > thr;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) warpCounts[warp] = __popc(m);
+            __syncthreads();
+            int before = 0, total = 0;
+            for (int w = 0; w < kOpThreads / 32; ++w) {
+                const int c = warpCounts[w];
+                if (w < warp) before += c;
+                total += c;
+            }
+            if (keep) {
+                const long long at = pos + before + __popc(m & ((1u << lane) - 1u));
+                if (at < cap) {
+                    rows[at] = static_cast<int>(g);
+                    vals[at] = static_cast<float>(v);
+                }
+            }
+            pos += total;
+            __syncthreads();
+        }
+    }
+}
+
+// Row norms of a batch of columns: every voxel of fb adds the squares of the columns
+// whose box holds it, in column order (deterministic), and zeroes them.
+constexpr int kMaxColumnsPerBatch = 64;
+__global__ void __launch_bounds__(kOpThreads) col_norm_kernel(double* __restrict__ colDose, ColBox fb,
+                                                              const LayerStateDev* __restrict__ ls, int nCols, int X,
+                                                              int Y, double* __restrict__ norm) {
+    __shared__ int sLo[kMaxColumnsPerBatch][3], sHi[kMaxColumnsPerBatch][3];
+    __shared__ int sAny[kMaxColumnsPerBatch];
+    for (int q = threadIdx.x; q < nCols; q += blockDim.x) {
+        int lo[3], hi[3];
+        sAny[q] = column_written_box(ls[q], X, Y, fb, lo, hi);
+        for (int i = 0; i < 3; ++i) {
+            sLo[q][i] = lo[i];
+            sHi[q][i] = hi[i];
+        }
+    }
+    __syncthreads();
+    const size_t fbN = static_cast<size_t>(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+    for (size_t at = blockIdx.x * size_t(blockDim.x) + threadIdx.x; at < fbN; at += size_t(gridDim.x) * blockDim.x) {
+        const int x = fb.lo[0] + static_cast<int>(at % fb.ext[0]);
+        const size_t r = at / fb.ext[0];
+        const int y = fb.lo[1] + static_cast<int>(r % fb.ext[1]);
+        const int z = fb.lo[2] + static_cast<int>(r / fb.ext[1]);
+        double acc = 0.0;
+        bool any = false;
+        for (int q = 0; q < nCols; ++q) {
+            if (!sAny[q] || x < sLo[q][0] || x > sHi[q][0] || y < sLo[q][1] || y > sHi[q][1] || z < sLo[q][2] ||
+                z > sHi[q][2])
+                continue;
+            double* d = colDose + static_cast<size_t>(q) * fbN + at;
+            const double v = *d;
+            *d = 0.0;
+            acc += v * v;
+            any = true;
+        }
+        if (any) norm[(static_cast<long long>(z) * Y + y) * X + x] += acc;
+    }
+}
+
 // The voxels the column just transferred can have written: the grid's dirty box,
 // or the whole grid when the context does not track one.
 OpBox dirty_op_box(const Context& c) {
@@ -271,9 +462,23 @@ OpBox dirty_op_box(const Context& c) {
     return a;
 }
 
-// Spots per batched pass of an influence export (one plan layer each; at most the
-// layers of one chunk's layer plan).
-constexpr int kColumnBatch = 64;
+// Spots per batched pass of an influence export (one plan layer and one BEV volume
+// and dose buffer each): at most the layers of one chunk's layer plan, and as many
+// as fit kColumnBudget bytes and half the free device memory.
+constexpr long long kColumnBudget = 6LL << 30;
+
+int column_batch_size(const Context& c, const BeamPlan& base, ColBox& fb, size_t& maxChunks) {
+    size_t cells = 0, perColumn = 0;
+    c.column_layout(base, fb, cells, perColumn);
+    const size_t fbN = size_t(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+    maxChunks = std::max<size_t>((fbN + kOpChunk - 1) / kOpChunk, 1);
+    if (c.compatBevZShift) return kMaxColumnsPerBatch;  // one layer at a time through the dose grid
+    size_t freeB = 0, totalB = 0;
+    long long budget = kColumnBudget;
+    if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess) budget = std::min<long long>(budget, (long long)(freeB / 2));
+    const long long k = budget / std::max<long long>((long long)perColumn, 1);
+    return static_cast<int>(std::max<long long>(1, std::min<long long>(k, kMaxColumnsPerBatch)));
+}
 
 int op_cuda(cudaError_t e, const char* where) {
     if (e == cudaSuccess) return PBS_OK;
@@ -578,14 +783,30 @@ int Context::influence_row_norms(const PbsBeamDesc& beam, int nuclear, long long
         return op_cuda(cudaGetLastError(), "row norm kernel");
     };
     if (!nuclear && !bioModel && !carbonProfile) {
+        // Batched: each batch's columns in their own dose buffers, their squares added
+        // voxel by voxel in column order.
         struct Sink : ColumnSink {
             Context& c;
             decltype(add)& run;
-            Sink(Context& ctx, decltype(add)& f) : c(ctx), run(f) {}
-            int column(int) override { return run(dirty_op_box(c), false); }
-        } sink(*this, add);
-        for (long long k0 = 0; k0 < spotCount; k0 += kColumnBatch) {
-            const int kb = static_cast<int>(std::min<long long>(kColumnBatch, spotCount - k0));
+            double* norm;
+            Sink(Context& ctx, decltype(add)& f, double* nm) : c(ctx), run(f), norm(nm) {}
+            int columns(int first, int count) override {
+                if (c.compatBevZShift) return run(dirty_op_box(c), false);
+                const ColBox fb = c.colBox;
+                const size_t fbN = size_t(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+                if (fbN == 0 || count <= 0) return PBS_OK;
+                const int blocks = static_cast<int>(std::min<size_t>((fbN + kOpThreads - 1) / kOpThreads, 148 * 8));
+                col_norm_kernel<<<blocks, kOpThreads, 0, c.stream>>>(
+                    static_cast<double*>(c.colDose.ptr), fb, static_cast<const LayerStateDev*>(c.ls.ptr) + first,
+                    count, c.doseGrid.dims[0], c.doseGrid.dims[1], norm);
+                return op_cuda(cudaGetLastError(), "column row norms");
+            }
+        } sink(*this, add, norm);
+        ColBox fb;
+        size_t maxChunks = 0;
+        const int batch = column_batch_size(*this, cp.base, fb, maxChunks);
+        for (long long k0 = 0; k0 < spotCount; k0 += batch) {
+            const int kb = static_cast<int>(std::min<long long>(batch, spotCount - k0));
             if (int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, k0 > 0))
                 return fail(rc);
         }
@@ -680,17 +901,54 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         return op_cuda(cudaGetLastError(), "influence kernels");
     };
     if (!nuclear && !bioModel && !carbonProfile) {
-        // Batched: kColumnBatch spots per pass, each compacted as soon as its layer's
-        // transfer is enqueued.
+        // Batched: each batch's columns in their own dose buffers, compacted with one
+        // count, one scan and one write launch per batch (column after column in the
+        // CSC order).
+        ColBox fb;
+        size_t maxChunks = 0;
+        const int batch = column_batch_size(*this, cp.base, fb, maxChunks);
+        if (int rc = opBlockOff.ensure((std::max<size_t>(size_t(maxBlocks), size_t(batch) * maxChunks + batch) + 1) *
+                                       sizeof(long long)))
+            return fail(rc);
+        dBlockOff = static_cast<long long*>(opBlockOff.ptr);
         struct Sink : ColumnSink {
             Context& c;
             decltype(compact)& run;
             long long first = 0;
+            double thr;
+            long long* off;
+            int* rows;
+            float* vals;
+            long long cap, *colPtr;
             Sink(Context& ctx, decltype(compact)& f) : c(ctx), run(f) {}
-            int column(int layer) override { return run(first + layer, dirty_op_box(c), false); }
+            int columns(int l, int count) override {
+                if (c.compatBevZShift) return run(first + l, dirty_op_box(c), false);
+                const ColBox fb = c.colBox;
+                const size_t fbN = size_t(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+                const int maxChunks = static_cast<int>(std::max<size_t>((fbN + kOpChunk - 1) / kOpChunk, 1));
+                long long* nChunks = off + size_t(count) * maxChunks;
+                const LayerStateDev* lsq = static_cast<const LayerStateDev*>(c.ls.ptr) + l;
+                const int X = c.doseGrid.dims[0], Y = c.doseGrid.dims[1];
+                // A few waves of blocks over all the batch's columns.
+                const int per = std::max(1, std::min(maxChunks, (148 * 4) / std::max(count, 1) + 1));
+                double* d = static_cast<double*>(c.colDose.ptr);
+                col_count_kernel<<<dim3(per, count), kOpThreads, 0, c.stream>>>(d, fb, lsq, X, Y, thr, off, maxChunks,
+                                                                                 nChunks);
+                col_scan_kernel<<<1, 1024, 0, c.stream>>>(off, maxChunks, nChunks, count, colPtr,
+                                                           static_cast<int>(first + l));
+                col_write_kernel<<<dim3(per, count), kOpThreads, 0, c.stream>>>(d, fb, lsq, X, Y, thr, off, maxChunks,
+                                                                                 rows, vals, cap);
+                return op_cuda(cudaGetLastError(), "column compaction");
+            }
         } sink(*this, compact);
-        for (long long k0 = 0; k0 < spotCount; k0 += kColumnBatch) {
-            const int kb = static_cast<int>(std::min<long long>(kColumnBatch, spotCount - k0));
+        sink.thr = threshold;
+        sink.off = dBlockOff;
+        sink.rows = dRows;
+        sink.vals = dVals;
+        sink.cap = capacity;
+        sink.colPtr = dColPtr;
+        for (long long k0 = 0; k0 < spotCount; k0 += batch) {
+            const int kb = static_cast<int>(std::min<long long>(batch, spotCount - k0));
             sink.first = k0;
             if (int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, k0 > 0))
                 return fail(rc);

@@ -49,6 +49,9 @@ struct LayerStateDev {
     // Padded BEV cells (x, y) and steps relative to firstInside (z) this layer's
     // one-layer items (work_scatter_kernel) can write; lo > hi while none.
     int liveLo[3], liveHi[3];
+    // Batched influence columns (one layer per column): the layer's own transfer box
+    // over its live cells, as transfer_planner_kernel lays one out.
+    int colStart[3], colMax[3], colValid;
 };
 
 // Beam-level values produced on the device.
@@ -89,6 +92,34 @@ struct BeamStateDev {
     int transferValid;
     int errorFlags;         // 1 work list overflow, 2 radius outside a kernel instance, 4 nuclear radius > 32
 };
+
+// Batched influence columns: the box of dose voxels (inclusive lo, extents) every
+// column's dose buffer is laid out over, x fastest: the host box over the whole
+// beam's transfer, which holds every layer's transfer box.
+struct ColBox {
+    int lo[3];
+    int ext[3];
+};
+
+// The voxels a column's transfer writes: its layer's transfer box with the launch's
+// block rounding in x (32) and y (8), as transfer_kernel walks a box, clipped to the
+// column buffers' box. False when empty.
+PBS_HD bool column_written_box(const LayerStateDev& st, int doseX, int doseY, const ColBox& fb, int lo[3],
+                                      int hi[3]) {
+    if (!st.colValid) return false;
+    for (int i = 0; i < 3; ++i) lo[i] = st.colStart[i];
+    const int nx = ((st.colMax[0] - lo[0] + 1 + 31) / 32) * 32, ny = ((st.colMax[1] - lo[1] + 1 + 7) / 8) * 8;
+    hi[0] = lo[0] + (nx < doseX - lo[0] ? nx : doseX - lo[0]) - 1;
+    hi[1] = lo[1] + (ny < doseY - lo[1] ? ny : doseY - lo[1]) - 1;
+    hi[2] = st.colMax[2];
+    bool any = true;
+    for (int i = 0; i < 3; ++i) {
+        if (lo[i] < fb.lo[i]) lo[i] = fb.lo[i];
+        if (hi[i] > fb.lo[i] + fb.ext[i] - 1) hi[i] = fb.lo[i] + fb.ext[i] - 1;
+        any = any && lo[i] <= hi[i];
+    }
+    return any;
+}
 
 // Everything a kernel needs to know about the beam geometry.
 struct BeamGeomDev {

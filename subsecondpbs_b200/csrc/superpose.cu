@@ -40,6 +40,8 @@
 // stay in registers over all the item's layers and are flushed once per item.
 // Radii 16..32, 8..15 and 0..7 run as three persistent instances with 128, 48 and
 // 40 registers: 2, 5 and 6 CTAs per SM.
+#include <algorithm>
+
 #include "device_util.cuh"
 #include "kernels.h"
 #include "launch_util.h"
@@ -503,7 +505,7 @@ template <bool kWide, int RLo, int RHi, int MinBlocks>
 __global__ void __launch_bounds__(kThreads, MinBlocks)
 superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
                  const int4* __restrict__ work, BeamStateDev* __restrict__ beam, unsigned long long* __restrict__ bev,
-                 int shiftOffset, int range) {
+                 int shiftOffset, int range, size_t layerBevStride) {
     extern __shared__ __align__(16) float sm[];
     __shared__ int sItem[2];
     // Per source column, its depositing sources over sy (radii 0..15: two buffers).
@@ -539,8 +541,10 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
         const int tx = tile % g.tilesX, ty = tile / g.tilesX;
         a.layers = static_cast<unsigned>(it.x);
         a.src = zRel * padPlane + static_cast<size_t>(ty * kTileY + (t >> 5)) * g.pitchX + tx * kTileX + (t & 31);
-        a.dst = bev + static_cast<size_t>(zRel) * bevPlane + static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX +
-                (tx * kTileX - R + kMaxR);
+        // One BEV volume per layer when layerBevStride is set (one-layer items: batched
+        // influence columns), else one volume for all layers.
+        a.dst = bev + (it.x & 0xff) * layerBevStride + static_cast<size_t>(zRel) * bevPlane +
+                static_cast<size_t>(ty * kTileY - R + kMaxR) * g.bevX + (tx * kTileX - R + kMaxR);
         bool ok;
         if constexpr (kWide) {
             float4* E4 = reinterpret_cast<float4*>(sm);                                       // [Q][256] e_s(4q..4q+3)
@@ -567,7 +571,7 @@ superpose_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __re
 template <bool kWide, int RLo, int RHi, int MinBlocks>
 cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                          BeamStateDev* beam, unsigned long long* bev, int shiftOffset, int gridBlocks, int range,
-                         bool overlap, cudaStream_t s) {
+                         bool overlap, size_t layerBevStride, cudaStream_t s) {
     auto k = superpose_kernel<kWide, RLo, RHi, MinBlocks>;
     const size_t smem = kWide ? WideShape<RHi>::kSmemBytes : PairShape<RHi>::kSmemBytes;
     cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
@@ -582,7 +586,7 @@ cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = overlap ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, k, g, idd, rsigma, work, beam, bev, shiftOffset, range);
+    return cudaLaunchKernelEx(&cfg, k, g, idd, rsigma, work, beam, bev, shiftOffset, range, layerBevStride);
 }
 
 // Adds the fixed-point BEV of the chunk to the float BEV and clears it for the next
@@ -630,20 +634,95 @@ constexpr int kNarrowBlocks = 6;
 
 }  // namespace
 
+namespace {
+
+// The three instances over `work` (items sorted by range: the wide radii first).
+cudaError_t launch_instances(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                             BeamStateDev* beam, unsigned long long* bevFixed, int shiftOffset, int numSMs,
+                             size_t layerBevStride, cudaStream_t s) {
+    cudaError_t e = launch_range<true, kSplitR + 1, kMaxR, kWideBlocks>(
+        g, idd, rsigma, work, beam, bevFixed, shiftOffset, numSMs * kWideBlocks, 0, false, layerBevStride, s);
+    if (e != cudaSuccess) return e;
+    e = launch_range<false, kSplitR2 + 1, kSplitR, kMidBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
+                                                               numSMs * kMidBlocks, 1, true, layerBevStride, s);
+    if (e != cudaSuccess) return e;
+    return launch_range<false, 0, kSplitR2, kNarrowBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
+                                                           numSMs * kNarrowBlocks, 2, true, layerBevStride, s);
+}
+
+// Batched influence columns: the superposition runs the chunk's whole one-layer work
+// list (work_scatter_kernel): radius block R is [rStart[R], rStart[R - 1]) (or up to
+// workCount), and the claim counters restart.
+__global__ void column_list_view_kernel(BeamStateDev* __restrict__ beam) {
+    const int t = threadIdx.x;
+    if (t <= kMaxR) {
+        const int end = t > 0 ? beam->rStart[t - 1] : beam->workCount;
+        beam->mergedR[t] = max(end - beam->rStart[t], 0);
+    }
+    if (t == 0) {
+        beam->workNext = 0;
+        beam->workNextSmall = 0;
+        beam->workNextTiny = 0;
+    }
+}
+
+// Batched influence columns: bev_fixed_to_float_kernel for volume q (blockIdx.y) over
+// its layer's live cells (LayerStateDev::liveLo/liveHi).
+__global__ void __launch_bounds__(256) column_fixed_to_float_kernel(BeamGeomDev g, const BeamStateDev* __restrict__ beam,
+                                                                    const LayerStateDev* __restrict__ ls,
+                                                                    unsigned long long* __restrict__ fixed,
+                                                                    float* __restrict__ bev, size_t stride) {
+    const int q = blockIdx.y;
+    const LayerStateDev& st = ls[q];
+    if (st.liveLo[0] > st.liveHi[0]) return;
+    const int x0 = max(st.liveLo[0], 0) & ~1, x1 = min(st.liveHi[0], g.bevX - 1) | 1;
+    const int y0 = max(st.liveLo[1], 0), y1 = min(st.liveHi[1], g.bevY - 1);
+    const int z0 = max(st.liveLo[2], 0), z1 = min(st.liveHi[2], g.steps - 1);
+    if (x1 < x0 || y1 < y0 || z1 < z0) return;
+    const int pw = (x1 - x0 + 1) / 2, rows = y1 - y0 + 1;
+    const size_t n = static_cast<size_t>(pw) * rows * (z1 - z0 + 1);
+    const double unit = ldexp(1.0, -beam->fixedShift);
+    // stride is even (bevX is), so every volume starts on a cell pair.
+    ulonglong2* f2 = reinterpret_cast<ulonglong2*>(fixed + static_cast<size_t>(q) * stride);
+    float2* b2 = reinterpret_cast<float2*>(bev + static_cast<size_t>(q) * stride);
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const int xp = static_cast<int>(i % pw);
+        const size_t r = i / pw;
+        const int y = y0 + static_cast<int>(r % rows);
+        const int z = z0 + static_cast<int>(r / rows);
+        const size_t pr = ((static_cast<size_t>(z) * g.bevY + y) * g.bevX + x0) / 2 + xp;
+        const ulonglong2 v = f2[pr];
+        if (v.x | v.y) {
+            float2 o = b2[pr];
+            o.x += float(double(v.x) * unit);
+            o.y += float(double(v.y) * unit);
+            b2[pr] = o;
+            f2[pr] = make_ulonglong2(0ull, 0ull);
+        }
+    }
+}
+
+}  // namespace
+
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                              BeamStateDev* beam, float* bev, unsigned long long* bevFixed, int shiftOffset, int numSMs,
                              cudaStream_t s) {
-    // Items are sorted by range: the wide radii come first.
-    cudaError_t e = launch_range<true, kSplitR + 1, kMaxR, kWideBlocks>(g, idd, rsigma, work, beam, bevFixed,
-                                                                        shiftOffset, numSMs * kWideBlocks, 0, false, s);
-    if (e != cudaSuccess) return e;
-    e = launch_range<false, kSplitR2 + 1, kSplitR, kMidBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
-                                                               numSMs * kMidBlocks, 1, true, s);
-    if (e != cudaSuccess) return e;
-    e = launch_range<false, 0, kSplitR2, kNarrowBlocks>(g, idd, rsigma, work, beam, bevFixed, shiftOffset,
-                                                        numSMs * kNarrowBlocks, 2, true, s);
+    cudaError_t e = launch_instances(g, idd, rsigma, work, beam, bevFixed, shiftOffset, numSMs, 0, s);
     if (e != cudaSuccess) return e;
     bev_fixed_to_float_kernel<<<numSMs * 8, 256, 0, s>>>(g, beam, bevFixed, bev, shiftOffset);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_superpose_columns(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                                     BeamStateDev* beam, const LayerStateDev* ls, int nCols, float* bev,
+                                     unsigned long long* bevFixed, size_t stride, int numSMs, cudaStream_t s) {
+    if (nCols <= 0) return cudaSuccess;
+    if (stride % 2) return cudaErrorInvalidValue;
+    column_list_view_kernel<<<1, 64, 0, s>>>(beam);
+    cudaError_t e = launch_instances(g, idd, rsigma, work, beam, bevFixed, 0, numSMs, stride, s);
+    if (e != cudaSuccess) return e;
+    const int per = std::max(1, (numSMs * 8) / nCols);
+    column_fixed_to_float_kernel<<<dim3(per, nCols), 256, 0, s>>>(g, beam, ls, bevFixed, bev, stride);
     return cudaGetLastError();
 }
 

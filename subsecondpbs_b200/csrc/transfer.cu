@@ -59,36 +59,27 @@ __device__ __forceinline__ float bev_sample(const float* __restrict__ v, int nx,
     return c0 + (c1 - c0) * tz;
 }
 
-// Transfer box from the eight BEV corners (wrapper.cu:5343-5394); the z range spans
-// the deepest superposed step of all layers, or of `layer` alone when it is given.
-// With `live` the corners are those of the cells the superposition items can have
-// written (BeamStateDev::liveLo/liveHi, one cell of trilinear reach added): every
+// Transfer box from the eight BEV corners (wrapper.cu:5343-5394) over the steps
+// [first, passive). With `live` the corners are those of the cells the superposition
+// items can have written (liveLo/liveHi, one cell of trilinear reach added): every
 // voxel outside samples only zero cells, so the transfer and the box's readers skip
-// it. No live cell gives an empty box.
-__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const LayerStateDev* layer, int live) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    // Last kernel of the beam's work list with one thread: hand the beam's error
-    // flags to the context's error word, which outlives the beam state.
-    if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
-    const int first = beam->firstInside;
-    const int passive = layer ? layer->calcPassive : beam->maxCalcPassive;
+// it. Returns whether the box holds a voxel; no live cell gives an empty box.
+__device__ bool plan_transfer_box(const BeamGeomDev& g, int first, int passive, bool live, const int* liveLo,
+                                  const int* liveHi, int start[3], int maxi[3]) {
+    start[0] = start[1] = start[2] = 0;
+    maxi[0] = maxi[1] = maxi[2] = -1;
     float xs[2] = {-float(kMaxR), float(g.pitchX + kMaxR - 1)};
     float ys[2] = {-float(kMaxR), float(g.pitchY + kMaxR - 1)};
     float zs[2] = {float(first), float(passive - 1)};
     if (live) {
-        if (beam->liveLo[0] > beam->liveHi[0]) {
-            beam->transferValid = 0;
-            beam->transferStart[0] = beam->transferStart[1] = beam->transferStart[2] = 0;
-            beam->transferMax[0] = beam->transferMax[1] = beam->transferMax[2] = -1;
-            return;
-        }
+        if (liveLo[0] > liveHi[0]) return false;
         // Padded BEV cell c is ray coordinate c - kMaxR.
-        xs[0] = fmaxf(xs[0], float(beam->liveLo[0] - kMaxR - 1));
-        xs[1] = fminf(xs[1], float(beam->liveHi[0] - kMaxR + 1));
-        ys[0] = fmaxf(ys[0], float(beam->liveLo[1] - kMaxR - 1));
-        ys[1] = fminf(ys[1], float(beam->liveHi[1] - kMaxR + 1));
-        zs[0] = fmaxf(zs[0], float(first + beam->liveLo[2] - 1));
-        zs[1] = fminf(zs[1], float(first + beam->liveHi[2] + 1));
+        xs[0] = fmaxf(xs[0], float(liveLo[0] - kMaxR - 1));
+        xs[1] = fminf(xs[1], float(liveHi[0] - kMaxR + 1));
+        ys[0] = fmaxf(ys[0], float(liveLo[1] - kMaxR - 1));
+        ys[1] = fminf(ys[1], float(liveHi[1] - kMaxR + 1));
+        zs[0] = fmaxf(zs[0], float(first + liveLo[2] - 1));
+        zs[1] = fminf(zs[1], float(first + liveHi[2] + 1));
     }
     V3 mx = v3(-1.0f, -1.0f, -1.0f), mn = v3(100000.0f, 100000.0f, 100000.0f);
     for (int zi = 0; zi < 2; ++zi)
@@ -102,17 +93,45 @@ __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const
                 mn.y = fminf(mn.y, p.y);
                 mn.z = fminf(mn.z, p.z);
             }
-    beam->transferStart[0] = max((int(floorf(mn.x)) / 32) * 32, 0);
-    beam->transferStart[1] = max(int(floorf(mn.y)), 0);
-    beam->transferStart[2] = max(int(floorf(mn.z)), 0);
-    beam->transferMax[0] = min(int(ceilf(mx.x)), g.doseX - 1);
-    beam->transferMax[1] = min(int(ceilf(mx.y)), g.doseY - 1);
-    beam->transferMax[2] = min(int(ceilf(mx.z)), g.doseZ - 1);
+    start[0] = max((int(floorf(mn.x)) / 32) * 32, 0);
+    start[1] = max(int(floorf(mn.y)), 0);
+    start[2] = max(int(floorf(mn.z)), 0);
+    maxi[0] = min(int(ceilf(mx.x)), g.doseX - 1);
+    maxi[1] = min(int(ceilf(mx.y)), g.doseY - 1);
+    maxi[2] = min(int(ceilf(mx.z)), g.doseZ - 1);
+    return passive > first && start[0] <= maxi[0] && start[1] <= maxi[1] && start[2] <= maxi[2];
+}
+
+// The beam's transfer box: over the deepest superposed step of all layers, or of
+// `layer` alone when it is given (plan_transfer_box), and the transfer parameters.
+__global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const LayerStateDev* layer, int live) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // Last kernel of the beam's work list with one thread: hand the beam's error
+    // flags to the context's error word, which outlives the beam state.
+    if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
+    const int first = beam->firstInside;
+    const int passive = layer ? layer->calcPassive : beam->maxCalcPassive;
     const ToFan t = invert_and_shift(g.rayIdxToDoseIdx, v3(float(kMaxR), float(kMaxR), -float(first)));
     beam->transfer = make_transfer_params(t);
-    beam->transferValid = passive > first && beam->transferStart[0] <= beam->transferMax[0] &&
-                          beam->transferStart[1] <= beam->transferMax[1] &&
-                          beam->transferStart[2] <= beam->transferMax[2];
+    beam->transferValid = plan_transfer_box(g, first, passive, live != 0, beam->liveLo, beam->liveHi,
+                                            beam->transferStart, beam->transferMax);
+}
+
+// Batched influence columns: every layer of the chunk [layer0, layer0 + nCols) gets
+// the transfer box of its own live cells (LayerStateDev::colStart/colMax/colValid);
+// the beam gets the transfer parameters, which do not depend on the layer.
+__global__ void column_transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, LayerStateDev* ls, int nCols) {
+    const int q = threadIdx.x;
+    const int first = beam->firstInside;
+    if (q == 0) {
+        if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
+        const ToFan t = invert_and_shift(g.rayIdxToDoseIdx, v3(float(kMaxR), float(kMaxR), -float(first)));
+        beam->transfer = make_transfer_params(t);
+    }
+    if (q < nCols) {
+        LayerStateDev& st = ls[q];
+        st.colValid = plan_transfer_box(g, first, st.calcPassive, true, st.liveLo, st.liveHi, st.colStart, st.colMax);
+    }
 }
 
 // primTransfDiv (src/algorithms/prim_transf_kernel.cu:11-44). The reference launches
@@ -193,7 +212,98 @@ __global__ void dose_box_kernel(double* dose, float* out, int3 dims, int3 lo, in
     }
 }
 
+// Batched influence columns: column q (blockIdx.y) samples its own BEV volume
+// (bev + q * bevStride) over its layer's transfer box (column_written_box) and adds
+// into its own FP64 dose buffer laid out over `fb`. Items and sampling as in
+// transfer_kernel; the blocks of a column stride over its items.
+__global__ void __launch_bounds__(256)
+column_transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, size_t bevStride,
+                       const BeamStateDev* __restrict__ beam, const LayerStateDev* __restrict__ ls, ColBox fb,
+                       double* __restrict__ colDose) {
+    const int q = blockIdx.y;
+    int lo[3], hi[3];
+    if (!column_written_box(ls[q], g.doseX, g.doseY, fb, lo, hi)) return;
+    const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1;
+    const int nzc = (hi[2] - lo[2] + kTransferZChunk) / kTransferZChunk;
+    const long long items = static_cast<long long>(nx) * ny * nzc;
+    const TransferParams T = beam->transfer;
+    const float* v0 = bev + static_cast<size_t>(q) * bevStride;
+    const size_t fbN = static_cast<size_t>(fb.ext[0]) * fb.ext[1] * fb.ext[2];
+    double* out = colDose + static_cast<size_t>(q) * fbN;
+    const size_t slice = static_cast<size_t>(fb.ext[0]) * fb.ext[1];
+    for (long long it = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = lo[0] + static_cast<int>(it % nx);
+        const long long r = it / nx;
+        const int y = lo[1] + static_cast<int>(r % ny);
+        const int z0 = lo[2] + static_cast<int>(r / ny) * kTransferZChunk;
+        const V3 start = transfer_start(T, x, y);
+        double* col = out + static_cast<size_t>(y - fb.lo[1]) * fb.ext[0] + (x - fb.lo[0]);
+        float v[kTransferZChunk];
+#pragma unroll
+        for (int k = 0; k < kTransferZChunk; ++k) {
+            const int z = z0 + k;
+            v[k] = 0.0f;
+            if (z <= hi[2]) {
+                const V3 f = transfer_fan_idx(T, start, z);
+                if (!(f.x + 0.5f < 0.0f || f.y + 0.5f < 0.0f || f.z + 0.5f < 0.0f))
+                    v[k] = bev_sample(v0, g.bevX, g.bevY, g.steps, f.x, f.y, f.z);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kTransferZChunk; ++k)
+            if (v[k] > 0.0f) col[static_cast<size_t>(z0 + k - fb.lo[2]) * slice] += double(v[k]);
+    }
+}
+
+// Batched influence columns: zeroes column q's float BEV volume over its layer's
+// live cells (the only cells its superposition wrote), so every volume is zero for
+// the next batch.
+__global__ void __launch_bounds__(256) column_bev_clear_kernel(BeamGeomDev g, float* __restrict__ bev, size_t bevStride,
+                                                               const LayerStateDev* __restrict__ ls) {
+    const int q = blockIdx.y;
+    const LayerStateDev& st = ls[q];
+    if (st.liveLo[0] > st.liveHi[0]) return;
+    const int x0 = max(st.liveLo[0], 0), x1 = min(st.liveHi[0], g.bevX - 1);
+    const int y0 = max(st.liveLo[1], 0), y1 = min(st.liveHi[1], g.bevY - 1);
+    const int z0 = max(st.liveLo[2], 0), z1 = min(st.liveHi[2], g.steps - 1);
+    if (x1 < x0 || y1 < y0 || z1 < z0) return;
+    const int w = x1 - x0 + 1, rows = y1 - y0 + 1;
+    const size_t n = static_cast<size_t>(w) * rows * (z1 - z0 + 1);
+    float* v0 = bev + static_cast<size_t>(q) * bevStride;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = x0 + static_cast<int>(i % w);
+        const size_t r = i / w;
+        const int y = y0 + static_cast<int>(r % rows);
+        const int z = z0 + static_cast<int>(r / rows);
+        v0[(static_cast<size_t>(z) * g.bevY + y) * g.bevX + x] = 0.0f;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_column_transfer(const BeamGeomDev& g, const float* bev, size_t bevStride, BeamStateDev* beam,
+                                   LayerStateDev* ls, int nCols, const ColBox& fb, double* colDose, cudaStream_t s) {
+    if (nCols <= 0) return cudaSuccess;
+    if (nCols > 1024) return cudaErrorInvalidValue;
+    column_transfer_planner_kernel<<<1, ((nCols + 31) / 32) * 32, 0, s>>>(g, beam, ls, nCols);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // Blocks per column: a few waves over all columns together.
+    const int per = std::max(1, (sms * kTransferBlocksPerSM) / nCols);
+    column_transfer_kernel<<<dim3(per, nCols), 256, 0, s>>>(g, bev, bevStride, beam, ls, fb, colDose);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_column_bev_clear(const BeamGeomDev& g, float* bev, size_t bevStride, const LayerStateDev* ls,
+                                    int nCols, cudaStream_t s) {
+    if (nCols <= 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per = std::max(1, (sms * 8) / nCols);
+    column_bev_clear_kernel<<<dim3(per, nCols), 256, 0, s>>>(g, bev, bevStride, ls);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_transfer_planner(const BeamGeomDev& g, BeamStateDev* beam, const LayerStateDev* layer, int live,
                                     cudaStream_t s) {
