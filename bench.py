@@ -336,12 +336,15 @@ def _carbon_plan(local: int, reps: int = 3) -> dict:
             "ms_per_plan": round(statistics.median(ms), 3), "timing": f"CUDA events, median of {reps}"}
 
 
-def _operator_export(local: int, n_spots: int = 256) -> dict:
-    """Influence-matrix export (pbs_context_influence_csc) of a batch of the headline
-    beam's spots: wall time of the call (all columns, entries compacted on the device
-    and copied to host memory), after one warm-up batch."""
+def _operator_export(local: int, n_spots: int = 1024, n_face: int = 256) -> dict:
+    """Influence-matrix export of the headline beam's spots: the C ABI call
+    (pbs_context_influence_csc: every column computed, compacted on the device and
+    copied to host arrays) on `n_spots` spots, and the Python face (which adds the
+    scipy CSC matrix) on `n_face` spots, wall time after a warm-up call each."""
+    import ctypes as C
     import time
 
+    from subsecondpbs_b200 import _lib
     from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
 
     case = _headline_case()
@@ -350,16 +353,35 @@ def _operator_export(local: int, n_spots: int = 256) -> dict:
     eng.set_ct(case["ct"], case["ct_dims"], case["ct_resolution"], case["ct_corner"])
     eng.set_dose_grid(case["dose_dims"], case["dose_resolution"], case["dose_corner"])
     beam = eng.prepare_beam(case["beam"])
-    begin = 1500
+    bd, _keep = beam
+    begin = 1000
     cap = 40000 * n_spots
-    eng.influence_csc(beam, spot_begin=begin - n_spots, spot_count=n_spots, capacity=cap)
+    col_ptr = np.zeros(n_spots + 1, dtype=np.int64)
+    rows = np.zeros(cap, dtype=np.int32)
+    vals = np.zeros(cap, dtype=np.float32)
+    nnz = C.c_longlong(0)
+
+    def c_call(first):
+        return eng._lib.pbs_context_influence_csc(
+            eng._h, C.byref(bd), 0, first, n_spots, 0.0, col_ptr.ctypes.data_as(C.POINTER(C.c_longlong)),
+            rows.ctypes.data_as(C.c_void_p), vals.ctypes.data_as(C.c_void_p), cap, C.byref(nnz))
+
+    _lib.check(c_call(0))
     t = time.perf_counter()
-    a = eng.influence_csc(beam, spot_begin=begin, spot_count=n_spots, capacity=cap)
-    ms = (time.perf_counter() - t) * 1e3
+    _lib.check(c_call(begin))
+    c_ms = (time.perf_counter() - t) * 1e3
+    entries = int(nnz.value)
+    fcap = 40000 * n_face
+    eng.influence_csc(beam, spot_begin=begin - n_face, spot_count=n_face, capacity=fcap)
+    t = time.perf_counter()
+    a = eng.influence_csc(beam, spot_begin=begin, spot_count=n_face, capacity=fcap)
+    f_ms = (time.perf_counter() - t) * 1e3
     eng.close()
     return {"workload": f"{n_spots} spots of the headline beam (from spot {begin}), threshold 0",
-            "ms": round(ms, 2), "ms_per_spot": round(ms / n_spots, 4), "entries": int(a.nnz),
-            "timing": "wall time of one pbs_context_influence_csc call after a warm-up batch"}
+            "ms": round(c_ms, 2), "ms_per_spot": round(c_ms / n_spots, 4), "entries": entries,
+            "timing": "wall time of one pbs_context_influence_csc call (C ABI, host arrays) after a warm-up call",
+            "python_face": {"spots": n_face, "ms": round(f_ms, 2), "ms_per_spot": round(f_ms / n_face, 4),
+                            "entries": int(a.nnz), "what": "DoseEngine.influence_csc, scipy CSC matrix included"}}
 
 
 def _upstream_cpu_conv(eng, stats: dict, spacing_mm: float, our_conv_ms: float, budget_s: float = 10.0) -> dict:
