@@ -12,6 +12,7 @@
 #include <algorithm>
 
 #include "device_util.cuh"
+#include "work_blocks.cuh"
 #include "kernels.h"
 #include "launch_util.h"
 
@@ -205,32 +206,53 @@ __device__ __forceinline__ void adjoint_dispatch(int r, const float* tileG, floa
     if constexpr (R < RHi) adjoint_dispatch<R + 1, RHi>(r, tileG, eRow, E4, P, dose, rs, rbarRay, sy, sx);
 }
 
-// Persistent CTAs over the whole work list of the (single) layer chunk; three per
-// SM, as many as their shared memory allows.
-__global__ void __launch_bounds__(kAdjThreads, 3)
+// Shared memory of an instance for radii up to RHi: the tile's gradient footprint,
+// then either the pair form's weight chunks and pair sums (RHi <= kSplitR) or each
+// source's weight row.
+template <int RHi>
+struct AdjShape {
+    static constexpr int kTile = (kTileY + 2 * RHi) * (kTileX + 2 * RHi);  // 16(4+R)(16+R) bytes: 16-byte aligned
+    static constexpr bool kPairs = RHi <= kSplitR;
+    static constexpr int kQ = (RHi + 1 + 3) / 4;
+    static constexpr int kPS = (RHi + 1) | 1;
+    static constexpr int kRest = kPairs ? kQ * kAdjThreads * 4 + kAdjThreads * kPS : kAdjThreads * kAdjEStride;
+    static constexpr size_t kSmemBytes = size_t(kTile + kRest) * sizeof(float);
+};
+
+// Persistent CTAs over the radii RLo..RHi of the chunk's one-layer work list, taken
+// radius block by radius block through the range's counter as in the forward
+// superposition. The three instances of a beam overlap in the same way: each CTA
+// lets the next instance launch at once (their items only add into the rays'
+// accumulators) and waits for the previous instance before it exits.
+template <int RLo, int RHi, int MinBlocks>
+__global__ void __launch_bounds__(kAdjThreads, MinBlocks)
 superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const float* __restrict__ rsig,
                          const int4* __restrict__ work, BeamStateDev* __restrict__ beam, const float* __restrict__ gradBev,
-                         float* __restrict__ rbar) {
+                         float* __restrict__ rbar, int range) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     extern __shared__ __align__(16) float adjSm[];
+    using Sh = AdjShape<RHi>;
     float* tileG = adjSm;                        // [8+2R][32+2R] BEV gradient of the tile's footprint
-    float* eS = adjSm + kAdjOutFloats;           // [256][kAdjEStride] each source's weights (R > kSplitR)
-    // Pair form (R <= kSplitR): the weights as float4 chunks [4][256] and the pair
-    // sums P [256][17], over the same space.
-    float4* E4 = reinterpret_cast<float4*>(eS);
-    float* P = eS + 4 * 4 * kAdjThreads;
-    __shared__ int sItem;
+    float* eS = adjSm + Sh::kTile;               // [256][kAdjEStride] each source's weights (R > kSplitR)
+    float4* E4 = reinterpret_cast<float4*>(eS);  // pair form: weight chunks [Q][256] ...
+    float* P = eS + Sh::kQ * kAdjThreads * 4;    // ... and pair sums [256][PS]
+    __shared__ int sItem[2];
+    __shared__ RadiusBlocks<RLo, RHi> sBlocks;
     const int t = threadIdx.x;
-    const int count = beam->workCount;
+    int* counter = range == 0 ? &beam->workNext : (range == 1 ? &beam->workNextSmall : &beam->workNextTiny);
     const size_t padPlane = static_cast<size_t>(g.pitchX) * g.pitchY;
     const size_t layerStride = static_cast<size_t>(g.steps) * padPlane;
     const size_t bevPlane = static_cast<size_t>(g.bevX) * g.bevY;
     const size_t rayPlane = static_cast<size_t>(g.rayX) * g.rayY;
+    load_blocks<RLo, RHi>(beam, sBlocks);
+    if (t == 0) sItem[0] = atomicAdd(counter, 1);
+    __syncthreads();
+    int buf = 0;
     for (;;) {
-        if (t == 0) sItem = atomicAdd(&beam->workNext, 1);
-        __syncthreads();
-        const int w = sItem;
-        if (w >= count) break;
-        const int4 it = work[w];
+        const int c = sItem[buf];
+        if (c >= sBlocks.total) break;
+        if (t == 0) sItem[buf ^ 1] = atomicAdd(counter, 1);
+        const int4 it = work[block_slot<RLo, RHi>(sBlocks, c)];
         const int lc = it.x & 0xff, tile = it.y, zRel = it.z, R = it.w;
         const int tx = tile % g.tilesX, ty = tile / g.tilesX;
         const int Ho = kTileY + 2 * R, Wo = kTileX + 2 * R;
@@ -246,12 +268,43 @@ superpose_adjoint_kernel(BeamGeomDev g, const float* __restrict__ idd, const flo
         const size_t s = lc * layerStride + zRel * padPlane + static_cast<size_t>(ry) * g.pitchX + rx;
         const float dose = idd[s];
         const bool live = dose > 0.0f && ry < g.rayY && rx < g.rayX;
-        adjoint_dispatch<0, kMaxR>(R, tileG, eS + t * kAdjEStride, E4, P, dose, live ? rsig[s] : 0.0f,
-                                   live ? rbar + lc * rayPlane + static_cast<size_t>(ry) * g.rayX + rx : nullptr,
-                                   sy, sx);
+        if (R >= RLo && R <= RHi)
+            adjoint_dispatch<RLo, RHi>(R, tileG, eS + t * kAdjEStride, E4, P, dose, live ? rsig[s] : 0.0f,
+                                       live ? rbar + lc * rayPlane + static_cast<size_t>(ry) * g.rayX + rx : nullptr,
+                                       sy, sx);
+        // Every thread is past the item (and has read sItem[buf]) before the next
+        // claim lands in that slot.
         __syncthreads();
+        buf ^= 1;
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
+
+template <int RLo, int RHi, int MinBlocks>
+cudaError_t launch_adjoint_range(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
+                                 BeamStateDev* beam, const float* gradBev, float* rbar, int numSMs, int range,
+                                 bool overlap, cudaStream_t s) {
+    auto k = superpose_adjoint_kernel<RLo, RHi, MinBlocks>;
+    const size_t smem = AdjShape<RHi>::kSmemBytes;
+    cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(k), smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(numSMs * MinBlocks);
+    cfg.blockDim = dim3(kAdjThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, g, idd, rsigma, work, beam, gradBev, rbar, range);
+}
+
+// Resident CTAs per SM of the adjoint instances (radii 16..32, 8..15, 0..7).
+constexpr int kAdjWideBlocks = 3;
+constexpr int kAdjMidBlocks = 4;
+constexpr int kAdjNarrowBlocks = 6;
 
 }  // namespace
 
@@ -268,11 +321,16 @@ cudaError_t launch_transfer_adjoint(const BeamGeomDev& g, const double* gradDose
 cudaError_t launch_superpose_adjoint(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                                      BeamStateDev* beam, const float* gradBev, float* rbar, int numSMs,
                                      cudaStream_t s) {
-    const size_t smem = (size_t(kAdjOutFloats) + size_t(kAdjThreads) * kAdjEStride) * sizeof(float);
-    cudaError_t e = set_smem_limit(reinterpret_cast<const void*>(superpose_adjoint_kernel), smem);
+    cudaError_t e = launch_one_layer_list_view(beam, s);
     if (e != cudaSuccess) return e;
-    superpose_adjoint_kernel<<<numSMs * 3, kAdjThreads, smem, s>>>(g, idd, rsigma, work, beam, gradBev, rbar);
-    return cudaGetLastError();
+    e = launch_adjoint_range<kSplitR + 1, kMaxR, kAdjWideBlocks>(g, idd, rsigma, work, beam, gradBev, rbar, numSMs,
+                                                                 0, false, s);
+    if (e != cudaSuccess) return e;
+    e = launch_adjoint_range<kSplitR2 + 1, kSplitR, kAdjMidBlocks>(g, idd, rsigma, work, beam, gradBev, rbar, numSMs,
+                                                                   1, true, s);
+    if (e != cudaSuccess) return e;
+    return launch_adjoint_range<0, kSplitR2, kAdjNarrowBlocks>(g, idd, rsigma, work, beam, gradBev, rbar, numSMs, 2,
+                                                               true, s);
 }
 
 }  // namespace pbs

@@ -115,6 +115,9 @@ cudaError_t launch_nuc_codes(const BeamGeomDev& gn, int layer0, int nLayers, con
 cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                              BeamStateDev* beam, float* bev, unsigned long long* bevFixed, int shiftOffset,
                              int numSMs, cudaStream_t s);
+// Radius blocks and claim counters of the chunk's one-layer work list
+// (merged == false in launch_bin_plan), for the superposition kernels.
+cudaError_t launch_one_layer_list_view(BeamStateDev* beam, cudaStream_t s);
 // Batched influence columns: the chunk's whole one-layer work list (layers
 // [0, nCols) of `ls`), item layer q into BEV volume q (bev / bevFixed + q * stride
 // cells), each volume converted over its layer's live cells.

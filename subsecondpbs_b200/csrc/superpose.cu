@@ -43,6 +43,7 @@
 #include <algorithm>
 
 #include "device_util.cuh"
+#include "work_blocks.cuh"
 #include "kernels.h"
 #include "launch_util.h"
 
@@ -453,42 +454,6 @@ __device__ __forceinline__ bool dispatch_wide(int r, float4* E4, float* EW, int*
 // The persistent kernel.
 // ============================================================================
 
-// Radius blocks of an instance: claim c of the instance is item c of the
-// concatenated merged items of radii RHi, RHi - 1, ..., RLo.
-template <int RLo, int RHi>
-struct RadiusBlocks {
-    int start[RHi - RLo + 1];
-    int count[RHi - RLo + 1];
-    int total;
-};
-
-template <int RLo, int RHi>
-__device__ __forceinline__ void load_blocks(const BeamStateDev* beam, RadiusBlocks<RLo, RHi>& b) {
-    const int t = threadIdx.x;
-    if (t <= RHi - RLo) {
-        const int R = RHi - t;
-        const int end = R > 0 ? beam->rStart[R - 1] : beam->workCount;
-        b.start[t] = beam->rStart[R];
-        b.count[t] = max(min(beam->mergedR[R], end - beam->rStart[R]), 0);
-    }
-    __syncthreads();
-    if (t == 0) {
-        int n = 0;
-        for (int i = 0; i <= RHi - RLo; ++i) n += b.count[i];
-        b.total = n;
-    }
-}
-
-template <int RLo, int RHi>
-__device__ __forceinline__ int block_slot(const RadiusBlocks<RLo, RHi>& b, int c) {
-#pragma unroll 1
-    for (int i = 0; i <= RHi - RLo; ++i) {
-        if (c < b.count[i]) return b.start[i] + c;
-        c -= b.count[i];
-    }
-    return -1;
-}
-
 // Persistent CTA loop over the merged items of radii RLo..RHi, claimed one at a
 // time through the range's counter (the next claim is issued before the current
 // item runs so that its latency is hidden). Items are taken radius block by radius
@@ -650,10 +615,10 @@ cudaError_t launch_instances(const BeamGeomDev& g, const float* idd, const float
                                                            numSMs * kNarrowBlocks, 2, true, layerBevStride, s);
 }
 
-// Batched influence columns: the superposition runs the chunk's whole one-layer work
-// list (work_scatter_kernel): radius block R is [rStart[R], rStart[R - 1]) (or up to
-// workCount), and the claim counters restart.
-__global__ void column_list_view_kernel(BeamStateDev* __restrict__ beam) {
+// A superposition over the chunk's whole one-layer work list (work_scatter_kernel):
+// radius block R is [rStart[R], rStart[R - 1]) (or up to workCount), and the claim
+// counters restart.
+__global__ void one_layer_list_view_kernel(BeamStateDev* __restrict__ beam) {
     const int t = threadIdx.x;
     if (t <= kMaxR) {
         const int end = t > 0 ? beam->rStart[t - 1] : beam->workCount;
@@ -713,12 +678,17 @@ cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float
     return cudaGetLastError();
 }
 
+cudaError_t launch_one_layer_list_view(BeamStateDev* beam, cudaStream_t s) {
+    one_layer_list_view_kernel<<<1, 64, 0, s>>>(beam);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_superpose_columns(const BeamGeomDev& g, const float* idd, const float* rsigma, const int4* work,
                                      BeamStateDev* beam, const LayerStateDev* ls, int nCols, float* bev,
                                      unsigned long long* bevFixed, size_t stride, int numSMs, cudaStream_t s) {
     if (nCols <= 0) return cudaSuccess;
     if (stride % 2) return cudaErrorInvalidValue;
-    column_list_view_kernel<<<1, 64, 0, s>>>(beam);
+    one_layer_list_view_kernel<<<1, 64, 0, s>>>(beam);
     cudaError_t e = launch_instances(g, idd, rsigma, work, beam, bevFixed, 0, numSMs, stride, s);
     if (e != cudaSuccess) return e;
     const int per = std::max(1, (numSMs * 8) / nCols);
