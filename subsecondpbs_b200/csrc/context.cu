@@ -1291,11 +1291,10 @@ int Context::run_beam(const PbsBeamDesc& b, int nuclear, const AdjointArgs* adj,
             }
             doseReady = true;
         }
-        // The box over the cells the items wrote: the whole beam's (work_merge_kernel),
-        // or a column's layer (work_layer_view_kernel); the per-layer transfers of the
-        // reference's depth convention take the box over the layer's steps.
-        PBS_CUDA(launch_transfer_planner(g, dbs, layer, layer == nullptr || columnLists, stream),
-                 "transfer_planner");
+        // The box over the cells the items wrote (work_merge_kernel) for the whole beam;
+        // the per-layer transfers of the reference's depth convention take the box over
+        // the layer's steps.
+        PBS_CUDA(launch_transfer_planner(g, dbs, layer, layer == nullptr, stream), "transfer_planner");
         PBS_CUDA(launch_transfer(g, dBev, dbs, static_cast<double*>(dose64.ptr), stream), "transfer");
         if (bio) {
             // The beam's own dose and the channels into the biological accumulators.

@@ -770,36 +770,6 @@ cudaError_t launch_idd(const BeamGeomDev& g, const LutsDev& luts, int layer0, in
     return cudaGetLastError();
 }
 
-// Points the forward superposition at one layer of the chunk's one-layer work list
-// (work_scatter_kernel): the layer's radius-R items are the block at ls.offR[R]
-// (the next block of the list starts at or after its end, so superpose_kernel's
-// block bounds hold), the claim counters restart, and the live-cell box is the
-// layer's, for the transfer planner.
-__global__ void work_layer_view_kernel(int layer0, int lc, const LayerStateDev* __restrict__ ls,
-                                       BeamStateDev* __restrict__ beam, int workCapacity) {
-    const LayerStateDev& st = ls[layer0 + lc];
-    const int t = threadIdx.x;
-    if (t <= kMaxR) {
-        beam->rStart[t] = st.offR[t];
-        beam->mergedR[t] = max(min(st.liveR[t], workCapacity - st.offR[t]), 0);
-    }
-    if (t < 3) {
-        beam->liveLo[t] = st.liveLo[t];
-        beam->liveHi[t] = st.liveHi[t];
-    }
-    if (t == 0) {
-        beam->workNext = 0;
-        beam->workNextSmall = 0;
-        beam->workNextTiny = 0;
-    }
-}
-
-cudaError_t launch_work_layer_view(int layer0, int lc, const LayerStateDev* ls, BeamStateDev* beam, int workCapacity,
-                                   cudaStream_t s) {
-    work_layer_view_kernel<<<1, 64, 0, s>>>(layer0, lc, ls, beam, workCapacity);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const uint8_t* codes, LayerStateDev* ls,
                             BeamStateDev* beam, int4* work, int workCapacity, bool merged,
                             const LayerStateDev* primaryLs, const BeamStateDev* primaryBeam, cudaStream_t s) {

@@ -95,10 +95,6 @@ cudaError_t launch_column_transfer(const BeamGeomDev& g, const float* bev, size_
                                    LayerStateDev* ls, int nCols, const ColBox& fb, double* colDose, cudaStream_t s);
 cudaError_t launch_column_bev_clear(const BeamGeomDev& g, float* bev, size_t bevStride, const LayerStateDev* ls,
                                     int nCols, cudaStream_t s);
-// Points the forward superposition at chunk layer `lc`'s items of the one-layer list
-// (merged == false above) and the transfer planner's live box at that layer's.
-cudaError_t launch_work_layer_view(int layer0, int lc, const LayerStateDev* ls, BeamStateDev* beam, int workCapacity,
-                                   cudaStream_t s);
 // Nuclear halo: clear the chunk's halo IDD (0) and sigma (+inf) before the IDD
 // kernel, and the halo tile codes and histograms after the primary layer plan.
 // `gn` is the halo grid (pitch = nucX x nucY).

@@ -556,9 +556,8 @@ cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rs
 
 // Adds the fixed-point BEV of the chunk to the float BEV and clears it for the next
 // superposition, over the cells the items can have written: the box of live cells
-// (BeamStateDev::liveLo/liveHi, from work_merge_kernel or, for one layer,
-// work_layer_view_kernel) within the planes written so far,
-// [0, maxCalcPassive - firstInside). Every cell is converted once, so the float BEV is
+// (BeamStateDev::liveLo/liveHi, from work_merge_kernel) within the planes written so
+// far, [0, maxCalcPassive - firstInside). Every cell is converted once, so the float BEV is
 // the same on every run.
 __global__ void __launch_bounds__(256) bev_fixed_to_float_kernel(BeamGeomDev g, const BeamStateDev* __restrict__ beam,
                                                                  unsigned long long* __restrict__ fixed,
