@@ -780,7 +780,8 @@ size_t Context::device_bytes() const {
                             &iddBuf, &rsBuf, &bev, &cpb, &subspots, &floatOut, &firstIn, &firstOut, &firstPassive,
                             &codes, &work, &lp, &ls, &bs, &stats, &nucWeight, &nucSqSigma, &rayToNuc, &nucIddBuf,
                             &nucRsBuf, &nucCodes, &nucWork, &nucBev, &bevFixed, &nucLs, &nucBs, &errWord, &gradDoseBuf, &bevGrad,
-                            &rbarBuf, &gradInterm, &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
+                            &rbarBuf, &gradInterm, &gradLattice, &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals,
+                            &opNorm, &opVoxels, &colBev, &colFixed, &colDose})
         n += b->bytes;
     return n;
 }
@@ -790,8 +791,10 @@ void Context::release_beam_buffers() {
     for (DevBuf* b : {&dens, &wepl, &weplMin, &rayW, &interm, &lattice, &iddBuf, &rsBuf, &bev, &cpb, &subspots,
                       &floatOut, &firstIn, &firstOut, &firstPassive, &codes, &work, &rayToNuc, &nucIddBuf, &nucRsBuf,
                       &nucCodes, &nucWork, &nucBev, &bevFixed, &gradDoseBuf, &bevGrad, &rbarBuf, &gradInterm, &gradLattice, &dose64,
-                      &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals})
+                      &weqBody, &opColPtr, &opBlockOff, &opRows, &opVals, &opNorm, &opVoxels, &colBev, &colFixed,
+                      &colDose})
         b->release();
+    colClean = false;
     hasDose = false;
     doseBoxed = false;
     lastBeamValid = false;
