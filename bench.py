@@ -303,7 +303,7 @@ def _serving(local: int, n_requests: int, slots: int, budget_mib: int) -> dict:
     }
 
 
-def _carbon_plan(local: int, reps: int = 3) -> dict:
+def _carbon_plan(local: int, reps: int = 3, with_dose: bool = False):
     """Carbon-ion plan with the nuclear halo (512x512x200 CT at 1 mm, three beams of
     40 layers 120-400 MeV/u, ~15,000 spots): device time of the whole plan on the
     context stream, median of `reps` after one warm-up."""
@@ -330,10 +330,30 @@ def _carbon_plan(local: int, reps: int = 3) -> dict:
         eng.synchronize()
         if rep:
             ms.append(e0.elapsed_time(e1))
+    dose = eng.read_dose64() if with_dose else None
     eng.close()
-    return {"workload": "carbon + nuclear halo (GAUSS_FIT), CT 512x512x200 at 1 mm, 3 beams (0/120/240 deg) x 40 "
-                        "layers 120-400 MeV/u, 14,520 spots, 9x9 subspots",
-            "ms_per_plan": round(statistics.median(ms), 3), "timing": f"CUDA events, median of {reps}"}
+    out = {"workload": "carbon + nuclear halo (GAUSS_FIT), CT 512x512x200 at 1 mm, 3 beams (0/120/240 deg) x 40 "
+                       "layers 120-400 MeV/u, 14,520 spots, 9x9 subspots",
+           "ms_per_plan": round(statistics.median(ms), 3), "timing": f"CUDA events, median of {reps}"}
+    return (out, dose, case) if with_dose else out
+
+
+def _carbon_precision(case: dict, dose) -> dict:
+    """Error of the carbon plan's dose against the FP64 oracle on the same inputs
+    (halo included), over the box of voxels above 1 % of the oracle's maximum with a
+    two-voxel margin (the gamma's neighbour shifts stay inside it)."""
+    from oracle import oracle as O
+    from subsecondpbs_b200 import precision as prec
+
+    t = time.perf_counter()
+    ref = O.dose(case, beams=case["beams"], nuclear_model=2, threads=os.cpu_count() or 1)["dose"]
+    oracle_s = time.perf_counter() - t
+    nz = np.nonzero(ref > 0.01 * ref.max())
+    box = tuple(slice(max(int(a.min()) - 2, 0), min(int(a.max()) + 3, n)) for a, n in zip(nz, ref.shape))
+    rep = prec.report(dose[box], ref[box], case["dose_resolution"])
+    return dict(rep, reference="FP64 oracle, same inputs, nuclear halo GAUSS_FIT",
+                region=f"voxels above 10 % of Dmax (box {[s.stop - s.start for s in box]} of {list(ref.shape)})",
+                oracle_s=round(oracle_s, 1))
 
 
 def _operator_export(local: int, n_spots: int = 1024, n_face: int = 256) -> dict:
@@ -658,7 +678,12 @@ def run_ours(args):
     adjoint = _adjoint_cost(local) if world == 1 and not args.no_adjoint else None
     served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
               if world == 1 and args.serving_requests > 0 else None)
-    carbon = _carbon_plan(local) if world == 1 and not args.no_adjoint else None
+    carbon = None
+    if world == 1 and not args.no_adjoint:
+        carbon, carbon_dose, carbon_case = _carbon_plan(local, with_dose=True)
+        if not args.no_cpu_baseline:
+            carbon["precision"] = _carbon_precision(carbon_case, carbon_dose)
+        del carbon_dose
     operator = _operator_export(local) if world == 1 and not args.no_adjoint else None
     reference_gpu = _reference_gpu(local, case, e2e_ms) if world == 1 and not args.no_reference_gpu else None
     upstream_conv = (_upstream_cpu_conv(eng, stats, float(case["beam"]["ray_spacing"][0]), stage_ms["conv"])
