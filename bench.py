@@ -386,6 +386,9 @@ def _operator_export(local: int, n_spots: int = 1024, n_face: int = 256) -> dict
             eng._h, C.byref(bd), 0, first, n_spots, 0.0, col_ptr.ctypes.data_as(C.POINTER(C.c_longlong)),
             rows.ctypes.data_as(C.c_void_p), vals.ctypes.data_as(C.c_void_p), cap, C.byref(nnz))
 
+    import torch
+
+    free_gib = torch.cuda.mem_get_info(local)[0] / 2**30
     _lib.check(c_call(0))
     t = time.perf_counter()
     _lib.check(c_call(begin))
@@ -400,6 +403,7 @@ def _operator_export(local: int, n_spots: int = 1024, n_face: int = 256) -> dict
     return {"workload": f"{n_spots} spots of the headline beam (from spot {begin}), threshold 0",
             "ms": round(c_ms, 2), "ms_per_spot": round(c_ms / n_spots, 4), "entries": entries,
             "timing": "wall time of one pbs_context_influence_csc call (C ABI, host arrays) after a warm-up call",
+            "device_free_gib_before": round(free_gib, 1),
             "python_face": {"spots": n_face, "ms": round(f_ms, 2), "ms_per_spot": round(f_ms / n_face, 4),
                             "entries": int(a.nnz), "what": "DoseEngine.influence_csc, scipy CSC matrix included"}}
 

@@ -294,6 +294,8 @@ struct Context {
     // plan with one layer per spot; sink.column(q) receives spot firstSpot + q.
     // Not for the nuclear halo, biological maps or the CarbonPBS profile model.
     int run_column_batch(ColumnPlan& cp, size_t firstSpot, int count, ColumnSink& sink, bool gridZero);
+    int run_column_batches(ColumnPlan& cp, long long spotBegin, long long spotCount, int batch, ColumnSink& sink,
+                           long long& first);
     int influence_csc(const PbsBeamDesc& b, int nuclear, long long spotBegin, long long spotCount, double threshold,
                       long long* colPtr, int* rows, float* vals, long long capacity, long long* nnz);
     int beam_stats(PbsBeamStats* out);

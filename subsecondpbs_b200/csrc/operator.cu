@@ -464,7 +464,8 @@ OpBox dirty_op_box(const Context& c) {
 
 // Spots per batched pass of an influence export (one plan layer and one BEV volume
 // and dose buffer each): at most the layers of one chunk's layer plan, and as many
-// as fit kColumnBudget bytes and half the free device memory.
+// as fit kColumnBudget bytes and a quarter of the device. A pass whose buffers do not
+// fit the free memory is retried with half as many spots (run_column_batches).
 constexpr long long kColumnBudget = 6LL << 30;
 
 int column_batch_size(const Context& c, const BeamPlan& base, ColBox& fb, size_t& maxChunks) {
@@ -475,7 +476,7 @@ int column_batch_size(const Context& c, const BeamPlan& base, ColBox& fb, size_t
     if (c.compatBevZShift) return kMaxColumnsPerBatch;  // one layer at a time through the dose grid
     size_t freeB = 0, totalB = 0;
     long long budget = kColumnBudget;
-    if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess) budget = std::min<long long>(budget, (long long)(freeB / 2));
+    if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess) budget = std::min<long long>(budget, (long long)(totalB / 4));
     const long long k = budget / std::max<long long>((long long)perColumn, 1);
     return static_cast<int>(std::max<long long>(1, std::min<long long>(k, kMaxColumnsPerBatch)));
 }
@@ -694,6 +695,34 @@ int Context::run_column(ColumnPlan& cp, size_t j, int nuclear, void* boxOut, boo
     return PBS_OK;
 }
 
+// Spots [spotBegin, spotBegin + spotCount) in passes of `batch` spots; a pass whose
+// device buffers do not fit is retried with half as many (after its buffers are
+// released and the default memory pool's unused memory is handed back). `first` is
+// set to each pass's first column before the pass.
+int Context::run_column_batches(ColumnPlan& cp, long long spotBegin, long long spotCount, int batch, ColumnSink& sink,
+                                long long& first) {
+    bool gridZero = false;
+    for (long long k0 = 0; k0 < spotCount;) {
+        const int kb = static_cast<int>(std::min<long long>(batch, spotCount - k0));
+        first = k0;
+        const int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, gridZero);
+        if (rc == PBS_ERR_OUT_OF_MEMORY && batch > 1) {
+            cudaGetLastError();
+            for (DevBuf* b : {&colBev, &colFixed, &colDose}) b->release();
+            colClean = false;
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+            batch /= 2;
+            gridZero = false;
+            continue;
+        }
+        if (rc) return rc;
+        gridZero = true;
+        k0 += kb;
+    }
+    return PBS_OK;
+}
+
 int Context::run_column_batch(ColumnPlan& cp, size_t firstSpot, int count, ColumnSink& sink, bool gridZero) {
     if (count <= 0) return PBS_OK;
     const size_t plane = static_cast<size_t>(cp.base.lattice.nx) * cp.base.lattice.ny;
@@ -805,11 +834,8 @@ int Context::influence_row_norms(const PbsBeamDesc& beam, int nuclear, long long
         ColBox fb;
         size_t maxChunks = 0;
         const int batch = column_batch_size(*this, cp.base, fb, maxChunks);
-        for (long long k0 = 0; k0 < spotCount; k0 += batch) {
-            const int kb = static_cast<int>(std::min<long long>(batch, spotCount - k0));
-            if (int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, k0 > 0))
-                return fail(rc);
-        }
+        long long first = 0;
+        if (int rc = run_column_batches(cp, spotBegin, spotCount, batch, sink, first)) return fail(rc);
     } else {
         for (long long k = 0; k < spotCount; ++k) {
             OpBox a{};
@@ -947,12 +973,7 @@ int Context::influence_csc(const PbsBeamDesc& beam, int nuclear, long long spotB
         sink.vals = dVals;
         sink.cap = capacity;
         sink.colPtr = dColPtr;
-        for (long long k0 = 0; k0 < spotCount; k0 += batch) {
-            const int kb = static_cast<int>(std::min<long long>(batch, spotCount - k0));
-            sink.first = k0;
-            if (int rc = run_column_batch(cp, static_cast<size_t>(spotBegin + k0), kb, sink, k0 > 0))
-                return fail(rc);
-        }
+        if (int rc = run_column_batches(cp, spotBegin, spotCount, batch, sink, sink.first)) return fail(rc);
     } else {
         for (long long k = 0; k < spotCount; ++k) {
             OpBox a{};
