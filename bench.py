@@ -668,16 +668,7 @@ def run_ours(args):
     launches_per_step = int(stats["kernel_launches"]) + 2  # + dose reset and float readout
     cpu = None
     precision = None
-    if world == 1 and not args.no_cpu_baseline:
-        cms, threads, runs, ref_dose = _cpu_oracle_ms(case)
-        cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "port",
-               "sample": f"full workload (one 20-layer beam) x {runs} runs, OpenMP over rays and steps"}
-        # Error of the benchmarked result against the FP64 oracle on the same inputs.
-        from subsecondpbs_b200 import precision as prec
-
-        precision = dict(prec.report(out.cpu().numpy(), ref_dose, case["dose_resolution"]),
-                         reference="FP64 oracle, same inputs", arithmetic="FP32 rays/superposition, "
-                         "int32 fixed-point tile footprints, Kahan WEPL, FP64 dose accumulation")
+    bench_dose = out.cpu().numpy() if world == 1 and not args.no_cpu_baseline else None
 
     adjoint = _adjoint_cost(local) if world == 1 and not args.no_adjoint else None
     served = (_serving(local, args.serving_requests, args.serving_slots, args.serving_budget_mib)
@@ -689,7 +680,18 @@ def run_ours(args):
     reference_gpu = _reference_gpu(local, case, e2e_ms) if world == 1 and not args.no_reference_gpu else None
     upstream_conv = (_upstream_cpu_conv(eng, stats, float(case["beam"]["ray_spacing"][0]), stage_ms["conv"])
                      if world == 1 and not args.no_cpu_baseline else None)
-    # The oracle check of the carbon plan runs on every host core: after the timed legs.
+    # The CPU legs run the oracle on every host core: after the timed GPU legs, whose
+    # host work they would otherwise share the cores with.
+    if bench_dose is not None:
+        cms, threads, runs, ref_dose = _cpu_oracle_ms(case)
+        cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "port",
+               "sample": f"full workload (one 20-layer beam) x {runs} runs, OpenMP over rays and steps"}
+        # Error of the benchmarked result against the FP64 oracle on the same inputs.
+        from subsecondpbs_b200 import precision as prec
+
+        precision = dict(prec.report(bench_dose, ref_dose, case["dose_resolution"]),
+                         reference="FP64 oracle, same inputs", arithmetic="FP32 rays/superposition, "
+                         "int32 fixed-point tile footprints, Kahan WEPL, FP64 dose accumulation")
     if carbon is not None and not args.no_cpu_baseline:
         carbon["precision"] = _carbon_precision(carbon_case, carbon_dose)
     del carbon_dose, carbon_case
