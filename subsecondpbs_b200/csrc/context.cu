@@ -438,6 +438,7 @@ int Context::reset_dose_region(const float* init, const int lo[3], const int hi[
         deferredHi[i] = hi[i];
     }
     pendingDoseInit = true;
+    initBoxed = true;
     return PBS_OK;
 }
 
@@ -581,6 +582,7 @@ int Context::reset_dose(const float* init, int onDevice) {
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
     if (int rc = join_side_work()) return rc;
     deferredInit = nullptr;  // superseded
+    initBoxed = false;
     if (init && !onDevice) {
         // The copy waits for the work already on the context stream (the CT upload
         // among it, which the next beam needs first) and then overlaps that beam.
@@ -652,9 +654,18 @@ int Context::flush_dose_init() {
     if (int rc = issue_dose_copy()) return rc;
     const size_t n = size_t(doseGrid.dims[0]) * doseGrid.dims[1] * doseGrid.dims[2];
     PBS_CUDA(cudaStreamWaitEvent(stream, doseCopied, 0), "cudaStreamWaitEvent");
-    PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), static_cast<const float*>(floatOut.ptr), n, stream),
-             "dose_init");
+    if (initBoxed) {
+        // Only the uploaded box: the voxels outside it are neither written by the
+        // call's beams nor copied back (reset_dose_region).
+        PBS_CUDA(launch_dose_box_init(static_cast<double*>(dose64.ptr), static_cast<const float*>(floatOut.ptr),
+                                      doseGrid.dims, deferredLo, deferredHi, stream),
+                 "dose_init");
+    } else {
+        PBS_CUDA(launch_dose_init(static_cast<double*>(dose64.ptr), static_cast<const float*>(floatOut.ptr), n, stream),
+                 "dose_init");
+    }
     pendingDoseInit = false;
+    initBoxed = false;
     return PBS_OK;
 }
 

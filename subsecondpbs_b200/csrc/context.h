@@ -94,6 +94,8 @@ struct Context {
     // the copy engine; the caller's buffer outlives the wrapper call.
     const float* deferredInit = nullptr;
     int deferredLo[3] = {0, 0, 0}, deferredHi[3] = {-1, -1, -1};
+    // The pending initialisation covers the deferred box only (reset_dose_region).
+    bool initBoxed = false;
     int issue_dose_copy();
     // While doseBoxed is set, the FP64 grid is exactly zero outside the inclusive
     // voxel box [dirtyLo, dirtyHi]: the union of the transfer boxes of the beams

@@ -150,6 +150,9 @@ cudaError_t launch_dose_init(double* dose, const float* init, size_t n, cudaStre
 cudaError_t launch_dose_to_float(const double* dose, float* out, size_t n, cudaStream_t s);
 // Inclusive voxel box [lo, hi] of the dose grid: zeroes the FP64 dose there when
 // `out` is null, else writes float(dose) to the same voxels of `out`.
+// Inclusive box [lo, hi] of the FP64 grid initialised from the float grid `init`.
+cudaError_t launch_dose_box_init(double* dose, const float* init, const int dims[3], const int lo[3], const int hi[3],
+                                 cudaStream_t s);
 cudaError_t launch_dose_box(double* dose, float* out, const int dims[3], const int lo[3], const int hi[3],
                             cudaStream_t s);
 

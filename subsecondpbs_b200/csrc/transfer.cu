@@ -280,7 +280,33 @@ __global__ void __launch_bounds__(256) column_bev_clear_kernel(BeamGeomDev g, fl
     }
 }
 
+// Box [lo, lo + ext) of the FP64 grid initialised from the same voxels of a float grid.
+__global__ void dose_box_init_kernel(double* dose, const float* init, int3 dims, int3 lo, int3 ext) {
+    const size_t total = size_t(ext.x) * ext.y * ext.z;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % size_t(ext.x));
+        const size_t r = i / size_t(ext.x);
+        const int y = int(r % size_t(ext.y));
+        const int z = int(r / size_t(ext.y));
+        const size_t v = (size_t(z + lo.z) * dims.y + (y + lo.y)) * size_t(dims.x) + (x + lo.x);
+        dose[v] = double(init[v]);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_dose_box_init(double* dose, const float* init, const int dims[3], const int lo[3], const int hi[3],
+                                 cudaStream_t s) {
+    for (int i = 0; i < 3; ++i)
+        if (lo[i] < 0 || hi[i] >= dims[i] || hi[i] < lo[i]) return cudaErrorInvalidValue;
+    const int3 d = make_int3(dims[0], dims[1], dims[2]);
+    const int3 l = make_int3(lo[0], lo[1], lo[2]);
+    const int3 e = make_int3(hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1);
+    const size_t total = size_t(e.x) * e.y * e.z;
+    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 32));
+    dose_box_init_kernel<<<blocks, 256, 0, s>>>(dose, init, d, l, e);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_column_transfer(const BeamGeomDev& g, const float* bev, size_t bevStride, BeamStateDev* beam,
                                    LayerStateDev* ls, int nCols, const ColBox& fb, double* colDose, cudaStream_t s) {
