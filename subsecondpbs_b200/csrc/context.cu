@@ -398,7 +398,12 @@ int Context::set_ct_region(const float* data, const GridDesc& g, const int lo[3]
         sample_ct_stats(data, n, mn, mx);
         type = auto_detect_ct_type(mn, mx);
     }
-    if ((rc = convert_ct(type, g))) return rc;
+    // Only the uploaded box is converted: the tracers sample nothing outside it.
+    if (!box_empty(lo, hi) && (rc = convert_ct_buffer(static_cast<float*>(ct.ptr), n, type, g.dims, lo, hi)))
+        return rc;
+    ctType = type;
+    ctGrid = g;
+    hasCt = true;
     return build_ct_quad_box(lo, hi);
 }
 
@@ -532,7 +537,7 @@ int Context::convert_ct(int type, const GridDesc& g) {
     return PBS_OK;
 }
 
-int Context::convert_ct_buffer(float* data, size_t n, int type) {
+int Context::convert_ct_buffer(float* data, size_t n, int type, const int* dims, const int* lo, const int* hi) {
     if (type == PBS_CT_DENSITY || type == PBS_CT_SPR) {
         if (!hasEnergy) {
             set_error("[CT_ADAPTER] density/SPR CT needs the lookup tables; call set_energy first");
@@ -545,11 +550,14 @@ int Context::convert_ct_buffer(float* data, size_t n, int type) {
             set_error("[CT_ADAPTER] LUT is empty or scale factor is 0; cannot convert");
             return PBS_ERR_INVALID_ARGUMENT;
         }
-        PBS_CUDA(launch_ct_convert(data, n, type, static_cast<const float*>(useDensity ? density.ptr : sp.ptr), lutN,
-                                   scale, stream),
+        const float* lut = static_cast<const float*>(useDensity ? density.ptr : sp.ptr);
+        PBS_CUDA(dims ? launch_ct_convert_box(data, dims, lo, hi, type, lut, lutN, scale, stream)
+                      : launch_ct_convert(data, n, type, lut, lutN, scale, stream),
                  "ct_convert");
     } else {
-        PBS_CUDA(launch_ct_convert(data, n, type, nullptr, 0, 1.0f, stream), "ct_convert");
+        PBS_CUDA(dims ? launch_ct_convert_box(data, dims, lo, hi, type, nullptr, 0, 1.0f, stream)
+                      : launch_ct_convert(data, n, type, nullptr, 0, 1.0f, stream),
+                 "ct_convert");
     }
     return PBS_OK;
 }

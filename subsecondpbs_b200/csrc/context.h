@@ -223,7 +223,9 @@ struct Context {
     int read_dose_region(float* out, const int lo[3], const int hi[3]);
     int convert_ct(int type, const GridDesc& g);
     // HU+1000 conversion of `n` device floats in place, on the context stream.
-    int convert_ct_buffer(float* data, size_t n, int type);
+    // With dims, only the inclusive box [lo, hi] of the [dims.z][dims.y][dims.x] CT.
+    int convert_ct_buffer(float* data, size_t n, int type, const int* dims = nullptr, const int* lo = nullptr,
+                          const int* hi = nullptr);
     // Per-beam buffers and the dose grid are allocated in stream order from here on.
     void use_stream_ordered_allocation();
     int set_dose_grid(const GridDesc& g);

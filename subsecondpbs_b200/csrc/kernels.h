@@ -12,6 +12,9 @@ namespace pbs {
 // Convert a float CT to HU+1000 in place according to `type` (PBS_CT_*).
 cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, int lutN, float lutScale,
                               cudaStream_t s);
+// The same conversion over the inclusive box [lo, hi] of a [dims.z][dims.y][dims.x] CT.
+cudaError_t launch_ct_convert_box(float* ct, const int dims[3], const int lo[3], const int hi[3], int type,
+                                  const float* lut, int lutN, float lutScale, cudaStream_t s);
 // min/max of a strided sample (the reference's ~100k-sample statistics).
 cudaError_t launch_ct_stats(const float* ct, size_t n, float* minmax2, cudaStream_t s);
 // The reference's ~100k-sample type detection and the conversion in one pass on

@@ -3,6 +3,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "device_util.cuh"
 #include "kernels.h"
@@ -490,14 +491,20 @@ __device__ __forceinline__ int ct_type_from_range(float mn, float mx) {
 
 // With `rangeKeys` (order keys of the sample minimum and maximum, from
 // ct_sample_range_kernel) the type is detected here; `lut` is then the density
-// table, the only one detection can call for.
-__global__ void ct_convert_kernel(float* ct, size_t n, int type, const float* __restrict__ lut, int lutN,
-                                  float lutScale, const unsigned* __restrict__ rangeKeys) {
+// table, the only one detection can call for. The voxels converted are the box
+// [lo, lo + ext) of the [dims.z][dims.y][dims.x] grid.
+__global__ void ct_convert_kernel(float* ct, int3 dims, int3 lo, int3 ext, int type, const float* __restrict__ lut,
+                                  int lutN, float lutScale, const unsigned* __restrict__ rangeKeys) {
     if (rangeKeys) {
         type = ct_type_from_range(float_from_order_key(rangeKeys[0]), float_from_order_key(rangeKeys[1]));
         if (type == PBS_CT_HU_PLUS_1000) return;
     }
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    const size_t total = size_t(ext.x) * ext.y * ext.z;
+    for (size_t b = blockIdx.x * size_t(blockDim.x) + threadIdx.x; b < total; b += size_t(gridDim.x) * blockDim.x) {
+        const size_t r = b / size_t(ext.x);
+        const size_t i = (size_t(int(r / size_t(ext.y)) + lo.z) * dims.y + (int(r % size_t(ext.y)) + lo.y)) *
+                             size_t(dims.x) +
+                         (int(b % size_t(ext.x)) + lo.x);
         const float v = ct[i];
         if (type == PBS_CT_HU) {
             ct[i] = v + 1000.0f;
@@ -600,8 +607,25 @@ __global__ void ct_stats_kernel(const float* __restrict__ ct, size_t n, size_t s
 cudaError_t launch_ct_convert(float* ct, size_t n, int type, const float* lut, int lutN, float lutScale,
                               cudaStream_t s) {
     if (type == PBS_CT_HU_PLUS_1000 || n == 0) return cudaSuccess;
+    // A flat buffer as one row of n voxels (n fits an int for every CT this takes).
+    if (n > size_t(INT_MAX)) return cudaErrorInvalidValue;
+    const int3 d = make_int3(int(n), 1, 1);
     const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
-    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, type, lut, lutN, lutScale, nullptr);
+    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, d, make_int3(0, 0, 0), d, type, lut, lutN, lutScale, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ct_convert_box(float* ct, const int dims[3], const int lo[3], const int hi[3], int type,
+                                  const float* lut, int lutN, float lutScale, cudaStream_t s) {
+    if (type == PBS_CT_HU_PLUS_1000) return cudaSuccess;
+    for (int i = 0; i < 3; ++i)
+        if (lo[i] < 0 || hi[i] >= dims[i] || hi[i] < lo[i]) return cudaErrorInvalidValue;
+    const int3 d = make_int3(dims[0], dims[1], dims[2]);
+    const int3 e = make_int3(hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1);
+    const size_t total = size_t(e.x) * e.y * e.z;
+    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 16));
+    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, d, make_int3(lo[0], lo[1], lo[2]), e, type, lut, lutN, lutScale,
+                                             nullptr);
     return cudaGetLastError();
 }
 
@@ -626,8 +650,12 @@ cudaError_t launch_ct_convert_detect(float* ct, size_t n, const float* hostCtMap
     for (int pass = 0; pass < 2; ++pass)
         ct_sample_range_kernel<<<unsigned((samples + 255) / 256), 256, 0, s>>>(hostCtMapped, ct, d, lo, hi, stride,
                                                                                samples, keys, pass);
-    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
-    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, n, PBS_CT_AUTO, densityLut, lutN, lutScale, keys);
+    // Only the uploaded box is converted: the tracers sample nothing outside it.
+    const int3 ext = make_int3(hi.x - lo.x + 1, hi.y - lo.y + 1, hi.z - lo.z + 1);
+    if (ext.x <= 0 || ext.y <= 0 || ext.z <= 0) return cudaGetLastError();
+    const size_t total = size_t(ext.x) * ext.y * ext.z;
+    const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 16));
+    ct_convert_kernel<<<blocks, 256, 0, s>>>(ct, d, lo, ext, PBS_CT_AUTO, densityLut, lutN, lutScale, keys);
     return cudaGetLastError();
 }
 
