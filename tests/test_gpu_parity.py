@@ -185,3 +185,33 @@ def test_stage_timers_and_stats(hetero_small_case):
     assert set(t) == set(L.STAGES) and all(v >= 0 for v in t.values())
     st = eng.beam_stats()
     assert st["live_tiles"] > 0 and st["superpose_fma"] > 0
+
+
+def test_headline_dose_is_linear_in_the_spot_weights(hetero_case):
+    """At the full headline size: the dose of w equals the sum of the doses of a
+    split of w (0.3 w + 0.7 w) and scales with a power-of-two factor of w, to 1e-5
+    of Dmax (the live-ray mask, ray weight < 1e-6, can drop a few rays near the
+    threshold in a part; the fixed-point BEV rounds each run at its own scale)."""
+    from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
+
+    c = hetero_case
+    eng = DoseEngine(0)
+    eng.set_energy(c["energy"])
+    eng.set_ct(c["ct"], c["ct_dims"], c["ct_resolution"], c["ct_corner"])
+    eng.set_dose_grid(c["dose_dims"], c["dose_resolution"], c["dose_corner"])
+    w = np.asarray(c["beam"]["spot_weights"], np.float32)
+
+    def dose(weights):
+        b = dict(c["beam"])
+        b["spot_weights"] = np.asarray(weights, np.float32)
+        eng.reset_dose()
+        eng.add_beam(b)
+        return eng.read_dose64()
+
+    full = dose(w)
+    dmax = full.max()
+    assert dmax > 0
+    parts = dose(0.3 * w) + dose(0.7 * w)
+    assert np.abs(parts - full).max() <= 1e-5 * dmax
+    assert np.abs(dose(4.0 * w) - 4.0 * full).max() <= 1e-5 * 4.0 * dmax
+    eng.close()
