@@ -189,9 +189,11 @@ def test_stage_timers_and_stats(hetero_small_case):
 
 def test_headline_dose_is_linear_in_the_spot_weights(hetero_case):
     """At the full headline size: the dose of w equals the sum of the doses of a
-    split of w (0.3 w + 0.7 w) and scales with a power-of-two factor of w, to 1e-5
-    of Dmax (the live-ray mask, ray weight < 1e-6, can drop a few rays near the
-    threshold in a part; the fixed-point BEV rounds each run at its own scale)."""
+    split of w (0.3 w + 0.7 w) and scales with a power-of-two factor of w, to 5e-5
+    of Dmax. The bound is the reference's live-ray mask: a ray weight below the
+    absolute 1e-6 (idd_sigma.cu:78) stops the ray, so 0.3 w drops the rays whose
+    weight under w lies in [1e-6, 3.3e-6) (measured 1.2e-5 of Dmax), and 4 w adds
+    those in [2.5e-7, 1e-6). The fixed-point BEV rounds each run at its own scale."""
     from subsecondpbs_b200.cudaCalDoseRTD import DoseEngine
 
     c = hetero_case
@@ -212,6 +214,6 @@ def test_headline_dose_is_linear_in_the_spot_weights(hetero_case):
     dmax = full.max()
     assert dmax > 0
     parts = dose(0.3 * w) + dose(0.7 * w)
-    assert np.abs(parts - full).max() <= 1e-5 * dmax
-    assert np.abs(dose(4.0 * w) - 4.0 * full).max() <= 1e-5 * 4.0 * dmax
+    assert np.abs(parts - full).max() <= 5e-5 * dmax
+    assert np.abs(dose(4.0 * w) - 4.0 * full).max() <= 5e-5 * 4.0 * dmax
     eng.close()
