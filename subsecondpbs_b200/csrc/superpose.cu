@@ -132,27 +132,41 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
     const int t = threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
 
+    // Up to radius 7 a warp holds at most one (column, |d|) unit, whose column sums stay
+    // in registers over the item's layers and are flushed once.
+    constexpr bool kOneFlush = kUnits <= kWarps;
+
     // H and Wo are even and `out` is 16-byte aligned.
     for (int i = t; i < H * Wo / 4; i += kThreads) reinterpret_cast<int4*>(out)[i] = make_int4(0, 0, 0, 0);
-    // Fixed-point scale from the dose of every layer of the item.
-    {
-        float rowDose = 0.0f;
+    // Fixed-point scale from the dose of every layer of the item: each thread sums its
+    // source over the layers, then the warps and the CTA add up. With one flush per
+    // item the sums run in the table phases and the scale is applied at the flush;
+    // with a flush per layer they run first and the scale is folded into the weights.
+    // Either way the total (the same additions in the same order) and the flushed
+    // values are the same.
+    float rowDose = 0.0f;
+    int sc = 0;
+    float scale = 1.0f;
+    auto item_scale = [&]() {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
+        if (lane == 0) sSum[warp] = rowDose;
+        __syncthreads();
+        float total = 0.0f;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) total += sSum[w];
+        sc = footprint_exponent(total);
+        scale = ldexpf(1.0f, sc);
+    };
+    if constexpr (!kOneFlush) {
 #pragma unroll 1
         for (int j = 0; j < kMergeLayers; ++j) {
             const unsigned lc = (a.layers >> (8 * j)) & 0xffu;
             if (lc == 0xffu) break;
             rowDose += fmaxf(a.idd[lc * a.layerStride + a.src], 0.0f);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) rowDose += __shfl_xor_sync(0xffffffffu, rowDose, o);
-        if (lane == 0) sSum[warp] = rowDose;
+        item_scale();
     }
-    __syncthreads();
-    float total = 0.0f;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) total += sSum[w];
-    const int sc = footprint_exponent(total);
-    const float scale = ldexpf(1.0f, sc);
 
     // Table phase of one layer (complete_superposition.cu:298-307): thread t is source
     // (sy, sx) = (warp, lane); its rows e_s(0..R) go in float4 chunks (chunk-major)
@@ -163,13 +177,14 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
     auto table = [&](unsigned lc, unsigned* colMask) {
         const size_t src = lc * a.layerStride + a.src;
         const float dose = a.idd[src];
+        if constexpr (kOneFlush) rowDose += fmaxf(dose, 0.0f);
         const bool live = dose > 0.0f;
         if (live) atomicOr(&colMask[lane], 1u << warp);
         float e[4 * Q];
         if (live) {
             float row[R + 1];
             superposition_row<R>(a.rsig[src], row);
-            const float doseScaled = dose * scale;
+            const float doseScaled = kOneFlush ? dose : dose * scale;
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 e[k] = row[k];
@@ -219,7 +234,7 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
     auto flush = [&](int sx, int d, const float (&acc)[H]) {
         int qv[H];
 #pragma unroll
-        for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(acc[i]);
+        for (int i = 0; i < H; ++i) qv[i] = __float2int_rn(kOneFlush ? acc[i] * scale : acc[i]);
         int* col = out + sx + R + d;
 #pragma unroll
         for (int i = 0; i < H; ++i) atomicAdd(col + i * Wo, qv[i]);
@@ -230,7 +245,7 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
         }
     };
 
-    if constexpr (kUnits <= kWarps) {
+    if constexpr (kOneFlush) {
         // One pair unit per warp: its column sums stay in registers over all the
         // item's layers and are flushed once. The column masks OR over the layers.
         const int g = lane / M;
@@ -258,6 +273,7 @@ __device__ __forceinline__ void pair_item(float4* __restrict__ E4, float* __rest
             // The next layer's tables overwrite these.
             __syncthreads();
         }
+        item_scale();
         const unsigned colAll = __shfl_sync(0xffffffffu, sCol[lane], sx);
         const unsigned colLive = valid ? colAll : 0u;
         if (colLive) flush(sx, d, acc);
