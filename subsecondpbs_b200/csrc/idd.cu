@@ -386,7 +386,6 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
                   const BeamStateDev* __restrict__ primaryBeam) {
     __shared__ int sLive[kMaxChunkLayers][kMaxR + 1];   // live items per layer and batched radius
     __shared__ int sCalc[kMaxChunkLayers];
-    __shared__ unsigned sIddBits[kMaxChunkLayers];
     __shared__ int sWarpSum[kMaxChunkLayers / 32];
     __shared__ long long sWarpFma[kMaxChunkLayers / 32];
     __shared__ int sSplit[2];
@@ -452,7 +451,6 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         }
         st.liveTiles = live;
         sCalc[lc] = st.calcPassive;
-        sIddBits[lc] = st.maxIddBits;
     }
     __syncthreads();
 
@@ -525,7 +523,7 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         // largest IDD of the chunk, so with that IDD below 2^ex every cell stays below
         // 2^(ex + 8 + ceil(log2 acc)); the shift puts that bound at 2^61.
         unsigned mb = 0;
-        for (int q = 0; q < nLayers; ++q) mb = max(mb, sIddBits[q]);
+        for (int q = 0; q < nLayers; ++q) mb = max(mb, ls[layer0 + q].maxIddBits);
         int ex = 0;
         frexpf(__uint_as_float(mb), &ex);
         int lg = 0;
