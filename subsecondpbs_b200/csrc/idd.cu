@@ -396,21 +396,30 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     if (lc < 2) sSplit[lc] = 0;
     if (lc < nLayers) {
         LayerStateDev& st = ls[layer0 + lc];
-        int hist[kBuckets];
-        for (int i = 0; i < kBuckets; ++i) hist[i] = st.histAll[i];
+        // Every input of the layer is read before its outputs are written: the outputs
+        // go to the same struct through indexed stores, so a load placed after them
+        // would wait for them to complete.
+        int hist[kBuckets], liveHist[kBuckets];
+        for (int i = 0; i < kBuckets; ++i) {
+            hist[i] = st.histAll[i];
+            liveHist[i] = st.liveHist[i];
+        }
+        const int afterLast = st.afterLast;
+        const int maxFirstPassive = st.maxFirstPassive;
+        int calc;
         if (nuclear) {
-            const int calc = primaryLs[layer0 + lc].calcPassive;
+            calc = primaryLs[layer0 + lc].calcPassive;
             st.afterLast = calc;
             st.calcPassive = calc;
             if (hist[kMaxR + 1] > 0) atomicOr(&beam->errorFlags, 4);
         } else {
-            int calc = st.maxFirstPassive;
+            calc = maxFirstPassive;
             if (calc < first + 1) calc = first + 1;
             if (calc < 0) calc = first + 1;
-            if (calc > st.afterLast) calc = st.afterLast;
+            if (calc > afterLast) calc = afterLast;
             if (calc > g.steps) calc = g.steps;
             st.calcPassive = calc;
-            if (st.afterLast > calc && st.afterLast > first) hist[0] -= (st.afterLast - max(calc, first)) * tiles;
+            if (afterLast > calc && afterLast > first) hist[0] -= (afterLast - max(calc, first)) * tiles;
         }
         for (int i = 0; i < kBuckets; ++i) st.hist[i] = hist[i];
         if (hist[kMaxR + 1] > 0) {
@@ -442,15 +451,15 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
         for (int i = 0; i <= kMaxR; ++i) liveR[i] = 0;
         for (int b = 0; b < kBuckets; ++b) {
             st.batchedR[b] = map[b];
-            liveR[map[b]] += st.liveHist[b];
-            live += st.liveHist[b];
+            liveR[map[b]] += liveHist[b];
+            live += liveHist[b];
         }
         for (int i = 0; i <= kMaxR; ++i) {
             st.liveR[i] = liveR[i];
             sLive[lc][i] = liveR[i];
         }
         st.liveTiles = live;
-        sCalc[lc] = st.calcPassive;
+        sCalc[lc] = calc;
     }
     __syncthreads();
 
