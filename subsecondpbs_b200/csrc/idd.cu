@@ -602,12 +602,13 @@ __global__ void work_scatter_kernel(BeamGeomDev g, int layer0, int nLayers, cons
     }
 }
 
-// Appends a merged item to the block of its radius. Merging only joins items of one
+// Appends a merged item to the block of its radius, [blockStart[R], blockStart[R - 1])
+// (R = 0: up to blockStart[kMaxR + 1], the item count). Merging only joins items of one
 // radius, so the merged items of R fit in the block its unmerged items occupy.
-__device__ __forceinline__ void emit_merged(BeamStateDev* beam, int4* work, unsigned layers, int tile, int zr,
-                                            int R) {
-    const int begin = beam->rStart[R];
-    const int end = R > 0 ? beam->rStart[R - 1] : beam->workCount;
+__device__ __forceinline__ void emit_merged(BeamStateDev* beam, const int* blockStart, int4* work, unsigned layers,
+                                            int tile, int zr, int R) {
+    const int begin = blockStart[R];
+    const int end = R > 0 ? blockStart[R - 1] : blockStart[kMaxR + 1];
     const int slot = begin + atomicAdd(&beam->mergedR[R], 1);
     if (slot < end) work[slot] = make_int4(static_cast<int>(layers), tile, zr, R);
 }
@@ -624,9 +625,14 @@ __device__ __forceinline__ void emit_merged(BeamStateDev* beam, int4* work, unsi
 __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const uint8_t* __restrict__ codes,
                                   const LayerStateDev* __restrict__ ls, BeamStateDev* __restrict__ beam,
                                   int4* __restrict__ work) {
-    // The block's extent of the cells its items write (min x, y, z; max x, y, z).
+    // The block's extent of the cells its items write (min x, y, z; max x, y, z), and
+    // the radius blocks of the list (read once: the claims below are atomics on the
+    // same beam state, which later reads of it would wait behind).
     __shared__ int sExt[6];
+    __shared__ int sStart[kMaxR + 2];
     if (threadIdx.x < 6) sExt[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    if (threadIdx.x <= kMaxR) sStart[threadIdx.x] = beam->rStart[threadIdx.x];
+    if (threadIdx.x == kMaxR + 1) sStart[kMaxR + 1] = beam->workCount;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int tiles = g.tilesX * g.tilesY;
@@ -648,7 +654,7 @@ __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const 
             rMax = max(rMax, R);
             const bool merge = R >= 0 && R <= kSplitR;
             const unsigned mergeLanes = __ballot_sync(0xffffffffu, merge);
-            if (R > kSplitR) emit_merged(beam, work, 0xffffff00u | unsigned(lc), tile, zr, R);
+            if (R > kSplitR) emit_merged(beam, sStart, work, 0xffffff00u | unsigned(lc), tile, zr, R);
             if (merge) {
                 // Lanes with this radius; every kMergeLayers-th of them (in lane
                 // order) writes the item of itself and the next ones.
@@ -663,7 +669,7 @@ __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const 
                         rest &= rest - 1u;
                         layers = (layers & ~(0xffu << (8 * n))) | (unsigned(base + l) << (8 * n));
                     }
-                    emit_merged(beam, work, layers, tile, zr, R);
+                    emit_merged(beam, sStart, work, layers, tile, zr, R);
                 }
             }
         }
