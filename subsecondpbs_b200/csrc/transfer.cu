@@ -111,10 +111,20 @@ __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const
     if (g.errWord && beam->errorFlags) atomicOr(g.errWord, beam->errorFlags);
     const int first = beam->firstInside;
     const int passive = layer ? layer->calcPassive : beam->maxCalcPassive;
+    // The live box is read before any field of the beam state is written.
+    int lo[3], hi[3], start[3], maxi[3];
+    for (int i = 0; i < 3; ++i) {
+        lo[i] = beam->liveLo[i];
+        hi[i] = beam->liveHi[i];
+    }
+    const int valid = plan_transfer_box(g, first, passive, live != 0, lo, hi, start, maxi);
     const ToFan t = invert_and_shift(g.rayIdxToDoseIdx, v3(float(kMaxR), float(kMaxR), -float(first)));
     beam->transfer = make_transfer_params(t);
-    beam->transferValid = plan_transfer_box(g, first, passive, live != 0, beam->liveLo, beam->liveHi,
-                                            beam->transferStart, beam->transferMax);
+    for (int i = 0; i < 3; ++i) {
+        beam->transferStart[i] = start[i];
+        beam->transferMax[i] = maxi[i];
+    }
+    beam->transferValid = valid;
 }
 
 // Batched influence columns: every layer of the chunk [layer0, layer0 + nCols) gets
