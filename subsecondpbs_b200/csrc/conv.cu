@@ -3,7 +3,9 @@
 //     x pass then y pass, all layers in one launch each.
 //   Mode B (legacy CPB): subspot Gaussians integrated over CPB cells, then the
 //     CPB -> ray area-overlap map.
+#include "device_util.cuh"
 #include "kernels.h"
+#include "launch_util.h"
 
 namespace pbs {
 
@@ -15,6 +17,7 @@ constexpr int kMaxGatherTaps = 1 << 16;   // bound on the gather loop
 // xConvGathResampGpu (src/algorithms/convolution.cu:198-228): interm[l][iy][x].
 __global__ void conv_x_kernel(BeamGeomDev g, const float* __restrict__ lattice, float* __restrict__ interm,
                               const LayerStateDev* __restrict__ ls, const BeamStateDev* __restrict__ beam) {
+    pdl_trigger();
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int l = blockIdx.z;
@@ -43,6 +46,7 @@ __global__ void conv_x_kernel(BeamGeomDev g, const float* __restrict__ lattice, 
 // yConvGathResampGpu (src/algorithms/convolution.cu:231-262): rayW[l][y][x].
 __global__ void conv_y_kernel(BeamGeomDev g, const float* __restrict__ interm, float* __restrict__ rayW,
                               const LayerStateDev* __restrict__ ls, const BeamStateDev* __restrict__ beam) {
+    pdl_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int l = blockIdx.z;
@@ -223,7 +227,8 @@ cudaError_t launch_conv_lattice(const BeamGeomDev& g, const float* lattice, floa
     dim3 gx((g.rayX + 31) / 32, (g.latNy + 7) / 8, g.numLayers);
     conv_x_kernel<<<gx, block, 0, s>>>(g, lattice, interm, ls, beam);
     dim3 gy((g.rayX + 31) / 32, (g.rayY + 7) / 8, g.numLayers);
-    conv_y_kernel<<<gy, block, 0, s>>>(g, interm, rayW, ls, beam);
+    cudaError_t e = launch_pdl(conv_y_kernel, gy, block, 0, s, g, static_cast<const float*>(interm), rayW, ls, beam);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -5,6 +5,12 @@
 
 namespace pbs {
 
+// Programmatic dependent launch: a kernel launched with launch_pdl calls pdl_wait()
+// first (its predecessor on the stream has completed and its writes are visible); a
+// kernel that may precede one calls pdl_trigger() to let it be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // tex1D with linear filtering, clamp addressing and unnormalised coordinates
 // (texel i centred at i + 0.5), evaluated with full-precision weights. The texel
 // coordinate is clamped to [0, n - 1] before the split into index and weight: below

@@ -389,6 +389,7 @@ layer_plan_kernel(BeamGeomDev g, int layer0, int nLayers, LayerStateDev* __restr
     __shared__ int sWarpSum[kMaxChunkLayers / 32];
     __shared__ long long sWarpFma[kMaxChunkLayers / 32];
     __shared__ int sSplit[2];
+    pdl_trigger();
     const int lc = threadIdx.x;
     const bool nuclear = primaryLs != nullptr;
     const int first = nuclear ? primaryBeam->firstInside : beam->firstInside;
@@ -630,6 +631,7 @@ __global__ void work_merge_kernel(BeamGeomDev g, int layer0, int nLayers, const 
     // same beam state, which later reads of it would wait behind).
     __shared__ int sExt[6];
     __shared__ int sStart[kMaxR + 2];
+    pdl_wait();
     if (threadIdx.x < 6) sExt[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     if (threadIdx.x <= kMaxR) sStart[threadIdx.x] = beam->rStart[threadIdx.x];
     if (threadIdx.x == kMaxR + 1) sStart[kMaxR + 1] = beam->workCount;
@@ -794,7 +796,9 @@ cudaError_t launch_bin_plan(const BeamGeomDev& g, int layer0, int nLayers, const
     if (merged) {
         const size_t warps = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY;
         const int blocks = int(std::min<size_t>((warps + 7) / 8, 148 * 16));
-        work_merge_kernel<<<blocks, 256, 0, s>>>(g, layer0, nLayers, codes, ls, beam, work);
+        cudaError_t e = launch_pdl(work_merge_kernel, dim3(blocks), dim3(256), 0, s, g, layer0, nLayers, codes,
+                                   static_cast<const LayerStateDev*>(ls), beam, work);
+        if (e != cudaSuccess) return e;
     } else {
         const size_t total = static_cast<size_t>(g.steps) * g.tilesX * g.tilesY * nLayers;
         const int blocks = int(std::min<size_t>((total + 255) / 256, 148 * 8));

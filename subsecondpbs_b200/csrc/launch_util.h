@@ -25,4 +25,23 @@ inline cudaError_t set_smem_limit(const void* func, size_t bytes) {
     return e;
 }
 
+// Launches `k` as a programmatic dependent of the previous kernel on `s`: it may be
+// scheduled while that kernel's last CTAs run. Every kernel launched this way waits
+// for its predecessor (pdl_wait) before it reads or writes anything, so the order of
+// the stream is kept; only the launch latency overlaps.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 }  // namespace pbs

@@ -578,6 +578,7 @@ cudaError_t launch_range(const BeamGeomDev& g, const float* idd, const float* rs
 __global__ void __launch_bounds__(256) bev_fixed_to_float_kernel(BeamGeomDev g, const BeamStateDev* __restrict__ beam,
                                                                  unsigned long long* __restrict__ fixed,
                                                                  float* __restrict__ bev, int shiftOffset) {
+    pdl_wait();
     const int planes = min(beam->maxCalcPassive - beam->firstInside, g.steps);
     if (planes <= 0 || beam->liveLo[0] > beam->liveHi[0]) return;
     // bevX is even (the padded ray pitch plus 2 kMaxR), so cells go in aligned pairs.
@@ -689,7 +690,9 @@ cudaError_t launch_superpose(const BeamGeomDev& g, const float* idd, const float
                              cudaStream_t s) {
     cudaError_t e = launch_instances(g, idd, rsigma, work, beam, bevFixed, shiftOffset, numSMs, 0, s);
     if (e != cudaSuccess) return e;
-    bev_fixed_to_float_kernel<<<numSMs * 8, 256, 0, s>>>(g, beam, bevFixed, bev, shiftOffset);
+    e = launch_pdl(bev_fixed_to_float_kernel, dim3(numSMs * 8), dim3(256), 0, s, g,
+                   static_cast<const BeamStateDev*>(beam), bevFixed, bev, shiftOffset);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

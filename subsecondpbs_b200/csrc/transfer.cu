@@ -7,7 +7,9 @@
 // the summed volume gives the same sum up to rounding.
 #include <algorithm>
 
+#include "device_util.cuh"
 #include "kernels.h"
+#include "launch_util.h"
 
 namespace pbs {
 
@@ -105,6 +107,7 @@ __device__ bool plan_transfer_box(const BeamGeomDev& g, int first, int passive, 
 // The beam's transfer box: over the deepest superposed step of all layers, or of
 // `layer` alone when it is given (plan_transfer_box), and the transfer parameters.
 __global__ void transfer_planner_kernel(BeamGeomDev g, BeamStateDev* beam, const LayerStateDev* layer, int live) {
+    pdl_trigger();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     // Last kernel of the beam's work list with one thread: hand the beam's error
     // flags to the context's error word, which outlives the beam state.
@@ -158,6 +161,7 @@ constexpr int kTransferBlocksPerSM = 8;
 __global__ void __launch_bounds__(256)
 transfer_kernel(BeamGeomDev g, const float* __restrict__ bev, const BeamStateDev* __restrict__ beam,
                 double* __restrict__ dose) {
+    pdl_wait();
     if (!beam->transferValid) return;
     const int sx = beam->transferStart[0], sy = beam->transferStart[1], sz = beam->transferStart[2];
     const int mx = beam->transferMax[0], my = beam->transferMax[1], mz = beam->transferMax[2];
@@ -355,7 +359,8 @@ cudaError_t launch_transfer(const BeamGeomDev& g, const float* bev, const BeamSt
     const long long cap = ((static_cast<long long>(g.doseX) * g.doseY) * ((g.doseZ + kTransferZChunk - 1) / kTransferZChunk) +
                            255) / 256;
     const int blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(cap, sms * kTransferBlocksPerSM)));
-    transfer_kernel<<<blocks, 256, 0, s>>>(g, bev, beam, dose);
+    cudaError_t e = launch_pdl(transfer_kernel, dim3(blocks), dim3(256), 0, s, g, bev, beam, dose);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
